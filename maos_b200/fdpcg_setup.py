@@ -1,0 +1,219 @@
+"""Fourier-domain preconditioner (FDPCG) tables.
+
+Restates ``maos/fdpcg.c:331-580`` (``fdpcg_prepare``).  Instead of assembling
+the full sparse Fourier-domain matrix and permuting it, each bs x bs block is
+built directly: a block gathers the layer frequencies that alias to one
+subaperture-grid frequency, and the only couplings between them come from the
+pupil frequencies that alias to the same members.  The block order and the
+member order inside a block are the reference's permutation
+(``fdpcg_perm``, ``maos/fdpcg.c:119``), so ``Mbinv[b]`` here equals the
+reference's ``fdpcg->Mbinv->p[b]`` and ``perm`` its ``fdpcg->perm``.
+
+Per block (complex, ``^H`` = conjugate transpose):
+
+    M = diag(invpsd) + sum_wfs P_w^H diag(|c|^2 (|gx|^2+|gy|^2)) P_w / neam_w^2
+    (scaled by nx*ny when every layer has the same oversampling)
+    Mbinv = pinv(Hermitian part of M), singular values below 1e-7 * max dropped
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class FdpcgTables:
+    bs: int                 # block size = sum(os^2)
+    nb: int                 # number of blocks = adim^2
+    adimx: int
+    adimy: int
+    scale: int              # 1: FFTs are normalised by 1/sqrt(nx*ny) (cfft2s)
+    perm: np.ndarray        # int64 [nb*bs]: index into the natural-order concatenated FFT of x
+    Mbinv: np.ndarray       # complex128 [nb, bs, bs]
+    nxtot: int
+
+
+def _saselect_center(nxp, nyp, dxp, salocx, salocy, saa):
+    """fdpcg_saselect (fdpcg.c:71): the clipped selection spectrum.
+
+    After clipping every coefficient whose magnitude is below the zero
+    frequency one, only the centre survives (checked here), and the
+    convolution operator built from it is that value times a shift, whose
+    effect cancels in sel^H sel."""
+    xsel = np.zeros((nyp, nxp), dtype=np.complex128)
+    offx, offy = nxp // 2, nyp // 2
+    for x, y, a in zip(salocx, salocy, saa):
+        if a > 0.9:
+            ix = int(x / dxp + offx)  # C truncation toward zero
+            iy = int(y / dxp + offy)
+            xsel[iy, ix] = 1.0 / (nxp * nyp)
+    f = np.fft.fftshift(np.fft.fft2(np.fft.fftshift(xsel)))
+    c = f[nyp // 2, nxp // 2].real
+    keep = np.abs(f) >= c
+    if keep.sum() != 1:
+        raise NotImplementedError("FDPCG subaperture selection couples more than one frequency")
+    return c
+
+
+def _fdpcg_g(nx, ny, dx, dsa):
+    """Average-gradient transfer functions gx, gy on the shifted pupil grid (fdpcg.c:199)."""
+    os_ = int(round(dsa / dx))
+    if abs(dsa - dx * os_) > 1e-10:
+        raise ValueError("dsa must be a multiple of dx")
+    wt = np.full(os_ + 1, 1.0 / os_ / dsa)
+    wt[0] = wt[os_] = 0.5 / os_ / dsa
+    st = np.arange(os_ + 1) * dx
+    fy = (np.arange(ny) - ny // 2) / (ny * dx)
+    fx = (np.arange(nx) - nx // 2) / (nx * dx)
+    FY, FX = np.meshgrid(fy, fx, indexing="ij")  # [iy, ix]
+    cf = 2j * math.pi
+    tx = np.zeros((ny, nx), np.complex128)
+    ty = np.zeros((ny, nx), np.complex128)
+    for k in range(os_ + 1):
+        tx += wt[k] * (np.exp(cf * (FX * dsa + FY * st[k])) - np.exp(cf * (FY * st[k])))
+        ty += wt[k] * (np.exp(cf * (FY * dsa + FX * st[k])) - np.exp(cf * (FX * st[k])))
+    return tx, ty
+
+
+def _invpsd_layer(nx, ny, dx, r0, wt, cxxscale, tomoscale):
+    """Spectrum of L2^T L2 for one periodic layer (fdpcg.c:375-403), shifted order."""
+    from .geometry import laplacian_coef
+    cf = laplacian_coef(r0, wt, dx) * math.sqrt(cxxscale * tomoscale)
+    k = np.zeros((ny, nx))
+    # column 0 of L2^T L2 with L2 = cf*(-I + 0.25*(4 neighbours)), periodic
+    for (ox, oy, v) in ((0, 0, 1.25), (1, 0, -0.5), (-1, 0, -0.5), (0, 1, -0.5), (0, -1, -0.5),
+                        (1, 1, 0.125), (1, -1, 0.125), (-1, 1, 0.125), (-1, -1, 0.125),
+                        (2, 0, 0.0625), (-2, 0, 0.0625), (0, 2, 0.0625), (0, -2, 0.0625)):
+        k[oy % ny, ox % nx] += v * cf * cf
+    psd = np.fft.fftshift(np.fft.fft2(k))
+    mx = np.abs(psd.real).max()
+    return psd.real + mx * math.sqrt(2.220446049250313e-16)
+
+
+def block_members(nx, ny, os_, adimx, adimy, shift):
+    """fdpcg_perm (fdpcg.c:119) with half=0: member index lists in block order."""
+    nps = len(nx)
+    noff = np.concatenate([[0], np.cumsum([a * b for a, b in zip(nx, ny)])])
+    out = []
+    blocks = []
+    adimx2 = adimx // 2
+    for ixh in range(2):
+        ix0, ix1 = (-adimx2, 1) if ixh == 0 else (1, adimx2)
+        for iy in range(-(adimy // 2), adimy // 2):
+            for ix in range(ix0, ix1):
+                blocks.append((ix, iy))
+                for ips in range(nps):
+                    for jos in range(os_[ips]):
+                        jy = iy + adimy * jos
+                        if shift:
+                            if jy < 0:
+                                jy += ny[ips]
+                        else:
+                            jy = jy + ny[ips] // 2
+                            if jy >= ny[ips]:
+                                jy -= ny[ips]
+                        for ios in range(os_[ips]):
+                            jx = ix + adimx * ios
+                            if shift:
+                                if jx < 0:
+                                    jx += nx[ips]
+                            else:
+                                jx = jx + nx[ips] // 2
+                                if jx >= nx[ips]:
+                                    jx -= nx[ips]
+                            out.append(noff[ips] + jx + jy * nx[ips])
+    return np.array(out, dtype=np.int64), blocks
+
+
+def fdpcg_prepare(sysm) -> FdpcgTables:
+    from .config import TOMOSCALE
+    cfg = sysm.cfg
+    w0 = sysm.wfs[0]
+    nps = len(sysm.xmaps)
+    pos = cfg.tomo_pos
+    os_ = [int(o) for o in sysm.os]
+    nx = [g.nx for g in sysm.xmaps]
+    ny = [g.ny for g in sysm.xmaps]
+    nxp = nx[0] // os_[0] * pos
+    nyp = ny[0] // os_[0] * pos
+    dxp = sysm.pmap.dx
+    needscale = int(any(o != os_[0] for o in os_))
+    bs = sum(o * o for o in os_)
+    adimx, adimy = nx[0] // os_[0], ny[0] // os_[0]
+    nb = adimx * adimy
+    nxtot = sum(a * b for a, b in zip(nx, ny))
+
+    c = _saselect_center(nxp, nyp, dxp, w0.salocx, w0.salocy, w0.saa)
+    gx, gy = _fdpcg_g(nxp, nyp, dxp, w0.dsa)
+    mmid = (c * c) * (np.abs(gx) ** 2 + np.abs(gy) ** 2)  # [iy, ix] shifted pupil grid
+    invpsd = [_invpsd_layer(nx[i], ny[i], sysm.xmaps[i].dx, cfg.r0, sysm.wt[i],
+                            cfg.tomo_cxxscale, TOMOSCALE) for i in range(nps)]
+    ht = np.array(cfg.atmr_ht, dtype=np.float64)
+    dkx = 1.0 / (nxp * dxp)
+    dky = 1.0 / (nyp * dxp)
+
+    perm0, blocks = block_members(nx, ny, os_, adimx, adimy, shift=0)
+    perm1, _ = block_members(nx, ny, os_, adimx, adimy, shift=1)
+    Mb = np.zeros((nb, bs, bs), dtype=np.complex128)
+    # member descriptors (layer, shifted jx, shifted jy) in block order
+    mem_l = np.concatenate([[ips] * (os_[ips] ** 2) for ips in range(nps)])
+    nxp2, nyp2 = nxp // 2, nyp // 2
+    for b, (ix, iy) in enumerate(blocks):
+        memb = perm0[b * bs:(b + 1) * bs]
+        # decode shifted layer coordinates
+        lj = []
+        for m, l in zip(memb, mem_l):
+            off = sum(nx[k] * ny[k] for k in range(l))
+            r = m - off
+            lj.append((l, r % nx[l], r // nx[l]))
+        M = np.diag([invpsd[l][jy, jx] for (l, jx, jy) in lj]).astype(np.complex128)
+        # pupil frequencies aliasing to this block: centred kx = ix + adimx*m
+        for mxp in range(pos):
+            for myp in range(pos):
+                kx = ix + adimx * mxp
+                ky = iy + adimy * myp
+                kx = (kx + nxp2) % nxp - nxp2
+                ky = (ky + nyp2) % nyp - nyp2
+                pxi, pyi = kx + nxp2, ky + nyp2
+                fxg, fyg = kx * dkx, ky * dky
+                d = mmid[pyi, pxi]
+                if d == 0:
+                    continue
+                for w in sysm.wfs:
+                    v = np.zeros(bs, np.complex128)
+                    for a, (l, jx, jy) in enumerate(lj):
+                        # layer frequency that pupil frequency (kx,ky) maps to
+                        ljx = (kx + nx[l] // 2 + nx[l]) % nx[l]
+                        ljy = (ky + ny[l] // 2 + ny[l]) % ny[l]
+                        if ljx != jx or ljy != jy:
+                            continue
+                        fx = (jx - nx[l] // 2) * dkx
+                        fy = (jy - ny[l] // 2) * dky
+                        dispx = ht[l] * w.thetax
+                        dispy = ht[l] * w.thetay
+                        shiftv = np.exp(2j * math.pi * (fx * dispx + fy * dispy))
+                        ratio = nxp // nx[l]
+                        if ratio in (0, 1):
+                            val = shiftv
+                        elif ratio == 2:
+                            val = shiftv * (1 + math.cos(2 * math.pi * fxg * dxp)) \
+                                * (1 + math.cos(2 * math.pi * fyg * dxp)) * 0.5
+                        else:
+                            raise ValueError("unsupported layer/pupil sampling ratio")
+                        v[a] = val / w.neam
+                    M += np.outer(np.conj(v), v) * d
+        if not needscale:
+            M *= nx[0] * ny[0]
+        M = 0.5 * (M + M.conj().T)
+        M[np.abs(M) < 1e-15] = 0  # cspdroptol(Mhat, EPS), EPS = 1e-15 (sys/common.h:88)
+        U, s, Vh = np.linalg.svd(M)
+        thr = 1e-7 * s[0]
+        si = np.where(s > thr, 1.0 / np.where(s > thr, s, 1.0), 0.0)
+        # reference drops all singular values from the first one under threshold
+        first = np.argmax(s <= thr) if np.any(s <= thr) else len(s)
+        si[first:] = 0.0
+        Mb[b] = (Vh.conj().T * si) @ U.conj().T
+    return FdpcgTables(bs=bs, nb=nb, adimx=adimx, adimy=adimy, scale=needscale,
+                       perm=perm1, Mbinv=Mb, nxtot=nxtot)

@@ -1,0 +1,399 @@
+/*
+ * Flat C driver around the reference MAOS CPU reconstruction -- TEST
+ * INFRASTRUCTURE ONLY.  It is linked into oracle/_ref/libmaosref.so together
+ * with the reference's own sys/, math/, lib/ and maos/ objects (see Makefile)
+ * and lets the Python tests run the reference's functions on exactly the
+ * tables the B200 path consumes:
+ *
+ *   TomoR, TomoL           maos/recon_utils.c:397,447
+ *   fdpcg_prepare          maos/fdpcg.c:331
+ *   fdpcg_precond          maos/fdpcg.c:661
+ *   pcg                    lib/pcg.c:28
+ *   mkg                    lib/mkg.c:470
+ *   dcellpinv (PTT)        used by maos/setup_recon.c:255
+ *   prop_grid_stat         lib/accphi.c + lib/prop_grid.c
+ *
+ * The driver fills only the PARMS_T / RECON_T / POWFS_T fields those
+ * functions read; everything else stays zero.  All arrays crossing this ABI
+ * are plain doubles / ints / longs, column-major like dmat.
+ */
+#include "maos/common.h"
+#include "maos/recon_utils.h"
+#include "maos/fdpcg.h"
+#include "lib/pcg.h"
+#include "lib/mkg.h"
+#include "lib/accphi.h"
+
+typedef struct {
+    int nwfs, nps, nthread;
+    PARMS_T *parms;
+    RECON_T *recon;
+    POWFS_T *powfs;
+    SIM_T *simu;
+    int *nsa;
+    long *goff; /* gradient offsets per wfs */
+    long *xoff; /* x offsets per layer */
+    int finalized;
+} refh_t;
+
+int maosref_driver_version(void) { return 2; }
+
+static map_t *mk_map(int nx, int ny, double dx, double dy, double ox, double oy) {
+    map_t *m = mapnew(nx, ny, dx, dy, NULL);
+    m->ox = ox;
+    m->oy = oy;
+    return m;
+}
+
+static loc_t *mk_square_loc(int nx, int ny, double dx, double dy, double ox, double oy) {
+    map_t *m = mk_map(nx, ny, dx, dy, ox, oy);
+    dset((dmat *)m, 1);
+    loc_t *loc = map2loc(m, 0);
+    mapfree(m);
+    return loc;
+}
+
+void *ref_new(int nwfs, int nps, int nthread) {
+    refh_t *h = calloc(1, sizeof(refh_t));
+    h->nwfs = nwfs;
+    h->nps = nps;
+    h->nthread = nthread > 0 ? nthread : 1;
+    h->parms = calloc(1, sizeof(PARMS_T));
+    h->recon = calloc(1, sizeof(RECON_T));
+    h->powfs = calloc(1, sizeof(POWFS_T));
+    h->simu = calloc(1, sizeof(SIM_T));
+    h->nsa = calloc(nwfs, sizeof(int));
+    h->goff = calloc(nwfs + 1, sizeof(long));
+    h->xoff = calloc(nps + 1, sizeof(long));
+    PARMS_T *parms = h->parms;
+    RECON_T *recon = h->recon;
+    parms->nwfs = parms->nwfsr = nwfs;
+    parms->npowfs = 1;
+    parms->powfs = calloc(1, sizeof(POWFS_CFG_T));
+    parms->wfs = calloc(nwfs, sizeof(WFS_CFG_T));
+    parms->wfsr = parms->wfs;
+    parms->powfs[0].nwfs = parms->powfs[0].nwfsr = nwfs;
+    parms->powfs[0].wfs = lnew(nwfs, 1);
+    parms->powfs[0].wfsr = lnew(nwfs, 1);
+    parms->powfs[0].wfsind = lnew(nwfs, 1);
+    for (int i = 0; i < nwfs; i++) {
+        parms->powfs[0].wfs->p[i] = i;
+        parms->powfs[0].wfsr->p[i] = i;
+        parms->powfs[0].wfsind->p[i] = i;
+    }
+    parms->powfs[0].dtrat = 1;
+    parms->tomo.square = 1;
+    parms->tomo.cxx = 0;
+    parms->tomo.cxxscale = 1;
+    parms->atmr.os = lnew(nps, 1);
+    parms->atmr.ht = dnew(nps, 1);
+    parms->atmr.wt = dnew(nps, 1);
+    parms->atmr.nps = nps;
+    recon->npsr = nps;
+    recon->ht = dnew(nps, 1);
+    recon->wt = dnew(nps, 1);
+    recon->os = dnew(nps, 1);
+    recon->dx = dnew(nps, 1);
+    recon->xloc = loccellnew(nps, 1);
+    recon->xmap = mapcellnew(nps, 1);
+    recon->xnx = lnew(nps, 1);
+    recon->xny = lnew(nps, 1);
+    recon->xnloc = lnew(nps, 1);
+    recon->GP = dspcellnew(nwfs, 1);
+    recon->saneai = dspcellnew(nwfs, nwfs);
+    recon->sanea = dspcellnew(nwfs, nwfs);
+    recon->TT = dcellnew(nwfs, nwfs);
+    recon->neam = dnew(nwfs, 1);
+    recon->nthread = h->nthread;
+    recon->cxx = 0;
+    if (!global) global = calloc(1, sizeof(GLOBAL_T));
+    return h;
+}
+
+void ref_set_system(void *hh, double r0, double cxxscale, double dt, int tomo_pos, int split,
+                    int precond, int maxit) {
+    refh_t *h = hh;
+    h->recon->r0 = r0;
+    h->parms->tomo.cxxscale = cxxscale;
+    h->parms->sim.dt = dt;
+    h->parms->tomo.pos = tomo_pos;
+    h->parms->recon.split = split;
+    h->parms->tomo.precond = precond;
+    h->parms->tomo.maxit = maxit;
+}
+
+void ref_set_pmap(void *hh, int nx, int ny, double dx, double ox, double oy) {
+    refh_t *h = hh;
+    RECON_T *recon = h->recon;
+    recon->ploc = mk_square_loc(nx, ny, dx, dx, ox, oy);
+    loc_create_map_npad(recon->ploc, 0, 0, 0);
+    recon->pmap = recon->ploc->map;
+    loc_create_stat(recon->ploc);
+}
+
+void ref_set_layer(void *hh, int ips, int nx, int ny, double dx, double ox, double oy, double ht,
+                   double wt, int os) {
+    refh_t *h = hh;
+    RECON_T *recon = h->recon;
+    recon->ht->p[ips] = ht;
+    recon->wt->p[ips] = wt;
+    recon->os->p[ips] = os;
+    recon->dx->p[ips] = dx;
+    h->parms->atmr.os->p[ips] = os;
+    h->parms->atmr.ht->p[ips] = ht;
+    h->parms->atmr.wt->p[ips] = wt;
+    recon->xloc->p[ips] = mk_square_loc(nx, ny, dx, dx, ox, oy);
+    recon->xloc->p[ips]->ht = ht;
+    loc_create_stat(recon->xloc->p[ips]);
+    recon->xmap->p[ips] = mk_map(nx, ny, dx, dx, ox, oy);
+    recon->xmap->p[ips]->h = ht;
+    recon->xnx->p[ips] = nx;
+    recon->xny->p[ips] = ny;
+    recon->xnloc->p[ips] = (long)nx * ny;
+}
+
+static dsp *mk_csc(long nrow, long ncol, const int *p, const int *i, const double *x) {
+    long nnz = p[ncol];
+    dsp *A = dspnew(nrow, ncol, nnz);
+    for (long k = 0; k <= ncol; k++) A->p[k] = p[k];
+    for (long k = 0; k < nnz; k++) { A->i[k] = i[k]; A->x[k] = x[k]; }
+    return A;
+}
+
+/* GP is passed in CSC (rows = 2*nsa gradients, cols = pupil points). */
+void ref_set_wfs(void *hh, int iwfs, double thetax, double thetay, double hs, int nsa, double dsa,
+                 const double *salocx, const double *salocy, const double *saa, const int *gp_p,
+                 const int *gp_i, const double *gp_x, const double *saneai, const double *sanea,
+                 int trs) {
+    refh_t *h = hh;
+    PARMS_T *parms = h->parms;
+    RECON_T *recon = h->recon;
+    parms->wfs[iwfs].thetax = thetax;
+    parms->wfs[iwfs].thetay = thetay;
+    parms->wfs[iwfs].hs = hs;
+    parms->wfs[iwfs].powfs = 0;
+    parms->powfs[0].trs = trs;
+    parms->powfs[0].hs = hs;
+    h->nsa[iwfs] = nsa;
+    if (iwfs == 0) {
+        loc_t *saloc = locnew(nsa, dsa, dsa);
+        memcpy(saloc->locx, salocx, sizeof(double) * nsa);
+        memcpy(saloc->locy, salocy, sizeof(double) * nsa);
+        h->powfs[0].saloc = saloc;
+        h->powfs[0].saa = dnew(nsa, 1);
+        memcpy(h->powfs[0].saa->p, saa, sizeof(double) * nsa);
+    }
+    recon->GP->p[iwfs] = mk_csc(2L * nsa, recon->ploc->nloc, gp_p, gp_i, gp_x);
+    recon->saneai->p[iwfs + iwfs * h->nwfs] = dspnewdiag(2L * nsa, (double *)saneai, 1.);
+    recon->sanea->p[iwfs + iwfs * h->nwfs] = dspnewdiag(2L * nsa, (double *)sanea, 1.);
+    if (trs) {
+        dmat *TT = dnew(2L * nsa, 2);
+        for (int isa = 0; isa < nsa; isa++) {
+            TT->p[isa] = 1;
+            TT->p[2L * nsa + nsa + isa] = 1;
+        }
+        recon->TT->p[iwfs + iwfs * h->nwfs] = TT;
+    }
+}
+
+void ref_set_neam(void *hh, int iwfs, double neam) { ((refh_t *)hh)->recon->neam->p[iwfs] = neam; }
+
+int ref_finalize(void *hh) {
+    refh_t *h = hh;
+    PARMS_T *parms = h->parms;
+    RECON_T *recon = h->recon;
+    int nps = h->nps, nwfs = h->nwfs;
+    h->goff[0] = 0;
+    for (int i = 0; i < nwfs; i++) h->goff[i + 1] = h->goff[i] + 2L * h->nsa[i];
+    h->xoff[0] = 0;
+    for (int i = 0; i < nps; i++) h->xoff[i + 1] = h->xoff[i] + recon->xnloc->p[i];
+    /* tip/tilt removal operators (setup_recon.c:255) */
+    int anytt = 0;
+    for (int i = 0; i < nwfs * nwfs; i++) anytt |= recon->TT->p[i] != NULL;
+    if (anytt) {
+        recon->PTT = dcellpinv(recon->TT, recon->saneai);
+        recon->TTF = dcellref(recon->TT);
+        recon->PTTF = dcellref(recon->PTT);
+    }
+    /* biharmonic regularisation (setup_recon.c:291-335), tomo.square=1 */
+    recon->L2 = dspcellnew(nps, nps);
+    for (int ips = 0; ips < nps; ips++) {
+        recon->L2->p[ips + nps * ips] =
+            mklaplacian_map(recon->xmap->p[ips]->nx, recon->xmap->p[ips]->nx,
+                            recon->xloc->p[ips]->dx, recon->r0, recon->wt->p[ips]);
+    }
+    dspcellscale(recon->L2, sqrt(parms->tomo.cxxscale * TOMOSCALE));
+    global->parms = parms;
+    global->recon = recon;
+    global->powfs = h->powfs;
+    global->simu = h->simu;
+    h->finalized = 1;
+    return 0;
+}
+
+/* PTT for one wfs as computed by the reference: 2 x 2nsa column-major */
+int ref_get_ptt(void *hh, int iwfs, double *out) {
+    refh_t *h = hh;
+    if (!h->recon->PTT) return -1;
+    dmat *P = h->recon->PTT->p[iwfs + iwfs * h->nwfs];
+    if (!P) return -1;
+    memcpy(out, P->p, sizeof(double) * P->nx * P->ny);
+    return (int)(P->nx * P->ny);
+}
+
+static dcell *vec2cell(const double *v, const long *off, int n) {
+    dcell *c = dcellnew(n, 1);
+    for (int i = 0; i < n; i++) {
+        c->p[i] = dnew(off[i + 1] - off[i], 1);
+        if (v) memcpy(c->p[i]->p, v + off[i], sizeof(double) * (off[i + 1] - off[i]));
+    }
+    return c;
+}
+static void cell2vec(double *v, const dcell *c, const long *off, int n) {
+    for (int i = 0; i < n; i++) {
+        long len = off[i + 1] - off[i];
+        if (c && c->p[i]) memcpy(v + off[i], c->p[i]->p, sizeof(double) * len);
+        else memset(v + off[i], 0, sizeof(double) * len);
+    }
+}
+
+void ref_tomoR(void *hh, const double *g, double alpha, double *xout) {
+    refh_t *h = hh;
+    dcell *gin = vec2cell(g, h->goff, h->nwfs);
+    dcell *x = vec2cell(NULL, h->xoff, h->nps);
+    TomoR(&x, h->recon, gin, alpha);
+    cell2vec(xout, x, h->xoff, h->nps);
+    dcellfree(gin);
+    dcellfree(x);
+}
+
+void ref_tomoL(void *hh, const double *xin, double alpha, double *xout) {
+    refh_t *h = hh;
+    dcell *x = vec2cell(xin, h->xoff, h->nps);
+    dcell *y = vec2cell(NULL, h->xoff, h->nps);
+    TomoL(&y, h->recon, x, alpha);
+    cell2vec(xout, y, h->xoff, h->nps);
+    dcellfree(x);
+    dcellfree(y);
+}
+
+/* Hx for one wfs: sum over layers of prop_grid_stat onto ploc */
+void ref_hx(void *hh, int iwfs, const double *xin, double *opd) {
+    refh_t *h = hh;
+    RECON_T *recon = h->recon;
+    PARMS_T *parms = h->parms;
+    long np = recon->ploc->nloc;
+    memset(opd, 0, sizeof(double) * np);
+    for (int ips = 0; ips < h->nps; ips++) {
+        double ht = recon->ht->p[ips];
+        map_t xmap;
+        memcpy(&xmap, recon->xmap->p[ips], sizeof(map_t));
+        xmap.p = (double *)xin + h->xoff[ips];
+        double scale = 1. - ht / parms->wfs[iwfs].hs;
+        prop_grid_stat(&xmap, recon->ploc->stat, opd, 1, parms->wfs[iwfs].thetax * ht,
+                       parms->wfs[iwfs].thetay * ht, scale, 0, 0, 0);
+    }
+}
+
+/* Build the reference FDPCG tables from the system. */
+int ref_fdpcg_prepare(void *hh, long *nb, long *bs) {
+    refh_t *h = hh;
+    h->parms->powfs[0].lo = 0;
+    h->parms->powfs[0].skip = 0;
+    h->recon->fdpcg = fdpcg_prepare(h->parms, h->recon, h->powfs, NULL);
+    if (!h->recon->fdpcg) return -1;
+    *nb = h->recon->fdpcg->Mbinv->nx;
+    *bs = h->recon->fdpcg->bs;
+    return h->recon->fdpcg->scale;
+}
+
+/* Export Mbinv (nb blocks of bs x bs complex, column-major, re/im interleaved) and perm. */
+void ref_fdpcg_get(void *hh, double *mbinv, long *perm) {
+    refh_t *h = hh;
+    FDPCG_T *fd = h->recon->fdpcg;
+    long bs = fd->bs;
+    for (long ib = 0; ib < fd->Mbinv->nx; ib++) {
+        cmat *B = fd->Mbinv->p[ib];
+        for (long k = 0; k < bs * bs; k++) {
+            mbinv[2 * (ib * bs * bs + k)] = creal(B->p[k]);
+            mbinv[2 * (ib * bs * bs + k) + 1] = cimag(B->p[k]);
+        }
+    }
+    memcpy(perm, fd->perm->p, sizeof(long) * fd->perm->nx);
+}
+
+/* Install externally built FDPCG tables (same layout as ref_fdpcg_get). */
+void ref_fdpcg_set(void *hh, long nb, long bs, const double *mbinv, const long *perm, int scale) {
+    refh_t *h = hh;
+    FDPCG_T *fd = calloc(1, sizeof(FDPCG_T));
+    fd->bs = bs;
+    fd->scale = scale;
+    fd->square = 1;
+    fd->xloc = h->recon->xloc;
+    fd->nxtot = h->xoff[h->nps];
+    fd->perm = lnew(nb * bs, 1);
+    memcpy(fd->perm->p, perm, sizeof(long) * nb * bs);
+    fd->Mbinv = ccellnew(nb, 1);
+    for (long ib = 0; ib < nb; ib++) {
+        fd->Mbinv->p[ib] = cnew(bs, bs);
+        for (long k = 0; k < bs * bs; k++)
+            fd->Mbinv->p[ib]->p[k] = mbinv[2 * (ib * bs * bs + k)] + I * mbinv[2 * (ib * bs * bs + k) + 1];
+    }
+    h->recon->fdpcg = fd;
+}
+
+void ref_fdpcg_precond(void *hh, const double *r, double *z) {
+    refh_t *h = hh;
+    dcell *rin = vec2cell(r, h->xoff, h->nps);
+    dcell *zout = NULL;
+    fdpcg_precond(&zout, h->recon, rin);
+    cell2vec(z, zout, h->xoff, h->nps);
+    dcellfree(rin);
+    dcellfree(zout);
+}
+
+/* Tomography solve with the reference pcg: x (in/out) warm start. */
+double ref_tomo_pcg(void *hh, const double *b, double *x, int warm, int maxit, int precond) {
+    refh_t *h = hh;
+    dcell *bb = vec2cell(b, h->xoff, h->nps);
+    dcell *xx = vec2cell(x, h->xoff, h->nps);
+    double res = pcg(&xx, TomoL, h->recon, precond ? fdpcg_precond : NULL, h->recon, bb, warm, maxit);
+    cell2vec(x, xx, h->xoff, h->nps);
+    dcellfree(bb);
+    dcellfree(xx);
+    return res;
+}
+
+/* mkg on a square pupil grid (OPD grid = pupil grid). Returns nnz; fills CSC if p != NULL. */
+static dsp *last_gp = NULL;
+long ref_mkg(int nx, int ny, double dx, double ox, double oy, const double *amp, int nsa, double dsa,
+             const double *salocx, const double *salocy) {
+    loc_t *ploc = mk_square_loc(nx, ny, dx, dx, ox, oy);
+    loc_create_map_npad(ploc, 0, 0, 0);
+    dmat *a = dnew(ploc->nloc, 1);
+    memcpy(a->p, amp, sizeof(double) * ploc->nloc);
+    loc_t *saloc = locnew(nsa, dsa, dsa);
+    memcpy(saloc->locx, salocx, sizeof(double) * nsa);
+    memcpy(saloc->locy, salocy, sizeof(double) * nsa);
+    if (last_gp) dspfree(last_gp);
+    last_gp = mkg(ploc, ploc, a, saloc, 1, 0, 0, 1);
+    dfree(a);
+    locfree(saloc);
+    locfree(ploc);
+    return last_gp->p[last_gp->ny];
+}
+void ref_mkg_get(int *p, int *i, double *x, long *nrow, long *ncol) {
+    *nrow = last_gp->nx;
+    *ncol = last_gp->ny;
+    long nnz = last_gp->p[last_gp->ny];
+    for (long k = 0; k <= last_gp->ny; k++) p[k] = last_gp->p[k];
+    for (long k = 0; k < nnz; k++) { i[k] = last_gp->i[k]; x[k] = last_gp->x[k]; }
+}
+
+/* loc ordering check: coordinates of a square loc built like ploc/xloc */
+void ref_loc_coords(int nx, int ny, double dx, double ox, double oy, double *x, double *y) {
+    loc_t *l = mk_square_loc(nx, ny, dx, dx, ox, oy);
+    memcpy(x, l->locx, sizeof(double) * l->nloc);
+    memcpy(y, l->locy, sizeof(double) * l->nloc);
+    locfree(l);
+}

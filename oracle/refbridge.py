@@ -1,0 +1,249 @@
+"""Bridge to the compiled reference CPU path -- TEST INFRASTRUCTURE ONLY.
+
+``oracle/_ref/libmaosref.so`` is the MAOS reference's own CPU reconstruction
+(sys/, math/, lib/, maos/ compiled from its sources by ``oracle/ref/Makefile``)
+plus a flat driver (``oracle/ref/ref_driver.c``).  It is loaded in a separate
+process started with ``spawn``: the reference installs signal handlers and its
+own OpenMP runtime at load time, and it reads ``$HOME``; the worker points
+``HOME`` at ``oracle/_ref/home`` so nothing is written outside the repository.
+
+Only tests, ``smoke()`` and the CPU-baseline leg of ``bench.py`` use this.
+"""
+from __future__ import annotations
+
+import ctypes
+import multiprocessing as mp
+import os
+from typing import Any
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_ref", "libmaosref.so")
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+# --------------------------------------------------------------------------
+# worker side
+# --------------------------------------------------------------------------
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_L = ctypes.POINTER(ctypes.c_long)
+
+
+def _dp(a):
+    return np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(_D)
+
+
+class _Worker:
+    def __init__(self, nthread: int):
+        self.lib = ctypes.CDLL(LIB)
+        L = self.lib
+        L.ref_new.restype = ctypes.c_void_p
+        L.ref_new.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        for name in ("ref_set_system", "ref_set_pmap", "ref_set_layer", "ref_set_wfs", "ref_set_neam",
+                     "ref_finalize", "ref_get_ptt", "ref_tomoR", "ref_tomoL", "ref_hx",
+                     "ref_fdpcg_prepare", "ref_fdpcg_get", "ref_fdpcg_set", "ref_fdpcg_precond",
+                     "ref_tomo_pcg"):
+            getattr(L, name).restype = ctypes.c_int
+        L.ref_tomo_pcg.restype = ctypes.c_double
+        L.ref_mkg.restype = ctypes.c_long
+        self.nthread = nthread
+        self.h = None
+        self.keep = []
+
+    def setup(self, d):
+        L = self.lib
+        h = L.ref_new(d["nwfs"], d["nps"], self.nthread)
+        self.h = ctypes.c_void_p(h)
+        L.ref_set_system(self.h, ctypes.c_double(d["r0"]), ctypes.c_double(d["cxxscale"]),
+                         ctypes.c_double(d["dt"]), d["pos"], d["split"], d["precond"], d["maxit"])
+        p = d["pmap"]
+        L.ref_set_pmap(self.h, p[0], p[1], ctypes.c_double(p[2]), ctypes.c_double(p[3]),
+                       ctypes.c_double(p[4]))
+        for i, lay in enumerate(d["layers"]):
+            nx, ny, dx, ox, oy, ht, wt, os_ = lay
+            L.ref_set_layer(self.h, i, nx, ny, ctypes.c_double(dx), ctypes.c_double(ox),
+                            ctypes.c_double(oy), ctypes.c_double(ht), ctypes.c_double(wt), os_)
+        for i, w in enumerate(d["wfs"]):
+            arrs = [np.ascontiguousarray(w[k], dtype=np.float64) for k in
+                    ("salocx", "salocy", "saa", "gp_x", "saneai", "sanea")]
+            gp_p = np.ascontiguousarray(w["gp_p"], dtype=np.int32)
+            gp_i = np.ascontiguousarray(w["gp_i"], dtype=np.int32)
+            self.keep += arrs + [gp_p, gp_i]
+            L.ref_set_wfs(self.h, i, ctypes.c_double(w["thetax"]), ctypes.c_double(w["thetay"]),
+                          ctypes.c_double(w["hs"]), w["nsa"], ctypes.c_double(w["dsa"]),
+                          arrs[0].ctypes.data_as(_D), arrs[1].ctypes.data_as(_D),
+                          arrs[2].ctypes.data_as(_D), gp_p.ctypes.data_as(_I),
+                          gp_i.ctypes.data_as(_I), arrs[3].ctypes.data_as(_D),
+                          arrs[4].ctypes.data_as(_D), arrs[5].ctypes.data_as(_D), int(w["trs"]))
+            L.ref_set_neam(self.h, i, ctypes.c_double(w["neam"]))
+        L.ref_finalize(self.h)
+        self.nx = d["nxtot"]
+        self.ng = d["ngrad"]
+        self.np = d["pmap"][0] * d["pmap"][1]
+        self.nsa = [w["nsa"] for w in d["wfs"]]
+        return True
+
+    def ptt(self, iwfs):
+        out = np.zeros(4 * self.nsa[iwfs])
+        n = self.lib.ref_get_ptt(self.h, iwfs, out.ctypes.data_as(_D))
+        return None if n < 0 else out.reshape(2, 2 * self.nsa[iwfs], order="F").copy()
+
+    def tomoR(self, g, alpha=1.0):
+        out = np.zeros(self.nx)
+        self.lib.ref_tomoR(self.h, _dp(g), ctypes.c_double(alpha), out.ctypes.data_as(_D))
+        return out
+
+    def tomoL(self, x, alpha=1.0):
+        out = np.zeros(self.nx)
+        self.lib.ref_tomoL(self.h, _dp(x), ctypes.c_double(alpha), out.ctypes.data_as(_D))
+        return out
+
+    def hx(self, iwfs, x):
+        out = np.zeros(self.np)
+        self.lib.ref_hx(self.h, iwfs, _dp(x), out.ctypes.data_as(_D))
+        return out
+
+    def fdpcg_prepare(self):
+        nb = ctypes.c_long(0)
+        bs = ctypes.c_long(0)
+        scale = self.lib.ref_fdpcg_prepare(self.h, ctypes.byref(nb), ctypes.byref(bs))
+        nb, bs = nb.value, bs.value
+        mb = np.zeros(nb * bs * bs * 2)
+        perm = np.zeros(nb * bs, dtype=np.int64)
+        self.lib.ref_fdpcg_get(self.h, mb.ctypes.data_as(_D), perm.ctypes.data_as(_L))
+        mbc = (mb[0::2] + 1j * mb[1::2]).reshape(nb, bs, bs).transpose(0, 2, 1)  # col-major blocks
+        return {"scale": scale, "Mbinv": mbc, "perm": perm}
+
+    def fdpcg_set(self, Mbinv, perm, scale):
+        nb, bs, _ = Mbinv.shape
+        cm = np.ascontiguousarray(Mbinv.transpose(0, 2, 1)).ravel()
+        mb = np.empty(cm.size * 2)
+        mb[0::2] = cm.real
+        mb[1::2] = cm.imag
+        pm = np.ascontiguousarray(perm, dtype=np.int64)
+        self.keep += [mb, pm]
+        self.lib.ref_fdpcg_set(self.h, ctypes.c_long(nb), ctypes.c_long(bs), mb.ctypes.data_as(_D),
+                               pm.ctypes.data_as(_L), int(scale))
+        return True
+
+    def fdpcg_precond(self, r):
+        out = np.zeros(self.nx)
+        self.lib.ref_fdpcg_precond(self.h, _dp(r), out.ctypes.data_as(_D))
+        return out
+
+    def pcg(self, b, x0, warm, maxit, precond):
+        x = np.array(x0, dtype=np.float64) if x0 is not None else np.zeros(self.nx)
+        res = self.lib.ref_tomo_pcg(self.h, _dp(b), x.ctypes.data_as(_D), int(warm), int(maxit),
+                                    int(precond))
+        return x, res
+
+    def mkg(self, grid, amp, salocx, salocy, dsa):
+        L = self.lib
+        nnz = L.ref_mkg(grid[0], grid[1], ctypes.c_double(grid[2]), ctypes.c_double(grid[3]),
+                        ctypes.c_double(grid[4]), _dp(amp), len(salocx), ctypes.c_double(dsa),
+                        _dp(salocx), _dp(salocy))
+        ncol = grid[0] * grid[1]
+        p = np.zeros(ncol + 1, dtype=np.int32)
+        i = np.zeros(nnz, dtype=np.int32)
+        x = np.zeros(nnz)
+        nr = ctypes.c_long(0)
+        nc = ctypes.c_long(0)
+        L.ref_mkg_get(p.ctypes.data_as(_I), i.ctypes.data_as(_I), x.ctypes.data_as(_D),
+                      ctypes.byref(nr), ctypes.byref(nc))
+        return p, i, x, nr.value, nc.value
+
+    def loc_coords(self, grid):
+        n = grid[0] * grid[1]
+        x = np.zeros(n)
+        y = np.zeros(n)
+        self.lib.ref_loc_coords(grid[0], grid[1], ctypes.c_double(grid[2]), ctypes.c_double(grid[3]),
+                                ctypes.c_double(grid[4]), x.ctypes.data_as(_D), y.ctypes.data_as(_D))
+        return x, y
+
+
+def _serve(conn, nthread):
+    w = _Worker(nthread)
+    while True:
+        msg = conn.recv()
+        if msg is None:
+            break
+        name, args, kw = msg
+        try:
+            conn.send(("ok", getattr(w, name)(*args, **kw)))
+        except Exception as e:  # pragma: no cover - surfaced to the caller
+            conn.send(("err", repr(e)))
+
+
+class RefProcess:
+    """Handle on a worker process holding the reference library."""
+
+    def __init__(self, nthread: int = 1):
+        if not available():
+            raise FileNotFoundError(f"{LIB} not built (make -C oracle/ref)")
+        ctx = mp.get_context("spawn")
+        self.conn, child = ctx.Pipe()
+        home = os.path.join(HERE, "_ref", "home")
+        os.makedirs(os.path.join(home, ".aos", "cache"), exist_ok=True)
+        env_backup = {k: os.environ.get(k) for k in ("HOME", "USER", "OMP_NUM_THREADS")}
+        os.environ["HOME"] = home
+        os.environ["USER"] = "maosref"
+        os.environ["OMP_NUM_THREADS"] = str(nthread)
+        try:
+            self.proc = ctx.Process(target=_serve, args=(child, nthread), daemon=True)
+            self.proc.start()
+        finally:
+            for k, v in env_backup.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+
+    def call(self, name: str, *args, **kw) -> Any:
+        self.conn.send((name, args, kw))
+        st, val = self.conn.recv()
+        if st != "ok":
+            raise RuntimeError(f"reference call {name} failed: {val}")
+        return val
+
+    def close(self):
+        try:
+            self.conn.send(None)
+        except Exception:
+            pass
+        self.proc.join(timeout=10)
+        if self.proc.is_alive():
+            self.proc.kill()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def system_desc(sysm, split: int = 1) -> dict:
+    """Flatten a TomoSystem into the driver's setup arguments."""
+    cfg = sysm.cfg
+    d = {"nwfs": len(sysm.wfs), "nps": len(sysm.xmaps), "r0": cfg.r0,
+         "cxxscale": cfg.tomo_cxxscale, "dt": cfg.sim_dt, "pos": cfg.tomo_pos, "split": split,
+         "precond": cfg.tomo_precond, "maxit": cfg.tomo_maxit, "nxtot": sysm.nx_total,
+         "ngrad": sysm.ngrad}
+    p = sysm.pmap
+    d["pmap"] = (p.nx, p.ny, p.dx, p.ox, p.oy)
+    d["layers"] = [(g.nx, g.ny, g.dx, g.ox, g.oy, float(sysm.ht[l]), float(sysm.wt[l]),
+                    int(sysm.os[l])) for l, g in enumerate(sysm.xmaps)]
+    ws = []
+    for w in sysm.wfs:
+        G = w.GP.tocsc()
+        G.sort_indices()
+        ws.append({"thetax": w.thetax, "thetay": w.thetay, "hs": w.hs, "nsa": w.nsa, "dsa": w.dsa,
+                   "salocx": w.salocx, "salocy": w.salocy, "saa": w.saa, "gp_p": G.indptr,
+                   "gp_i": G.indices, "gp_x": G.data, "saneai": w.saneai, "sanea": w.sanea,
+                   "trs": w.trs, "neam": w.neam})
+    d["wfs"] = ws
+    return d

@@ -1,0 +1,94 @@
+"""Pin the FP64 oracle against the reference's own compiled CPU path.
+
+The reference (sys/, math/, lib/, maos/ of MAOS) is built by
+``oracle/ref/Makefile`` into ``oracle/_ref/libmaosref.so``; these tests run its
+``TomoR``/``TomoL``/``fdpcg_prepare``/``fdpcg_precond``/``pcg``/``mkg``/
+``dcellpinv`` on the same tables as the oracle and require agreement to FP64
+round-off.
+"""
+import numpy as np
+import pytest
+
+from oracle import refbridge
+from oracle.recon_oracle import TomoOracle, pcg
+
+pytestmark = [pytest.mark.ref,
+              pytest.mark.skipif(not refbridge.available(), reason="reference library not built")]
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def ref_proc():
+    with refbridge.RefProcess(nthread=4) as R:
+        yield R
+
+
+@pytest.mark.parametrize("name", ["ltao_8m", "mcao_30m"])
+@pytest.mark.parametrize("split", [1, 0])
+def test_tomo_operators_match_reference(name, split, ref_proc):
+    from conftest import get_system
+    s = get_system(name)
+    R = ref_proc
+    R.call("setup", refbridge.system_desc(s, split=split))
+    o = TomoOracle(s, split=split)
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal(s.nx_total)
+    g = rng.standard_normal(s.ngrad)
+    # pupil/layer grids are stored like the reference's loc_t (x fastest)
+    px, py = R.call("loc_coords", (s.pmap.nx, s.pmap.ny, s.pmap.dx, s.pmap.ox, s.pmap.oy))
+    assert np.allclose(px, np.tile(s.pmap.xs(), s.pmap.ny))
+    assert np.allclose(py, np.repeat(s.pmap.ys(), s.pmap.nx))
+    for iw, w in enumerate(s.wfs):
+        assert rel(o.hx(x)[iw], R.call("hx", iw, x)) < 1e-12
+        if w.PTT is not None:
+            assert rel(w.PTT, R.call("ptt", iw)) < 1e-12
+    assert rel(o.tomo_R(g), R.call("tomoR", g)) < 1e-12
+    assert rel(o.tomo_L(x), R.call("tomoL", x)) < 1e-12
+    assert rel(o.tomo_L(x, alpha=-0.5), R.call("tomoL", x, -0.5)) < 1e-12
+
+
+def test_fdpcg_tables_and_apply_match_reference(ref_proc, mcao):
+    s = mcao
+    R = ref_proc
+    R.call("setup", refbridge.system_desc(s, split=1))
+    fd = R.call("fdpcg_prepare")
+    assert fd["scale"] == s.fdpcg.scale
+    assert np.array_equal(fd["perm"], s.fdpcg.perm)
+    assert rel(s.fdpcg.Mbinv, fd["Mbinv"]) < 1e-8  # SVD pseudo-inverses, FP64
+    R.call("fdpcg_set", s.fdpcg.Mbinv, s.fdpcg.perm, s.fdpcg.scale)
+    o = TomoOracle(s)
+    r = np.random.default_rng(5).standard_normal(s.nx_total)
+    assert rel(o.fdpcg_precond(r), R.call("fdpcg_precond", r)) < 1e-12
+
+
+@pytest.mark.parametrize("name,warm", [("ltao_8m", False), ("mcao_30m", False), ("mcao_30m", True)])
+def test_pcg_matches_reference(name, warm, ref_proc):
+    from conftest import get_system
+    s = get_system(name)
+    R = ref_proc
+    R.call("setup", refbridge.system_desc(s, split=1))
+    if s.fdpcg is not None:
+        R.call("fdpcg_set", s.fdpcg.Mbinv, s.fdpcg.perm, s.fdpcg.scale)
+    o = TomoOracle(s)
+    rng = np.random.default_rng(7)
+    b = o.tomo_R(rng.standard_normal(s.ngrad))
+    x0 = rng.standard_normal(s.nx_total) * 1e-3 if warm else None
+    M = o.fdpcg_precond if s.fdpcg is not None else None
+    x1, r1 = pcg(x0, o.tomo_L, M, b, warm, s.cfg.tomo_maxit)
+    x2, r2 = R.call("pcg", b, x0, int(warm), s.cfg.tomo_maxit, int(s.fdpcg is not None))
+    assert rel(x1, x2) < 1e-10
+    assert abs(r1 - r2) <= 1e-10 * abs(r2)
+
+
+def test_gradient_operator_matches_reference_mkg(ref_proc, ltao):
+    s = ltao
+    w = s.wfs[0]
+    p, i, x, nr, nc = ref_proc.call("mkg", (s.pmap.nx, s.pmap.ny, s.pmap.dx, s.pmap.ox, s.pmap.oy),
+                                    s.amp, w.salocx, w.salocy, w.dsa)
+    import scipy.sparse as sps
+    G = sps.csc_matrix((x, i, p), shape=(nr, nc)).toarray()
+    assert G.shape == w.GP.shape
+    assert np.abs(G - w.GP.toarray()).max() <= 1e-12 * np.abs(G).max()
