@@ -1,0 +1,344 @@
+"""Benchmark of the per-step wavefront reconstruction on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl reference]
+
+Workload (one "step"): the 30 m NFIRAOS-like MCAO system (6 LGS, 60x60
+subapertures, 33,840 gradients, 6 layers / 27,648 unknowns), seeded
+frozen-flow von Karman gradients in, warm-started FP32 FDPCG tomography with
+30 iterations out, for B independent instances resident on each GPU.  The
+instances share the operator tables and advance together in one CUDA graph.
+
+value     aggregate steps/s over all GPUs (N * B * K / max-over-ranks device time),
+          inputs resident in HBM, L2 flushed (256 MiB write) before every step.
+e2e       the same metric through the host API mb_tomo (FP64 host gradients in,
+          FP64 host layer OPD out, copies inside the timed region).
+roofline  the kernel with the largest share of the step, its algorithmic bytes
+          per launch over its measured launch time, against the measured HBM
+          copy bandwidth.
+cpu_baseline  the reference's own CPU reconstruction (compiled from its
+          sources into oracle/_ref) timed on this host's cores on a bounded
+          sample of the same workload.
+
+Multi-GPU (--gpus N, launched by torch.distributed.run): every rank owns its
+own B instances (weak scaling; no data-path collective), ranks meet at a
+barrier around the timed region and the slowest rank's time is used.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+WORKLOAD = "mcao_30m"
+METRIC = "recon steps/s (FP32 FDPCG tomography, 30 iterations, 30 m MCAO)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str, batch: int):
+    """DRAM bytes per launch from the committed ncu summary, scaled to `batch`."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic_per_launch.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = line.split()
+        if len(f) >= 3 and not line.startswith("#") and f[0] == kernel:
+            b0, by = int(f[1]), float(f[2])
+            return by * batch / b0
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.p is None:
+            return out
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        out["sm_mhz"] = statistics.median(sm) if sm else None
+        out["sm_max_mhz"] = max(mx) if mx else None
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(rows)
+        return out
+
+
+class RefRunner:
+    """The reference's own CPU reconstruction (oracle/_ref) on this host's cores."""
+
+    def __init__(self, sysm, frames):
+        from oracle import refbridge
+        self.ncores = os.cpu_count() or 1
+        self.frames = frames
+        self.maxit = sysm.cfg.tomo_maxit
+        self.R = refbridge.RefProcess(nthread=self.ncores)
+        self.R.call("setup", refbridge.system_desc(sysm, split=1))
+        self.R.call("fdpcg_set", sysm.fdpcg.Mbinv, sysm.fdpcg.perm, sysm.fdpcg.scale)
+        self.x = None
+        self.k = 0
+
+    def step(self):
+        g = self.frames[self.k % len(self.frames)]
+        b = self.R.call("tomoR", g)
+        self.x, _ = self.R.call("pcg", b, self.x, int(self.x is not None), self.maxit, 1)
+        self.k += 1
+
+    def rate(self, seconds: float):
+        """Run warm steps for about `seconds`; returns (steps/s, steps, elapsed)."""
+        n = 0
+        t0 = time.perf_counter()
+        while True:
+            self.step()
+            n += 1
+            dt = time.perf_counter() - t0
+            if dt >= seconds or n >= 1000:
+                return n / dt, n, dt
+
+    def close(self):
+        self.R.close()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from maos_b200 import config, geometry, turbulence
+    sysm = geometry.build_tomo(config.PRESETS[WORKLOAD]())
+    frames = turbulence.gradient_frames(sysm, seed=1, nframe=4)
+    run = RefRunner(sysm, frames)
+    for _ in range(max(1, args.warmup)):
+        run.step()
+    per = args.cpu_seconds / max(1, args.steps)
+    rates = []
+    total = 0
+    for _ in range(args.steps):
+        r, n, _dt = run.rate(per)
+        rates.append(r)
+        total += n
+    run.close()
+    value = statistics.median(rates)
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded von Karman frozen-flow gradients)",
+            "config": {"workload": f"{WORKLOAD} FDPCG tomography, 30 iterations, warm start",
+                       "instances": 1},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": run.ncores, "kind": "reference",
+                             "sample": f"{total} warm reference CPU steps in {args.steps} samples"},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+    from maos_b200 import config, geometry, native, turbulence
+    from maos_b200.recon import Reconstructor
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    sysm = geometry.build_tomo(config.PRESETS[WORKLOAD]())
+    B = args.batch
+    nframe = 4
+    # gradients: 4 frozen-flow frames for each of 4 seeds, tiled over instances
+    seeds = [1 + 101 * rank + k for k in range(4)]
+    fr = np.stack([turbulence.gradient_frames(sysm, seed=s, nframe=nframe) for s in seeds])
+    grads = np.stack([np.stack([fr[b % len(seeds), k] for b in range(B)]) for k in range(nframe)])
+    grads_dev = torch.tensor(grads, dtype=torch.float32, device="cuda")  # [nframe][B][ngrad]
+    host_grads = [np.ascontiguousarray(grads[k]) for k in range(nframe)]
+
+    lib = native.load()
+    R = Reconstructor(sysm, nbatch=B, device=local)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step(k):
+        R.tomo_device(grads_dev[k % nframe].data_ptr(), sp)
+
+    with torch.cuda.stream(stream):
+        for k in range(args.warmup):
+            step(k)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    lib.mb_kernel_launches(1)
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            step(k)
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    launches = lib.mb_kernel_launches(1)
+    clocks = clk.stop()
+    times = [a.elapsed_time(b) for a, b in ev]
+    total = sum(times)
+    t = torch.tensor([total], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_max = float(t.item())
+    value = world * B * args.steps / (total_max / 1000.0)
+    times_sorted = sorted(times)
+    p50 = statistics.median(times)
+    p99 = times_sorted[min(len(times) - 1, int(math.ceil(0.99 * len(times))) - 1)]
+
+    # end to end through the host API (FP64 host gradients in, FP64 OPD out)
+    K2 = max(3, min(args.steps, 20))
+    for k in range(2):
+        R.tomo(host_grads[k % nframe])
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(K2):
+        R.tomo(host_grads[k % nframe])
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * B * K2 / float(te.item())
+
+    # roofline of the dominant kernel (live timing on the reconstructor's stream)
+    ns = lib.mb_num_stages()
+    import ctypes as C
+    ms = (C.c_float * ns)()
+    by = (C.c_double * ns)()
+    lp = (C.c_int * ns)()
+    native.check(lib.mb_time_stages(R.h, 20, ms, by, lp), "mb_time_stages")
+    stages = []
+    for i in range(ns):
+        stages.append({"name": lib.mb_stage_name(i).decode(), "ms": ms[i], "bytes": by[i],
+                       "launches": lp[i], "share_ms": ms[i] * lp[i]})
+    tot_stage = sum(s["share_ms"] for s in stages) or 1.0
+    dom = max(stages, key=lambda s: s["share_ms"])
+    peak, peak_kind = measured_peaks()
+    achieved = dom["bytes"] / (dom["ms"] / 1000.0) / 1e9
+    roof = {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+            "traffic": ncu_traffic(dom["name"], B),
+            "share_of_step": dom["share_ms"] / tot_stage,
+            "stage_ms_per_step": {s["name"]: round(s["share_ms"], 4) for s in stages}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import refbridge
+        if refbridge.available():
+            run = RefRunner(sysm, fr[0])
+            run.step()
+            rate, n, dt = run.rate(args.cpu_seconds)
+            run.close()
+            cpu = {"value": rate, "unit": "steps/s", "cores": run.ncores, "kind": "reference",
+                   "sample": f"{n} warm steps of one {WORKLOAD} instance in {dt:.1f} s"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded von Karman frozen-flow gradients, 4 seeds x 4 frames)",
+                "config": {"workload": f"{WORKLOAD} FDPCG tomography, 30 iterations, warm start",
+                           "instances_per_gpu": B, "ngrad": int(sysm.ngrad),
+                           "nxtot": int(sysm.nx_total), "l2": "flushed before every step (256 MiB write)",
+                           "parallelism": f"replicas x{world}"},
+                "latency_ms": {"p50": p50, "p99": p99, "note": "one batched step of all instances"},
+                "e2e": {"value": e2e_value, "unit": "steps/s",
+                        "h2d_bytes_per_step": int(B * sysm.ngrad * 4),
+                        "d2h_bytes_per_step": int(B * sysm.nx_total * 4 + B * 4)},
+                "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    R.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,908 @@
+// Host side of the tomography reconstructor: table preparation, buffers,
+// the CG/FDPCG schedule captured in one CUDA graph, and the C ABI
+// (include/maos_b200.h).
+//
+// Table preparation mirrors what the reference does when it copies RECON_T to
+// the GPU (cuda/tomo.cu:30-139 prep_GP/prep_saptr/convert_neai,
+// cuda/prop_wrap.cu:357 gpu_map2map_prep), with two differences chosen for
+// parity with the reference CPU path: GP is kept exactly (FP32 stencil
+// coefficients, not short2-quantised) and every transpose is the exact
+// transpose of the forward table, evaluated in gather form.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <atomic>
+#include <vector>
+
+#include "common.cuh"
+#include "tomo_kernels.cuh"
+
+namespace mb {
+
+static thread_local char g_err[1024] = "";
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+const char *last_error() { return g_err; }
+static std::atomic<long> g_launches{0};
+void count_launches(long n) { g_launches += n; }
+
+static inline unsigned nblocks(long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
+
+struct CufftError {};
+#define MB_CUFFT_TRY(call)                                                          \
+    do {                                                                            \
+        cufftResult r_ = (call);                                                    \
+        if (r_ != CUFFT_SUCCESS) {                                                  \
+            mb::set_error("%s:%d %s: cufft error %d", __FILE__, __LINE__, #call, (int)r_); \
+            throw mb::CudaError{MB_ECUDA};                                          \
+        }                                                                           \
+    } while (0)
+
+struct Recon {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int nb = 1;  // batch
+    int nwfs = 0, nps = 0, nxp = 0, nyp = 0, np = 0;
+    long nxtot = 0, ngrad = 0;
+    int maxit = 0, precond = 0, split = 1;
+    int nsc = 0;            // scalars per instance
+    int nblk_x = 0;         // blocks over nxtot
+    int nblk_tt = 0;        // blocks over the largest nsa
+    std::vector<long> xoff, goff;
+    std::vector<int> nsa;
+
+    // tables
+    DevBuf<AxisW> hx_tab;
+    DevBuf<LayerDev> lay;
+    std::vector<LayerDev> lay_h;
+    DevBuf<int> gi_ptr, gi_idxptr;
+    DevBuf<GatherW> gi_ent;
+    DevBuf<WfsDev> wfs;
+    std::vector<std::unique_ptr<DevBuf<int2>>> saptr;
+    std::vector<std::unique_ptr<DevBuf<float2>>> gp;
+    std::vector<std::unique_ptr<DevBuf<int>>> samap;
+    std::vector<std::unique_ptr<DevBuf<float>>> neai, ptt;
+    std::vector<WfsDev> wfs_h;
+    // FDPCG
+    int fd_nb = 0, fd_bs = 0;
+    DevBuf<cufftComplex> fd_M;
+    DevBuf<FdIndex> fd_idx;
+    DevBuf<int> fd_soff;
+    std::vector<cufftHandle> plans;
+    std::vector<long> plan_off;   // element offset of each plan's first slab
+    DevBuf<cufftComplex> spec, spec2;
+
+    // state and work buffers
+    DevBuf<float> x, r, p, z, Ap, rhs, opd, opd2, grad, gin;
+    DevBuf<double> tt_part, pap_part, rr_part, rz_part, bb_part, sc;
+    DevBuf<float> res;
+
+    cudaGraphExec_t graph = nullptr;
+    long graph_kernels = 0;
+
+    ~Recon() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (auto h : plans) cufftDestroy(h);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    // ------------------------------------------------------------------
+    void build(const mb_tomo_desc *d);
+    void build_hx_tables(const mb_tomo_desc *d);
+    void build_wfs_tables(const mb_tomo_desc *d);
+    void build_fdpcg(const mb_fdpcg_desc *fd);
+    void set_neai(int iwfs, const double *neai, const double *ptt);
+    void set_l2c(const double *l2c);
+
+    // operator pieces (enqueue on `s`)
+    void op_hx(const float *xin, cudaStream_t s);
+    void op_rhs(const float *g, float *out, cudaStream_t s);
+    void op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t s);
+    void op_fdpcg(const float *rin, float *zout, double *rz_part, cudaStream_t s);
+    void enqueue_solve(cudaStream_t s);
+    void time_stages(int reps, float *ms, double *bytes, int *launches);
+    void capture_graph();
+    void run_graph(cudaStream_t s);
+};
+
+// ---------------------------------------------------------------------------
+// tables
+// ---------------------------------------------------------------------------
+
+// Bilinear weights of one axis: pupil coordinate c maps to layer index
+// u = (c*scale + disp - o)/d.  Same inclusion rule as the reference CPU ray
+// tracer (lib/prop_grid.c): 0 <= u <= n-1, a point on the last sample uses
+// that sample alone.
+static void axis_weights(const mb_grid &pm, int n_out, double o_out, double d_out, bool isy,
+                         double scale, double disp, const mb_grid &g, std::vector<AxisW> &out) {
+    const double o_in = isy ? g.oy : g.ox, d_in = isy ? g.dy : g.dx;
+    const int n_in = isy ? g.ny : g.nx;
+    (void)pm;
+    for (int i = 0; i < n_out; i++) {
+        const double c = o_out + i * d_out;
+        const double u = (c * scale + disp - o_in) / d_in;
+        long k = (long)std::floor(u);
+        double f = u - k;
+        if (k == n_in - 1 && f < 1e-12) {
+            k = n_in - 2;
+            f = 1.0;
+        }
+        AxisW e;
+        if (u >= 0 && k >= 0 && k <= n_in - 2) {
+            e.k = (int)k;
+            e.w0 = (float)(1.0 - f);
+            e.w1 = (float)f;
+        } else {
+            e.k = -1;
+            e.w0 = e.w1 = 0.f;
+        }
+        out.push_back(e);
+    }
+}
+
+void Recon::build_hx_tables(const mb_tomo_desc *d) {
+    const mb_grid &pm = d->pmap;
+    std::vector<AxisW> tab;
+    tab.reserve((size_t)nwfs * nps * (nxp + nyp));
+    for (int w = 0; w < nwfs; w++) {
+        const mb_wfs_desc &W = d->wfs[w];
+        for (int l = 0; l < nps; l++) {
+            const mb_grid &g = d->xmap[l];
+            const double ht = g.ht;
+            const double scale = std::isinf(W.hs) ? 1.0 : 1.0 - ht / W.hs;
+            axis_weights(pm, nxp, pm.ox, pm.dx, false, scale, W.thetax * ht, g, tab);
+            axis_weights(pm, nyp, pm.oy, pm.dy, true, scale, W.thetay * ht, g, tab);
+        }
+    }
+    hx_tab.upload(tab);
+    // transposed tables: for each (w, l, axis) a CSR over layer indices
+    std::vector<int> ptr, idxptr;
+    std::vector<GatherW> ent;
+    for (int w = 0; w < nwfs; w++) {
+        for (int l = 0; l < nps; l++) {
+            const AxisW *t = tab.data() + (size_t)(w * nps + l) * (nxp + nyp);
+            for (int axis = 0; axis < 2; axis++) {
+                const int n_in = axis ? d->xmap[l].ny : d->xmap[l].nx;
+                const int n_out = axis ? nyp : nxp;
+                const AxisW *ta = t + (axis ? nxp : 0);
+                ptr.push_back((int)idxptr.size());
+                std::vector<std::vector<GatherW>> lists(n_in);
+                for (int i = 0; i < n_out; i++) {
+                    if (ta[i].k < 0) continue;
+                    lists[ta[i].k].push_back(GatherW{i, ta[i].w0});
+                    lists[ta[i].k + 1].push_back(GatherW{i, ta[i].w1});
+                }
+                for (int j = 0; j < n_in; j++) {
+                    idxptr.push_back((int)ent.size());
+                    for (auto &e : lists[j]) ent.push_back(e);
+                }
+                idxptr.push_back((int)ent.size());
+            }
+        }
+    }
+    // ptr[] points at the start of each CSR's row-pointer block
+    gi_ptr.upload(ptr);
+    gi_idxptr.upload(idxptr);
+    gi_ent.upload(ent);
+}
+
+void Recon::build_wfs_tables(const mb_tomo_desc *d) {
+    const mb_grid &pm = d->pmap;
+    wfs_h.resize(nwfs);
+    for (int w = 0; w < nwfs; w++) {
+        const mb_wfs_desc &W = d->wfs[w];
+        const int ns = W.nsa;
+        MB_REQUIRE(ns > 0 && W.salocx && W.salocy && W.gp_p && W.gp_i && W.gp_x && W.neai,
+                   "wfs %d: missing arrays", w);
+        const double posd = W.dsa / pm.dx;
+        const int pos = (int)std::lround(posd);
+        if (!(pos == 1 || pos == 2) || std::fabs(posd - pos) > 1e-9) {
+            set_error("wfs %d: subaperture/pupil sampling ratio %g is not 1 or 2", w, posd);
+            throw InvalidArg{MB_EUNSUP};
+        }
+        const int n1 = pos + 1;
+        // share tables between WFS that pass identical arrays (like tomo.cu:259-276)
+        int share = -1;
+        for (int v = 0; v < w; v++) {
+            const mb_wfs_desc &V = d->wfs[v];
+            if (V.gp_x == W.gp_x && V.gp_p == W.gp_p && V.salocx == W.salocx && V.nsa == ns &&
+                V.dsa == W.dsa)
+                share = v;
+        }
+        std::vector<int2> sp(ns);
+        std::vector<float2> coef((size_t)ns * n1 * n1, make_float2(0.f, 0.f));
+        if (share < 0) {
+            std::vector<int> sm(np, -1);
+            for (int s = 0; s < ns; s++) {
+                const long ix = std::lround((W.salocx[s] - pm.ox) / pm.dx);
+                const long iy = std::lround((W.salocy[s] - pm.oy) / pm.dy);
+                MB_REQUIRE(ix >= 0 && iy >= 0 && ix + pos < nxp && iy + pos < nyp,
+                           "wfs %d subaperture %d lies outside the pupil grid", w, s);
+                sp[s] = make_int2((int)ix, (int)iy);
+                MB_REQUIRE(sm[iy * nxp + ix] < 0, "wfs %d: two subapertures share a corner", w);
+                sm[iy * nxp + ix] = s;
+            }
+            // GP in CSC: columns are pupil points, rows gradients
+            for (int col = 0; col < np; col++) {
+                const int px = col % nxp, py = col / nxp;
+                for (int k = W.gp_p[col]; k < W.gp_p[col + 1]; k++) {
+                    const int row = W.gp_i[k];
+                    MB_REQUIRE(row >= 0 && row < 2 * ns, "wfs %d: GP row %d out of range", w, row);
+                    const int s = row < ns ? row : row - ns;
+                    const int tx = px - sp[s].x, ty = py - sp[s].y;
+                    if (tx < 0 || tx > pos || ty < 0 || ty > pos) {
+                        if (std::fabs(W.gp_x[k]) > 0) {
+                            set_error("wfs %d: GP couples subaperture %d to a pupil point outside "
+                                      "its %dx%d stencil", w, s, n1, n1);
+                            throw InvalidArg{MB_EUNSUP};
+                        }
+                        continue;
+                    }
+                    float2 &c = coef[(size_t)s * n1 * n1 + ty * n1 + tx];
+                    if (row < ns) c.x += (float)W.gp_x[k];
+                    else c.y += (float)W.gp_x[k];
+                }
+            }
+            saptr.emplace_back(new DevBuf<int2>());
+            saptr.back()->upload(sp);
+            gp.emplace_back(new DevBuf<float2>());
+            gp.back()->upload(coef);
+            samap.emplace_back(new DevBuf<int>());
+            samap.back()->upload(sm);
+            wfs_h[w].saptr = saptr.back()->p;
+            wfs_h[w].gp = gp.back()->p;
+            wfs_h[w].samap = samap.back()->p;
+        } else {
+            wfs_h[w].saptr = wfs_h[share].saptr;
+            wfs_h[w].gp = wfs_h[share].gp;
+            wfs_h[w].samap = wfs_h[share].samap;
+        }
+        wfs_h[w].nsa = ns;
+        wfs_h[w].pos = pos;
+        wfs_h[w].goff = (int)goff[w];
+        neai.emplace_back(new DevBuf<float>());
+        ptt.emplace_back(new DevBuf<float>());
+        set_neai(w, W.neai, W.ptt);
+    }
+    wfs.upload(wfs_h);
+}
+
+void Recon::set_neai(int w, const double *ne, const double *pt) {
+    const int ns = nsa[w];
+    std::vector<float> h(3 * (size_t)ns);
+    for (size_t i = 0; i < h.size(); i++) {
+        MB_REQUIRE(std::isfinite(ne[i]), "wfs %d: non-finite NEA", w);
+        h[i] = (float)ne[i];
+    }
+    neai[w]->upload(h);
+    wfs_h[w].neai = neai[w]->p;
+    if (pt) {
+        std::vector<float> q(4 * (size_t)ns);
+        for (size_t i = 0; i < q.size(); i++) q[i] = (float)pt[i];
+        ptt[w]->upload(q);
+        wfs_h[w].ptt = ptt[w]->p;
+        wfs_h[w].has_ptt = 1;
+    } else {
+        wfs_h[w].ptt = nullptr;
+        wfs_h[w].has_ptt = 0;
+    }
+}
+
+void Recon::set_l2c(const double *l2c) {
+    for (int l = 0; l < nps; l++) {
+        MB_REQUIRE(std::isfinite(l2c[l]) && l2c[l] >= 0, "layer %d: invalid l2c", l);
+        lay_h[l].l2c = (float)l2c[l];
+    }
+    lay.upload(lay_h);
+}
+
+void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
+    MB_REQUIRE(fd && fd->perm && fd->mbinv && fd->nb > 0 && fd->bs > 0, "fdpcg tables missing");
+    MB_REQUIRE((long)fd->nb * fd->bs == nxtot, "fdpcg: nb*bs=%ld differs from nxtot=%ld",
+               (long)fd->nb * fd->bs, nxtot);
+    fd_nb = fd->nb;
+    fd_bs = fd->bs;
+    // spectra layout: layer-major, soff[l] = sum_{l'<l} nb * n_l'
+    std::vector<int> soff(nps);
+    long acc = 0;
+    for (int l = 0; l < nps; l++) {
+        soff[l] = (int)acc;
+        acc += (long)nb * lay_h[l].nx * lay_h[l].ny;
+    }
+    MB_REQUIRE(acc < (1L << 31), "fdpcg: batch too large for 32-bit spectrum index");
+    std::vector<FdIndex> idx(nxtot);
+    std::vector<double> sc(nxtot);
+    for (long i = 0; i < nxtot; i++) {
+        long q = fd->perm[i];
+        if (q < 0) q = -q;  // conjugate flag only appears in the half spectrum
+        MB_REQUIRE(q < nxtot, "fdpcg: perm out of range");
+        int l = 0;
+        while (l + 1 < nps && q >= xoff[l + 1]) l++;
+        const long local = q - xoff[l];
+        const long nl = (long)lay_h[l].nx * lay_h[l].ny;
+        idx[i].base = (int)(soff[l] + local);
+        idx[i].stride = (int)nl;
+        sc[i] = fd->scale ? 1.0 / std::sqrt((double)nl) : 1.0;
+    }
+    // fold the 1/sqrt(n) of the forward and inverse FFTs into the blocks
+    std::vector<cufftComplex> M((size_t)fd_nb * fd_bs * fd_bs);
+    for (long b = 0; b < fd_nb; b++)
+        for (int j = 0; j < fd_bs; j++)
+            for (int i = 0; i < fd_bs; i++) {
+                const size_t k = (size_t)b * fd_bs * fd_bs + (size_t)j * fd_bs + i;
+                const double s = sc[b * fd_bs + i] * sc[b * fd_bs + j];
+                M[k] = make_cuFloatComplex((float)(fd->mbinv[2 * k] * s), (float)(fd->mbinv[2 * k + 1] * s));
+            }
+    fd_M.upload(M);
+    fd_idx.upload(idx);
+    fd_soff.upload(soff);
+    spec.alloc(acc);
+    spec2.alloc(acc);
+    // one batched 2-D plan per run of consecutive equal-size layers
+    for (auto h : plans) cufftDestroy(h);
+    plans.clear();
+    plan_off.clear();
+    int l0 = 0;
+    while (l0 < nps) {
+        int l1 = l0 + 1;
+        while (l1 < nps && lay_h[l1].nx == lay_h[l0].nx && lay_h[l1].ny == lay_h[l0].ny) l1++;
+        int n[2] = {lay_h[l0].ny, lay_h[l0].nx};
+        const int dist = n[0] * n[1];
+        cufftHandle h;
+        MB_CUFFT_TRY(cufftPlanMany(&h, 2, n, nullptr, 1, dist, nullptr, 1, dist, CUFFT_C2C,
+                                   nb * (l1 - l0)));
+        MB_CUFFT_TRY(cufftSetStream(h, stream));
+        plans.push_back(h);
+        plan_off.push_back(soff[l0]);
+        l0 = l1;
+    }
+}
+
+void Recon::build(const mb_tomo_desc *d) {
+    MB_REQUIRE(d, "null descriptor");
+    MB_REQUIRE(d->nps > 0 && d->nwfs > 0 && d->xmap && d->wfs && d->l2c, "empty descriptor");
+    MB_REQUIRE(d->nbatch >= 1, "nbatch must be >= 1");
+    MB_REQUIRE(d->maxit >= 1, "maxit must be >= 1");
+    MB_REQUIRE(d->precond == 0 || d->precond == 1, "precond must be 0 or 1");
+    MB_CUDA_TRY(cudaGetDevice(&device));
+    MB_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    nb = d->nbatch;
+    nwfs = d->nwfs;
+    nps = d->nps;
+    nxp = d->pmap.nx;
+    nyp = d->pmap.ny;
+    np = nxp * nyp;
+    maxit = d->maxit;
+    precond = d->precond;
+    split = d->split;
+    MB_REQUIRE(nxp > 1 && nyp > 1 && d->pmap.dx > 0, "invalid pupil grid");
+    xoff.assign(nps + 1, 0);
+    lay_h.resize(nps);
+    for (int l = 0; l < nps; l++) {
+        const mb_grid &g = d->xmap[l];
+        MB_REQUIRE(g.nx >= 5 && g.ny >= 5 && g.dx > 0 && g.dy > 0, "layer %d: invalid grid", l);
+        lay_h[l].nx = g.nx;
+        lay_h[l].ny = g.ny;
+        lay_h[l].off = xoff[l];
+        xoff[l + 1] = xoff[l] + (long)g.nx * g.ny;
+    }
+    nxtot = xoff[nps];
+    goff.assign(nwfs + 1, 0);
+    nsa.resize(nwfs);
+    int nsamax = 0;
+    for (int w = 0; w < nwfs; w++) {
+        nsa[w] = d->wfs[w].nsa;
+        nsamax = std::max(nsamax, nsa[w]);
+        goff[w + 1] = goff[w] + 2L * nsa[w];
+    }
+    ngrad = goff[nwfs];
+    set_l2c(d->l2c);
+    build_hx_tables(d);
+    build_wfs_tables(d);
+    nblk_x = (int)nblocks(nxtot);
+    nblk_tt = (int)nblocks(nsamax);
+    nsc = maxit + 3;
+    const size_t NX = (size_t)nb * nxtot;
+    x.alloc(NX); r.alloc(NX); p.alloc(NX); z.alloc(NX); Ap.alloc(NX); rhs.alloc(NX);
+    opd.alloc((size_t)nb * nwfs * np);
+    opd2.alloc((size_t)nb * nwfs * np);
+    grad.alloc((size_t)nb * ngrad);
+    gin.alloc((size_t)nb * ngrad);
+    tt_part.alloc((size_t)nb * nwfs * nblk_tt * 2);
+    pap_part.alloc((size_t)nb * nblk_x);
+    rr_part.alloc((size_t)nb * nblk_x);
+    rz_part.alloc((size_t)nb * nblk_x);
+    bb_part.alloc((size_t)nb * nblk_x);
+    sc.alloc((size_t)nb * nsc);
+    res.alloc(nb);
+    if (precond) build_fdpcg(d->fdpcg);
+    x.zero_async(stream);
+    gin.zero_async(stream);
+    sc.zero_async(stream);
+    res.zero_async(stream);
+    MB_CUDA_TRY(cudaStreamSynchronize(stream));
+    capture_graph();
+}
+
+// ---------------------------------------------------------------------------
+// operators
+// ---------------------------------------------------------------------------
+void Recon::op_hx(const float *xin, cudaStream_t s) {
+    k_hx<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(xin, opd.p, hx_tab.p, lay.p, nps, nwfs,
+                                                         nxp, nyp, nxtot);
+    MB_CHECK_LAUNCH();
+}
+
+void Recon::op_rhs(const float *g, float *out, cudaStream_t s) {
+    // TomoR: x = Hx^T GP^T NEA^-1 (I - TT PTT) g   (recon_utils.c:397, tomo.cu:607)
+    k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, s>>>(nullptr, g, grad.p, tt_part.p, wfs.p, nwfs,
+                                                      nxp, np, ngrad, 1);
+    MB_CHECK_LAUNCH();
+    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt_part.p, opd2.p, wfs.p, nwfs,
+                                                          nxp, nyp, ngrad, nblk_tt, 1, 1.f);
+    MB_CHECK_LAUNCH();
+    GatherIndex gi{gi_ptr.p, gi_idxptr.p, gi_ent.p};
+    k_hxt<<<dim3(nblk_x, nb), kThreads, 0, s>>>(opd2.p, nullptr, out, nullptr, gi, lay.p, nps, nwfs,
+                                               nxp, nyp, nxtot, 0, 1.f);
+    MB_CHECK_LAUNCH();
+}
+
+void Recon::op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t s) {
+    // TomoL: Hx^T GP^T NEA^-1 (I - TT PTT) GP Hx x + L2^T L2 x   (recon_utils.c:447, tomo.cu:639)
+    op_hx(xin, s);
+    const int do_tt = split ? 0 : 1;
+    k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, s>>>(opd.p, nullptr, grad.p, tt_part.p, wfs.p,
+                                                      nwfs, nxp, np, ngrad, do_tt);
+    MB_CHECK_LAUNCH();
+    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt_part.p, opd2.p, wfs.p, nwfs,
+                                                          nxp, nyp, ngrad, nblk_tt, do_tt, 1.f);
+    MB_CHECK_LAUNCH();
+    GatherIndex gi{gi_ptr.p, gi_idxptr.p, gi_ent.p};
+    k_hxt<<<dim3(nblk_x, nb), kThreads, 0, s>>>(opd2.p, xin, out, dot_part, gi, lay.p, nps, nwfs,
+                                               nxp, nyp, nxtot, 1, 1.f);
+    MB_CHECK_LAUNCH();
+}
+
+void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s) {
+    // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT
+    k_fd_pack<<<dim3(nblk_x, nb), kThreads, 0, s>>>(rin, spec.p, lay.p, fd_soff.p, nps, nxtot);
+    MB_CHECK_LAUNCH();
+    for (size_t i = 0; i < plans.size(); i++) {
+        MB_CUFFT_TRY(cufftSetStream(plans[i], s));
+        MB_CUFFT_TRY(cufftExecC2C(plans[i], spec.p + plan_off[i], spec.p + plan_off[i], CUFFT_FORWARD));
+        count_launches(1);
+    }
+    k_fd_mul<<<dim3(nblocks((long)fd_nb * fd_bs), nb), kThreads, 0, s>>>(spec.p, spec2.p, fd_M.p,
+                                                                        fd_idx.p, fd_nb, fd_bs);
+    MB_CHECK_LAUNCH();
+    for (size_t i = 0; i < plans.size(); i++) {
+        MB_CUFFT_TRY(cufftExecC2C(plans[i], spec2.p + plan_off[i], spec2.p + plan_off[i], CUFFT_INVERSE));
+        count_launches(1);
+    }
+    k_fd_unpack<<<dim3(nblk_x, nb), kThreads, 0, s>>>(spec2.p, rin, zout, rzp, lay.p, fd_soff.p, nps,
+                                                     nxtot);
+    MB_CHECK_LAUNCH();
+}
+
+// The whole per-step tomography: RHS, then (FD)PCG from the warm start in x
+// (lib/pcg.c:28 / cuda/pcg.cu:87 schedule; restart every 100 iterations is
+// never reached for maxit <= 100).
+void Recon::enqueue_solve(cudaStream_t s) {
+    op_rhs(gin.p, rhs.p, s);
+    // r = b - A x ; bb
+    op_lhs(x.p, Ap.p, nullptr, s);
+    k_cg_init_r<<<dim3(nblk_x, nb), kThreads, 0, s>>>(rhs.p, Ap.p, r.p, bb_part.p, nxtot);
+    MB_CHECK_LAUNCH();
+    float *zp = r.p;
+    if (precond) {
+        op_fdpcg(r.p, z.p, rz_part.p, s);
+        zp = z.p;
+    } else {
+        // no preconditioner: z aliases r, so r.z = r.r
+        k_dot_self<<<dim3(nblk_x, nb), kThreads, 0, s>>>(r.p, rz_part.p, nxtot);
+        MB_CHECK_LAUNCH();
+    }
+    k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, s>>>(p.p, zp, rz_part.p, sc.p, nsc, 0, nxtot,
+                                                       nblk_x, 1);
+    MB_CHECK_LAUNCH();
+    for (int k = 0; k < maxit; k++) {
+        op_lhs(p.p, Ap.p, pap_part.p, s);
+        k_cg_update_xr<<<dim3(nblk_x, nb), kThreads, 0, s>>>(x.p, r.p, p.p, Ap.p, pap_part.p,
+                                                            rr_part.p, sc.p, nsc, k, nxtot, nblk_x);
+        MB_CHECK_LAUNCH();
+        if (k + 1 == maxit) break;
+        const double *rzp_k = rr_part.p;
+        if (precond) {
+            op_fdpcg(r.p, z.p, rz_part.p, s);
+            rzp_k = rz_part.p;
+        }
+        k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, s>>>(p.p, zp, rzp_k, sc.p, nsc, k, nxtot,
+                                                           nblk_x, 0);
+        MB_CHECK_LAUNCH();
+    }
+    k_cg_residual<<<dim3(1, nb), 32, 0, s>>>(rr_part.p, bb_part.p, sc.p, res.p, nsc, maxit + 2,
+                                            nblk_x);
+    MB_CHECK_LAUNCH();
+}
+
+// Time each iteration stage alone and report its algorithmic traffic.
+void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
+    const int ns = mb_num_stages();
+    cudaEvent_t e0, e1;
+    MB_CUDA_TRY(cudaEventCreate(&e0));
+    MB_CUDA_TRY(cudaEventCreate(&e1));
+    const double B = nb, F = 4.0, D = 8.0;
+    const double gp_tab = 0;  // per-WFS stencil tables, counted below
+    (void)gp_tab;
+    double tab_gp = 0, tab_gpt = 0;
+    for (int w = 0; w < nwfs; w++) {
+        const int n1 = wfs_h[w].pos + 1;
+        tab_gp += nsa[w] * (8.0 + 8.0 * n1 * n1 + 16.0);              // saptr, coefs, ptt
+        tab_gpt += nsa[w] * (8.0 * n1 * n1 + 12.0) + 4.0 * np;       // coefs, neai, samap
+    }
+    const double nxw = (double)nwfs * np;
+    const double ngr = (double)ngrad;
+    const double nx = (double)nxtot;
+    const double gather = (double)gi_ent.n * 8.0 + (double)gi_idxptr.n * 4.0;
+    const double nbk = (double)fd_nb * fd_bs;
+    // bytes per launch: operands read + written once
+    double by[11] = {
+        B * (F * nx + F * nxw) + (double)hx_tab.n * 12.0,             // hx: x -> opd
+        B * (F * nxw + F * ngr + D * 2 * nwfs * nblk_tt) + tab_gp,     // gp: opd -> grad
+        B * (F * ngr + F * nxw) + tab_gpt,                             // gpt: grad -> opd2
+        B * (F * nxw + 2 * F * nx) + gather,                           // hxt: opd2, p -> Ap
+        B * (5 * F * nx),                                              // x,r,p,Ap r/w
+        B * (3 * F * nx),                                              // p,z -> p
+        B * (F * nx + 2 * F * nx),                                     // r -> complex spec
+        B * (16.0 * nx),                                               // C2C read+write
+        B * (16.0 * nbk) + 8.0 * nbk * fd_bs + 8.0 * nbk,              // spec, spec2, M, idx
+        B * (16.0 * nx),
+        B * (2 * F * nx + F * nx + F * nx)};                           // spec (re), r -> z
+    const int lps[11] = {maxit + 1, maxit + 2, maxit + 2, maxit + 2, maxit, maxit - 1 + 1,
+                         precond ? maxit : 0, precond ? maxit : 0, precond ? maxit : 0,
+                         precond ? maxit : 0, precond ? maxit : 0};
+    GatherIndex gi{gi_ptr.p, gi_idxptr.p, gi_ent.p};
+    for (int st = 0; st < ns; st++) {
+        bytes[st] = by[st];
+        launches[st] = lps[st];
+        ms[st] = 0.f;
+        if (st >= 6 && !precond) continue;
+        auto launch = [&]() {
+            switch (st) {
+                case 0: op_hx(p.p, stream); break;
+                case 1:
+                    k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, stream>>>(opd.p, nullptr, grad.p, tt_part.p,
+                                                                          wfs.p, nwfs, nxp, np, ngrad, 1);
+                    MB_CHECK_LAUNCH();
+                    break;
+                case 2:
+                    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, stream>>>(grad.p, tt_part.p, opd2.p,
+                                                                               wfs.p, nwfs, nxp, nyp, ngrad,
+                                                                               nblk_tt, 1, 1.f);
+                    MB_CHECK_LAUNCH();
+                    break;
+                case 3:
+                    k_hxt<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(opd2.p, p.p, Ap.p, pap_part.p, gi, lay.p,
+                                                                    nps, nwfs, nxp, nyp, nxtot, 1, 1.f);
+                    MB_CHECK_LAUNCH();
+                    break;
+                case 4:
+                    // alpha reads the current scalars; the vectors are scratch here
+                    k_cg_update_xr<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(z.p, rhs.p, p.p, Ap.p, pap_part.p,
+                                                                             rr_part.p, sc.p, nsc, 0, nxtot,
+                                                                             nblk_x);
+                    MB_CHECK_LAUNCH();
+                    break;
+                case 5:
+                    k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(rhs.p, z.p, rz_part.p, sc.p, nsc,
+                                                                            maxit + 1, nxtot, nblk_x, 0);
+                    MB_CHECK_LAUNCH();
+                    break;
+                case 6:
+                    k_fd_pack<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(r.p, spec.p, lay.p, fd_soff.p, nps, nxtot);
+                    MB_CHECK_LAUNCH();
+                    break;
+                case 7:
+                case 9:
+                    for (size_t i = 0; i < plans.size(); i++) {
+                        MB_CUFFT_TRY(cufftSetStream(plans[i], stream));
+                        MB_CUFFT_TRY(cufftExecC2C(plans[i], spec.p + plan_off[i], spec.p + plan_off[i],
+                                                  st == 7 ? CUFFT_FORWARD : CUFFT_INVERSE));
+                        count_launches(1);
+                    }
+                    break;
+                case 8:
+                    k_fd_mul<<<dim3(nblocks((long)fd_nb * fd_bs), nb), kThreads, 0, stream>>>(
+                        spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nb, fd_bs);
+                    MB_CHECK_LAUNCH();
+                    break;
+                case 10:
+                    k_fd_unpack<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(spec2.p, r.p, z.p, rz_part.p, lay.p,
+                                                                          fd_soff.p, nps, nxtot);
+                    MB_CHECK_LAUNCH();
+                    break;
+            }
+        };
+        launch();  // warm
+        MB_CUDA_TRY(cudaEventRecord(e0, stream));
+        for (int i = 0; i < reps; i++) launch();
+        MB_CUDA_TRY(cudaEventRecord(e1, stream));
+        MB_CUDA_TRY(cudaEventSynchronize(e1));
+        float t = 0;
+        MB_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+        ms[st] = t / reps;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+void Recon::capture_graph() {
+    if (graph) {
+        cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
+    cudaGraph_t g;
+    const long before = g_launches.load();
+    MB_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        enqueue_solve(stream);
+    } catch (...) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    MB_CUDA_TRY(cudaStreamEndCapture(stream, &g));
+    graph_kernels = g_launches.load() - before;
+    g_launches -= graph_kernels;  // captured, not launched
+    MB_CUDA_TRY(cudaGraphInstantiate(&graph, g, 0));
+    cudaGraphDestroy(g);
+}
+
+void Recon::run_graph(cudaStream_t s) {
+    MB_CUDA_TRY(cudaGraphLaunch(graph, s));
+    count_launches(graph_kernels);
+}
+
+}  // namespace mb
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+struct mb_recon {
+    mb::Recon R;
+};
+
+using mb::CudaError;
+using mb::InvalidArg;
+
+#define MB_API_BEGIN try {
+#define MB_API_END                                   \
+    }                                                \
+    catch (const CudaError &e) { return e.code; }    \
+    catch (const InvalidArg &e) { return e.code; }   \
+    catch (const std::bad_alloc &) {                 \
+        mb::set_error("host allocation failed");     \
+        return MB_ENOMEM;                            \
+    }                                                \
+    catch (...) {                                    \
+        mb::set_error("unexpected C++ exception");   \
+        return MB_ECUDA;                             \
+    }                                                \
+    return MB_OK;
+
+extern "C" {
+
+int mb_version(void) { return 1; }
+
+const char *mb_error_string(int code) {
+    switch (code) {
+        case MB_OK: return "ok";
+        case MB_EINVAL: return "invalid argument";
+        case MB_ECUDA: return "CUDA error";
+        case MB_ENOMEM: return "out of device memory";
+        case MB_ESTATE: return "invalid state";
+        case MB_EUNSUP: return "unsupported geometry";
+        case MB_ENUM: return "numerical failure";
+        default: return "unknown error";
+    }
+}
+const char *mb_last_error_message(void) { return mb::last_error(); }
+
+long mb_kernel_launches(int reset) {
+    long v = mb::g_launches.load();
+    if (reset) mb::g_launches = 0;
+    return v;
+}
+
+int mb_init(int device) {
+    MB_API_BEGIN
+    int n = 0;
+    MB_CUDA_TRY(cudaGetDeviceCount(&n));
+    MB_REQUIRE(device >= 0 && device < n, "device %d out of range (%d devices)", device, n);
+    MB_CUDA_TRY(cudaSetDevice(device));
+    MB_API_END
+}
+
+void mb_cleanup(void) {}
+
+int mb_setup_recon(const mb_tomo_desc *desc, mb_recon **out) {
+    if (!out) {
+        mb::set_error("out is NULL");
+        return MB_EINVAL;
+    }
+    *out = nullptr;
+    mb_recon *h = new (std::nothrow) mb_recon();
+    if (!h) return MB_ENOMEM;
+    try {
+        h->R.build(desc);
+    } catch (const CudaError &e) {
+        delete h;
+        return e.code;
+    } catch (const InvalidArg &e) {
+        delete h;
+        return e.code;
+    } catch (...) {
+        delete h;
+        mb::set_error("unexpected exception in setup");
+        return MB_ECUDA;
+    }
+    *out = h;
+    return MB_OK;
+}
+
+void mb_recon_free(mb_recon *r) { delete r; }
+
+long mb_ngrad(const mb_recon *r) { return r ? r->R.ngrad : -1; }
+long mb_nxtot(const mb_recon *r) { return r ? r->R.nxtot : -1; }
+int mb_nbatch(const mb_recon *r) { return r ? r->R.nb : -1; }
+
+int mb_recon_reset(mb_recon *h) {
+    MB_API_BEGIN
+    MB_REQUIRE(h, "null handle");
+    h->R.x.zero_async(h->R.stream);
+    MB_CUDA_TRY(cudaStreamSynchronize(h->R.stream));
+    MB_API_END
+}
+
+int mb_update_recon_nea(mb_recon *h, int iwfs, const double *neai, const double *ptt) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && neai && iwfs >= 0 && iwfs < h->R.nwfs, "invalid arguments");
+    MB_CUDA_TRY(cudaStreamSynchronize(h->R.stream));
+    h->R.set_neai(iwfs, neai, ptt);
+    h->R.wfs.upload(h->R.wfs_h);
+    h->R.capture_graph();
+    MB_API_END
+}
+
+int mb_update_recon_cn2(mb_recon *h, const double *l2c, const mb_fdpcg_desc *fd) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && l2c, "invalid arguments");
+    MB_CUDA_TRY(cudaStreamSynchronize(h->R.stream));
+    h->R.set_l2c(l2c);
+    if (h->R.precond) h->R.build_fdpcg(fd);
+    h->R.capture_graph();
+    MB_API_END
+}
+
+static void to_float_dev(float *d, const double *hsrc, size_t n, cudaStream_t s) {
+    std::vector<float> tmp(n);
+    for (size_t i = 0; i < n; i++) tmp[i] = (float)hsrc[i];
+    MB_CUDA_TRY(cudaMemcpyAsync(d, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
+    MB_CUDA_TRY(cudaStreamSynchronize(s));
+}
+static void from_float_dev(double *hdst, const float *d, size_t n, cudaStream_t s) {
+    std::vector<float> tmp(n);
+    MB_CUDA_TRY(cudaMemcpyAsync(tmp.data(), d, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    MB_CUDA_TRY(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < n; i++) hdst[i] = tmp[i];
+}
+
+int mb_tomo(mb_recon *h, const double *grad, double *opdr, float *cgres) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && grad, "invalid arguments");
+    mb::Recon &R = h->R;
+    const size_t ng = (size_t)R.nb * R.ngrad;
+    for (size_t i = 0; i < ng; i++)
+        if (!std::isfinite(grad[i])) {
+            mb::set_error("gradient %zu is not finite", i);
+            return MB_ENUM;
+        }
+    to_float_dev(R.gin.p, grad, ng, R.stream);
+    R.run_graph(R.stream);
+    if (opdr) from_float_dev(opdr, R.x.p, (size_t)R.nb * R.nxtot, R.stream);
+    if (cgres) MB_CUDA_TRY(cudaMemcpyAsync(cgres, R.res.p, R.nb * sizeof(float), cudaMemcpyDeviceToHost, R.stream));
+    MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
+    MB_API_END
+}
+
+int mb_tomo_device(mb_recon *h, const float *d_grad, void *stream) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && d_grad, "invalid arguments");
+    mb::Recon &R = h->R;
+    cudaStream_t s = (cudaStream_t)stream;
+    MB_CUDA_TRY(cudaMemcpyAsync(R.gin.p, d_grad, (size_t)R.nb * R.ngrad * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s));
+    R.run_graph(s);
+    MB_API_END
+}
+
+const float *mb_tomo_solution(mb_recon *h) { return h ? h->R.x.p : nullptr; }
+
+void *mb_recon_stream(mb_recon *h) { return h ? (void *)h->R.stream : nullptr; }
+
+static const char *kStageNames[] = {"hx", "gp", "gpt", "hxt_l2", "cg_update_xr", "cg_update_p",
+                                    "fd_pack", "fd_fft_fwd", "fd_mul", "fd_fft_inv", "fd_unpack"};
+int mb_num_stages(void) { return (int)(sizeof(kStageNames) / sizeof(kStageNames[0])); }
+const char *mb_stage_name(int i) { return (i >= 0 && i < mb_num_stages()) ? kStageNames[i] : ""; }
+
+int mb_time_stages(mb_recon *h, int reps, float *ms, double *bytes, int *launches) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && ms && bytes && launches && reps > 0, "invalid arguments");
+    h->R.time_stages(reps, ms, bytes, launches);
+    MB_API_END
+}
+
+int mb_tomo_residual(mb_recon *h, float *cgres) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && cgres, "invalid arguments");
+    MB_CUDA_TRY(cudaMemcpyAsync(cgres, h->R.res.p, h->R.nb * sizeof(float), cudaMemcpyDeviceToHost,
+                                h->R.stream));
+    MB_CUDA_TRY(cudaStreamSynchronize(h->R.stream));
+    MB_API_END
+}
+
+int mb_apply_tomo_R(mb_recon *h, const double *grad, double *xout) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && grad && xout, "invalid arguments");
+    mb::Recon &R = h->R;
+    to_float_dev(R.gin.p, grad, (size_t)R.nb * R.ngrad, R.stream);
+    R.op_rhs(R.gin.p, R.rhs.p, R.stream);
+    from_float_dev(xout, R.rhs.p, (size_t)R.nb * R.nxtot, R.stream);
+    MB_API_END
+}
+
+int mb_apply_tomo_L(mb_recon *h, const double *xin, double *xout) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && xin && xout, "invalid arguments");
+    mb::Recon &R = h->R;
+    to_float_dev(R.z.p, xin, (size_t)R.nb * R.nxtot, R.stream);
+    R.op_lhs(R.z.p, R.Ap.p, nullptr, R.stream);
+    from_float_dev(xout, R.Ap.p, (size_t)R.nb * R.nxtot, R.stream);
+    MB_API_END
+}
+
+int mb_apply_fdpcg(mb_recon *h, const double *xin, double *xout) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && xin && xout, "invalid arguments");
+    mb::Recon &R = h->R;
+    if (!R.precond) {
+        mb::set_error("reconstructor has no FDPCG preconditioner");
+        return MB_ESTATE;
+    }
+    to_float_dev(R.Ap.p, xin, (size_t)R.nb * R.nxtot, R.stream);
+    R.op_fdpcg(R.Ap.p, R.z.p, R.rz_part.p, R.stream);
+    from_float_dev(xout, R.z.p, (size_t)R.nb * R.nxtot, R.stream);
+    MB_API_END
+}
+
+int mb_apply_hx(mb_recon *h, const double *xin, double *opd) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && xin && opd, "invalid arguments");
+    mb::Recon &R = h->R;
+    to_float_dev(R.z.p, xin, (size_t)R.nb * R.nxtot, R.stream);
+    R.op_hx(R.z.p, R.stream);
+    from_float_dev(opd, R.opd.p, (size_t)R.nb * R.nwfs * R.np, R.stream);
+    MB_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,476 @@
+// Tomography kernels for B200 (sm_100a).
+//
+// Every kernel is batched: blockIdx.z (or .y) selects one of `nb` independent
+// instances that share the operator tables.  Instance vectors are stored
+// instance-major (x[b*nxtot + ...]).  Reductions are deterministic: each block
+// writes one FP64 partial, and consumers add the partials in a fixed order.
+//
+// Reference counterparts (cuda/tomo.cu, cuda/prop_wrap.cu, cuda/pcg.cu):
+//   k_hx        gpu_map2map_do forward (prop_wrap.cu:35)      -- bilinear gather
+//   k_gp        gpu_gp_do (tomo.cu:362)                       -- GP stencil + TT sums
+//   k_gpt       gpu_gpt_do (tomo.cu:485)                      -- gather form, no atomics
+//   k_hxt       gpu_map2map_do 't' + gpu_laplacian_do         -- gather form, no atomics
+//   k_cg_*      gpu_pcg scalar kernels (pcg.cu:27-57)         -- FP64 scalars
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+namespace mb {
+
+constexpr int kThreads = 256;
+
+// One axis entry of the forward bilinear table: source index k (-1: the
+// pupil point misses the layer) and the two weights for k and k+1.
+struct AxisW {
+    int k;
+    float w0, w1;
+};
+// One entry of the transposed (gather) table: pupil index and weight.
+struct GatherW {
+    int i;
+    float w;
+};
+
+struct WfsDev {
+    int nsa;
+    int pos;        // stencil is (pos+1)^2 points
+    int goff;       // offset of this WFS's gradients inside one instance
+    int has_ptt;
+    const int2 *saptr;     // [nsa] lower-left corner on the pupil grid
+    const float2 *gp;      // [nsa][(pos+1)^2] (x coefficient, y coefficient)
+    const int *samap;      // [np] subaperture whose corner is at this pupil point, -1 if none
+    const float *neai;     // [nsa][3] cx, cy, cxy
+    const float *ptt;      // [2][2*nsa] column-major (k + 2*i)
+};
+
+struct LayerDev {
+    int nx, ny;
+    long off;       // offset inside one instance
+    float l2c;      // biharmonic weight
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of one double; result valid in thread 0.
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double t = 0;
+    if (wid == 0) {
+        t = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.0;
+        t = warp_sum(t);
+    }
+    __syncthreads();
+    return t;
+}
+
+// Sum `n` partials in fixed order with one warp; result broadcast to the warp.
+__device__ __forceinline__ double warp_sum_partials(const double *part, int n) {
+    double v = 0;
+    for (int i = threadIdx.x & 31; i < n; i += 32) v += part[i];
+    v = warp_sum(v);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// ---------------------------------------------------------------------------
+// Hx: opd[b][w][p] = sum_l bilinear(x_l) at the ray of pupil point p.
+// grid: (ceil(np/256), nwfs, nb)
+// ---------------------------------------------------------------------------
+__global__ void k_hx(const float *__restrict__ x, float *__restrict__ opd,
+                     const AxisW *__restrict__ tab, const LayerDev *__restrict__ lay, int nps,
+                     int nwfs, int nxp, int nyp, long nxtot) {
+    const int np = nxp * nyp;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int w = blockIdx.y, b = blockIdx.z;
+    if (p >= np) return;
+    const int ix = p % nxp, iy = p / nxp;
+    const float *xb = x + (size_t)b * nxtot;
+    float acc = 0.f;
+    for (int l = 0; l < nps; l++) {
+        const AxisW *t = tab + (size_t)(w * nps + l) * (nxp + nyp);
+        const AxisW tx = t[ix], ty = t[nxp + iy];
+        if (tx.k < 0 || ty.k < 0) continue;
+        const int nx = lay[l].nx;
+        const float *X = xb + lay[l].off + (size_t)ty.k * nx + tx.k;
+        const float a = tx.w0 * X[0] + tx.w1 * X[1];
+        const float c = tx.w0 * X[nx] + tx.w1 * X[nx + 1];
+        acc += ty.w0 * a + ty.w1 * c;
+    }
+    opd[((size_t)b * nwfs + w) * np + p] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// GP: grad = GP * opd (or the input gradients for the right-hand side), and
+// per-block partial sums of PTT * grad for the tip/tilt removal.
+// grid: (nblk, nwfs, nb); tt_part[((b*nwfs+w)*nblk + blk)*2 + k]
+// ---------------------------------------------------------------------------
+__global__ void k_gp(const float *__restrict__ opd, const float *__restrict__ gin,
+                     float *__restrict__ grad, double *__restrict__ tt_part,
+                     const WfsDev *__restrict__ wfs, int nwfs, int nxp, int np, long ngrad,
+                     int do_tt) {
+    __shared__ double sh[32];
+    const int w = blockIdx.y, b = blockIdx.z;
+    const WfsDev W = wfs[w];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    float gx = 0.f, gy = 0.f;
+    if (s < W.nsa) {
+        float *g = grad + (size_t)b * ngrad + W.goff;
+        if (gin) {
+            const float *gi = gin + (size_t)b * ngrad + W.goff;
+            gx = gi[s];
+            gy = gi[s + W.nsa];
+        } else {
+            const int2 c = W.saptr[s];
+            const int n1 = W.pos + 1;
+            const float2 *cf = W.gp + (size_t)s * n1 * n1;
+            const float *o = opd + ((size_t)b * nwfs + w) * np + (size_t)c.y * nxp + c.x;
+            for (int ty = 0; ty < n1; ty++)
+                for (int tx = 0; tx < n1; tx++) {
+                    const float v = o[ty * nxp + tx];
+                    const float2 k = cf[ty * n1 + tx];
+                    gx += k.x * v;
+                    gy += k.y * v;
+                }
+        }
+        g[s] = gx;
+        g[s + W.nsa] = gy;
+    }
+    if (do_tt && W.has_ptt) {
+        double tx = 0, ty = 0;
+        if (s < W.nsa) {
+            const float *P = W.ptt;
+            tx = (double)P[2 * s] * gx + (double)P[2 * (s + W.nsa)] * gy;
+            ty = (double)P[2 * s + 1] * gx + (double)P[2 * (s + W.nsa) + 1] * gy;
+        }
+        tx = block_sum(tx, sh);
+        ty = block_sum(ty, sh);
+        if (threadIdx.x == 0) {
+            double *o = tt_part + (((size_t)b * nwfs + w) * gridDim.x + blockIdx.x) * 2;
+            o[0] = tx;
+            o[1] = ty;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// GP^T NEA^-1 (I - TT PTT) in gather form: each pupil point collects from the
+// (pos+1)^2 subapertures whose stencil covers it.
+// grid: (ceil(np/256), nwfs, nb)
+// ---------------------------------------------------------------------------
+__global__ void k_gpt(const float *__restrict__ grad, const double *__restrict__ tt_part,
+                      float *__restrict__ opd2, const WfsDev *__restrict__ wfs, int nwfs,
+                      int nxp, int nyp, long ngrad, int nblk_tt, int do_tt, float alpha) {
+    __shared__ float s_tt[2];
+    const int w = blockIdx.y, b = blockIdx.z;
+    const WfsDev W = wfs[w];
+    const bool use_tt = do_tt && W.has_ptt;
+    if (threadIdx.x < 32) {
+        double t0 = 0, t1 = 0;
+        if (use_tt) {
+            const double *tp = tt_part + ((size_t)b * nwfs + w) * nblk_tt * 2;
+            for (int i = threadIdx.x; i < nblk_tt; i += 32) {
+                t0 += tp[2 * i];
+                t1 += tp[2 * i + 1];
+            }
+            t0 = warp_sum(t0);
+            t1 = warp_sum(t1);
+        }
+        if (threadIdx.x == 0) {
+            s_tt[0] = (float)(-t0);
+            s_tt[1] = (float)(-t1);
+        }
+    }
+    __syncthreads();
+    const int np = nxp * nyp;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const int px = p % nxp, py = p / nxp;
+    const int n1 = W.pos + 1;
+    const float *g = grad + (size_t)b * ngrad + W.goff;
+    const float ttx = s_tt[0], tty = s_tt[1];
+    float acc = 0.f;
+    for (int dy = 0; dy < n1; dy++) {
+        const int cy = py - dy;
+        if (cy < 0) break;
+        for (int dx = 0; dx < n1; dx++) {
+            const int cx = px - dx;
+            if (cx < 0) break;
+            const int s = W.samap[cy * nxp + cx];
+            if (s < 0) continue;
+            const float gx = g[s] + ttx;
+            const float gy = g[s + W.nsa] + tty;
+            const float *ne = W.neai + 3 * s;
+            const float nx_ = ne[0] * gx + ne[2] * gy;
+            const float ny_ = ne[2] * gx + ne[1] * gy;
+            const float2 k = W.gp[(size_t)s * n1 * n1 + dy * n1 + dx];
+            acc += k.x * nx_ + k.y * ny_;
+        }
+    }
+    opd2[((size_t)b * nwfs + w) * np + p] = alpha * acc;
+}
+
+// ---------------------------------------------------------------------------
+// Hx^T in gather form (+ L2^T L2 regularisation and p.Ap partial for the LHS).
+// Layer points are flattened over all layers; grid: (nblk_x, nb).
+// The transposed table for (w, l, axis) is a CSR list per layer column/row.
+// ---------------------------------------------------------------------------
+struct GatherIndex {
+    const int *ptr;        // [ntab] offsets of each (w,l,axis) CSR in `idx_ptr`
+    const int *idx_ptr;    // concatenated CSR row pointers
+    const GatherW *ent;    // concatenated entries
+};
+
+__global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ xin,
+                      float *__restrict__ out, double *__restrict__ dot_part, GatherIndex gi,
+                      const LayerDev *__restrict__ lay, int nps, int nwfs, int nxp, int nyp,
+                      long nxtot, int do_l2, float alpha) {
+    __shared__ double sh[32];
+    const int b = blockIdx.y;
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double dotv = 0;
+    if (j < nxtot) {
+        int l = 0;
+        while (l + 1 < nps && j >= lay[l + 1].off) l++;
+        const LayerDev L = lay[l];
+        const int jj = (int)(j - L.off);
+        const int jx = jj % L.nx, jy = jj / L.nx;
+        const int np = nxp * nyp;
+        float acc = 0.f;
+        for (int w = 0; w < nwfs; w++) {
+            const int tx = gi.ptr[(w * nps + l) * 2 + 0];
+            const int ty = gi.ptr[(w * nps + l) * 2 + 1];
+            const int ax0 = gi.idx_ptr[tx + jx], ax1 = gi.idx_ptr[tx + jx + 1];
+            const int ay0 = gi.idx_ptr[ty + jy], ay1 = gi.idx_ptr[ty + jy + 1];
+            if (ax0 == ax1 || ay0 == ay1) continue;
+            const float *o = opd2 + ((size_t)b * nwfs + w) * np;
+            for (int ay = ay0; ay < ay1; ay++) {
+                const GatherW ey = gi.ent[ay];
+                float rs = 0.f;
+                for (int ax = ax0; ax < ax1; ax++) {
+                    const GatherW ex = gi.ent[ax];
+                    rs += ex.w * o[ey.i * nxp + ex.i];
+                }
+                acc += ey.w * rs;
+            }
+        }
+        const float *X = xin ? xin + (size_t)b * nxtot + L.off : nullptr;
+        if (do_l2) {
+            const int nx = L.nx, ny = L.ny;
+            auto at = [&](int dx, int dy) {
+                int xx = jx + dx, yy = jy + dy;
+                xx += (xx < 0) ? nx : 0;
+                xx -= (xx >= nx) ? nx : 0;
+                yy += (yy < 0) ? ny : 0;
+                yy -= (yy >= ny) ? ny : 0;
+                return X[yy * nx + xx];
+            };
+            const float st = 20.f * at(0, 0) -
+                             8.f * (at(-1, 0) + at(1, 0) + at(0, -1) + at(0, 1)) +
+                             2.f * (at(-1, -1) + at(1, -1) + at(-1, 1) + at(1, 1)) +
+                             (at(0, -2) + at(-2, 0) + at(2, 0) + at(0, 2));
+            acc = alpha * acc + alpha * L.l2c * st;
+        } else {
+            acc = alpha * acc;
+        }
+        out[(size_t)b * nxtot + j] = acc;
+        if (dot_part && X) dotv = (double)acc * (double)X[jj];
+    }
+    if (dot_part) {
+        dotv = block_sum(dotv, sh);
+        if (threadIdx.x == 0) dot_part[(size_t)b * gridDim.x + blockIdx.x] = dotv;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CG vector kernels.  Scalars per instance: sc[b*nsc + k].
+// layout: [0..maxit] r.z per iteration, [maxit+1] b.b, [maxit+2] residual
+// ---------------------------------------------------------------------------
+
+// r = b - Ax, and b.b partials.  grid: (nblk_x, nb)
+__global__ void k_cg_init_r(const float *__restrict__ bvec, const float *__restrict__ Ax,
+                            float *__restrict__ r, double *__restrict__ bb_part, long n) {
+    __shared__ double sh[32];
+    const int b = blockIdx.y;
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0;
+    if (j < n) {
+        const size_t o = (size_t)b * n + j;
+        const float bv = bvec[o];
+        r[o] = bv - Ax[o];
+        v = (double)bv * bv;
+    }
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) bb_part[(size_t)b * gridDim.x + blockIdx.x] = v;
+}
+
+// alpha = rz[k] / sum(pAp partials); x += alpha p; r -= alpha Ap; r.r partials.
+// When z aliases r (no preconditioner) the r.r partials double as r.z.
+__global__ void k_cg_update_xr(float *__restrict__ x, float *__restrict__ r,
+                               const float *__restrict__ p, const float *__restrict__ Ap,
+                               const double *__restrict__ pap_part, double *__restrict__ rr_part,
+                               double *__restrict__ sc, int nsc, int k, long n, int nblk) {
+    __shared__ double sh[32];
+    __shared__ float s_alpha;
+    const int b = blockIdx.y;
+    if (threadIdx.x < 32) {
+        const double pap = warp_sum_partials(pap_part + (size_t)b * nblk, nblk);
+        if (threadIdx.x == 0) {
+            double a = sc[(size_t)b * nsc + k] / pap;
+            if (!isfinite(a)) a = 0;  // pcg.c:80-83, pcg.cu:27-30
+            s_alpha = (float)a;
+        }
+    }
+    __syncthreads();
+    const float a = s_alpha;
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0;
+    if (j < n) {
+        const size_t o = (size_t)b * n + j;
+        x[o] += a * p[o];
+        const float rv = r[o] - a * Ap[o];
+        r[o] = rv;
+        v = (double)rv * rv;
+    }
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) rr_part[(size_t)b * gridDim.x + blockIdx.x] = v;
+}
+
+// beta = sum(rz partials) / rz[k]; p = z + beta p; rz[k+1] stored by block 0.
+// init != 0: p = z and rz[0] = sum (start or restart of the iteration).
+__global__ void k_cg_update_p(float *__restrict__ p, const float *__restrict__ z,
+                              const double *__restrict__ rz_part, double *__restrict__ sc, int nsc,
+                              int k, long n, int nblk, int init) {
+    __shared__ float s_beta;
+    const int b = blockIdx.y;
+    if (threadIdx.x < 32) {
+        const double rz = warp_sum_partials(rz_part + (size_t)b * nblk, nblk);
+        if (threadIdx.x == 0) {
+            double be = 0;
+            if (init) {
+                if (blockIdx.x == 0) sc[(size_t)b * nsc + 0] = rz;
+            } else {
+                be = rz / sc[(size_t)b * nsc + k];
+                if (!isfinite(be)) be = 0;
+                if (blockIdx.x == 0) sc[(size_t)b * nsc + k + 1] = rz;
+            }
+            s_beta = (float)be;
+        }
+    }
+    __syncthreads();
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) {
+        const size_t o = (size_t)b * n + j;
+        p[o] = init ? z[o] : z[o] + s_beta * p[o];
+    }
+}
+
+// v.v partials.  grid: (nblk_x, nb)
+__global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ part, long n) {
+    __shared__ double sh[32];
+    const int b = blockIdx.y;
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double t = 0;
+    if (j < n) {
+        const float a = v[(size_t)b * n + j];
+        t = (double)a * a;
+    }
+    t = block_sum(t, sh);
+    if (threadIdx.x == 0) part[(size_t)b * gridDim.x + blockIdx.x] = t;
+}
+
+// residual = sqrt(r.r / b.b) per instance.  grid: (1, nb), 32 threads
+__global__ void k_cg_residual(const double *__restrict__ rr_part, const double *__restrict__ bb_part,
+                              double *__restrict__ sc, float *__restrict__ res, int nsc, int resslot,
+                              int nblk) {
+    const int b = blockIdx.y;
+    const double rr = warp_sum_partials(rr_part + (size_t)b * nblk, nblk);
+    const double bb = warp_sum_partials(bb_part + (size_t)b * nblk, nblk);
+    if (threadIdx.x == 0) {
+        const double v = sqrt(rr / bb);
+        sc[(size_t)b * nsc + resslot] = v;
+        res[b] = (float)v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FDPCG.  Spectra are stored layer-major: S[soff[l] + b*n_l + local].
+// ---------------------------------------------------------------------------
+struct FdIndex {
+    int base;    // soff[l] + local for the permuted member
+    int stride;  // n_l
+};
+
+// real r (instance-major) -> complex spectra buffer (layer-major)
+__global__ void k_fd_pack(const float *__restrict__ r, cufftComplex *__restrict__ S,
+                          const LayerDev *__restrict__ lay, const int *__restrict__ soff, int nps,
+                          long nxtot) {
+    const int b = blockIdx.y;
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nxtot) return;
+    int l = 0;
+    while (l + 1 < nps && j >= lay[l + 1].off) l++;
+    const long local = j - lay[l].off;
+    const long n_l = (long)lay[l].nx * lay[l].ny;
+    S[soff[l] + b * n_l + local] = make_cuFloatComplex(r[(size_t)b * nxtot + j], 0.f);
+}
+
+// Per-frequency block solve: Y[perm(i)] = sum_j M[blk][j*bs+i] X[perm(j)].
+// One thread per (block, row); grid: (ceil(nb*bs/256), nbatch)
+__global__ void k_fd_mul(const cufftComplex *__restrict__ X, cufftComplex *__restrict__ Y,
+                         const cufftComplex *__restrict__ M, const FdIndex *__restrict__ idx,
+                         int nblk, int bs) {
+    const int b = blockIdx.y;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nblk * bs) return;
+    const int blk = t / bs, i = t - blk * bs;
+    const cufftComplex *Mb = M + (size_t)blk * bs * bs;
+    const FdIndex *ib = idx + (size_t)blk * bs;
+    float re = 0.f, im = 0.f;
+    for (int jj = 0; jj < bs; jj++) {
+        const FdIndex q = ib[jj];
+        const cufftComplex xv = X[q.base + (size_t)b * q.stride];
+        const cufftComplex m = Mb[jj * bs + i];
+        re += m.x * xv.x - m.y * xv.y;
+        im += m.x * xv.y + m.y * xv.x;
+    }
+    const FdIndex o = ib[i];
+    Y[o.base + (size_t)b * o.stride] = make_cuFloatComplex(re, im);
+}
+
+// z = Re(spectra), and r.z partials.  grid: (nblk_x, nb)
+__global__ void k_fd_unpack(const cufftComplex *__restrict__ S, const float *__restrict__ r,
+                            float *__restrict__ z, double *__restrict__ rz_part,
+                            const LayerDev *__restrict__ lay, const int *__restrict__ soff, int nps,
+                            long nxtot) {
+    __shared__ double sh[32];
+    const int b = blockIdx.y;
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0;
+    if (j < nxtot) {
+        int l = 0;
+        while (l + 1 < nps && j >= lay[l + 1].off) l++;
+        const long local = j - lay[l].off;
+        const long n_l = (long)lay[l].nx * lay[l].ny;
+        const float zv = S[soff[l] + b * n_l + local].x;
+        const size_t o = (size_t)b * nxtot + j;
+        z[o] = zv;
+        v = (double)zv * r[o];
+    }
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) rz_part[(size_t)b * gridDim.x + blockIdx.x] = v;
+}
+
+// float <-> double staging helpers for the host-facing API
+__global__ void k_scale_copy(const float *__restrict__ a, float *__restrict__ o, float s, long n) {
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) o[j] = s * a[j];
+}
+
+}  // namespace mb

@@ -1,0 +1,107 @@
+"""ctypes binding of the C ABI declared in ``include/maos_b200.h``.
+
+The structs below mirror the header field by field.  Loading fails loudly when
+``libmaosb200.so`` is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmaosb200.so")
+
+MB_OK = 0
+ERRORS = {-1: "MB_EINVAL", -2: "MB_ECUDA", -3: "MB_ENOMEM", -4: "MB_ESTATE", -5: "MB_EUNSUP",
+          -6: "MB_ENUM"}
+
+
+class MbGrid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
+                ("ox", C.c_double), ("oy", C.c_double), ("ht", C.c_double)]
+
+
+class MbWfsDesc(C.Structure):
+    _fields_ = [("thetax", C.c_double), ("thetay", C.c_double), ("hs", C.c_double),
+                ("nsa", C.c_int), ("dsa", C.c_double),
+                ("salocx", C.POINTER(C.c_double)), ("salocy", C.POINTER(C.c_double)),
+                ("gp_p", C.POINTER(C.c_int)), ("gp_i", C.POINTER(C.c_int)),
+                ("gp_x", C.POINTER(C.c_double)), ("neai", C.POINTER(C.c_double)),
+                ("ptt", C.POINTER(C.c_double))]
+
+
+class MbFdpcgDesc(C.Structure):
+    _fields_ = [("nb", C.c_int), ("bs", C.c_int), ("scale", C.c_int),
+                ("perm", C.POINTER(C.c_long)), ("mbinv", C.POINTER(C.c_double))]
+
+
+class MbTomoDesc(C.Structure):
+    _fields_ = [("pmap", MbGrid), ("nps", C.c_int), ("xmap", C.POINTER(MbGrid)),
+                ("l2c", C.POINTER(C.c_double)), ("nwfs", C.c_int),
+                ("wfs", C.POINTER(MbWfsDesc)), ("maxit", C.c_int), ("precond", C.c_int),
+                ("split", C.c_int), ("fdpcg", C.POINTER(MbFdpcgDesc)), ("nbatch", C.c_int)]
+
+
+# every symbol the header declares, with (restype, argtypes)
+_D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
+SIGNATURES = {
+    "mb_init": (C.c_int, [C.c_int]),
+    "mb_cleanup": (None, []),
+    "mb_setup_recon": (C.c_int, [C.POINTER(MbTomoDesc), C.POINTER(C.c_void_p)]),
+    "mb_recon_free": (None, [C.c_void_p]),
+    "mb_recon_reset": (C.c_int, [C.c_void_p]),
+    "mb_update_recon_nea": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
+    "mb_update_recon_cn2": (C.c_int, [C.c_void_p, _D, C.POINTER(MbFdpcgDesc)]),
+    "mb_tomo": (C.c_int, [C.c_void_p, _D, _D, _F]),
+    "mb_tomo_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mb_tomo_solution": (C.c_void_p, [C.c_void_p]),
+    "mb_recon_stream": (C.c_void_p, [C.c_void_p]),
+    "mb_num_stages": (C.c_int, []),
+    "mb_stage_name": (C.c_char_p, [C.c_int]),
+    "mb_time_stages": (C.c_int, [C.c_void_p, C.c_int, _F, _D, C.POINTER(C.c_int)]),
+    "mb_tomo_residual": (C.c_int, [C.c_void_p, _F]),
+    "mb_ngrad": (C.c_long, [C.c_void_p]),
+    "mb_nxtot": (C.c_long, [C.c_void_p]),
+    "mb_nbatch": (C.c_int, [C.c_void_p]),
+    "mb_apply_tomo_R": (C.c_int, [C.c_void_p, _D, _D]),
+    "mb_apply_tomo_L": (C.c_int, [C.c_void_p, _D, _D]),
+    "mb_apply_fdpcg": (C.c_int, [C.c_void_p, _D, _D]),
+    "mb_apply_hx": (C.c_int, [C.c_void_p, _D, _D]),
+    "mb_kernel_launches": (C.c_long, [C.c_int]),
+    "mb_error_string": (C.c_char_p, [C.c_int]),
+    "mb_last_error_message": (C.c_char_p, []),
+    "mb_version": (C.c_int, []),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load the native library (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"maos_b200 native library not built: {path} "
+                           "(run python -m maos_b200.build)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class MbError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        lib = load()
+        msg = lib.mb_last_error_message().decode(errors="replace")
+        super().__init__(f"{where}: {ERRORS.get(code, code)} ({msg})")
+        self.code = code
+
+
+def check(code: int, where: str) -> None:
+    if code != MB_OK:
+        raise MbError(code, where)

@@ -1,0 +1,198 @@
+"""Host-side mirror of the reference's GPU reconstruction interface.
+
+``Reconstructor`` wraps one ``mb_recon`` handle.  Its methods follow the
+entry points of ``cuda/gpu.h`` that ``maos/recon.c`` and ``maos/sim.c`` call:
+
+=====================  ==========================================
+reference (cuda/gpu.h)  here
+=====================  ==========================================
+gpu_setup_recon        ``Reconstructor(system, nbatch=...)``
+gpu_update_recon       ``update_nea(iwfs, neai, ptt)``
+gpu_update_recon_cn2   ``update_cn2(l2c, fdpcg)``
+gpu_recon_reset        ``reset()``
+gpu_tomo               ``tomo(grad)`` -> (opdr, cgres)
+gpu_recon_free         ``close()``
+=====================  ==========================================
+
+Argument meaning and units are the reference's (gradients in radians, x then
+y per WFS; OPD in metres).  Errors raise :class:`maos_b200.native.MbError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import native
+from .native import MbFdpcgDesc, MbGrid, MbTomoDesc, MbWfsDesc, check
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _grid(g) -> MbGrid:
+    return MbGrid(int(g.nx), int(g.ny), float(g.dx), float(g.dy), float(g.ox), float(g.oy),
+                  float(getattr(g, "ht", 0.0)))
+
+
+def fdpcg_desc(fd, keep: list) -> MbFdpcgDesc:
+    perm = np.ascontiguousarray(fd.perm, dtype=np.int64)
+    # column-major complex blocks, interleaved re/im
+    mb = np.ascontiguousarray(fd.Mbinv.transpose(0, 2, 1)).ravel()
+    mbi = np.empty(mb.size * 2)
+    mbi[0::2] = mb.real
+    mbi[1::2] = mb.imag
+    keep += [perm, mbi]
+    return MbFdpcgDesc(int(fd.nb), int(fd.bs), int(fd.scale),
+                       perm.ctypes.data_as(C.POINTER(C.c_long)), _dptr(mbi))
+
+
+def tomo_desc(sysm, nbatch: int = 1, split: int = 1, maxit: Optional[int] = None):
+    """Flatten a :class:`maos_b200.geometry.TomoSystem` into an ``mb_tomo_desc``.
+
+    Returns (desc, keep) -- ``keep`` holds the numpy arrays the descriptor
+    points into and must outlive the setup call."""
+    keep = []
+    cfg = sysm.cfg
+    xm = (MbGrid * len(sysm.xmaps))(*[_grid(g) for g in sysm.xmaps])
+    l2c = np.ascontiguousarray(sysm.l2c, dtype=np.float64)
+    keep += [xm, l2c]
+    ws = (MbWfsDesc * len(sysm.wfs))()
+    gp_cache = {}
+    for i, w in enumerate(sysm.wfs):
+        key = id(w.GP)
+        if key not in gp_cache:
+            G = w.GP.tocsc()
+            G.sort_indices()
+            arrs = (np.ascontiguousarray(w.salocx, dtype=np.float64),
+                    np.ascontiguousarray(w.salocy, dtype=np.float64),
+                    np.ascontiguousarray(G.indptr, dtype=np.int32),
+                    np.ascontiguousarray(G.indices, dtype=np.int32),
+                    np.ascontiguousarray(G.data, dtype=np.float64))
+            gp_cache[key] = arrs
+            keep += list(arrs)
+        sx, sy, gpp, gpi, gpx = gp_cache[key]
+        neai = np.zeros((w.nsa, 3))
+        neai[:, 0] = w.saneai[:w.nsa]
+        neai[:, 1] = w.saneai[w.nsa:]
+        neai = np.ascontiguousarray(neai.ravel())
+        keep.append(neai)
+        ptt = None
+        if w.PTT is not None:
+            ptt = np.ascontiguousarray(w.PTT.ravel(order="F"))
+            keep.append(ptt)
+        ws[i] = MbWfsDesc(float(w.thetax), float(w.thetay), float(w.hs), int(w.nsa), float(w.dsa),
+                          _dptr(sx), _dptr(sy), gpp.ctypes.data_as(C.POINTER(C.c_int)),
+                          gpi.ctypes.data_as(C.POINTER(C.c_int)), _dptr(gpx), _dptr(neai),
+                          _dptr(ptt) if ptt is not None else C.POINTER(C.c_double)())
+    keep.append(ws)
+    fdp = C.POINTER(MbFdpcgDesc)()
+    if cfg.tomo_precond == 1:
+        fd = fdpcg_desc(sysm.fdpcg, keep)
+        keep.append(fd)
+        fdp = C.pointer(fd)
+    d = MbTomoDesc(_grid(sysm.pmap), len(sysm.xmaps), xm, _dptr(l2c), len(sysm.wfs), ws,
+                   int(cfg.tomo_maxit if maxit is None else maxit), int(cfg.tomo_precond),
+                   int(split), fdp, int(nbatch))
+    return d, keep
+
+
+class Reconstructor:
+    """One tomography reconstructor (``curecon_t``) on the current GPU."""
+
+    def __init__(self, sysm, nbatch: int = 1, split: int = 1, maxit: Optional[int] = None,
+                 device: int = 0):
+        self.lib = native.load()
+        check(self.lib.mb_init(device), "mb_init")
+        self.sys = sysm
+        self.nbatch = nbatch
+        d, keep = tomo_desc(sysm, nbatch=nbatch, split=split, maxit=maxit)
+        h = C.c_void_p()
+        check(self.lib.mb_setup_recon(C.byref(d), C.byref(h)), "mb_setup_recon")
+        self.h = h
+        self.ngrad = int(self.lib.mb_ngrad(h))
+        self.nxtot = int(self.lib.mb_nxtot(h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mb_recon_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _vec(self, a, n):
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(self.nbatch, n)
+        return a
+
+    def reset(self):
+        check(self.lib.mb_recon_reset(self.h), "mb_recon_reset")
+
+    def tomo(self, grad):
+        g = self._vec(grad, self.ngrad)
+        x = np.empty((self.nbatch, self.nxtot))
+        res = np.empty(self.nbatch, dtype=np.float32)
+        check(self.lib.mb_tomo(self.h, _dptr(g), _dptr(x), res.ctypes.data_as(C.POINTER(C.c_float))),
+              "mb_tomo")
+        return x, res
+
+    def tomo_device(self, d_grad_ptr: int, stream_ptr: int = 0):
+        check(self.lib.mb_tomo_device(self.h, C.c_void_p(d_grad_ptr), C.c_void_p(stream_ptr)),
+              "mb_tomo_device")
+
+    def solution_ptr(self) -> int:
+        return int(self.lib.mb_tomo_solution(self.h))
+
+    def residual(self):
+        res = np.empty(self.nbatch, dtype=np.float32)
+        check(self.lib.mb_tomo_residual(self.h, res.ctypes.data_as(C.POINTER(C.c_float))),
+              "mb_tomo_residual")
+        return res
+
+    def update_nea(self, iwfs: int, neai: np.ndarray, ptt: Optional[np.ndarray]):
+        ne = np.ascontiguousarray(neai, dtype=np.float64)
+        pt = np.ascontiguousarray(ptt, dtype=np.float64) if ptt is not None else None
+        check(self.lib.mb_update_recon_nea(self.h, iwfs, _dptr(ne),
+                                           _dptr(pt) if pt is not None else C.POINTER(C.c_double)()),
+              "mb_update_recon_nea")
+
+    def update_cn2(self, l2c, fd=None):
+        keep = []
+        l2 = np.ascontiguousarray(l2c, dtype=np.float64)
+        fdp = C.POINTER(MbFdpcgDesc)()
+        if fd is not None:
+            d = fdpcg_desc(fd, keep)
+            keep.append(d)
+            fdp = C.pointer(d)
+        check(self.lib.mb_update_recon_cn2(self.h, _dptr(l2), fdp), "mb_update_recon_cn2")
+
+    # operator applications (parity tests)
+    def apply_R(self, grad):
+        g = self._vec(grad, self.ngrad)
+        out = np.empty((self.nbatch, self.nxtot))
+        check(self.lib.mb_apply_tomo_R(self.h, _dptr(g), _dptr(out)), "mb_apply_tomo_R")
+        return out
+
+    def apply_L(self, x):
+        xi = self._vec(x, self.nxtot)
+        out = np.empty((self.nbatch, self.nxtot))
+        check(self.lib.mb_apply_tomo_L(self.h, _dptr(xi), _dptr(out)), "mb_apply_tomo_L")
+        return out
+
+    def apply_fdpcg(self, x):
+        xi = self._vec(x, self.nxtot)
+        out = np.empty((self.nbatch, self.nxtot))
+        check(self.lib.mb_apply_fdpcg(self.h, _dptr(xi), _dptr(out)), "mb_apply_fdpcg")
+        return out
+
+    def apply_hx(self, x):
+        xi = self._vec(x, self.nxtot)
+        np_ = self.sys.pmap.n
+        out = np.empty((self.nbatch, len(self.sys.wfs), np_))
+        check(self.lib.mb_apply_hx(self.h, _dptr(xi), _dptr(out)), "mb_apply_hx")
+        return out

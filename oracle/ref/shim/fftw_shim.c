@@ -6,7 +6,7 @@
  * smallest prime factor,
  *     X[k] = sum_{r<p} w_n^{r k} Y_r[k mod m],   Y_r = DFT_m( x[r + p j] ),
  * w_n = exp(sign*2*pi*i/n).  Prime lengths fall back to the direct O(n^2) sum.
- * Twiddles are evaluated from (r*k mod n) so they stay exact in argument.
+ * Twiddles come from one table per transform, indexed by (r*k mod n).
  * Transforms are unnormalised, like FFTW.  Multi-dimensional and "many"
  * transforms are executed line by line over strided views; float plans run
  * through the double-precision kernel.
@@ -33,8 +33,11 @@ struct maosref_fft_plan {
     void *ri, *ii, *ro, *io; /* split arrays */
 };
 
-static void dft_rec(cplx *x, long n, int sign, cplx *tmp) {
+/* x: n points; tw: twiddles of the top-level length N (tw[k] = w_N^k);
+ * n divides N and w_n^e = tw[e * (N/n)]. */
+static void dft_rec(cplx *x, long n, const cplx *tw, long N, cplx *tmp) {
     if (n <= 1) return;
+    const long ts = N / n;
     long p = 0;
     for (long f = 2; f * f <= n; f++) {
         if (n % f == 0) { p = f; break; }
@@ -42,39 +45,37 @@ static void dft_rec(cplx *x, long n, int sign, cplx *tmp) {
     if (!p) { /* prime: direct sum */
         for (long k = 0; k < n; k++) {
             cplx s = 0;
-            for (long j = 0; j < n; j++) {
-                long e = (j * k) % n;
-                double a = sign * 2.0 * M_PI * (double)e / (double)n;
-                s += x[j] * (cos(a) + I * sin(a));
-            }
+            for (long j = 0; j < n; j++) s += x[j] * tw[((j * k) % n) * ts];
             tmp[k] = s;
         }
         memcpy(x, tmp, sizeof(cplx) * n);
         return;
     }
     long m = n / p;
-    /* gather the p decimated subsequences contiguously into tmp, transform */
     for (long r = 0; r < p; r++)
         for (long j = 0; j < m; j++) tmp[r * m + j] = x[r + p * j];
     cplx *scratch = (cplx *)malloc(sizeof(cplx) * m);
-    for (long r = 0; r < p; r++) dft_rec(tmp + r * m, m, sign, scratch);
+    for (long r = 0; r < p; r++) dft_rec(tmp + r * m, m, tw, N, scratch);
     free(scratch);
     for (long k = 0; k < n; k++) {
         cplx s = 0;
         long km = k % m;
-        for (long r = 0; r < p; r++) {
-            long e = (r * k) % n;
-            double a = sign * 2.0 * M_PI * (double)e / (double)n;
-            s += tmp[r * m + km] * (cos(a) + I * sin(a));
-        }
+        for (long r = 0; r < p; r++) s += tmp[r * m + km] * tw[((r * k) % n) * ts];
         x[k] = s;
     }
 }
 
 static void dft_line(cplx *buf, long n, int sign) {
-    cplx *tmp = (cplx *)malloc(sizeof(cplx) * (n > 0 ? n : 1));
-    dft_rec(buf, n, sign, tmp);
+    if (n <= 1) return;
+    cplx *tw = (cplx *)malloc(sizeof(cplx) * n);
+    for (long k = 0; k < n; k++) {
+        double a = sign * 2.0 * M_PI * (double)k / (double)n;
+        tw[k] = cos(a) + I * sin(a);
+    }
+    cplx *tmp = (cplx *)malloc(sizeof(cplx) * n);
+    dft_rec(buf, n, tw, n, tmp);
     free(tmp);
+    free(tw);
 }
 
 /* element accessors on the four storage forms */

@@ -1,0 +1,95 @@
+"""GPU parity of the tomography path against the FP64 oracle.
+
+The oracle (oracle/recon_oracle.py) is pinned to the reference's compiled CPU
+code by test_oracle_pin.py.  Tolerances (relative L2, FP32 on the GPU):
+  single operator applications: 5e-5
+  full CG / FDPCG solve (30 iterations): 2e-3 on the layer OPD
+"""
+import numpy as np
+import pytest
+
+from oracle.recon_oracle import TomoOracle, tomo_solve
+
+pytestmark = pytest.mark.gpu
+
+OP_TOL = 5e-5
+SOLVE_TOL = 2e-3
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module", params=["ltao_8m", "mcao_30m"])
+def setup(request):
+    from conftest import get_system
+    from maos_b200.recon import Reconstructor
+    s = get_system(request.param)
+    R = Reconstructor(s, nbatch=2)
+    yield s, R, TomoOracle(s)
+    R.close()
+
+
+def test_hx(setup):
+    s, R, o = setup
+    x = np.random.default_rng(1).standard_normal((2, s.nx_total)) * 1e-7
+    got = R.apply_hx(x)
+    for b in range(2):
+        want = o.hx(x[b])
+        for w in range(len(s.wfs)):
+            assert rel(got[b, w], want[w]) < OP_TOL
+
+
+def test_tomo_R(setup):
+    s, R, o = setup
+    g = np.random.default_rng(2).standard_normal((2, s.ngrad)) * 1e-6
+    got = R.apply_R(g)
+    for b in range(2):
+        assert rel(got[b], o.tomo_R(g[b])) < OP_TOL
+
+
+def test_tomo_L(setup):
+    s, R, o = setup
+    x = np.random.default_rng(3).standard_normal((2, s.nx_total)) * 1e-7
+    got = R.apply_L(x)
+    for b in range(2):
+        assert rel(got[b], o.tomo_L(x[b])) < OP_TOL
+
+
+def test_fdpcg(setup):
+    s, R, o = setup
+    if s.fdpcg is None:
+        pytest.skip("plain CG configuration")
+    x = np.random.default_rng(4).standard_normal((2, s.nx_total))
+    got = R.apply_fdpcg(x)
+    for b in range(2):
+        assert rel(got[b], o.fdpcg_precond(x[b])) < OP_TOL
+
+
+def test_solve_cold_then_warm(setup):
+    s, R, o = setup
+    rng = np.random.default_rng(5)
+    g1 = rng.standard_normal((2, s.ngrad)) * 1e-6
+    g2 = g1 + rng.standard_normal((2, s.ngrad)) * 1e-7
+    R.reset()
+    x1, r1 = R.tomo(g1)
+    x2, r2 = R.tomo(g2)  # warm-started from x1
+    for b in range(2):
+        w1, res1 = tomo_solve(o, g1[b])
+        w2, res2 = tomo_solve(o, g2[b], x0=w1)
+        assert rel(x1[b], w1) < SOLVE_TOL
+        assert rel(x2[b], w2) < SOLVE_TOL
+        assert abs(r1[b] - res1) < 0.05 * res1 + 1e-6
+        assert abs(r2[b] - res2) < 0.05 * res2 + 1e-6
+
+
+def test_batch_instances_are_independent(setup):
+    s, R, o = setup
+    from maos_b200.recon import Reconstructor
+    R1 = Reconstructor(s, nbatch=1)
+    g = np.random.default_rng(6).standard_normal((2, s.ngrad)) * 1e-6
+    R.reset()
+    xb, _ = R.tomo(g)
+    x1, _ = R1.tomo(g[1:2])
+    R1.close()
+    assert rel(xb[1], x1[0]) < 1e-6
