@@ -3,10 +3,13 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl reference]
 
 Workload (one "step"): the 30 m NFIRAOS-like MCAO system (6 LGS, 60x60
-subapertures, 33,840 gradients, 6 layers / 27,648 unknowns), seeded
-frozen-flow von Karman gradients in, warm-started FP32 FDPCG tomography with
-30 iterations out, for B independent instances resident on each GPU.  The
-instances share the operator tables and advance together in one CUDA graph.
+subapertures, 33,840 gradients, 6 layers / 27,648 unknowns, 2 DMs / 9,745
+actuators, 9 fit directions), seeded frozen-flow von Karman gradients in,
+warm-started FP32 FDPCG tomography with 30 iterations, then the DM-fit CG with
+4 iterations, actuator commands out -- for B independent instances resident on
+each GPU.  The instances share the operator tables and advance together in
+one CUDA graph.  The line also carries the control-matrix MVM alternative at
+the same size (M = 9,745 x 33,840) in FP32, BF16 and FP8-E4M3.
 
 value     aggregate steps/s over all GPUs (N * B * K / max-over-ranks device time),
           inputs resident in HBM, L2 flushed (256 MiB write) before every step.
@@ -40,7 +43,8 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 WORKLOAD = "mcao_30m"
-METRIC = "recon steps/s (FP32 FDPCG tomography, 30 iterations, 30 m MCAO)"
+WORKLOAD_TEXT = "mcao_30m: FDPCG tomography 30 it + DM fit CG 4 it, warm start"
+METRIC = "recon steps/s (30 m MCAO: FP32 FDPCG tomography 30 it + DM fit 4 it)"
 
 
 def parse():
@@ -52,6 +56,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mvm-batch", type=int, default=1)
     return ap.parse_args()
 
 
@@ -129,21 +134,28 @@ class ClockSampler:
 class RefRunner:
     """The reference's own CPU reconstruction (oracle/_ref) on this host's cores."""
 
-    def __init__(self, sysm, frames):
+    def __init__(self, sysm, frames, fit=None):
         from oracle import refbridge
         self.ncores = os.cpu_count() or 1
         self.frames = frames
         self.maxit = sysm.cfg.tomo_maxit
+        self.fit_maxit = fit.maxit if fit is not None else 0
         self.R = refbridge.RefProcess(nthread=self.ncores)
         self.R.call("setup", refbridge.system_desc(sysm, split=1))
         self.R.call("fdpcg_set", sysm.fdpcg.Mbinv, sysm.fdpcg.perm, sysm.fdpcg.scale)
+        if fit is not None:
+            self.R.call("fit_setup", refbridge.fit_desc(fit))
         self.x = None
+        self.a = None
         self.k = 0
 
     def step(self):
         g = self.frames[self.k % len(self.frames)]
         b = self.R.call("tomoR", g)
         self.x, _ = self.R.call("pcg", b, self.x, int(self.x is not None), self.maxit, 1)
+        if self.fit_maxit:
+            fb = self.R.call("fitR", self.x)
+            self.a, _ = self.R.call("fit_pcg", fb, self.a, int(self.a is not None), self.fit_maxit)
         self.k += 1
 
     def rate(self, seconds: float):
@@ -165,10 +177,11 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from maos_b200 import config, geometry, turbulence
+    from maos_b200 import config, fit_setup, geometry, turbulence
     sysm = geometry.build_tomo(config.PRESETS[WORKLOAD]())
+    fit = fit_setup.build_fit(sysm)
     frames = turbulence.gradient_frames(sysm, seed=1, nframe=4)
-    run = RefRunner(sysm, frames)
+    run = RefRunner(sysm, frames, fit)
     for _ in range(max(1, args.warmup)):
         run.step()
     per = args.cpu_seconds / max(1, args.steps)
@@ -184,8 +197,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded von Karman frozen-flow gradients)",
-            "config": {"workload": f"{WORKLOAD} FDPCG tomography, 30 iterations, warm start",
-                       "instances": 1},
+            "config": {"workload": WORKLOAD_TEXT, "instances": 1},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "steps/s", "cores": run.ncores, "kind": "reference",
                              "sample": f"{total} warm reference CPU steps in {args.steps} samples"},
@@ -195,10 +207,46 @@ def run_reference(args):
     return 0
 
 
+def mvm_rates(lib, native, nact: int, ngrad: int, batch: int, stream):
+    """Control-matrix MVM steps/s per storage type (random M of the system's size)."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(3)
+    M = np.asfortranarray(rng.standard_normal((nact, ngrad)) * 1e-3)
+    g = torch.randn(batch, ngrad, device="cuda")
+    out = torch.empty(batch, nact, device="cuda")
+    res = {"batch": batch, "shape": [nact, ngrad]}
+    peak, _ = measured_peaks()
+    for name, dt in (("fp32", 0), ("bf16", 1), ("fp8_e4m3", 2)):
+        h = C.c_void_p()
+        native.check(lib.mb_mvm_create(M.ctypes.data_as(C.POINTER(C.c_double)), nact, ngrad, dt, batch,
+                                       C.byref(h)), "mb_mvm_create")
+        sp = stream.cuda_stream
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                lib.mb_mvm_apply_device(h, C.c_void_p(g.data_ptr()), C.c_void_p(out.data_ptr()), C.c_void_p(sp))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            n = 20
+            e0.record(stream)
+            for _ in range(n):
+                lib.mb_mvm_apply_device(h, C.c_void_p(g.data_ptr()), C.c_void_p(out.data_ptr()), C.c_void_p(sp))
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / n
+        nbytes = lib.mb_mvm_bytes(h)
+        res[name] = {"steps_per_s": batch * 1000.0 / ms, "ms": ms, "matrix_bytes": int(nbytes),
+                     "hbm_frac": nbytes / (ms / 1000.0) / 1e9 / peak}
+        lib.mb_mvm_free(h)
+    del M
+    return res
+
+
 def run_gpu(args):
     import numpy as np
     import torch
-    from maos_b200 import config, geometry, native, turbulence
+    from maos_b200 import config, fit_setup, geometry, native, turbulence
     from maos_b200.recon import Reconstructor
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -212,6 +260,7 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     sysm = geometry.build_tomo(config.PRESETS[WORKLOAD]())
+    fit = fit_setup.build_fit(sysm)
     B = args.batch
     nframe = 4
     # gradients: 4 frozen-flow frames for each of 4 seeds, tiled over instances
@@ -222,13 +271,13 @@ def run_gpu(args):
     host_grads = [np.ascontiguousarray(grads[k]) for k in range(nframe)]
 
     lib = native.load()
-    R = Reconstructor(sysm, nbatch=B, device=local)
+    R = Reconstructor(sysm, nbatch=B, device=local, fit=fit)
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def step(k):
-        R.tomo_device(grads_dev[k % nframe].data_ptr(), sp)
+        R.step_device(grads_dev[k % nframe].data_ptr(), sp)
 
     with torch.cuda.stream(stream):
         for k in range(args.warmup):
@@ -262,16 +311,19 @@ def run_gpu(args):
     p50 = statistics.median(times)
     p99 = times_sorted[min(len(times) - 1, int(math.ceil(0.99 * len(times))) - 1)]
 
-    # end to end through the host API (FP64 host gradients in, FP64 OPD out)
+    # end to end through the host API: gpu_tomo then gpu_fit (FP64 host
+    # gradients in, FP64 host actuator commands out)
     K2 = max(3, min(args.steps, 20))
     for k in range(2):
-        R.tomo(host_grads[k % nframe])
+        R.tomo_only(host_grads[k % nframe])
+        R.fit()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for k in range(K2):
-        R.tomo(host_grads[k % nframe])
+        R.tomo_only(host_grads[k % nframe])
+        R.fit()
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if dist:
@@ -299,11 +351,13 @@ def run_gpu(args):
             "share_of_step": dom["share_ms"] / tot_stage,
             "stage_ms_per_step": {s["name"]: round(s["share_ms"], 4) for s in stages}}
 
+    mvm_line = mvm_rates(lib, native, int(fit.nact), int(sysm.ngrad), args.mvm_batch, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import refbridge
         if refbridge.available():
-            run = RefRunner(sysm, fr[0])
+            run = RefRunner(sysm, fr[0], fit)
             run.step()
             rate, n, dt = run.rate(args.cpu_seconds)
             run.close()
@@ -315,14 +369,15 @@ def run_gpu(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded von Karman frozen-flow gradients, 4 seeds x 4 frames)",
-                "config": {"workload": f"{WORKLOAD} FDPCG tomography, 30 iterations, warm start",
-                           "instances_per_gpu": B, "ngrad": int(sysm.ngrad),
+                "config": {"workload": WORKLOAD_TEXT,
+                           "instances_per_gpu": B, "ngrad": int(sysm.ngrad), "nact": int(fit.nact),
                            "nxtot": int(sysm.nx_total), "l2": "flushed before every step (256 MiB write)",
                            "parallelism": f"replicas x{world}"},
                 "latency_ms": {"p50": p50, "p99": p99, "note": "one batched step of all instances"},
                 "e2e": {"value": e2e_value, "unit": "steps/s",
                         "h2d_bytes_per_step": int(B * sysm.ngrad * 4),
-                        "d2h_bytes_per_step": int(B * sysm.nx_total * 4 + B * 4)},
+                        "d2h_bytes_per_step": int(B * fit.nact * 4 + 2 * B * 4)},
+                "mvm": mvm_line,
                 "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)

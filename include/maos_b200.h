@@ -76,7 +76,31 @@ typedef struct {
     const double *mbinv; /* [nb*bs*bs*2] fdpcg->Mbinv, complex, column-major blocks */
 } mb_fdpcg_desc;
 
-/* Everything gpu_setup_recon (cuda/recon.cu:477) reads for tomography. */
+/* DM fit in grid form (cuda/fit.cu cufit_grid; recon->fit, maos/setup_recon_fit.c):
+ *   FitR x = sum_f wt_f HA_f^T (W0 - W1 W1^T) Hxp_f x
+ *   FitL a = sum_f wt_f HA_f^T (W0 - W1 W1^T) HA_f a + NW NW^T a
+ * HA and Hxp are bilinear ray tracing onto the fit grid, built internally from
+ * the grids below (the grid form requires fit.square=1: every point of each
+ * DM grid is an actuator, maos/setup_parms.c:3001). */
+typedef struct {
+    mb_grid floc;          /* fit grid (recon->fmap) */
+    int nfit;              /* fit directions */
+    const double *thetax;  /* [nfit] (rad) */
+    const double *thetay;
+    const double *wt;      /* [nfit] fit.wt */
+    const double *hs;      /* [nfit] fit.hs (INFINITY for science directions) */
+    const int *w0_p;       /* W0: nfloc x nfloc CSC (recon->W0) */
+    const int *w0_i;
+    const double *w0_x;
+    const double *w1;      /* [nfloc] recon->W1 */
+    int ndm;
+    const mb_grid *amap;   /* [ndm] actuator grids with ht (recon->amap) */
+    int nnw;               /* low-rank columns (fit->NW) */
+    const double *nw;      /* [nact_total x nnw] column-major, DMs concatenated */
+    int maxit;             /* fit.maxit */
+} mb_fit_desc;
+
+/* Everything gpu_setup_recon (cuda/recon.cu:477) reads. */
 typedef struct {
     mb_grid pmap;          /* pupil grid of ploc (tomo.square=1) */
     int nps;               /* reconstructed layers */
@@ -89,7 +113,8 @@ typedef struct {
     int split;             /* recon.split: non-zero skips tip/tilt removal in the LHS */
     const mb_fdpcg_desc *fdpcg; /* required when precond==1 */
     int nbatch;            /* independent instances sharing these tables (>=1) */
-} mb_tomo_desc;
+    const mb_fit_desc *fit; /* optional DM fit (NULL: tomography only) */
+} mb_recon_desc;
 
 /* gpu_init (cuda/gpu.h:27): select the device for subsequent setups. */
 int mb_init(int device);
@@ -97,7 +122,7 @@ int mb_init(int device);
 void mb_cleanup(void);
 
 /* gpu_setup_recon (cuda/gpu.h:47): build a reconstructor on the current device. */
-int mb_setup_recon(const mb_tomo_desc *desc, mb_recon **out);
+int mb_setup_recon(const mb_recon_desc *desc, mb_recon **out);
 /* gpu_recon_free (declared at cuda/gpu.h:54). */
 void mb_recon_free(mb_recon *r);
 /* gpu_recon_reset (cuda/gpu.h:52): zero the warm-start state of every instance. */
@@ -111,6 +136,19 @@ int mb_update_recon_cn2(mb_recon *r, const double *l2c, const mb_fdpcg_desc *fdp
  * grad: [nbatch][ngrad] host FP64 gradients.  opdr: optional host output
  * [nbatch][nxtot].  cgres: optional [nbatch] final CG residual |r|/|b|. */
 int mb_tomo(mb_recon *r, const double *grad, double *opdr, float *cgres);
+
+/* gpu_fit (cuda/gpu.h:56, curecon_t::fit cuda/recon.cu:277): DM fit of the
+ * current tomography solution.  dmout: [nbatch][nact] host FP64 actuator
+ * commands (overwritten, like add2cpu(...,0,...) at recon.cu:285).  cgres:
+ * optional [nbatch] fit CG residual. */
+int mb_fit(mb_recon *r, double *dmout, float *cgres);
+/* One whole reconstruction step (tomography then fit) on the device, one
+ * graph launch: d_grad [nbatch][ngrad] FP32 device in; the actuator commands
+ * stay on the device (mb_fit_solution). */
+int mb_recon_step_device(mb_recon *r, const float *d_grad, void *stream);
+/* Device pointer to the FP32 DM commands [nbatch][nact]. */
+const float *mb_fit_solution(mb_recon *r);
+long mb_nact(const mb_recon *r);
 
 /* Device-resident form of mb_tomo for batched serving and benchmarks:
  * d_grad is a device FP32 buffer [nbatch][ngrad]; stream is a cudaStream_t
@@ -133,6 +171,27 @@ int mb_apply_tomo_R(mb_recon *r, const double *grad, double *xout);    /* TomoR 
 int mb_apply_tomo_L(mb_recon *r, const double *xin, double *xout);     /* TomoL */
 int mb_apply_fdpcg(mb_recon *r, const double *xin, double *xout);      /* fdpcg_precond */
 int mb_apply_hx(mb_recon *r, const double *xin, double *opd);          /* Hx: [nbatch][nwfs][np] */
+int mb_apply_fit_R(mb_recon *r, const double *xin, double *aout);      /* FitR */
+int mb_apply_fit_L(mb_recon *r, const double *ain, double *aout);      /* FitL */
+
+/* ---- Control-matrix MVM (recon.mvm): a = M g ---- */
+#define MB_MVM_F32 0   /* FP32 storage */
+#define MB_MVM_BF16 1  /* BF16 storage */
+#define MB_MVM_FP8 2   /* FP8-E4M3 storage with one FP32 scale per row */
+typedef struct mb_mvm mb_mvm;
+/* gpu_setup_recon_mvm (cuda/gpu.h:48): install the control matrix.  Mcol is
+ * recon->MVM: nact x ngrad, column-major FP64.  It is converted once to the
+ * requested storage type; products accumulate in FP32.  nbatch instances
+ * share M and are applied together. */
+int mb_mvm_create(const double *Mcol, long nact, long ngrad, int dtype, int nbatch, mb_mvm **out);
+void mb_mvm_free(mb_mvm *m);
+/* Bytes of control-matrix storage on the device (M plus row scales). */
+long mb_mvm_bytes(const mb_mvm *m);
+/* gpu_recon_mvm (cuda/gpu.h:57): host FP64 gradients [nbatch][ngrad] in,
+ * host FP64 DM commands [nbatch][nact] out (overwritten). */
+int mb_recon_mvm(mb_mvm *m, const double *grad, double *dmout);
+/* Device form: FP32 [nbatch][ngrad] in, FP32 [nbatch][nact] out, on `stream`. */
+int mb_mvm_apply_device(mb_mvm *m, const float *d_grad, float *d_out, void *stream);
 
 /* Per-stage timing for roofline accounting.  Stages are the kernels of one
  * CG iteration (see mb_stage_name).  For each stage: average device time of

@@ -1,0 +1,296 @@
+// Control-matrix MVM: a = M g for a batch of instances sharing M
+// (gpu_recon_mvm, cuda/gpu.h:57; curecon_t::mvm cuda/recon.cu:345, which is a
+// cuBLAS sgemv in the reference, cuda/solve.h:131).
+//
+// M is stored row-major [nact][ldm] (ldm = ngrad rounded up to the K tile) in
+// FP32, BF16, or FP8-E4M3 with one FP32 scale per row; accumulation is FP32.
+// The kernel is split-K: CTA (rt, ks) multiplies a tile of kRows rows by a
+// kK-column slab, with that slab of every instance's gradients staged in
+// shared memory, and writes per-split partial sums; a second kernel adds the
+// splits in fixed order and applies the row scale (deterministic, no atomics).
+// Each warp streams rows with 16-byte vector loads, so M is read exactly once.
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mb {
+
+constexpr int kK = 2048;       // columns per split
+constexpr int kRows = 32;      // rows per CTA (4 per warp)
+constexpr int kMvmThreads = 256;
+constexpr int kMaxBatch = 16;  // instances per launch pass
+
+template <int DT>
+struct Elem;
+template <>
+struct Elem<MB_MVM_F32> {
+    using T = float;
+    static constexpr int kVec = 4;  // elements per 16 bytes
+    __device__ static void load(const T *p, float *v) {
+        const float4 q = *reinterpret_cast<const float4 *>(p);
+        v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    }
+};
+template <>
+struct Elem<MB_MVM_BF16> {
+    using T = __nv_bfloat16;
+    static constexpr int kVec = 8;
+    __device__ static void load(const T *p, float *v) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(p);
+        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float2 f = __bfloat1622float2(h[i]);
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+        }
+    }
+};
+template <>
+struct Elem<MB_MVM_FP8> {
+    using T = __nv_fp8_e4m3;
+    static constexpr int kVec = 16;
+    __device__ static void load(const T *p, float *v) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(p);
+        const __nv_fp8x2_e4m3 *h = reinterpret_cast<const __nv_fp8x2_e4m3 *>(&q);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const float2 f = static_cast<float2>(h[i]);
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+        }
+    }
+};
+
+// part[(ks*nbatch + b)*nact + row] = sum over this K slab of M[row][k] g[b][k]
+template <int DT, int NB>
+__global__ void __launch_bounds__(kMvmThreads)
+k_mvm_split(const typename Elem<DT>::T *__restrict__ M, long ldm, const float *__restrict__ g,
+            long ngrad, float *__restrict__ part, int nact, int nbatch, int b0) {
+    using E = Elem<DT>;
+    constexpr int V = E::kVec;
+    extern __shared__ float sg[];  // [NB][kK]
+    const int ks = blockIdx.y;
+    const long k0 = (long)ks * kK;
+    const int kn = (int)((ngrad - k0) < kK ? (ngrad - k0) : kK);
+    for (int i = threadIdx.x; i < NB * kK; i += blockDim.x) {
+        const int b = i / kK, k = i - b * kK;
+        sg[i] = (b0 + b < nbatch && k < kn) ? g[(size_t)(b0 + b) * ngrad + k0 + k] : 0.f;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int kRowsPerWarp = kRows / (kMvmThreads / 32);
+    for (int rr = 0; rr < kRowsPerWarp; rr++) {
+        const int row = blockIdx.x * kRows + warp * kRowsPerWarp + rr;
+        if (row >= nact) break;
+        const typename E::T *mrow = M + (size_t)row * ldm + k0;
+        float acc[NB];
+#pragma unroll
+        for (int b = 0; b < NB; b++) acc[b] = 0.f;
+        // lanes stride by V elements; the slab is a multiple of 32*V elements
+        for (int c = lane * V; c < kK; c += 32 * V) {
+            float v[V];
+            E::load(mrow + c, v);
+#pragma unroll
+            for (int b = 0; b < NB; b++) {
+                const float4 *gb = reinterpret_cast<const float4 *>(sg + b * kK + c);
+#pragma unroll
+                for (int e4 = 0; e4 < V / 4; e4++) {
+                    const float4 q = gb[e4];
+                    acc[b] += v[4 * e4] * q.x + v[4 * e4 + 1] * q.y + v[4 * e4 + 2] * q.z +
+                              v[4 * e4 + 3] * q.w;
+                }
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            float t = acc[b];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0 && b0 + b < nbatch) part[((size_t)ks * nbatch + b0 + b) * nact + row] = t;
+        }
+    }
+}
+
+// out[b][row] = scale[row] * sum_ks part[ks][b][row]
+__global__ void k_mvm_reduce(const float *__restrict__ part, const float *__restrict__ scale,
+                             float *__restrict__ out, int nact, int nbatch, int nks) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)nact * nbatch) return;
+    const int b = (int)(t / nact), row = (int)(t - (long)b * nact);
+    float s = 0.f;
+    for (int k = 0; k < nks; k++) s += part[((size_t)k * nbatch + b) * nact + row];
+    out[(size_t)b * nact + row] = scale ? s * scale[row] : s;
+}
+
+struct Mvm {
+    int dtype = MB_MVM_F32;
+    int nact = 0, nbatch = 1, nks = 0;
+    long ngrad = 0, ldm = 0;
+    DevBuf<unsigned char> m;  // raw storage
+    DevBuf<float> scale, part, g, out;
+    cudaStream_t stream = nullptr;
+    ~Mvm() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <int DT, int NB>
+    void launch_t(const float *dg, float *dout, cudaStream_t s) {
+        const size_t smem = (size_t)NB * kK * sizeof(float);
+        static bool attr = false;
+        if (!attr) {
+            MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_split<DT, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem));
+            attr = true;
+        }
+        const dim3 grid((nact + kRows - 1) / kRows, nks);
+        for (int b0 = 0; b0 < nbatch; b0 += NB) {
+            k_mvm_split<DT, NB><<<grid, kMvmThreads, smem, s>>>(
+                reinterpret_cast<const typename Elem<DT>::T *>(m.p), ldm, dg, ngrad, part.p, nact, nbatch, b0);
+            MB_CHECK_LAUNCH();
+        }
+        const long n = (long)nact * nbatch;
+        k_mvm_reduce<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part.p, dtype == MB_MVM_FP8 ? scale.p : nullptr,
+                                                                dout, nact, nbatch, nks);
+        MB_CHECK_LAUNCH();
+    }
+    template <int DT>
+    void launch_dt(const float *dg, float *dout, cudaStream_t s) {
+        if (nbatch == 1) launch_t<DT, 1>(dg, dout, s);
+        else if (nbatch == 2) launch_t<DT, 2>(dg, dout, s);
+        else if (nbatch <= 4) launch_t<DT, 4>(dg, dout, s);
+        else if (nbatch <= 8) launch_t<DT, 8>(dg, dout, s);
+        else launch_t<DT, kMaxBatch>(dg, dout, s);
+    }
+    void apply(const float *dg, float *dout, cudaStream_t s) {
+        switch (dtype) {
+            case MB_MVM_F32: launch_dt<MB_MVM_F32>(dg, dout, s); break;
+            case MB_MVM_BF16: launch_dt<MB_MVM_BF16>(dg, dout, s); break;
+            default: launch_dt<MB_MVM_FP8>(dg, dout, s); break;
+        }
+    }
+};
+
+}  // namespace mb
+
+struct mb_mvm {
+    mb::Mvm M;
+};
+
+extern "C" {
+
+int mb_mvm_create(const double *Mcol, long nact, long ngrad, int dtype, int nbatch, mb_mvm **out) {
+    if (!out || !Mcol || nact <= 0 || ngrad <= 0 || nbatch < 1 || nact > (1L << 30)) {
+        mb::set_error("mb_mvm_create: invalid arguments");
+        return MB_EINVAL;
+    }
+    if (dtype != MB_MVM_F32 && dtype != MB_MVM_BF16 && dtype != MB_MVM_FP8) {
+        mb::set_error("mb_mvm_create: unknown dtype %d", dtype);
+        return MB_EINVAL;
+    }
+    *out = nullptr;
+    mb_mvm *h = new (std::nothrow) mb_mvm();
+    if (!h) return MB_ENOMEM;
+    try {
+        mb::Mvm &V = h->M;
+        V.dtype = dtype;
+        V.nact = (int)nact;
+        V.ngrad = ngrad;
+        V.nbatch = nbatch;
+        V.nks = (int)((ngrad + mb::kK - 1) / mb::kK);
+        V.ldm = (long)V.nks * mb::kK;
+        MB_CUDA_TRY(cudaStreamCreateWithFlags(&V.stream, cudaStreamNonBlocking));
+        const size_t nel = (size_t)nact * V.ldm;
+        std::vector<float> sc(nact, 1.f);
+        if (dtype == MB_MVM_F32) {
+            std::vector<float> h32(nel, 0.f);
+            for (long r = 0; r < nact; r++)
+                for (long c = 0; c < ngrad; c++) h32[(size_t)r * V.ldm + c] = (float)Mcol[(size_t)c * nact + r];
+            V.m.alloc(nel * 4);
+            MB_CUDA_TRY(cudaMemcpy(V.m.p, h32.data(), nel * 4, cudaMemcpyHostToDevice));
+        } else if (dtype == MB_MVM_BF16) {
+            std::vector<__nv_bfloat16> h16(nel, __float2bfloat16(0.f));
+            for (long r = 0; r < nact; r++)
+                for (long c = 0; c < ngrad; c++)
+                    h16[(size_t)r * V.ldm + c] = __float2bfloat16((float)Mcol[(size_t)c * nact + r]);
+            V.m.alloc(nel * 2);
+            MB_CUDA_TRY(cudaMemcpy(V.m.p, h16.data(), nel * 2, cudaMemcpyHostToDevice));
+        } else {
+            // per-row scale maps the row's largest magnitude to the e4m3 maximum (448)
+            std::vector<__nv_fp8_e4m3> h8(nel, __nv_fp8_e4m3(0.f));
+            for (long r = 0; r < nact; r++) {
+                double mx = 0;
+                for (long c = 0; c < ngrad; c++) mx = std::max(mx, std::fabs(Mcol[(size_t)c * nact + r]));
+                const double s = mx > 0 ? mx / 448.0 : 1.0;
+                sc[r] = (float)s;
+                for (long c = 0; c < ngrad; c++)
+                    h8[(size_t)r * V.ldm + c] = __nv_fp8_e4m3((float)(Mcol[(size_t)c * nact + r] / s));
+            }
+            V.m.alloc(nel);
+            MB_CUDA_TRY(cudaMemcpy(V.m.p, h8.data(), nel, cudaMemcpyHostToDevice));
+        }
+        V.scale.upload(sc);
+        V.part.alloc((size_t)V.nks * nbatch * nact);
+        V.g.alloc((size_t)nbatch * ngrad);
+        V.out.alloc((size_t)nbatch * nact);
+    } catch (const mb::CudaError &e) {
+        delete h;
+        return e.code;
+    } catch (...) {
+        delete h;
+        mb::set_error("mb_mvm_create: unexpected exception");
+        return MB_ECUDA;
+    }
+    *out = h;
+    return MB_OK;
+}
+
+void mb_mvm_free(mb_mvm *h) { delete h; }
+
+long mb_mvm_bytes(const mb_mvm *h) {
+    if (!h) return -1;
+    const mb::Mvm &V = h->M;
+    const long el = V.dtype == MB_MVM_F32 ? 4 : V.dtype == MB_MVM_BF16 ? 2 : 1;
+    return (long)V.nact * V.ngrad * el + (V.dtype == MB_MVM_FP8 ? 4L * V.nact : 0);
+}
+
+int mb_mvm_apply_device(mb_mvm *h, const float *d_grad, float *d_out, void *stream) {
+    if (!h || !d_grad || !d_out) {
+        mb::set_error("mb_mvm_apply_device: invalid arguments");
+        return MB_EINVAL;
+    }
+    try {
+        h->M.apply(d_grad, d_out, (cudaStream_t)stream);
+    } catch (const mb::CudaError &e) {
+        return e.code;
+    }
+    return MB_OK;
+}
+
+int mb_recon_mvm(mb_mvm *h, const double *grad, double *dmout) {
+    if (!h || !grad || !dmout) {
+        mb::set_error("mb_recon_mvm: invalid arguments");
+        return MB_EINVAL;
+    }
+    try {
+        mb::Mvm &V = h->M;
+        const size_t ng = (size_t)V.nbatch * V.ngrad, na = (size_t)V.nbatch * V.nact;
+        std::vector<float> tmp(std::max(ng, na));
+        for (size_t i = 0; i < ng; i++) tmp[i] = (float)grad[i];
+        MB_CUDA_TRY(cudaMemcpyAsync(V.g.p, tmp.data(), ng * 4, cudaMemcpyHostToDevice, V.stream));
+        V.apply(V.g.p, V.out.p, V.stream);
+        MB_CUDA_TRY(cudaMemcpyAsync(tmp.data(), V.out.p, na * 4, cudaMemcpyDeviceToHost, V.stream));
+        MB_CUDA_TRY(cudaStreamSynchronize(V.stream));
+        for (size_t i = 0; i < na; i++) dmout[i] = tmp[i];
+    } catch (const mb::CudaError &e) {
+        return e.code;
+    }
+    return MB_OK;
+}
+
+}  // extern "C"

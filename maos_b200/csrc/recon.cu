@@ -18,6 +18,9 @@
 #include <memory>
 #include <mutex>
 #include <atomic>
+#include <climits>
+#include <cstdint>
+#include <functional>
 #include <vector>
 
 #include "common.cuh"
@@ -48,6 +51,17 @@ struct CufftError {};
         }                                                                           \
     } while (0)
 
+// Forward tables for (direction d, source grid t) and their exact transposes
+// as per-axis CSR lists over the source grid (gather form).
+struct RayTables {
+    DevBuf<AxisW> fwd;
+    DevBuf<int> ptr, idxptr;
+    DevBuf<GatherW> ent;
+    std::vector<int> h_ptr, h_idxptr;  // host copies for tiling decisions
+    std::vector<GatherW> h_ent;
+    GatherIndex gi() const { return GatherIndex{ptr.p, idxptr.p, ent.p}; }
+};
+
 struct Recon {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -62,11 +76,14 @@ struct Recon {
     std::vector<int> nsa;
 
     // tables
-    DevBuf<AxisW> hx_tab;
+    RayTables hx;
+    DevBuf<TileDesc> tiles;
+    DevBuf<int2> rowrange;
+    int ntiles = 0, tile_rows = 0, maxrows = 0, maxnx = 0, maxent = 0;
+    size_t hxt_smem = 0;
     DevBuf<LayerDev> lay;
     std::vector<LayerDev> lay_h;
-    DevBuf<int> gi_ptr, gi_idxptr;
-    DevBuf<GatherW> gi_ent;
+    std::vector<mb_grid> xgrid;   // host copy of the layer grids
     DevBuf<WfsDev> wfs;
     std::vector<std::unique_ptr<DevBuf<int2>>> saptr;
     std::vector<std::unique_ptr<DevBuf<float2>>> gp;
@@ -87,20 +104,39 @@ struct Recon {
     DevBuf<double> tt_part, pap_part, rr_part, rz_part, bb_part, sc;
     DevBuf<float> res;
 
-    cudaGraphExec_t graph = nullptr;
-    long graph_kernels = 0;
+    // DM fit
+    int has_fit = 0, nfit = 0, ndm = 0, nfx = 0, nfy = 0, nf = 0, nnw = 0, fit_maxit = 0;
+    int nblk_a = 0, nblk_f = 0, fnsc = 0;
+    long nact = 0;
+    RayTables hxp, ha;
+    DevBuf<LayerDev> dmlay;
+    std::vector<LayerDev> dmlay_h;
+    DevBuf<int> w0_rp, w0_ci;
+    DevBuf<float> w0_v, w1v, fwt, nwv;
+    DevBuf<float> fa, fr, fp, fAp, frhs, opdf, opdw;
+    DevBuf<double> w1_part, nw_part, f_pap, f_rr, f_rz, f_bb, fsc;
+    DevBuf<float> fres;
+
+    cudaGraphExec_t graph = nullptr;       // tomography step
+    cudaGraphExec_t graph_fit = nullptr;   // fit step
+    cudaGraphExec_t graph_step = nullptr;  // tomography + fit
+    long graph_kernels = 0, graph_fit_kernels = 0, graph_step_kernels = 0;
 
     ~Recon() {
         if (graph) cudaGraphExecDestroy(graph);
+        if (graph_fit) cudaGraphExecDestroy(graph_fit);
+        if (graph_step) cudaGraphExecDestroy(graph_step);
         for (auto h : plans) cufftDestroy(h);
         if (stream) cudaStreamDestroy(stream);
     }
 
     // ------------------------------------------------------------------
-    void build(const mb_tomo_desc *d);
-    void build_hx_tables(const mb_tomo_desc *d);
-    void build_wfs_tables(const mb_tomo_desc *d);
+    void build(const mb_recon_desc *d);
+    void build_hx_tables(const mb_recon_desc *d);
+    void build_tiles();
+    void build_wfs_tables(const mb_recon_desc *d);
     void build_fdpcg(const mb_fdpcg_desc *fd);
+    void build_fit(const mb_fit_desc *f);
     void set_neai(int iwfs, const double *neai, const double *ptt);
     void set_l2c(const double *l2c);
 
@@ -110,8 +146,22 @@ struct Recon {
     void op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t s);
     void op_fdpcg(const float *rin, float *zout, double *rz_part, cudaStream_t s);
     void enqueue_solve(cudaStream_t s);
+    struct CgBufs {
+        float *x, *r, *p, *z, *Ap, *rhs;
+        double *pap, *rr, *rz, *bb, *sc;
+        float *res;
+        int nsc;
+        int nblk_pap;  // partials the A-multiply writes for p.Ap
+    };
+    void enqueue_cg(const CgBufs &B, long n, int nblk, int iters,
+                    const std::function<void(const float *, float *, double *)> &Amul,
+                    const std::function<void(const float *, float *, double *)> &Mmul, cudaStream_t s);
+    void op_fitR(const float *xin, float *out, cudaStream_t s);
+    void op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t s);
+    void enqueue_fit(cudaStream_t s);
     void time_stages(int reps, float *ms, double *bytes, int *launches);
     void capture_graph();
+    cudaGraphExec_t capture(const std::function<void(cudaStream_t)> &body, long &nkernels);
     void run_graph(cudaStream_t s);
 };
 
@@ -119,18 +169,21 @@ struct Recon {
 // tables
 // ---------------------------------------------------------------------------
 
-// Bilinear weights of one axis: pupil coordinate c maps to layer index
+// Bilinear weights of one axis: output coordinate c maps to source index
 // u = (c*scale + disp - o)/d.  Same inclusion rule as the reference CPU ray
 // tracer (lib/prop_grid.c): 0 <= u <= n-1, a point on the last sample uses
-// that sample alone.
-static void axis_weights(const mb_grid &pm, int n_out, double o_out, double d_out, bool isy,
-                         double scale, double disp, const mb_grid &g, std::vector<AxisW> &out) {
-    const double o_in = isy ? g.oy : g.ox, d_in = isy ? g.dy : g.dx;
-    const int n_in = isy ? g.ny : g.nx;
-    (void)pm;
+// that sample alone.  With `snap`, coordinates within 1e-9 of a sample are
+// moved onto it first (lib/mkh.c keeps a corner whose weight exceeds EPS, so
+// a ray a rounding error outside the first or last sample still counts).
+static void axis_weights(int n_out, double o_out, double d_out, double scale, double disp,
+                         double o_in, double d_in, int n_in, bool snap, std::vector<AxisW> &out) {
     for (int i = 0; i < n_out; i++) {
         const double c = o_out + i * d_out;
-        const double u = (c * scale + disp - o_in) / d_in;
+        double u = (c * scale + disp - o_in) / d_in;
+        if (snap) {
+            const double r = std::round(u);
+            if (std::fabs(u - r) < 1e-9) u = r;
+        }
         long k = (long)std::floor(u);
         double f = u - k;
         if (k == n_in - 1 && f < 1e-12) {
@@ -150,31 +203,31 @@ static void axis_weights(const mb_grid &pm, int n_out, double o_out, double d_ou
     }
 }
 
-void Recon::build_hx_tables(const mb_tomo_desc *d) {
-    const mb_grid &pm = d->pmap;
+
+static void build_ray_tables(const mb_grid &og, int ndir, int nt, const mb_grid *tg,
+                             const std::function<void(int, int, double &, double &, double &)> &geom,
+                             bool snap, RayTables &rt) {
+    const int nxo = og.nx, nyo = og.ny;
     std::vector<AxisW> tab;
-    tab.reserve((size_t)nwfs * nps * (nxp + nyp));
-    for (int w = 0; w < nwfs; w++) {
-        const mb_wfs_desc &W = d->wfs[w];
-        for (int l = 0; l < nps; l++) {
-            const mb_grid &g = d->xmap[l];
-            const double ht = g.ht;
-            const double scale = std::isinf(W.hs) ? 1.0 : 1.0 - ht / W.hs;
-            axis_weights(pm, nxp, pm.ox, pm.dx, false, scale, W.thetax * ht, g, tab);
-            axis_weights(pm, nyp, pm.oy, pm.dy, true, scale, W.thetay * ht, g, tab);
+    tab.reserve((size_t)ndir * nt * (nxo + nyo));
+    for (int d = 0; d < ndir; d++)
+        for (int t = 0; t < nt; t++) {
+            double scale, dx, dy;
+            geom(d, t, scale, dx, dy);
+            const mb_grid &g = tg[t];
+            axis_weights(nxo, og.ox, og.dx, scale, dx, g.ox, g.dx, g.nx, snap, tab);
+            axis_weights(nyo, og.oy, og.dy, scale, dy, g.oy, g.dy, g.ny, snap, tab);
         }
-    }
-    hx_tab.upload(tab);
-    // transposed tables: for each (w, l, axis) a CSR over layer indices
+    rt.fwd.upload(tab);
     std::vector<int> ptr, idxptr;
     std::vector<GatherW> ent;
-    for (int w = 0; w < nwfs; w++) {
-        for (int l = 0; l < nps; l++) {
-            const AxisW *t = tab.data() + (size_t)(w * nps + l) * (nxp + nyp);
+    for (int d = 0; d < ndir; d++)
+        for (int t = 0; t < nt; t++) {
+            const AxisW *tt = tab.data() + (size_t)(d * nt + t) * (nxo + nyo);
             for (int axis = 0; axis < 2; axis++) {
-                const int n_in = axis ? d->xmap[l].ny : d->xmap[l].nx;
-                const int n_out = axis ? nyp : nxp;
-                const AxisW *ta = t + (axis ? nxp : 0);
+                const int n_in = axis ? tg[t].ny : tg[t].nx;
+                const int n_out = axis ? nyo : nxo;
+                const AxisW *ta = tt + (axis ? nxo : 0);
                 ptr.push_back((int)idxptr.size());
                 std::vector<std::vector<GatherW>> lists(n_in);
                 for (int i = 0; i < n_out; i++) {
@@ -189,14 +242,74 @@ void Recon::build_hx_tables(const mb_tomo_desc *d) {
                 idxptr.push_back((int)ent.size());
             }
         }
-    }
-    // ptr[] points at the start of each CSR's row-pointer block
-    gi_ptr.upload(ptr);
-    gi_idxptr.upload(idxptr);
-    gi_ent.upload(ent);
+    rt.ptr.upload(ptr);
+    rt.idxptr.upload(idxptr);
+    rt.ent.upload(ent);
+    rt.h_ptr = std::move(ptr);
+    rt.h_idxptr = std::move(idxptr);
+    rt.h_ent = std::move(ent);
 }
 
-void Recon::build_wfs_tables(const mb_tomo_desc *d) {
+void Recon::build_hx_tables(const mb_recon_desc *d) {
+    build_ray_tables(d->pmap, nwfs, nps, d->xmap,
+                     [&](int w, int l, double &scale, double &dx, double &dy) {
+                         const mb_wfs_desc &W = d->wfs[w];
+                         const double ht = d->xmap[l].ht;
+                         scale = std::isinf(W.hs) ? 1.0 : 1.0 - ht / W.hs;
+                         dx = W.thetax * ht;
+                         dy = W.thetay * ht;
+                     },
+                     false, hx);
+}
+
+// Row tiles of every layer and, per tile and WFS, the pupil rows whose
+// transposed bilinear weights reach the tile (union of the y-gather lists).
+void Recon::build_tiles() {
+    maxnx = 0;
+    for (int l = 0; l < nps; l++) maxnx = std::max(maxnx, lay_h[l].nx);
+    MB_REQUIRE(maxnx <= kThreads * kMaxOwn, "layer grid too wide (%d)", maxnx);
+    int rows = std::min(8, kThreads * kMaxOwn / maxnx);
+    auto count = [&](int r) {
+        int n = 0;
+        for (int l = 0; l < nps; l++) n += (lay_h[l].ny + r - 1) / r;
+        return n;
+    };
+    while (rows > 1 && (long)count(rows) * nb < 2 * 148) rows /= 2;  // keep >= 2 waves on 148 SMs
+    tile_rows = rows;
+    std::vector<TileDesc> tl;
+    for (int l = 0; l < nps; l++)
+        for (int y0 = 0; y0 < lay_h[l].ny; y0 += rows) tl.push_back(TileDesc{l, y0, std::min(rows, lay_h[l].ny - y0)});
+    ntiles = (int)tl.size();
+    std::vector<int2> rr((size_t)ntiles * nwfs);
+    maxrows = 1;
+    maxent = 1;
+    for (int w = 0; w < nwfs; w++)
+        for (int l = 0; l < nps; l++) {
+            const int tx = hx.h_ptr[(w * nps + l) * 2 + 0];
+            maxent = std::max(maxent, hx.h_idxptr[tx + lay_h[l].nx] - hx.h_idxptr[tx]);
+        }
+    for (int t = 0; t < ntiles; t++) {
+        const TileDesc &T = tl[t];
+        for (int w = 0; w < nwfs; w++) {
+            const int ty = hx.h_ptr[(w * nps + T.l) * 2 + 1];
+            int lo = INT32_MAX, hi = -1;
+            for (int jy = T.jy0; jy < T.jy0 + T.ny; jy++)
+                for (int a = hx.h_idxptr[ty + jy]; a < hx.h_idxptr[ty + jy + 1]; a++) {
+                    lo = std::min(lo, hx.h_ent[a].i);
+                    hi = std::max(hi, hx.h_ent[a].i);
+                }
+            rr[(size_t)t * nwfs + w] = hi < 0 ? make_int2(1, 0) : make_int2(lo, hi);
+            if (hi >= 0) maxrows = std::max(maxrows, hi - lo + 1);
+        }
+    }
+    tiles.upload(tl);
+    rowrange.upload(rr);
+    hxt_smem = (size_t)maxrows * maxnx * 4 + (size_t)((maxnx + 2) & ~1) * 4 + (size_t)maxent * sizeof(GatherW);
+    MB_REQUIRE(hxt_smem <= 200 * 1024, "Hx^T tile needs %zu bytes of shared memory", hxt_smem);
+    MB_CUDA_TRY(cudaFuncSetAttribute(k_hxt_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hxt_smem));
+}
+
+void Recon::build_wfs_tables(const mb_recon_desc *d) {
     const mb_grid &pm = d->pmap;
     wfs_h.resize(nwfs);
     for (int w = 0; w < nwfs; w++) {
@@ -368,7 +481,7 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
     }
 }
 
-void Recon::build(const mb_tomo_desc *d) {
+void Recon::build(const mb_recon_desc *d) {
     MB_REQUIRE(d, "null descriptor");
     MB_REQUIRE(d->nps > 0 && d->nwfs > 0 && d->xmap && d->wfs && d->l2c, "empty descriptor");
     MB_REQUIRE(d->nbatch >= 1, "nbatch must be >= 1");
@@ -397,6 +510,7 @@ void Recon::build(const mb_tomo_desc *d) {
         xoff[l + 1] = xoff[l] + (long)g.nx * g.ny;
     }
     nxtot = xoff[nps];
+    xgrid.assign(d->xmap, d->xmap + nps);
     goff.assign(nwfs + 1, 0);
     nsa.resize(nwfs);
     int nsamax = 0;
@@ -408,6 +522,7 @@ void Recon::build(const mb_tomo_desc *d) {
     ngrad = goff[nwfs];
     set_l2c(d->l2c);
     build_hx_tables(d);
+    build_tiles();
     build_wfs_tables(d);
     nblk_x = (int)nblocks(nxtot);
     nblk_tt = (int)nblocks(nsamax);
@@ -419,13 +534,14 @@ void Recon::build(const mb_tomo_desc *d) {
     grad.alloc((size_t)nb * ngrad);
     gin.alloc((size_t)nb * ngrad);
     tt_part.alloc((size_t)nb * nwfs * nblk_tt * 2);
-    pap_part.alloc((size_t)nb * nblk_x);
+    pap_part.alloc((size_t)nb * std::max(nblk_x, ntiles));
     rr_part.alloc((size_t)nb * nblk_x);
     rz_part.alloc((size_t)nb * nblk_x);
     bb_part.alloc((size_t)nb * nblk_x);
     sc.alloc((size_t)nb * nsc);
     res.alloc(nb);
     if (precond) build_fdpcg(d->fdpcg);
+    if (d->fit) build_fit(d->fit);
     x.zero_async(stream);
     gin.zero_async(stream);
     sc.zero_async(stream);
@@ -438,8 +554,8 @@ void Recon::build(const mb_tomo_desc *d) {
 // operators
 // ---------------------------------------------------------------------------
 void Recon::op_hx(const float *xin, cudaStream_t s) {
-    k_hx<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(xin, opd.p, hx_tab.p, lay.p, nps, nwfs,
-                                                         nxp, nyp, nxtot);
+    k_hx<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(xin, opd.p, hx.fwd.p, lay.p, nps, nwfs,
+                                                         nxp, nyp, nxtot, nullptr, nullptr);
     MB_CHECK_LAUNCH();
 }
 
@@ -451,9 +567,9 @@ void Recon::op_rhs(const float *g, float *out, cudaStream_t s) {
     k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt_part.p, opd2.p, wfs.p, nwfs,
                                                           nxp, nyp, ngrad, nblk_tt, 1, 1.f);
     MB_CHECK_LAUNCH();
-    GatherIndex gi{gi_ptr.p, gi_idxptr.p, gi_ent.p};
-    k_hxt<<<dim3(nblk_x, nb), kThreads, 0, s>>>(opd2.p, nullptr, out, nullptr, gi, lay.p, nps, nwfs,
-                                               nxp, nyp, nxtot, 0, 1.f);
+    k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, s>>>(opd2.p, nullptr, out, nullptr, hx.gi(), lay.p,
+                                                            tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
+                                                            nxtot, 0, 1.f, maxrows, maxnx, maxent);
     MB_CHECK_LAUNCH();
 }
 
@@ -467,9 +583,9 @@ void Recon::op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t 
     k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt_part.p, opd2.p, wfs.p, nwfs,
                                                           nxp, nyp, ngrad, nblk_tt, do_tt, 1.f);
     MB_CHECK_LAUNCH();
-    GatherIndex gi{gi_ptr.p, gi_idxptr.p, gi_ent.p};
-    k_hxt<<<dim3(nblk_x, nb), kThreads, 0, s>>>(opd2.p, xin, out, dot_part, gi, lay.p, nps, nwfs,
-                                               nxp, nyp, nxtot, 1, 1.f);
+    k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, s>>>(opd2.p, xin, out, dot_part, hx.gi(), lay.p,
+                                                            tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
+                                                            nxtot, 1, 1.f, maxrows, maxnx, maxent);
     MB_CHECK_LAUNCH();
 }
 
@@ -494,45 +610,185 @@ void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s)
     MB_CHECK_LAUNCH();
 }
 
-// The whole per-step tomography: RHS, then (FD)PCG from the warm start in x
-// (lib/pcg.c:28 / cuda/pcg.cu:87 schedule; restart every 100 iterations is
-// never reached for maxit <= 100).
+// (Preconditioned) CG with FP64 scalars, the schedule of lib/pcg.c:28 and
+// cuda/pcg.cu:87 (the restart every 100/500 iterations is never reached for
+// the iteration counts used per step).  x holds the warm start.
+void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters,
+                       const std::function<void(const float *, float *, double *)> &Amul,
+                       const std::function<void(const float *, float *, double *)> &Mmul,
+                       cudaStream_t s) {
+    // r = b - A x ; b.b
+    Amul(B.x, B.Ap, nullptr);
+    k_cg_init_r<<<dim3(nblk, nb), kThreads, 0, s>>>(B.rhs, B.Ap, B.r, B.bb, n);
+    MB_CHECK_LAUNCH();
+    float *zp = B.r;
+    if (Mmul) {
+        Mmul(B.r, B.z, B.rz);
+        zp = B.z;
+    } else {
+        k_dot_self<<<dim3(nblk, nb), kThreads, 0, s>>>(B.r, B.rz, n);  // z aliases r
+        MB_CHECK_LAUNCH();
+    }
+    k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, B.rz, B.sc, B.nsc, 0, n, nblk, 1);
+    MB_CHECK_LAUNCH();
+    for (int k = 0; k < iters; k++) {
+        Amul(B.p, B.Ap, B.pap);
+        k_cg_update_xr<<<dim3(nblk, nb), kThreads, 0, s>>>(B.x, B.r, B.p, B.Ap, B.pap, B.rr, B.sc,
+                                                          B.nsc, k, n, B.nblk_pap);
+        MB_CHECK_LAUNCH();
+        if (k + 1 == iters) break;
+        const double *rzp_k = B.rr;
+        if (Mmul) {
+            Mmul(B.r, B.z, B.rz);
+            rzp_k = B.rz;
+        }
+        k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, rzp_k, B.sc, B.nsc, k, n, nblk, 0);
+        MB_CHECK_LAUNCH();
+    }
+    k_cg_residual<<<dim3(1, nb), 32, 0, s>>>(B.rr, B.bb, B.sc, B.res, B.nsc, iters + 2, nblk);
+    MB_CHECK_LAUNCH();
+}
+
+// The whole per-step tomography: RHS, then (FD)PCG from the warm start in x.
 void Recon::enqueue_solve(cudaStream_t s) {
     op_rhs(gin.p, rhs.p, s);
-    // r = b - A x ; bb
-    op_lhs(x.p, Ap.p, nullptr, s);
-    k_cg_init_r<<<dim3(nblk_x, nb), kThreads, 0, s>>>(rhs.p, Ap.p, r.p, bb_part.p, nxtot);
+    CgBufs B{x.p, r.p, p.p, z.p, Ap.p, rhs.p, pap_part.p, rr_part.p, rz_part.p, bb_part.p, sc.p, res.p, nsc,
+             ntiles};
+    auto A = [&](const float *in, float *out, double *dot) { op_lhs(in, out, dot, s); };
+    std::function<void(const float *, float *, double *)> M;
+    if (precond) M = [&](const float *in, float *out, double *dot) { op_fdpcg(in, out, dot, s); };
+    enqueue_cg(B, nxtot, nblk_x, maxit, A, M, s);
+}
+
+// FitR: sum_f wt_f HA_f^T (W0 - W1 W1^T) Hxp_f x   (recon_utils.c:483, fit.cu:190)
+void Recon::op_fitR(const float *xin, float *out, cudaStream_t s) {
+    k_hx<<<dim3(nblk_f, nfit, nb), kThreads, 0, s>>>(xin, opdf.p, hxp.fwd.p, lay.p, nps, nfit, nfx, nfy,
+                                                    nxtot, w1v.p, w1_part.p);
     MB_CHECK_LAUNCH();
-    float *zp = r.p;
-    if (precond) {
-        op_fdpcg(r.p, z.p, rz_part.p, s);
-        zp = z.p;
-    } else {
-        // no preconditioner: z aliases r, so r.z = r.r
-        k_dot_self<<<dim3(nblk_x, nb), kThreads, 0, s>>>(r.p, rz_part.p, nxtot);
+    k_fit_w<<<dim3(nblk_f, nfit, nb), kThreads, 0, s>>>(opdf.p, opdw.p, w0_rp.p, w0_ci.p, w0_v.p, w1v.p,
+                                                       fwt.p, w1_part.p, nblk_f, nf, nfit);
+    MB_CHECK_LAUNCH();
+    k_hxt<<<dim3(nblk_a, nb), kThreads, 0, s>>>(opdw.p, nullptr, out, nullptr, ha.gi(), dmlay.p, ndm,
+                                               nfit, nfx, nfy, nact, 0, 1.f, LowRank{});
+    MB_CHECK_LAUNCH();
+}
+
+// FitL: sum_f wt_f HA_f^T (W0 - W1 W1^T) HA_f a + NW NW^T a   (recon_utils.c:536, fit.cu:213)
+void Recon::op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t s) {
+    LowRank lr{};
+    if (nnw) {
+        k_lowrank_dot<<<dim3(nblk_a, nb), kThreads, 0, s>>>(ain, nwv.p, nw_part.p, nnw, nact);
         MB_CHECK_LAUNCH();
+        lr = LowRank{nwv.p, nw_part.p, nnw, nblk_a};
     }
-    k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, s>>>(p.p, zp, rz_part.p, sc.p, nsc, 0, nxtot,
-                                                       nblk_x, 1);
+    k_hx<<<dim3(nblk_f, nfit, nb), kThreads, 0, s>>>(ain, opdf.p, ha.fwd.p, dmlay.p, ndm, nfit, nfx, nfy,
+                                                    nact, w1v.p, w1_part.p);
     MB_CHECK_LAUNCH();
-    for (int k = 0; k < maxit; k++) {
-        op_lhs(p.p, Ap.p, pap_part.p, s);
-        k_cg_update_xr<<<dim3(nblk_x, nb), kThreads, 0, s>>>(x.p, r.p, p.p, Ap.p, pap_part.p,
-                                                            rr_part.p, sc.p, nsc, k, nxtot, nblk_x);
-        MB_CHECK_LAUNCH();
-        if (k + 1 == maxit) break;
-        const double *rzp_k = rr_part.p;
-        if (precond) {
-            op_fdpcg(r.p, z.p, rz_part.p, s);
-            rzp_k = rz_part.p;
+    k_fit_w<<<dim3(nblk_f, nfit, nb), kThreads, 0, s>>>(opdf.p, opdw.p, w0_rp.p, w0_ci.p, w0_v.p, w1v.p,
+                                                       fwt.p, w1_part.p, nblk_f, nf, nfit);
+    MB_CHECK_LAUNCH();
+    k_hxt<<<dim3(nblk_a, nb), kThreads, 0, s>>>(opdw.p, ain, out, dot_part, ha.gi(), dmlay.p, ndm, nfit,
+                                               nfx, nfy, nact, 0, 1.f, lr);
+    MB_CHECK_LAUNCH();
+}
+
+// The DM fit of one step: RHS from the tomography solution, then CG warm-
+// started from the previous commands (curecon_t::fit, cuda/recon.cu:277).
+void Recon::enqueue_fit(cudaStream_t s) {
+    op_fitR(x.p, frhs.p, s);
+    CgBufs B{fa.p, fr.p, fp.p, fr.p, fAp.p, frhs.p, f_pap.p, f_rr.p, f_rz.p, f_bb.p, fsc.p, fres.p, fnsc,
+             nblk_a};
+    auto A = [&](const float *in, float *out, double *dot) { op_fitL(in, out, dot, s); };
+    enqueue_cg(B, nact, nblk_a, fit_maxit, A, nullptr, s);
+}
+
+void Recon::build_fit(const mb_fit_desc *f) {
+    MB_REQUIRE(f->nfit >= 1 && f->ndm >= 1 && f->thetax && f->thetay && f->wt && f->hs && f->amap,
+               "fit: missing arrays");
+    MB_REQUIRE(f->w0_p && f->w0_i && f->w0_x && f->w1, "fit: W0/W1 missing");
+    MB_REQUIRE(f->nnw >= 0 && f->nnw <= 8 && (f->nnw == 0 || f->nw), "fit: 0..8 low-rank columns");
+    MB_REQUIRE(f->maxit >= 1, "fit: maxit must be >= 1");
+    has_fit = 1;
+    nfit = f->nfit;
+    ndm = f->ndm;
+    nfx = f->floc.nx;
+    nfy = f->floc.ny;
+    nf = nfx * nfy;
+    nnw = f->nnw;
+    fit_maxit = f->maxit;
+    dmlay_h.resize(ndm);
+    long off = 0;
+    for (int d = 0; d < ndm; d++) {
+        MB_REQUIRE(f->amap[d].nx >= 2 && f->amap[d].ny >= 2 && f->amap[d].dx > 0, "fit: DM %d grid", d);
+        dmlay_h[d].nx = f->amap[d].nx;
+        dmlay_h[d].ny = f->amap[d].ny;
+        dmlay_h[d].off = off;
+        dmlay_h[d].l2c = 0.f;
+        off += (long)f->amap[d].nx * f->amap[d].ny;
+    }
+    nact = off;
+    dmlay.upload(dmlay_h);
+    // the layer grids are needed for Hxp: keep a host copy of the layer grids
+    build_ray_tables(f->floc, nfit, nps, xgrid.data(),
+                     [&](int d, int t, double &scale, double &dx, double &dy) {
+                         const double ht = xgrid[t].ht - f->floc.ht;
+                         scale = std::isinf(f->hs[d]) ? 1.0 : 1.0 - ht / f->hs[d];
+                         dx = f->thetax[d] * ht;
+                         dy = f->thetay[d] * ht;
+                     },
+                     true, hxp);
+    build_ray_tables(f->floc, nfit, ndm, f->amap,
+                     [&](int d, int t, double &scale, double &dx, double &dy) {
+                         const double ht = f->amap[t].ht - f->floc.ht;
+                         scale = std::isinf(f->hs[d]) ? 1.0 : 1.0 - ht / f->hs[d];
+                         dx = f->thetax[d] * ht;
+                         dy = f->thetay[d] * ht;
+                     },
+                     true, ha);
+    // W0: CSC -> CSR
+    std::vector<int> rp(nf + 1, 0), ci;
+    std::vector<float> cv;
+    const long nnz = f->w0_p[nf];
+    for (long k = 0; k < nnz; k++) {
+        MB_REQUIRE(f->w0_i[k] >= 0 && f->w0_i[k] < nf, "fit: W0 row out of range");
+        rp[f->w0_i[k] + 1]++;
+    }
+    for (int i = 0; i < nf; i++) rp[i + 1] += rp[i];
+    ci.resize(nnz);
+    cv.resize(nnz);
+    std::vector<int> fill(rp.begin(), rp.end() - 1);
+    for (int c = 0; c < nf; c++)
+        for (int k = f->w0_p[c]; k < f->w0_p[c + 1]; k++) {
+            const int r = f->w0_i[k];
+            ci[fill[r]] = c;
+            cv[fill[r]++] = (float)f->w0_x[k];
         }
-        k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, s>>>(p.p, zp, rzp_k, sc.p, nsc, k, nxtot,
-                                                           nblk_x, 0);
-        MB_CHECK_LAUNCH();
-    }
-    k_cg_residual<<<dim3(1, nb), 32, 0, s>>>(rr_part.p, bb_part.p, sc.p, res.p, nsc, maxit + 2,
-                                            nblk_x);
-    MB_CHECK_LAUNCH();
+    w0_rp.upload(rp);
+    w0_ci.upload(ci);
+    w0_v.upload(cv);
+    std::vector<float> h1(nf), hw(nfit), hn((size_t)nact * nnw);
+    for (int i = 0; i < nf; i++) h1[i] = (float)f->w1[i];
+    for (int i = 0; i < nfit; i++) hw[i] = (float)f->wt[i];
+    for (size_t i = 0; i < hn.size(); i++) hn[i] = (float)f->nw[i];
+    w1v.upload(h1);
+    fwt.upload(hw);
+    if (nnw) nwv.upload(hn);
+    nblk_a = (int)nblocks(nact);
+    nblk_f = (int)nblocks(nf);
+    fnsc = fit_maxit + 3;
+    const size_t NA = (size_t)nb * nact;
+    fa.alloc(NA); fr.alloc(NA); fp.alloc(NA); fAp.alloc(NA); frhs.alloc(NA);
+    opdf.alloc((size_t)nb * nfit * nf);
+    opdw.alloc((size_t)nb * nfit * nf);
+    w1_part.alloc((size_t)nb * nfit * nblk_f);
+    nw_part.alloc((size_t)nb * std::max(nnw, 1) * nblk_a);
+    f_pap.alloc((size_t)nb * nblk_a); f_rr.alloc((size_t)nb * nblk_a);
+    f_rz.alloc((size_t)nb * nblk_a); f_bb.alloc((size_t)nb * nblk_a);
+    fsc.alloc((size_t)nb * fnsc);
+    fres.alloc(nb);
+    fa.zero_async(stream);
+    fsc.zero_async(stream);
+    fres.zero_async(stream);
 }
 
 // Time each iteration stage alone and report its algorithmic traffic.
@@ -553,11 +809,11 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     const double nxw = (double)nwfs * np;
     const double ngr = (double)ngrad;
     const double nx = (double)nxtot;
-    const double gather = (double)gi_ent.n * 8.0 + (double)gi_idxptr.n * 4.0;
+    const double gather = (double)hx.ent.n * 8.0 + (double)hx.idxptr.n * 4.0;
     const double nbk = (double)fd_nb * fd_bs;
     // bytes per launch: operands read + written once
     double by[11] = {
-        B * (F * nx + F * nxw) + (double)hx_tab.n * 12.0,             // hx: x -> opd
+        B * (F * nx + F * nxw) + (double)hx.fwd.n * 12.0,             // hx: x -> opd
         B * (F * nxw + F * ngr + D * 2 * nwfs * nblk_tt) + tab_gp,     // gp: opd -> grad
         B * (F * ngr + F * nxw) + tab_gpt,                             // gpt: grad -> opd2
         B * (F * nxw + 2 * F * nx) + gather,                           // hxt: opd2, p -> Ap
@@ -571,7 +827,7 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     const int lps[11] = {maxit + 1, maxit + 2, maxit + 2, maxit + 2, maxit, maxit - 1 + 1,
                          precond ? maxit : 0, precond ? maxit : 0, precond ? maxit : 0,
                          precond ? maxit : 0, precond ? maxit : 0};
-    GatherIndex gi{gi_ptr.p, gi_idxptr.p, gi_ent.p};
+    GatherIndex gi = hx.gi();
     for (int st = 0; st < ns; st++) {
         bytes[st] = by[st];
         launches[st] = lps[st];
@@ -592,15 +848,16 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                     MB_CHECK_LAUNCH();
                     break;
                 case 3:
-                    k_hxt<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(opd2.p, p.p, Ap.p, pap_part.p, gi, lay.p,
-                                                                    nps, nwfs, nxp, nyp, nxtot, 1, 1.f);
+                    k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, stream>>>(
+                        opd2.p, p.p, Ap.p, pap_part.p, gi, lay.p, tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
+                        nxtot, 1, 1.f, maxrows, maxnx, maxent);
                     MB_CHECK_LAUNCH();
                     break;
                 case 4:
                     // alpha reads the current scalars; the vectors are scratch here
                     k_cg_update_xr<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(z.p, rhs.p, p.p, Ap.p, pap_part.p,
                                                                              rr_part.p, sc.p, nsc, 0, nxtot,
-                                                                             nblk_x);
+                                                                             ntiles);
                     MB_CHECK_LAUNCH();
                     break;
                 case 5:
@@ -646,26 +903,46 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     cudaEventDestroy(e1);
 }
 
-void Recon::capture_graph() {
-    if (graph) {
-        cudaGraphExecDestroy(graph);
-        graph = nullptr;
-    }
-    cudaGraph_t g;
+cudaGraphExec_t Recon::capture(const std::function<void(cudaStream_t)> &body, long &nkernels) {
+    cudaGraph_t g = nullptr;
     const long before = g_launches.load();
     MB_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     try {
-        enqueue_solve(stream);
+        body(stream);
     } catch (...) {
         cudaStreamEndCapture(stream, &g);
         if (g) cudaGraphDestroy(g);
         throw;
     }
     MB_CUDA_TRY(cudaStreamEndCapture(stream, &g));
-    graph_kernels = g_launches.load() - before;
-    g_launches -= graph_kernels;  // captured, not launched
-    MB_CUDA_TRY(cudaGraphInstantiate(&graph, g, 0));
+    nkernels = g_launches.load() - before;
+    g_launches -= nkernels;  // captured, not launched
+    cudaGraphExec_t ge = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        set_error("cudaGraphInstantiate: %s", cudaGetErrorString(e));
+        throw CudaError{MB_ECUDA};
+    }
+    return ge;
+}
+
+void Recon::capture_graph() {
+    for (cudaGraphExec_t *gp : {&graph, &graph_fit, &graph_step})
+        if (*gp) {
+            cudaGraphExecDestroy(*gp);
+            *gp = nullptr;
+        }
+    graph = capture([&](cudaStream_t s) { enqueue_solve(s); }, graph_kernels);
+    if (has_fit) {
+        graph_fit = capture([&](cudaStream_t s) { enqueue_fit(s); }, graph_fit_kernels);
+        graph_step = capture(
+            [&](cudaStream_t s) {
+                enqueue_solve(s);
+                enqueue_fit(s);
+            },
+            graph_step_kernels);
+    }
 }
 
 void Recon::run_graph(cudaStream_t s) {
@@ -735,7 +1012,7 @@ int mb_init(int device) {
 
 void mb_cleanup(void) {}
 
-int mb_setup_recon(const mb_tomo_desc *desc, mb_recon **out) {
+int mb_setup_recon(const mb_recon_desc *desc, mb_recon **out) {
     if (!out) {
         mb::set_error("out is NULL");
         return MB_EINVAL;
@@ -770,6 +1047,7 @@ int mb_recon_reset(mb_recon *h) {
     MB_API_BEGIN
     MB_REQUIRE(h, "null handle");
     h->R.x.zero_async(h->R.stream);
+    if (h->R.has_fit) h->R.fa.zero_async(h->R.stream);
     MB_CUDA_TRY(cudaStreamSynchronize(h->R.stream));
     MB_API_END
 }
@@ -837,6 +1115,60 @@ int mb_tomo_device(mb_recon *h, const float *d_grad, void *stream) {
 }
 
 const float *mb_tomo_solution(mb_recon *h) { return h ? h->R.x.p : nullptr; }
+const float *mb_fit_solution(mb_recon *h) { return h && h->R.has_fit ? h->R.fa.p : nullptr; }
+long mb_nact(const mb_recon *h) { return h && h->R.has_fit ? h->R.nact : 0; }
+
+int mb_fit(mb_recon *h, double *dmout, float *cgres) {
+    MB_API_BEGIN
+    MB_REQUIRE(h, "null handle");
+    mb::Recon &R = h->R;
+    if (!R.has_fit) {
+        mb::set_error("reconstructor was set up without a DM fit");
+        return MB_ESTATE;
+    }
+    MB_CUDA_TRY(cudaGraphLaunch(R.graph_fit, R.stream));
+    mb::count_launches(R.graph_fit_kernels);
+    if (dmout) from_float_dev(dmout, R.fa.p, (size_t)R.nb * R.nact, R.stream);
+    if (cgres) MB_CUDA_TRY(cudaMemcpyAsync(cgres, R.fres.p, R.nb * sizeof(float), cudaMemcpyDeviceToHost, R.stream));
+    MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
+    MB_API_END
+}
+
+int mb_recon_step_device(mb_recon *h, const float *d_grad, void *stream) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && d_grad, "invalid arguments");
+    mb::Recon &R = h->R;
+    if (!R.has_fit) {
+        mb::set_error("reconstructor was set up without a DM fit");
+        return MB_ESTATE;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    MB_CUDA_TRY(cudaMemcpyAsync(R.gin.p, d_grad, (size_t)R.nb * R.ngrad * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s));
+    MB_CUDA_TRY(cudaGraphLaunch(R.graph_step, s));
+    mb::count_launches(R.graph_step_kernels);
+    MB_API_END
+}
+
+int mb_apply_fit_R(mb_recon *h, const double *xin, double *aout) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && xin && aout && h->R.has_fit, "invalid arguments or no fit");
+    mb::Recon &R = h->R;
+    to_float_dev(R.z.p, xin, (size_t)R.nb * R.nxtot, R.stream);
+    R.op_fitR(R.z.p, R.frhs.p, R.stream);
+    from_float_dev(aout, R.frhs.p, (size_t)R.nb * R.nact, R.stream);
+    MB_API_END
+}
+
+int mb_apply_fit_L(mb_recon *h, const double *ain, double *aout) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && ain && aout && h->R.has_fit, "invalid arguments or no fit");
+    mb::Recon &R = h->R;
+    to_float_dev(R.fp.p, ain, (size_t)R.nb * R.nact, R.stream);
+    R.op_fitL(R.fp.p, R.fAp.p, nullptr, R.stream);
+    from_float_dev(aout, R.fAp.p, (size_t)R.nb * R.nact, R.stream);
+    MB_API_END
+}
 
 void *mb_recon_stream(mb_recon *h) { return h ? (void *)h->R.stream : nullptr; }
 

@@ -85,25 +85,33 @@ __device__ __forceinline__ double warp_sum_partials(const double *part, int n) {
 // ---------------------------------------------------------------------------
 __global__ void k_hx(const float *__restrict__ x, float *__restrict__ opd,
                      const AxisW *__restrict__ tab, const LayerDev *__restrict__ lay, int nps,
-                     int nwfs, int nxp, int nyp, long nxtot) {
+                     int nwfs, int nxp, int nyp, long nxtot, const float *__restrict__ w1,
+                     double *__restrict__ w1_part) {
+    __shared__ double sh[32];
     const int np = nxp * nyp;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int w = blockIdx.y, b = blockIdx.z;
-    if (p >= np) return;
-    const int ix = p % nxp, iy = p / nxp;
-    const float *xb = x + (size_t)b * nxtot;
     float acc = 0.f;
-    for (int l = 0; l < nps; l++) {
-        const AxisW *t = tab + (size_t)(w * nps + l) * (nxp + nyp);
-        const AxisW tx = t[ix], ty = t[nxp + iy];
-        if (tx.k < 0 || ty.k < 0) continue;
-        const int nx = lay[l].nx;
-        const float *X = xb + lay[l].off + (size_t)ty.k * nx + tx.k;
-        const float a = tx.w0 * X[0] + tx.w1 * X[1];
-        const float c = tx.w0 * X[nx] + tx.w1 * X[nx + 1];
-        acc += ty.w0 * a + ty.w1 * c;
+    if (p < np) {
+        const int ix = p % nxp, iy = p / nxp;
+        const float *xb = x + (size_t)b * nxtot;
+        for (int l = 0; l < nps; l++) {
+            const AxisW *t = tab + (size_t)(w * nps + l) * (nxp + nyp);
+            const AxisW tx = t[ix], ty = t[nxp + iy];
+            if (tx.k < 0 || ty.k < 0) continue;
+            const int nx = lay[l].nx;
+            const float *X = xb + lay[l].off + (size_t)ty.k * nx + tx.k;
+            const float a = tx.w0 * X[0] + tx.w1 * X[1];
+            const float c = tx.w0 * X[nx] + tx.w1 * X[nx + 1];
+            acc += ty.w0 * a + ty.w1 * c;
+        }
+        opd[((size_t)b * nwfs + w) * np + p] = acc;
     }
-    opd[((size_t)b * nwfs + w) * np + p] = acc;
+    if (w1_part) {  // W1' opd partials for the piston-removed fit weighting
+        double v = (p < np) ? (double)w1[p] * acc : 0.0;
+        v = block_sum(v, sh);
+        if (threadIdx.x == 0) w1_part[((size_t)b * nwfs + w) * gridDim.x + blockIdx.x] = v;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -227,12 +235,27 @@ struct GatherIndex {
     const GatherW *ent;    // concatenated entries
 };
 
+struct LowRank {
+    const float *nw;        // [n][nnw] column-major (nw[k*n + j]); null: no term
+    const double *part;     // NW' x partials [b][k][nblk]
+    int nnw, nblk;
+};
+
 __global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ xin,
                       float *__restrict__ out, double *__restrict__ dot_part, GatherIndex gi,
                       const LayerDev *__restrict__ lay, int nps, int nwfs, int nxp, int nyp,
-                      long nxtot, int do_l2, float alpha) {
+                      long nxtot, int do_l2, float alpha, LowRank lr) {
     __shared__ double sh[32];
+    __shared__ float s_t[8];
     const int b = blockIdx.y;
+    if (lr.nw) {  // t_k = NW_k' x, summed from partials in fixed order
+        const int wid = threadIdx.x >> 5;
+        if (wid < lr.nnw) {
+            const double t = warp_sum_partials(lr.part + ((size_t)b * lr.nnw + wid) * lr.nblk, lr.nblk);
+            if ((threadIdx.x & 31) == 0) s_t[wid] = (float)t;
+        }
+        __syncthreads();
+    }
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double dotv = 0;
     if (j < nxtot) {
@@ -279,12 +302,164 @@ __global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ 
         } else {
             acc = alpha * acc;
         }
+        if (lr.nw) {
+            float lt = 0.f;
+            for (int k = 0; k < lr.nnw; k++) lt += lr.nw[(size_t)k * nxtot + j] * s_t[k];
+            acc += alpha * lt;
+        }
         out[(size_t)b * nxtot + j] = acc;
         if (dot_part && X) dotv = (double)acc * (double)X[jj];
     }
     if (dot_part) {
         dotv = block_sum(dotv, sh);
         if (threadIdx.x == 0) dot_part[(size_t)b * gridDim.x + blockIdx.x] = dotv;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tiled Hx^T (+ L2^T L2 and p.Ap partials) for the tomography.
+// One CTA = one instance x one tile of `ny` consecutive rows of one layer.
+// The bilinear transpose is separable, so per WFS the CTA
+//   1. stages that WFS's x-gather lists for the layer in shared memory,
+//   2. x pass: t[iy][jx] = sum_x w * opd2[iy][ix] for the pupil rows that
+//      reach the tile (coalesced reads along each pupil row),
+//   3. y pass: acc[jy][jx] += sum_y w * t[iy][jx] into registers.
+// grid: (ntiles, nb); dynamic smem: maxrows*maxnx floats + lists.
+// ---------------------------------------------------------------------------
+struct TileDesc {
+    int l;     // layer
+    int jy0;   // first layer row
+    int ny;    // rows in this tile
+};
+constexpr int kMaxOwn = 8;  // layer points per thread (tile rows * nx <= 256 * kMaxOwn)
+
+__global__ void __launch_bounds__(kThreads)
+k_hxt_tiled(const float *__restrict__ opd2, const float *__restrict__ xin, float *__restrict__ out,
+            double *__restrict__ dot_part, GatherIndex gi, const LayerDev *__restrict__ lay,
+            const TileDesc *__restrict__ tiles, const int2 *__restrict__ rowrange, int nps, int nwfs,
+            int nxp, int nyp, long nxtot, int do_l2, float alpha, int maxrows, int maxnx,
+            int maxent) {
+    extern __shared__ float smem[];
+    __shared__ double sh[32];
+    const int tid = blockIdx.x, b = blockIdx.y;
+    const TileDesc T = tiles[tid];
+    const LayerDev L = lay[T.l];
+    const int nx = L.nx;
+    const int nown = T.ny * nx;
+    float *t = smem;
+    int *xptr = reinterpret_cast<int *>(t + (size_t)maxrows * maxnx);
+    GatherW *xent = reinterpret_cast<GatherW *>(xptr + ((maxnx + 2) & ~1));
+    const int np = nxp * nyp;
+    float acc[kMaxOwn];
+#pragma unroll
+    for (int k = 0; k < kMaxOwn; k++) acc[k] = 0.f;
+    for (int w = 0; w < nwfs; w++) {
+        const int2 rr = rowrange[(size_t)tid * nwfs + w];
+        if (rr.y < rr.x) continue;  // uniform over the CTA
+        const int tx = gi.ptr[(w * nps + T.l) * 2 + 0];
+        const int ty = gi.ptr[(w * nps + T.l) * 2 + 1];
+        const int e0 = gi.idx_ptr[tx];
+        const int ne = gi.idx_ptr[tx + nx] - e0;
+        for (int i = threadIdx.x; i <= nx; i += blockDim.x) xptr[i] = gi.idx_ptr[tx + i] - e0;
+        for (int i = threadIdx.x; i < ne && i < maxent; i += blockDim.x) xent[i] = gi.ent[e0 + i];
+        __syncthreads();
+        const int nr = rr.y - rr.x + 1;
+        const float *o = opd2 + ((size_t)b * nwfs + w) * np + (size_t)rr.x * nxp;
+        for (int idx = threadIdx.x; idx < nr * nx; idx += blockDim.x) {
+            const int r = idx / nx, jx = idx - r * nx;
+            float sx = 0.f;
+            for (int e = xptr[jx]; e < xptr[jx + 1]; e++) {
+                const GatherW ge = xent[e];
+                sx += ge.w * o[(size_t)r * nxp + ge.i];
+            }
+            t[r * maxnx + jx] = sx;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kMaxOwn; k++) {
+            const int oi = threadIdx.x + k * kThreads;
+            if (oi < nown) {
+                const int jy = T.jy0 + oi / nx, jx = oi % nx;
+                const int a0 = gi.idx_ptr[ty + jy], a1 = gi.idx_ptr[ty + jy + 1];
+                float sy = 0.f;
+                for (int a = a0; a < a1; a++) {
+                    const GatherW ge = gi.ent[a];
+                    sy += ge.w * t[(ge.i - rr.x) * maxnx + jx];
+                }
+                acc[k] += sy;
+            }
+        }
+        __syncthreads();
+    }
+    const float *X = xin ? xin + (size_t)b * nxtot + L.off : nullptr;
+    double dotv = 0;
+#pragma unroll
+    for (int k = 0; k < kMaxOwn; k++) {
+        const int oi = threadIdx.x + k * kThreads;
+        if (oi < nown) {
+            const int jy = T.jy0 + oi / nx, jx = oi % nx;
+            float v = alpha * acc[k];
+            if (do_l2) {
+                const int ny_ = L.ny;
+                auto at = [&](int dx, int dy) {
+                    int xx = jx + dx, yy = jy + dy;
+                    xx += (xx < 0) ? nx : 0;
+                    xx -= (xx >= nx) ? nx : 0;
+                    yy += (yy < 0) ? ny_ : 0;
+                    yy -= (yy >= ny_) ? ny_ : 0;
+                    return X[yy * nx + xx];
+                };
+                const float st = 20.f * at(0, 0) - 8.f * (at(-1, 0) + at(1, 0) + at(0, -1) + at(0, 1)) +
+                                 2.f * (at(-1, -1) + at(1, -1) + at(-1, 1) + at(1, 1)) +
+                                 (at(0, -2) + at(-2, 0) + at(2, 0) + at(0, 2));
+                v += alpha * L.l2c * st;
+            }
+            const long j = L.off + (long)jy * nx + jx;
+            out[(size_t)b * nxtot + j] = v;
+            if (dot_part && X) dotv += (double)v * (double)X[jy * nx + jx];
+        }
+    }
+    if (dot_part) {
+        dotv = block_sum(dotv, sh);
+        if (threadIdx.x == 0) dot_part[(size_t)b * gridDim.x + blockIdx.x] = dotv;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fit weighting: y = wt_f (W0 v - W1 (W1' v)) on the fit grid, W0 in CSR.
+// grid: (ceil(nf/256), nfit, nb); W1' v from the partials written by k_hx.
+// ---------------------------------------------------------------------------
+__global__ void k_fit_w(const float *__restrict__ v, float *__restrict__ y,
+                        const int *__restrict__ rp, const int *__restrict__ ci,
+                        const float *__restrict__ cv, const float *__restrict__ w1,
+                        const float *__restrict__ wt, const double *__restrict__ w1_part,
+                        int nblk_w1, int nf, int nfit) {
+    __shared__ float s_dot;
+    const int f = blockIdx.y, b = blockIdx.z;
+    if (threadIdx.x < 32) {
+        const double d = warp_sum_partials(w1_part + ((size_t)b * nfit + f) * nblk_w1, nblk_w1);
+        if (threadIdx.x == 0) s_dot = (float)d;
+    }
+    __syncthreads();
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nf) return;
+    const float *vb = v + ((size_t)b * nfit + f) * nf;
+    float acc = 0.f;
+    for (int k = rp[p]; k < rp[p + 1]; k++) acc += cv[k] * vb[ci[k]];
+    y[((size_t)b * nfit + f) * nf + p] = wt[f] * (acc - w1[p] * s_dot);
+}
+
+// NW' x partials: part[(b*nnw + k)*nblk + blk].  grid: (nblk, nb)
+__global__ void k_lowrank_dot(const float *__restrict__ x, const float *__restrict__ nw,
+                              double *__restrict__ part, int nnw, long n) {
+    __shared__ double sh[32];
+    const int b = blockIdx.y;
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const float xv = (j < n) ? x[(size_t)b * n + j] : 0.f;
+    for (int k = 0; k < nnw; k++) {
+        double v = (j < n) ? (double)nw[(size_t)k * n + j] * xv : 0.0;
+        v = block_sum(v, sh);
+        if (threadIdx.x == 0) part[((size_t)b * nnw + k) * gridDim.x + blockIdx.x] = v;
     }
 }
 
@@ -315,12 +490,12 @@ __global__ void k_cg_init_r(const float *__restrict__ bvec, const float *__restr
 __global__ void k_cg_update_xr(float *__restrict__ x, float *__restrict__ r,
                                const float *__restrict__ p, const float *__restrict__ Ap,
                                const double *__restrict__ pap_part, double *__restrict__ rr_part,
-                               double *__restrict__ sc, int nsc, int k, long n, int nblk) {
+                               double *__restrict__ sc, int nsc, int k, long n, int nblk_pap) {
     __shared__ double sh[32];
     __shared__ float s_alpha;
     const int b = blockIdx.y;
     if (threadIdx.x < 32) {
-        const double pap = warp_sum_partials(pap_part + (size_t)b * nblk, nblk);
+        const double pap = warp_sum_partials(pap_part + (size_t)b * nblk_pap, nblk_pap);
         if (threadIdx.x == 0) {
             double a = sc[(size_t)b * nsc + k] / pap;
             if (!isfinite(a)) a = 0;  // pcg.c:80-83, pcg.cu:27-30

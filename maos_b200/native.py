@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmaosb200.so")
 
 MB_OK = 0
+MB_MVM_F32, MB_MVM_BF16, MB_MVM_FP8 = 0, 1, 2
 ERRORS = {-1: "MB_EINVAL", -2: "MB_ECUDA", -3: "MB_ENOMEM", -4: "MB_ESTATE", -5: "MB_EUNSUP",
           -6: "MB_ENUM"}
 
@@ -35,11 +36,21 @@ class MbFdpcgDesc(C.Structure):
                 ("perm", C.POINTER(C.c_long)), ("mbinv", C.POINTER(C.c_double))]
 
 
-class MbTomoDesc(C.Structure):
+class MbFitDesc(C.Structure):
+    _fields_ = [("floc", MbGrid), ("nfit", C.c_int), ("thetax", C.POINTER(C.c_double)),
+                ("thetay", C.POINTER(C.c_double)), ("wt", C.POINTER(C.c_double)),
+                ("hs", C.POINTER(C.c_double)), ("w0_p", C.POINTER(C.c_int)),
+                ("w0_i", C.POINTER(C.c_int)), ("w0_x", C.POINTER(C.c_double)),
+                ("w1", C.POINTER(C.c_double)), ("ndm", C.c_int), ("amap", C.POINTER(MbGrid)),
+                ("nnw", C.c_int), ("nw", C.POINTER(C.c_double)), ("maxit", C.c_int)]
+
+
+class MbReconDesc(C.Structure):
     _fields_ = [("pmap", MbGrid), ("nps", C.c_int), ("xmap", C.POINTER(MbGrid)),
                 ("l2c", C.POINTER(C.c_double)), ("nwfs", C.c_int),
                 ("wfs", C.POINTER(MbWfsDesc)), ("maxit", C.c_int), ("precond", C.c_int),
-                ("split", C.c_int), ("fdpcg", C.POINTER(MbFdpcgDesc)), ("nbatch", C.c_int)]
+                ("split", C.c_int), ("fdpcg", C.POINTER(MbFdpcgDesc)), ("nbatch", C.c_int),
+                ("fit", C.POINTER(MbFitDesc))]
 
 
 # every symbol the header declares, with (restype, argtypes)
@@ -48,13 +59,19 @@ _F = C.POINTER(C.c_float)
 SIGNATURES = {
     "mb_init": (C.c_int, [C.c_int]),
     "mb_cleanup": (None, []),
-    "mb_setup_recon": (C.c_int, [C.POINTER(MbTomoDesc), C.POINTER(C.c_void_p)]),
+    "mb_setup_recon": (C.c_int, [C.POINTER(MbReconDesc), C.POINTER(C.c_void_p)]),
     "mb_recon_free": (None, [C.c_void_p]),
     "mb_recon_reset": (C.c_int, [C.c_void_p]),
     "mb_update_recon_nea": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
     "mb_update_recon_cn2": (C.c_int, [C.c_void_p, _D, C.POINTER(MbFdpcgDesc)]),
     "mb_tomo": (C.c_int, [C.c_void_p, _D, _D, _F]),
     "mb_tomo_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mb_fit": (C.c_int, [C.c_void_p, _D, _F]),
+    "mb_recon_step_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mb_fit_solution": (C.c_void_p, [C.c_void_p]),
+    "mb_nact": (C.c_long, [C.c_void_p]),
+    "mb_apply_fit_R": (C.c_int, [C.c_void_p, _D, _D]),
+    "mb_apply_fit_L": (C.c_int, [C.c_void_p, _D, _D]),
     "mb_tomo_solution": (C.c_void_p, [C.c_void_p]),
     "mb_recon_stream": (C.c_void_p, [C.c_void_p]),
     "mb_num_stages": (C.c_int, []),
@@ -69,6 +86,11 @@ SIGNATURES = {
     "mb_apply_fdpcg": (C.c_int, [C.c_void_p, _D, _D]),
     "mb_apply_hx": (C.c_int, [C.c_void_p, _D, _D]),
     "mb_kernel_launches": (C.c_long, [C.c_int]),
+    "mb_mvm_create": (C.c_int, [_D, C.c_long, C.c_long, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "mb_mvm_free": (None, [C.c_void_p]),
+    "mb_mvm_bytes": (C.c_long, [C.c_void_p]),
+    "mb_recon_mvm": (C.c_int, [C.c_void_p, _D, _D]),
+    "mb_mvm_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mb_error_string": (C.c_char_p, [C.c_int]),
     "mb_last_error_message": (C.c_char_p, []),
     "mb_version": (C.c_int, []),

@@ -11,6 +11,7 @@ gpu_update_recon       ``update_nea(iwfs, neai, ptt)``
 gpu_update_recon_cn2   ``update_cn2(l2c, fdpcg)``
 gpu_recon_reset        ``reset()``
 gpu_tomo               ``tomo(grad)`` -> (opdr, cgres)
+gpu_fit                ``fit()`` -> (dmfit, cgres)
 gpu_recon_free         ``close()``
 =====================  ==========================================
 
@@ -25,7 +26,7 @@ from typing import Optional
 import numpy as np
 
 from . import native
-from .native import MbFdpcgDesc, MbGrid, MbTomoDesc, MbWfsDesc, check
+from .native import MbFdpcgDesc, MbFitDesc, MbGrid, MbReconDesc, MbWfsDesc, check
 
 
 def _dptr(a: np.ndarray):
@@ -49,8 +50,26 @@ def fdpcg_desc(fd, keep: list) -> MbFdpcgDesc:
                        perm.ctypes.data_as(C.POINTER(C.c_long)), _dptr(mbi))
 
 
-def tomo_desc(sysm, nbatch: int = 1, split: int = 1, maxit: Optional[int] = None):
-    """Flatten a :class:`maos_b200.geometry.TomoSystem` into an ``mb_tomo_desc``.
+def fit_desc(fs, keep: list) -> MbFitDesc:
+    """Flatten a :class:`maos_b200.fit_setup.FitSystem` into an ``mb_fit_desc``."""
+    W0 = fs.W0.tocsc()
+    W0.sort_indices()
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
+            (fs.thetax, fs.thetay, fs.wt, fs.hs, W0.data, fs.W1)]
+    w0p = np.ascontiguousarray(W0.indptr, dtype=np.int32)
+    w0i = np.ascontiguousarray(W0.indices, dtype=np.int32)
+    am = (MbGrid * len(fs.dms))(*[_grid(d.amap) for d in fs.dms])
+    nw = np.ascontiguousarray(fs.NW.ravel(order="F"), dtype=np.float64)
+    keep += arrs + [w0p, w0i, am, nw]
+    return MbFitDesc(_grid(fs.floc), len(fs.thetax), _dptr(arrs[0]), _dptr(arrs[1]), _dptr(arrs[2]),
+                     _dptr(arrs[3]), w0p.ctypes.data_as(C.POINTER(C.c_int)),
+                     w0i.ctypes.data_as(C.POINTER(C.c_int)), _dptr(arrs[4]), _dptr(arrs[5]),
+                     len(fs.dms), am, int(fs.NW.shape[1]), _dptr(nw), int(fs.maxit))
+
+
+def tomo_desc(sysm, nbatch: int = 1, split: int = 1, maxit: Optional[int] = None, fit=None):
+    """Flatten a :class:`maos_b200.geometry.TomoSystem` (and optionally a
+    :class:`maos_b200.fit_setup.FitSystem`) into an ``mb_recon_desc``.
 
     Returns (desc, keep) -- ``keep`` holds the numpy arrays the descriptor
     points into and must outlive the setup call."""
@@ -93,9 +112,14 @@ def tomo_desc(sysm, nbatch: int = 1, split: int = 1, maxit: Optional[int] = None
         fd = fdpcg_desc(sysm.fdpcg, keep)
         keep.append(fd)
         fdp = C.pointer(fd)
-    d = MbTomoDesc(_grid(sysm.pmap), len(sysm.xmaps), xm, _dptr(l2c), len(sysm.wfs), ws,
-                   int(cfg.tomo_maxit if maxit is None else maxit), int(cfg.tomo_precond),
-                   int(split), fdp, int(nbatch))
+    fitp = C.POINTER(MbFitDesc)()
+    if fit is not None:
+        fd = fit_desc(fit, keep)
+        keep.append(fd)
+        fitp = C.pointer(fd)
+    d = MbReconDesc(_grid(sysm.pmap), len(sysm.xmaps), xm, _dptr(l2c), len(sysm.wfs), ws,
+                    int(cfg.tomo_maxit if maxit is None else maxit), int(cfg.tomo_precond),
+                    int(split), fdp, int(nbatch), fitp)
     return d, keep
 
 
@@ -103,17 +127,19 @@ class Reconstructor:
     """One tomography reconstructor (``curecon_t``) on the current GPU."""
 
     def __init__(self, sysm, nbatch: int = 1, split: int = 1, maxit: Optional[int] = None,
-                 device: int = 0):
+                 device: int = 0, fit=None):
         self.lib = native.load()
         check(self.lib.mb_init(device), "mb_init")
         self.sys = sysm
+        self.fit_sys = fit
         self.nbatch = nbatch
-        d, keep = tomo_desc(sysm, nbatch=nbatch, split=split, maxit=maxit)
+        d, keep = tomo_desc(sysm, nbatch=nbatch, split=split, maxit=maxit, fit=fit)
         h = C.c_void_p()
         check(self.lib.mb_setup_recon(C.byref(d), C.byref(h)), "mb_setup_recon")
         self.h = h
         self.ngrad = int(self.lib.mb_ngrad(h))
         self.nxtot = int(self.lib.mb_nxtot(h))
+        self.nact = int(self.lib.mb_nact(h))
 
     def close(self):
         if getattr(self, "h", None):
@@ -140,6 +166,39 @@ class Reconstructor:
         check(self.lib.mb_tomo(self.h, _dptr(g), _dptr(x), res.ctypes.data_as(C.POINTER(C.c_float))),
               "mb_tomo")
         return x, res
+
+    def tomo_only(self, grad):
+        """gpu_tomo without copying the layer OPD back (the fit reads it on the device)."""
+        g = self._vec(grad, self.ngrad)
+        check(self.lib.mb_tomo(self.h, _dptr(g), C.POINTER(C.c_double)(), C.POINTER(C.c_float)()),
+              "mb_tomo")
+
+    def fit(self):
+        """gpu_fit: DM fit of the current tomography solution -> (dmfit, cgres)."""
+        a = np.empty((self.nbatch, self.nact))
+        res = np.empty(self.nbatch, dtype=np.float32)
+        check(self.lib.mb_fit(self.h, _dptr(a), res.ctypes.data_as(C.POINTER(C.c_float))), "mb_fit")
+        return a, res
+
+    def step_device(self, d_grad_ptr: int, stream_ptr: int = 0):
+        """Tomography + fit of one step on the device (one graph launch)."""
+        check(self.lib.mb_recon_step_device(self.h, C.c_void_p(d_grad_ptr), C.c_void_p(stream_ptr)),
+              "mb_recon_step_device")
+
+    def fit_solution_ptr(self) -> int:
+        return int(self.lib.mb_fit_solution(self.h))
+
+    def apply_fit_R(self, x):
+        xi = self._vec(x, self.nxtot)
+        out = np.empty((self.nbatch, self.nact))
+        check(self.lib.mb_apply_fit_R(self.h, _dptr(xi), _dptr(out)), "mb_apply_fit_R")
+        return out
+
+    def apply_fit_L(self, a):
+        ai = self._vec(a, self.nact)
+        out = np.empty((self.nbatch, self.nact))
+        check(self.lib.mb_apply_fit_L(self.h, _dptr(ai), _dptr(out)), "mb_apply_fit_L")
+        return out
 
     def tomo_device(self, d_grad_ptr: int, stream_ptr: int = 0):
         check(self.lib.mb_tomo_device(self.h, C.c_void_p(d_grad_ptr), C.c_void_p(stream_ptr)),

@@ -233,3 +233,60 @@ def tomo_solve(orc: TomoOracle, grad, x0=None, maxit=None):
 def mvm(M: np.ndarray, g: np.ndarray) -> np.ndarray:
     """``maos/recon.c:300``: DM commands from the control matrix."""
     return np.asarray(M, dtype=np.float64) @ np.asarray(g, dtype=np.float64)
+
+
+class FitOracle:
+    """FP64 DM-fit operators (grid form) on a :class:`maos_b200.fit_setup.FitSystem`.
+
+    ``fit_R``: ``maos/recon_utils.c:483`` FitR with HXF (bilinear ray tracing
+    from the layers onto the fit grid along each fit direction);
+    ``fit_L``: ``maos/recon_utils.c:536`` FitL (no slaving term)."""
+
+    def __init__(self, tomo_sys, fit_sys):
+        self.t = tomo_sys
+        self.f = fit_sys
+        self.HXF = [[prop_matrix(g, fit_sys.floc, tx * g.ht, ty * g.ht, 1.0) for g in tomo_sys.xmaps]
+                    for tx, ty in zip(fit_sys.thetax, fit_sys.thetay)]
+        self.xoff = tomo_sys.x_offsets()
+        self.aoff = fit_sys.act_offsets()
+
+    def _applyW(self, v, f):
+        wt = self.f.wt[f]
+        return wt * (self.f.W0 @ v) - wt * self.f.W1 * (self.f.W1 @ v)
+
+    def _hat(self, xp):
+        out = []
+        for d in range(len(self.f.dms)):
+            acc = np.zeros(len(self.f.dms[d].act))
+            for f in range(len(xp)):
+                acc += self.f.HA[f][d].T @ xp[f]
+            out.append(acc)
+        return np.concatenate(out)
+
+    def fit_R(self, x, alpha=1.0):
+        x = np.asarray(x, dtype=np.float64)
+        xs = [x[self.xoff[l]:self.xoff[l + 1]] for l in range(len(self.t.xmaps))]
+        xp = []
+        for f in range(len(self.f.thetax)):
+            v = sum(self.HXF[f][l] @ xs[l] for l in range(len(xs)))
+            xp.append(self._applyW(v, f))
+        return alpha * self._hat(xp)
+
+    def fit_L(self, a, alpha=1.0):
+        a = np.asarray(a, dtype=np.float64)
+        As = [a[self.aoff[d]:self.aoff[d + 1]] for d in range(len(self.f.dms))]
+        xp = []
+        for f in range(len(self.f.thetax)):
+            v = sum(self.f.HA[f][d] @ As[d] for d in range(len(As)))
+            xp.append(self._applyW(v, f))
+        out = self._hat(xp)
+        if self.f.NW.shape[1]:
+            out = out + self.f.NW @ (self.f.NW.T @ a)
+        return alpha * out
+
+
+def fit_solve(fo: FitOracle, x_layers, a0=None, maxit=None):
+    """DM fit of one step: FitR then CG on FitL, warm-started from a0 (recon.c:89-93)."""
+    maxit = fo.f.maxit if maxit is None else maxit
+    rhs = fo.fit_R(x_layers)
+    return pcg(a0, fo.fit_L, None, rhs, a0 is not None, maxit)

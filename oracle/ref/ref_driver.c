@@ -23,6 +23,8 @@
 #include "lib/pcg.h"
 #include "lib/mkg.h"
 #include "lib/accphi.h"
+#include "lib/mkh.h"
+#include "lib/mkw.h"
 
 typedef struct {
     int nwfs, nps, nthread;
@@ -396,4 +398,147 @@ void ref_loc_coords(int nx, int ny, double dx, double ox, double oy, double *x, 
     memcpy(x, l->locx, sizeof(double) * l->nloc);
     memcpy(y, l->locy, sizeof(double) * l->nloc);
     locfree(l);
+}
+
+/* ------------------------------------------------------------------------
+ * DM fit.  FIT_T is filled from the caller's fit grid, W0/W1, DM actuator
+ * locations and low-rank NW; HA and HXF are built by the reference's own mkh
+ * (lib/mkh.c:47) exactly as setup_fit_HA / setup_fit_HXF do
+ * (maos/setup_recon_fit.c:26-70).
+ * ---------------------------------------------------------------------- */
+static FIT_T *g_fit = NULL;
+static long *g_aoff = NULL;
+static int g_ndm = 0;
+
+int ref_fit_setup(void *hh, int nfit, const double *thetax, const double *thetay, const double *wt,
+                  const double *hs, int nf, const int *w0p, const int *w0i, const double *w0x,
+                  const double *w1, int ndm, const double *dmht, const double *dmdx, const int *nact,
+                  const double *alocx, const double *alocy, int nnw, const double *nw) {
+    refh_t *h = hh;
+    FIT_T *fit = calloc(1, sizeof(FIT_T));
+    fit->thetax = dnew(nfit, 1);
+    fit->thetay = dnew(nfit, 1);
+    fit->wt = dnew(nfit, 1);
+    fit->hs = dnew(nfit, 1);
+    for (int i = 0; i < nfit; i++) {
+        fit->thetax->p[i] = thetax[i];
+        fit->thetay->p[i] = thetay[i];
+        fit->wt->p[i] = wt[i];
+        fit->hs->p[i] = hs[i];
+    }
+    fit->floc = h->recon->ploc; /* fit grid is the pupil grid */
+    fit->xloc = h->recon->xloc;
+    fit->W0 = mk_csc(nf, nf, w0p, w0i, w0x);
+    fit->W1 = dnew(nf, 1);
+    memcpy(fit->W1->p, w1, sizeof(double) * nf);
+    fit->aloc = loccellnew(ndm, 1);
+    free(g_aoff);
+    g_aoff = calloc(ndm + 1, sizeof(long));
+    g_ndm = ndm;
+    for (int d = 0; d < ndm; d++) {
+        loc_t *a = locnew(nact[d], dmdx[d], dmdx[d]);
+        memcpy(a->locx, alocx + g_aoff[d], sizeof(double) * nact[d]);
+        memcpy(a->locy, alocy + g_aoff[d], sizeof(double) * nact[d]);
+        a->ht = dmht[d];
+        fit->aloc->p[d] = a;
+        g_aoff[d + 1] = g_aoff[d] + nact[d];
+    }
+    const int npsr = h->nps;
+    fit->HXF = dspcellnew(nfit, npsr);
+    fit->HA = dspcellnew(nfit, ndm);
+    for (int f = 0; f < nfit; f++) {
+        for (int ips = 0; ips < npsr; ips++) {
+            const double ht = fit->xloc->p[ips]->ht - fit->floc->ht;
+            const double scale = 1. - ht / hs[f];
+            fit->HXF->p[f + ips * nfit] =
+                mkh(fit->xloc->p[ips], fit->floc, thetax[f] * ht, thetay[f] * ht, scale);
+        }
+        for (int d = 0; d < ndm; d++) {
+            const double ht = fit->aloc->p[d]->ht - fit->floc->ht;
+            const double scale = 1. - ht / hs[f];
+            fit->HA->p[f + d * nfit] =
+                mkh(fit->aloc->p[d], fit->floc, thetax[f] * ht, thetay[f] * ht, scale);
+        }
+    }
+    if (nnw > 0) {
+        fit->NW = dcellnew(ndm, 1);
+        long ntot = g_aoff[ndm];
+        for (int d = 0; d < ndm; d++) {
+            fit->NW->p[d] = dnew(nact[d], nnw);
+            for (int k = 0; k < nnw; k++)
+                memcpy(fit->NW->p[d]->p + (long)k * nact[d], nw + (long)k * ntot + g_aoff[d],
+                       sizeof(double) * nact[d]);
+        }
+    }
+    g_fit = fit;
+    return 0;
+}
+
+/* HA[f][d] of the reference (CSC, nfloc x nact). Returns nnz; fills when p != NULL. */
+long ref_fit_ha(int f, int d, int *p, int *i, double *x) {
+    dsp *A = g_fit->HA->p[f + d * g_fit->thetax->nx];
+    long nnz = A->p[A->ny];
+    if (p) {
+        for (long k = 0; k <= A->ny; k++) p[k] = A->p[k];
+        for (long k = 0; k < nnz; k++) { i[k] = A->i[k]; x[k] = A->x[k]; }
+    }
+    return nnz;
+}
+
+static dcell *avec2cell(const double *v) {
+    dcell *c = dcellnew(g_ndm, 1);
+    for (int d = 0; d < g_ndm; d++) {
+        c->p[d] = dnew(g_aoff[d + 1] - g_aoff[d], 1);
+        if (v) memcpy(c->p[d]->p, v + g_aoff[d], sizeof(double) * (g_aoff[d + 1] - g_aoff[d]));
+    }
+    return c;
+}
+
+void ref_fitR(void *hh, const double *xin, double alpha, double *aout) {
+    refh_t *h = hh;
+    dcell *x = vec2cell(xin, h->xoff, h->nps);
+    dcell *a = avec2cell(NULL);
+    FitR(&a, g_fit, x, alpha);
+    cell2vec(aout, a, g_aoff, g_ndm);
+    dcellfree(x);
+    dcellfree(a);
+}
+
+void ref_fitL(void *hh, const double *ain, double alpha, double *aout) {
+    (void)hh;
+    dcell *a = avec2cell(ain);
+    dcell *y = avec2cell(NULL);
+    FitL(&y, g_fit, a, alpha);
+    cell2vec(aout, y, g_aoff, g_ndm);
+    dcellfree(a);
+    dcellfree(y);
+}
+
+double ref_fit_pcg(void *hh, const double *b, double *a, int warm, int maxit) {
+    (void)hh;
+    dcell *bb = avec2cell(b);
+    dcell *aa = avec2cell(a);
+    double res = pcg(&aa, FitL, g_fit, NULL, NULL, bb, warm, maxit);
+    cell2vec(a, aa, g_aoff, g_ndm);
+    dcellfree(bb);
+    dcellfree(aa);
+    return res;
+}
+
+/* mkw_amp (lib/mkw.c:41) on a square grid; returns nnz of W0 (CSC) */
+static dsp *last_w0 = NULL;
+static dmat *last_w1 = NULL;
+long ref_mkw_amp(int nx, int ny, double dx, double ox, double oy, const double *amp) {
+    loc_t *loc = mk_square_loc(nx, ny, dx, dx, ox, oy);
+    if (last_w0) dspfree(last_w0);
+    if (last_w1) dfree(last_w1);
+    mkw_amp(loc, (double *)amp, &last_w0, &last_w1);
+    locfree(loc);
+    return last_w0->p[last_w0->ny];
+}
+void ref_mkw_amp_get(int *p, int *i, double *x, double *w1) {
+    long nnz = last_w0->p[last_w0->ny];
+    for (long k = 0; k <= last_w0->ny; k++) p[k] = last_w0->p[k];
+    for (long k = 0; k < nnz; k++) { i[k] = last_w0->i[k]; x[k] = last_w0->x[k]; }
+    memcpy(w1, last_w1->p, sizeof(double) * last_w1->nx);
 }

@@ -4,8 +4,9 @@
 (sys/, math/, lib/, maos/ compiled from its sources by ``oracle/ref/Makefile``)
 plus a flat driver (``oracle/ref/ref_driver.c``).  It is loaded in a separate
 process started with ``spawn``: the reference installs signal handlers and its
-own OpenMP runtime at load time, and it reads ``$HOME``; the worker points
-``HOME`` at ``oracle/_ref/home`` so nothing is written outside the repository.
+own OpenMP runtime at load time, and it reads ``$HOME``; the worker runs in
+``oracle/_ref/home`` with ``HOME=.`` so nothing is written outside the
+repository.
 
 Only tests, ``smoke()`` and the CPU-baseline leg of ``bench.py`` use this.
 """
@@ -157,6 +158,69 @@ class _Worker:
                       ctypes.byref(nr), ctypes.byref(nc))
         return p, i, x, nr.value, nc.value
 
+    def fit_setup(self, fd):
+        L = self.lib
+        keep = []
+
+        def d(a):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(a)
+            return a.ctypes.data_as(_D)
+
+        def i32(a):
+            a = np.ascontiguousarray(a, dtype=np.int32)
+            keep.append(a)
+            return a.ctypes.data_as(_I)
+
+        L.ref_fit_setup(self.h, fd["nfit"], d(fd["thetax"]), d(fd["thetay"]), d(fd["wt"]),
+                        d(fd["hs"]), fd["nf"], i32(fd["w0_p"]), i32(fd["w0_i"]), d(fd["w0_x"]),
+                        d(fd["w1"]), fd["ndm"], d(fd["dmht"]), d(fd["dmdx"]), i32(fd["nact"]),
+                        d(fd["alocx"]), d(fd["alocy"]), fd["nnw"], d(fd["nw"]))
+        self.keep += keep
+        self.na = int(np.sum(fd["nact"]))
+        self.nfit = fd["nfit"]
+        return True
+
+    def fitR(self, x, alpha=1.0):
+        out = np.zeros(self.na)
+        self.lib.ref_fitR(self.h, _dp(x), ctypes.c_double(alpha), out.ctypes.data_as(_D))
+        return out
+
+    def fitL(self, a, alpha=1.0):
+        out = np.zeros(self.na)
+        self.lib.ref_fitL(self.h, _dp(a), ctypes.c_double(alpha), out.ctypes.data_as(_D))
+        return out
+
+    def fit_pcg(self, b, a0, warm, maxit):
+        a = np.array(a0, dtype=np.float64) if a0 is not None else np.zeros(self.na)
+        self.lib.ref_fit_pcg.restype = ctypes.c_double
+        res = self.lib.ref_fit_pcg(self.h, _dp(b), a.ctypes.data_as(_D), int(warm), int(maxit))
+        return a, res
+
+    def fit_ha(self, f, d, nrow, ncol):
+        L = self.lib
+        L.ref_fit_ha.restype = ctypes.c_long
+        nnz = L.ref_fit_ha(f, d, None, None, None)
+        p = np.zeros(ncol + 1, dtype=np.int32)
+        i = np.zeros(nnz, dtype=np.int32)
+        x = np.zeros(nnz)
+        L.ref_fit_ha(f, d, p.ctypes.data_as(_I), i.ctypes.data_as(_I), x.ctypes.data_as(_D))
+        return p, i, x
+
+    def mkw_amp(self, grid, amp):
+        L = self.lib
+        L.ref_mkw_amp.restype = ctypes.c_long
+        nnz = L.ref_mkw_amp(grid[0], grid[1], ctypes.c_double(grid[2]), ctypes.c_double(grid[3]),
+                            ctypes.c_double(grid[4]), _dp(amp))
+        n = grid[0] * grid[1]
+        p = np.zeros(n + 1, dtype=np.int32)
+        i = np.zeros(nnz, dtype=np.int32)
+        x = np.zeros(nnz)
+        w1 = np.zeros(n)
+        L.ref_mkw_amp_get(p.ctypes.data_as(_I), i.ctypes.data_as(_I), x.ctypes.data_as(_D),
+                          w1.ctypes.data_as(_D))
+        return p, i, x, w1
+
     def loc_coords(self, grid):
         n = grid[0] * grid[1]
         x = np.zeros(n)
@@ -166,7 +230,14 @@ class _Worker:
         return x, y
 
 
-def _serve(conn, nthread):
+def _serve(conn, nthread, home):
+    # The reference formats $HOME/.aos/... into a 64-byte buffer
+    # (math/fft.c fnwisdom); run from inside the home folder with HOME="."
+    # so the path stays short wherever the repository lives.
+    os.chdir(home)
+    os.environ["HOME"] = "."
+    os.environ["USER"] = "maosref"
+    os.environ["OMP_NUM_THREADS"] = str(nthread)
     w = _Worker(nthread)
     while True:
         msg = conn.recv()
@@ -189,19 +260,8 @@ class RefProcess:
         self.conn, child = ctx.Pipe()
         home = os.path.join(HERE, "_ref", "home")
         os.makedirs(os.path.join(home, ".aos", "cache"), exist_ok=True)
-        env_backup = {k: os.environ.get(k) for k in ("HOME", "USER", "OMP_NUM_THREADS")}
-        os.environ["HOME"] = home
-        os.environ["USER"] = "maosref"
-        os.environ["OMP_NUM_THREADS"] = str(nthread)
-        try:
-            self.proc = ctx.Process(target=_serve, args=(child, nthread), daemon=True)
-            self.proc.start()
-        finally:
-            for k, v in env_backup.items():
-                if v is None:
-                    os.environ.pop(k, None)
-                else:
-                    os.environ[k] = v
+        self.proc = ctx.Process(target=_serve, args=(child, nthread, home), daemon=True)
+        self.proc.start()
 
     def call(self, name: str, *args, **kw) -> Any:
         self.conn.send((name, args, kw))
@@ -224,6 +284,20 @@ class RefProcess:
 
     def __exit__(self, *a):
         self.close()
+
+
+def fit_desc(fs) -> dict:
+    """Flatten a FitSystem for ``ref_fit_setup``."""
+    W0 = fs.W0.tocsc()
+    W0.sort_indices()
+    return {"nfit": len(fs.thetax), "thetax": fs.thetax, "thetay": fs.thetay, "wt": fs.wt,
+            "hs": np.where(np.isfinite(fs.hs), fs.hs, np.inf), "nf": fs.floc.n,
+            "w0_p": W0.indptr, "w0_i": W0.indices, "w0_x": W0.data, "w1": fs.W1,
+            "ndm": len(fs.dms), "dmht": [d.ht for d in fs.dms], "dmdx": [d.amap.dx for d in fs.dms],
+            "nact": [len(d.act) for d in fs.dms],
+            "alocx": np.concatenate([d.locx for d in fs.dms]),
+            "alocy": np.concatenate([d.locy for d in fs.dms]),
+            "nnw": fs.NW.shape[1], "nw": np.asfortranarray(fs.NW).ravel(order="F")}
 
 
 def system_desc(sysm, split: int = 1) -> dict:

@@ -24,6 +24,17 @@ def get_system(name: str):
     return _SYS_CACHE[name]
 
 
+_FIT_CACHE = {}
+
+
+def get_fit(name: str):
+    """Build (once per session) the DM-fit tables of a preset."""
+    if name not in _FIT_CACHE:
+        from maos_b200 import fit_setup
+        _FIT_CACHE[name] = fit_setup.build_fit(get_system(name))
+    return _FIT_CACHE[name]
+
+
 @pytest.fixture(scope="session")
 def ltao():
     return get_system("ltao_8m")

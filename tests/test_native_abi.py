@@ -57,3 +57,14 @@ def test_null_arguments_are_rejected_without_a_gpu(lib):
     assert lib.mb_setup_recon(None, None) == -1
     assert lib.mb_tomo(None, None, None, None) == -1
     assert lib.mb_recon_reset(None) == -1
+
+
+def test_mvm_rejects_bad_arguments(lib):
+    import numpy as np
+    h = ctypes.c_void_p()
+    M = np.zeros(4)
+    P = ctypes.POINTER(ctypes.c_double)
+    lib.mb_mvm_create.argtypes = [P, ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_void_p)]
+    assert lib.mb_mvm_create(M.ctypes.data_as(P), 2, 2, 7, 1, ctypes.byref(h)) == -1
+    assert lib.mb_mvm_create(None, 2, 2, 0, 1, ctypes.byref(h)) == -1

@@ -92,3 +92,41 @@ def test_gradient_operator_matches_reference_mkg(ref_proc, ltao):
     G = sps.csc_matrix((x, i, p), shape=(nr, nc)).toarray()
     assert G.shape == w.GP.shape
     assert np.abs(G - w.GP.toarray()).max() <= 1e-12 * np.abs(G).max()
+
+
+@pytest.mark.parametrize("name", ["ltao_8m", "mcao_30m"])
+def test_fit_operators_match_reference(name, ref_proc):
+    """FitR/FitL/CG of the oracle vs the reference's FitR/FitL/pcg, whose HA
+    and HXF the driver builds with the reference's own mkh."""
+    from conftest import get_system, get_fit
+    from oracle.recon_oracle import FitOracle
+    s = get_system(name)
+    fs = get_fit(name)
+    R = ref_proc
+    R.call("setup", refbridge.system_desc(s, split=1))
+    R.call("fit_setup", refbridge.fit_desc(fs))
+    fo = FitOracle(s, fs)
+    rng = np.random.default_rng(21)
+    x = rng.standard_normal(s.nx_total)
+    a = rng.standard_normal(fs.nact)
+    assert rel(fo.fit_R(x), R.call("fitR", x)) < 1e-12
+    assert rel(fo.fit_L(a), R.call("fitL", a)) < 1e-12
+    b = fo.fit_R(x)
+    a1, r1 = pcg(None, fo.fit_L, None, b, False, fs.maxit)
+    a2, r2 = R.call("fit_pcg", b, None, 0, fs.maxit)
+    assert rel(a1, a2) < 1e-10
+
+
+def test_fit_weighting_matches_reference_mkw_amp(ref_proc, ltao):
+    import scipy.sparse as sps
+    from maos_b200.fit_setup import mkw_amp
+    from maos_b200.geometry import annulus_fraction
+    g = ltao.pmap
+    X, Y = np.meshgrid(g.xs() - g.dx / 2, g.ys() - g.dy / 2)
+    amp = annulus_fraction(X.ravel(), Y.ravel(), g.dx, 0.5, 4.0, nsub=8)
+    amp /= amp.sum()
+    W0, W1 = mkw_amp(g, amp)
+    p, i, x, w1 = ref_proc.call("mkw_amp", (g.nx, g.ny, g.dx, g.ox, g.oy), amp)
+    Wr = sps.csc_matrix((x, i, p), shape=(g.n, g.n))
+    assert abs(W0 - Wr).max() <= 1e-14 * abs(Wr).max()
+    assert np.abs(W1 - w1).max() <= 1e-14 * np.abs(w1).max()
