@@ -193,6 +193,24 @@ int mb_recon_mvm(mb_mvm *m, const double *grad, double *dmout);
 /* Device form: FP32 [nbatch][ngrad] in, FP32 [nbatch][nact] out, on `stream`. */
 int mb_mvm_apply_device(mb_mvm *m, const float *d_grad, float *d_out, void *stream);
 
+/* Allocation-free FP32 MVM.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory -- a real-time control loop
+ * that must never block on cudaMalloc (which can synchronise the device and
+ * take unbounded time), or code that runs where allocation is not allowed.
+ * The caller passes M (device, FP32, row-major nact x ngrad with leading
+ * dimension ldm: ldm >= ngrad, ldm a multiple of 4, M 16-byte aligned), the
+ * gradients d_grad [nbatch][ngrad] and the output d_out [nbatch][nact], all on
+ * the device.  The split-K partial sums go to one static device array of
+ * MB_NOALLOC_MAX_PARTIALS floats (4 MiB, held by every GPU that loads the
+ * library until exit); a call needing more, ceil(ngrad/2048)*nbatch*nact,
+ * returns MB_EINVAL with the sizes in the message.  The first call on a device
+ * looks up the array's address on that device; make that first call before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU
+ * race.  It calls no cudaMalloc/cudaFree. */
+#define MB_NOALLOC_MAX_PARTIALS 1048576
+int mb_mvm_apply_noalloc(const float *d_M, long nact, long ngrad, long ldm, const float *d_grad,
+                         float *d_out, int nbatch, void *stream);
+
 /* Per-stage timing for roofline accounting.  Stages are the kernels of one
  * CG iteration (see mb_stage_name).  For each stage: average device time of
  * one launch over `reps` back-to-back launches on the reconstructor's stream

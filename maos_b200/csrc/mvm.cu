@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -182,6 +184,109 @@ struct mb_mvm {
     mb::Mvm M;
 };
 
+// ---------------------------------------------------------------------------
+// Allocation-free MVM for callers that must not allocate device memory.
+//
+// The split-K partial sums live in one file-scope device array of
+// MB_NOALLOC_MAX_PARTIALS floats (4 MiB), which every GPU that loads this
+// library holds until the process exits.  Host code cannot pass the array's
+// name to a kernel (on the host it is only a stand-in symbol), so the first
+// call on each device looks up its device address with cudaGetSymbolAddress,
+// with that device current, and keeps it.  Every partial that the reduction
+// reads is written by the same call first, so nothing needs clearing between
+// calls; calls that overlap on the GPU share the array and race.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) float g_noalloc_partials[MB_NOALLOC_MAX_PARTIALS];
+
+namespace mb {
+
+// Same split-K product as k_mvm_split for an FP32 row-major M with any
+// ngrad: full 16-byte vectors up to the last multiple of 4 in the slab, then
+// a scalar tail.  ldm must be a multiple of 4 and M 16-byte aligned.
+template <int NB>
+__global__ void __launch_bounds__(kMvmThreads)
+k_mvm_split_f32_ragged(const float *__restrict__ M, long ldm, const float *__restrict__ g,
+                       long ngrad, float *__restrict__ part, int nact, int nbatch, int b0) {
+    extern __shared__ float sg[];  // [NB][kK]
+    const int ks = blockIdx.y;
+    const long k0 = (long)ks * kK;
+    const int kn = (int)((ngrad - k0) < kK ? (ngrad - k0) : kK);
+    const int kn4 = kn & ~3;
+    for (int i = threadIdx.x; i < NB * kK; i += blockDim.x) {
+        const int b = i / kK, k = i - b * kK;
+        sg[i] = (b0 + b < nbatch && k < kn) ? g[(size_t)(b0 + b) * ngrad + k0 + k] : 0.f;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int kRowsPerWarp = kRows / (kMvmThreads / 32);
+    for (int rr = 0; rr < kRowsPerWarp; rr++) {
+        const int row = blockIdx.x * kRows + warp * kRowsPerWarp + rr;
+        if (row >= nact) break;
+        const float *mrow = M + (size_t)row * ldm + k0;
+        float acc[NB];
+#pragma unroll
+        for (int b = 0; b < NB; b++) acc[b] = 0.f;
+        for (int c = lane * 4; c < kn4; c += 128) {
+            const float4 v = *reinterpret_cast<const float4 *>(mrow + c);
+#pragma unroll
+            for (int b = 0; b < NB; b++) {
+                const float4 q = *reinterpret_cast<const float4 *>(sg + b * kK + c);
+                acc[b] += v.x * q.x + v.y * q.y + v.z * q.z + v.w * q.w;
+            }
+        }
+        for (int c = kn4 + lane; c < kn; c += 32) {
+            const float v = mrow[c];
+#pragma unroll
+            for (int b = 0; b < NB; b++) acc[b] += v * sg[b * kK + c];
+        }
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            float t = acc[b];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0 && b0 + b < nbatch) part[((size_t)ks * nbatch + b0 + b) * nact + row] = t;
+        }
+    }
+}
+
+static std::mutex g_noalloc_mu;
+static float *g_noalloc_ptr[256] = {};
+
+// Once per device, with that device current: the scratch array's device
+// address and the shared-memory opt-in of the kernel variants.
+static float *noalloc_scratch(int dev) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        float *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_partials);
+        if (e != cudaSuccess || !ptr) {
+            set_error("cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+            throw CudaError{MB_ECUDA};
+        }
+        MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_split_f32_ragged<1>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 1 * kK * 4));
+        MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_split_f32_ragged<4>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * kK * 4));
+        MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_split_f32_ragged<8>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * kK * 4));
+        g_noalloc_ptr[dev] = ptr;
+    }
+    return g_noalloc_ptr[dev];
+}
+
+template <int NB>
+static void noalloc_launch(const float *M, long ldm, const float *g, long ngrad, float *part, int nact,
+                           int nbatch, int nks, cudaStream_t s) {
+    const dim3 grid((nact + kRows - 1) / kRows, nks);
+    for (int b0 = 0; b0 < nbatch; b0 += NB) {
+        k_mvm_split_f32_ragged<NB><<<grid, kMvmThreads, (size_t)NB * kK * 4, s>>>(M, ldm, g, ngrad, part, nact,
+                                                                                  nbatch, b0);
+        MB_CHECK_LAUNCH();
+    }
+}
+
+}  // namespace mb
+
 extern "C" {
 
 int mb_mvm_create(const double *Mcol, long nact, long ngrad, int dtype, int nbatch, mb_mvm **out) {
@@ -266,6 +371,44 @@ int mb_mvm_apply_device(mb_mvm *h, const float *d_grad, float *d_out, void *stre
     }
     try {
         h->M.apply(d_grad, d_out, (cudaStream_t)stream);
+    } catch (const mb::CudaError &e) {
+        return e.code;
+    }
+    return MB_OK;
+}
+
+int mb_mvm_apply_noalloc(const float *d_M, long nact, long ngrad, long ldm, const float *d_grad,
+                         float *d_out, int nbatch, void *stream) {
+    if (!d_M || !d_grad || !d_out || nact <= 0 || ngrad <= 0 || nbatch < 1 || ldm < ngrad ||
+        (ldm & 3) || ((uintptr_t)d_M & 15)) {
+        mb::set_error("mb_mvm_apply_noalloc: invalid arguments (ldm >= ngrad, ldm %% 4 == 0, "
+                      "M 16-byte aligned)");
+        return MB_EINVAL;
+    }
+    const long nks = (ngrad + mb::kK - 1) / mb::kK;
+    const long need = nks * (long)nbatch * nact;
+    if (need > MB_NOALLOC_MAX_PARTIALS) {
+        mb::set_error("mb_mvm_apply_noalloc: needs %ld partial sums (%ld K slabs x %d instances x %ld "
+                      "rows); the static scratch holds %d",
+                      need, nks, nbatch, nact, (int)MB_NOALLOC_MAX_PARTIALS);
+        return MB_EINVAL;
+    }
+    try {
+        int dev = 0;
+        MB_CUDA_TRY(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 256) {
+            mb::set_error("mb_mvm_apply_noalloc: device index %d", dev);
+            return MB_EINVAL;
+        }
+        float *part = mb::noalloc_scratch(dev);
+        cudaStream_t s = (cudaStream_t)stream;
+        if (nbatch == 1) mb::noalloc_launch<1>(d_M, ldm, d_grad, ngrad, part, (int)nact, nbatch, (int)nks, s);
+        else if (nbatch <= 4) mb::noalloc_launch<4>(d_M, ldm, d_grad, ngrad, part, (int)nact, nbatch, (int)nks, s);
+        else mb::noalloc_launch<8>(d_M, ldm, d_grad, ngrad, part, (int)nact, nbatch, (int)nks, s);
+        const long n = nact * (long)nbatch;
+        mb::k_mvm_reduce<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part, nullptr, d_out, (int)nact, nbatch,
+                                                                    (int)nks);
+        MB_CHECK_LAUNCH();
     } catch (const mb::CudaError &e) {
         return e.code;
     }

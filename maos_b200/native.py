@@ -91,6 +91,8 @@ SIGNATURES = {
     "mb_mvm_bytes": (C.c_long, [C.c_void_p]),
     "mb_recon_mvm": (C.c_int, [C.c_void_p, _D, _D]),
     "mb_mvm_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mb_mvm_apply_noalloc": (C.c_int, [C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_void_p, C.c_void_p,
+                                       C.c_int, C.c_void_p]),
     "mb_error_string": (C.c_char_p, [C.c_int]),
     "mb_last_error_message": (C.c_char_p, []),
     "mb_version": (C.c_int, []),
