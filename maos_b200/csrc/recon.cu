@@ -102,7 +102,9 @@ struct Recon {
     // state and work buffers
     DevBuf<float> x, r, p, z, Ap, rhs, opd, opd2, grad, gin;
     DevBuf<double> tt_part, pap_part, rr_part, rz_part, bb_part, sc;
-    DevBuf<float> res;
+    DevBuf<float> res, ab, tt;
+    DevBuf<unsigned> cnt, cnt_tt;
+    CgScal scal() const { return CgScal{sc.p, nsc, ab.p, cnt.p, res.p}; }
 
     // DM fit
     int has_fit = 0, nfit = 0, ndm = 0, nfx = 0, nfy = 0, nf = 0, nnw = 0, fit_maxit = 0;
@@ -115,7 +117,9 @@ struct Recon {
     DevBuf<float> w0_v, w1v, fwt, nwv;
     DevBuf<float> fa, fr, fp, fAp, frhs, opdf, opdw;
     DevBuf<double> w1_part, nw_part, f_pap, f_rr, f_rz, f_bb, fsc;
-    DevBuf<float> fres;
+    DevBuf<float> fres, fab;
+    DevBuf<unsigned> fcnt;
+    CgScal fscal() const { return CgScal{fsc.p, fnsc, fab.p, fcnt.p, fres.p}; }
 
     cudaGraphExec_t graph = nullptr;       // tomography step
     cudaGraphExec_t graph_fit = nullptr;   // fit step
@@ -143,21 +147,21 @@ struct Recon {
     // operator pieces (enqueue on `s`)
     void op_hx(const float *xin, cudaStream_t s);
     void op_rhs(const float *g, float *out, cudaStream_t s);
-    void op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t s);
-    void op_fdpcg(const float *rin, float *zout, double *rz_part, cudaStream_t s);
+    void op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t s, int k = 0);
+    void op_fdpcg(const float *rin, float *zout, double *rz_part, cudaStream_t s, int k = 0,
+                  int init = 0, bool in_cg = false);
     void enqueue_solve(cudaStream_t s);
     struct CgBufs {
         float *x, *r, *p, *z, *Ap, *rhs;
-        double *pap, *rr, *rz, *bb, *sc;
-        float *res;
-        int nsc;
-        int nblk_pap;  // partials the A-multiply writes for p.Ap
+        double *pap, *rr, *rz, *bb;
+        CgScal S;
     };
-    void enqueue_cg(const CgBufs &B, long n, int nblk, int iters,
-                    const std::function<void(const float *, float *, double *)> &Amul,
-                    const std::function<void(const float *, float *, double *)> &Mmul, cudaStream_t s);
+    using AmulFn = std::function<void(const float *, float *, double *, int)>;
+    using MmulFn = std::function<void(const float *, float *, double *, int, int)>;
+    void enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulFn &Amul,
+                    const MmulFn &Mmul, cudaStream_t s);
     void op_fitR(const float *xin, float *out, cudaStream_t s);
-    void op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t s);
+    void op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t s, int k = 0);
     void enqueue_fit(cudaStream_t s);
     void time_stages(int reps, float *ms, double *bytes, int *launches);
     void capture_graph();
@@ -540,12 +544,20 @@ void Recon::build(const mb_recon_desc *d) {
     bb_part.alloc((size_t)nb * nblk_x);
     sc.alloc((size_t)nb * nsc);
     res.alloc(nb);
+    ab.alloc((size_t)nb * 2);
+    tt.alloc((size_t)nb * nwfs * 2);
+    cnt.alloc(nb);
+    cnt_tt.alloc((size_t)nb * nwfs);
     if (precond) build_fdpcg(d->fdpcg);
     if (d->fit) build_fit(d->fit);
     x.zero_async(stream);
     gin.zero_async(stream);
     sc.zero_async(stream);
     res.zero_async(stream);
+    ab.zero_async(stream);
+    tt.zero_async(stream);
+    cnt.zero_async(stream);
+    cnt_tt.zero_async(stream);
     MB_CUDA_TRY(cudaStreamSynchronize(stream));
     capture_graph();
 }
@@ -562,34 +574,37 @@ void Recon::op_hx(const float *xin, cudaStream_t s) {
 void Recon::op_rhs(const float *g, float *out, cudaStream_t s) {
     // TomoR: x = Hx^T GP^T NEA^-1 (I - TT PTT) g   (recon_utils.c:397, tomo.cu:607)
     k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, s>>>(nullptr, g, grad.p, tt_part.p, wfs.p, nwfs,
-                                                      nxp, np, ngrad, 1);
+                                                      nxp, np, ngrad, 1, tt.p, cnt_tt.p);
     MB_CHECK_LAUNCH();
-    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt_part.p, opd2.p, wfs.p, nwfs,
-                                                          nxp, nyp, ngrad, nblk_tt, 1, 1.f);
+    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt.p, opd2.p, wfs.p, nwfs, nxp, nyp,
+                                                          ngrad, 1, 1.f);
     MB_CHECK_LAUNCH();
     k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, s>>>(opd2.p, nullptr, out, nullptr, hx.gi(), lay.p,
                                                             tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
-                                                            nxtot, 0, 1.f, maxrows, maxnx, maxent);
+                                                            nxtot, 0, 1.f, maxrows, maxnx, maxent,
+                                                            scal(), 0);
     MB_CHECK_LAUNCH();
 }
 
-void Recon::op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t s) {
+void Recon::op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t s, int k) {
     // TomoL: Hx^T GP^T NEA^-1 (I - TT PTT) GP Hx x + L2^T L2 x   (recon_utils.c:447, tomo.cu:639)
     op_hx(xin, s);
     const int do_tt = split ? 0 : 1;
     k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, s>>>(opd.p, nullptr, grad.p, tt_part.p, wfs.p,
-                                                      nwfs, nxp, np, ngrad, do_tt);
+                                                      nwfs, nxp, np, ngrad, do_tt, tt.p, cnt_tt.p);
     MB_CHECK_LAUNCH();
-    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt_part.p, opd2.p, wfs.p, nwfs,
-                                                          nxp, nyp, ngrad, nblk_tt, do_tt, 1.f);
+    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt.p, opd2.p, wfs.p, nwfs, nxp, nyp,
+                                                          ngrad, do_tt, 1.f);
     MB_CHECK_LAUNCH();
     k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, s>>>(opd2.p, xin, out, dot_part, hx.gi(), lay.p,
                                                             tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
-                                                            nxtot, 1, 1.f, maxrows, maxnx, maxent);
+                                                            nxtot, 1, 1.f, maxrows, maxnx, maxent,
+                                                            scal(), k);
     MB_CHECK_LAUNCH();
 }
 
-void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s) {
+void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s, int k, int init,
+                     bool in_cg) {
     // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT
     k_fd_pack<<<dim3(nblk_x, nb), kThreads, 0, s>>>(rin, spec.p, lay.p, fd_soff.p, nps, nxtot);
     MB_CHECK_LAUNCH();
@@ -605,58 +620,53 @@ void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s)
         MB_CUFFT_TRY(cufftExecC2C(plans[i], spec2.p + plan_off[i], spec2.p + plan_off[i], CUFFT_INVERSE));
         count_launches(1);
     }
+    CgScal S = in_cg ? scal() : CgScal{};
     k_fd_unpack<<<dim3(nblk_x, nb), kThreads, 0, s>>>(spec2.p, rin, zout, rzp, lay.p, fd_soff.p, nps,
-                                                     nxtot);
+                                                     nxtot, S, k, init);
     MB_CHECK_LAUNCH();
 }
 
 // (Preconditioned) CG with FP64 scalars, the schedule of lib/pcg.c:28 and
 // cuda/pcg.cu:87 (the restart every 100/500 iterations is never reached for
 // the iteration counts used per step).  x holds the warm start.
-void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters,
-                       const std::function<void(const float *, float *, double *)> &Amul,
-                       const std::function<void(const float *, float *, double *)> &Mmul,
-                       cudaStream_t s) {
+void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulFn &Amul,
+                       const MmulFn &Mmul, cudaStream_t s) {
     // r = b - A x ; b.b
-    Amul(B.x, B.Ap, nullptr);
-    k_cg_init_r<<<dim3(nblk, nb), kThreads, 0, s>>>(B.rhs, B.Ap, B.r, B.bb, n);
+    Amul(B.x, B.Ap, nullptr, 0);
+    k_cg_init_r<<<dim3(nblk, nb), kThreads, 0, s>>>(B.rhs, B.Ap, B.r, B.bb, n, B.S, iters);
     MB_CHECK_LAUNCH();
     float *zp = B.r;
     if (Mmul) {
-        Mmul(B.r, B.z, B.rz);
+        Mmul(B.r, B.z, B.rz, 0, 1);
         zp = B.z;
     } else {
-        k_dot_self<<<dim3(nblk, nb), kThreads, 0, s>>>(B.r, B.rz, n);  // z aliases r
+        k_dot_self<<<dim3(nblk, nb), kThreads, 0, s>>>(B.r, B.rz, n, B.S);  // z aliases r
         MB_CHECK_LAUNCH();
     }
-    k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, B.rz, B.sc, B.nsc, 0, n, nblk, 1);
+    k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, n, B.S, 1);
     MB_CHECK_LAUNCH();
     for (int k = 0; k < iters; k++) {
-        Amul(B.p, B.Ap, B.pap);
-        k_cg_update_xr<<<dim3(nblk, nb), kThreads, 0, s>>>(B.x, B.r, B.p, B.Ap, B.pap, B.rr, B.sc,
-                                                          B.nsc, k, n, B.nblk_pap);
+        Amul(B.p, B.Ap, B.pap, k);  // its last block leaves alpha_k
+        k_cg_update_xr<<<dim3(nblk, nb), kThreads, 0, s>>>(B.x, B.r, B.p, B.Ap, B.rr, n, B.S, k, iters,
+                                                          Mmul ? 0 : 1);
         MB_CHECK_LAUNCH();
         if (k + 1 == iters) break;
-        const double *rzp_k = B.rr;
-        if (Mmul) {
-            Mmul(B.r, B.z, B.rz);
-            rzp_k = B.rz;
-        }
-        k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, rzp_k, B.sc, B.nsc, k, n, nblk, 0);
+        if (Mmul) Mmul(B.r, B.z, B.rz, k, 0);  // its last block leaves beta_k
+        k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, n, B.S, 0);
         MB_CHECK_LAUNCH();
     }
-    k_cg_residual<<<dim3(1, nb), 32, 0, s>>>(B.rr, B.bb, B.sc, B.res, B.nsc, iters + 2, nblk);
-    MB_CHECK_LAUNCH();
 }
 
 // The whole per-step tomography: RHS, then (FD)PCG from the warm start in x.
 void Recon::enqueue_solve(cudaStream_t s) {
     op_rhs(gin.p, rhs.p, s);
-    CgBufs B{x.p, r.p, p.p, z.p, Ap.p, rhs.p, pap_part.p, rr_part.p, rz_part.p, bb_part.p, sc.p, res.p, nsc,
-             ntiles};
-    auto A = [&](const float *in, float *out, double *dot) { op_lhs(in, out, dot, s); };
-    std::function<void(const float *, float *, double *)> M;
-    if (precond) M = [&](const float *in, float *out, double *dot) { op_fdpcg(in, out, dot, s); };
+    CgBufs B{x.p, r.p, p.p, z.p, Ap.p, rhs.p, pap_part.p, rr_part.p, rz_part.p, bb_part.p, scal()};
+    AmulFn A = [&](const float *in, float *out, double *dot, int k) { op_lhs(in, out, dot, s, k); };
+    MmulFn M;
+    if (precond)
+        M = [&](const float *in, float *out, double *dot, int k, int init) {
+            op_fdpcg(in, out, dot, s, k, init, true);
+        };
     enqueue_cg(B, nxtot, nblk_x, maxit, A, M, s);
 }
 
@@ -669,12 +679,12 @@ void Recon::op_fitR(const float *xin, float *out, cudaStream_t s) {
                                                        fwt.p, w1_part.p, nblk_f, nf, nfit);
     MB_CHECK_LAUNCH();
     k_hxt<<<dim3(nblk_a, nb), kThreads, 0, s>>>(opdw.p, nullptr, out, nullptr, ha.gi(), dmlay.p, ndm,
-                                               nfit, nfx, nfy, nact, 0, 1.f, LowRank{});
+                                               nfit, nfx, nfy, nact, 0, 1.f, LowRank{}, fscal(), 0);
     MB_CHECK_LAUNCH();
 }
 
 // FitL: sum_f wt_f HA_f^T (W0 - W1 W1^T) HA_f a + NW NW^T a   (recon_utils.c:536, fit.cu:213)
-void Recon::op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t s) {
+void Recon::op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t s, int k) {
     LowRank lr{};
     if (nnw) {
         k_lowrank_dot<<<dim3(nblk_a, nb), kThreads, 0, s>>>(ain, nwv.p, nw_part.p, nnw, nact);
@@ -688,7 +698,7 @@ void Recon::op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t
                                                        fwt.p, w1_part.p, nblk_f, nf, nfit);
     MB_CHECK_LAUNCH();
     k_hxt<<<dim3(nblk_a, nb), kThreads, 0, s>>>(opdw.p, ain, out, dot_part, ha.gi(), dmlay.p, ndm, nfit,
-                                               nfx, nfy, nact, 0, 1.f, lr);
+                                               nfx, nfy, nact, 0, 1.f, lr, fscal(), k);
     MB_CHECK_LAUNCH();
 }
 
@@ -696,10 +706,9 @@ void Recon::op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t
 // started from the previous commands (curecon_t::fit, cuda/recon.cu:277).
 void Recon::enqueue_fit(cudaStream_t s) {
     op_fitR(x.p, frhs.p, s);
-    CgBufs B{fa.p, fr.p, fp.p, fr.p, fAp.p, frhs.p, f_pap.p, f_rr.p, f_rz.p, f_bb.p, fsc.p, fres.p, fnsc,
-             nblk_a};
-    auto A = [&](const float *in, float *out, double *dot) { op_fitL(in, out, dot, s); };
-    enqueue_cg(B, nact, nblk_a, fit_maxit, A, nullptr, s);
+    CgBufs B{fa.p, fr.p, fp.p, fr.p, fAp.p, frhs.p, f_pap.p, f_rr.p, f_rz.p, f_bb.p, fscal()};
+    AmulFn A = [&](const float *in, float *out, double *dot, int k) { op_fitL(in, out, dot, s, k); };
+    enqueue_cg(B, nact, nblk_a, fit_maxit, A, MmulFn(), s);
 }
 
 void Recon::build_fit(const mb_fit_desc *f) {
@@ -786,9 +795,13 @@ void Recon::build_fit(const mb_fit_desc *f) {
     f_rz.alloc((size_t)nb * nblk_a); f_bb.alloc((size_t)nb * nblk_a);
     fsc.alloc((size_t)nb * fnsc);
     fres.alloc(nb);
+    fab.alloc((size_t)nb * 2);
+    fcnt.alloc(nb);
     fa.zero_async(stream);
     fsc.zero_async(stream);
     fres.zero_async(stream);
+    fab.zero_async(stream);
+    fcnt.zero_async(stream);
 }
 
 // Time each iteration stage alone and report its algorithmic traffic.
@@ -838,31 +851,31 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                 case 0: op_hx(p.p, stream); break;
                 case 1:
                     k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, stream>>>(opd.p, nullptr, grad.p, tt_part.p,
-                                                                          wfs.p, nwfs, nxp, np, ngrad, 1);
+                                                                          wfs.p, nwfs, nxp, np, ngrad, 1, tt.p,
+                                                                          cnt_tt.p);
                     MB_CHECK_LAUNCH();
                     break;
                 case 2:
-                    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, stream>>>(grad.p, tt_part.p, opd2.p,
-                                                                               wfs.p, nwfs, nxp, nyp, ngrad,
-                                                                               nblk_tt, 1, 1.f);
+                    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, stream>>>(grad.p, tt.p, opd2.p,
+                                                                               wfs.p, nwfs, nxp, nyp, ngrad, 1,
+                                                                               1.f);
                     MB_CHECK_LAUNCH();
                     break;
                 case 3:
                     k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, stream>>>(
                         opd2.p, p.p, Ap.p, pap_part.p, gi, lay.p, tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
-                        nxtot, 1, 1.f, maxrows, maxnx, maxent);
+                        nxtot, 1, 1.f, maxrows, maxnx, maxent, scal(), 0);
                     MB_CHECK_LAUNCH();
                     break;
                 case 4:
                     // alpha reads the current scalars; the vectors are scratch here
-                    k_cg_update_xr<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(z.p, rhs.p, p.p, Ap.p, pap_part.p,
-                                                                             rr_part.p, sc.p, nsc, 0, nxtot,
-                                                                             ntiles);
+                    // the vectors are scratch here (x, r -> z, rhs)
+                    k_cg_update_xr<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(z.p, rhs.p, p.p, Ap.p, rr_part.p,
+                                                                             nxtot, scal(), 0, maxit, 0);
                     MB_CHECK_LAUNCH();
                     break;
                 case 5:
-                    k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(rhs.p, z.p, rz_part.p, sc.p, nsc,
-                                                                            maxit + 1, nxtot, nblk_x, 0);
+                    k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(rhs.p, z.p, nxtot, scal(), 0);
                     MB_CHECK_LAUNCH();
                     break;
                 case 6:
@@ -885,7 +898,7 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                     break;
                 case 10:
                     k_fd_unpack<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(spec2.p, r.p, z.p, rz_part.p, lay.p,
-                                                                          fd_soff.p, nps, nxtot);
+                                                                          fd_soff.p, nps, nxtot, CgScal{}, 0, 0);
                     MB_CHECK_LAUNCH();
                     break;
             }

@@ -79,6 +79,39 @@ __device__ __forceinline__ double warp_sum_partials(const double *part, int n) {
     return __shfl_sync(0xffffffffu, v, 0);
 }
 
+// Per-CG scalar state, per instance.  sc holds r.z of every iteration
+// (0..iters), b.b at iters+1 and the final residual at iters+2; ab the alpha
+// and beta of the current iteration; cnt the arrival counters of the
+// last-block reductions (zero between kernels).
+struct CgScal {
+    double *sc;
+    int nsc;
+    float *ab;       // [nb][2]
+    unsigned *cnt;   // [nb]
+    float *res;      // [nb]
+};
+
+// Every block calls this after writing its partial; it returns true in the
+// block that arrived last.  That block alone then adds the partials in a
+// fixed order (deterministic) and resets the counter.
+__device__ __forceinline__ bool last_block(unsigned *cnt, unsigned nblocks) {
+    __shared__ bool s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(cnt, 1u) == nblocks - 1);
+    __syncthreads();
+    return s_last;
+}
+
+// Sum n partials (written by other blocks of this kernel) with one warp,
+// bypassing L1; the result is valid in every lane.
+__device__ __forceinline__ double warp_sum_fresh(const double *part, int n) {
+    double v = 0;
+    for (int i = threadIdx.x & 31; i < n; i += 32) v += __ldcg(part + i);
+    v = warp_sum(v);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
 // ---------------------------------------------------------------------------
 // Hx: opd[b][w][p] = sum_l bilinear(x_l) at the ray of pupil point p.
 // grid: (ceil(np/256), nwfs, nb)
@@ -122,7 +155,7 @@ __global__ void k_hx(const float *__restrict__ x, float *__restrict__ opd,
 __global__ void k_gp(const float *__restrict__ opd, const float *__restrict__ gin,
                      float *__restrict__ grad, double *__restrict__ tt_part,
                      const WfsDev *__restrict__ wfs, int nwfs, int nxp, int np, long ngrad,
-                     int do_tt) {
+                     int do_tt, float *__restrict__ tt_out, unsigned *__restrict__ cnt) {
     __shared__ double sh[32];
     const int w = blockIdx.y, b = blockIdx.z;
     const WfsDev W = wfs[w];
@@ -159,10 +192,24 @@ __global__ void k_gp(const float *__restrict__ opd, const float *__restrict__ gi
         }
         tx = block_sum(tx, sh);
         ty = block_sum(ty, sh);
+        double *base = tt_part + ((size_t)b * nwfs + w) * gridDim.x * 2;
         if (threadIdx.x == 0) {
-            double *o = tt_part + (((size_t)b * nwfs + w) * gridDim.x + blockIdx.x) * 2;
-            o[0] = tx;
-            o[1] = ty;
+            base[blockIdx.x * 2] = tx;
+            base[blockIdx.x * 2 + 1] = ty;
+        }
+        if (last_block(cnt + (size_t)b * nwfs + w, gridDim.x) && threadIdx.x < 32) {
+            double t0 = 0, t1 = 0;
+            for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) {
+                t0 += __ldcg(base + 2 * i);
+                t1 += __ldcg(base + 2 * i + 1);
+            }
+            t0 = warp_sum(t0);
+            t1 = warp_sum(t1);
+            if (threadIdx.x == 0) {
+                tt_out[((size_t)b * nwfs + w) * 2] = (float)(-t0);
+                tt_out[((size_t)b * nwfs + w) * 2 + 1] = (float)(-t1);
+                cnt[(size_t)b * nwfs + w] = 0;
+            }
         }
     }
 }
@@ -172,37 +219,20 @@ __global__ void k_gp(const float *__restrict__ opd, const float *__restrict__ gi
 // (pos+1)^2 subapertures whose stencil covers it.
 // grid: (ceil(np/256), nwfs, nb)
 // ---------------------------------------------------------------------------
-__global__ void k_gpt(const float *__restrict__ grad, const double *__restrict__ tt_part,
+__global__ void k_gpt(const float *__restrict__ grad, const float *__restrict__ tt,
                       float *__restrict__ opd2, const WfsDev *__restrict__ wfs, int nwfs,
-                      int nxp, int nyp, long ngrad, int nblk_tt, int do_tt, float alpha) {
-    __shared__ float s_tt[2];
+                      int nxp, int nyp, long ngrad, int do_tt, float alpha) {
     const int w = blockIdx.y, b = blockIdx.z;
     const WfsDev W = wfs[w];
     const bool use_tt = do_tt && W.has_ptt;
-    if (threadIdx.x < 32) {
-        double t0 = 0, t1 = 0;
-        if (use_tt) {
-            const double *tp = tt_part + ((size_t)b * nwfs + w) * nblk_tt * 2;
-            for (int i = threadIdx.x; i < nblk_tt; i += 32) {
-                t0 += tp[2 * i];
-                t1 += tp[2 * i + 1];
-            }
-            t0 = warp_sum(t0);
-            t1 = warp_sum(t1);
-        }
-        if (threadIdx.x == 0) {
-            s_tt[0] = (float)(-t0);
-            s_tt[1] = (float)(-t1);
-        }
-    }
-    __syncthreads();
     const int np = nxp * nyp;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np) return;
     const int px = p % nxp, py = p / nxp;
     const int n1 = W.pos + 1;
     const float *g = grad + (size_t)b * ngrad + W.goff;
-    const float ttx = s_tt[0], tty = s_tt[1];
+    const float ttx = use_tt ? tt[((size_t)b * nwfs + w) * 2] : 0.f;
+    const float tty = use_tt ? tt[((size_t)b * nwfs + w) * 2 + 1] : 0.f;
     float acc = 0.f;
     for (int dy = 0; dy < n1; dy++) {
         const int cy = py - dy;
@@ -235,6 +265,19 @@ struct GatherIndex {
     const GatherW *ent;    // concatenated entries
 };
 
+// alpha_k = (r.z)_k / (p.Ap), reduced by the last block of the p.Ap producer.
+__device__ __forceinline__ void cg_alpha_last(const double *part_b, const CgScal &S, int b, int k) {
+    if (last_block(S.cnt + b, gridDim.x) && threadIdx.x < 32) {
+        const double pap = warp_sum_fresh(part_b, gridDim.x);
+        if (threadIdx.x == 0) {
+            double a = S.sc[(size_t)b * S.nsc + k] / pap;
+            if (!isfinite(a)) a = 0;  // pcg.c:80-83, pcg.cu:27-30
+            S.ab[2 * b] = (float)a;
+            S.cnt[b] = 0;
+        }
+    }
+}
+
 struct LowRank {
     const float *nw;        // [n][nnw] column-major (nw[k*n + j]); null: no term
     const double *part;     // NW' x partials [b][k][nblk]
@@ -244,7 +287,7 @@ struct LowRank {
 __global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ xin,
                       float *__restrict__ out, double *__restrict__ dot_part, GatherIndex gi,
                       const LayerDev *__restrict__ lay, int nps, int nwfs, int nxp, int nyp,
-                      long nxtot, int do_l2, float alpha, LowRank lr) {
+                      long nxtot, int do_l2, float alpha, LowRank lr, CgScal S, int k) {
     __shared__ double sh[32];
     __shared__ float s_t[8];
     const int b = blockIdx.y;
@@ -313,6 +356,7 @@ __global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ 
     if (dot_part) {
         dotv = block_sum(dotv, sh);
         if (threadIdx.x == 0) dot_part[(size_t)b * gridDim.x + blockIdx.x] = dotv;
+        cg_alpha_last(dot_part + (size_t)b * gridDim.x, S, b, k);
     }
 }
 
@@ -338,7 +382,7 @@ k_hxt_tiled(const float *__restrict__ opd2, const float *__restrict__ xin, float
             double *__restrict__ dot_part, GatherIndex gi, const LayerDev *__restrict__ lay,
             const TileDesc *__restrict__ tiles, const int2 *__restrict__ rowrange, int nps, int nwfs,
             int nxp, int nyp, long nxtot, int do_l2, float alpha, int maxrows, int maxnx,
-            int maxent) {
+            int maxent, CgScal S, int kit) {
     extern __shared__ float smem[];
     __shared__ double sh[32];
     const int tid = blockIdx.x, b = blockIdx.y;
@@ -422,6 +466,7 @@ k_hxt_tiled(const float *__restrict__ opd2, const float *__restrict__ xin, float
     if (dot_part) {
         dotv = block_sum(dotv, sh);
         if (threadIdx.x == 0) dot_part[(size_t)b * gridDim.x + blockIdx.x] = dotv;
+        cg_alpha_last(dot_part + (size_t)b * gridDim.x, S, b, kit);
     }
 }
 
@@ -468,9 +513,10 @@ __global__ void k_lowrank_dot(const float *__restrict__ x, const float *__restri
 // layout: [0..maxit] r.z per iteration, [maxit+1] b.b, [maxit+2] residual
 // ---------------------------------------------------------------------------
 
-// r = b - Ax, and b.b partials.  grid: (nblk_x, nb)
+// r = b - Ax; b.b is reduced by the last block into sc[iters+1].  grid: (nblk, nb)
 __global__ void k_cg_init_r(const float *__restrict__ bvec, const float *__restrict__ Ax,
-                            float *__restrict__ r, double *__restrict__ bb_part, long n) {
+                            float *__restrict__ r, double *__restrict__ bb_part, long n, CgScal S,
+                            int iters) {
     __shared__ double sh[32];
     const int b = blockIdx.y;
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -482,72 +528,39 @@ __global__ void k_cg_init_r(const float *__restrict__ bvec, const float *__restr
         v = (double)bv * bv;
     }
     v = block_sum(v, sh);
-    if (threadIdx.x == 0) bb_part[(size_t)b * gridDim.x + blockIdx.x] = v;
-}
-
-// alpha = rz[k] / sum(pAp partials); x += alpha p; r -= alpha Ap; r.r partials.
-// When z aliases r (no preconditioner) the r.r partials double as r.z.
-__global__ void k_cg_update_xr(float *__restrict__ x, float *__restrict__ r,
-                               const float *__restrict__ p, const float *__restrict__ Ap,
-                               const double *__restrict__ pap_part, double *__restrict__ rr_part,
-                               double *__restrict__ sc, int nsc, int k, long n, int nblk_pap) {
-    __shared__ double sh[32];
-    __shared__ float s_alpha;
-    const int b = blockIdx.y;
-    if (threadIdx.x < 32) {
-        const double pap = warp_sum_partials(pap_part + (size_t)b * nblk_pap, nblk_pap);
+    double *pb = bb_part + (size_t)b * gridDim.x;
+    if (threadIdx.x == 0) pb[blockIdx.x] = v;
+    if (last_block(S.cnt + b, gridDim.x) && threadIdx.x < 32) {
+        const double bb = warp_sum_fresh(pb, gridDim.x);
         if (threadIdx.x == 0) {
-            double a = sc[(size_t)b * nsc + k] / pap;
-            if (!isfinite(a)) a = 0;  // pcg.c:80-83, pcg.cu:27-30
-            s_alpha = (float)a;
+            S.sc[(size_t)b * S.nsc + iters + 1] = bb;
+            S.cnt[b] = 0;
         }
     }
-    __syncthreads();
-    const float a = s_alpha;
-    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    double v = 0;
-    if (j < n) {
-        const size_t o = (size_t)b * n + j;
-        x[o] += a * p[o];
-        const float rv = r[o] - a * Ap[o];
-        r[o] = rv;
-        v = (double)rv * rv;
-    }
-    v = block_sum(v, sh);
-    if (threadIdx.x == 0) rr_part[(size_t)b * gridDim.x + blockIdx.x] = v;
 }
 
-// beta = sum(rz partials) / rz[k]; p = z + beta p; rz[k+1] stored by block 0.
-// init != 0: p = z and rz[0] = sum (start or restart of the iteration).
-__global__ void k_cg_update_p(float *__restrict__ p, const float *__restrict__ z,
-                              const double *__restrict__ rz_part, double *__restrict__ sc, int nsc,
-                              int k, long n, int nblk, int init) {
-    __shared__ float s_beta;
-    const int b = blockIdx.y;
-    if (threadIdx.x < 32) {
-        const double rz = warp_sum_partials(rz_part + (size_t)b * nblk, nblk);
+// (r.z) reduction shared by the kernels that produce z: the last block
+// stores (r.z)_0 when init, otherwise beta = (r.z)_{k+1} / (r.z)_k.
+__device__ __forceinline__ void cg_rz_last(const double *part_b, const CgScal &S, int b, int k,
+                                           int init) {
+    if (last_block(S.cnt + b, gridDim.x) && threadIdx.x < 32) {
+        const double rz = warp_sum_fresh(part_b, gridDim.x);
         if (threadIdx.x == 0) {
-            double be = 0;
             if (init) {
-                if (blockIdx.x == 0) sc[(size_t)b * nsc + 0] = rz;
+                S.sc[(size_t)b * S.nsc] = rz;
             } else {
-                be = rz / sc[(size_t)b * nsc + k];
+                double be = rz / S.sc[(size_t)b * S.nsc + k];
                 if (!isfinite(be)) be = 0;
-                if (blockIdx.x == 0) sc[(size_t)b * nsc + k + 1] = rz;
+                S.ab[2 * b + 1] = (float)be;
+                S.sc[(size_t)b * S.nsc + k + 1] = rz;
             }
-            s_beta = (float)be;
+            S.cnt[b] = 0;
         }
-    }
-    __syncthreads();
-    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < n) {
-        const size_t o = (size_t)b * n + j;
-        p[o] = init ? z[o] : z[o] + s_beta * p[o];
     }
 }
 
-// v.v partials.  grid: (nblk_x, nb)
-__global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ part, long n) {
+// v.v partials and (when z aliases r) the start-of-CG r.z.  grid: (nblk, nb)
+__global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ part, long n, CgScal S) {
     __shared__ double sh[32];
     const int b = blockIdx.y;
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -558,19 +571,55 @@ __global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ par
     }
     t = block_sum(t, sh);
     if (threadIdx.x == 0) part[(size_t)b * gridDim.x + blockIdx.x] = t;
+    cg_rz_last(part + (size_t)b * gridDim.x, S, b, 0, 1);
 }
 
-// residual = sqrt(r.r / b.b) per instance.  grid: (1, nb), 32 threads
-__global__ void k_cg_residual(const double *__restrict__ rr_part, const double *__restrict__ bb_part,
-                              double *__restrict__ sc, float *__restrict__ res, int nsc, int resslot,
-                              int nblk) {
+// x += alpha p; r -= alpha Ap; r.r partials.  The last block either finishes
+// the solve (residual sqrt(r.r/b.b) at the final iteration) or, when z aliases
+// r (no preconditioner), produces beta.
+__global__ void k_cg_update_xr(float *__restrict__ x, float *__restrict__ r,
+                               const float *__restrict__ p, const float *__restrict__ Ap,
+                               double *__restrict__ rr_part, long n, CgScal S, int k, int iters,
+                               int z_is_r) {
+    __shared__ double sh[32];
     const int b = blockIdx.y;
-    const double rr = warp_sum_partials(rr_part + (size_t)b * nblk, nblk);
-    const double bb = warp_sum_partials(bb_part + (size_t)b * nblk, nblk);
-    if (threadIdx.x == 0) {
-        const double v = sqrt(rr / bb);
-        sc[(size_t)b * nsc + resslot] = v;
-        res[b] = (float)v;
+    const float a = S.ab[2 * b];
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0;
+    if (j < n) {
+        const size_t o = (size_t)b * n + j;
+        x[o] += a * p[o];
+        const float rv = r[o] - a * Ap[o];
+        r[o] = rv;
+        v = (double)rv * rv;
+    }
+    v = block_sum(v, sh);
+    double *pb = rr_part + (size_t)b * gridDim.x;
+    if (threadIdx.x == 0) pb[blockIdx.x] = v;
+    if (k + 1 == iters) {
+        if (last_block(S.cnt + b, gridDim.x) && threadIdx.x < 32) {
+            const double rr = warp_sum_fresh(pb, gridDim.x);
+            if (threadIdx.x == 0) {
+                const double res = sqrt(rr / S.sc[(size_t)b * S.nsc + iters + 1]);
+                S.sc[(size_t)b * S.nsc + iters + 2] = res;
+                S.res[b] = (float)res;
+                S.cnt[b] = 0;
+            }
+        }
+    } else if (z_is_r) {
+        cg_rz_last(pb, S, b, k, 0);
+    }
+}
+
+// p = z + beta p (init: p = z).  grid: (nblk, nb)
+__global__ void k_cg_update_p(float *__restrict__ p, const float *__restrict__ z, long n, CgScal S,
+                              int init) {
+    const int b = blockIdx.y;
+    const float be = init ? 0.f : S.ab[2 * b + 1];
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) {
+        const size_t o = (size_t)b * n + j;
+        p[o] = init ? z[o] : z[o] + be * p[o];
     }
 }
 
@@ -623,7 +672,7 @@ __global__ void k_fd_mul(const cufftComplex *__restrict__ X, cufftComplex *__res
 __global__ void k_fd_unpack(const cufftComplex *__restrict__ S, const float *__restrict__ r,
                             float *__restrict__ z, double *__restrict__ rz_part,
                             const LayerDev *__restrict__ lay, const int *__restrict__ soff, int nps,
-                            long nxtot) {
+                            long nxtot, CgScal SC, int k, int init) {
     __shared__ double sh[32];
     const int b = blockIdx.y;
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -640,6 +689,7 @@ __global__ void k_fd_unpack(const cufftComplex *__restrict__ S, const float *__r
     }
     v = block_sum(v, sh);
     if (threadIdx.x == 0) rz_part[(size_t)b * gridDim.x + blockIdx.x] = v;
+    if (SC.sc) cg_rz_last(rz_part + (size_t)b * gridDim.x, SC, b, k, init);
 }
 
 // float <-> double staging helpers for the host-facing API
