@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mvm-batch", type=int, default=1)
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--no-serve", action="store_true")
     return ap.parse_args()
 
 
@@ -243,6 +245,63 @@ def mvm_rates(lib, native, nact: int, ngrad: int, batch: int, stream):
     return res
 
 
+SERVE_MIX = (("scao_8m", 26), ("ltao_8m", 26), ("mcao_30m", 12))
+
+
+def served_mix(seconds: float, mcao_frames=None):
+    """The served mix: 64 systems (26 8 m SCAO, 26 8 m LTAO, 12 30 m MCAO), each
+    sending Poisson requests at a rate drawn from U[500, 1000] Hz, all admitted,
+    warm state resident, newest frame wins when a system falls behind."""
+    import numpy as np
+    import torch
+    from maos_b200 import config, fit_setup, geometry, serve, turbulence
+    rng = np.random.default_rng(17)
+    types, frames = [], []
+    for name, n in SERVE_MIX:
+        sysm = geometry.build_tomo(config.PRESETS[name]())
+        fs = fit_setup.build_fit(sysm)
+        types.append(serve.SystemType(name, sysm, fs, capacity=n))
+        if name == "mcao_30m" and mcao_frames is not None:
+            fr = np.asarray(mcao_frames, dtype=np.float32)
+        else:
+            fr = turbulence.gradient_frames(sysm, seed=5, nframe=4).astype(np.float32)
+        frames.append(fr)
+    systems = []
+    for t, (name, n) in enumerate(SERVE_MIX):
+        for _ in range(n):
+            systems.append((t, float(rng.uniform(500.0, 1000.0)), frames[t]))
+    budget = sum(serve.slot_footprint_bytes(t) * t.capacity for t in types)
+    srv = serve.Server(types, budget, drop_stale=True)
+    # warm the graphs of every pool (all slots), then reset the state
+    for p in srv.pools:
+        m = np.ones(p.cap, np.int32)
+        for _ in range(3):
+            p.R.serve_step(m, p.g_host.data_ptr(), p.a_host.data_ptr(), p.stream.cuda_stream)
+    torch.cuda.synchronize()
+    srv, done, wall = serve.run_served(types, systems, duration=seconds, hbm_budget=budget, seed=3,
+                                       server=srv)
+    offered = [0] * len(types)
+    for r in done + srv.dropped:
+        offered[systems[r.system][0]] += 1
+    out = {"mix": " + ".join(f"{n} {name}" for name, n in SERVE_MIX),
+           "rate_hz": "U[500,1000] Poisson per system", "seconds": seconds,
+           "policy": "one masked batch per pool in flight, newest frame wins",
+           "hbm_budget_bytes": int(budget),
+           "served_steps_per_s": len(done) / seconds, "offered_per_s": (len(done) + len(srv.dropped)) / seconds,
+           "dropped_frac": len(srv.dropped) / max(1, len(done) + len(srv.dropped)),
+           "latency_ms": serve.latency_stats(done), "per_type": {}}
+    for t, (name, n) in enumerate(SERVE_MIX):
+        d = [r for r in done if systems[r.system][0] == t]
+        nd = sum(1 for r in srv.dropped if systems[r.system][0] == t)
+        out["per_type"][name] = {"systems": n, "served_per_s": len(d) / seconds,
+                                 "dropped_frac": nd / max(1, len(d) + nd),
+                                 "batches": srv.pools[t].batches,
+                                 "mean_batch": srv.pools[t].slot_steps / max(1, srv.pools[t].batches),
+                                 "latency_ms": serve.latency_stats(d)}
+    srv.close()
+    return out
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -353,6 +412,10 @@ def run_gpu(args):
 
     mvm_line = mvm_rates(lib, native, int(fit.nact), int(sysm.ngrad), args.mvm_batch, stream)
 
+    served = None
+    if world == 1 and not args.no_serve and args.serve_seconds > 0:
+        served = served_mix(args.serve_seconds, mcao_frames=fr[0])
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import refbridge
@@ -378,6 +441,7 @@ def run_gpu(args):
                         "h2d_bytes_per_step": int(B * sysm.ngrad * 4),
                         "d2h_bytes_per_step": int(B * fit.nact * 4 + 2 * B * 4)},
                 "mvm": mvm_line,
+                "served": served,
                 "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)

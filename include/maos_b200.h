@@ -161,6 +161,30 @@ const float *mb_tomo_solution(mb_recon *r);
 /* Copy the last residuals [nbatch] (synchronises the stream). */
 int mb_tomo_residual(mb_recon *r, float *cgres);
 
+/* ---- Serving: instances as slots ----
+ * No counterpart in the reference (one curecon_t serves one simulation).
+ * Each of the nbatch instances is a slot holding one AO system's warm-start
+ * state.  A masked step advances only the slots whose flag is non-zero;
+ * every other slot's state is left untouched and no slot's result depends on
+ * which other slots ran.  All four calls enqueue on `stream` and return. */
+/* Zero one slot's warm-start state (layer OPD and DM commands). */
+int mb_recon_reset_slot(mb_recon *r, int slot, void *stream);
+/* Copy one slot's FP32 gradients [ngrad] (host, pinned for asynchrony, or
+ * device) into the reconstructor. */
+int mb_slot_upload(mb_recon *r, int slot, const float *grad, void *stream);
+/* Copy one slot's FP32 result out: DM commands [nact] with a fit, else the
+ * layer OPD [nxtot]. */
+int mb_slot_download(mb_recon *r, int slot, float *out, void *stream);
+/* One step (tomography, then the fit if set up) of the slots with
+ * active[slot] != 0; active is a host array [nbatch], read before return. */
+int mb_recon_step_slots(mb_recon *r, const int *active, void *stream);
+/* The three in one call: gradients of the active slots from grad
+ * [nbatch][ngrad], one masked step, their results into out [nbatch][nact]
+ * (or [nbatch][nxtot] without a fit); rows of inactive slots are neither
+ * read nor written.  Pinned host or device buffers; one copy per run of
+ * consecutive active slots each way. */
+int mb_recon_serve_step(mb_recon *r, const int *active, const float *grad, float *out, void *stream);
+
 /* Sizes of the bound geometry. */
 long mb_ngrad(const mb_recon *r);
 long mb_nxtot(const mb_recon *r);

@@ -106,6 +106,17 @@ struct Recon {
     DevBuf<unsigned> cnt, cnt_tt;
     CgScal scal() const { return CgScal{sc.p, nsc, ab.p, cnt.p, res.p}; }
 
+    // Serving: per-instance participation flags read by every kernel of the
+    // step (1: run, 0: leave the instance untouched).  All ones except while a
+    // masked step is queued; the host copy is pinned so the upload is
+    // asynchronous, and `mask_ev` guards its reuse.
+    DevBuf<int> active;
+    int *mask_host = nullptr;
+    cudaEvent_t mask_ev = nullptr;
+    bool mask_all = true;
+    const int *act() const { return active.p; }
+    void set_mask(const int *m, cudaStream_t s);
+
     // DM fit
     int has_fit = 0, nfit = 0, ndm = 0, nfx = 0, nfy = 0, nf = 0, nnw = 0, fit_maxit = 0;
     int nblk_a = 0, nblk_f = 0, fnsc = 0;
@@ -127,6 +138,8 @@ struct Recon {
     long graph_kernels = 0, graph_fit_kernels = 0, graph_step_kernels = 0;
 
     ~Recon() {
+        if (mask_ev) cudaEventDestroy(mask_ev);
+        if (mask_host) cudaFreeHost(mask_host);
         if (graph) cudaGraphExecDestroy(graph);
         if (graph_fit) cudaGraphExecDestroy(graph_fit);
         if (graph_step) cudaGraphExecDestroy(graph_step);
@@ -465,6 +478,8 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
     fd_soff.upload(soff);
     spec.alloc(acc);
     spec2.alloc(acc);
+    spec.zero_async(stream);  // spectra of instances that never ran stay finite
+    spec2.zero_async(stream);
     // one batched 2-D plan per run of consecutive equal-size layers
     for (auto h : plans) cufftDestroy(h);
     plans.clear();
@@ -548,6 +563,12 @@ void Recon::build(const mb_recon_desc *d) {
     tt.alloc((size_t)nb * nwfs * 2);
     cnt.alloc(nb);
     cnt_tt.alloc((size_t)nb * nwfs);
+    active.alloc(nb);
+    MB_CUDA_TRY(cudaHostAlloc(&mask_host, (size_t)nb * sizeof(int), cudaHostAllocDefault));
+    MB_CUDA_TRY(cudaEventCreateWithFlags(&mask_ev, cudaEventDisableTiming));
+    for (int b = 0; b < nb; b++) mask_host[b] = 1;
+    MB_CUDA_TRY(cudaMemcpyAsync(active.p, mask_host, (size_t)nb * sizeof(int), cudaMemcpyHostToDevice, stream));
+    MB_CUDA_TRY(cudaEventRecord(mask_ev, stream));
     if (precond) build_fdpcg(d->fdpcg);
     if (d->fit) build_fit(d->fit);
     x.zero_async(stream);
@@ -567,22 +588,22 @@ void Recon::build(const mb_recon_desc *d) {
 // ---------------------------------------------------------------------------
 void Recon::op_hx(const float *xin, cudaStream_t s) {
     k_hx<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(xin, opd.p, hx.fwd.p, lay.p, nps, nwfs,
-                                                         nxp, nyp, nxtot, nullptr, nullptr);
+                                                         nxp, nyp, nxtot, nullptr, nullptr, act());
     MB_CHECK_LAUNCH();
 }
 
 void Recon::op_rhs(const float *g, float *out, cudaStream_t s) {
     // TomoR: x = Hx^T GP^T NEA^-1 (I - TT PTT) g   (recon_utils.c:397, tomo.cu:607)
     k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, s>>>(nullptr, g, grad.p, tt_part.p, wfs.p, nwfs,
-                                                      nxp, np, ngrad, 1, tt.p, cnt_tt.p);
+                                                      nxp, np, ngrad, 1, tt.p, cnt_tt.p, act());
     MB_CHECK_LAUNCH();
     k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt.p, opd2.p, wfs.p, nwfs, nxp, nyp,
-                                                          ngrad, 1, 1.f);
+                                                          ngrad, 1, 1.f, act());
     MB_CHECK_LAUNCH();
     k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, s>>>(opd2.p, nullptr, out, nullptr, hx.gi(), lay.p,
                                                             tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
                                                             nxtot, 0, 1.f, maxrows, maxnx, maxent,
-                                                            scal(), 0);
+                                                            scal(), 0, act());
     MB_CHECK_LAUNCH();
 }
 
@@ -591,22 +612,22 @@ void Recon::op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t 
     op_hx(xin, s);
     const int do_tt = split ? 0 : 1;
     k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, s>>>(opd.p, nullptr, grad.p, tt_part.p, wfs.p,
-                                                      nwfs, nxp, np, ngrad, do_tt, tt.p, cnt_tt.p);
+                                                      nwfs, nxp, np, ngrad, do_tt, tt.p, cnt_tt.p, act());
     MB_CHECK_LAUNCH();
     k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt.p, opd2.p, wfs.p, nwfs, nxp, nyp,
-                                                          ngrad, do_tt, 1.f);
+                                                          ngrad, do_tt, 1.f, act());
     MB_CHECK_LAUNCH();
     k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, s>>>(opd2.p, xin, out, dot_part, hx.gi(), lay.p,
                                                             tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
                                                             nxtot, 1, 1.f, maxrows, maxnx, maxent,
-                                                            scal(), k);
+                                                            scal(), k, act());
     MB_CHECK_LAUNCH();
 }
 
 void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s, int k, int init,
                      bool in_cg) {
     // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT
-    k_fd_pack<<<dim3(nblk_x, nb), kThreads, 0, s>>>(rin, spec.p, lay.p, fd_soff.p, nps, nxtot);
+    k_fd_pack<<<dim3(nblk_x, nb), kThreads, 0, s>>>(rin, spec.p, lay.p, fd_soff.p, nps, nxtot, act());
     MB_CHECK_LAUNCH();
     for (size_t i = 0; i < plans.size(); i++) {
         MB_CUFFT_TRY(cufftSetStream(plans[i], s));
@@ -614,7 +635,7 @@ void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s,
         count_launches(1);
     }
     k_fd_mul<<<dim3(nblocks((long)fd_nb * fd_bs), nb), kThreads, 0, s>>>(spec.p, spec2.p, fd_M.p,
-                                                                        fd_idx.p, fd_nb, fd_bs);
+                                                                        fd_idx.p, fd_nb, fd_bs, act());
     MB_CHECK_LAUNCH();
     for (size_t i = 0; i < plans.size(); i++) {
         MB_CUFFT_TRY(cufftExecC2C(plans[i], spec2.p + plan_off[i], spec2.p + plan_off[i], CUFFT_INVERSE));
@@ -622,7 +643,7 @@ void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s,
     }
     CgScal S = in_cg ? scal() : CgScal{};
     k_fd_unpack<<<dim3(nblk_x, nb), kThreads, 0, s>>>(spec2.p, rin, zout, rzp, lay.p, fd_soff.p, nps,
-                                                     nxtot, S, k, init);
+                                                     nxtot, S, k, init, act());
     MB_CHECK_LAUNCH();
 }
 
@@ -633,26 +654,26 @@ void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulF
                        const MmulFn &Mmul, cudaStream_t s) {
     // r = b - A x ; b.b
     Amul(B.x, B.Ap, nullptr, 0);
-    k_cg_init_r<<<dim3(nblk, nb), kThreads, 0, s>>>(B.rhs, B.Ap, B.r, B.bb, n, B.S, iters);
+    k_cg_init_r<<<dim3(nblk, nb), kThreads, 0, s>>>(B.rhs, B.Ap, B.r, B.bb, n, B.S, iters, act());
     MB_CHECK_LAUNCH();
     float *zp = B.r;
     if (Mmul) {
         Mmul(B.r, B.z, B.rz, 0, 1);
         zp = B.z;
     } else {
-        k_dot_self<<<dim3(nblk, nb), kThreads, 0, s>>>(B.r, B.rz, n, B.S);  // z aliases r
+        k_dot_self<<<dim3(nblk, nb), kThreads, 0, s>>>(B.r, B.rz, n, B.S, act());  // z aliases r
         MB_CHECK_LAUNCH();
     }
-    k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, n, B.S, 1);
+    k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, n, B.S, 1, act());
     MB_CHECK_LAUNCH();
     for (int k = 0; k < iters; k++) {
         Amul(B.p, B.Ap, B.pap, k);  // its last block leaves alpha_k
         k_cg_update_xr<<<dim3(nblk, nb), kThreads, 0, s>>>(B.x, B.r, B.p, B.Ap, B.rr, n, B.S, k, iters,
-                                                          Mmul ? 0 : 1);
+                                                          Mmul ? 0 : 1, act());
         MB_CHECK_LAUNCH();
         if (k + 1 == iters) break;
         if (Mmul) Mmul(B.r, B.z, B.rz, k, 0);  // its last block leaves beta_k
-        k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, n, B.S, 0);
+        k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, n, B.S, 0, act());
         MB_CHECK_LAUNCH();
     }
 }
@@ -673,13 +694,13 @@ void Recon::enqueue_solve(cudaStream_t s) {
 // FitR: sum_f wt_f HA_f^T (W0 - W1 W1^T) Hxp_f x   (recon_utils.c:483, fit.cu:190)
 void Recon::op_fitR(const float *xin, float *out, cudaStream_t s) {
     k_hx<<<dim3(nblk_f, nfit, nb), kThreads, 0, s>>>(xin, opdf.p, hxp.fwd.p, lay.p, nps, nfit, nfx, nfy,
-                                                    nxtot, w1v.p, w1_part.p);
+                                                    nxtot, w1v.p, w1_part.p, act());
     MB_CHECK_LAUNCH();
     k_fit_w<<<dim3(nblk_f, nfit, nb), kThreads, 0, s>>>(opdf.p, opdw.p, w0_rp.p, w0_ci.p, w0_v.p, w1v.p,
-                                                       fwt.p, w1_part.p, nblk_f, nf, nfit);
+                                                       fwt.p, w1_part.p, nblk_f, nf, nfit, act());
     MB_CHECK_LAUNCH();
     k_hxt<<<dim3(nblk_a, nb), kThreads, 0, s>>>(opdw.p, nullptr, out, nullptr, ha.gi(), dmlay.p, ndm,
-                                               nfit, nfx, nfy, nact, 0, 1.f, LowRank{}, fscal(), 0);
+                                               nfit, nfx, nfy, nact, 0, 1.f, LowRank{}, fscal(), 0, act());
     MB_CHECK_LAUNCH();
 }
 
@@ -687,18 +708,18 @@ void Recon::op_fitR(const float *xin, float *out, cudaStream_t s) {
 void Recon::op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t s, int k) {
     LowRank lr{};
     if (nnw) {
-        k_lowrank_dot<<<dim3(nblk_a, nb), kThreads, 0, s>>>(ain, nwv.p, nw_part.p, nnw, nact);
+        k_lowrank_dot<<<dim3(nblk_a, nb), kThreads, 0, s>>>(ain, nwv.p, nw_part.p, nnw, nact, act());
         MB_CHECK_LAUNCH();
         lr = LowRank{nwv.p, nw_part.p, nnw, nblk_a};
     }
     k_hx<<<dim3(nblk_f, nfit, nb), kThreads, 0, s>>>(ain, opdf.p, ha.fwd.p, dmlay.p, ndm, nfit, nfx, nfy,
-                                                    nact, w1v.p, w1_part.p);
+                                                    nact, w1v.p, w1_part.p, act());
     MB_CHECK_LAUNCH();
     k_fit_w<<<dim3(nblk_f, nfit, nb), kThreads, 0, s>>>(opdf.p, opdw.p, w0_rp.p, w0_ci.p, w0_v.p, w1v.p,
-                                                       fwt.p, w1_part.p, nblk_f, nf, nfit);
+                                                       fwt.p, w1_part.p, nblk_f, nf, nfit, act());
     MB_CHECK_LAUNCH();
     k_hxt<<<dim3(nblk_a, nb), kThreads, 0, s>>>(opdw.p, ain, out, dot_part, ha.gi(), dmlay.p, ndm, nfit,
-                                               nfx, nfy, nact, 0, 1.f, lr, fscal(), k);
+                                               nfx, nfy, nact, 0, 1.f, lr, fscal(), k, act());
     MB_CHECK_LAUNCH();
 }
 
@@ -807,6 +828,7 @@ void Recon::build_fit(const mb_fit_desc *f) {
 // Time each iteration stage alone and report its algorithmic traffic.
 void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     const int ns = mb_num_stages();
+    set_mask(nullptr, stream);
     cudaEvent_t e0, e1;
     MB_CUDA_TRY(cudaEventCreate(&e0));
     MB_CUDA_TRY(cudaEventCreate(&e1));
@@ -852,34 +874,34 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                 case 1:
                     k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, stream>>>(opd.p, nullptr, grad.p, tt_part.p,
                                                                           wfs.p, nwfs, nxp, np, ngrad, 1, tt.p,
-                                                                          cnt_tt.p);
+                                                                          cnt_tt.p, act());
                     MB_CHECK_LAUNCH();
                     break;
                 case 2:
                     k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, stream>>>(grad.p, tt.p, opd2.p,
                                                                                wfs.p, nwfs, nxp, nyp, ngrad, 1,
-                                                                               1.f);
+                                                                               1.f, act());
                     MB_CHECK_LAUNCH();
                     break;
                 case 3:
                     k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, stream>>>(
                         opd2.p, p.p, Ap.p, pap_part.p, gi, lay.p, tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
-                        nxtot, 1, 1.f, maxrows, maxnx, maxent, scal(), 0);
+                        nxtot, 1, 1.f, maxrows, maxnx, maxent, scal(), 0, act());
                     MB_CHECK_LAUNCH();
                     break;
                 case 4:
                     // alpha reads the current scalars; the vectors are scratch here
                     // the vectors are scratch here (x, r -> z, rhs)
                     k_cg_update_xr<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(z.p, rhs.p, p.p, Ap.p, rr_part.p,
-                                                                             nxtot, scal(), 0, maxit, 0);
+                                                                             nxtot, scal(), 0, maxit, 0, act());
                     MB_CHECK_LAUNCH();
                     break;
                 case 5:
-                    k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(rhs.p, z.p, nxtot, scal(), 0);
+                    k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(rhs.p, z.p, nxtot, scal(), 0, act());
                     MB_CHECK_LAUNCH();
                     break;
                 case 6:
-                    k_fd_pack<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(r.p, spec.p, lay.p, fd_soff.p, nps, nxtot);
+                    k_fd_pack<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(r.p, spec.p, lay.p, fd_soff.p, nps, nxtot, act());
                     MB_CHECK_LAUNCH();
                     break;
                 case 7:
@@ -893,12 +915,12 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                     break;
                 case 8:
                     k_fd_mul<<<dim3(nblocks((long)fd_nb * fd_bs), nb), kThreads, 0, stream>>>(
-                        spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nb, fd_bs);
+                        spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nb, fd_bs, act());
                     MB_CHECK_LAUNCH();
                     break;
                 case 10:
                     k_fd_unpack<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(spec2.p, r.p, z.p, rz_part.p, lay.p,
-                                                                          fd_soff.p, nps, nxtot, CgScal{}, 0, 0);
+                                                                          fd_soff.p, nps, nxtot, CgScal{}, 0, 0, act());
                     MB_CHECK_LAUNCH();
                     break;
             }
@@ -958,7 +980,18 @@ void Recon::capture_graph() {
     }
 }
 
+// Queue the upload of a participation mask (null: all instances) on `s`.
+void Recon::set_mask(const int *m, cudaStream_t s) {
+    if (!m && mask_all) return;
+    MB_CUDA_TRY(cudaEventSynchronize(mask_ev));  // the previous upload has left mask_host
+    for (int b = 0; b < nb; b++) mask_host[b] = m ? (m[b] != 0) : 1;
+    MB_CUDA_TRY(cudaMemcpyAsync(active.p, mask_host, (size_t)nb * sizeof(int), cudaMemcpyHostToDevice, s));
+    MB_CUDA_TRY(cudaEventRecord(mask_ev, s));
+    mask_all = (m == nullptr);
+}
+
 void Recon::run_graph(cudaStream_t s) {
+    set_mask(nullptr, s);
     MB_CUDA_TRY(cudaGraphLaunch(graph, s));
     count_launches(graph_kernels);
 }
@@ -1139,6 +1172,7 @@ int mb_fit(mb_recon *h, double *dmout, float *cgres) {
         mb::set_error("reconstructor was set up without a DM fit");
         return MB_ESTATE;
     }
+    R.set_mask(nullptr, R.stream);
     MB_CUDA_TRY(cudaGraphLaunch(R.graph_fit, R.stream));
     mb::count_launches(R.graph_fit_kernels);
     if (dmout) from_float_dev(dmout, R.fa.p, (size_t)R.nb * R.nact, R.stream);
@@ -1158,6 +1192,7 @@ int mb_recon_step_device(mb_recon *h, const float *d_grad, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     MB_CUDA_TRY(cudaMemcpyAsync(R.gin.p, d_grad, (size_t)R.nb * R.ngrad * sizeof(float),
                                 cudaMemcpyDeviceToDevice, s));
+    R.set_mask(nullptr, s);
     MB_CUDA_TRY(cudaGraphLaunch(R.graph_step, s));
     mb::count_launches(R.graph_step_kernels);
     MB_API_END
@@ -1167,6 +1202,7 @@ int mb_apply_fit_R(mb_recon *h, const double *xin, double *aout) {
     MB_API_BEGIN
     MB_REQUIRE(h && xin && aout && h->R.has_fit, "invalid arguments or no fit");
     mb::Recon &R = h->R;
+    R.set_mask(nullptr, R.stream);
     to_float_dev(R.z.p, xin, (size_t)R.nb * R.nxtot, R.stream);
     R.op_fitR(R.z.p, R.frhs.p, R.stream);
     from_float_dev(aout, R.frhs.p, (size_t)R.nb * R.nact, R.stream);
@@ -1177,6 +1213,7 @@ int mb_apply_fit_L(mb_recon *h, const double *ain, double *aout) {
     MB_API_BEGIN
     MB_REQUIRE(h && ain && aout && h->R.has_fit, "invalid arguments or no fit");
     mb::Recon &R = h->R;
+    R.set_mask(nullptr, R.stream);
     to_float_dev(R.fp.p, ain, (size_t)R.nb * R.nact, R.stream);
     R.op_fitL(R.fp.p, R.fAp.p, nullptr, R.stream);
     from_float_dev(aout, R.fAp.p, (size_t)R.nb * R.nact, R.stream);
@@ -1210,6 +1247,7 @@ int mb_apply_tomo_R(mb_recon *h, const double *grad, double *xout) {
     MB_API_BEGIN
     MB_REQUIRE(h && grad && xout, "invalid arguments");
     mb::Recon &R = h->R;
+    R.set_mask(nullptr, R.stream);
     to_float_dev(R.gin.p, grad, (size_t)R.nb * R.ngrad, R.stream);
     R.op_rhs(R.gin.p, R.rhs.p, R.stream);
     from_float_dev(xout, R.rhs.p, (size_t)R.nb * R.nxtot, R.stream);
@@ -1220,6 +1258,7 @@ int mb_apply_tomo_L(mb_recon *h, const double *xin, double *xout) {
     MB_API_BEGIN
     MB_REQUIRE(h && xin && xout, "invalid arguments");
     mb::Recon &R = h->R;
+    R.set_mask(nullptr, R.stream);
     to_float_dev(R.z.p, xin, (size_t)R.nb * R.nxtot, R.stream);
     R.op_lhs(R.z.p, R.Ap.p, nullptr, R.stream);
     from_float_dev(xout, R.Ap.p, (size_t)R.nb * R.nxtot, R.stream);
@@ -1230,6 +1269,7 @@ int mb_apply_fdpcg(mb_recon *h, const double *xin, double *xout) {
     MB_API_BEGIN
     MB_REQUIRE(h && xin && xout, "invalid arguments");
     mb::Recon &R = h->R;
+    R.set_mask(nullptr, R.stream);
     if (!R.precond) {
         mb::set_error("reconstructor has no FDPCG preconditioner");
         return MB_ESTATE;
@@ -1240,10 +1280,105 @@ int mb_apply_fdpcg(mb_recon *h, const double *xin, double *xout) {
     MB_API_END
 }
 
+// ---------------------------------------------------------------------------
+// Serving: per-slot state and masked steps
+// ---------------------------------------------------------------------------
+static void check_slot(const mb_recon *h, int slot) {
+    MB_REQUIRE(h, "null handle");
+    MB_REQUIRE(slot >= 0 && slot < h->R.nb, "slot %d out of range (%d slots)", slot, h->R.nb);
+}
+
+int mb_recon_reset_slot(mb_recon *h, int slot, void *stream) {
+    MB_API_BEGIN
+    check_slot(h, slot);
+    mb::Recon &R = h->R;
+    cudaStream_t s = (cudaStream_t)stream;
+    MB_CUDA_TRY(cudaMemsetAsync(R.x.p + (size_t)slot * R.nxtot, 0, R.nxtot * sizeof(float), s));
+    if (R.has_fit) MB_CUDA_TRY(cudaMemsetAsync(R.fa.p + (size_t)slot * R.nact, 0, R.nact * sizeof(float), s));
+    MB_API_END
+}
+
+int mb_slot_upload(mb_recon *h, int slot, const float *grad, void *stream) {
+    MB_API_BEGIN
+    check_slot(h, slot);
+    MB_REQUIRE(grad, "null gradients");
+    mb::Recon &R = h->R;
+    MB_CUDA_TRY(cudaMemcpyAsync(R.gin.p + (size_t)slot * R.ngrad, grad, R.ngrad * sizeof(float),
+                                cudaMemcpyDefault, (cudaStream_t)stream));
+    MB_API_END
+}
+
+int mb_slot_download(mb_recon *h, int slot, float *out, void *stream) {
+    MB_API_BEGIN
+    check_slot(h, slot);
+    MB_REQUIRE(out, "null output");
+    mb::Recon &R = h->R;
+    const float *src = R.has_fit ? R.fa.p + (size_t)slot * R.nact : R.x.p + (size_t)slot * R.nxtot;
+    const size_t n = R.has_fit ? (size_t)R.nact : (size_t)R.nxtot;
+    MB_CUDA_TRY(cudaMemcpyAsync(out, src, n * sizeof(float), cudaMemcpyDefault, (cudaStream_t)stream));
+    MB_API_END
+}
+
+int mb_recon_step_slots(mb_recon *h, const int *active, void *stream) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && active, "invalid arguments");
+    mb::Recon &R = h->R;
+    cudaStream_t s = (cudaStream_t)stream;
+    R.set_mask(active, s);
+    if (R.has_fit) {
+        MB_CUDA_TRY(cudaGraphLaunch(R.graph_step, s));
+        mb::count_launches(R.graph_step_kernels);
+    } else {
+        MB_CUDA_TRY(cudaGraphLaunch(R.graph, s));
+        mb::count_launches(R.graph_kernels);
+    }
+    MB_API_END
+}
+
+int mb_recon_serve_step(mb_recon *h, const int *active, const float *grad, float *out, void *stream) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && active && grad && out, "invalid arguments");
+    mb::Recon &R = h->R;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nout = R.has_fit ? (size_t)R.nact : (size_t)R.nxtot;
+    float *res = R.has_fit ? R.fa.p : R.x.p;
+    // one copy per run of consecutive active slots, each way
+    auto runs = [&](const std::function<void(int, int)> &f) {
+        for (int b = 0; b < R.nb;) {
+            if (!active[b]) {
+                b++;
+                continue;
+            }
+            int e = b;
+            while (e < R.nb && active[e]) e++;
+            f(b, e - b);
+            b = e;
+        }
+    };
+    runs([&](int b, int n) {
+        MB_CUDA_TRY(cudaMemcpyAsync(R.gin.p + (size_t)b * R.ngrad, grad + (size_t)b * R.ngrad,
+                                    (size_t)n * R.ngrad * sizeof(float), cudaMemcpyDefault, s));
+    });
+    R.set_mask(active, s);
+    if (R.has_fit) {
+        MB_CUDA_TRY(cudaGraphLaunch(R.graph_step, s));
+        mb::count_launches(R.graph_step_kernels);
+    } else {
+        MB_CUDA_TRY(cudaGraphLaunch(R.graph, s));
+        mb::count_launches(R.graph_kernels);
+    }
+    runs([&](int b, int n) {
+        MB_CUDA_TRY(cudaMemcpyAsync(out + (size_t)b * nout, res + (size_t)b * nout, (size_t)n * nout * sizeof(float),
+                                    cudaMemcpyDefault, s));
+    });
+    MB_API_END
+}
+
 int mb_apply_hx(mb_recon *h, const double *xin, double *opd) {
     MB_API_BEGIN
     MB_REQUIRE(h && xin && opd, "invalid arguments");
     mb::Recon &R = h->R;
+    R.set_mask(nullptr, R.stream);
     to_float_dev(R.z.p, xin, (size_t)R.nb * R.nxtot, R.stream);
     R.op_hx(R.z.p, R.stream);
     from_float_dev(opd, R.opd.p, (size_t)R.nb * R.nwfs * R.np, R.stream);

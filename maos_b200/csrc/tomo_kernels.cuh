@@ -112,6 +112,12 @@ __device__ __forceinline__ double warp_sum_fresh(const double *part, int n) {
     return __shfl_sync(0xffffffffu, v, 0);
 }
 
+// Serving: `act` (null: every instance) marks the instances that take part in
+// this launch.  Blocks of an inactive instance return before touching memory,
+// so its warm-start state stays as it was and no other instance's result
+// depends on which instances are active.  Block-uniform (b is a block index).
+__device__ __forceinline__ bool inactive(const int *act, int b) { return act && __ldg(act + b) == 0; }
+
 // ---------------------------------------------------------------------------
 // Hx: opd[b][w][p] = sum_l bilinear(x_l) at the ray of pupil point p.
 // grid: (ceil(np/256), nwfs, nb)
@@ -119,7 +125,8 @@ __device__ __forceinline__ double warp_sum_fresh(const double *part, int n) {
 __global__ void k_hx(const float *__restrict__ x, float *__restrict__ opd,
                      const AxisW *__restrict__ tab, const LayerDev *__restrict__ lay, int nps,
                      int nwfs, int nxp, int nyp, long nxtot, const float *__restrict__ w1,
-                     double *__restrict__ w1_part) {
+                     double *__restrict__ w1_part, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.z)) return;
     __shared__ double sh[32];
     const int np = nxp * nyp;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -155,7 +162,9 @@ __global__ void k_hx(const float *__restrict__ x, float *__restrict__ opd,
 __global__ void k_gp(const float *__restrict__ opd, const float *__restrict__ gin,
                      float *__restrict__ grad, double *__restrict__ tt_part,
                      const WfsDev *__restrict__ wfs, int nwfs, int nxp, int np, long ngrad,
-                     int do_tt, float *__restrict__ tt_out, unsigned *__restrict__ cnt) {
+                     int do_tt, float *__restrict__ tt_out, unsigned *__restrict__ cnt,
+                     const int *__restrict__ act) {
+    if (inactive(act, blockIdx.z)) return;
     __shared__ double sh[32];
     const int w = blockIdx.y, b = blockIdx.z;
     const WfsDev W = wfs[w];
@@ -221,7 +230,9 @@ __global__ void k_gp(const float *__restrict__ opd, const float *__restrict__ gi
 // ---------------------------------------------------------------------------
 __global__ void k_gpt(const float *__restrict__ grad, const float *__restrict__ tt,
                       float *__restrict__ opd2, const WfsDev *__restrict__ wfs, int nwfs,
-                      int nxp, int nyp, long ngrad, int do_tt, float alpha) {
+                      int nxp, int nyp, long ngrad, int do_tt, float alpha,
+                      const int *__restrict__ act) {
+    if (inactive(act, blockIdx.z)) return;
     const int w = blockIdx.y, b = blockIdx.z;
     const WfsDev W = wfs[w];
     const bool use_tt = do_tt && W.has_ptt;
@@ -287,7 +298,9 @@ struct LowRank {
 __global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ xin,
                       float *__restrict__ out, double *__restrict__ dot_part, GatherIndex gi,
                       const LayerDev *__restrict__ lay, int nps, int nwfs, int nxp, int nyp,
-                      long nxtot, int do_l2, float alpha, LowRank lr, CgScal S, int k) {
+                      long nxtot, int do_l2, float alpha, LowRank lr, CgScal S, int k,
+                      const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     __shared__ float s_t[8];
     const int b = blockIdx.y;
@@ -382,7 +395,8 @@ k_hxt_tiled(const float *__restrict__ opd2, const float *__restrict__ xin, float
             double *__restrict__ dot_part, GatherIndex gi, const LayerDev *__restrict__ lay,
             const TileDesc *__restrict__ tiles, const int2 *__restrict__ rowrange, int nps, int nwfs,
             int nxp, int nyp, long nxtot, int do_l2, float alpha, int maxrows, int maxnx,
-            int maxent, CgScal S, int kit) {
+            int maxent, CgScal S, int kit, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
     extern __shared__ float smem[];
     __shared__ double sh[32];
     const int tid = blockIdx.x, b = blockIdx.y;
@@ -478,7 +492,8 @@ __global__ void k_fit_w(const float *__restrict__ v, float *__restrict__ y,
                         const int *__restrict__ rp, const int *__restrict__ ci,
                         const float *__restrict__ cv, const float *__restrict__ w1,
                         const float *__restrict__ wt, const double *__restrict__ w1_part,
-                        int nblk_w1, int nf, int nfit) {
+                        int nblk_w1, int nf, int nfit, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.z)) return;
     __shared__ float s_dot;
     const int f = blockIdx.y, b = blockIdx.z;
     if (threadIdx.x < 32) {
@@ -496,7 +511,8 @@ __global__ void k_fit_w(const float *__restrict__ v, float *__restrict__ y,
 
 // NW' x partials: part[(b*nnw + k)*nblk + blk].  grid: (nblk, nb)
 __global__ void k_lowrank_dot(const float *__restrict__ x, const float *__restrict__ nw,
-                              double *__restrict__ part, int nnw, long n) {
+                              double *__restrict__ part, int nnw, long n, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     const int b = blockIdx.y;
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -516,7 +532,8 @@ __global__ void k_lowrank_dot(const float *__restrict__ x, const float *__restri
 // r = b - Ax; b.b is reduced by the last block into sc[iters+1].  grid: (nblk, nb)
 __global__ void k_cg_init_r(const float *__restrict__ bvec, const float *__restrict__ Ax,
                             float *__restrict__ r, double *__restrict__ bb_part, long n, CgScal S,
-                            int iters) {
+                            int iters, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     const int b = blockIdx.y;
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -560,7 +577,9 @@ __device__ __forceinline__ void cg_rz_last(const double *part_b, const CgScal &S
 }
 
 // v.v partials and (when z aliases r) the start-of-CG r.z.  grid: (nblk, nb)
-__global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ part, long n, CgScal S) {
+__global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ part, long n, CgScal S,
+                           const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     const int b = blockIdx.y;
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -580,7 +599,8 @@ __global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ par
 __global__ void k_cg_update_xr(float *__restrict__ x, float *__restrict__ r,
                                const float *__restrict__ p, const float *__restrict__ Ap,
                                double *__restrict__ rr_part, long n, CgScal S, int k, int iters,
-                               int z_is_r) {
+                               int z_is_r, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     const int b = blockIdx.y;
     const float a = S.ab[2 * b];
@@ -613,7 +633,8 @@ __global__ void k_cg_update_xr(float *__restrict__ x, float *__restrict__ r,
 
 // p = z + beta p (init: p = z).  grid: (nblk, nb)
 __global__ void k_cg_update_p(float *__restrict__ p, const float *__restrict__ z, long n, CgScal S,
-                              int init) {
+                              int init, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
     const int b = blockIdx.y;
     const float be = init ? 0.f : S.ab[2 * b + 1];
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -634,7 +655,8 @@ struct FdIndex {
 // real r (instance-major) -> complex spectra buffer (layer-major)
 __global__ void k_fd_pack(const float *__restrict__ r, cufftComplex *__restrict__ S,
                           const LayerDev *__restrict__ lay, const int *__restrict__ soff, int nps,
-                          long nxtot) {
+                          long nxtot, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
     const int b = blockIdx.y;
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nxtot) return;
@@ -649,7 +671,8 @@ __global__ void k_fd_pack(const float *__restrict__ r, cufftComplex *__restrict_
 // One thread per (block, row); grid: (ceil(nb*bs/256), nbatch)
 __global__ void k_fd_mul(const cufftComplex *__restrict__ X, cufftComplex *__restrict__ Y,
                          const cufftComplex *__restrict__ M, const FdIndex *__restrict__ idx,
-                         int nblk, int bs) {
+                         int nblk, int bs, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
     const int b = blockIdx.y;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nblk * bs) return;
@@ -672,7 +695,8 @@ __global__ void k_fd_mul(const cufftComplex *__restrict__ X, cufftComplex *__res
 __global__ void k_fd_unpack(const cufftComplex *__restrict__ S, const float *__restrict__ r,
                             float *__restrict__ z, double *__restrict__ rz_part,
                             const LayerDev *__restrict__ lay, const int *__restrict__ soff, int nps,
-                            long nxtot, CgScal SC, int k, int init) {
+                            long nxtot, CgScal SC, int k, int init, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     const int b = blockIdx.y;
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -78,6 +78,11 @@ SIGNATURES = {
     "mb_stage_name": (C.c_char_p, [C.c_int]),
     "mb_time_stages": (C.c_int, [C.c_void_p, C.c_int, _F, _D, C.POINTER(C.c_int)]),
     "mb_tomo_residual": (C.c_int, [C.c_void_p, _F]),
+    "mb_recon_reset_slot": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "mb_slot_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "mb_slot_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "mb_recon_step_slots": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p]),
+    "mb_recon_serve_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p]),
     "mb_ngrad": (C.c_long, [C.c_void_p]),
     "mb_nxtot": (C.c_long, [C.c_void_p]),
     "mb_nbatch": (C.c_int, [C.c_void_p]),

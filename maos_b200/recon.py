@@ -188,6 +188,36 @@ class Reconstructor:
     def fit_solution_ptr(self) -> int:
         return int(self.lib.mb_fit_solution(self.h))
 
+    # serving: instances as slots (no counterpart in the reference)
+    def reset_slot(self, slot: int, stream_ptr: int = 0):
+        check(self.lib.mb_recon_reset_slot(self.h, int(slot), C.c_void_p(stream_ptr)), "mb_recon_reset_slot")
+
+    def slot_upload(self, slot: int, grad_ptr: int, stream_ptr: int = 0):
+        """Enqueue the copy of one slot's FP32 gradients (host or device pointer)."""
+        check(self.lib.mb_slot_upload(self.h, int(slot), C.c_void_p(grad_ptr), C.c_void_p(stream_ptr)),
+              "mb_slot_upload")
+
+    def slot_download(self, slot: int, out_ptr: int, stream_ptr: int = 0):
+        """Enqueue the copy of one slot's FP32 DM commands (or layer OPD without a fit)."""
+        check(self.lib.mb_slot_download(self.h, int(slot), C.c_void_p(out_ptr), C.c_void_p(stream_ptr)),
+              "mb_slot_download")
+
+    def serve_step(self, active, grad_ptr: int, out_ptr: int, stream_ptr: int = 0):
+        """Upload the active slots' gradients, step them, download their results."""
+        m = np.ascontiguousarray(active, dtype=np.int32)
+        if m.shape != (self.nbatch,):
+            raise ValueError(f"active must have {self.nbatch} entries")
+        check(self.lib.mb_recon_serve_step(self.h, m.ctypes.data_as(C.POINTER(C.c_int)), C.c_void_p(grad_ptr),
+                                           C.c_void_p(out_ptr), C.c_void_p(stream_ptr)), "mb_recon_serve_step")
+
+    def step_slots(self, active, stream_ptr: int = 0):
+        """One step of the slots whose flag in `active` [nbatch] is non-zero."""
+        m = np.ascontiguousarray(active, dtype=np.int32)
+        if m.shape != (self.nbatch,):
+            raise ValueError(f"active must have {self.nbatch} entries")
+        check(self.lib.mb_recon_step_slots(self.h, m.ctypes.data_as(C.POINTER(C.c_int)),
+                                           C.c_void_p(stream_ptr)), "mb_recon_step_slots")
+
     def apply_fit_R(self, x):
         xi = self._vec(x, self.nxtot)
         out = np.empty((self.nbatch, self.nact))
