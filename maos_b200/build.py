@@ -34,7 +34,7 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB] + [os.path.join(HERE, s) for s in SOURCES] + ["-lcufft"]
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB] + [os.path.join(HERE, s) for s in SOURCES]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -9,7 +9,6 @@
 // coefficients, not short2-quantised) and every transpose is the exact
 // transpose of the forward table, evaluated in gather form.
 #include <cuda_runtime.h>
-#include <cufft.h>
 
 #include <algorithm>
 #include <cmath>
@@ -40,16 +39,6 @@ static std::atomic<long> g_launches{0};
 void count_launches(long n) { g_launches += n; }
 
 static inline unsigned nblocks(long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
-
-struct CufftError {};
-#define MB_CUFFT_TRY(call)                                                          \
-    do {                                                                            \
-        cufftResult r_ = (call);                                                    \
-        if (r_ != CUFFT_SUCCESS) {                                                  \
-            mb::set_error("%s:%d %s: cufft error %d", __FILE__, __LINE__, #call, (int)r_); \
-            throw mb::CudaError{MB_ECUDA};                                          \
-        }                                                                           \
-    } while (0)
 
 // Forward tables for (direction d, source grid t) and their exact transposes
 // as per-axis CSR lists over the source grid (gather form).
@@ -91,13 +80,14 @@ struct Recon {
     std::vector<std::unique_ptr<DevBuf<float>>> neai, ptt;
     std::vector<WfsDev> wfs_h;
     // FDPCG
-    int fd_nb = 0, fd_bs = 0;
-    DevBuf<cufftComplex> fd_M;
+    int fd_nb = 0, fd_bs = 0, fd_nbh = 0;  // blocks, block size, blocks solved (half spectrum)
+    DevBuf<cplx> fd_M;
     DevBuf<FdIndex> fd_idx;
-    DevBuf<int> fd_soff;
-    std::vector<cufftHandle> plans;
-    std::vector<long> plan_off;   // element offset of each plan's first slab
-    DevBuf<cufftComplex> spec, spec2;
+    DevBuf<FdLayer> fd_lay;                 // per layer: FFT geometry and radices
+    DevBuf<cplx> fd_tw;                     // twiddle tables exp(-2 pi i k/n)
+    int fd_bufn = 0;                        // complex elements per FFT shared buffer
+    size_t fd_smem = 0;
+    DevBuf<cplx> spec, spec2;               // half spectra
 
     // state and work buffers
     DevBuf<float> x, r, p, z, Ap, rhs, opd, opd2, grad, gin;
@@ -143,7 +133,6 @@ struct Recon {
         if (graph) cudaGraphExecDestroy(graph);
         if (graph_fit) cudaGraphExecDestroy(graph_fit);
         if (graph_step) cudaGraphExecDestroy(graph_step);
-        for (auto h : plans) cufftDestroy(h);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -436,68 +425,143 @@ void Recon::set_l2c(const double *l2c) {
     lay.upload(lay_h);
 }
 
+// FDPCG tables for the half spectrum.  The reference orders the frequency
+// blocks with the non-positive x frequencies first (maos/fdpcg.c:119-197,
+// fdpcg_perm); those leading blocks reach every stored bin of each layer's
+// real-to-complex spectrum, some bins twice (once directly, once as a
+// conjugate).  Each stored bin gets exactly one writer, preferring the
+// direct member, so the result does not depend on write order.
 void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
     MB_REQUIRE(fd && fd->perm && fd->mbinv && fd->nb > 0 && fd->bs > 0, "fdpcg tables missing");
     MB_REQUIRE((long)fd->nb * fd->bs == nxtot, "fdpcg: nb*bs=%ld differs from nxtot=%ld",
                (long)fd->nb * fd->bs, nxtot);
+    MB_REQUIRE(fd->bs <= kThreads, "fdpcg: block size %d above %d", fd->bs, kThreads);
     fd_nb = fd->nb;
     fd_bs = fd->bs;
-    // spectra layout: layer-major, soff[l] = sum_{l'<l} nb * n_l'
-    std::vector<int> soff(nps);
+    std::vector<long> hoff(nps), hsz(nps);
     long acc = 0;
     for (int l = 0; l < nps; l++) {
-        soff[l] = (int)acc;
-        acc += (long)nb * lay_h[l].nx * lay_h[l].ny;
+        MB_REQUIRE(lay_h[l].nx % 2 == 0 && lay_h[l].ny % 2 == 0, "fdpcg: layer %d grid %dx%d is not even", l,
+                   lay_h[l].nx, lay_h[l].ny);
+        hsz[l] = (long)lay_h[l].ny * (lay_h[l].nx / 2 + 1);
+        hoff[l] = acc;
+        acc += (long)nb * hsz[l];
     }
     MB_REQUIRE(acc < (1L << 31), "fdpcg: batch too large for 32-bit spectrum index");
-    std::vector<FdIndex> idx(nxtot);
-    std::vector<double> sc(nxtot);
-    for (long i = 0; i < nxtot; i++) {
-        long q = fd->perm[i];
-        if (q < 0) q = -q;  // conjugate flag only appears in the half spectrum
+    struct Mem { int l; long pos; bool conj; };
+    auto member = [&](long q) {
+        if (q < 0) q = -q;
         MB_REQUIRE(q < nxtot, "fdpcg: perm out of range");
         int l = 0;
         while (l + 1 < nps && q >= xoff[l + 1]) l++;
         const long local = q - xoff[l];
-        const long nl = (long)lay_h[l].nx * lay_h[l].ny;
-        idx[i].base = (int)(soff[l] + local);
-        idx[i].stride = (int)nl;
-        sc[i] = fd->scale ? 1.0 / std::sqrt((double)nl) : 1.0;
+        const int nx = lay_h[l].nx, ny = lay_h[l].ny;
+        long jx = local % nx, jy = local / nx;
+        bool cj = false;
+        if (jx > nx / 2) {  // bin of a positive-x frequency: the conjugate of a stored bin
+            cj = true;
+            jx = nx - jx;
+            jy = (ny - jy) % ny;
+        }
+        return Mem{l, jy * (nx / 2 + 1) + jx, cj};
+    };
+    // solve the leading blocks until every stored bin has a writer
+    std::vector<std::vector<long>> writer(nps);
+    long ntot = 0, nreach = 0;
+    for (int l = 0; l < nps; l++) {
+        writer[l].assign(hsz[l], -1);
+        ntot += hsz[l];
+    }
+    int nbh = 0;
+    for (int blk = 0; blk < fd_nb && nreach < ntot; blk++, nbh++)
+        for (int m = 0; m < fd_bs; m++) {
+            const long i = (long)blk * fd_bs + m;
+            const Mem e = member(fd->perm[i]);
+            long &wr = writer[e.l][e.pos];
+            if (wr < 0) {
+                wr = i;
+                nreach++;
+            } else if (!e.conj && member(fd->perm[wr]).conj) {
+                wr = i;  // prefer the direct member
+            }
+        }
+    if (nreach < ntot) {
+        set_error("fdpcg: the block ordering does not reach the half spectrum (%ld of %ld bins)", nreach, ntot);
+        throw InvalidArg{MB_EUNSUP};
+    }
+    fd_nbh = nbh;
+    std::vector<FdIndex> idx((size_t)nbh * fd_bs);
+    std::vector<double> sc((size_t)nbh * fd_bs);
+    for (long i = 0; i < (long)nbh * fd_bs; i++) {
+        const Mem e = member(fd->perm[i]);
+        idx[i].base = (int)(hoff[e.l] + e.pos);
+        idx[i].stride = (int)hsz[e.l];
+        idx[i].flags = (e.conj ? kFdConj : 0) | (writer[e.l][e.pos] == i ? kFdStore : 0);
+        idx[i].pad = 0;
+        sc[i] = fd->scale ? 1.0 / std::sqrt((double)lay_h[e.l].nx * lay_h[e.l].ny) : 1.0;
     }
     // fold the 1/sqrt(n) of the forward and inverse FFTs into the blocks
-    std::vector<cufftComplex> M((size_t)fd_nb * fd_bs * fd_bs);
-    for (long b = 0; b < fd_nb; b++)
+    std::vector<cplx> M((size_t)nbh * fd_bs * fd_bs);
+    for (long b = 0; b < nbh; b++)
         for (int j = 0; j < fd_bs; j++)
             for (int i = 0; i < fd_bs; i++) {
                 const size_t k = (size_t)b * fd_bs * fd_bs + (size_t)j * fd_bs + i;
                 const double s = sc[b * fd_bs + i] * sc[b * fd_bs + j];
-                M[k] = make_cuFloatComplex((float)(fd->mbinv[2 * k] * s), (float)(fd->mbinv[2 * k + 1] * s));
+                M[k] = make_float2((float)(fd->mbinv[2 * k] * s), (float)(fd->mbinv[2 * k + 1] * s));
             }
     fd_M.upload(M);
     fd_idx.upload(idx);
-    fd_soff.upload(soff);
     spec.alloc(acc);
     spec2.alloc(acc);
     spec.zero_async(stream);  // spectra of instances that never ran stay finite
     spec2.zero_async(stream);
-    // one batched 2-D plan per run of consecutive equal-size layers
-    for (auto h : plans) cufftDestroy(h);
-    plans.clear();
-    plan_off.clear();
-    int l0 = 0;
-    while (l0 < nps) {
-        int l1 = l0 + 1;
-        while (l1 < nps && lay_h[l1].nx == lay_h[l0].nx && lay_h[l1].ny == lay_h[l0].ny) l1++;
-        int n[2] = {lay_h[l0].ny, lay_h[l0].nx};
-        const int dist = n[0] * n[1];
-        cufftHandle h;
-        MB_CUFFT_TRY(cufftPlanMany(&h, 2, n, nullptr, 1, dist, nullptr, 1, dist, CUFFT_C2C,
-                                   nb * (l1 - l0)));
-        MB_CUFFT_TRY(cufftSetStream(h, stream));
-        plans.push_back(h);
-        plan_off.push_back(soff[l0]);
-        l0 = l1;
+    // FFT geometry per layer: radix stages (4 first, then 2, 3, 5) and one
+    // twiddle table per distinct length, computed in FP64
+    std::vector<FdLayer> fl(nps);
+    std::vector<cplx> tw;
+    std::vector<std::pair<int, int>> twof;  // (n, offset)
+    auto table = [&](int n) {
+        for (auto &e : twof)
+            if (e.first == n) return e.second;
+        const int o = (int)tw.size();
+        for (int k = 0; k < n; k++) {
+            const double a = -2.0 * M_PI * k / n;
+            tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+        }
+        twof.push_back({n, o});
+        return o;
+    };
+    auto radices = [&](int n, signed char *rad, int &nr) {
+        nr = 0;
+        for (int R : {4, 2, 3, 5})
+            while (n % R == 0 && nr < 8) {
+                rad[nr++] = (signed char)R;
+                n /= R;
+            }
+        return n == 1;
+    };
+    fd_bufn = 0;
+    for (int l = 0; l < nps; l++) {
+        FdLayer &F = fl[l];
+        F.nx = lay_h[l].nx;
+        F.ny = lay_h[l].ny;
+        if (!radices(F.nx, F.rx, F.nrx) || !radices(F.ny, F.ry, F.nry)) {
+            set_error("fdpcg: layer %d grid %dx%d is not a product of 2, 3 and 5 in 8 stages", l, F.nx, F.ny);
+            throw InvalidArg{MB_EUNSUP};
+        }
+        F.off = lay_h[l].off;
+        F.hoff = (int)hoff[l];
+        F.hs = (int)hsz[l];
+        F.twx = table(F.nx);
+        F.twy = table(F.ny);
+        fd_bufn = std::max(fd_bufn, std::max(F.ny / 2 * F.nx, F.ny * (F.nx / 2 + 1)));
     }
+    fd_lay.upload(fl);
+    fd_tw.upload(tw);
+    fd_smem = 2 * (size_t)fd_bufn * sizeof(cplx);
+    MB_REQUIRE(fd_smem <= 200 * 1024, "fdpcg: layer FFT needs %zu bytes of shared memory", fd_smem);
+    MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
+    MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
 }
 
 void Recon::build(const mb_recon_desc *d) {
@@ -626,24 +690,17 @@ void Recon::op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t 
 
 void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s, int k, int init,
                      bool in_cg) {
-    // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT
-    k_fd_pack<<<dim3(nblk_x, nb), kThreads, 0, s>>>(rin, spec.p, lay.p, fd_soff.p, nps, nxtot, act());
+    // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT,
+    // on the half spectrum as in cuda/fdpcg.cu (fdpcg_mul_block_sync_half)
+    k_fd_fwd<<<dim3(nps, nb), kThreads, fd_smem, s>>>(rin, spec.p, fd_lay.p, fd_tw.p, nxtot, fd_bufn, act());
     MB_CHECK_LAUNCH();
-    for (size_t i = 0; i < plans.size(); i++) {
-        MB_CUFFT_TRY(cufftSetStream(plans[i], s));
-        MB_CUFFT_TRY(cufftExecC2C(plans[i], spec.p + plan_off[i], spec.p + plan_off[i], CUFFT_FORWARD));
-        count_launches(1);
-    }
-    k_fd_mul<<<dim3(nblocks((long)fd_nb * fd_bs), nb), kThreads, 0, s>>>(spec.p, spec2.p, fd_M.p,
-                                                                        fd_idx.p, fd_nb, fd_bs, act());
+    const int per = kThreads / fd_bs;
+    k_fd_mul<<<dim3((fd_nbh + per - 1) / per, nb), kThreads, 0, s>>>(spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh,
+                                                                    fd_bs, act());
     MB_CHECK_LAUNCH();
-    for (size_t i = 0; i < plans.size(); i++) {
-        MB_CUFFT_TRY(cufftExecC2C(plans[i], spec2.p + plan_off[i], spec2.p + plan_off[i], CUFFT_INVERSE));
-        count_launches(1);
-    }
     CgScal S = in_cg ? scal() : CgScal{};
-    k_fd_unpack<<<dim3(nblk_x, nb), kThreads, 0, s>>>(spec2.p, rin, zout, rzp, lay.p, fd_soff.p, nps,
-                                                     nxtot, S, k, init, act());
+    k_fd_inv<<<dim3(nps, nb), kThreads, fd_smem, s>>>(spec2.p, rin, zout, rzp, fd_lay.p, fd_tw.p, nxtot, fd_bufn, S,
+                                                     k, init, act());
     MB_CHECK_LAUNCH();
 }
 
@@ -845,23 +902,22 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     const double ngr = (double)ngrad;
     const double nx = (double)nxtot;
     const double gather = (double)hx.ent.n * 8.0 + (double)hx.idxptr.n * 4.0;
-    const double nbk = (double)fd_nb * fd_bs;
+    const double nbk = (double)fd_nbh * fd_bs;
+    double nh = 0;  // half-spectrum bins per instance
+    for (int l = 0; l < nps; l++) nh += (double)lay_h[l].ny * (lay_h[l].nx / 2 + 1);
     // bytes per launch: operands read + written once
-    double by[11] = {
+    double by[9] = {
         B * (F * nx + F * nxw) + (double)hx.fwd.n * 12.0,             // hx: x -> opd
         B * (F * nxw + F * ngr + D * 2 * nwfs * nblk_tt) + tab_gp,     // gp: opd -> grad
         B * (F * ngr + F * nxw) + tab_gpt,                             // gpt: grad -> opd2
         B * (F * nxw + 2 * F * nx) + gather,                           // hxt: opd2, p -> Ap
         B * (5 * F * nx),                                              // x,r,p,Ap r/w
         B * (3 * F * nx),                                              // p,z -> p
-        B * (F * nx + 2 * F * nx),                                     // r -> complex spec
-        B * (16.0 * nx),                                               // C2C read+write
-        B * (16.0 * nbk) + 8.0 * nbk * fd_bs + 8.0 * nbk,              // spec, spec2, M, idx
-        B * (16.0 * nx),
-        B * (2 * F * nx + F * nx + F * nx)};                           // spec (re), r -> z
-    const int lps[11] = {maxit + 1, maxit + 2, maxit + 2, maxit + 2, maxit, maxit - 1 + 1,
-                         precond ? maxit : 0, precond ? maxit : 0, precond ? maxit : 0,
-                         precond ? maxit : 0, precond ? maxit : 0};
+        B * (F * nx + 8.0 * nh),                                       // r -> half spectra
+        B * (16.0 * nbk) + 8.0 * nbk * fd_bs + 16.0 * nbk,             // spec, spec2, M, idx
+        B * (8.0 * nh + 2 * F * nx)};                                  // half spectra, r -> z
+    const int lps[9] = {maxit + 1, maxit + 2, maxit + 2, maxit + 2, maxit, maxit,
+                        precond ? maxit : 0, precond ? maxit : 0, precond ? maxit : 0};
     GatherIndex gi = hx.gi();
     for (int st = 0; st < ns; st++) {
         bytes[st] = by[st];
@@ -901,26 +957,19 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                     MB_CHECK_LAUNCH();
                     break;
                 case 6:
-                    k_fd_pack<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(r.p, spec.p, lay.p, fd_soff.p, nps, nxtot, act());
+                    k_fd_fwd<<<dim3(nps, nb), kThreads, fd_smem, stream>>>(r.p, spec.p, fd_lay.p, fd_tw.p, nxtot,
+                                                                           fd_bufn, act());
                     MB_CHECK_LAUNCH();
                     break;
                 case 7:
-                case 9:
-                    for (size_t i = 0; i < plans.size(); i++) {
-                        MB_CUFFT_TRY(cufftSetStream(plans[i], stream));
-                        MB_CUFFT_TRY(cufftExecC2C(plans[i], spec.p + plan_off[i], spec.p + plan_off[i],
-                                                  st == 7 ? CUFFT_FORWARD : CUFFT_INVERSE));
-                        count_launches(1);
-                    }
-                    break;
-                case 8:
-                    k_fd_mul<<<dim3(nblocks((long)fd_nb * fd_bs), nb), kThreads, 0, stream>>>(
-                        spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nb, fd_bs, act());
+                    k_fd_mul<<<dim3((fd_nbh + kThreads / fd_bs - 1) / (kThreads / fd_bs), nb), kThreads, 0,
+                               stream>>>(spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh, fd_bs, act());
                     MB_CHECK_LAUNCH();
                     break;
-                case 10:
-                    k_fd_unpack<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(spec2.p, r.p, z.p, rz_part.p, lay.p,
-                                                                          fd_soff.p, nps, nxtot, CgScal{}, 0, 0, act());
+                case 8:
+                    k_fd_inv<<<dim3(nps, nb), kThreads, fd_smem, stream>>>(spec2.p, r.p, z.p, rz_part.p, fd_lay.p,
+                                                                           fd_tw.p, nxtot, fd_bufn, CgScal{}, 0, 0,
+                                                                           act());
                     MB_CHECK_LAUNCH();
                     break;
             }
@@ -1223,7 +1272,7 @@ int mb_apply_fit_L(mb_recon *h, const double *ain, double *aout) {
 void *mb_recon_stream(mb_recon *h) { return h ? (void *)h->R.stream : nullptr; }
 
 static const char *kStageNames[] = {"hx", "gp", "gpt", "hxt_l2", "cg_update_xr", "cg_update_p",
-                                    "fd_pack", "fd_fft_fwd", "fd_mul", "fd_fft_inv", "fd_unpack"};
+                                    "fd_fwd", "fd_mul", "fd_inv"};
 int mb_num_stages(void) { return (int)(sizeof(kStageNames) / sizeof(kStageNames[0])); }
 const char *mb_stage_name(int i) { return (i >= 0 && i < mb_num_stages()) ? kStageNames[i] : ""; }
 

@@ -13,12 +13,12 @@
 //   k_cg_*      gpu_pcg scalar kernels (pcg.cu:27-57)         -- FP64 scalars
 #pragma once
 #include <cuda_runtime.h>
-#include <cufft.h>
 #include <stdint.h>
 
 namespace mb {
 
 constexpr int kThreads = 256;
+using cplx = float2;  // single-precision complex (re, im)
 
 // One axis entry of the forward bilinear table: source index k (-1: the
 // pupil point misses the layer) and the two weights for k and k+1.
@@ -645,75 +645,240 @@ __global__ void k_cg_update_p(float *__restrict__ p, const float *__restrict__ z
 }
 
 // ---------------------------------------------------------------------------
-// FDPCG.  Spectra are stored layer-major: S[soff[l] + b*n_l + local].
+// FDPCG on the half spectrum.  Each layer's forward transform reads the
+// residual straight from the instance-major vector and writes
+// H[hoff_l + b*hs_l + ky*(nx/2+1) + kx], hs_l = ny*(nx/2+1); the inverse
+// writes z back the same way.
 // ---------------------------------------------------------------------------
+enum { kFdConj = 1, kFdStore = 2 };
 struct FdIndex {
-    int base;    // soff[l] + local for the permuted member
-    int stride;  // n_l
+    int base;    // hoff_l + position of the member in the layer's half spectrum
+    int stride;  // hs_l (instance stride)
+    int flags;   // kFdConj: the member is the conjugate of the stored value;
+                 // kFdStore: this member writes the stored value
+    int pad;
 };
 
-// real r (instance-major) -> complex spectra buffer (layer-major)
-__global__ void k_fd_pack(const float *__restrict__ r, cufftComplex *__restrict__ S,
-                          const LayerDev *__restrict__ lay, const int *__restrict__ soff, int nps,
-                          long nxtot, const int *__restrict__ act) {
-    if (inactive(act, blockIdx.y)) return;
-    const int b = blockIdx.y;
-    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= nxtot) return;
-    int l = 0;
-    while (l + 1 < nps && j >= lay[l + 1].off) l++;
-    const long local = j - lay[l].off;
-    const long n_l = (long)lay[l].nx * lay[l].ny;
-    S[soff[l] + b * n_l + local] = make_cuFloatComplex(r[(size_t)b * nxtot + j], 0.f);
+// Batched 2-D real FFTs of the layer grids, one CTA per (layer, instance),
+// entirely in shared memory.  Length-n complex transforms are mixed-radix
+// Stockham stages (radix 2, 3, 4, 5; no reordering pass), twiddles
+// exp(-2 pi i k/n) come from a table computed on the host in FP64.  Two real
+// rows travel as one complex row.  Forward: rows, then columns of the half
+// spectrum; output layout [ky][kx], kx <= nx/2.  Inverse: columns, then
+// rows, with the imaginary parts of the kx = 0 and kx = nx/2 bins dropped
+// (the real part of the inverse of the Hermitian extension).  Neither
+// direction is normalised.
+struct FdLayer {
+    int nx, ny;          // grid (x fastest); both even
+    long off;            // offset of the layer in an instance vector
+    int hoff, hs;        // half-spectrum offset of instance 0 and the instance stride
+    int twx, twy;        // offsets of the twiddle tables for n = nx and n = ny
+    int nrx, nry;        // radix stages along x and y
+    signed char rx[8], ry[8];
+};
+
+__device__ __forceinline__ cplx cmul(cplx a, cplx b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ cplx cadd(cplx a, cplx b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ cplx csub(cplx a, cplx b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ cplx cconj(cplx a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ cplx mul_mi(cplx a) { return make_float2(a.y, -a.x); }  // -i a
+
+// One Stockham stage of radix R over `count` transforms of length n
+// (element stride es, transform stride ts), a -> b.  Ns = product of the
+// radices of the previous stages.
+template <int R>
+__device__ __forceinline__ void fft_stage(const cplx *__restrict__ a, cplx *__restrict__ b, int n, int count,
+                                          int es, int ts, int Ns, const cplx *__restrict__ tw, bool inv) {
+    const int nbf = n / R;
+    const int tmul = n / (Ns * R);
+    const int tot = nbf * count;
+    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+        const int c = t / nbf, j = t - c * nbf;
+        const cplx *src = a + (size_t)c * ts;
+        cplx *dst = b + (size_t)c * ts;
+        const int jm = j % Ns;
+        cplx v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            cplx x = src[(j + r * nbf) * es];
+            if (r > 0 && jm > 0) {
+                cplx w = tw[r * jm * tmul];
+                if (inv) w.y = -w.y;
+                x = cmul(x, w);
+            }
+            v[r] = x;
+        }
+        const int o = (j / Ns) * Ns * R + jm;
+        if (R == 2) {
+            dst[o * es] = cadd(v[0], v[1]);
+            dst[(o + Ns) * es] = csub(v[0], v[1]);
+        } else if (R == 4) {
+            const cplx s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+            const cplx s13 = cadd(v[1], v[3]);
+            cplx d13 = mul_mi(csub(v[1], v[3]));  // -i (v1 - v3)
+            if (inv) d13 = make_float2(-d13.x, -d13.y);
+            dst[o * es] = cadd(s02, s13);
+            dst[(o + Ns) * es] = cadd(d02, d13);
+            dst[(o + 2 * Ns) * es] = csub(s02, s13);
+            dst[(o + 3 * Ns) * es] = csub(d02, d13);
+        } else {
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                cplx acc = v[0];
+#pragma unroll
+                for (int r = 1; r < R; r++) {
+                    cplx w = tw[((r * q) % R) * nbf];
+                    if (inv) w.y = -w.y;
+                    acc = cadd(acc, cmul(v[r], w));
+                }
+                dst[(o + q * Ns) * es] = acc;
+            }
+        }
+    }
 }
 
-// Per-frequency block solve: Y[perm(i)] = sum_j M[blk][j*bs+i] X[perm(j)].
-// One thread per (block, row); grid: (ceil(nb*bs/256), nbatch)
-__global__ void k_fd_mul(const cufftComplex *__restrict__ X, cufftComplex *__restrict__ Y,
-                         const cufftComplex *__restrict__ M, const FdIndex *__restrict__ idx,
-                         int nblk, int bs, const int *__restrict__ act) {
+// All stages of `count` length-n transforms, ping-ponging between a and b;
+// returns the buffer that holds the result.  Ends with a barrier.
+__device__ cplx *fft_many(cplx *a, cplx *b, int n, int count, int es, int ts, const signed char *rad, int nr,
+                          const cplx *__restrict__ tw, bool inv) {
+    int Ns = 1;
+    for (int s = 0; s < nr; s++) {
+        const int R = rad[s];
+        switch (R) {
+            case 2: fft_stage<2>(a, b, n, count, es, ts, Ns, tw, inv); break;
+            case 3: fft_stage<3>(a, b, n, count, es, ts, Ns, tw, inv); break;
+            case 4: fft_stage<4>(a, b, n, count, es, ts, Ns, tw, inv); break;
+            default: fft_stage<5>(a, b, n, count, es, ts, Ns, tw, inv); break;
+        }
+        __syncthreads();
+        cplx *t = a;
+        a = b;
+        b = t;
+        Ns *= R;
+    }
+    return a;
+}
+
+// Forward: r (instance-major) -> half spectra H.  grid: (nps, nb); dynamic
+// shared memory: two buffers of `bufn` complex values.
+__global__ void __launch_bounds__(kThreads)
+k_fd_fwd(const float *__restrict__ r, cplx *__restrict__ H, const FdLayer *__restrict__ fl,
+         const cplx *__restrict__ tw, long nxtot, int bufn, const int *__restrict__ act) {
     if (inactive(act, blockIdx.y)) return;
+    extern __shared__ cplx fsm[];
+    const FdLayer L = fl[blockIdx.x];
     const int b = blockIdx.y;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nblk * bs) return;
-    const int blk = t / bs, i = t - blk * bs;
-    const cufftComplex *Mb = M + (size_t)blk * bs * bs;
-    const FdIndex *ib = idx + (size_t)blk * bs;
+    const int nx = L.nx, ny = L.ny, h = nx / 2 + 1, np2 = ny / 2;
+    cplx *A = fsm, *B = fsm + bufn;
+    const float *rb = r + (size_t)b * nxtot + L.off;
+    for (int i = threadIdx.x; i < np2 * nx; i += blockDim.x) {
+        const int p = i / nx, x = i - p * nx;
+        A[i] = make_float2(rb[(2 * p) * nx + x], rb[(2 * p + 1) * nx + x]);
+    }
+    __syncthreads();
+    cplx *Z = fft_many(A, B, nx, np2, 1, nx, L.rx, L.nrx, tw + L.twx, false);
+    cplx *S = (Z == A) ? B : A;
+    for (int i = threadIdx.x; i < np2 * h; i += blockDim.x) {
+        const int p = i / h, k = i - p * h;
+        const cplx zk = Z[p * nx + k], zm = cconj(Z[p * nx + (nx - k) % nx]);
+        S[(2 * p) * h + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+        const cplx d = csub(zk, zm);
+        S[(2 * p + 1) * h + k] = make_float2(0.5f * d.y, -0.5f * d.x);  // -i/2 (zk - conj(z_-k))
+    }
+    __syncthreads();
+    const cplx *C = fft_many(S, Z, ny, h, h, 1, L.ry, L.nry, tw + L.twy, false);
+    cplx *out = H + L.hoff + (size_t)b * L.hs;
+    for (int i = threadIdx.x; i < ny * h; i += blockDim.x) out[i] = C[i];
+}
+
+// Per-frequency block solve on the blocks of the non-positive x frequencies
+// (the leading blocks of the reference's ordering, which reach every stored
+// bin): Y_i = sum_j M[blk][j*bs+i] X_j.  A CTA takes floor(256/bs) whole
+// blocks: every thread first stages its own member X_i in shared memory,
+// then forms its row from the block's staged members.
+// grid: (ceil(nblk / floor(256/bs)), nbatch)
+__global__ void __launch_bounds__(kThreads)
+k_fd_mul(const cplx *__restrict__ X, cplx *__restrict__ Y, const cplx *__restrict__ M,
+         const FdIndex *__restrict__ idx, int nblk, int bs, const int *__restrict__ act) {
+    if (inactive(act, blockIdx.y)) return;
+    __shared__ cplx xs[kThreads];
+    const int b = blockIdx.y;
+    const int per = kThreads / bs;
+    const int lb = threadIdx.x / bs, i = threadIdx.x - lb * bs;
+    const int blk = blockIdx.x * per + lb;
+    const bool live = lb < per && blk < nblk;
+    FdIndex o{};
+    if (live) {
+        o = idx[(size_t)blk * bs + i];
+        cplx xv = X[o.base + (size_t)b * o.stride];
+        if (o.flags & kFdConj) xv.y = -xv.y;
+        xs[threadIdx.x] = xv;
+    }
+    __syncthreads();
+    if (!live) return;
+    const cplx *Mb = M + (size_t)blk * bs * bs + i;
+    const cplx *xb = xs + lb * bs;
     float re = 0.f, im = 0.f;
+#pragma unroll 4
     for (int jj = 0; jj < bs; jj++) {
-        const FdIndex q = ib[jj];
-        const cufftComplex xv = X[q.base + (size_t)b * q.stride];
-        const cufftComplex m = Mb[jj * bs + i];
+        const cplx m = Mb[jj * bs];
+        const cplx xv = xb[jj];
         re += m.x * xv.x - m.y * xv.y;
         im += m.x * xv.y + m.y * xv.x;
     }
-    const FdIndex o = ib[i];
-    Y[o.base + (size_t)b * o.stride] = make_cuFloatComplex(re, im);
+    if (o.flags & kFdStore)
+        Y[o.base + (size_t)b * o.stride] = make_float2(re, (o.flags & kFdConj) ? -im : im);
 }
 
-// z = Re(spectra), and r.z partials.  grid: (nblk_x, nb)
-__global__ void k_fd_unpack(const cufftComplex *__restrict__ S, const float *__restrict__ r,
-                            float *__restrict__ z, double *__restrict__ rz_part,
-                            const LayerDev *__restrict__ lay, const int *__restrict__ soff, int nps,
-                            long nxtot, CgScal SC, int k, int init, const int *__restrict__ act) {
+// Inverse: half spectra H -> z (instance-major), plus the r.z partial of this
+// (layer, instance); the last CTA of an instance leaves (r.z)_0 or beta.
+// grid: (nps, nb)
+__global__ void __launch_bounds__(kThreads)
+k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restrict__ z,
+         double *__restrict__ rz_part, const FdLayer *__restrict__ fl, const cplx *__restrict__ tw, long nxtot,
+         int bufn, CgScal SC, int kit, int init, const int *__restrict__ act) {
     if (inactive(act, blockIdx.y)) return;
+    extern __shared__ cplx fsm[];
     __shared__ double sh[32];
+    const FdLayer L = fl[blockIdx.x];
     const int b = blockIdx.y;
-    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = L.nx, ny = L.ny, h = nx / 2 + 1, np2 = ny / 2;
+    cplx *A = fsm, *B = fsm + bufn;
+    const cplx *in = H + L.hoff + (size_t)b * L.hs;
+    for (int i = threadIdx.x; i < ny * h; i += blockDim.x) A[i] = in[i];
+    __syncthreads();
+    cplx *C = fft_many(A, B, ny, h, h, 1, L.ry, L.nry, tw + L.twy, true);
+    cplx *Zb = (C == A) ? B : A;
+    for (int i = threadIdx.x; i < np2 * nx; i += blockDim.x) {
+        const int p = i / nx, k = i - p * nx;
+        const bool hi = k > nx / 2;
+        const int kk = hi ? nx - k : k;
+        cplx a = C[(2 * p) * h + kk], c = C[(2 * p + 1) * h + kk];
+        if (kk == 0 || kk == nx / 2) {
+            a.y = 0.f;
+            c.y = 0.f;
+        }
+        if (hi) {
+            a = cconj(a);
+            c = cconj(c);
+        }
+        Zb[i] = make_float2(a.x - c.y, a.y + c.x);  // a + i c
+    }
+    __syncthreads();
+    const cplx *Zo = fft_many(Zb, C, nx, np2, 1, nx, L.rx, L.nrx, tw + L.twx, true);
+    const size_t base = (size_t)b * nxtot + L.off;
     double v = 0;
-    if (j < nxtot) {
-        int l = 0;
-        while (l + 1 < nps && j >= lay[l + 1].off) l++;
-        const long local = j - lay[l].off;
-        const long n_l = (long)lay[l].nx * lay[l].ny;
-        const float zv = S[soff[l] + b * n_l + local].x;
-        const size_t o = (size_t)b * nxtot + j;
-        z[o] = zv;
-        v = (double)zv * r[o];
+    for (int i = threadIdx.x; i < np2 * nx; i += blockDim.x) {
+        const int p = i / nx, x = i - p * nx;
+        const cplx q = Zo[i];
+        const size_t o0 = base + (size_t)(2 * p) * nx + x, o1 = o0 + nx;
+        z[o0] = q.x;
+        z[o1] = q.y;
+        v += (double)q.x * r[o0] + (double)q.y * r[o1];
     }
     v = block_sum(v, sh);
     if (threadIdx.x == 0) rz_part[(size_t)b * gridDim.x + blockIdx.x] = v;
-    if (SC.sc) cg_rz_last(rz_part + (size_t)b * gridDim.x, SC, b, k, init);
+    if (SC.sc) cg_rz_last(rz_part + (size_t)b * gridDim.x, SC, b, kit, init);
 }
 
 // float <-> double staging helpers for the host-facing API
