@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -66,10 +67,14 @@ struct Recon {
 
     // tables
     RayTables hx;
-    DevBuf<TileDesc> tiles;
-    DevBuf<int2> rowrange;
-    int ntiles = 0, tile_rows = 0, maxrows = 0, maxnx = 0, maxent = 0;
-    size_t hxt_smem = 0;
+    // separable Hx^T: fixed-width transposed lists and the pupil-row buffer
+    DevBuf<GatherW> xpad, ypad;
+    int kx = 0, ky = 0, maxnx = 0, maxny = 0;
+    int prows = 0, ptiles = 0, ncols = 0;  // pupil rows per CTA, CTAs per WFS, sum of layer widths
+    long tw = 0;                           // row-buffer floats per (instance, WFS)
+    size_t pupil_smem = 0;
+    DevBuf<float> tbuf;
+    PadIndex pad() const { return PadIndex{xpad.p, ypad.p, kx, ky, maxnx, maxny}; }
     DevBuf<LayerDev> lay;
     std::vector<LayerDev> lay_h;
     std::vector<mb_grid> xgrid;   // host copy of the layer grids
@@ -90,7 +95,7 @@ struct Recon {
     DevBuf<cplx> spec, spec2;               // half spectra
 
     // state and work buffers
-    DevBuf<float> x, r, p, z, Ap, rhs, opd, opd2, grad, gin;
+    DevBuf<float> x, r, p, z, Ap, rhs, opd, grad, gin;
     DevBuf<double> tt_part, pap_part, rr_part, rz_part, bb_part, sc;
     DevBuf<float> res, ab, tt;
     DevBuf<unsigned> cnt, cnt_tt;
@@ -139,7 +144,9 @@ struct Recon {
     // ------------------------------------------------------------------
     void build(const mb_recon_desc *d);
     void build_hx_tables(const mb_recon_desc *d);
-    void build_tiles();
+    void build_pad();
+    void pupil_rows(bool from_x, const float *xin, cudaStream_t s);
+    void hxt_rows(const float *xin, float *out, double *dot_part, int do_l2, int k, cudaStream_t s);
     void build_wfs_tables(const mb_recon_desc *d);
     void build_fdpcg(const mb_fdpcg_desc *fd);
     void build_fit(const mb_fit_desc *f);
@@ -268,51 +275,85 @@ void Recon::build_hx_tables(const mb_recon_desc *d) {
                      false, hx);
 }
 
-// Row tiles of every layer and, per tile and WFS, the pupil rows whose
-// transposed bilinear weights reach the tile (union of the y-gather lists).
-void Recon::build_tiles() {
-    maxnx = 0;
-    for (int l = 0; l < nps; l++) maxnx = std::max(maxnx, lay_h[l].nx);
-    MB_REQUIRE(maxnx <= kThreads * kMaxOwn, "layer grid too wide (%d)", maxnx);
-    int rows = std::min(8, kThreads * kMaxOwn / maxnx);
-    auto count = [&](int r) {
-        int n = 0;
-        for (int l = 0; l < nps; l++) n += (lay_h[l].ny + r - 1) / r;
-        return n;
-    };
-    while (rows > 1 && (long)count(rows) * nb < 2 * 148) rows /= 2;  // keep >= 2 waves on 148 SMs
-    tile_rows = rows;
-    std::vector<TileDesc> tl;
-    for (int l = 0; l < nps; l++)
-        for (int y0 = 0; y0 < lay_h[l].ny; y0 += rows) tl.push_back(TileDesc{l, y0, std::min(rows, lay_h[l].ny - y0)});
-    ntiles = (int)tl.size();
-    std::vector<int2> rr((size_t)ntiles * nwfs);
-    maxrows = 1;
-    maxent = 1;
-    for (int w = 0; w < nwfs; w++)
-        for (int l = 0; l < nps; l++) {
-            const int tx = hx.h_ptr[(w * nps + l) * 2 + 0];
-            maxent = std::max(maxent, hx.h_idxptr[tx + lay_h[l].nx] - hx.h_idxptr[tx]);
-        }
-    for (int t = 0; t < ntiles; t++) {
-        const TileDesc &T = tl[t];
-        for (int w = 0; w < nwfs; w++) {
-            const int ty = hx.h_ptr[(w * nps + T.l) * 2 + 1];
-            int lo = INT32_MAX, hi = -1;
-            for (int jy = T.jy0; jy < T.jy0 + T.ny; jy++)
-                for (int a = hx.h_idxptr[ty + jy]; a < hx.h_idxptr[ty + jy + 1]; a++) {
-                    lo = std::min(lo, hx.h_ent[a].i);
-                    hi = std::max(hi, hx.h_ent[a].i);
-                }
-            rr[(size_t)t * nwfs + w] = hi < 0 ? make_int2(1, 0) : make_int2(lo, hi);
-            if (hi >= 0) maxrows = std::max(maxrows, hi - lo + 1);
-        }
+// Fixed-width copies of the transposed x and y lists of every (WFS, layer),
+// padded with (index 0, weight 0) after the real entries, and the pupil-row
+// blocking of k_pupil_rows.
+void Recon::build_pad() {
+    maxnx = maxny = 0;
+    for (int l = 0; l < nps; l++) {
+        maxnx = std::max(maxnx, lay_h[l].nx);
+        maxny = std::max(maxny, lay_h[l].ny);
     }
-    tiles.upload(tl);
-    rowrange.upload(rr);
-    hxt_smem = (size_t)maxrows * maxnx * 4 + (size_t)((maxnx + 2) & ~1) * 4 + (size_t)maxent * sizeof(GatherW);
-    MB_REQUIRE(hxt_smem <= 200 * 1024, "Hx^T tile needs %zu bytes of shared memory", hxt_smem);
-    MB_CUDA_TRY(cudaFuncSetAttribute(k_hxt_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hxt_smem));
+    kx = ky = 1;
+    for (int w = 0; w < nwfs; w++)
+        for (int l = 0; l < nps; l++)
+            for (int axis = 0; axis < 2; axis++) {
+                const int tb = hx.h_ptr[(w * nps + l) * 2 + axis];
+                const int n = axis ? lay_h[l].ny : lay_h[l].nx;
+                int &K = axis ? ky : kx;
+                for (int j = 0; j < n; j++) K = std::max(K, hx.h_idxptr[tb + j + 1] - hx.h_idxptr[tb + j]);
+            }
+    MB_REQUIRE(nps <= kMaxLayers, "at most %d reconstructed layers (%d)", kMaxLayers, nps);
+    MB_REQUIRE(kx <= kMaxPadX, "transposed x lists wider than %d (%d)", kMaxPadX, kx);
+    MB_REQUIRE(ky <= kMaxPadY, "transposed y lists wider than %d (%d)", kMaxPadY, ky);
+    MB_REQUIRE(nxp <= kThreads, "pupil grid wider than %d (%d)", kThreads, nxp);
+    std::vector<GatherW> xp((size_t)nwfs * ncols * kx, GatherW{0, 0.f});
+    std::vector<GatherW> yp((size_t)nwfs * nps * maxny * ky, GatherW{0, 0.f});
+    for (int w = 0; w < nwfs; w++)
+        for (int l = 0; l < nps; l++)
+            for (int axis = 0; axis < 2; axis++) {
+                const int tb = hx.h_ptr[(w * nps + l) * 2 + axis];
+                const int n = axis ? lay_h[l].ny : lay_h[l].nx;
+                for (int j = 0; j < n; j++) {
+                    GatherW *d = axis ? yp.data() + ((size_t)(w * nps + l) * maxny + j) * ky
+                                      : xp.data() + ((size_t)w * ncols + lay_h[l].tcol + j) * kx;
+                    for (int a = hx.h_idxptr[tb + j], k = 0; a < hx.h_idxptr[tb + j + 1]; a++, k++) d[k] = hx.h_ent[a];
+                }
+            }
+    xpad.upload(xp);
+    ypad.upload(yp);
+    // pupil rows per CTA: the largest of 16, 8, 4 that still gives about two
+    // waves of 256-thread CTAs on 148 SMs (4 resident each)
+    prows = 16;
+    while (prows > 4 && (long)((nyp + prows - 1) / prows) * nwfs * nb < 2 * 148 * 4) prows /= 2;
+    if (const char *e = std::getenv("MAOS_B200_PUPIL_ROWS")) {  // tuning override
+        const int v = std::atoi(e);
+        if (v >= 1 && v <= 64) prows = v;
+    }
+    ptiles = (nyp + prows - 1) / prows;
+    tw = (long)nyp * ncols;
+    pupil_smem = (size_t)pupil_rows_smem_floats(prows, nxp, nps, ncols, kx) * sizeof(float);
+    MB_REQUIRE(pupil_smem <= 200 * 1024, "pupil row block needs %zu bytes of shared memory", pupil_smem);
+    for (auto k : {k_pupil_rows<true, 1>, k_pupil_rows<true, 2>, k_pupil_rows<false, 1>, k_pupil_rows<false, 2>})
+        MB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pupil_smem));
+}
+
+// Launch k_pupil_rows over every WFS: one launch per run of consecutive WFS
+// with the same subaperture/pupil ratio.
+void Recon::pupil_rows(bool from_x, const float *xin, cudaStream_t s) {
+    for (int w0 = 0; w0 < nwfs;) {
+        int w1 = w0 + 1;
+        while (w1 < nwfs && wfs_h[w1].pos == wfs_h[w0].pos) w1++;
+        const bool p2 = wfs_h[w0].pos == 2;
+        auto kern = from_x ? (p2 ? k_pupil_rows<true, 2> : k_pupil_rows<true, 1>)
+                           : (p2 ? k_pupil_rows<false, 2> : k_pupil_rows<false, 1>);
+        kern<<<dim3(ptiles, w1 - w0, nb), kThreads, pupil_smem, s>>>(
+            xin, grad.p, tt.p, tbuf.p, hx.fwd.p, lay.p, wfs.p, pad(), w0, nps, nwfs, nxp, nyp, nxtot, ngrad, tw,
+            ncols, prows, from_x ? 0 : 1, act());
+        MB_CHECK_LAUNCH();
+        w0 = w1;
+    }
+}
+
+// k_hxt_rows at the padded y-list width.
+void Recon::hxt_rows(const float *xin, float *out, double *dot_part, int do_l2, int k, cudaStream_t s) {
+    using K = void (*)(const float *, const float *, float *, double *, PadIndex, const LayerDev *, int, int, int,
+                       long, long, int, CgScal, int, const int *);
+    static const K tabk[kMaxPadY] = {k_hxt_rows<1>, k_hxt_rows<2>, k_hxt_rows<3>, k_hxt_rows<4>,
+                                     k_hxt_rows<5>, k_hxt_rows<6>, k_hxt_rows<7>, k_hxt_rows<8>};
+    tabk[ky - 1]<<<dim3(nblk_x, nb), kThreads, 0, s>>>(tbuf.p, xin, out, dot_part, pad(), lay.p, nps, nwfs, nyp,
+                                                        nxtot, tw, do_l2, scal(), k, act());
+    MB_CHECK_LAUNCH();
 }
 
 void Recon::build_wfs_tables(const mb_recon_desc *d) {
@@ -590,6 +631,8 @@ void Recon::build(const mb_recon_desc *d) {
         lay_h[l].nx = g.nx;
         lay_h[l].ny = g.ny;
         lay_h[l].off = xoff[l];
+        lay_h[l].tcol = ncols;
+        ncols += g.nx;
         xoff[l + 1] = xoff[l] + (long)g.nx * g.ny;
     }
     nxtot = xoff[nps];
@@ -605,7 +648,7 @@ void Recon::build(const mb_recon_desc *d) {
     ngrad = goff[nwfs];
     set_l2c(d->l2c);
     build_hx_tables(d);
-    build_tiles();
+    build_pad();
     build_wfs_tables(d);
     nblk_x = (int)nblocks(nxtot);
     nblk_tt = (int)nblocks(nsamax);
@@ -613,11 +656,11 @@ void Recon::build(const mb_recon_desc *d) {
     const size_t NX = (size_t)nb * nxtot;
     x.alloc(NX); r.alloc(NX); p.alloc(NX); z.alloc(NX); Ap.alloc(NX); rhs.alloc(NX);
     opd.alloc((size_t)nb * nwfs * np);
-    opd2.alloc((size_t)nb * nwfs * np);
+    tbuf.alloc((size_t)nb * nwfs * tw);
     grad.alloc((size_t)nb * ngrad);
     gin.alloc((size_t)nb * ngrad);
     tt_part.alloc((size_t)nb * nwfs * nblk_tt * 2);
-    pap_part.alloc((size_t)nb * std::max(nblk_x, ntiles));
+    pap_part.alloc((size_t)nb * nblk_x);
     rr_part.alloc((size_t)nb * nblk_x);
     rz_part.alloc((size_t)nb * nblk_x);
     bb_part.alloc((size_t)nb * nblk_x);
@@ -661,31 +704,22 @@ void Recon::op_rhs(const float *g, float *out, cudaStream_t s) {
     k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, s>>>(nullptr, g, grad.p, tt_part.p, wfs.p, nwfs,
                                                       nxp, np, ngrad, 1, tt.p, cnt_tt.p, act());
     MB_CHECK_LAUNCH();
-    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt.p, opd2.p, wfs.p, nwfs, nxp, nyp,
-                                                          ngrad, 1, 1.f, act());
-    MB_CHECK_LAUNCH();
-    k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, s>>>(opd2.p, nullptr, out, nullptr, hx.gi(), lay.p,
-                                                            tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
-                                                            nxtot, 0, 1.f, maxrows, maxnx, maxent,
-                                                            scal(), 0, act());
-    MB_CHECK_LAUNCH();
+    pupil_rows(false, nullptr, s);
+    hxt_rows(nullptr, out, nullptr, 0, 0, s);
 }
 
 void Recon::op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t s, int k) {
     // TomoL: Hx^T GP^T NEA^-1 (I - TT PTT) GP Hx x + L2^T L2 x   (recon_utils.c:447, tomo.cu:639)
-    op_hx(xin, s);
-    const int do_tt = split ? 0 : 1;
-    k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, s>>>(opd.p, nullptr, grad.p, tt_part.p, wfs.p,
-                                                      nwfs, nxp, np, ngrad, do_tt, tt.p, cnt_tt.p, act());
-    MB_CHECK_LAUNCH();
-    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, s>>>(grad.p, tt.p, opd2.p, wfs.p, nwfs, nxp, nyp,
-                                                          ngrad, do_tt, 1.f, act());
-    MB_CHECK_LAUNCH();
-    k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, s>>>(opd2.p, xin, out, dot_part, hx.gi(), lay.p,
-                                                            tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
-                                                            nxtot, 1, 1.f, maxrows, maxnx, maxent,
-                                                            scal(), k, act());
-    MB_CHECK_LAUNCH();
+    if (split) {  // no tip/tilt term: Hx, GP, NEA, GP^T fused per pupil-row block
+        pupil_rows(true, xin, s);
+    } else {      // the tip/tilt projection needs every gradient of a WFS first
+        op_hx(xin, s);
+        k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, s>>>(opd.p, nullptr, grad.p, tt_part.p, wfs.p,
+                                                          nwfs, nxp, np, ngrad, 1, tt.p, cnt_tt.p, act());
+        MB_CHECK_LAUNCH();
+        pupil_rows(false, nullptr, s);
+    }
+    hxt_rows(xin, out, dot_part, 1, k, s);
 }
 
 void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s, int k, int init,
@@ -889,84 +923,60 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     cudaEvent_t e0, e1;
     MB_CUDA_TRY(cudaEventCreate(&e0));
     MB_CUDA_TRY(cudaEventCreate(&e1));
-    const double B = nb, F = 4.0, D = 8.0;
-    const double gp_tab = 0;  // per-WFS stencil tables, counted below
-    (void)gp_tab;
-    double tab_gp = 0, tab_gpt = 0;
+    const double B = nb, F = 4.0;
+    double tab_wfs = 0;  // stencil coefficients, NEA, corner map
     for (int w = 0; w < nwfs; w++) {
         const int n1 = wfs_h[w].pos + 1;
-        tab_gp += nsa[w] * (8.0 + 8.0 * n1 * n1 + 16.0);              // saptr, coefs, ptt
-        tab_gpt += nsa[w] * (8.0 * n1 * n1 + 12.0) + 4.0 * np;       // coefs, neai, samap
+        tab_wfs += nsa[w] * (8.0 * n1 * n1 + 12.0) + 4.0 * np;
     }
-    const double nxw = (double)nwfs * np;
-    const double ngr = (double)ngrad;
     const double nx = (double)nxtot;
-    const double gather = (double)hx.ent.n * 8.0 + (double)hx.idxptr.n * 4.0;
+    const double trow = (double)nwfs * tw;  // row-buffer floats per instance
     const double nbk = (double)fd_nbh * fd_bs;
     double nh = 0;  // half-spectrum bins per instance
     for (int l = 0; l < nps; l++) nh += (double)lay_h[l].ny * (lay_h[l].nx / 2 + 1);
-    // bytes per launch: operands read + written once
-    double by[9] = {
-        B * (F * nx + F * nxw) + (double)hx.fwd.n * 12.0,             // hx: x -> opd
-        B * (F * nxw + F * ngr + D * 2 * nwfs * nblk_tt) + tab_gp,     // gp: opd -> grad
-        B * (F * ngr + F * nxw) + tab_gpt,                             // gpt: grad -> opd2
-        B * (F * nxw + 2 * F * nx) + gather,                           // hxt: opd2, p -> Ap
+    // bytes per launch: each operand read or written once (the row buffer is
+    // an operand of both halves; the halo rows of the pupil blocks are not)
+    double by[7] = {
+        B * (F * nx + F * trow) + (double)hx.fwd.n * 12.0 + tab_wfs + (double)xpad.n * 8.0,  // x -> t
+        B * (F * trow + 2 * F * nx) + (double)ypad.n * 8.0,                                // t, p -> Ap
         B * (5 * F * nx),                                              // x,r,p,Ap r/w
         B * (3 * F * nx),                                              // p,z -> p
         B * (F * nx + 8.0 * nh),                                       // r -> half spectra
         B * (16.0 * nbk) + 8.0 * nbk * fd_bs + 16.0 * nbk,             // spec, spec2, M, idx
         B * (8.0 * nh + 2 * F * nx)};                                  // half spectra, r -> z
-    const int lps[9] = {maxit + 1, maxit + 2, maxit + 2, maxit + 2, maxit, maxit,
-                        precond ? maxit : 0, precond ? maxit : 0, precond ? maxit : 0};
-    GatherIndex gi = hx.gi();
+    const int lps[7] = {maxit + 2, maxit + 2, maxit, maxit, precond ? maxit : 0, precond ? maxit : 0,
+                        precond ? maxit : 0};
     for (int st = 0; st < ns; st++) {
         bytes[st] = by[st];
         launches[st] = lps[st];
         ms[st] = 0.f;
-        if (st >= 6 && !precond) continue;
+        if (st >= 4 && !precond) continue;
         auto launch = [&]() {
             switch (st) {
-                case 0: op_hx(p.p, stream); break;
-                case 1:
-                    k_gp<<<dim3(nblk_tt, nwfs, nb), kThreads, 0, stream>>>(opd.p, nullptr, grad.p, tt_part.p,
-                                                                          wfs.p, nwfs, nxp, np, ngrad, 1, tt.p,
-                                                                          cnt_tt.p, act());
-                    MB_CHECK_LAUNCH();
-                    break;
+                case 0: pupil_rows(true, p.p, stream); break;
+                case 1: hxt_rows(p.p, Ap.p, pap_part.p, 1, 0, stream); break;
                 case 2:
-                    k_gpt<<<dim3(nblocks(np), nwfs, nb), kThreads, 0, stream>>>(grad.p, tt.p, opd2.p,
-                                                                               wfs.p, nwfs, nxp, nyp, ngrad, 1,
-                                                                               1.f, act());
-                    MB_CHECK_LAUNCH();
-                    break;
-                case 3:
-                    k_hxt_tiled<<<dim3(ntiles, nb), kThreads, hxt_smem, stream>>>(
-                        opd2.p, p.p, Ap.p, pap_part.p, gi, lay.p, tiles.p, rowrange.p, nps, nwfs, nxp, nyp,
-                        nxtot, 1, 1.f, maxrows, maxnx, maxent, scal(), 0, act());
-                    MB_CHECK_LAUNCH();
-                    break;
-                case 4:
                     // alpha reads the current scalars; the vectors are scratch here
                     // the vectors are scratch here (x, r -> z, rhs)
                     k_cg_update_xr<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(z.p, rhs.p, p.p, Ap.p, rr_part.p,
                                                                              nxtot, scal(), 0, maxit, 0, act());
                     MB_CHECK_LAUNCH();
                     break;
-                case 5:
+                case 3:
                     k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(rhs.p, z.p, nxtot, scal(), 0, act());
                     MB_CHECK_LAUNCH();
                     break;
-                case 6:
+                case 4:
                     k_fd_fwd<<<dim3(nps, nb), kThreads, fd_smem, stream>>>(r.p, spec.p, fd_lay.p, fd_tw.p, nxtot,
                                                                            fd_bufn, act());
                     MB_CHECK_LAUNCH();
                     break;
-                case 7:
+                case 5:
                     k_fd_mul<<<dim3((fd_nbh + kThreads / fd_bs - 1) / (kThreads / fd_bs), nb), kThreads, 0,
                                stream>>>(spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh, fd_bs, act());
                     MB_CHECK_LAUNCH();
                     break;
-                case 8:
+                case 6:
                     k_fd_inv<<<dim3(nps, nb), kThreads, fd_smem, stream>>>(spec2.p, r.p, z.p, rz_part.p, fd_lay.p,
                                                                            fd_tw.p, nxtot, fd_bufn, CgScal{}, 0, 0,
                                                                            act());
@@ -1271,7 +1281,7 @@ int mb_apply_fit_L(mb_recon *h, const double *ain, double *aout) {
 
 void *mb_recon_stream(mb_recon *h) { return h ? (void *)h->R.stream : nullptr; }
 
-static const char *kStageNames[] = {"hx", "gp", "gpt", "hxt_l2", "cg_update_xr", "cg_update_p",
+static const char *kStageNames[] = {"lhs_pupil", "lhs_layer", "cg_update_xr", "cg_update_p",
                                     "fd_fwd", "fd_mul", "fd_inv"};
 int mb_num_stages(void) { return (int)(sizeof(kStageNames) / sizeof(kStageNames[0])); }
 const char *mb_stage_name(int i) { return (i >= 0 && i < mb_num_stages()) ? kStageNames[i] : ""; }

@@ -6,11 +6,14 @@
 // writes one FP64 partial, and consumers add the partials in a fixed order.
 //
 // Reference counterparts (cuda/tomo.cu, cuda/prop_wrap.cu, cuda/pcg.cu):
-//   k_hx        gpu_map2map_do forward (prop_wrap.cu:35)      -- bilinear gather
-//   k_gp        gpu_gp_do (tomo.cu:362)                       -- GP stencil + TT sums
-//   k_gpt       gpu_gpt_do (tomo.cu:485)                      -- gather form, no atomics
-//   k_hxt       gpu_map2map_do 't' + gpu_laplacian_do         -- gather form, no atomics
-//   k_cg_*      gpu_pcg scalar kernels (pcg.cu:27-57)         -- FP64 scalars
+//   k_hx          gpu_map2map_do forward (prop_wrap.cu:35)    -- bilinear gather
+//   k_gp          gpu_gp_do (tomo.cu:362)                     -- GP stencil + TT sums
+//   k_pupil_rows  gpu_map2map_do + gpu_gp_do + gpu_gpt_do (tomo.cu:485) + the x half
+//                 of gpu_map2map_do 't', fused per block of pupil rows
+//   k_hxt_rows    y half of gpu_map2map_do 't' + gpu_laplacian_do (tomo.cu:317)
+//   k_hxt         gpu_map2map_do 't' in gather form (DM fit)  -- no atomics
+//   k_fd_*        cufdpcg_t::P (fdpcg.cu:168)                 -- own FFTs, half spectrum
+//   k_cg_*        gpu_pcg scalar kernels (pcg.cu:27-57)       -- FP64 scalars
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -48,6 +51,7 @@ struct LayerDev {
     int nx, ny;
     long off;       // offset inside one instance
     float l2c;      // biharmonic weight
+    int tcol;       // first column of this layer in the row buffer of the separable Hx^T
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -224,48 +228,6 @@ __global__ void k_gp(const float *__restrict__ opd, const float *__restrict__ gi
 }
 
 // ---------------------------------------------------------------------------
-// GP^T NEA^-1 (I - TT PTT) in gather form: each pupil point collects from the
-// (pos+1)^2 subapertures whose stencil covers it.
-// grid: (ceil(np/256), nwfs, nb)
-// ---------------------------------------------------------------------------
-__global__ void k_gpt(const float *__restrict__ grad, const float *__restrict__ tt,
-                      float *__restrict__ opd2, const WfsDev *__restrict__ wfs, int nwfs,
-                      int nxp, int nyp, long ngrad, int do_tt, float alpha,
-                      const int *__restrict__ act) {
-    if (inactive(act, blockIdx.z)) return;
-    const int w = blockIdx.y, b = blockIdx.z;
-    const WfsDev W = wfs[w];
-    const bool use_tt = do_tt && W.has_ptt;
-    const int np = nxp * nyp;
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
-    const int px = p % nxp, py = p / nxp;
-    const int n1 = W.pos + 1;
-    const float *g = grad + (size_t)b * ngrad + W.goff;
-    const float ttx = use_tt ? tt[((size_t)b * nwfs + w) * 2] : 0.f;
-    const float tty = use_tt ? tt[((size_t)b * nwfs + w) * 2 + 1] : 0.f;
-    float acc = 0.f;
-    for (int dy = 0; dy < n1; dy++) {
-        const int cy = py - dy;
-        if (cy < 0) break;
-        for (int dx = 0; dx < n1; dx++) {
-            const int cx = px - dx;
-            if (cx < 0) break;
-            const int s = W.samap[cy * nxp + cx];
-            if (s < 0) continue;
-            const float gx = g[s] + ttx;
-            const float gy = g[s + W.nsa] + tty;
-            const float *ne = W.neai + 3 * s;
-            const float nx_ = ne[0] * gx + ne[2] * gy;
-            const float ny_ = ne[2] * gx + ne[1] * gy;
-            const float2 k = W.gp[(size_t)s * n1 * n1 + dy * n1 + dx];
-            acc += k.x * nx_ + k.y * ny_;
-        }
-    }
-    opd2[((size_t)b * nwfs + w) * np + p] = alpha * acc;
-}
-
-// ---------------------------------------------------------------------------
 // Hx^T in gather form (+ L2^T L2 regularisation and p.Ap partial for the LHS).
 // Layer points are flattened over all layers; grid: (nblk_x, nb).
 // The transposed table for (w, l, axis) is a CSR list per layer column/row.
@@ -374,108 +336,253 @@ __global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// Tiled Hx^T (+ L2^T L2 and p.Ap partials) for the tomography.
-// One CTA = one instance x one tile of `ny` consecutive rows of one layer.
-// The bilinear transpose is separable, so per WFS the CTA
-//   1. stages that WFS's x-gather lists for the layer in shared memory,
-//   2. x pass: t[iy][jx] = sum_x w * opd2[iy][ix] for the pupil rows that
-//      reach the tile (coalesced reads along each pupil row),
-//   3. y pass: acc[jy][jx] += sum_y w * t[iy][jx] into registers.
-// grid: (ntiles, nb); dynamic smem: maxrows*maxnx floats + lists.
+// Tomography normal-equation operator in two kernels.
+//
+// The bilinear transpose Hx^T is separable: for WFS w and layer l,
+//   (Hx^T o)[jy][jx] = sum_{iy in Y(jy)} wy * sum_{ix in X(jx)} wx * o[iy][ix].
+// k_pupil_rows works on a block of pupil rows of one (instance, WFS): it
+// forms the pupil OPD (Hx, with a halo of `pos` rows), the NEA-weighted
+// gradients (GP, NEA) and GP^T of them entirely in shared memory, then
+// applies the x half of every layer's transpose and writes the partial
+// sums t[w][l][iy][jx] (coalesced).  k_hxt_rows then finishes each layer
+// point with the y half over all WFS, adds L2^T L2 x and the p.Ap partial.
+// The transposed lists are stored with a fixed width (padding: weight 0 on
+// pupil index 0), in the same order as the CSR lists, so the sums are the
+// exact adjoint of Hx and independent of the tiling.
 // ---------------------------------------------------------------------------
-struct TileDesc {
-    int l;     // layer
-    int jy0;   // first layer row
-    int ny;    // rows in this tile
+struct PadIndex {
+    const GatherW *x;   // [(w*ncols + tcol_l + jx)*kx + e]   (per WFS, all layers' columns)
+    const GatherW *y;   // [((w*nps + l)*maxny + jy)*ky + e]
+    int kx, ky, maxnx, maxny;
 };
-constexpr int kMaxOwn = 8;  // layer points per thread (tile rows * nx <= 256 * kMaxOwn)
 
-__global__ void __launch_bounds__(kThreads)
-k_hxt_tiled(const float *__restrict__ opd2, const float *__restrict__ xin, float *__restrict__ out,
-            double *__restrict__ dot_part, GatherIndex gi, const LayerDev *__restrict__ lay,
-            const TileDesc *__restrict__ tiles, const int2 *__restrict__ rowrange, int nps, int nwfs,
-            int nxp, int nyp, long nxtot, int do_l2, float alpha, int maxrows, int maxnx,
-            int maxent, CgScal S, int kit, const int *__restrict__ act) {
-    if (inactive(act, blockIdx.y)) return;
-    extern __shared__ float smem[];
-    __shared__ double sh[32];
-    const int tid = blockIdx.x, b = blockIdx.y;
-    const TileDesc T = tiles[tid];
-    const LayerDev L = lay[T.l];
-    const int nx = L.nx;
-    const int nown = T.ny * nx;
-    float *t = smem;
-    int *xptr = reinterpret_cast<int *>(t + (size_t)maxrows * maxnx);
-    GatherW *xent = reinterpret_cast<GatherW *>(xptr + ((maxnx + 2) & ~1));
-    const int np = nxp * nyp;
-    float acc[kMaxOwn];
-#pragma unroll
-    for (int k = 0; k < kMaxOwn; k++) acc[k] = 0.f;
-    for (int w = 0; w < nwfs; w++) {
-        const int2 rr = rowrange[(size_t)tid * nwfs + w];
-        if (rr.y < rr.x) continue;  // uniform over the CTA
-        const int tx = gi.ptr[(w * nps + T.l) * 2 + 0];
-        const int ty = gi.ptr[(w * nps + T.l) * 2 + 1];
-        const int e0 = gi.idx_ptr[tx];
-        const int ne = gi.idx_ptr[tx + nx] - e0;
-        for (int i = threadIdx.x; i <= nx; i += blockDim.x) xptr[i] = gi.idx_ptr[tx + i] - e0;
-        for (int i = threadIdx.x; i < ne && i < maxent; i += blockDim.x) xent[i] = gi.ent[e0 + i];
-        __syncthreads();
-        const int nr = rr.y - rr.x + 1;
-        const float *o = opd2 + ((size_t)b * nwfs + w) * np + (size_t)rr.x * nxp;
-        for (int idx = threadIdx.x; idx < nr * nx; idx += blockDim.x) {
-            const int r = idx / nx, jx = idx - r * nx;
-            float sx = 0.f;
-            for (int e = xptr[jx]; e < xptr[jx + 1]; e++) {
-                const GatherW ge = xent[e];
-                sx += ge.w * o[(size_t)r * nxp + ge.i];
-            }
-            t[r * maxnx + jx] = sx;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < kMaxOwn; k++) {
-            const int oi = threadIdx.x + k * kThreads;
-            if (oi < nown) {
-                const int jy = T.jy0 + oi / nx, jx = oi % nx;
-                const int a0 = gi.idx_ptr[ty + jy], a1 = gi.idx_ptr[ty + jy + 1];
-                float sy = 0.f;
-                for (int a = a0; a < a1; a++) {
-                    const GatherW ge = gi.ent[a];
-                    sy += ge.w * t[(ge.i - rr.x) * maxnx + jx];
-                }
-                acc[k] += sy;
+constexpr int kMaxLayers = 8;   // layers unrolled in the Hx gather
+constexpr int kMaxPadX = 8;     // widest x list
+constexpr int kMaxPadY = 8;     // widest y list (k_hxt_rows is instantiated up to this)
+
+// Dynamic shared memory of k_pupil_rows, in floats, for `rows` output rows.
+__host__ __device__ constexpr int pupil_rows_smem_floats(int rows, int nxp, int nps, int ncols, int kx) {
+    return nxp * (3 * (rows + 2) + rows + (rows + 4))      // wg, sid, opd2, opd
+           + 3 * nps * (nxp + rows + 4)                     // staged Hx axis tables
+           + 2 * ncols * kx;                                // staged x lists of the WFS
+}
+
+// grid: (ceil(nyp/rows), nw, nb), WFS w = wbase + blockIdx.y, all with
+// subaperture/pupil ratio POS.  FROM_X: the operator input is the layer
+// vector x (Hx, GP in shared memory; no tip/tilt term).  Otherwise the input
+// is a gradient vector already in `grad` (right-hand side, or the LHS with
+// the tip/tilt projection), with -PTT g per WFS in `tt` when do_tt.
+// Thread layout: each thread owns one pupil column (and a phase of the rows)
+// for the pupil-grid stages and whole layer columns for the x half of Hx^T,
+// so per-item index arithmetic is a few adds; index tables are staged in
+// shared memory and a pupil point's layer taps are issued together.
+template <bool FROM_X, int POS>
+__global__ void __launch_bounds__(kThreads, 4)
+k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const float *__restrict__ tt,
+             float *__restrict__ t, const AxisW *__restrict__ tab, const LayerDev *__restrict__ lay,
+             const WfsDev *__restrict__ wfs, PadIndex pi, int wbase, int nps, int nwfs, int nxp, int nyp,
+             long nxtot, long ngrad, long tw, int ncols, int rows, int do_tt,
+             const int *__restrict__ act) {
+    constexpr int N1 = POS + 1;
+    const int w = wbase + blockIdx.y, b = blockIdx.z;
+    if (inactive(act, b)) return;
+    extern __shared__ float sm[];
+    __shared__ int s_lnx[kMaxLayers], s_tcol[kMaxLayers + 1];
+    __shared__ long s_loff[kMaxLayers];
+    const WfsDev W = wfs[w];
+    const int r0 = blockIdx.x * rows;
+    const int r1 = min(nyp, r0 + rows);      // output pupil rows [r0, r1)
+    const int ca = max(0, r0 - POS);         // subaperture corner rows [ca, cb)
+    const int cb = min(nyp - POS, r1);
+    const int nh = cb + POS - ca;            // pupil rows of the Hx halo block
+    const int cr = rows + 2;
+    const int ts = nxp + rows + 4;           // staged axis entries per layer
+    float2 *s_wg = reinterpret_cast<float2 *>(sm);                  // [cr][nxp]
+    int *s_sid = reinterpret_cast<int *>(sm + 2 * cr * nxp);         // [cr][nxp]
+    float *s_opd2 = sm + 3 * cr * nxp;                               // [rows][nxp]
+    float *s_opd = s_opd2 + rows * nxp;                              // [rows+4][nxp]
+    AxisW *s_tab = reinterpret_cast<AxisW *>(s_opd + (rows + 4) * nxp);  // [nps][ts]
+    GatherW *s_xp = reinterpret_cast<GatherW *>(reinterpret_cast<float *>(s_tab) + 3 * nps * ts);
+    const int nph = blockDim.x / nxp;        // row phases (nxp <= blockDim)
+    const int ph = threadIdx.x / nxp, ix = threadIdx.x - ph * nxp;
+    const bool colthr = ph < nph;
+
+    // stage the layer geometry, the x lists of this WFS and, for Hx, the axis tables
+    if (threadIdx.x < nps) {
+        const LayerDev L = lay[threadIdx.x];
+        s_lnx[threadIdx.x] = L.nx;
+        s_loff[threadIdx.x] = L.off;
+        s_tcol[threadIdx.x] = L.tcol;
+    }
+    if (threadIdx.x == 0) s_tcol[nps] = ncols;
+    {
+        const GatherW *src = pi.x + (size_t)w * ncols * pi.kx;
+        for (int i = threadIdx.x; i < ncols * pi.kx; i += blockDim.x) s_xp[i] = src[i];
+        if (FROM_X) {
+            const AxisW *tw0 = tab + (size_t)w * nps * (nxp + nyp);
+            for (int l = 0; l < nps; l++) {
+                const AxisW *tl = tw0 + (size_t)l * (nxp + nyp);
+                for (int i = threadIdx.x; i < nxp + nh; i += blockDim.x)
+                    s_tab[l * ts + i] = tl[i < nxp ? i : nxp + ca + (i - nxp)];
             }
         }
         __syncthreads();
     }
-    const float *X = xin ? xin + (size_t)b * nxtot + L.off : nullptr;
-    double dotv = 0;
+    if (FROM_X) {  // Hx for pupil rows [ca, cb + POS): a point's layer taps are issued together
+        const float *xb = x + (size_t)b * nxtot;
+        if (colthr)
+            for (int r = ph; r < nh; r += nph) {
+                float acc = 0.f;
 #pragma unroll
-    for (int k = 0; k < kMaxOwn; k++) {
-        const int oi = threadIdx.x + k * kThreads;
-        if (oi < nown) {
-            const int jy = T.jy0 + oi / nx, jx = oi % nx;
-            float v = alpha * acc[k];
-            if (do_l2) {
-                const int ny_ = L.ny;
-                auto at = [&](int dx, int dy) {
-                    int xx = jx + dx, yy = jy + dy;
-                    xx += (xx < 0) ? nx : 0;
-                    xx -= (xx >= nx) ? nx : 0;
-                    yy += (yy < 0) ? ny_ : 0;
-                    yy -= (yy >= ny_) ? ny_ : 0;
-                    return X[yy * nx + xx];
-                };
-                const float st = 20.f * at(0, 0) - 8.f * (at(-1, 0) + at(1, 0) + at(0, -1) + at(0, 1)) +
-                                 2.f * (at(-1, -1) + at(1, -1) + at(-1, 1) + at(1, 1)) +
-                                 (at(0, -2) + at(-2, 0) + at(2, 0) + at(0, 2));
-                v += alpha * L.l2c * st;
+                for (int l = 0; l < kMaxLayers; l++) {
+                    if (l < nps) {
+                        const AxisW tx = s_tab[l * ts + ix], ty = s_tab[l * ts + nxp + r];
+                        const bool ok = tx.k >= 0 && ty.k >= 0;
+                        const int nx = s_lnx[l];
+                        const float *X = xb + s_loff[l] + (ok ? ty.k * nx + tx.k : 0);
+                        const float a = tx.w0 * X[0] + tx.w1 * X[1];
+                        const float c = tx.w0 * X[nx] + tx.w1 * X[nx + 1];
+                        if (ok) acc += ty.w0 * a + ty.w1 * c;
+                    }
+                }
+                s_opd[r * nxp + ix] = acc;
             }
-            const long j = L.off + (long)jy * nx + jx;
-            out[(size_t)b * nxtot + j] = v;
-            if (dot_part && X) dotv += (double)v * (double)X[jy * nx + jx];
+        __syncthreads();
+    }
+    {  // NEA-weighted gradients of the subapertures with corners in rows [ca, cb)
+        const float *g = FROM_X ? nullptr : grad + (size_t)b * ngrad + W.goff;
+        const bool use_tt = !FROM_X && do_tt && W.has_ptt;
+        const float ttx = use_tt ? tt[((size_t)b * nwfs + w) * 2] : 0.f;
+        const float tty = use_tt ? tt[((size_t)b * nwfs + w) * 2 + 1] : 0.f;
+        if (colthr)
+            for (int rr = ph; rr < cb - ca; rr += nph) {
+                const int i = rr * nxp + ix;
+                const int s = __ldg(W.samap + (ca + rr) * nxp + ix);
+                s_sid[i] = s;
+                if (s < 0) continue;
+                const float *ne = W.neai + 3 * s;
+                const float n0 = ne[0], n1_ = ne[1], n2 = ne[2];
+                float gx = 0.f, gy = 0.f;
+                if (FROM_X) {
+                    const float2 *cf = W.gp + (size_t)s * N1 * N1;
+                    float2 k[N1 * N1];
+#pragma unroll
+                    for (int q = 0; q < N1 * N1; q++) k[q] = cf[q];
+                    const float *o = s_opd + i;
+#pragma unroll
+                    for (int ty = 0; ty < N1; ty++)
+#pragma unroll
+                        for (int tx = 0; tx < N1; tx++) {
+                            const float v = o[ty * nxp + tx];
+                            gx += k[ty * N1 + tx].x * v;
+                            gy += k[ty * N1 + tx].y * v;
+                        }
+                } else {
+                    gx = g[s] + ttx;
+                    gy = g[s + W.nsa] + tty;
+                }
+                s_wg[i] = make_float2(n0 * gx + n2 * gy, n2 * gx + n1_ * gy);
+            }
+        __syncthreads();
+    }
+    if (colthr) {  // GP^T for the output rows (gather over the covering subapertures)
+        for (int pr = ph; pr < r1 - r0; pr += nph) {
+            const int py = r0 + pr;
+            float2 k[N1 * N1], v[N1 * N1];
+#pragma unroll
+            for (int dy = 0; dy < N1; dy++)
+#pragma unroll
+                for (int dx = 0; dx < N1; dx++) {
+                    const int cy = py - dy, cx = ix - dx;
+                    const int q = dy * N1 + dx;
+                    const bool in = cy >= ca && cy < cb && cx >= 0;
+                    const int j = in ? (cy - ca) * nxp + cx : 0;
+                    const int s = in ? s_sid[j] : -1;
+                    k[q] = s >= 0 ? W.gp[(size_t)s * N1 * N1 + q] : make_float2(0.f, 0.f);
+                    v[q] = s >= 0 ? s_wg[j] : make_float2(0.f, 0.f);
+                }
+            float acc = 0.f;
+#pragma unroll
+            for (int q = 0; q < N1 * N1; q++) acc += k[q].x * v[q].x + k[q].y * v[q].y;
+            s_opd2[pr * nxp + ix] = acc;
         }
+    }
+    __syncthreads();
+    {  // x half of Hx^T for every layer: t[w][l][iy][jx]; a thread owns whole layer columns
+        float *tb = t + (size_t)(b * nwfs + w) * tw;
+        const int kx = pi.kx, nr = r1 - r0;
+        for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+            int l = 0;
+            while (l + 1 < nps && c >= s_tcol[l + 1]) l++;
+            const int tc = s_tcol[l], lnx = s_lnx[l];
+            GatherW e[kMaxPadX];
+#pragma unroll
+            for (int k = 0; k < kMaxPadX; k++) e[k] = k < kx ? s_xp[c * kx + k] : GatherW{0, 0.f};
+            float *dst = tb + (size_t)nyp * tc + (size_t)r0 * lnx + (c - tc);
+            for (int r = 0; r < nr; r++) {
+                const float *o = s_opd2 + r * nxp;
+                float sx = 0.f;
+#pragma unroll
+                for (int k = 0; k < kMaxPadX; k++)
+                    if (k < kx) sx += e[k].w * o[e[k].i];
+                dst[r * lnx] = sx;
+            }
+        }
+    }
+}
+
+// y half of Hx^T over all WFS, + L2^T L2 x and p.Ap partials (last block:
+// alpha).  One thread per layer point; grid: (ceil(nxtot/256), nb).  KY is
+// the padded y-list width: a WFS's KY row loads are issued together.
+template <int KY>
+__global__ void __launch_bounds__(kThreads)
+k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__restrict__ out,
+           double *__restrict__ dot_part, PadIndex pi, const LayerDev *__restrict__ lay, int nps,
+           int nwfs, int nyp, long nxtot, long tw, int do_l2, CgScal S, int kit,
+           const int *__restrict__ act) {
+    const int b = blockIdx.y;
+    if (inactive(act, b)) return;
+    __shared__ double sh[32];
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double dotv = 0;
+    if (j < nxtot) {
+        int l = 0;
+        while (l + 1 < nps && j >= lay[l + 1].off) l++;
+        const LayerDev L = lay[l];
+        const int nx = L.nx, ny = L.ny;
+        const int jj = (int)(j - L.off);
+        const int jy = jj / nx, jx = jj - jy * nx;
+        const float *tl = t + (size_t)b * nwfs * tw + (size_t)nyp * L.tcol + jx;
+        const GatherW *e = pi.y + ((size_t)l * pi.maxny + jy) * KY;
+        const int estep = nps * pi.maxny * KY;
+        float acc = 0.f;
+#pragma unroll 2
+        for (int w = 0; w < nwfs; w++, e += estep, tl += tw) {
+            GatherW ge[KY];
+            float tv[KY];
+#pragma unroll
+            for (int k = 0; k < KY; k++) ge[k] = e[k];
+#pragma unroll
+            for (int k = 0; k < KY; k++) tv[k] = tl[ge[k].i * nx];
+            float sy = 0.f;
+#pragma unroll
+            for (int k = 0; k < KY; k++) sy += ge[k].w * tv[k];
+            acc += sy;
+        }
+        const float *X = xin ? xin + (size_t)b * nxtot + L.off : nullptr;
+        float v = acc;
+        if (do_l2) {  // periodic 13-point biharmonic stencil (tomo.cu gpu_laplacian_do)
+            auto wy = [&](int d) { int y = jy + d; y += (y < 0) ? ny : 0; y -= (y >= ny) ? ny : 0; return X + y * nx; };
+            auto wx = [&](int d) { int q = jx + d; q += (q < 0) ? nx : 0; q -= (q >= nx) ? nx : 0; return q; };
+            const float *Rm2 = wy(-2), *Rm1 = wy(-1), *R0 = X + jy * nx, *Rp1 = wy(1), *Rp2 = wy(2);
+            const int xm2 = wx(-2), xm1 = wx(-1), xp1 = wx(1), xp2 = wx(2);
+            const float st = 20.f * R0[jx] - 8.f * (R0[xm1] + R0[xp1] + Rm1[jx] + Rp1[jx]) +
+                             2.f * (Rm1[xm1] + Rm1[xp1] + Rp1[xm1] + Rp1[xp1]) +
+                             (Rm2[jx] + R0[xm2] + R0[xp2] + Rp2[jx]);
+            v += L.l2c * st;
+        }
+        out[(size_t)b * nxtot + j] = v;
+        if (dot_part && X) dotv = (double)v * (double)X[jj];
     }
     if (dot_part) {
         dotv = block_sum(dotv, sh);

@@ -93,3 +93,26 @@ def test_batch_instances_are_independent(setup):
     x1, _ = R1.tomo(g[1:2])
     R1.close()
     assert rel(xb[1], x1[0]) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["ltao_8m", "mcao_30m"])
+def test_integrated_tip_tilt_split0(name):
+    """recon.split=0: the LHS carries the tip/tilt projection too."""
+    from conftest import get_system
+    from maos_b200.recon import Reconstructor
+    s = get_system(name)
+    o = TomoOracle(s, split=0)
+    R = Reconstructor(s, nbatch=2, split=0)
+    try:
+        rng = np.random.default_rng(8)
+        x = rng.standard_normal((2, s.nx_total)) * 1e-7
+        got = R.apply_L(x)
+        for b in range(2):
+            assert rel(got[b], o.tomo_L(x[b])) < OP_TOL
+        g = rng.standard_normal((2, s.ngrad)) * 1e-6
+        xs, _ = R.tomo(g)
+        for b in range(2):
+            w, _ = tomo_solve(o, g[b])
+            assert rel(xs[b], w) < SOLVE_TOL
+    finally:
+        R.close()
