@@ -590,6 +590,8 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
             set_error("fdpcg: layer %d grid %dx%d is not a product of 2, 3 and 5 in 8 stages", l, F.nx, F.ny);
             throw InvalidArg{MB_EUNSUP};
         }
+        MB_REQUIRE(F.nx <= kThreads && F.ny <= 2 * kThreads, "fdpcg: layer %d grid %dx%d too large", l, F.nx,
+                   F.ny);
         F.off = lay_h[l].off;
         F.hoff = (int)hoff[l];
         F.hs = (int)hsz[l];

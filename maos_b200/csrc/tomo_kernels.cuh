@@ -792,30 +792,38 @@ __device__ __forceinline__ cplx mul_mi(cplx a) { return make_float2(a.y, -a.x); 
 
 // One Stockham stage of radix R over `count` transforms of length n
 // (element stride es, transform stride ts), a -> b.  Ns = product of the
-// radices of the previous stages.
+// radices of the previous stages.  A thread keeps one butterfly position j
+// (and its twiddles) for the whole stage and steps over the transforms.
+// Requires n / R <= blockDim.x.
 template <int R>
 __device__ __forceinline__ void fft_stage(const cplx *__restrict__ a, cplx *__restrict__ b, int n, int count,
                                           int es, int ts, int Ns, const cplx *__restrict__ tw, bool inv) {
     const int nbf = n / R;
+    const int cstep = blockDim.x / nbf;
+    const int c0 = threadIdx.x / nbf, j = threadIdx.x - c0 * nbf;
+    if (c0 >= cstep) return;
+    const int jm = j % Ns;
     const int tmul = n / (Ns * R);
-    const int tot = nbf * count;
-    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-        const int c = t / nbf, j = t - c * nbf;
+    cplx w[R], d[R];  // stage twiddles, radix-R roots of unity
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        w[r] = tw[r * jm * tmul];
+        d[r] = tw[r * nbf];
+        if (inv) {
+            w[r].y = -w[r].y;
+            d[r].y = -d[r].y;
+        }
+    }
+    const int o = (j / Ns) * Ns * R + jm;
+    for (int c = c0; c < count; c += cstep) {
         const cplx *src = a + (size_t)c * ts;
         cplx *dst = b + (size_t)c * ts;
-        const int jm = j % Ns;
         cplx v[R];
 #pragma unroll
         for (int r = 0; r < R; r++) {
-            cplx x = src[(j + r * nbf) * es];
-            if (r > 0 && jm > 0) {
-                cplx w = tw[r * jm * tmul];
-                if (inv) w.y = -w.y;
-                x = cmul(x, w);
-            }
-            v[r] = x;
+            const cplx x = src[(j + r * nbf) * es];
+            v[r] = r == 0 ? x : cmul(x, w[r]);
         }
-        const int o = (j / Ns) * Ns * R + jm;
         if (R == 2) {
             dst[o * es] = cadd(v[0], v[1]);
             dst[(o + Ns) * es] = csub(v[0], v[1]);
@@ -833,11 +841,7 @@ __device__ __forceinline__ void fft_stage(const cplx *__restrict__ a, cplx *__re
             for (int q = 0; q < R; q++) {
                 cplx acc = v[0];
 #pragma unroll
-                for (int r = 1; r < R; r++) {
-                    cplx w = tw[((r * q) % R) * nbf];
-                    if (inv) w.y = -w.y;
-                    acc = cadd(acc, cmul(v[r], w));
-                }
+                for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], d[(r * q) % R]));
                 dst[(o + q * Ns) * es] = acc;
             }
         }
@@ -878,16 +882,16 @@ k_fd_fwd(const float *__restrict__ r, cplx *__restrict__ H, const FdLayer *__res
     const int nx = L.nx, ny = L.ny, h = nx / 2 + 1, np2 = ny / 2;
     cplx *A = fsm, *B = fsm + bufn;
     const float *rb = r + (size_t)b * nxtot + L.off;
-    for (int i = threadIdx.x; i < np2 * nx; i += blockDim.x) {
-        const int p = i / nx, x = i - p * nx;
-        A[i] = make_float2(rb[(2 * p) * nx + x], rb[(2 * p + 1) * nx + x]);
-    }
+    const int xs = blockDim.x / nx, x0 = threadIdx.x / nx, xc = threadIdx.x - x0 * nx;  // nx <= blockDim
+    if (x0 < xs)
+        for (int p = x0; p < np2; p += xs)
+            A[p * nx + xc] = make_float2(rb[(2 * p) * nx + xc], rb[(2 * p + 1) * nx + xc]);
     __syncthreads();
     cplx *Z = fft_many(A, B, nx, np2, 1, nx, L.rx, L.nrx, tw + L.twx, false);
     cplx *S = (Z == A) ? B : A;
-    for (int i = threadIdx.x; i < np2 * h; i += blockDim.x) {
-        const int p = i / h, k = i - p * h;
-        const cplx zk = Z[p * nx + k], zm = cconj(Z[p * nx + (nx - k) % nx]);
+    const int hs_ = blockDim.x / h, h0 = threadIdx.x / h, k = threadIdx.x - h0 * h;
+    for (int p = h0; h0 < hs_ && p < np2; p += hs_) {
+        const cplx zk = Z[p * nx + k], zm = cconj(Z[p * nx + (k == 0 ? 0 : nx - k)]);
         S[(2 * p) * h + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
         const cplx d = csub(zk, zm);
         S[(2 * p + 1) * h + k] = make_float2(0.5f * d.y, -0.5f * d.x);  // -i/2 (zk - conj(z_-k))
@@ -956,8 +960,9 @@ k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restr
     __syncthreads();
     cplx *C = fft_many(A, B, ny, h, h, 1, L.ry, L.nry, tw + L.twy, true);
     cplx *Zb = (C == A) ? B : A;
-    for (int i = threadIdx.x; i < np2 * nx; i += blockDim.x) {
-        const int p = i / nx, k = i - p * nx;
+    const int xs = blockDim.x / nx, x0 = threadIdx.x / nx, k = threadIdx.x - x0 * nx;
+    for (int p = x0; x0 < xs && p < np2; p += xs) {
+        const int i = p * nx + k;
         const bool hi = k > nx / 2;
         const int kk = hi ? nx - k : k;
         cplx a = C[(2 * p) * h + kk], c = C[(2 * p + 1) * h + kk];
@@ -975,8 +980,8 @@ k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restr
     const cplx *Zo = fft_many(Zb, C, nx, np2, 1, nx, L.rx, L.nrx, tw + L.twx, true);
     const size_t base = (size_t)b * nxtot + L.off;
     double v = 0;
-    for (int i = threadIdx.x; i < np2 * nx; i += blockDim.x) {
-        const int p = i / nx, x = i - p * nx;
+    for (int p = x0; x0 < xs && p < np2; p += xs) {
+        const int x = k, i = p * nx + k;
         const cplx q = Zo[i];
         const size_t o0 = base + (size_t)(2 * p) * nx + x, o1 = o0 + nx;
         z[o0] = q.x;
