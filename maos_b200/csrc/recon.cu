@@ -92,6 +92,7 @@ struct Recon {
     DevBuf<cplx> fd_tw;                     // twiddle tables exp(-2 pi i k/n)
     int fd_bufn = 0;                        // complex elements per FFT shared buffer
     size_t fd_smem = 0;
+
     DevBuf<cplx> spec, spec2;               // half spectra
 
     // state and work buffers
@@ -157,8 +158,9 @@ struct Recon {
     void op_hx(const float *xin, cudaStream_t s);
     void op_rhs(const float *g, float *out, cudaStream_t s);
     void op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t s, int k = 0);
-    void op_fdpcg(const float *rin, float *zout, double *rz_part, cudaStream_t s, int k = 0,
-                  int init = 0, bool in_cg = false);
+    void op_fdpcg(float *rin, float *zout, double *rz_part, cudaStream_t s, int k = 0, int init = 0,
+                  bool in_cg = false, float *xupd = nullptr, const float *pupd = nullptr,
+                  const float *Apupd = nullptr);
     void enqueue_solve(cudaStream_t s);
     struct CgBufs {
         float *x, *r, *p, *z, *Ap, *rhs;
@@ -166,9 +168,10 @@ struct Recon {
         CgScal S;
     };
     using AmulFn = std::function<void(const float *, float *, double *, int)>;
-    using MmulFn = std::function<void(const float *, float *, double *, int, int)>;
+    using MmulFn = std::function<void(float *, float *, double *, int, int)>;
+    using XrMmulFn = std::function<void(int)>;
     void enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulFn &Amul,
-                    const MmulFn &Mmul, cudaStream_t s);
+                    const MmulFn &Mmul, cudaStream_t s, const XrMmulFn &XrMmul = XrMmulFn());
     void op_fitR(const float *xin, float *out, cudaStream_t s);
     void op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t s, int k = 0);
     void enqueue_fit(cudaStream_t s);
@@ -476,7 +479,7 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
     MB_REQUIRE(fd && fd->perm && fd->mbinv && fd->nb > 0 && fd->bs > 0, "fdpcg tables missing");
     MB_REQUIRE((long)fd->nb * fd->bs == nxtot, "fdpcg: nb*bs=%ld differs from nxtot=%ld",
                (long)fd->nb * fd->bs, nxtot);
-    MB_REQUIRE(fd->bs <= kThreads, "fdpcg: block size %d above %d", fd->bs, kThreads);
+    MB_REQUIRE(fd->bs <= kMaxBs, "fdpcg: block size %d above %d", fd->bs, kMaxBs);
     fd_nb = fd->nb;
     fd_bs = fd->bs;
     std::vector<long> hoff(nps), hsz(nps);
@@ -590,8 +593,8 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
             set_error("fdpcg: layer %d grid %dx%d is not a product of 2, 3 and 5 in 8 stages", l, F.nx, F.ny);
             throw InvalidArg{MB_EUNSUP};
         }
-        MB_REQUIRE(F.nx <= kThreads && F.ny <= 2 * kThreads, "fdpcg: layer %d grid %dx%d too large", l, F.nx,
-                   F.ny);
+        MB_REQUIRE(F.nx <= kFftThreads && F.ny <= 2 * kFftThreads, "fdpcg: layer %d grid %dx%d too large", l,
+                   F.nx, F.ny);
         F.off = lay_h[l].off;
         F.hoff = (int)hoff[l];
         F.hs = (int)hsz[l];
@@ -605,6 +608,7 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
     MB_REQUIRE(fd_smem <= 200 * 1024, "fdpcg: layer FFT needs %zu bytes of shared memory", fd_smem);
     MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
     MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
+
 }
 
 void Recon::build(const mb_recon_desc *d) {
@@ -724,27 +728,30 @@ void Recon::op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t 
     hxt_rows(xin, out, dot_part, 1, k, s);
 }
 
-void Recon::op_fdpcg(const float *rin, float *zout, double *rzp, cudaStream_t s, int k, int init,
-                     bool in_cg) {
+void Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k, int init, bool in_cg,
+                     float *xupd, const float *pupd, const float *Apupd) {
     // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT,
     // on the half spectrum as in cuda/fdpcg.cu (fdpcg_mul_block_sync_half)
-    k_fd_fwd<<<dim3(nps, nb), kThreads, fd_smem, s>>>(rin, spec.p, fd_lay.p, fd_tw.p, nxtot, fd_bufn, act());
+    k_fd_fwd<<<dim3(nps, nb), kFftThreads, fd_smem, s>>>(rin, spec.p, fd_lay.p, fd_tw.p, nxtot, fd_bufn, xupd,
+                                                        pupd, Apupd, xupd ? ab.p : nullptr, act());
     MB_CHECK_LAUNCH();
     const int per = kThreads / fd_bs;
-    k_fd_mul<<<dim3((fd_nbh + per - 1) / per, nb), kThreads, 0, s>>>(spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh,
-                                                                    fd_bs, act());
+    k_fd_mul<<<dim3((fd_nbh + per - 1) / per, (nb + kFdInst - 1) / kFdInst), kThreads, 0, s>>>(
+        spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh, fd_bs, nb, act());
     MB_CHECK_LAUNCH();
     CgScal S = in_cg ? scal() : CgScal{};
-    k_fd_inv<<<dim3(nps, nb), kThreads, fd_smem, s>>>(spec2.p, rin, zout, rzp, fd_lay.p, fd_tw.p, nxtot, fd_bufn, S,
-                                                     k, init, act());
+    k_fd_inv<<<dim3(nps, nb), kFftThreads, fd_smem, s>>>(spec2.p, rin, zout, rzp, fd_lay.p, fd_tw.p, nxtot, fd_bufn,
+                                                        S, k, init, act());
     MB_CHECK_LAUNCH();
 }
 
 // (Preconditioned) CG with FP64 scalars, the schedule of lib/pcg.c:28 and
 // cuda/pcg.cu:87 (the restart every 100/500 iterations is never reached for
 // the iteration counts used per step).  x holds the warm start.
+// XrMmul, when given, performs the x/r update of a non-final iteration
+// together with the preconditioner.
 void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulFn &Amul,
-                       const MmulFn &Mmul, cudaStream_t s) {
+                       const MmulFn &Mmul, cudaStream_t s, const XrMmulFn &XrMmul) {
     // r = b - A x ; b.b
     Amul(B.x, B.Ap, nullptr, 0);
     k_cg_init_r<<<dim3(nblk, nb), kThreads, 0, s>>>(B.rhs, B.Ap, B.r, B.bb, n, B.S, iters, act());
@@ -761,11 +768,15 @@ void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulF
     MB_CHECK_LAUNCH();
     for (int k = 0; k < iters; k++) {
         Amul(B.p, B.Ap, B.pap, k);  // its last block leaves alpha_k
-        k_cg_update_xr<<<dim3(nblk, nb), kThreads, 0, s>>>(B.x, B.r, B.p, B.Ap, B.rr, n, B.S, k, iters,
-                                                          Mmul ? 0 : 1, act());
-        MB_CHECK_LAUNCH();
-        if (k + 1 == iters) break;
-        if (Mmul) Mmul(B.r, B.z, B.rz, k, 0);  // its last block leaves beta_k
+        if (XrMmul && k + 1 < iters) {
+            XrMmul(k);  // x, r update and preconditioner; its last block leaves beta_k
+        } else {
+            k_cg_update_xr<<<dim3(nblk, nb), kThreads, 0, s>>>(B.x, B.r, B.p, B.Ap, B.rr, n, B.S, k, iters,
+                                                              Mmul ? 0 : 1, act());
+            MB_CHECK_LAUNCH();
+            if (k + 1 == iters) break;
+            if (Mmul) Mmul(B.r, B.z, B.rz, k, 0);  // its last block leaves beta_k
+        }
         k_cg_update_p<<<dim3(nblk, nb), kThreads, 0, s>>>(B.p, zp, n, B.S, 0, act());
         MB_CHECK_LAUNCH();
     }
@@ -777,11 +788,12 @@ void Recon::enqueue_solve(cudaStream_t s) {
     CgBufs B{x.p, r.p, p.p, z.p, Ap.p, rhs.p, pap_part.p, rr_part.p, rz_part.p, bb_part.p, scal()};
     AmulFn A = [&](const float *in, float *out, double *dot, int k) { op_lhs(in, out, dot, s, k); };
     MmulFn M;
-    if (precond)
-        M = [&](const float *in, float *out, double *dot, int k, int init) {
-            op_fdpcg(in, out, dot, s, k, init, true);
-        };
-    enqueue_cg(B, nxtot, nblk_x, maxit, A, M, s);
+    XrMmulFn XM;
+    if (precond) {
+        M = [&](float *in, float *out, double *dot, int k, int init) { op_fdpcg(in, out, dot, s, k, init, true); };
+        XM = [&](int k) { op_fdpcg(r.p, z.p, rz_part.p, s, k, 0, true, x.p, p.p, Ap.p); };
+    }
+    enqueue_cg(B, nxtot, nblk_x, maxit, A, M, s, XM);
 }
 
 // FitR: sum_f wt_f HA_f^T (W0 - W1 W1^T) Hxp_f x   (recon_utils.c:483, fit.cu:190)
@@ -938,16 +950,16 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     for (int l = 0; l < nps; l++) nh += (double)lay_h[l].ny * (lay_h[l].nx / 2 + 1);
     // bytes per launch: each operand read or written once (the row buffer is
     // an operand of both halves; the halo rows of the pupil blocks are not)
-    double by[7] = {
+    (void)nh;
+    double by[5] = {
         B * (F * nx + F * trow) + (double)hx.fwd.n * 12.0 + tab_wfs + (double)xpad.n * 8.0,  // x -> t
         B * (F * trow + 2 * F * nx) + (double)ypad.n * 8.0,                                // t, p -> Ap
         B * (5 * F * nx),                                              // x,r,p,Ap r/w
         B * (3 * F * nx),                                              // p,z -> p
-        B * (F * nx + 8.0 * nh),                                       // r -> half spectra
-        B * (16.0 * nbk) + 8.0 * nbk * fd_bs + 16.0 * nbk,             // spec, spec2, M, idx
-        B * (8.0 * nh + 2 * F * nx)};                                  // half spectra, r -> z
-    const int lps[7] = {maxit + 2, maxit + 2, maxit, maxit, precond ? maxit : 0, precond ? maxit : 0,
-                        precond ? maxit : 0};
+        B * (3 * F * nx + 8.0 * nbk * fd_bs + 16.0 * nbk)};           // r (twice), z, M and idx per instance
+    // with the preconditioner, the x/r update of all but the last iteration
+    // runs inside fd_fwd (timed here without it)
+    const int lps[5] = {maxit + 2, maxit + 2, precond ? 1 : maxit, maxit, precond ? maxit : 0};
     for (int st = 0; st < ns; st++) {
         bytes[st] = by[st];
         launches[st] = lps[st];
@@ -968,22 +980,7 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                     k_cg_update_p<<<dim3(nblk_x, nb), kThreads, 0, stream>>>(rhs.p, z.p, nxtot, scal(), 0, act());
                     MB_CHECK_LAUNCH();
                     break;
-                case 4:
-                    k_fd_fwd<<<dim3(nps, nb), kThreads, fd_smem, stream>>>(r.p, spec.p, fd_lay.p, fd_tw.p, nxtot,
-                                                                           fd_bufn, act());
-                    MB_CHECK_LAUNCH();
-                    break;
-                case 5:
-                    k_fd_mul<<<dim3((fd_nbh + kThreads / fd_bs - 1) / (kThreads / fd_bs), nb), kThreads, 0,
-                               stream>>>(spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh, fd_bs, act());
-                    MB_CHECK_LAUNCH();
-                    break;
-                case 6:
-                    k_fd_inv<<<dim3(nps, nb), kThreads, fd_smem, stream>>>(spec2.p, r.p, z.p, rz_part.p, fd_lay.p,
-                                                                           fd_tw.p, nxtot, fd_bufn, CgScal{}, 0, 0,
-                                                                           act());
-                    MB_CHECK_LAUNCH();
-                    break;
+                case 4: op_fdpcg(r.p, z.p, rz_part.p, stream); break;
             }
         };
         launch();  // warm
@@ -1283,8 +1280,7 @@ int mb_apply_fit_L(mb_recon *h, const double *ain, double *aout) {
 
 void *mb_recon_stream(mb_recon *h) { return h ? (void *)h->R.stream : nullptr; }
 
-static const char *kStageNames[] = {"lhs_pupil", "lhs_layer", "cg_update_xr", "cg_update_p",
-                                    "fd_fwd", "fd_mul", "fd_inv"};
+static const char *kStageNames[] = {"lhs_pupil", "lhs_layer", "cg_update_xr", "cg_update_p", "fdpcg"};
 int mb_num_stages(void) { return (int)(sizeof(kStageNames) / sizeof(kStageNames[0])); }
 const char *mb_stage_name(int i) { return (i >= 0 && i < mb_num_stages()) ? kStageNames[i] : ""; }
 

@@ -870,22 +870,45 @@ __device__ cplx *fft_many(cplx *a, cplx *b, int n, int count, int es, int ts, co
     return a;
 }
 
-// Forward: r (instance-major) -> half spectra H.  grid: (nps, nb); dynamic
-// shared memory: two buffers of `bufn` complex values.
-__global__ void __launch_bounds__(kThreads)
-k_fd_fwd(const float *__restrict__ r, cplx *__restrict__ H, const FdLayer *__restrict__ fl,
-         const cplx *__restrict__ tw, long nxtot, int bufn, const int *__restrict__ act) {
+constexpr int kFftThreads = 512;  // threads of a layer-FFT CTA
+
+// Forward: r (instance-major) -> half spectra H.  grid: (nps, nb), block:
+// kFftThreads; dynamic shared memory: two buffers of `bufn` complex values.  With `ab`, the CG
+// update of this iteration comes first on the layer's points:
+// x += alpha p, r -= alpha Ap (alpha = ab[2b]), and the updated r is
+// transformed (the k_cg_update_xr of a non-final iteration, fused).
+__global__ void __launch_bounds__(kFftThreads)
+k_fd_fwd(float *r, cplx *__restrict__ H, const FdLayer *__restrict__ fl, const cplx *__restrict__ tw,
+         long nxtot, int bufn, float *__restrict__ xw, const float *__restrict__ pv,
+         const float *__restrict__ Apv, const float *__restrict__ ab, const int *__restrict__ act) {
     if (inactive(act, blockIdx.y)) return;
     extern __shared__ cplx fsm[];
     const FdLayer L = fl[blockIdx.x];
     const int b = blockIdx.y;
     const int nx = L.nx, ny = L.ny, h = nx / 2 + 1, np2 = ny / 2;
     cplx *A = fsm, *B = fsm + bufn;
-    const float *rb = r + (size_t)b * nxtot + L.off;
+    const size_t base = (size_t)b * nxtot + L.off;
+    float *rb = r + base;
     const int xs = blockDim.x / nx, x0 = threadIdx.x / nx, xc = threadIdx.x - x0 * nx;  // nx <= blockDim
-    if (x0 < xs)
-        for (int p = x0; p < np2; p += xs)
-            A[p * nx + xc] = make_float2(rb[(2 * p) * nx + xc], rb[(2 * p + 1) * nx + xc]);
+    if (x0 < xs) {
+        if (ab) {
+            const float a = ab[2 * b];
+            float *xb = xw + base;
+            const float *pb = pv + base, *qb = Apv + base;
+            for (int p = x0; p < np2; p += xs) {
+                const int o0 = (2 * p) * nx + xc, o1 = o0 + nx;
+                xb[o0] += a * pb[o0];
+                xb[o1] += a * pb[o1];
+                const float r0 = rb[o0] - a * qb[o0], r1 = rb[o1] - a * qb[o1];
+                rb[o0] = r0;
+                rb[o1] = r1;
+                A[p * nx + xc] = make_float2(r0, r1);
+            }
+        } else {
+            for (int p = x0; p < np2; p += xs)
+                A[p * nx + xc] = make_float2(rb[(2 * p) * nx + xc], rb[(2 * p + 1) * nx + xc]);
+        }
+    }
     __syncthreads();
     cplx *Z = fft_many(A, B, nx, np2, 1, nx, L.rx, L.nrx, tw + L.twx, false);
     cplx *S = (Z == A) ? B : A;
@@ -905,46 +928,60 @@ k_fd_fwd(const float *__restrict__ r, cplx *__restrict__ H, const FdLayer *__res
 // Per-frequency block solve on the blocks of the non-positive x frequencies
 // (the leading blocks of the reference's ordering, which reach every stored
 // bin): Y_i = sum_j M[blk][j*bs+i] X_j.  A CTA takes floor(256/bs) whole
-// blocks: every thread first stages its own member X_i in shared memory,
-// then forms its row from the block's staged members.
-// grid: (ceil(nblk / floor(256/bs)), nbatch)
+// blocks and up to kFdInst instances: a thread keeps its row of M in
+// registers for all of them, and per instance first stages its own member
+// X_i in shared memory, then forms its row from the block's staged members.
+// grid: (ceil(nblk / floor(256/bs)), ceil(nbatch / kFdInst))
+constexpr int kFdInst = 8;
+constexpr int kMaxBs = 16;
+
 __global__ void __launch_bounds__(kThreads)
 k_fd_mul(const cplx *__restrict__ X, cplx *__restrict__ Y, const cplx *__restrict__ M,
-         const FdIndex *__restrict__ idx, int nblk, int bs, const int *__restrict__ act) {
-    if (inactive(act, blockIdx.y)) return;
+         const FdIndex *__restrict__ idx, int nblk, int bs, int nbatch, const int *__restrict__ act) {
     __shared__ cplx xs[kThreads];
-    const int b = blockIdx.y;
     const int per = kThreads / bs;
     const int lb = threadIdx.x / bs, i = threadIdx.x - lb * bs;
     const int blk = blockIdx.x * per + lb;
     const bool live = lb < per && blk < nblk;
     FdIndex o{};
+    cplx m[kMaxBs];
     if (live) {
         o = idx[(size_t)blk * bs + i];
-        cplx xv = X[o.base + (size_t)b * o.stride];
-        if (o.flags & kFdConj) xv.y = -xv.y;
-        xs[threadIdx.x] = xv;
+        const cplx *Mb = M + (size_t)blk * bs * bs + i;
+#pragma unroll
+        for (int jj = 0; jj < kMaxBs; jj++) m[jj] = jj < bs ? Mb[jj * bs] : make_float2(0.f, 0.f);
     }
-    __syncthreads();
-    if (!live) return;
-    const cplx *Mb = M + (size_t)blk * bs * bs + i;
-    const cplx *xb = xs + lb * bs;
-    float re = 0.f, im = 0.f;
-#pragma unroll 4
-    for (int jj = 0; jj < bs; jj++) {
-        const cplx m = Mb[jj * bs];
-        const cplx xv = xb[jj];
-        re += m.x * xv.x - m.y * xv.y;
-        im += m.x * xv.y + m.y * xv.x;
+    const int b1 = min(nbatch, (int)(blockIdx.y + 1) * kFdInst);
+    for (int b = blockIdx.y * kFdInst; b < b1; b++) {
+        if (inactive(act, b)) continue;  // uniform over the CTA
+        if (live) {
+            cplx xv = X[o.base + (size_t)b * o.stride];
+            if (o.flags & kFdConj) xv.y = -xv.y;
+            xs[threadIdx.x] = xv;
+        }
+        __syncthreads();
+        if (live) {
+            const cplx *xb = xs + lb * bs;
+            float re = 0.f, im = 0.f;
+#pragma unroll
+            for (int jj = 0; jj < kMaxBs; jj++) {
+                if (jj < bs) {
+                    const cplx xv = xb[jj];
+                    re += m[jj].x * xv.x - m[jj].y * xv.y;
+                    im += m[jj].x * xv.y + m[jj].y * xv.x;
+                }
+            }
+            if (o.flags & kFdStore)
+                Y[o.base + (size_t)b * o.stride] = make_float2(re, (o.flags & kFdConj) ? -im : im);
+        }
+        __syncthreads();
     }
-    if (o.flags & kFdStore)
-        Y[o.base + (size_t)b * o.stride] = make_float2(re, (o.flags & kFdConj) ? -im : im);
 }
 
 // Inverse: half spectra H -> z (instance-major), plus the r.z partial of this
 // (layer, instance); the last CTA of an instance leaves (r.z)_0 or beta.
 // grid: (nps, nb)
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kFftThreads)
 k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restrict__ z,
          double *__restrict__ rz_part, const FdLayer *__restrict__ fl, const cplx *__restrict__ tw, long nxtot,
          int bufn, CgScal SC, int kit, int init, const int *__restrict__ act) {

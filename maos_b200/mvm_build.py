@@ -1,0 +1,75 @@
+"""Control-matrix build on the GPU: many right-hand sides through the same
+tomography + fit operators at once.
+
+The reference assembles its MVM control matrix by solving the tomography and
+fit normal equations for every gradient (``maos/setup_recon_mvm.c:115-229``;
+on the GPU ``cuda/mvm_trans.cu:46-360``), with the iteration counts raised well
+above the per-step ones so that the result approximates the converged linear
+operator ``M = FitL^-1 FitR TomoL^-1 TomoR``.  Here column ``c`` of ``M`` is the
+DM command vector that a cold-started reconstruction step returns for the
+unit gradient ``e_c``; ``rhs_batch`` columns run as the instances of one
+batched reconstructor (shared operator tables, one CUDA graph per batch).
+FP32 arithmetic with FP64 CG scalars, like every solve in this package.
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+from typing import Optional
+
+import numpy as np
+
+from .native import check
+
+
+def build_control_matrix(sysm, fit, rhs_batch: int = 256, tomo_maxit: Optional[int] = None,
+                         fit_maxit: Optional[int] = None, columns=None, device: int = 0,
+                         scale: float = 1e-6):
+    """M (nact x ngrad, FP32) and a report dict.
+
+    ``columns``: gradient indices to build (default: all, giving the whole
+    matrix); the returned array then has one column per requested index.
+    ``scale``: size of the unit gradient actually applied (the result is
+    divided by it), keeping the solves in the usual FP32 range."""
+    import torch
+    from .recon import Reconstructor
+    tomo_maxit = int(tomo_maxit or 10 * sysm.cfg.tomo_maxit)
+    fs = dataclasses.replace(fit, maxit=int(fit_maxit or 10 * fit.maxit))
+    ngrad, nact = int(sysm.ngrad), int(fs.nact)
+    cols = np.arange(ngrad) if columns is None else np.asarray(columns, dtype=np.int64)
+    B = int(min(rhs_batch, len(cols)))
+    R = Reconstructor(sysm, nbatch=B, maxit=tomo_maxit, fit=fs, device=device)
+    out = np.empty((nact, len(cols)), dtype=np.float32)
+    stream = torch.cuda.Stream(device=device)
+    g = torch.zeros((B, ngrad), dtype=torch.float32, device=f"cuda:{device}")
+    a = torch.empty((B, nact), dtype=torch.float32, device=f"cuda:{device}")
+    worst = 0.0
+    t0 = time.perf_counter()
+    try:
+        for c0 in range(0, len(cols), B):
+            n = min(B, len(cols) - c0)
+            with torch.cuda.stream(stream):
+                g.zero_()
+                rows = torch.arange(n, device=g.device)
+                g[rows, torch.as_tensor(cols[c0:c0 + n], device=g.device)] = scale
+            stream.synchronize()
+            check(R.lib.mb_recon_reset(R.h), "mb_recon_reset")
+            R.step_device(g.data_ptr(), stream.cuda_stream)
+            stream.synchronize()
+            a.copy_(torch.as_tensor(_DeviceArray(R.fit_solution_ptr(), (B, nact)), device=g.device))
+            torch.cuda.synchronize(device)
+            out[:, c0:c0 + n] = (a[:n].cpu().numpy().T / scale)
+            worst = max(worst, float(np.max(R.residual()[:n])))
+    finally:
+        R.close()
+    report = {"columns": int(len(cols)), "rhs_batch": B, "tomo_maxit": tomo_maxit, "fit_maxit": fs.maxit,
+              "max_tomo_residual": worst, "seconds": time.perf_counter() - t0}
+    return out, report
+
+
+class _DeviceArray:
+    """A library-owned FP32 device array, seen through the CUDA array interface."""
+
+    def __init__(self, ptr: int, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (int(ptr), True),
+                                         "version": 3}
