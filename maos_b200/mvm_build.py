@@ -71,5 +71,5 @@ class _DeviceArray:
     """A library-owned FP32 device array, seen through the CUDA array interface."""
 
     def __init__(self, ptr: int, shape):
-        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (int(ptr), True),
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (int(ptr), False),
                                          "version": 3}

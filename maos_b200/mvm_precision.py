@@ -23,25 +23,28 @@ import numpy as np
 
 from . import native
 from .native import check
-from .turbulence import FrozenFlowAtmosphere, geometric_gradients
+from .turbulence import DeviceAtmosphere, FrozenFlowAtmosphere
 
 DTYPES = (("fp32", native.MB_MVM_F32), ("bf16", native.MB_MVM_BF16), ("fp8_e4m3", native.MB_MVM_FP8))
 
 
-def frozen_flow(sysm, fit, nsteps: int, seed: int = 11, dt: float = None):
+def frozen_flow(sysm, fit, nsteps: int, seed: int = 11, dt: float = None, device: str = "cuda"):
     """Gradients [nsteps][ngrad] with noise and the true science OPD on the
-    fit grid [nsteps][nfloc] of consecutive frozen-flow steps."""
+    fit grid [nsteps][nfloc] of consecutive frozen-flow steps (sampled on
+    `device`, FP64)."""
+    import torch
     dt = sysm.cfg.sim_dt if dt is None else dt
-    atm = FrozenFlowAtmosphere(sysm.cfg, seed)
+    atm = DeviceAtmosphere(FrozenFlowAtmosphere(sysm.cfg, seed), device=device)
     rng = np.random.default_rng(seed + 104729)
     fl = fit.floc
-    fx = (fl.ox + np.arange(fl.nx) * fl.dx)[None, :].repeat(fl.ny, 0).ravel()
-    fy = (fl.oy + np.arange(fl.ny) * fl.dy)[:, None].repeat(fl.nx, 1).ravel()
+    fx = torch.as_tensor((fl.ox + np.arange(fl.nx) * fl.dx)[None, :].repeat(fl.ny, 0).ravel(), device=device)
+    fy = torch.as_tensor((fl.oy + np.arange(fl.ny) * fl.dy)[:, None].repeat(fl.nx, 1).ravel(), device=device)
     g = np.empty((nsteps, sysm.ngrad))
-    phi = np.empty((nsteps, fx.size))
+    phi = np.empty((nsteps, fx.numel()))
     for k in range(nsteps):
-        g[k] = geometric_gradients(sysm, atm, k * dt, rng, noise=True)
-        phi[k] = atm.opd(fx, fy, float(fit.thetax[0]), float(fit.thetay[0]), float(fit.hs[0]), k * dt)
+        g[k] = atm.gradients(sysm, k * dt, rng, noise=True)
+        phi[k] = atm.opd(fx, fy, float(fit.thetax[0]), float(fit.thetay[0]), float(fit.hs[0]),
+                         k * dt).cpu().numpy()
     return g, phi
 
 
@@ -75,19 +78,21 @@ def mvm_apply(M: np.ndarray, g: np.ndarray, dtype: int, batch: int = 64) -> np.n
     return out
 
 
-def study(sysm, fit, M: np.ndarray, nsteps: int = 400, seed: int = 11, gate: float = 0.01) -> dict:
+def study(sysm, fit, M: np.ndarray, nsteps: int = 400, seed: int = 11, gate: float = 0.01,
+          device: str = "cuda") -> dict:
     """The precision report: residual WFE, each storage type's command error
     (nm RMS and as a fraction of the residual) and whether it is within
     ``gate`` of the residual."""
-    g, phi = frozen_flow(sysm, fit, nsteps, seed)
-    HA0 = np.hstack([fit.HA[0][d].toarray() for d in range(len(fit.dms))])
+    g, phi = frozen_flow(sysm, fit, nsteps, seed, device=device)
+    import scipy.sparse as sps
+    HA0 = sps.hstack([fit.HA[0][d] for d in range(len(fit.dms))]).tocsr()
     a64 = g @ np.asarray(M, dtype=np.float64).T
-    res = _wfe(fit, phi - a64 @ HA0.T)
+    res = _wfe(fit, phi - (HA0 @ a64.T).T)
     out = {"steps": int(nsteps), "dt_s": float(sysm.cfg.sim_dt), "shape": [int(M.shape[0]), int(M.shape[1])],
            "residual_wfe_nm": float(np.sqrt(np.mean(res ** 2)) * 1e9), "gate_fraction": gate, "dtypes": {}}
     for name, dt in DTYPES:
         a = mvm_apply(M, g, dt)
-        err = _wfe(fit, (a - a64) @ HA0.T)
+        err = _wfe(fit, (HA0 @ (a - a64).T).T)
         e = float(np.sqrt(np.mean(err ** 2)))
         frac = e / math.sqrt(np.mean(res ** 2))
         rel = float(np.linalg.norm(a - a64) / np.linalg.norm(a64))

@@ -111,3 +111,63 @@ def gradient_frames(sysm, seed: int, nframe: int, dt: float = None, noise: bool 
     atm = FrozenFlowAtmosphere(sysm.cfg, seed)
     rng = np.random.default_rng(seed + 7919)
     return np.stack([geometric_gradients(sysm, atm, k * dt, rng, noise) for k in range(nframe)])
+
+
+class DeviceAtmosphere:
+    """The same frozen-flow atmosphere sampled with torch on a device (FP64):
+    ``opd`` and ``gradients`` restate ``FrozenFlowAtmosphere.opd`` and
+    ``geometric_gradients`` so that long gradient sequences of large systems
+    take seconds instead of minutes."""
+
+    def __init__(self, atm: FrozenFlowAtmosphere, device: str = "cuda"):
+        import torch
+        self.atm = atm
+        self.dev = device
+        self.screens = [torch.as_tensor(s, dtype=torch.float64, device=device) for s in atm.screens]
+
+    def opd(self, x, y, thetax: float, thetay: float, hs: float, t: float):
+        import torch
+        a = self.atm
+        out = torch.zeros_like(x, dtype=torch.float64)
+        n = a.n
+        for l, h in enumerate(a.cfg.atm_ht):
+            scale = 1.0 - h / hs if math.isfinite(hs) else 1.0
+            u = (x * scale + thetax * h - float(a.vx[l]) * t) / a.dx + n / 2
+            v = (y * scale + thetay * h - float(a.vy[l]) * t) / a.dx + n / 2
+            iu = torch.floor(u)
+            iv = torch.floor(v)
+            fu = u - iu
+            fv = v - iv
+            iu = iu.long() % n
+            iv = iv.long() % n
+            iu1 = (iu + 1) % n
+            iv1 = (iv + 1) % n
+            S = self.screens[l]
+            out += ((1 - fu) * (1 - fv) * S[iv, iu] + fu * (1 - fv) * S[iv, iu1]
+                    + (1 - fu) * fv * S[iv1, iu] + fu * fv * S[iv1, iu1])
+        return out
+
+    def gradients(self, sysm, t: float, rng: np.random.Generator, noise: bool = True, nedge: int = 8):
+        """Average-slope gradients (rad) of every WFS, x then y, plus noise (host array)."""
+        import torch
+        s = torch.arange(nedge + 1, dtype=torch.float64, device=self.dev) / nedge
+        wq = torch.full((nedge + 1,), 1.0 / nedge, dtype=torch.float64, device=self.dev)
+        wq[0] = wq[-1] = 0.5 / nedge
+        out = []
+        for w in sysm.wfs:
+            dsa = w.dsa
+            x0 = torch.as_tensor(w.salocx, dtype=torch.float64, device=self.dev)[:, None]
+            y0 = torch.as_tensor(w.salocy, dtype=torch.float64, device=self.dev)[:, None]
+            e = s[None, :] * dsa
+            shp = (w.nsa, nedge + 1)
+            right = self.opd((x0 + dsa).expand(shp), y0 + e, w.thetax, w.thetay, w.hs, t)
+            left = self.opd(x0.expand(shp), y0 + e, w.thetax, w.thetay, w.hs, t)
+            gx = ((right - left) * wq).sum(dim=1) / dsa
+            top = self.opd(x0 + e, (y0 + dsa).expand(shp), w.thetax, w.thetay, w.hs, t)
+            bot = self.opd(x0 + e, y0.expand(shp), w.thetax, w.thetay, w.hs, t)
+            gy = ((top - bot) * wq).sum(dim=1) / dsa
+            g = torch.cat([gx, gy]).cpu().numpy()
+            if noise:
+                g = g + rng.standard_normal(g.size) * np.sqrt(w.sanea)
+            out.append(g)
+        return np.concatenate(out)

@@ -1,0 +1,66 @@
+"""Control-matrix build on the GPU and the storage precision of its MVM.
+
+The build applies the batched tomography + fit to unit gradients (256
+right-hand sides per batched solve, FP32 with FP64 CG scalars); 64 seeded
+columns are compared with the FP64 oracle solving the same cold-started
+problems with the same iteration counts.  Tolerance: 5e-3 relative L2 per
+column (FP32 CG over 100+ iterations against FP64).
+
+The precision study then applies the built matrix to frozen-flow gradients in
+FP32, BF16 and FP8-E4M3 storage and measures the DM-command error as
+wavefront error against the residual WFE of the FP64 product; BF16 must stay
+within 1% of the residual (the serving target), FP8 is reported.
+"""
+import numpy as np
+import pytest
+
+from oracle.recon_oracle import FitOracle, TomoOracle, fit_solve, tomo_solve
+
+pytestmark = pytest.mark.gpu
+
+COL_TOL = 5e-3
+TOMO_IT, FIT_IT = 100, 40
+
+
+@pytest.fixture(scope="module")
+def ltao_matrix():
+    from conftest import get_fit, get_system
+    from maos_b200.mvm_build import build_control_matrix
+    s, fs = get_system("ltao_8m"), get_fit("ltao_8m")
+    M, rep = build_control_matrix(s, fs, rhs_batch=256, tomo_maxit=TOMO_IT, fit_maxit=FIT_IT)
+    return s, fs, M, rep
+
+
+def test_columns_match_fp64_oracle(ltao_matrix):
+    s, fs, M, rep = ltao_matrix
+    assert M.shape == (fs.nact, s.ngrad) and np.all(np.isfinite(M))
+    to, fo = TomoOracle(s), FitOracle(s, fs)
+    cols = np.random.default_rng(64).choice(s.ngrad, 64, replace=False)
+    for c in cols:
+        g = np.zeros(s.ngrad)
+        g[c] = 1e-6
+        x, _ = tomo_solve(to, g, maxit=TOMO_IT)
+        a, _ = fit_solve(fo, x, maxit=FIT_IT)
+        want = a / 1e-6
+        assert np.linalg.norm(M[:, c] - want) <= COL_TOL * np.linalg.norm(want), int(c)
+
+
+def test_partial_build_equals_full_columns(ltao_matrix):
+    from maos_b200.mvm_build import build_control_matrix
+    s, fs, M, rep = ltao_matrix
+    cols = np.array([3, 700, 1500, 2655])
+    Mp, _ = build_control_matrix(s, fs, rhs_batch=4, tomo_maxit=TOMO_IT, fit_maxit=FIT_IT, columns=cols)
+    for k, c in enumerate(cols):
+        assert np.linalg.norm(Mp[:, k] - M[:, c]) <= 1e-5 * np.linalg.norm(M[:, c])
+
+
+def test_mvm_storage_precision_gate(ltao_matrix):
+    from maos_b200.mvm_precision import study
+    s, fs, M, rep = ltao_matrix
+    r = study(s, fs, M, nsteps=200, gate=0.01)
+    assert r["residual_wfe_nm"] > 0
+    d = r["dtypes"]
+    assert d["fp32"]["fraction_of_residual"] < 1e-4
+    assert d["bf16"]["within_gate"], d["bf16"]
+    assert d["bf16"]["fraction_of_residual"] < d["fp8_e4m3"]["fraction_of_residual"]
+    assert np.isfinite(d["fp8_e4m3"]["command_error_wfe_nm"])
