@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mvm-batch", type=int, default=1)
     ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--precision-steps", type=int, default=2000)
     ap.add_argument("--no-serve", action="store_true")
     return ap.parse_args()
 
@@ -209,13 +210,15 @@ def run_reference(args):
     return 0
 
 
-def mvm_rates(lib, native, nact: int, ngrad: int, batch: int, stream):
-    """Control-matrix MVM steps/s per storage type (random M of the system's size)."""
+def mvm_rates(lib, native, nact: int, ngrad: int, batch: int, stream, M=None):
+    """Control-matrix MVM steps/s per storage type (M: the built control
+    matrix, else a random matrix of the system's size)."""
     import ctypes as C
     import numpy as np
     import torch
-    rng = np.random.default_rng(3)
-    M = np.asfortranarray(rng.standard_normal((nact, ngrad)) * 1e-3)
+    if M is None:
+        M = np.random.default_rng(3).standard_normal((nact, ngrad)) * 1e-3
+    M = np.asfortranarray(M, dtype=np.float64)
     g = torch.randn(batch, ngrad, device="cuda")
     out = torch.empty(batch, nact, device="cuda")
     res = {"batch": batch, "shape": [nact, ngrad]}
@@ -410,7 +413,20 @@ def run_gpu(args):
             "share_of_step": dom["share_ms"] / tot_stage,
             "stage_ms_per_step": {s["name"]: round(s["share_ms"], 4) for s in stages}}
 
-    mvm_line = mvm_rates(lib, native, int(fit.nact), int(sysm.ngrad), args.mvm_batch, stream)
+    # control matrix of this system (batched cold solves of unit gradients,
+    # 256 per launch) and the storage precision of its MVM on frozen flow
+    Mctl, precision = None, None
+    if world == 1 and args.precision_steps > 0:
+        from maos_b200 import mvm_precision
+        from maos_b200.mvm_build import build_control_matrix
+        Mctl, build = build_control_matrix(sysm, fit, rhs_batch=256, tomo_maxit=90, fit_maxit=40)
+        precision = mvm_precision.study(sysm, fit, Mctl, nsteps=args.precision_steps)
+        precision["control_matrix_build"] = build
+    mvm_line = mvm_rates(lib, native, int(fit.nact), int(sysm.ngrad), args.mvm_batch, stream, Mctl)
+    mvm_line["matrix"] = "built control matrix" if Mctl is not None else "random, same shape"
+    if precision is not None:
+        mvm_line["precision"] = precision
+    del Mctl
 
     served = None
     if world == 1 and not args.no_serve and args.serve_seconds > 0:

@@ -116,6 +116,17 @@ __device__ __forceinline__ double warp_sum_fresh(const double *part, int n) {
     return __shfl_sync(0xffffffffu, v, 0);
 }
 
+// Programmatic dependent launch: the first statement of every kernel here.
+// A kernel launched with programmatic stream serialisation may be scheduled
+// while its predecessor is still running; griddepcontrol.wait blocks until
+// the predecessor has completed and its writes are visible, and
+// launch_dependents lets the successor's CTAs be scheduled early.  Both are
+// no-ops for an ordinary launch.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Serving: `act` (null: every instance) marks the instances that take part in
 // this launch.  Blocks of an inactive instance return before touching memory,
 // so its warm-start state stays as it was and no other instance's result
@@ -130,6 +141,7 @@ __global__ void k_hx(const float *__restrict__ x, float *__restrict__ opd,
                      const AxisW *__restrict__ tab, const LayerDev *__restrict__ lay, int nps,
                      int nwfs, int nxp, int nyp, long nxtot, const float *__restrict__ w1,
                      double *__restrict__ w1_part, const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.z)) return;
     __shared__ double sh[32];
     const int np = nxp * nyp;
@@ -168,6 +180,7 @@ __global__ void k_gp(const float *__restrict__ opd, const float *__restrict__ gi
                      const WfsDev *__restrict__ wfs, int nwfs, int nxp, int np, long ngrad,
                      int do_tt, float *__restrict__ tt_out, unsigned *__restrict__ cnt,
                      const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.z)) return;
     __shared__ double sh[32];
     const int w = blockIdx.y, b = blockIdx.z;
@@ -262,6 +275,7 @@ __global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ 
                       const LayerDev *__restrict__ lay, int nps, int nwfs, int nxp, int nyp,
                       long nxtot, int do_l2, float alpha, LowRank lr, CgScal S, int k,
                       const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     __shared__ float s_t[8];
@@ -383,6 +397,7 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
              const WfsDev *__restrict__ wfs, PadIndex pi, int wbase, int nps, int nwfs, int nxp, int nyp,
              long nxtot, long ngrad, long tw, int ncols, int rows, int do_tt,
              const int *__restrict__ act) {
+    pdl_enter();
     constexpr int N1 = POS + 1;
     const int w = wbase + blockIdx.y, b = blockIdx.z;
     if (inactive(act, b)) return;
@@ -540,6 +555,7 @@ k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__
            double *__restrict__ dot_part, PadIndex pi, const LayerDev *__restrict__ lay, int nps,
            int nwfs, int nyp, long nxtot, long tw, int do_l2, CgScal S, int kit,
            const int *__restrict__ act) {
+    pdl_enter();
     const int b = blockIdx.y;
     if (inactive(act, b)) return;
     __shared__ double sh[32];
@@ -600,6 +616,7 @@ __global__ void k_fit_w(const float *__restrict__ v, float *__restrict__ y,
                         const float *__restrict__ cv, const float *__restrict__ w1,
                         const float *__restrict__ wt, const double *__restrict__ w1_part,
                         int nblk_w1, int nf, int nfit, const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.z)) return;
     __shared__ float s_dot;
     const int f = blockIdx.y, b = blockIdx.z;
@@ -619,6 +636,7 @@ __global__ void k_fit_w(const float *__restrict__ v, float *__restrict__ y,
 // NW' x partials: part[(b*nnw + k)*nblk + blk].  grid: (nblk, nb)
 __global__ void k_lowrank_dot(const float *__restrict__ x, const float *__restrict__ nw,
                               double *__restrict__ part, int nnw, long n, const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     const int b = blockIdx.y;
@@ -640,6 +658,7 @@ __global__ void k_lowrank_dot(const float *__restrict__ x, const float *__restri
 __global__ void k_cg_init_r(const float *__restrict__ bvec, const float *__restrict__ Ax,
                             float *__restrict__ r, double *__restrict__ bb_part, long n, CgScal S,
                             int iters, const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     const int b = blockIdx.y;
@@ -686,6 +705,7 @@ __device__ __forceinline__ void cg_rz_last(const double *part_b, const CgScal &S
 // v.v partials and (when z aliases r) the start-of-CG r.z.  grid: (nblk, nb)
 __global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ part, long n, CgScal S,
                            const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     const int b = blockIdx.y;
@@ -707,6 +727,7 @@ __global__ void k_cg_update_xr(float *__restrict__ x, float *__restrict__ r,
                                const float *__restrict__ p, const float *__restrict__ Ap,
                                double *__restrict__ rr_part, long n, CgScal S, int k, int iters,
                                int z_is_r, const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
     const int b = blockIdx.y;
@@ -741,6 +762,7 @@ __global__ void k_cg_update_xr(float *__restrict__ x, float *__restrict__ r,
 // p = z + beta p (init: p = z).  grid: (nblk, nb)
 __global__ void k_cg_update_p(float *__restrict__ p, const float *__restrict__ z, long n, CgScal S,
                               int init, const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     const int b = blockIdx.y;
     const float be = init ? 0.f : S.ab[2 * b + 1];
@@ -881,6 +903,7 @@ __global__ void __launch_bounds__(kFftThreads)
 k_fd_fwd(float *r, cplx *__restrict__ H, const FdLayer *__restrict__ fl, const cplx *__restrict__ tw,
          long nxtot, int bufn, float *__restrict__ xw, const float *__restrict__ pv,
          const float *__restrict__ Apv, const float *__restrict__ ab, const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     extern __shared__ cplx fsm[];
     const FdLayer L = fl[blockIdx.x];
@@ -938,6 +961,7 @@ constexpr int kMaxBs = 16;
 __global__ void __launch_bounds__(kThreads)
 k_fd_mul(const cplx *__restrict__ X, cplx *__restrict__ Y, const cplx *__restrict__ M,
          const FdIndex *__restrict__ idx, int nblk, int bs, int nbatch, const int *__restrict__ act) {
+    pdl_enter();
     __shared__ cplx xs[kThreads];
     const int per = kThreads / bs;
     const int lb = threadIdx.x / bs, i = threadIdx.x - lb * bs;
@@ -985,6 +1009,7 @@ __global__ void __launch_bounds__(kFftThreads)
 k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restrict__ z,
          double *__restrict__ rz_part, const FdLayer *__restrict__ fl, const cplx *__restrict__ tw, long nxtot,
          int bufn, CgScal SC, int kit, int init, const int *__restrict__ act) {
+    pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     extern __shared__ cplx fsm[];
     __shared__ double sh[32];
@@ -1032,6 +1057,7 @@ k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restr
 
 // float <-> double staging helpers for the host-facing API
 __global__ void k_scale_copy(const float *__restrict__ a, float *__restrict__ o, float s, long n) {
+    pdl_enter();
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j < n) o[j] = s * a[j];
 }
