@@ -156,4 +156,29 @@ def scao_8m(seed: int = 1) -> AOConfig:
         fit_lrt_tt=False, dms=[DmSpec(ht=0.0, dx=0.4, order=21)], seed=seed)
 
 
-PRESETS = {"ltao_8m": ltao_8m, "mcao_30m": mcao_30m, "scao_8m": scao_8m}
+def elt_39m(seed: int = 1) -> AOConfig:
+    """39 m ELT-like MCAO for the large control-matrix build: 6 LGS at 90 km on a
+    45" hexagon, 80x80 x 0.4875 m, 9 reconstructed layers at 0-20 km
+    (0.4875 m grids at 0 and 0.5 km, 0.975 m above), 3 DMs at 0, 4 and 12.7 km."""
+    lgs = PowfsSpec(order=80, dsa=39.0 / 80, hs=90e3, nea_range_as=(0.02, 0.1), trs=True)
+    wfs = [WfsSpec(0, 45 * AS2RAD * math.cos(math.pi * k / 3), 45 * AS2RAD * math.sin(math.pi * k / 3))
+           for k in range(6)]
+    fx = [0, 0.5, 0, -0.5, 0, 0.5, -0.5, -0.5, 0.5]
+    fy = [0, 0, 0.5, 0, -0.5, 0.5, 0.5, -0.5, -0.5]
+    fw = [4 / 9, 1 / 9, 1 / 9, 1 / 9, 1 / 9, 1 / 36, 1 / 36, 1 / 36, 1 / 36]
+    ht = [0.0, 500.0, 1000.0, 2000.0, 4000.0, 8000.0, 12000.0, 16000.0, 20000.0]
+    wt = [0.45, 0.13, 0.05, 0.05, 0.09, 0.09, 0.06, 0.05, 0.03]
+    return AOConfig(
+        name="elt_39m", D=39.0, din=4.0, powfs=[lgs], wfs=wfs,
+        atmr_dx=0.975, atmr_ht=ht, atmr_wt=wt, atmr_os=[2, 2, 1, 1, 1, 1, 1, 1, 1],
+        r0=0.186, L0=30.0, atm_ht=ht, atm_wt=wt,
+        atm_ws=[5.6, 5.8, 6.3, 7.6, 13.3, 19.1, 15.0, 12.1, 10.0], atm_dx=0.25,
+        tomo_pos=2, tomo_maxit=30, tomo_precond=1,
+        fit_thetax=[v * 40 * AS2RAD for v in fx], fit_thetay=[v * 40 * AS2RAD for v in fy],
+        fit_wt=fw, fit_maxit=4,
+        dms=[DmSpec(ht=0.0, dx=39.0 / 80, order=81), DmSpec(ht=4e3, dx=39.0 / 80, order=85, offset=0.5),
+             DmSpec(ht=12.7e3, dx=0.975, order=49)],
+        seed=seed)
+
+
+PRESETS = {"ltao_8m": ltao_8m, "mcao_30m": mcao_30m, "scao_8m": scao_8m, "elt_39m": elt_39m}

@@ -370,7 +370,7 @@ struct PadIndex {
     int kx, ky, maxnx, maxny;
 };
 
-constexpr int kMaxLayers = 8;   // layers unrolled in the Hx gather
+constexpr int kMaxLayers = 12;  // layers unrolled in the Hx gather
 constexpr int kMaxPadX = 8;     // widest x list
 constexpr int kMaxPadY = 8;     // widest y list (k_hxt_rows is instantiated up to this)
 

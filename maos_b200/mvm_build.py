@@ -73,3 +73,44 @@ class _DeviceArray:
     def __init__(self, ptr: int, shape):
         self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (int(ptr), False),
                                          "version": 3}
+
+
+def column_shard(ngrad: int, rank: int, world: int, block: int = 256):
+    """Gradient indices this rank builds: whole RHS blocks, dealt out in
+    contiguous runs (rank r gets blocks [r*nblk/world, (r+1)*nblk/world))."""
+    nblk = (ngrad + block - 1) // block
+    b0, b1 = rank * nblk // world, (rank + 1) * nblk // world
+    return np.arange(b0 * block, min(b1 * block, ngrad), dtype=np.int64)
+
+
+def gather_columns(local: np.ndarray, ngrad: int, group=None, block: int = 256) -> np.ndarray:
+    """Assemble the full matrix on every rank from each rank's column shard
+    (one all_gather of equal-size padded slabs; NCCL over NVLink between GPUs,
+    gloo on the host)."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    nact = local.shape[0]
+    width = max(len(column_shard(ngrad, r, world, block)) for r in range(world))
+    backend = dist.get_backend(group)
+    dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    slab = torch.zeros((nact, width), dtype=torch.float32, device=dev)
+    slab[:, :local.shape[1]] = torch.as_tensor(local, device=dev)
+    parts = [torch.empty_like(slab) for _ in range(world)]
+    dist.all_gather(parts, slab, group=group)
+    out = np.empty((nact, ngrad), dtype=np.float32)
+    for r in range(world):
+        cols = column_shard(ngrad, r, world, block)
+        out[:, cols] = parts[r][:, :len(cols)].cpu().numpy()
+    return out
+
+
+def build_control_matrix_distributed(sysm, fit, rhs_batch: int = 256, group=None, **kw):
+    """The control matrix built by all ranks of the process group, each on its
+    own GPU with its own share of the unit gradients (no data exchange until
+    the final gather).  Returns (M on every rank, this rank's report)."""
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    cols = column_shard(int(sysm.ngrad), rank, world, rhs_batch)
+    local, rep = build_control_matrix(sysm, fit, rhs_batch=rhs_batch, columns=cols, **kw)
+    return gather_columns(local, int(sysm.ngrad), group, rhs_batch), rep

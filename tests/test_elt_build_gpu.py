@@ -1,0 +1,36 @@
+"""Large multi-RHS build: the 39 m ELT-like system (6 LGS on a 45" hexagon,
+80x80 subapertures, 60,240 gradients, 9 layers / 61,440 unknowns, 3 DMs).
+
+Control-matrix columns come from FDPCG tomography + fit on unit gradients,
+all 64 checked columns in one batched launch, FP32 with FP64 CG scalars;
+they are compared with the FP64 oracle solving the same cold-started
+problems with the same iteration counts.  Tolerance: 5e-3 relative L2 per
+column.
+"""
+import numpy as np
+import pytest
+
+from oracle.recon_oracle import FitOracle, TomoOracle, fit_solve, tomo_solve
+
+pytestmark = pytest.mark.gpu
+
+COL_TOL = 5e-3
+TOMO_IT, FIT_IT = 30, 20
+
+
+def test_elt_columns_match_fp64_oracle():
+    from conftest import get_fit, get_system
+    from maos_b200.mvm_build import build_control_matrix
+    s, fs = get_system("elt_39m"), get_fit("elt_39m")
+    assert s.ngrad > 60000 and len(s.xmaps) == 9 and len(fs.dms) == 3
+    cols = np.sort(np.random.default_rng(39).choice(s.ngrad, 64, replace=False))
+    M, rep = build_control_matrix(s, fs, rhs_batch=256, tomo_maxit=TOMO_IT, fit_maxit=FIT_IT, columns=cols)
+    assert M.shape == (fs.nact, 64) and np.all(np.isfinite(M))
+    to, fo = TomoOracle(s), FitOracle(s, fs)
+    for k, c in enumerate(cols):
+        g = np.zeros(s.ngrad)
+        g[c] = 1e-6
+        x, _ = tomo_solve(to, g, maxit=TOMO_IT)
+        a, _ = fit_solve(fo, x, maxit=FIT_IT)
+        want = a / 1e-6
+        assert np.linalg.norm(M[:, k] - want) <= COL_TOL * np.linalg.norm(want), int(c)
