@@ -358,7 +358,9 @@ void Recon::build_pad() {
     tw = (long)nyp * ncols;
     pupil_smem = (size_t)pupil_rows_smem_floats(prows, nxp, nps, ncols, kx) * sizeof(float);
     MB_REQUIRE(pupil_smem <= 200 * 1024, "pupil row block needs %zu bytes of shared memory", pupil_smem);
-    for (auto k : {k_pupil_rows<true, 1>, k_pupil_rows<true, 2>, k_pupil_rows<false, 1>, k_pupil_rows<false, 2>})
+    for (auto k : {k_pupil_rows<true, 1, 8>, k_pupil_rows<true, 2, 8>, k_pupil_rows<false, 1, 8>,
+                   k_pupil_rows<false, 2, 8>, k_pupil_rows<true, 1, 16>, k_pupil_rows<true, 2, 16>,
+                   k_pupil_rows<false, 1, 16>, k_pupil_rows<false, 2, 16>})
         MB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pupil_smem));
 }
 
@@ -369,8 +371,11 @@ void Recon::pupil_rows(bool from_x, const float *xin, cudaStream_t s) {
         int w1 = w0 + 1;
         while (w1 < nwfs && wfs_h[w1].pos == wfs_h[w0].pos) w1++;
         const bool p2 = wfs_h[w0].pos == 2;
-        auto kern = from_x ? (p2 ? k_pupil_rows<true, 2> : k_pupil_rows<true, 1>)
-                           : (p2 ? k_pupil_rows<false, 2> : k_pupil_rows<false, 1>);
+        const bool few = nps <= 8;
+        auto kern = from_x ? (p2 ? (few ? k_pupil_rows<true, 2, 8> : k_pupil_rows<true, 2, 16>)
+                                 : (few ? k_pupil_rows<true, 1, 8> : k_pupil_rows<true, 1, 16>))
+                           : (p2 ? (few ? k_pupil_rows<false, 2, 8> : k_pupil_rows<false, 2, 16>)
+                                 : (few ? k_pupil_rows<false, 1, 8> : k_pupil_rows<false, 1, 16>));
         launch(kern, dim3(ptiles, w1 - w0, nb), dim3(kThreads), pupil_smem, s, 
             xin, grad.p, tt.p, tbuf.p, hx.fwd.p, lay.p, wfs.p, pad(), w0, nps, nwfs, nxp, nyp, nxtot, ngrad, tw,
             ncols, prows, from_x ? 0 : 1, act());
@@ -424,7 +429,13 @@ void Recon::build_wfs_tables(const mb_recon_desc *d) {
                 MB_REQUIRE(sm[iy * nxp + ix] < 0, "wfs %d: two subapertures share a corner", w);
                 sm[iy * nxp + ix] = s;
             }
-            // GP in CSC: columns are pupil points, rows gradients
+            // GP in CSC: columns are pupil points, rows gradients.  Entries
+            // outside a subaperture's stencil are accepted only as rounding
+            // noise of the GP construction (below 1e-9 of the largest
+            // coefficient, e.g. 1e-14 when dsa is not exact in binary) and
+            // dropped.
+            double gmax = 0;
+            for (long k = 0; k < W.gp_p[np]; k++) gmax = std::max(gmax, std::fabs(W.gp_x[k]));
             for (int col = 0; col < np; col++) {
                 const int px = col % nxp, py = col / nxp;
                 for (int k = W.gp_p[col]; k < W.gp_p[col + 1]; k++) {
@@ -433,7 +444,7 @@ void Recon::build_wfs_tables(const mb_recon_desc *d) {
                     const int s = row < ns ? row : row - ns;
                     const int tx = px - sp[s].x, ty = py - sp[s].y;
                     if (tx < 0 || tx > pos || ty < 0 || ty > pos) {
-                        if (std::fabs(W.gp_x[k]) > 0) {
+                        if (std::fabs(W.gp_x[k]) > 1e-9 * gmax) {
                             set_error("wfs %d: GP couples subaperture %d to a pupil point outside "
                                       "its %dx%d stencil", w, s, n1, n1);
                             throw InvalidArg{MB_EUNSUP};

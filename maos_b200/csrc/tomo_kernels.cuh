@@ -370,7 +370,7 @@ struct PadIndex {
     int kx, ky, maxnx, maxny;
 };
 
-constexpr int kMaxLayers = 12;  // layers unrolled in the Hx gather
+constexpr int kMaxLayers = 16;  // most reconstructed layers (the Hx gather unrolls 8 or 16)
 constexpr int kMaxPadX = 8;     // widest x list
 constexpr int kMaxPadY = 8;     // widest y list (k_hxt_rows is instantiated up to this)
 
@@ -382,7 +382,7 @@ __host__ __device__ constexpr int pupil_rows_smem_floats(int rows, int nxp, int 
 }
 
 // grid: (ceil(nyp/rows), nw, nb), WFS w = wbase + blockIdx.y, all with
-// subaperture/pupil ratio POS.  FROM_X: the operator input is the layer
+// subaperture/pupil ratio POS; ML >= nps bounds the unrolled layer loop.  FROM_X: the operator input is the layer
 // vector x (Hx, GP in shared memory; no tip/tilt term).  Otherwise the input
 // is a gradient vector already in `grad` (right-hand side, or the LHS with
 // the tip/tilt projection), with -PTT g per WFS in `tt` when do_tt.
@@ -390,7 +390,7 @@ __host__ __device__ constexpr int pupil_rows_smem_floats(int rows, int nxp, int 
 // for the pupil-grid stages and whole layer columns for the x half of Hx^T,
 // so per-item index arithmetic is a few adds; index tables are staged in
 // shared memory and a pupil point's layer taps are issued together.
-template <bool FROM_X, int POS>
+template <bool FROM_X, int POS, int ML>
 __global__ void __launch_bounds__(kThreads, 4)
 k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const float *__restrict__ tt,
              float *__restrict__ t, const AxisW *__restrict__ tab, const LayerDev *__restrict__ lay,
@@ -449,7 +449,7 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
             for (int r = ph; r < nh; r += nph) {
                 float acc = 0.f;
 #pragma unroll
-                for (int l = 0; l < kMaxLayers; l++) {
+                for (int l = 0; l < ML; l++) {
                     if (l < nps) {
                         const AxisW tx = s_tab[l * ts + ix], ty = s_tab[l * ts + nxp + r];
                         const bool ok = tx.k >= 0 && ty.k >= 0;
