@@ -13,8 +13,10 @@ the same size (M = 9,745 x 33,840) in FP32, BF16 and FP8-E4M3.
 
 value     aggregate steps/s over all GPUs (N * B * K / max-over-ranks device time),
           inputs resident in HBM, L2 flushed (256 MiB write) before every step.
-e2e       the same metric through the host API mb_tomo (FP64 host gradients in,
-          FP64 host layer OPD out, copies inside the timed region).
+e2e       the same metric through the C ABI with host buffers
+          (mb_recon_serve_step: pinned FP32 gradients in, pinned FP32 DM
+          commands out, copies inside the timed region); the FP64 gpu_tomo +
+          gpu_fit shaped calls are reported beside it.
 roofline  the kernel with the largest share of the step, its algorithmic bytes
           per launch over its measured launch time, against the measured HBM
           copy bandwidth.
@@ -373,24 +375,41 @@ def run_gpu(args):
     p50 = statistics.median(times)
     p99 = times_sorted[min(len(times) - 1, int(math.ceil(0.99 * len(times))) - 1)]
 
-    # end to end through the host API: gpu_tomo then gpu_fit (FP64 host
-    # gradients in, FP64 host actuator commands out)
+    # end to end through the C ABI with host buffers: every step copies that
+    # step's FP32 gradients from pinned host memory, runs the graph step and
+    # copies the DM commands back to pinned host memory
+    # (mb_recon_serve_step with every slot active), timed on the host clock
     K2 = max(3, min(args.steps, 20))
+    allslots = np.ones(B, np.int32)
+    g_pin = [torch.tensor(host_grads[k], dtype=torch.float32).pin_memory() for k in range(nframe)]
+    a_pin = torch.empty((B, int(fit.nact)), dtype=torch.float32).pin_memory()
+
+    def e2e_step(k):
+        R.serve_step(allslots, g_pin[k % nframe].data_ptr(), a_pin.data_ptr(), sp)
+        stream.synchronize()
+
     for k in range(2):
-        R.tomo_only(host_grads[k % nframe])
-        R.fit()
-    torch.cuda.synchronize()
+        e2e_step(k)
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for k in range(K2):
-        R.tomo_only(host_grads[k % nframe])
-        R.fit()
+        e2e_step(k)
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * B * K2 / float(te.item())
+    # the reference-shaped FP64 calls (gpu_tomo then gpu_fit, pageable host
+    # arrays converted on the host), for comparison
+    for k in range(2):
+        R.tomo_only(host_grads[k % nframe])
+        R.fit()
+    t0 = time.perf_counter()
+    for k in range(K2):
+        R.tomo_only(host_grads[k % nframe])
+        R.fit()
+    fp64_api_value = B * K2 / (time.perf_counter() - t0)
 
     # roofline of the dominant kernel (live timing on the reconstructor's stream)
     ns = lib.mb_num_stages()
@@ -455,7 +474,9 @@ def run_gpu(args):
                 "latency_ms": {"p50": p50, "p99": p99, "note": "one batched step of all instances"},
                 "e2e": {"value": e2e_value, "unit": "steps/s",
                         "h2d_bytes_per_step": int(B * sysm.ngrad * 4),
-                        "d2h_bytes_per_step": int(B * fit.nact * 4 + 2 * B * 4)},
+                        "d2h_bytes_per_step": int(B * fit.nact * 4),
+                        "api": "mb_recon_serve_step, pinned FP32 host buffers",
+                        "fp64_gpu_tomo_gpu_fit_steps_per_s": fp64_api_value},
                 "mvm": mvm_line,
                 "served": served,
                 "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,

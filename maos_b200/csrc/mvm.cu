@@ -33,6 +33,10 @@ template <>
 struct Elem<MB_MVM_F32> {
     using T = float;
     static constexpr int kVec = 4;  // elements per 16 bytes
+    __device__ static void from_raw(const uint4 &r, float *v) {
+        v[0] = __uint_as_float(r.x); v[1] = __uint_as_float(r.y);
+        v[2] = __uint_as_float(r.z); v[3] = __uint_as_float(r.w);
+    }
     __device__ static void load(const T *p, float *v) {
         const float4 q = *reinterpret_cast<const float4 *>(p);
         v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
@@ -42,6 +46,15 @@ template <>
 struct Elem<MB_MVM_BF16> {
     using T = __nv_bfloat16;
     static constexpr int kVec = 8;
+    __device__ static void from_raw(const uint4 &q, float *v) {
+        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float2 f = __bfloat1622float2(h[i]);
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+        }
+    }
     __device__ static void load(const T *p, float *v) {
         const uint4 q = *reinterpret_cast<const uint4 *>(p);
         const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
@@ -57,6 +70,15 @@ template <>
 struct Elem<MB_MVM_FP8> {
     using T = __nv_fp8_e4m3;
     static constexpr int kVec = 16;
+    __device__ static void from_raw(const uint4 &q, float *v) {
+        const __nv_fp8x2_e4m3 *h = reinterpret_cast<const __nv_fp8x2_e4m3 *>(&q);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const float2 f = static_cast<float2>(h[i]);
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+        }
+    }
     __device__ static void load(const T *p, float *v) {
         const uint4 q = *reinterpret_cast<const uint4 *>(p);
         const __nv_fp8x2_e4m3 *h = reinterpret_cast<const __nv_fp8x2_e4m3 *>(&q);
@@ -87,36 +109,125 @@ k_mvm_split(const typename Elem<DT>::T *__restrict__ M, long ldm, const float *_
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int kRowsPerWarp = kRows / (kMvmThreads / 32);
-    for (int rr = 0; rr < kRowsPerWarp; rr++) {
-        const int row = blockIdx.x * kRows + warp * kRowsPerWarp + rr;
-        if (row >= nact) break;
-        const typename E::T *mrow = M + (size_t)row * ldm + k0;
-        float acc[NB];
+    // small batches: a warp carries RW rows at once, so every lane keeps RW
+    // independent 16-byte loads in flight and each staged gradient value
+    // serves RW rows
+    constexpr int RW = NB <= 2 ? kRowsPerWarp : 1;
+    for (int rr = 0; rr < kRowsPerWarp; rr += RW) {
+        const int row0 = blockIdx.x * kRows + warp * kRowsPerWarp + rr;
+        if (row0 >= nact) break;
+        const typename E::T *mrow[RW];
+        bool live[RW];
 #pragma unroll
-        for (int b = 0; b < NB; b++) acc[b] = 0.f;
+        for (int q = 0; q < RW; q++) {
+            live[q] = row0 + q < nact;
+            mrow[q] = M + (size_t)(live[q] ? row0 + q : row0) * ldm + k0;
+        }
+        float acc[RW][NB];
+#pragma unroll
+        for (int q = 0; q < RW; q++)
+#pragma unroll
+            for (int b = 0; b < NB; b++) acc[q][b] = 0.f;
         // lanes stride by V elements; the slab is a multiple of 32*V elements
         for (int c = lane * V; c < kK; c += 32 * V) {
-            float v[V];
-            E::load(mrow + c, v);
+            float v[RW][V];
+#pragma unroll
+            for (int q = 0; q < RW; q++) E::load(mrow[q] + c, v[q]);
 #pragma unroll
             for (int b = 0; b < NB; b++) {
                 const float4 *gb = reinterpret_cast<const float4 *>(sg + b * kK + c);
 #pragma unroll
                 for (int e4 = 0; e4 < V / 4; e4++) {
-                    const float4 q = gb[e4];
-                    acc[b] += v[4 * e4] * q.x + v[4 * e4 + 1] * q.y + v[4 * e4 + 2] * q.z +
-                              v[4 * e4 + 3] * q.w;
+                    const float4 g4 = gb[e4];
+#pragma unroll
+                    for (int q = 0; q < RW; q++)
+                        acc[q][b] += v[q][4 * e4] * g4.x + v[q][4 * e4 + 1] * g4.y + v[q][4 * e4 + 2] * g4.z +
+                                     v[q][4 * e4 + 3] * g4.w;
                 }
             }
         }
 #pragma unroll
-        for (int b = 0; b < NB; b++) {
-            float t = acc[b];
+        for (int q = 0; q < RW; q++)
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-            if (lane == 0 && b0 + b < nbatch) part[((size_t)ks * nbatch + b0 + b) * nact + row] = t;
+            for (int b = 0; b < NB; b++) {
+                float t = acc[q][b];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+                if (lane == 0 && live[q] && b0 + b < nbatch)
+                    part[((size_t)ks * nbatch + b0 + b) * nact + row0 + q] = t;
+            }
+    }
+}
+
+// Batched form (NB >= 4): a thread owns kRT rows and all NB instances
+// (kRT x NB accumulators in registers).  Each step reads 16 bytes of each of
+// its rows (all kRT loads issued together) and, per element, one gradient
+// vector of NB values from shared memory as a broadcast (every lane reads the
+// same address) that feeds kRT x NB FMAs.
+// part[(ks*nbatch + b)*nact + row]; grid: (ceil(nact/(kRowThreads*kRT)), nks)
+constexpr int kRT = 4;
+constexpr int kRowThreads = 128;
+
+template <int DT, int NB>
+__global__ void __launch_bounds__(kRowThreads)
+k_mvm_rows(const typename Elem<DT>::T *__restrict__ M, long ldm, const float *__restrict__ g, long ngrad,
+           float *__restrict__ part, int nact, int nbatch, int b0) {
+    static_assert(NB % 4 == 0, "batched form takes multiples of 4 instances");
+    using E = Elem<DT>;
+    constexpr int V = E::kVec;
+    extern __shared__ float sg[];  // [kK][NB]: the NB values of one column are adjacent
+    const int ks = blockIdx.y;
+    const long k0 = (long)ks * kK;
+    const int kn = (int)((ngrad - k0) < kK ? (ngrad - k0) : kK);
+    for (int i = threadIdx.x; i < NB * kK; i += blockDim.x) {
+        const int b = i / kK, k = i - b * kK;
+        sg[k * NB + b] = (b0 + b < nbatch && k < kn) ? g[(size_t)(b0 + b) * ngrad + k0 + k] : 0.f;
+    }
+    __syncthreads();
+    // rows r0 + q*kRowThreads: the lanes of a warp own consecutive rows
+    const int r0 = blockIdx.x * kRowThreads * kRT + threadIdx.x;
+    const typename E::T *mrow[kRT];
+    bool live[kRT];
+#pragma unroll
+    for (int q = 0; q < kRT; q++) {
+        const int row = r0 + q * kRowThreads;
+        live[q] = row < nact;
+        mrow[q] = M + (size_t)(live[q] ? row : 0) * ldm + k0;
+    }
+    float acc[kRT][NB];
+#pragma unroll
+    for (int q = 0; q < kRT; q++)
+#pragma unroll
+        for (int b = 0; b < NB; b++) acc[q][b] = 0.f;
+    for (int c = 0; c < kK; c += V) {
+        uint4 raw[kRT];
+#pragma unroll
+        for (int q = 0; q < kRT; q++) raw[q] = *reinterpret_cast<const uint4 *>(mrow[q] + c);
+        float v[kRT][V];
+#pragma unroll
+        for (int q = 0; q < kRT; q++) E::from_raw(raw[q], v[q]);
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            const float4 *gc = reinterpret_cast<const float4 *>(sg + (c + e) * NB);
+#pragma unroll
+            for (int u = 0; u < NB / 4; u++) {
+                const float4 g4 = gc[u];
+#pragma unroll
+                for (int q = 0; q < kRT; q++) {
+                    acc[q][4 * u] += v[q][e] * g4.x;
+                    acc[q][4 * u + 1] += v[q][e] * g4.y;
+                    acc[q][4 * u + 2] += v[q][e] * g4.z;
+                    acc[q][4 * u + 3] += v[q][e] * g4.w;
+                }
+            }
         }
     }
+#pragma unroll
+    for (int q = 0; q < kRT; q++)
+        if (live[q])
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+                if (b0 + b < nbatch) part[((size_t)ks * nbatch + b0 + b) * nact + r0 + q * kRowThreads] = acc[q][b];
 }
 
 // out[b][row] = scale[row] * sum_ks part[ks][b][row]
@@ -145,15 +256,20 @@ struct Mvm {
     void launch_t(const float *dg, float *dout, cudaStream_t s) {
         const size_t smem = (size_t)NB * kK * sizeof(float);
         static bool attr = false;
+        auto kern = [] {
+            if constexpr (NB >= 4) return k_mvm_rows<DT, NB>;
+            else return k_mvm_split<DT, NB>;
+        }();
         if (!attr) {
-            MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_split<DT, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem));
+            MB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr = true;
         }
-        const dim3 grid((nact + kRows - 1) / kRows, nks);
+        const dim3 grid(NB >= 4 ? (nact + kRowThreads * kRT - 1) / (kRowThreads * kRT) : (nact + kRows - 1) / kRows,
+                        nks);
+        const int threads = NB >= 4 ? kRowThreads : kMvmThreads;
         for (int b0 = 0; b0 < nbatch; b0 += NB) {
-            k_mvm_split<DT, NB><<<grid, kMvmThreads, smem, s>>>(
-                reinterpret_cast<const typename Elem<DT>::T *>(m.p), ldm, dg, ngrad, part.p, nact, nbatch, b0);
+            kern<<<grid, threads, smem, s>>>(reinterpret_cast<const typename Elem<DT>::T *>(m.p), ldm, dg, ngrad,
+                                            part.p, nact, nbatch, b0);
             MB_CHECK_LAUNCH();
         }
         const long n = (long)nact * nbatch;

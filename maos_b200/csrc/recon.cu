@@ -177,6 +177,8 @@ struct Recon {
     void build(const mb_recon_desc *d);
     void build_hx_tables(const mb_recon_desc *d);
     void build_pad();
+    void set_pupil_rows(int rows);
+    int autotune(int reps, float *ms_out);
     void pupil_rows(bool from_x, const float *xin, cudaStream_t s);
     void hxt_rows(const float *xin, float *out, double *dot_part, int do_l2, int k, cudaStream_t s);
     void build_wfs_tables(const mb_recon_desc *d);
@@ -348,16 +350,25 @@ void Recon::build_pad() {
     ypad.upload(yp);
     // pupil rows per CTA: the largest of 16, 8, 4 that still gives about two
     // waves of 256-thread CTAs on 148 SMs (4 resident each)
-    prows = 16;
-    while (prows > 4 && (long)((nyp + prows - 1) / prows) * nwfs * nb < 2 * 148 * 4) prows /= 2;
+    // pupil rows per CTA: the largest of 16, 8, 4 that still gives about two
+    // waves of 256-thread CTAs on 148 SMs (4 resident each); Recon::autotune
+    // replaces this guess by measurement
+    int rows = 16;
+    while (rows > 4 && (long)((nyp + rows - 1) / rows) * nwfs * nb < 2 * 148 * 4) rows /= 2;
     if (const char *e = std::getenv("MAOS_B200_PUPIL_ROWS")) {  // tuning override
         const int v = std::atoi(e);
-        if (v >= 1 && v <= 64) prows = v;
+        if (v >= 1 && v <= 64) rows = v;
     }
-    ptiles = (nyp + prows - 1) / prows;
     tw = (long)nyp * ncols;
-    pupil_smem = (size_t)pupil_rows_smem_floats(prows, nxp, nps, ncols, kx) * sizeof(float);
-    MB_REQUIRE(pupil_smem <= 200 * 1024, "pupil row block needs %zu bytes of shared memory", pupil_smem);
+    set_pupil_rows(rows);
+}
+
+void Recon::set_pupil_rows(int rows) {
+    const size_t sm = (size_t)pupil_rows_smem_floats(rows, nxp, nps, ncols, kx) * sizeof(float);
+    MB_REQUIRE(sm <= 200 * 1024, "pupil row block needs %zu bytes of shared memory", sm);
+    prows = rows;
+    ptiles = (nyp + prows - 1) / prows;
+    pupil_smem = sm;
     for (auto k : {k_pupil_rows<true, 1, 8>, k_pupil_rows<true, 2, 8>, k_pupil_rows<false, 1, 8>,
                    k_pupil_rows<false, 2, 8>, k_pupil_rows<true, 1, 16>, k_pupil_rows<true, 2, 16>,
                    k_pupil_rows<false, 1, 16>, k_pupil_rows<false, 2, 16>})
@@ -1016,6 +1027,43 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     cudaEventDestroy(e1);
 }
 
+// Time the tomography operator with each admissible pupil-row blocking and
+// keep the fastest (results do not depend on the blocking); the graphs are
+// captured again.  ms_out[i]: ms per operator for 4, 8, 16 rows (-1: not
+// admissible).  Returns the rows kept.
+int Recon::autotune(int reps, float *ms_out) {
+    const int cand[3] = {4, 8, 16};
+    set_mask(nullptr, stream);
+    cudaEvent_t e0, e1;
+    MB_CUDA_TRY(cudaEventCreate(&e0));
+    MB_CUDA_TRY(cudaEventCreate(&e1));
+    int best = prows;
+    float tbest = 1e30f;
+    for (int c = 0; c < 3; c++) {
+        if (ms_out) ms_out[c] = -1.f;
+        if ((size_t)pupil_rows_smem_floats(cand[c], nxp, nps, ncols, kx) * sizeof(float) > 200 * 1024) continue;
+        set_pupil_rows(cand[c]);
+        op_lhs(p.p, Ap.p, nullptr, stream);  // warm
+        MB_CUDA_TRY(cudaEventRecord(e0, stream));
+        for (int i = 0; i < reps; i++) op_lhs(p.p, Ap.p, nullptr, stream);
+        MB_CUDA_TRY(cudaEventRecord(e1, stream));
+        MB_CUDA_TRY(cudaEventSynchronize(e1));
+        float t = 0;
+        MB_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+        t /= reps;
+        if (ms_out) ms_out[c] = t;
+        if (t < tbest) {
+            tbest = t;
+            best = cand[c];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    set_pupil_rows(best);
+    capture_graph();
+    return best;
+}
+
 cudaGraphExec_t Recon::capture(const std::function<void(cudaStream_t)> &body, long &nkernels) {
     cudaGraph_t g = nullptr;
     const long before = g_launches.load();
@@ -1308,6 +1356,15 @@ int mb_time_stages(mb_recon *h, int reps, float *ms, double *bytes, int *launche
     MB_API_BEGIN
     MB_REQUIRE(h && ms && bytes && launches && reps > 0, "invalid arguments");
     h->R.time_stages(reps, ms, bytes, launches);
+    MB_API_END
+}
+
+int mb_autotune(mb_recon *h, int reps, int *rows, float *ms) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && reps > 0, "invalid arguments");
+    MB_CUDA_TRY(cudaStreamSynchronize(h->R.stream));
+    const int r = h->R.autotune(reps, ms);
+    if (rows) *rows = r;
     MB_API_END
 }
 

@@ -83,6 +83,7 @@ SIGNATURES = {
     "mb_slot_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "mb_recon_step_slots": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p]),
     "mb_recon_serve_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mb_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "mb_ngrad": (C.c_long, [C.c_void_p]),
     "mb_nxtot": (C.c_long, [C.c_void_p]),
     "mb_nbatch": (C.c_int, [C.c_void_p]),

@@ -156,6 +156,14 @@ class Reconstructor:
         a = np.ascontiguousarray(a, dtype=np.float64).reshape(self.nbatch, n)
         return a
 
+    def autotune(self, reps: int = 20):
+        """Pick the fastest pupil-row blocking for this batch (mb_autotune);
+        returns (rows kept, {rows: ms per operator})."""
+        rows = C.c_int()
+        ms = (C.c_float * 3)()
+        check(self.lib.mb_autotune(self.h, int(reps), C.byref(rows), ms), "mb_autotune")
+        return rows.value, {r: ms[i] for i, r in enumerate((4, 8, 16)) if ms[i] >= 0}
+
     def reset(self):
         check(self.lib.mb_recon_reset(self.h), "mb_recon_reset")
 

@@ -116,3 +116,21 @@ def test_integrated_tip_tilt_split0(name):
             assert rel(xs[b], w) < SOLVE_TOL
     finally:
         R.close()
+
+
+def test_autotune_keeps_results():
+    """The autotuner only changes the pupil-row blocking: same solution bit for bit."""
+    from conftest import get_system
+    from maos_b200.recon import Reconstructor
+    s = get_system("mcao_30m")
+    g = np.random.default_rng(9).standard_normal((4, s.ngrad)) * 1e-6
+    R = Reconstructor(s, nbatch=4)
+    try:
+        x0, _ = R.tomo(g)
+        rows, ms = R.autotune(reps=3)
+        assert rows in ms and ms[rows] == min(ms.values())
+        R.reset()
+        x1, _ = R.tomo(g)
+        assert np.array_equal(x0, x1)
+    finally:
+        R.close()
