@@ -14,11 +14,13 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstdint>
 #include <mutex>
 #include <vector>
 
 #include "common.cuh"
+#include "mvm_tc.cuh"
 
 namespace mb {
 
@@ -247,6 +249,7 @@ struct Mvm {
     long ngrad = 0, ldm = 0;
     DevBuf<unsigned char> m;  // raw storage
     DevBuf<float> scale, part, g, out;
+    DevBuf<int> err;  // set when a tensor-core MMA wait timed out
     cudaStream_t stream = nullptr;
     ~Mvm() {
         if (stream) cudaStreamDestroy(stream);
@@ -277,8 +280,42 @@ struct Mvm {
                                                                 dout, nact, nbatch, nks);
         MB_CHECK_LAUNCH();
     }
+    // Batches of 4 or more with BF16 or FP8 storage: the GEMM on the tensor
+    // cores (mvm_tc.cuh); MAOS_B200_MVM_TC=0 keeps the FMA kernels.
+    static bool tc_enabled() {
+        static const bool on = [] {
+            const char *e = std::getenv("MAOS_B200_MVM_TC");
+            return !(e && e[0] == '0');
+        }();
+        return on;
+    }
+    template <int DT, int N>
+    void launch_tc(const float *dg, float *dout, cudaStream_t s) {
+        const size_t smem = (size_t)kTcRows * kTcK * 2 + (size_t)kTcTerms * N * kTcK * 2;
+        static bool attr = false;
+        if (!attr) {
+            MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_tc<DT, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr = true;
+        }
+        const dim3 grid((nact + kTcRows - 1) / kTcRows, nks, (nbatch + N - 1) / N);
+        k_mvm_tc<DT, N><<<grid, kTcThreads, smem, s>>>(reinterpret_cast<const typename TcA<DT>::T *>(m.p), ldm, dg,
+                                                      ngrad, part.p, nact, nbatch, kK, err.p);
+        MB_CHECK_LAUNCH();
+        const long n = (long)nact * nbatch;
+        k_mvm_reduce<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part.p, dtype == MB_MVM_FP8 ? scale.p : nullptr,
+                                                                dout, nact, nbatch, nks);
+        MB_CHECK_LAUNCH();
+    }
     template <int DT>
     void launch_dt(const float *dg, float *dout, cudaStream_t s) {
+        if constexpr (DT != MB_MVM_F32) {
+            if (nbatch >= 4 && tc_enabled()) {
+                if (nbatch <= 16) launch_tc<DT, 16>(dg, dout, s);
+                else if (nbatch <= 32) launch_tc<DT, 32>(dg, dout, s);
+                else launch_tc<DT, 64>(dg, dout, s);
+                return;
+            }
+        }
         if (nbatch == 1) launch_t<DT, 1>(dg, dout, s);
         else if (nbatch == 2) launch_t<DT, 2>(dg, dout, s);
         else if (nbatch <= 4) launch_t<DT, 4>(dg, dout, s);
@@ -456,6 +493,8 @@ int mb_mvm_create(const double *Mcol, long nact, long ngrad, int dtype, int nbat
             MB_CUDA_TRY(cudaMemcpy(V.m.p, h8.data(), nel, cudaMemcpyHostToDevice));
         }
         V.scale.upload(sc);
+        V.err.alloc(1);
+        V.err.zero_async(V.stream);
         V.part.alloc((size_t)V.nks * nbatch * nact);
         V.g.alloc((size_t)nbatch * ngrad);
         V.out.alloc((size_t)nbatch * nact);
@@ -544,7 +583,14 @@ int mb_recon_mvm(mb_mvm *h, const double *grad, double *dmout) {
         MB_CUDA_TRY(cudaMemcpyAsync(V.g.p, tmp.data(), ng * 4, cudaMemcpyHostToDevice, V.stream));
         V.apply(V.g.p, V.out.p, V.stream);
         MB_CUDA_TRY(cudaMemcpyAsync(tmp.data(), V.out.p, na * 4, cudaMemcpyDeviceToHost, V.stream));
+        int flag = 0;
+        MB_CUDA_TRY(cudaMemcpyAsync(&flag, V.err.p, sizeof(int), cudaMemcpyDeviceToHost, V.stream));
         MB_CUDA_TRY(cudaStreamSynchronize(V.stream));
+        if (flag) {
+            MB_CUDA_TRY(cudaMemsetAsync(V.err.p, 0, sizeof(int), V.stream));
+            mb::set_error("mb_recon_mvm: a tensor-core MMA did not complete in time");
+            return MB_ECUDA;
+        }
         for (size_t i = 0; i < na; i++) dmout[i] = tmp[i];
     } catch (const mb::CudaError &e) {
         return e.code;

@@ -100,12 +100,13 @@ struct Recon {
     RayTables hx;
     // separable Hx^T: fixed-width transposed lists and the pupil-row buffer
     DevBuf<GatherW> xpad, ypad;
+    DevBuf<int4> footprint;
     int kx = 0, ky = 0, maxnx = 0, maxny = 0;
     int prows = 0, ptiles = 0, ncols = 0;  // pupil rows per CTA, CTAs per WFS, sum of layer widths
     long tw = 0;                           // row-buffer floats per (instance, WFS)
     size_t pupil_smem = 0;
     DevBuf<float> tbuf;
-    PadIndex pad() const { return PadIndex{xpad.p, ypad.p, kx, ky, maxnx, maxny}; }
+    PadIndex pad() const { return PadIndex{xpad.p, ypad.p, footprint.p, kx, ky, maxnx, maxny}; }
     DevBuf<LayerDev> lay;
     std::vector<LayerDev> lay_h;
     std::vector<mb_grid> xgrid;   // host copy of the layer grids
@@ -348,6 +349,25 @@ void Recon::build_pad() {
             }
     xpad.upload(xp);
     ypad.upload(yp);
+    // footprint of every WFS on every layer: first and last+1 column and row
+    // with a non-empty transposed list
+    std::vector<int4> fp((size_t)nwfs * nps);
+    for (int w = 0; w < nwfs; w++)
+        for (int l = 0; l < nps; l++) {
+            int lo[2] = {INT32_MAX, INT32_MAX}, hi[2] = {-1, -1};
+            for (int axis = 0; axis < 2; axis++) {
+                const int tb = hx.h_ptr[(w * nps + l) * 2 + axis];
+                const int n = axis ? lay_h[l].ny : lay_h[l].nx;
+                for (int j = 0; j < n; j++)
+                    if (hx.h_idxptr[tb + j + 1] > hx.h_idxptr[tb + j]) {
+                        lo[axis] = std::min(lo[axis], j);
+                        hi[axis] = j;
+                    }
+            }
+            fp[(size_t)w * nps + l] = hi[0] < 0 || hi[1] < 0 ? make_int4(0, 0, 0, 0)
+                                                             : make_int4(lo[0], hi[0] + 1, lo[1], hi[1] + 1);
+        }
+    footprint.upload(fp);
     // pupil rows per CTA: the largest of 16, 8, 4 that still gives about two
     // waves of 256-thread CTAs on 148 SMs (4 resident each)
     // pupil rows per CTA: the largest of 16, 8, 4 that still gives about two

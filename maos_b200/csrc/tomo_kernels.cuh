@@ -362,11 +362,14 @@ __global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ 
 // point with the y half over all WFS, adds L2^T L2 x and the p.Ap partial.
 // The transposed lists are stored with a fixed width (padding: weight 0 on
 // pupil index 0), in the same order as the CSR lists, so the sums are the
-// exact adjoint of Hx and independent of the tiling.
+// exact adjoint of Hx and independent of the tiling.  Only the footprint of
+// each WFS on each layer (the columns and rows whose lists are not empty) is
+// computed and read; outside it every term is an exact zero.
 // ---------------------------------------------------------------------------
 struct PadIndex {
     const GatherW *x;   // [(w*ncols + tcol_l + jx)*kx + e]   (per WFS, all layers' columns)
     const GatherW *y;   // [((w*nps + l)*maxny + jy)*ky + e]
+    const int4 *fp;     // [w*nps + l]: footprint of the WFS on the layer: columns [x, y), rows [z, w)
     int kx, ky, maxnx, maxny;
 };
 
@@ -530,6 +533,8 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
             int l = 0;
             while (l + 1 < nps && c >= s_tcol[l + 1]) l++;
             const int tc = s_tcol[l], lnx = s_lnx[l];
+            const int4 f = pi.fp[w * nps + l];
+            if (c - tc < f.x || c - tc >= f.y) continue;  // no pupil column reaches it: never read
             GatherW e[kMaxPadX];
 #pragma unroll
             for (int k = 0; k < kMaxPadX; k++) e[k] = k < kx ? s_xp[c * kx + k] : GatherW{0, 0.f};
@@ -574,6 +579,8 @@ k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__
         float acc = 0.f;
 #pragma unroll 2
         for (int w = 0; w < nwfs; w++, e += estep, tl += tw) {
+            const int4 f = pi.fp[w * nps + l];
+            if (jx < f.x || jx >= f.y || jy < f.z || jy >= f.w) continue;  // outside this WFS's footprint
             GatherW ge[KY];
             float tv[KY];
 #pragma unroll

@@ -18,7 +18,8 @@ continuously:
   tomography + fit on the pool's own stream (``mb_recon_serve_step``: the
   uploads, the masked step and the downloads in one call);
 * pools run on separate streams, so batches of different sizes overlap on the
-  device;
+  device; the streams carry priorities by step cost (cheapest highest), so
+  short steps are not queued behind long ones on the SMs;
 * requests that arrive while a batch is in flight wait for the next one;
 * when a batch completes, each active slot's DM commands have been copied
   back and the request's latency (arrival to result on the host) is recorded.
@@ -64,6 +65,30 @@ class Request:
     dropped: bool = field(default=False, compare=False)
 
 
+def step_cost(stype: SystemType) -> float:
+    """Relative device work of one step of one system (unknowns x iterations)."""
+    t = stype.tomo
+    return float(t.nx_total) * (t.cfg.tomo_maxit + 2) + float(stype.nact) * (stype.fit.maxit + 2)
+
+
+def stream_priorities(types: List[SystemType]) -> List[int]:
+    """CUDA stream priority per pool: the cheapest system type gets the
+    highest priority, so short steps are not queued behind long ones on the
+    SMs (shortest job first); distinct costs map onto the device's range."""
+    try:
+        import torch
+        least, greatest = torch.cuda.Stream.priority_range()
+    except Exception:
+        least, greatest = 0, 0
+    order = sorted(set(step_cost(t) for t in types))
+    levels = list(range(greatest, least + 1))  # greatest (highest priority) first
+    out = []
+    for t in types:
+        k = order.index(step_cost(t))
+        out.append(levels[min(k, len(levels) - 1)] if len(order) > 1 else least)
+    return out
+
+
 def slot_footprint_bytes(stype: SystemType) -> int:
     """Device bytes one slot of this type holds (vectors, scratch, spectra)."""
     t = stype.tomo
@@ -78,13 +103,13 @@ def slot_footprint_bytes(stype: SystemType) -> int:
 class Pool:
     """One reconstructor with `capacity` slots for one system type."""
 
-    def __init__(self, stype: SystemType, device: int = 0):
+    def __init__(self, stype: SystemType, device: int = 0, priority: int = 0):
         import torch
         from .recon import Reconstructor
         self.type = stype
         self.cap = stype.capacity
         self.R = Reconstructor(stype.tomo, nbatch=self.cap, fit=stype.fit, device=device)
-        self.stream = torch.cuda.Stream(device=device)
+        self.stream = torch.cuda.Stream(device=device, priority=priority)
         self.owner: List[Optional[int]] = [None] * self.cap
         self.queue: Dict[int, List[Request]] = {}
         self.inflight: Optional[Tuple[object, List[Tuple[int, Request]]]] = None
@@ -174,9 +199,12 @@ class Server:
 
     def __init__(self, types: List[SystemType], hbm_budget: int,
                  pool_factory: Optional[Callable[[SystemType], object]] = None,
-                 drop_stale: bool = False, slot_bytes: Optional[List[int]] = None):
-        factory = pool_factory or Pool
-        self.pools = [factory(t) for t in types]
+                 drop_stale: bool = False, slot_bytes: Optional[List[int]] = None, prioritize: bool = True):
+        if pool_factory is None:
+            prio = stream_priorities(types) if prioritize else [0] * len(types)
+            self.pools = [Pool(t, priority=p) for t, p in zip(types, prio)]
+        else:
+            self.pools = [pool_factory(t) for t in types]
         self.slot_bytes = slot_bytes or [slot_footprint_bytes(t) for t in types]
         self.budget = int(hbm_budget)
         self.used = 0

@@ -69,7 +69,7 @@ def _types(cap=(2, 1)):
     t = []
     for k, c in enumerate(cap):
         tomo = SimpleNamespace(ngrad=8 + k, nx_total=10, pmap=SimpleNamespace(n=4), wfs=[0], fdpcg=None)
-        fit = SimpleNamespace(nact=3 + k, thetax=[0.0], floc=SimpleNamespace(n=4))
+        fit = SimpleNamespace(nact=3 + k, thetax=[0.0], floc=SimpleNamespace(n=4), maxit=4)
         t.append(serve.SystemType(f"t{k}", tomo, fit, capacity=c))
     return t
 
@@ -159,3 +159,13 @@ def test_run_served_poisson_with_departures():
     assert st["n"] == 25 and st["p99_ms"] >= st["p50_ms"] >= 0
     # waiters got slots as others left (3 systems of type 0 for 2 slots, 2 of type 1 for 1 slot)
     assert len(srv.admit_log) == 5
+
+
+def test_priorities_favour_cheap_steps():
+    t = _types((1, 1))
+    t[0].tomo.cfg = SimpleNamespace(tomo_maxit=30)
+    t[1].tomo.cfg = SimpleNamespace(tomo_maxit=30)
+    t[1].tomo.nx_total = 1000
+    assert serve.step_cost(t[0]) < serve.step_cost(t[1])
+    p = serve.stream_priorities(t)
+    assert p[0] <= p[1]   # lower number = higher priority in CUDA
