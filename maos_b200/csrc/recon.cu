@@ -414,14 +414,18 @@ void Recon::pupil_rows(bool from_x, const float *xin, cudaStream_t s) {
     }
 }
 
-// k_hxt_rows at the padded y-list width.
+// k_hxt_rows at the padded y-list width, two instances per thread when the
+// batch has more than one.
 void Recon::hxt_rows(const float *xin, float *out, double *dot_part, int do_l2, int k, cudaStream_t s) {
     using K = void (*)(const float *, const float *, float *, double *, PadIndex, const LayerDev *, int, int, int,
-                       long, long, int, CgScal, int, const int *);
-    static const K tabk[kMaxPadY] = {k_hxt_rows<1>, k_hxt_rows<2>, k_hxt_rows<3>, k_hxt_rows<4>,
-                                     k_hxt_rows<5>, k_hxt_rows<6>, k_hxt_rows<7>, k_hxt_rows<8>};
-    launch(tabk[ky - 1], dim3(nblk_x, nb), dim3(kThreads), 0, s, tbuf.p, xin, out, dot_part, pad(), lay.p, nps, nwfs, nyp,
-                                                        nxtot, tw, do_l2, scal(), k, act());
+                       long, long, int, CgScal, int, int, const int *);
+    static const K tab1[kMaxPadY] = {k_hxt_rows<1, 1>, k_hxt_rows<2, 1>, k_hxt_rows<3, 1>, k_hxt_rows<4, 1>,
+                                     k_hxt_rows<5, 1>, k_hxt_rows<6, 1>, k_hxt_rows<7, 1>, k_hxt_rows<8, 1>};
+    static const K tab2[kMaxPadY] = {k_hxt_rows<1, 2>, k_hxt_rows<2, 2>, k_hxt_rows<3, 2>, k_hxt_rows<4, 2>,
+                                     k_hxt_rows<5, 2>, k_hxt_rows<6, 2>, k_hxt_rows<7, 2>, k_hxt_rows<8, 2>};
+    const int ni = nb > 1 ? 2 : 1;
+    launch(ni == 2 ? tab2[ky - 1] : tab1[ky - 1], dim3(nblk_x, (nb + ni - 1) / ni), dim3(kThreads), 0, s, tbuf.p,
+           xin, out, dot_part, pad(), lay.p, nps, nwfs, nyp, nxtot, tw, do_l2, scal(), k, nb, act());
 }
 
 void Recon::build_wfs_tables(const mb_recon_desc *d) {

@@ -552,20 +552,31 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
 }
 
 // y half of Hx^T over all WFS, + L2^T L2 x and p.Ap partials (last block:
-// alpha).  One thread per layer point; grid: (ceil(nxtot/256), nb).  KY is
-// the padded y-list width: a WFS's KY row loads are issued together.
-template <int KY>
+// alpha).  One thread per layer point and NI instances (the index work, the
+// footprint tests and the list entries are shared by the instances, and each
+// dependent step issues NI times the independent loads);
+// grid: (ceil(nxtot/256), ceil(nb/NI)).  KY is the padded y-list width.
+template <int KY, int NI>
 __global__ void __launch_bounds__(kThreads)
 k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__restrict__ out,
            double *__restrict__ dot_part, PadIndex pi, const LayerDev *__restrict__ lay, int nps,
-           int nwfs, int nyp, long nxtot, long tw, int do_l2, CgScal S, int kit,
+           int nwfs, int nyp, long nxtot, long tw, int do_l2, CgScal S, int kit, int nb,
            const int *__restrict__ act) {
     pdl_enter();
-    const int b = blockIdx.y;
-    if (inactive(act, b)) return;
+    const int b0 = blockIdx.y * NI;
+    bool on[NI];
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < NI; q++) {
+        on[q] = b0 + q < nb && !inactive(act, b0 + q);
+        any = any || on[q];
+    }
+    if (!any) return;
     __shared__ double sh[32];
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    double dotv = 0;
+    double dotv[NI];
+#pragma unroll
+    for (int q = 0; q < NI; q++) dotv[q] = 0;
     if (j < nxtot) {
         int l = 0;
         while (l + 1 < nps && j >= lay[l + 1].off) l++;
@@ -573,44 +584,62 @@ k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__
         const int nx = L.nx, ny = L.ny;
         const int jj = (int)(j - L.off);
         const int jy = jj / nx, jx = jj - jy * nx;
-        const float *tl = t + (size_t)b * nwfs * tw + (size_t)nyp * L.tcol + jx;
+        const float *tl = t + (size_t)b0 * nwfs * tw + (size_t)nyp * L.tcol + jx;
+        const size_t tinst = (size_t)nwfs * tw;  // row-buffer stride between instances
         const GatherW *e = pi.y + ((size_t)l * pi.maxny + jy) * KY;
         const int estep = nps * pi.maxny * KY;
-        float acc = 0.f;
+        float acc[NI];
+#pragma unroll
+        for (int q = 0; q < NI; q++) acc[q] = 0.f;
 #pragma unroll 2
         for (int w = 0; w < nwfs; w++, e += estep, tl += tw) {
             const int4 f = pi.fp[w * nps + l];
             if (jx < f.x || jx >= f.y || jy < f.z || jy >= f.w) continue;  // outside this WFS's footprint
             GatherW ge[KY];
-            float tv[KY];
+            float tv[NI][KY];
 #pragma unroll
             for (int k = 0; k < KY; k++) ge[k] = e[k];
 #pragma unroll
-            for (int k = 0; k < KY; k++) tv[k] = tl[ge[k].i * nx];
-            float sy = 0.f;
+            for (int q = 0; q < NI; q++)
 #pragma unroll
-            for (int k = 0; k < KY; k++) sy += ge[k].w * tv[k];
-            acc += sy;
+                for (int k = 0; k < KY; k++) tv[q][k] = on[q] ? tl[q * tinst + ge[k].i * nx] : 0.f;
+#pragma unroll
+            for (int q = 0; q < NI; q++) {
+                float sy = 0.f;
+#pragma unroll
+                for (int k = 0; k < KY; k++) sy += ge[k].w * tv[q][k];
+                acc[q] += sy;
+            }
         }
-        const float *X = xin ? xin + (size_t)b * nxtot + L.off : nullptr;
-        float v = acc;
-        if (do_l2) {  // periodic 13-point biharmonic stencil (tomo.cu gpu_laplacian_do)
-            auto wy = [&](int d) { int y = jy + d; y += (y < 0) ? ny : 0; y -= (y >= ny) ? ny : 0; return X + y * nx; };
-            auto wx = [&](int d) { int q = jx + d; q += (q < 0) ? nx : 0; q -= (q >= nx) ? nx : 0; return q; };
-            const float *Rm2 = wy(-2), *Rm1 = wy(-1), *R0 = X + jy * nx, *Rp1 = wy(1), *Rp2 = wy(2);
-            const int xm2 = wx(-2), xm1 = wx(-1), xp1 = wx(1), xp2 = wx(2);
-            const float st = 20.f * R0[jx] - 8.f * (R0[xm1] + R0[xp1] + Rm1[jx] + Rp1[jx]) +
-                             2.f * (Rm1[xm1] + Rm1[xp1] + Rp1[xm1] + Rp1[xp1]) +
-                             (Rm2[jx] + R0[xm2] + R0[xp2] + Rp2[jx]);
-            v += L.l2c * st;
+#pragma unroll
+        for (int q = 0; q < NI; q++) {
+            if (!on[q]) continue;
+            const int b = b0 + q;
+            const float *X = xin ? xin + (size_t)b * nxtot + L.off : nullptr;
+            float v = acc[q];
+            if (do_l2) {  // periodic 13-point biharmonic stencil (tomo.cu gpu_laplacian_do)
+                auto wy = [&](int d) { int y = jy + d; y += (y < 0) ? ny : 0; y -= (y >= ny) ? ny : 0; return X + y * nx; };
+                auto wx = [&](int d) { int u = jx + d; u += (u < 0) ? nx : 0; u -= (u >= nx) ? nx : 0; return u; };
+                const float *Rm2 = wy(-2), *Rm1 = wy(-1), *R0 = X + jy * nx, *Rp1 = wy(1), *Rp2 = wy(2);
+                const int xm2 = wx(-2), xm1 = wx(-1), xp1 = wx(1), xp2 = wx(2);
+                const float st = 20.f * R0[jx] - 8.f * (R0[xm1] + R0[xp1] + Rm1[jx] + Rp1[jx]) +
+                                 2.f * (Rm1[xm1] + Rm1[xp1] + Rp1[xm1] + Rp1[xp1]) +
+                                 (Rm2[jx] + R0[xm2] + R0[xp2] + Rp2[jx]);
+                v += L.l2c * st;
+            }
+            out[(size_t)b * nxtot + j] = v;
+            if (dot_part && X) dotv[q] = (double)v * (double)X[jj];
         }
-        out[(size_t)b * nxtot + j] = v;
-        if (dot_part && X) dotv = (double)v * (double)X[jj];
     }
     if (dot_part) {
-        dotv = block_sum(dotv, sh);
-        if (threadIdx.x == 0) dot_part[(size_t)b * gridDim.x + blockIdx.x] = dotv;
-        cg_alpha_last(dot_part + (size_t)b * gridDim.x, S, b, kit);
+#pragma unroll
+        for (int q = 0; q < NI; q++) {
+            if (!on[q]) continue;  // uniform over the CTA
+            const int b = b0 + q;
+            const double d = block_sum(dotv[q], sh);
+            if (threadIdx.x == 0) dot_part[(size_t)b * gridDim.x + blockIdx.x] = d;
+            cg_alpha_last(dot_part + (size_t)b * gridDim.x, S, b, kit);
+        }
     }
 }
 
