@@ -253,10 +253,12 @@ def mvm_rates(lib, native, nact: int, ngrad: int, batch: int, stream, M=None):
 SERVE_MIX = (("scao_8m", 26), ("ltao_8m", 26), ("mcao_30m", 12))
 
 
-def served_mix(seconds: float, mcao_frames=None):
+def served_mix(seconds: float, mcao_frames=None, mvm: bool = False):
     """The served mix: 64 systems (26 8 m SCAO, 26 8 m LTAO, 12 30 m MCAO), each
     sending Poisson requests at a rate drawn from U[500, 1000] Hz, all admitted,
-    warm state resident, newest frame wins when a system falls behind."""
+    warm state resident, newest frame wins when a system falls behind.
+    mvm: every type is served by the BF16 MVM of its control matrix (built on
+    the GPU by batched solves) instead of the iterative reconstructor."""
     import numpy as np
     import torch
     from maos_b200 import config, fit_setup, geometry, serve, turbulence
@@ -276,12 +278,28 @@ def served_mix(seconds: float, mcao_frames=None):
         for _ in range(n):
             systems.append((t, float(rng.uniform(500.0, 1000.0)), frames[t]))
     budget = sum(serve.slot_footprint_bytes(t) * t.capacity for t in types)
-    srv = serve.Server(types, budget, drop_stale=True)
-    # warm the graphs of every pool (all slots), then reset the state
-    for p in srv.pools:
-        m = np.ones(p.cap, np.int32)
-        for _ in range(3):
-            p.R.serve_step(m, p.g_host.data_ptr(), p.a_host.data_ptr(), p.stream.cuda_stream)
+    build_s = None
+    if mvm:
+        from maos_b200.mvm_build import build_control_matrix
+        t0 = time.perf_counter()
+        Ms = {t.name: build_control_matrix(t.tomo, t.fit, rhs_batch=256, tomo_maxit=90, fit_maxit=40)[0]
+              for t in types}
+        build_s = time.perf_counter() - t0
+        srv = serve.Server(types, 1 << 62, drop_stale=True,
+                           pool_factory=lambda t: serve.MvmPool(t, Ms[t.name], dtype=1))
+        del Ms
+        import ctypes as C
+        for p in srv.pools:  # warm
+            for _ in range(3):
+                p.lib.mb_mvm_apply_device(p.h, C.c_void_p(p.g_dev.data_ptr()), C.c_void_p(p.a_dev.data_ptr()),
+                                          C.c_void_p(p.stream.cuda_stream))
+    else:
+        srv = serve.Server(types, budget, drop_stale=True)
+        # warm the graphs of every pool (all slots), then reset the state
+        for p in srv.pools:
+            m = np.ones(p.cap, np.int32)
+            for _ in range(3):
+                p.R.serve_step(m, p.g_host.data_ptr(), p.a_host.data_ptr(), p.stream.cuda_stream)
     torch.cuda.synchronize()
     srv, done, wall = serve.run_served(types, systems, duration=seconds, hbm_budget=budget, seed=3,
                                        server=srv)
@@ -289,6 +307,8 @@ def served_mix(seconds: float, mcao_frames=None):
     for r in done + srv.dropped:
         offered[systems[r.system][0]] += 1
     out = {"mix": " + ".join(f"{n} {name}" for name, n in SERVE_MIX),
+           "path": "BF16 MVM of each type's control matrix" if mvm else "FDPCG/CG tomography + fit, FP32",
+           "control_matrix_build_s": build_s,
            "rate_hz": "U[500,1000] Poisson per system", "seconds": seconds,
            "policy": "one masked batch per pool in flight, newest frame wins",
            "hbm_budget_bytes": int(budget),
@@ -447,9 +467,10 @@ def run_gpu(args):
         mvm_line["precision"] = precision
     del Mctl
 
-    served = None
+    served = served_mvm = None
     if world == 1 and not args.no_serve and args.serve_seconds > 0:
         served = served_mix(args.serve_seconds, mcao_frames=fr[0])
+        served_mvm = served_mix(args.serve_seconds, mcao_frames=fr[0], mvm=True)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -479,6 +500,7 @@ def run_gpu(args):
                         "fp64_gpu_tomo_gpu_fit_steps_per_s": fp64_api_value},
                 "mvm": mvm_line,
                 "served": served,
+                "served_mvm": served_mvm,
                 "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)

@@ -190,6 +190,75 @@ class Pool:
         self.R.close()
 
 
+class MvmPool(Pool):
+    """A pool served by the control-matrix MVM instead of the iterative
+    reconstructor: `capacity` rows of a batched MVM (BF16 by default) of the
+    type's control matrix.  The MVM keeps no state between steps, so a slot
+    only maps a system to a row; rows of systems without a request carry zero
+    gradients."""
+
+    def __init__(self, stype: SystemType, M, dtype: int = 1, device: int = 0, priority: int = 0):
+        import ctypes as C
+        import torch
+        from . import native
+        self.type = stype
+        self.cap = stype.capacity
+        self.lib = native.load()
+        Mc = np.asfortranarray(M, dtype=np.float64)
+        h = C.c_void_p()
+        native.check(self.lib.mb_mvm_create(Mc.ctypes.data_as(C.POINTER(C.c_double)), int(M.shape[0]),
+                                            int(M.shape[1]), int(dtype), self.cap, C.byref(h)), "mb_mvm_create")
+        self.h = h
+        self.stream = torch.cuda.Stream(device=device, priority=priority)
+        self.owner = [None] * self.cap
+        self.queue = {}
+        self.inflight = None
+        self.g_host = torch.zeros(self.cap * stype.ngrad, dtype=torch.float32).pin_memory()
+        self.a_host = torch.empty(self.cap * stype.nact, dtype=torch.float32).pin_memory()
+        self.g_dev = torch.zeros(self.cap * stype.ngrad, dtype=torch.float32, device=f"cuda:{device}")
+        self.a_dev = torch.empty(self.cap * stype.nact, dtype=torch.float32, device=f"cuda:{device}")
+        self.batches = 0
+        self.slot_steps = 0
+
+    def admit(self, system: int) -> int:
+        slot = self.free_slots()[0]
+        self.owner[slot] = system
+        self.queue[system] = []
+        return slot
+
+    def try_launch(self, drop_stale: bool = False) -> List[Request]:
+        import ctypes as C
+        import torch
+        from . import native
+        if self.inflight is not None:
+            return []
+        batch, dropped = self.take_batch(drop_stale)
+        if not batch:
+            return dropped
+        ng = self.type.ngrad
+        gh = self.g_host.numpy()
+        gh[:] = 0.0
+        for slot, req in batch:
+            gh[slot * ng:(slot + 1) * ng] = req.grad
+        with torch.cuda.stream(self.stream):
+            self.g_dev.copy_(self.g_host, non_blocking=True)
+            native.check(self.lib.mb_mvm_apply_device(self.h, C.c_void_p(self.g_dev.data_ptr()),
+                                                      C.c_void_p(self.a_dev.data_ptr()),
+                                                      C.c_void_p(self.stream.cuda_stream)), "mb_mvm_apply_device")
+            self.a_host.copy_(self.a_dev, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(self.stream)
+        self.inflight = (ev, batch)
+        self.batches += 1
+        self.slot_steps += len(batch)
+        return dropped
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mb_mvm_free(self.h)
+            self.h = None
+
+
 class Server:
     """Admission, continuous batching and latency accounting over pools.
 

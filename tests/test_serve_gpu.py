@@ -162,3 +162,25 @@ def test_served_mix_replays_standalone():
         assert st["n"] == 5 * nsteps and st["p99_ms"] > 0
     finally:
         srv.close()
+
+
+def test_served_through_bf16_mvm():
+    """Systems served by MvmPool get M_bf16 g for their own gradients (1e-5)."""
+    import torch
+    from conftest import get_fit, get_system
+    from maos_b200 import serve
+    t = serve.SystemType("scao_8m", get_system("scao_8m"), get_fit("scao_8m"), capacity=5)
+    rng = np.random.default_rng(4)
+    M = rng.standard_normal((t.nact, t.ngrad)) * 1e-2
+    systems = [(0, 300.0, (rng.standard_normal((4, t.ngrad)) * 1e-6).astype(np.float32)) for _ in range(5)]
+    srv, done, wall = serve.run_served([t], systems, duration=5.0, hbm_budget=1 << 40, steps_per_system=4, seed=2,
+                                       pool_factory=lambda st: serve.MvmPool(st, M, dtype=1))
+    try:
+        assert len(done) == 20
+        Mb = torch.from_numpy(M).to(torch.bfloat16).to(torch.float64).numpy()
+        for r in done:
+            g = systems[r.system][2][r.step % 4].astype(np.float64)
+            want = Mb @ g
+            assert rel(r.result, want) < 1e-5
+    finally:
+        srv.close()
