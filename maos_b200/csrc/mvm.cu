@@ -4,6 +4,8 @@
 //
 // M is stored row-major [nact][ldm] (ldm = ngrad rounded up to the K tile) in
 // FP32, BF16, or FP8-E4M3 with one FP32 scale per row; accumulation is FP32.
+// A BF16 or FP8 matrix installed for batches of 4 or more is stored instead
+// in the tensor-core tile order of mvm_tc.cuh and multiplied there.
 // The kernel is split-K: CTA (rt, ks) multiplies a tile of kRows rows by a
 // kK-column slab, with that slab of every instance's gradients staged in
 // shared memory, and writes per-split partial sums; a second kernel adds the
@@ -247,7 +249,10 @@ struct Mvm {
     int dtype = MB_MVM_F32;
     int nact = 0, nbatch = 1, nks = 0;
     long ngrad = 0, ldm = 0;
+    bool tiled = false;  // m holds the tensor-core tiles (mvm_tc.cuh) instead of rows
+    long nch = 0;        // 64-column chunks per row when tiled (ldm / 64)
     DevBuf<unsigned char> m;  // raw storage
+    DevBuf<unsigned char> gs;  // tiled: the gradients' BF16 terms (k_gsplit)
     DevBuf<float> scale, part, g, out;
     DevBuf<int> err;  // set when a tensor-core MMA wait timed out
     cudaStream_t stream = nullptr;
@@ -281,7 +286,7 @@ struct Mvm {
         MB_CHECK_LAUNCH();
     }
     // Batches of 4 or more with BF16 or FP8 storage: the GEMM on the tensor
-    // cores (mvm_tc.cuh); MAOS_B200_MVM_TC=0 keeps the FMA kernels.
+    // cores (mvm_tc.cuh); MAOS_B200_MVM_TC=0 (read once) keeps the FMA kernels.
     static bool tc_enabled() {
         static const bool on = [] {
             const char *e = std::getenv("MAOS_B200_MVM_TC");
@@ -291,15 +296,21 @@ struct Mvm {
     }
     template <int DT, int N>
     void launch_tc(const float *dg, float *dout, cudaStream_t s) {
-        const size_t smem = (size_t)kTcRows * kTcK * 2 + (size_t)kTcTerms * N * kTcK * 2;
+        constexpr int smem = tc_smem_bytes(DT, N);
         static bool attr = false;
         if (!attr) {
-            MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_tc<DT, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_tc<DT, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
             attr = true;
         }
-        const dim3 grid((nact + kTcRows - 1) / kTcRows, nks, (nbatch + N - 1) / N);
-        k_mvm_tc<DT, N><<<grid, kTcThreads, smem, s>>>(reinterpret_cast<const typename TcA<DT>::T *>(m.p), ldm, dg,
-                                                      ngrad, part.p, nact, nbatch, kK, err.p);
+        const int nz = (nbatch + N - 1) / N;
+        const long items = (long)nz * nch * N * 8;
+        k_gsplit<N><<<(unsigned)((items + 255) / 256), 256, 0, s>>>(dg, ngrad, nbatch, nch, nz,
+                                                                    reinterpret_cast<char *>(gs.p));
+        MB_CHECK_LAUNCH();
+        const dim3 grid((nact + kTcRows - 1) / kTcRows, nks, nz);
+        k_mvm_tc<DT, N><<<grid, kTcThreads, smem, s>>>(reinterpret_cast<const char *>(m.p),
+                                                      reinterpret_cast<const char *>(gs.p), nch, kK / kTcK, part.p,
+                                                      nact, nbatch, err.p);
         MB_CHECK_LAUNCH();
         const long n = (long)nact * nbatch;
         k_mvm_reduce<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part.p, dtype == MB_MVM_FP8 ? scale.p : nullptr,
@@ -309,7 +320,7 @@ struct Mvm {
     template <int DT>
     void launch_dt(const float *dg, float *dout, cudaStream_t s) {
         if constexpr (DT != MB_MVM_F32) {
-            if (nbatch >= 4 && tc_enabled()) {
+            if (tiled) {
                 if (nbatch <= 16) launch_tc<DT, 16>(dg, dout, s);
                 else if (nbatch <= 32) launch_tc<DT, 32>(dg, dout, s);
                 else launch_tc<DT, 64>(dg, dout, s);
@@ -463,7 +474,20 @@ int mb_mvm_create(const double *Mcol, long nact, long ngrad, int dtype, int nbat
         V.nks = (int)((ngrad + mb::kK - 1) / mb::kK);
         V.ldm = (long)V.nks * mb::kK;
         MB_CUDA_TRY(cudaStreamCreateWithFlags(&V.stream, cudaStreamNonBlocking));
-        const size_t nel = (size_t)nact * V.ldm;
+        // Batches of 4 or more with BF16 or FP8 storage run on the tensor
+        // cores and keep M in their tile order; MAOS_B200_MVM_TC=0 keeps rows.
+        V.tiled = dtype != MB_MVM_F32 && nbatch >= 4 && mb::Mvm::tc_enabled();
+        V.nch = V.ldm / mb::kTcK;
+        const long nrow = V.tiled ? (nact + mb::kTcRows - 1) / mb::kTcRows * mb::kTcRows : nact;
+        const size_t nel = (size_t)nrow * V.ldm;
+        // byte offset of element (r, c) for an element size of el bytes
+        auto at = [&](long r, long c, int el) -> size_t {
+            if (!V.tiled) return ((size_t)r * V.ldm + c) * el;
+            const size_t tile = (size_t)(r / mb::kTcRows) * V.nch + c / mb::kTcK;
+            const int rr = (int)(r % mb::kTcRows), cc = (int)(c % mb::kTcK);
+            return el == 2 ? tile * mb::kTcTileBf16 + mb::tile_off(rr, cc >> 3) + (cc & 7) * 2
+                           : tile * mb::kTcTileFp8 + mb::tc_fp8_off(rr, cc);
+        };
         std::vector<float> sc(nact, 1.f);
         if (dtype == MB_MVM_F32) {
             std::vector<float> h32(nel, 0.f);
@@ -475,7 +499,7 @@ int mb_mvm_create(const double *Mcol, long nact, long ngrad, int dtype, int nbat
             std::vector<__nv_bfloat16> h16(nel, __float2bfloat16(0.f));
             for (long r = 0; r < nact; r++)
                 for (long c = 0; c < ngrad; c++)
-                    h16[(size_t)r * V.ldm + c] = __float2bfloat16((float)Mcol[(size_t)c * nact + r]);
+                    h16[at(r, c, 2) / 2] = __float2bfloat16((float)Mcol[(size_t)c * nact + r]);
             V.m.alloc(nel * 2);
             MB_CUDA_TRY(cudaMemcpy(V.m.p, h16.data(), nel * 2, cudaMemcpyHostToDevice));
         } else {
@@ -487,10 +511,14 @@ int mb_mvm_create(const double *Mcol, long nact, long ngrad, int dtype, int nbat
                 const double s = mx > 0 ? mx / 448.0 : 1.0;
                 sc[r] = (float)s;
                 for (long c = 0; c < ngrad; c++)
-                    h8[(size_t)r * V.ldm + c] = __nv_fp8_e4m3((float)(Mcol[(size_t)c * nact + r] / s));
+                    h8[at(r, c, 1)] = __nv_fp8_e4m3((float)(Mcol[(size_t)c * nact + r] / s));
             }
             V.m.alloc(nel);
             MB_CUDA_TRY(cudaMemcpy(V.m.p, h8.data(), nel, cudaMemcpyHostToDevice));
+        }
+        if (V.tiled) {
+            const int N = nbatch <= 16 ? 16 : nbatch <= 32 ? 32 : 64;
+            V.gs.alloc((size_t)((nbatch + N - 1) / N) * V.nch * mb::tc_b_bytes(N));
         }
         V.scale.upload(sc);
         V.err.alloc(1);

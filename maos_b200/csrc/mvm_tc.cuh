@@ -1,19 +1,38 @@
 // Batched control-matrix MVM on the 5th-generation tensor cores (tcgen05).
 //
 // For nbatch instances sharing one BF16 or FP8 control matrix the MVM is a
-// GEMM: part[ks][b][row] = sum_{k in slab ks} M[row][k] g[b][k].  One CTA of
-// 128 threads owns 128 rows x one K slab; per chunk of 64 columns it stages
-// the M tile (FP8 widened to BF16, exact) and the gradient tile in shared
-// memory in the K-major core-matrix layout (8 rows x 16 bytes per core
-// matrix), and one thread issues tcgen05.mma (M=128, N = batch tile, K=16)
-// accumulating in TMEM.  The gradients enter as three BF16 terms
-// g = hi + mid + lo (each the BF16 rounding of what the previous terms left),
-// so the products carry FP32-level accuracy in g; only M's storage type
-// rounds.  The epilogue reads the accumulators with tcgen05.ld (warp w owns
-// TMEM lanes 32w..32w+31 = rows) and writes the split-K partials.
+// GEMM: part[ks][b][row] = sum_{k in slab ks} M[row][k] g[b][k], with M the
+// A operand (UMMA M = 128 rows) and the gradients the B operand (UMMA N = the
+// batch tile), accumulated in FP32 in tensor memory.
 //
-// Every wait on the MMA-completion mbarrier is bounded: on timeout the CTA
-// records an error, waits once more (bounded) and still frees its TMEM.
+// Layout in HBM.  M is stored pre-tiled: tile (row block rb, chunk c) holds
+// rows 128rb.. and columns 64c.. contiguously, already in the order the
+// tensor core reads from shared memory (K-major, no swizzle: 8x16-byte core
+// matrices, core matrix (r/8, k/8) at ((r/8)*8 + k/8)*128 bytes, row r%8 at
+// 16*(r%8)).  A BF16 tile is 16 KB; an FP8 tile is 8 KB in an order whose
+// 16-byte rows widen to two BF16 core-matrix rows (tc_fp8_off).  The
+// gradients are split once per call by k_gsplit into three BF16 terms
+// g = hi + mid + lo (each the BF16 rounding of what the previous terms left,
+// so the products carry FP32-level accuracy in g; only M's storage type
+// rounds), stored per (batch tile, chunk) as three [N x 64] tiles in the same
+// core-matrix order.  Every pipeline stage is therefore two contiguous bulk
+// copies (cp.async.bulk, completing on an mbarrier by byte count): no tensor
+// map, no per-element address arithmetic, no shared-memory bank conflicts.
+//
+// CTA (rb, ks, z): 128 threads, 128 rows x one K slab x one batch tile.
+// Thread 0 keeps up to S-1 stages of copies in flight and issues
+// tcgen05.mma (4 K-steps x 3 terms per 64-column chunk), committing each
+// chunk to the stage's "empty" mbarrier; a stage is refilled once its MMAs
+// completed.  FP8 tiles are widened to BF16 (exact) by all 128 threads into
+// one of two shared-memory tiles between the copy and the MMA.  The
+// epilogue reads the accumulators with tcgen05.ld (warp w owns TMEM lanes
+// 32w..32w+31 = rows) and writes the split-K partials.
+//
+// Every mbarrier wait is bounded.  On a timeout the CTA records an error,
+// stops issuing, waits (bounded) for the copies and MMAs it already issued,
+// and still frees its tensor memory.  Abort decisions that all threads act
+// on are taken through __syncthreads_or, so every thread passes the same
+// sequence of barriers.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
@@ -23,9 +42,34 @@
 namespace mb {
 
 constexpr int kTcRows = 128;     // UMMA M
-constexpr int kTcK = 64;         // columns per shared-memory chunk (4 MMAs of K=16)
+constexpr int kTcK = 64;         // columns per chunk (4 MMAs of K=16)
 constexpr int kTcThreads = 128;  // 4 warps, one per TMEM lane quarter
 constexpr int kTcTerms = 3;      // BF16 terms of the gradients
+constexpr int kTcTileBf16 = kTcRows * kTcK * 2;  // bytes of a BF16 M tile
+constexpr int kTcTileFp8 = kTcRows * kTcK;       // bytes of an FP8 M tile
+
+__host__ __device__ constexpr int tc_a_bytes(int dt) { return dt == MB_MVM_BF16 ? kTcTileBf16 : kTcTileFp8; }
+__host__ __device__ constexpr int tc_b_bytes(int n) { return kTcTerms * n * kTcK * 2; }
+// Pipeline depth: batch tiles of 16 and 32 keep two CTAs per SM (about
+// 110 KB each); the 64 tile runs one CTA per SM with a deeper ring.
+__host__ __device__ constexpr int tc_stages(int dt, int n) {
+    return n <= 16 ? 5 : n <= 32 ? 4 : (dt == MB_MVM_BF16 ? 5 : 6);
+}
+__host__ __device__ constexpr int tc_smem_bytes(int dt, int n) {
+    return tc_stages(dt, n) * (tc_a_bytes(dt) + tc_b_bytes(n)) + (dt == MB_MVM_BF16 ? 0 : 2 * kTcTileBf16);
+}
+
+// Byte offset of the 16-byte row holding columns 8*kgrp.. of row r in a
+// BF16 [rows x 64] K-major core-matrix tile.
+__host__ __device__ __forceinline__ uint32_t tile_off(int r, int kgrp) {
+    return (uint32_t)(((r >> 3) * 8 + kgrp) * 128 + (r & 7) * 16);
+}
+// Byte offset of element (r, k) in an FP8 [128 x 64] tile: 16-byte row
+// ((r/8)*4 + k/16)*8 + r%8 holds columns 16(k/16).. of row r, which widen
+// to BF16 core-matrix rows (r, 2(k/16)) and (r, 2(k/16)+1).
+__host__ __device__ __forceinline__ uint32_t tc_fp8_off(int r, int k) {
+    return (uint32_t)((((r >> 3) * 4 + (k >> 4)) * 8 + (r & 7)) * 16 + (k & 15));
+}
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -43,11 +87,9 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
 }
 
-// Byte offset of element (r, k) of a [rows x 64] K-major tile: core matrix
-// (r/8, k/8) at ((r/8)*8 + k/8)*128 bytes, row r%8 at 16*(r%8).
-__device__ __forceinline__ uint32_t tile_off(int r, int kgrp) { return (uint32_t)(((r >> 3) * 8 + kgrp) * 128 + (r & 7) * 16); }
-
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+// Bounded parity wait; gives up early once a thread of the CTA has raised
+// the abort hint.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const volatile int *abort = nullptr) {
     for (int i = 0; i < (1 << 22); i++) {
         uint32_t done;
         asm volatile(
@@ -58,57 +100,136 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
             : "r"(bar), "r"(phase)
             : "memory");
         if (done) return true;
+        if (abort && *abort) return false;
     }
     return false;
 }
 
-template <int DT>
-struct TcA;  // the M tile: 16 bytes of a row (global) -> BF16 core-matrix rows
-template <>
-struct TcA<MB_MVM_BF16> {
-    using T = __nv_bfloat16;
-    static constexpr int kVec = 8;  // elements per 16-byte load
-    __device__ static void stage(const uint4 &q, char *tile, int r, int kgrp) {
-        *reinterpret_cast<uint4 *>(tile + tile_off(r, kgrp)) = q;
+__device__ __forceinline__ void mbar_init(uint32_t bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
+}
+
+// One stage: the M tile and the three gradient-term tiles, both landing on
+// the stage's full barrier.
+__device__ __forceinline__ void tc_load_stage(uint32_t bar, uint32_t sa, const void *ga, int abytes, uint32_t sb,
+                                              const void *gb, int bbytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(abytes + bbytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(sa), "l"(ga), "r"(abytes), "r"(bar) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(sb), "l"(gb), "r"(bbytes), "r"(bar) : "memory");
+}
+
+// The 12 MMAs of one 64-column chunk: 4 K-steps of 16, 3 gradient terms.
+__device__ __forceinline__ void tc_mma_chunk(uint32_t tmem, uint32_t abase, uint32_t bbase, int term_bytes,
+                                             uint32_t idesc, bool first) {
+#pragma unroll
+    for (int s = 0; s < kTcK / 16; s++) {
+        const uint64_t ad = umma_desc(abase + s * 256, 128, 1024);
+#pragma unroll
+        for (int t = 0; t < kTcTerms; t++) {
+            const uint64_t bd = umma_desc(bbase + t * term_bytes + s * 256, 128, 1024);
+            const uint32_t acc = (!first || s > 0 || t > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
+        }
     }
-};
-template <>
-struct TcA<MB_MVM_FP8> {
-    using T = __nv_fp8_e4m3;
-    static constexpr int kVec = 16;
-    __device__ static void stage(const uint4 &q, char *tile, int r, int kgrp) {
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(bar)
+                 : "memory");
+}
+
+// Gradients -> three BF16 terms in per-(batch tile, chunk) core-matrix tiles.
+// gs: [nz][nch][kTcTerms][N x 64] BF16, zero past nbatch and ngrad.  One
+// thread per 8 columns of one instance; consecutive threads write
+// consecutive 16-byte rows.
+template <int N>
+__global__ void __launch_bounds__(256)
+k_gsplit(const float *__restrict__ g, long ngrad, int nbatch, long nch, int nz, char *__restrict__ gs) {
+    const long item = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= (long)nz * nch * N * 8) return;
+    // item = ((z*nch + c)*(N/8) + n/8)*64 + kg*8 + n%8
+    const int r8 = (int)(item & 7), kg = (int)((item >> 3) & 7);
+    const long rest = item >> 6;
+    const int ng = (int)(rest % (N / 8));
+    const long zc = rest / (N / 8);
+    const long c = zc % nch;
+    const int n = ng * 8 + r8, b = (int)(zc / nch) * N + n;
+    float v[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+        const long col = c * kTcK + kg * 8 + e;
+        v[e] = (b < nbatch && col < ngrad) ? g[(size_t)b * ngrad + col] : 0.f;
+    }
+    char *base = gs + (size_t)zc * tc_b_bytes(N);
+#pragma unroll
+    for (int t = 0; t < kTcTerms; t++) {
+        uint32_t w[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
+            const float2 back = __bfloat1622float2(h);
+            v[2 * e] -= back.x;
+            v[2 * e + 1] -= back.y;
+            w[e] = *reinterpret_cast<const uint32_t *>(&h);
+        }
+        *reinterpret_cast<uint4 *>(base + t * (N * kTcK * 2) + tile_off(n, kg)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+// Widen one FP8 tile (shared) to a BF16 core-matrix tile (shared): item i is
+// the 16-byte FP8 row i, which lands in two BF16 rows of the same row r.
+// Eight consecutive threads write eight different 16-byte rows of one
+// 128-byte core matrix, so the stores are conflict-free.
+__device__ __forceinline__ void tc_widen_fp8(const char *raw, char *tile) {
+#pragma unroll
+    for (int it = 0; it < kTcTileFp8 / 16 / kTcThreads; it++) {
+        const int i = it * kTcThreads + threadIdx.x;
+        const int r = (i >> 5) * 8 + (i & 7), j = (i >> 3) & 3;
+        const uint4 q = *reinterpret_cast<const uint4 *>(raw + i * 16);
         const __nv_fp8x2_e4m3 *h = reinterpret_cast<const __nv_fp8x2_e4m3 *>(&q);
         uint32_t w[8];
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const float2 f = static_cast<float2>(h[i]);
+        for (int e = 0; e < 8; e++) {
+            const float2 f = static_cast<float2>(h[e]);
             const __nv_bfloat162 b = __floats2bfloat162_rn(f.x, f.y);  // exact: E4M3 fits BF16
-            w[i] = *reinterpret_cast<const uint32_t *>(&b);
+            w[e] = *reinterpret_cast<const uint32_t *>(&b);
         }
-        *reinterpret_cast<uint4 *>(tile + tile_off(r, kgrp)) = make_uint4(w[0], w[1], w[2], w[3]);
-        *reinterpret_cast<uint4 *>(tile + tile_off(r, kgrp + 1)) = make_uint4(w[4], w[5], w[6], w[7]);
+        *reinterpret_cast<uint4 *>(tile + tile_off(r, 2 * j)) = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4 *>(tile + tile_off(r, 2 * j + 1)) = make_uint4(w[4], w[5], w[6], w[7]);
     }
-};
+}
 
-// grid: (ceil(nact/128), nks, ceil(nbatch/N)); block kTcThreads; dynamic
-// shared memory: A tile (16 KB) + kTcTerms gradient tiles (N*128 bytes each).
+// grid: (row blocks, K slabs, batch tiles); block kTcThreads; dynamic shared
+// memory tc_smem_bytes(DT, N).  Mt: pre-tiled M ([row blocks][nch] tiles of
+// tc_a_bytes(DT)); gs: k_gsplit's output; each slab is `cps` chunks.
 template <int DT, int N>
 __global__ void __launch_bounds__(kTcThreads)
-k_mvm_tc(const typename TcA<DT>::T *__restrict__ M, long ldm, const float *__restrict__ g, long ngrad,
-         float *__restrict__ part, int nact, int nbatch, int kslab, int *__restrict__ err) {
+k_mvm_tc(const char *__restrict__ Mt, const char *__restrict__ gs, long nch, int cps, float *__restrict__ part,
+         int nact, int nbatch, int *__restrict__ err) {
     static_assert(N == 16 || N == 32 || N == 64, "batch tile");
     constexpr int NCOL = N < 32 ? 32 : N;  // TMEM columns (power of 2, >= 32)
-    using A = TcA<DT>;
+    constexpr int S = tc_stages(DT, N);
+    constexpr int AB = tc_a_bytes(DT), BB = tc_b_bytes(N), SB = AB + BB;
+    constexpr bool kWiden = DT != MB_MVM_BF16;
+    constexpr uint32_t idesc = umma_idesc_bf16(N);
     extern __shared__ __align__(128) char tcsm[];
-    char *ta = tcsm;                                // [128 x 64] BF16
-    char *tb = tcsm + kTcRows * kTcK * 2;           // kTcTerms x [N x 64] BF16
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t full[S], empty[S], done;
     __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_abort;  // hint that shortens waits once a thread gave up
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row0 = blockIdx.x * kTcRows;
-    const long k0 = (long)blockIdx.y * kslab;
-    const int kn = (int)((ngrad - k0) < kslab ? (ngrad - k0) : kslab);
-    const int b0 = blockIdx.z * N;
+    const int rb = blockIdx.x, ks = blockIdx.y, z = blockIdx.z;
+    const long c0 = (long)ks * cps;
+    const int nchunk = (int)((nch - c0) < cps ? (nch - c0) : cps);
+    const char *ga = Mt + ((size_t)rb * nch + c0) * AB;
+    const char *gb = gs + ((size_t)z * nch + c0) * BB;
+    char *widen = tcsm + S * SB;  // FP8 only: two BF16 tiles
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -116,107 +237,116 @@ k_mvm_tc(const typename TcA<DT>::T *__restrict__ M, long ldm, const float *__res
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar)) : "memory");
+        for (int i = 0; i < S; i++) {
+            mbar_init(smem_addr(&full[i]));
+            mbar_init(smem_addr(&empty[i]));
+        }
+        mbar_init(smem_addr(&done));
+        s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    const uint32_t bar_a = smem_addr(&bar);
-    bool ok = true;
-    uint32_t phase = 0;
-    const int nchunk = (kn + kTcK - 1) / kTcK;
-    for (int ch = 0; ch < nchunk; ch++) {
-        const int kc = ch * kTcK;
-        if (ch > 0) {  // the previous chunk's MMAs have read the tiles
-            ok = ok && mbar_wait(bar_a, phase);
-            phase ^= 1;
-        }
-        // M tile: row r, 16-byte group u (A::kVec elements); zero past the matrix
-        constexpr int UPR = kTcK / A::kVec;  // 16-byte loads per row
-        for (int q = threadIdx.x; q < kTcRows * UPR; q += blockDim.x) {
-            const int r = q / UPR, u = q - r * UPR;
-            const int row = row0 + r, col = kc + u * A::kVec;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (row < nact && col < kn) v = *reinterpret_cast<const uint4 *>(M + (size_t)row * ldm + k0 + col);
-            A::stage(v, ta, r, u * A::kVec / 8);
-        }
-        // gradient tiles: instance n, 8 columns per item, split into three BF16 terms
-        for (int q = threadIdx.x; q < N * (kTcK / 8); q += blockDim.x) {
-            const int n = q >> 3, kg = q & 7;
-            const int b = b0 + n;
-            float v[8];
-#pragma unroll
-            for (int e = 0; e < 8; e++) {
-                const long col = k0 + kc + kg * 8 + e;
-                v[e] = (b < nbatch && kc + kg * 8 + e < kn) ? g[(size_t)b * ngrad + col] : 0.f;
-            }
-#pragma unroll
-            for (int t = 0; t < kTcTerms; t++) {
-                uint32_t w[4];
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
-                    const float2 back = __bfloat1622float2(h);
-                    v[2 * e] -= back.x;
-                    v[2 * e + 1] -= back.y;
-                    w[e] = *reinterpret_cast<const uint32_t *>(&h);
-                }
-                *reinterpret_cast<uint4 *>(tb + t * (N * kTcK * 2) + tile_off(n, kg)) =
-                    make_uint4(w[0], w[1], w[2], w[3]);
-            }
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            constexpr uint32_t idesc = umma_idesc_bf16(N);
-            const uint32_t abase = smem_addr(ta), bbase = smem_addr(tb);
-#pragma unroll
-            for (int s = 0; s < kTcK / 16; s++) {
-                const uint64_t ad = umma_desc(abase + s * 256, 128, 1024);
-#pragma unroll
-                for (int t = 0; t < kTcTerms; t++) {
-                    const uint64_t bd = umma_desc(bbase + t * (N * kTcK * 2) + s * 256, 128, 1024);
-                    const uint32_t acc = (ch > 0 || s > 0 || t > 0) ? 1u : 0u;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                        :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
+    const uint32_t sbase = smem_addr(tcsm);
+    int issued = 0;    // chunks whose copies thread 0 issued
+    int consumed = 0;  // chunks whose copies thread 0 saw land
+    int mmas = 0;      // chunks whose MMAs thread 0 issued
+    bool ok = true;    // this thread's waits all succeeded
+
+    if (threadIdx.x == 0)
+        for (; issued < (nchunk < S ? nchunk : S); issued++)
+            tc_load_stage(smem_addr(&full[issued]), sbase + issued * SB, ga + (size_t)issued * AB, AB,
+                          sbase + issued * SB + AB, gb + (size_t)issued * BB, BB);
+
+    if constexpr (!kWiden) {
+        // BF16: the main loop is thread 0's alone
+        if (threadIdx.x == 0)
+            for (int ch = 0; ch < nchunk; ch++) {
+                const int st = ch % S;
+                if (!mbar_wait(smem_addr(&full[st]), (uint32_t)((ch / S) & 1))) break;
+                consumed = ch + 1;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                tc_mma_chunk(tmem, sbase + st * SB, sbase + st * SB + AB, N * kTcK * 2, idesc, ch == 0);
+                tc_commit(smem_addr(&empty[st]));
+                mmas = ch + 1;
+                // refill the stage chunk ch-1 used once its MMAs are done
+                if (ch >= 1 && issued < nchunk) {
+                    const int ps = (ch - 1) % S;
+                    if (!mbar_wait(smem_addr(&empty[ps]), (uint32_t)(((ch - 1) / S) & 1))) break;
+                    tc_load_stage(smem_addr(&full[ps]), sbase + ps * SB, ga + (size_t)issued * AB, AB,
+                                  sbase + ps * SB + AB, gb + (size_t)issued * BB, BB);
+                    issued++;
                 }
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         :: "r"(bar_a) : "memory");
+        if (warp == 0) __syncwarp();  // lanes 1..31 block here instead of polling beside lane 0
+    } else {
+        for (int ch = 0; ch < nchunk; ch++) {
+            const int st = ch % S;
+            // the copy landed, and the MMAs of chunk ch-2 (the last reader of
+            // this BF16 tile) completed
+            if (ok) ok = mbar_wait(smem_addr(&full[st]), (uint32_t)((ch / S) & 1), &s_abort);
+            if (ok && ch >= 2) ok = mbar_wait(smem_addr(&empty[(ch - 2) % S]), (uint32_t)(((ch - 2) / S) & 1), &s_abort);
+            if (!ok) s_abort = 1;
+            char *tile = widen + (ch & 1) * kTcTileBf16;
+            if (ok) tc_widen_fp8(tcsm + st * SB, tile);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (__syncthreads_or(!ok)) break;
+            if (threadIdx.x == 0) {
+                consumed = ch + 1;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                tc_mma_chunk(tmem, smem_addr(tile), sbase + st * SB + AB, N * kTcK * 2, idesc, ch == 0);
+                tc_commit(smem_addr(&empty[st]));
+                mmas = ch + 1;
+                if (ch >= 1 && issued < nchunk) {
+                    const int ps = (ch - 1) % S;
+                    if (mbar_wait(smem_addr(&empty[ps]), (uint32_t)(((ch - 1) / S) & 1), &s_abort)) {
+                        tc_load_stage(smem_addr(&full[ps]), sbase + ps * SB, ga + (size_t)issued * AB, AB,
+                                      sbase + ps * SB + AB, gb + (size_t)issued * BB, BB);
+                        issued++;
+                    } else {
+                        ok = false;  // seen by every thread at the next barrier
+                        s_abort = 1;
+                    }
+                }
+            }
         }
     }
-    if (nchunk > 0) {
-        ok = ok && mbar_wait(bar_a, phase);
-        if (!ok) {
-            if (lane == 0) atomicExch(err, 1);
-            mbar_wait(bar_a, phase);  // bounded, before the accumulators are freed
+    bool fail = false;
+    if (threadIdx.x == 0) {
+        if (mmas < nchunk) {  // gave up: record it and drain the copies in flight
+            fail = true;
+            atomicExch(err, 1);
+            for (int c = consumed; c < issued; c++) mbar_wait(smem_addr(&full[c % S]), (uint32_t)((c / S) & 1));
         }
+        tc_commit(smem_addr(&done));  // tracks every MMA this thread issued
     }
+    if (!mbar_wait(smem_addr(&done), 0)) {
+        fail = true;
+        if (lane == 0) atomicExch(err, 1);
+        mbar_wait(smem_addr(&done), 0);  // bounded, before the accumulators are freed
+    }
+    const bool skip = __syncthreads_or(fail) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     // epilogue: warp w reads TMEM lanes 32w.. (rows), N columns (instances)
-    if (ok && nchunk > 0) {
+    if (!skip && nchunk > 0) {
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-        const int row = row0 + warp * 32 + lane;
+        const int row = rb * kTcRows + warp * 32 + lane;
 #pragma unroll
-        for (int c0 = 0; c0 < N; c0 += 16) {
+        for (int cc = 0; cc < N; cc += 16) {
             uint32_t r[16];
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                : "r"(taddr + (uint32_t)c0));
+                : "r"(taddr + (uint32_t)cc));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (row < nact)
 #pragma unroll
                 for (int j = 0; j < 16; j++) {
-                    const int b = b0 + c0 + j;
-                    if (b < nbatch) part[((size_t)blockIdx.y * nbatch + b) * nact + row] = __uint_as_float(r[j]);
+                    const int b = z * N + cc + j;
+                    if (b < nbatch) part[((size_t)ks * nbatch + b) * nact + row] = __uint_as_float(r[j]);
                 }
         }
     }
