@@ -660,6 +660,7 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
         return n == 1;
     };
     fd_bufn = 0;
+    int twn = 0;  // twiddle entries a layer CTA stages (nx + ny)
     for (int l = 0; l < nps; l++) {
         FdLayer &F = fl[l];
         F.nx = lay_h[l].nx;
@@ -675,11 +676,19 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
         F.hs = (int)hsz[l];
         F.twx = table(F.nx);
         F.twy = table(F.ny);
+        F.px = F.py = -1;  // two-pass FFT where a factor pair is listed
+        for (int i = 0; i < kNumFftPairs; i++) {
+            if (F.px < 0 && kFftPairs[i][0] * kFftPairs[i][1] == F.nx) F.px = i;
+            if (F.py < 0 && kFftPairs[i][0] * kFftPairs[i][1] == F.ny) F.py = i;
+        }
         fd_bufn = std::max(fd_bufn, std::max(F.ny / 2 * F.nx, F.ny * (F.nx / 2 + 1)));
+        if (F.px >= 0) fd_bufn = std::max(fd_bufn, fft2_scratch(F.px, true, F.ny / 2));
+        if (F.py >= 0) fd_bufn = std::max(fd_bufn, fft2_scratch(F.py, false, F.nx / 2 + 1));
+        twn = std::max(twn, F.nx + F.ny);
     }
     fd_lay.upload(fl);
     fd_tw.upload(tw);
-    fd_smem = 2 * (size_t)fd_bufn * sizeof(cplx);
+    fd_smem = (2 * (size_t)fd_bufn + twn) * sizeof(cplx);
     MB_REQUIRE(fd_smem <= 200 * 1024, "fdpcg: layer FFT needs %zu bytes of shared memory", fd_smem);
     MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
     MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));

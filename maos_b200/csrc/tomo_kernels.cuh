@@ -840,7 +840,14 @@ struct FdLayer {
     int twx, twy;        // offsets of the twiddle tables for n = nx and n = ny
     int nrx, nry;        // radix stages along x and y
     signed char rx[8], ry[8];
+    int px, py;          // two-pass factor pair (index into kFftPairs) along x and y, -1: stages
 };
+
+// Lengths the two-pass FFT handles, as n = N1 * N2 (both passes' DFTs held
+// in registers).  The host picks the first pair whose product is n.
+constexpr int kFftPairs[][2] = {{4, 4}, {8, 4}, {6, 6}, {8, 5}, {8, 6}, {10, 6}, {8, 8}, {12, 6}, {10, 8},
+                                {12, 8}, {10, 10}, {12, 10}, {12, 12}, {16, 10}, {16, 12}, {16, 16}, {16, 8}};
+constexpr int kNumFftPairs = (int)(sizeof(kFftPairs) / sizeof(kFftPairs[0]));
 
 __device__ __forceinline__ cplx cmul(cplx a, cplx b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 __device__ __forceinline__ cplx cadd(cplx a, cplx b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -928,15 +935,172 @@ __device__ cplx *fft_many(cplx *a, cplx *b, int n, int count, int es, int ts, co
     return a;
 }
 
+// ---------------------------------------------------------------------------
+// Two-pass (four-step) FFT of length n = N1 * N2.  With input index
+// i = k2 + N2 m and output index k = k1 + N1 j2:
+//   X[k1 + N1 j2] = sum_k2 W_N2^(k2 j2) W_n^(k2 k1) sum_m x[k2 + N2 m] W_N1^(m k1).
+// Pass 1 (one item per (transform, k2)) does the N1-point DFT over m in
+// registers and the twiddle W_n^(k2 k1); pass 2 (one item per (transform,
+// k1)) does the N2-point DFT over k2.  Between the passes the values go
+// through a scratch buffer laid out so that both passes read and write
+// shared memory without bank conflicts: rows of a row transform are padded
+// to an odd stride, column transforms keep the column index fastest.  Two
+// barriers per transform instead of one per radix stage.  All twiddles come
+// from the n-entry table tw (W_n^e = tw[e], conjugated for the inverse).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ cplx tw_at(const cplx *tw, int e, bool inv) {
+    cplx w = tw[e];
+    if (inv) w.y = -w.y;
+    return w;
+}
+
+// In-register DFT of N points; W_N^m = tw[m * ts].
+template <int N>
+__device__ __forceinline__ void rdft(cplx *v, const cplx *tw, int ts, bool inv) {
+    if constexpr (N == 1) {
+        return;
+    } else if constexpr (N == 2) {
+        const cplx a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (N == 4) {
+        const cplx s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        const cplx s13 = cadd(v[1], v[3]);
+        cplx d13 = mul_mi(csub(v[1], v[3]));  // -i (v1 - v3)
+        if (inv) d13 = make_float2(-d13.x, -d13.y);
+        v[0] = cadd(s02, s13);
+        v[1] = cadd(d02, d13);
+        v[2] = csub(s02, s13);
+        v[3] = csub(d02, d13);
+    } else if constexpr (N == 3 || N == 5) {
+        cplx o[N];
+#pragma unroll
+        for (int q = 0; q < N; q++) {
+            cplx acc = v[0];
+#pragma unroll
+            for (int r = 1; r < N; r++) acc = cadd(acc, cmul(v[r], tw_at(tw, ((r * q) % N) * ts, inv)));
+            o[q] = acc;
+        }
+#pragma unroll
+        for (int q = 0; q < N; q++) v[q] = o[q];
+    } else {
+        constexpr int A = (N % 4 == 0) ? 4 : (N % 2 == 0) ? 2 : (N % 3 == 0) ? 3 : 5;
+        constexpr int B = N / A;
+        static_assert(A * B == N, "radix");
+        cplx t[N];
+#pragma unroll
+        for (int b = 0; b < B; b++) {
+            cplx u[A];
+#pragma unroll
+            for (int a = 0; a < A; a++) u[a] = v[b + B * a];
+            rdft<A>(u, tw, ts * B, inv);
+#pragma unroll
+            for (int ka = 0; ka < A; ka++)
+                t[b + B * ka] = (b * ka == 0) ? u[ka] : cmul(u[ka], tw_at(tw, b * ka * ts, inv));
+        }
+#pragma unroll
+        for (int ka = 0; ka < A; ka++) {
+            cplx w[B];
+#pragma unroll
+            for (int b = 0; b < B; b++) w[b] = t[b + B * ka];
+            rdft<B>(w, tw, ts * A, inv);
+#pragma unroll
+            for (int kb = 0; kb < B; kb++) v[ka + A * kb] = w[kb];
+        }
+    }
+}
+
+// `count` transforms of length N1*N2 over x -> x, scratch s.  ROWS: transform
+// c is x[c*ld + i] (contiguous); otherwise x[i*ld + c] (columns).  Ends with
+// a barrier.
+template <bool ROWS, int N1, int N2>
+__device__ void fft2(cplx *x, cplx *s, int count, int ld, const cplx *tw, bool inv) {
+    constexpr int P = N2 | 1;  // padded scratch row (odd stride) for row transforms
+    for (int it = threadIdx.x; it < count * N2; it += blockDim.x) {
+        int c, k2;
+        if (ROWS) {
+            c = it / N2;
+            k2 = it - c * N2;
+        } else {
+            k2 = it / count;
+            c = it - k2 * count;
+        }
+        cplx v[N1];
+#pragma unroll
+        for (int m = 0; m < N1; m++) v[m] = ROWS ? x[c * ld + k2 + N2 * m] : x[(k2 + N2 * m) * ld + c];
+        rdft<N1>(v, tw, N2, inv);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) {
+            const cplx y = k1 == 0 ? v[0] : cmul(v[k1], tw_at(tw, k1 * k2, inv));
+            if (ROWS) s[(c * N1 + k1) * P + k2] = y;
+            else s[(k1 * N2 + k2) * count + c] = y;
+        }
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < count * N1; it += blockDim.x) {
+        int c, k1;
+        if (ROWS) {
+            c = it / N1;
+            k1 = it - c * N1;
+        } else {
+            k1 = it / count;
+            c = it - k1 * count;
+        }
+        cplx w[N2];
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) w[k2] = ROWS ? s[(c * N1 + k1) * P + k2] : s[(k1 * N2 + k2) * count + c];
+        rdft<N2>(w, tw, N1, inv);
+#pragma unroll
+        for (int j2 = 0; j2 < N2; j2++) {
+            if (ROWS) x[c * ld + k1 + N1 * j2] = w[j2];
+            else x[(k1 + N1 * j2) * ld + c] = w[j2];
+        }
+    }
+    __syncthreads();
+}
+
+// Scratch (complex values) fft2 needs for `count` transforms of pair `pair`.
+inline int fft2_scratch(int pair, bool rows, int count) {
+    const int n1 = kFftPairs[pair][0], n2 = kFftPairs[pair][1];
+    return rows ? count * n1 * (n2 | 1) : count * n1 * n2;
+}
+
+// Transforms of one direction of a layer: the two-pass form when the
+// length has a factor pair (pair >= 0; result in place in a), else the
+// radix stages (result in a or b).  Returns the buffer with the result.
+template <bool ROWS>
+__device__ cplx *fft_dir(int pair, cplx *a, cplx *b, int n, int count, int ld, const signed char *rad, int nr,
+                         const cplx *tw, bool inv) {
+    switch (pair) {
+#define MB_FFT_CASE(i)                                                          \
+    case i:                                                                     \
+        fft2<ROWS, kFftPairs[i][0], kFftPairs[i][1]>(a, b, count, ld, tw, inv); \
+        return a;
+        MB_FFT_CASE(0) MB_FFT_CASE(1) MB_FFT_CASE(2) MB_FFT_CASE(3) MB_FFT_CASE(4) MB_FFT_CASE(5)
+        MB_FFT_CASE(6) MB_FFT_CASE(7) MB_FFT_CASE(8) MB_FFT_CASE(9) MB_FFT_CASE(10) MB_FFT_CASE(11)
+        MB_FFT_CASE(12) MB_FFT_CASE(13) MB_FFT_CASE(14) MB_FFT_CASE(15) MB_FFT_CASE(16)
+#undef MB_FFT_CASE
+        default:
+            return ROWS ? fft_many(a, b, n, count, 1, ld, rad, nr, tw, inv)
+                        : fft_many(a, b, n, count, ld, 1, rad, nr, tw, inv);
+    }
+}
+static_assert(kNumFftPairs == 17, "fft_dir lists one case per factor pair");
+
 constexpr int kFftThreads = 512;  // threads of a layer-FFT CTA
 
 // Forward: r (instance-major) -> half spectra H.  grid: (nps, nb), block:
-// kFftThreads; dynamic shared memory: two buffers of `bufn` complex values.  With `ab`, the CG
+// kFftThreads; dynamic shared memory: two buffers of `bufn` complex values,
+// then the layer's twiddle tables for n = nx and n = ny.  With `ab`, the CG
 // update of this iteration comes first on the layer's points:
 // x += alpha p, r -= alpha Ap (alpha = ab[2b]), and the updated r is
-// transformed (the k_cg_update_xr of a non-final iteration, fused).
-__global__ void __launch_bounds__(kFftThreads)
-k_fd_fwd(float *r, cplx *__restrict__ H, const FdLayer *__restrict__ fl, const cplx *__restrict__ tw,
+// transformed (the k_cg_update_xr of a non-final iteration, fused).  A thread
+// issues the loads of kFdLoads row pairs before using any of them, so the
+// global round trips overlap instead of following one another.
+constexpr int kFdLoads = 5;
+
+__global__ void __launch_bounds__(kFftThreads, 2)
+k_fd_fwd(float *__restrict__ r, cplx *__restrict__ H, const FdLayer *__restrict__ fl, const cplx *__restrict__ tw,
          long nxtot, int bufn, float *__restrict__ xw, const float *__restrict__ pv,
          const float *__restrict__ Apv, const float *__restrict__ ab, const int *__restrict__ act) {
     pdl_enter();
@@ -945,7 +1109,9 @@ k_fd_fwd(float *r, cplx *__restrict__ H, const FdLayer *__restrict__ fl, const c
     const FdLayer L = fl[blockIdx.x];
     const int b = blockIdx.y;
     const int nx = L.nx, ny = L.ny, h = nx / 2 + 1, np2 = ny / 2;
-    cplx *A = fsm, *B = fsm + bufn;
+    cplx *A = fsm, *B = fsm + bufn, *twx = fsm + 2 * bufn, *twy = twx + nx;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) twx[i] = tw[L.twx + i];
+    for (int i = threadIdx.x; i < ny; i += blockDim.x) twy[i] = tw[L.twy + i];
     const size_t base = (size_t)b * nxtot + L.off;
     float *rb = r + base;
     const int xs = blockDim.x / nx, x0 = threadIdx.x / nx, xc = threadIdx.x - x0 * nx;  // nx <= blockDim
@@ -954,22 +1120,58 @@ k_fd_fwd(float *r, cplx *__restrict__ H, const FdLayer *__restrict__ fl, const c
             const float a = ab[2 * b];
             float *xb = xw + base;
             const float *pb = pv + base, *qb = Apv + base;
-            for (int p = x0; p < np2; p += xs) {
-                const int o0 = (2 * p) * nx + xc, o1 = o0 + nx;
-                xb[o0] += a * pb[o0];
-                xb[o1] += a * pb[o1];
-                const float r0 = rb[o0] - a * qb[o0], r1 = rb[o1] - a * qb[o1];
-                rb[o0] = r0;
-                rb[o1] = r1;
-                A[p * nx + xc] = make_float2(r0, r1);
+            for (int p0 = x0; p0 < np2; p0 += kFdLoads * xs) {
+                float xv[kFdLoads][2], pp[kFdLoads][2], rv[kFdLoads][2], qq[kFdLoads][2];
+#pragma unroll
+                for (int u = 0; u < kFdLoads; u++) {
+                    const int p = p0 + u * xs;
+                    if (p < np2) {
+                        const int o0 = (2 * p) * nx + xc, o1 = o0 + nx;
+                        xv[u][0] = xb[o0];
+                        xv[u][1] = xb[o1];
+                        pp[u][0] = pb[o0];
+                        pp[u][1] = pb[o1];
+                        rv[u][0] = rb[o0];
+                        rv[u][1] = rb[o1];
+                        qq[u][0] = qb[o0];
+                        qq[u][1] = qb[o1];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kFdLoads; u++) {
+                    const int p = p0 + u * xs;
+                    if (p < np2) {
+                        const int o0 = (2 * p) * nx + xc, o1 = o0 + nx;
+                        xb[o0] = xv[u][0] + a * pp[u][0];
+                        xb[o1] = xv[u][1] + a * pp[u][1];
+                        const float r0 = rv[u][0] - a * qq[u][0], r1 = rv[u][1] - a * qq[u][1];
+                        rb[o0] = r0;
+                        rb[o1] = r1;
+                        A[p * nx + xc] = make_float2(r0, r1);
+                    }
+                }
             }
         } else {
-            for (int p = x0; p < np2; p += xs)
-                A[p * nx + xc] = make_float2(rb[(2 * p) * nx + xc], rb[(2 * p + 1) * nx + xc]);
+            for (int p0 = x0; p0 < np2; p0 += kFdLoads * xs) {
+                float rv[kFdLoads][2];
+#pragma unroll
+                for (int u = 0; u < kFdLoads; u++) {
+                    const int p = p0 + u * xs;
+                    if (p < np2) {
+                        rv[u][0] = rb[(2 * p) * nx + xc];
+                        rv[u][1] = rb[(2 * p + 1) * nx + xc];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kFdLoads; u++) {
+                    const int p = p0 + u * xs;
+                    if (p < np2) A[p * nx + xc] = make_float2(rv[u][0], rv[u][1]);
+                }
+            }
         }
     }
     __syncthreads();
-    cplx *Z = fft_many(A, B, nx, np2, 1, nx, L.rx, L.nrx, tw + L.twx, false);
+    cplx *Z = fft_dir<true>(L.px, A, B, nx, np2, nx, L.rx, L.nrx, twx, false);
     cplx *S = (Z == A) ? B : A;
     const int hs_ = blockDim.x / h, h0 = threadIdx.x / h, k = threadIdx.x - h0 * h;
     for (int p = h0; h0 < hs_ && p < np2; p += hs_) {
@@ -979,7 +1181,7 @@ k_fd_fwd(float *r, cplx *__restrict__ H, const FdLayer *__restrict__ fl, const c
         S[(2 * p + 1) * h + k] = make_float2(0.5f * d.y, -0.5f * d.x);  // -i/2 (zk - conj(z_-k))
     }
     __syncthreads();
-    const cplx *C = fft_many(S, Z, ny, h, h, 1, L.ry, L.nry, tw + L.twy, false);
+    const cplx *C = fft_dir<false>(L.py, S, Z, ny, h, h, L.ry, L.nry, twy, false);
     cplx *out = H + L.hoff + (size_t)b * L.hs;
     for (int i = threadIdx.x; i < ny * h; i += blockDim.x) out[i] = C[i];
 }
@@ -1040,8 +1242,8 @@ k_fd_mul(const cplx *__restrict__ X, cplx *__restrict__ Y, const cplx *__restric
 
 // Inverse: half spectra H -> z (instance-major), plus the r.z partial of this
 // (layer, instance); the last CTA of an instance leaves (r.z)_0 or beta.
-// grid: (nps, nb)
-__global__ void __launch_bounds__(kFftThreads)
+// grid: (nps, nb); shared memory as k_fd_fwd.
+__global__ void __launch_bounds__(kFftThreads, 2)
 k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restrict__ z,
          double *__restrict__ rz_part, const FdLayer *__restrict__ fl, const cplx *__restrict__ tw, long nxtot,
          int bufn, CgScal SC, int kit, int init, const int *__restrict__ act) {
@@ -1052,11 +1254,26 @@ k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restr
     const FdLayer L = fl[blockIdx.x];
     const int b = blockIdx.y;
     const int nx = L.nx, ny = L.ny, h = nx / 2 + 1, np2 = ny / 2;
-    cplx *A = fsm, *B = fsm + bufn;
+    cplx *A = fsm, *B = fsm + bufn, *twx = fsm + 2 * bufn, *twy = twx + nx;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) twx[i] = tw[L.twx + i];
+    for (int i = threadIdx.x; i < ny; i += blockDim.x) twy[i] = tw[L.twy + i];
     const cplx *in = H + L.hoff + (size_t)b * L.hs;
-    for (int i = threadIdx.x; i < ny * h; i += blockDim.x) A[i] = in[i];
+    constexpr int kLd = 2 * kFdLoads;  // spectrum values a thread loads before storing any
+    for (int i0 = threadIdx.x; i0 < ny * h; i0 += kLd * blockDim.x) {
+        cplx v[kLd];
+#pragma unroll
+        for (int u = 0; u < kLd; u++) {
+            const int i = i0 + u * blockDim.x;
+            if (i < ny * h) v[u] = in[i];
+        }
+#pragma unroll
+        for (int u = 0; u < kLd; u++) {
+            const int i = i0 + u * blockDim.x;
+            if (i < ny * h) A[i] = v[u];
+        }
+    }
     __syncthreads();
-    cplx *C = fft_many(A, B, ny, h, h, 1, L.ry, L.nry, tw + L.twy, true);
+    cplx *C = fft_dir<false>(L.py, A, B, ny, h, h, L.ry, L.nry, twy, true);
     cplx *Zb = (C == A) ? B : A;
     const int xs = blockDim.x / nx, x0 = threadIdx.x / nx, k = threadIdx.x - x0 * nx;
     for (int p = x0; x0 < xs && p < np2; p += xs) {
@@ -1075,16 +1292,31 @@ k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restr
         Zb[i] = make_float2(a.x - c.y, a.y + c.x);  // a + i c
     }
     __syncthreads();
-    const cplx *Zo = fft_many(Zb, C, nx, np2, 1, nx, L.rx, L.nrx, tw + L.twx, true);
+    const cplx *Zo = fft_dir<true>(L.px, Zb, C, nx, np2, nx, L.rx, L.nrx, twx, true);
     const size_t base = (size_t)b * nxtot + L.off;
     double v = 0;
-    for (int p = x0; x0 < xs && p < np2; p += xs) {
-        const int x = k, i = p * nx + k;
-        const cplx q = Zo[i];
-        const size_t o0 = base + (size_t)(2 * p) * nx + x, o1 = o0 + nx;
-        z[o0] = q.x;
-        z[o1] = q.y;
-        v += (double)q.x * r[o0] + (double)q.y * r[o1];
+    for (int p0 = x0; x0 < xs && p0 < np2; p0 += kFdLoads * xs) {
+        float rv[kFdLoads][2];
+#pragma unroll
+        for (int u = 0; u < kFdLoads; u++) {
+            const int p = p0 + u * xs;
+            if (p < np2) {
+                const size_t o0 = base + (size_t)(2 * p) * nx + k;
+                rv[u][0] = r[o0];
+                rv[u][1] = r[o0 + nx];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kFdLoads; u++) {
+            const int p = p0 + u * xs;
+            if (p < np2) {
+                const cplx q = Zo[p * nx + k];
+                const size_t o0 = base + (size_t)(2 * p) * nx + k, o1 = o0 + nx;
+                z[o0] = q.x;
+                z[o1] = q.y;
+                v += (double)q.x * rv[u][0] + (double)q.y * rv[u][1];
+            }
+        }
     }
     v = block_sum(v, sh);
     if (threadIdx.x == 0) rz_part[(size_t)b * gridDim.x + blockIdx.x] = v;
