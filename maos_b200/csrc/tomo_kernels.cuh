@@ -1190,8 +1190,9 @@ k_fd_fwd(float *__restrict__ r, cplx *__restrict__ H, const FdLayer *__restrict_
 // (the leading blocks of the reference's ordering, which reach every stored
 // bin): Y_i = sum_j M[blk][j*bs+i] X_j.  A CTA takes floor(256/bs) whole
 // blocks and up to kFdInst instances: a thread keeps its row of M in
-// registers for all of them, and per instance first stages its own member
-// X_i in shared memory, then forms its row from the block's staged members.
+// registers for all of them, gathers its own member X_i of every instance
+// at once (one round trip, not one per instance), stages them in shared
+// memory, then forms its row of each instance from the block's members.
 // grid: (ceil(nblk / floor(256/bs)), ceil(nbatch / kFdInst))
 constexpr int kFdInst = 8;
 constexpr int kMaxBs = 16;
@@ -1200,11 +1201,15 @@ __global__ void __launch_bounds__(kThreads)
 k_fd_mul(const cplx *__restrict__ X, cplx *__restrict__ Y, const cplx *__restrict__ M,
          const FdIndex *__restrict__ idx, int nblk, int bs, int nbatch, const int *__restrict__ act) {
     pdl_enter();
-    __shared__ cplx xs[kThreads];
+    __shared__ cplx xs[kFdInst][kThreads];
     const int per = kThreads / bs;
     const int lb = threadIdx.x / bs, i = threadIdx.x - lb * bs;
     const int blk = blockIdx.x * per + lb;
     const bool live = lb < per && blk < nblk;
+    const int b0 = blockIdx.y * kFdInst, nq = min(kFdInst, nbatch - b0);
+    bool on[kFdInst];
+#pragma unroll
+    for (int q = 0; q < kFdInst; q++) on[q] = q < nq && !inactive(act, b0 + q);
     FdIndex o{};
     cplx m[kMaxBs];
     if (live) {
@@ -1212,31 +1217,32 @@ k_fd_mul(const cplx *__restrict__ X, cplx *__restrict__ Y, const cplx *__restric
         const cplx *Mb = M + (size_t)blk * bs * bs + i;
 #pragma unroll
         for (int jj = 0; jj < kMaxBs; jj++) m[jj] = jj < bs ? Mb[jj * bs] : make_float2(0.f, 0.f);
-    }
-    const int b1 = min(nbatch, (int)(blockIdx.y + 1) * kFdInst);
-    for (int b = blockIdx.y * kFdInst; b < b1; b++) {
-        if (inactive(act, b)) continue;  // uniform over the CTA
-        if (live) {
-            cplx xv = X[o.base + (size_t)b * o.stride];
-            if (o.flags & kFdConj) xv.y = -xv.y;
-            xs[threadIdx.x] = xv;
-        }
-        __syncthreads();
-        if (live) {
-            const cplx *xb = xs + lb * bs;
-            float re = 0.f, im = 0.f;
+        cplx xv[kFdInst];
 #pragma unroll
-            for (int jj = 0; jj < kMaxBs; jj++) {
-                if (jj < bs) {
-                    const cplx xv = xb[jj];
-                    re += m[jj].x * xv.x - m[jj].y * xv.y;
-                    im += m[jj].x * xv.y + m[jj].y * xv.x;
-                }
-            }
-            if (o.flags & kFdStore)
-                Y[o.base + (size_t)b * o.stride] = make_float2(re, (o.flags & kFdConj) ? -im : im);
+        for (int q = 0; q < kFdInst; q++)
+            xv[q] = on[q] ? X[o.base + (size_t)(b0 + q) * o.stride] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < kFdInst; q++) {
+            if (o.flags & kFdConj) xv[q].y = -xv[q].y;
+            xs[q][threadIdx.x] = xv[q];
         }
-        __syncthreads();
+    }
+    __syncthreads();
+    if (!live || !(o.flags & kFdStore)) return;
+#pragma unroll
+    for (int q = 0; q < kFdInst; q++) {
+        if (!on[q]) continue;
+        const cplx *xb = xs[q] + lb * bs;
+        float re = 0.f, im = 0.f;
+#pragma unroll
+        for (int jj = 0; jj < kMaxBs; jj++) {
+            if (jj < bs) {
+                const cplx xv = xb[jj];
+                re += m[jj].x * xv.x - m[jj].y * xv.y;
+                im += m[jj].x * xv.y + m[jj].y * xv.x;
+            }
+        }
+        Y[o.base + (size_t)(b0 + q) * o.stride] = make_float2(re, (o.flags & kFdConj) ? -im : im);
     }
 }
 
