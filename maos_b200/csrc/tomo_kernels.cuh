@@ -366,6 +366,20 @@ __global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ 
 // each WFS on each layer (the columns and rows whose lists are not empty) is
 // computed and read; outside it every term is an exact zero.
 // ---------------------------------------------------------------------------
+// Asynchronous 4-byte global -> shared copies (cp.async): a CTA issues all of
+// a table's words at once and waits once, instead of one round trip per
+// loop iteration.
+__device__ __forceinline__ void cp_async_word(void *sdst, const void *gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;"
+                 :: "r"((unsigned)__cvta_generic_to_shared(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// words [0, n) of src -> dst, spread over the CTA
+__device__ __forceinline__ void cp_async_words(void *dst, const void *src, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        cp_async_word(static_cast<float *>(dst) + i, static_cast<const float *>(src) + i);
+}
+
 struct PadIndex {
     const GatherW *x;   // [(w*ncols + tcol_l + jx)*kx + e]   (per WFS, all layers' columns)
     const GatherW *y;   // [((w*nps + l)*maxny + jy)*ky + e]
@@ -407,6 +421,7 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
     extern __shared__ float sm[];
     __shared__ int s_lnx[kMaxLayers], s_tcol[kMaxLayers + 1];
     __shared__ long s_loff[kMaxLayers];
+    __shared__ int4 s_fp[kMaxLayers];
     const WfsDev W = wfs[w];
     const int r0 = blockIdx.x * rows;
     const int r1 = min(nyp, r0 + rows);      // output pupil rows [r0, r1)
@@ -425,25 +440,30 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
     const int ph = threadIdx.x / nxp, ix = threadIdx.x - ph * nxp;
     const bool colthr = ph < nph;
 
-    // stage the layer geometry, the x lists of this WFS and, for Hx, the axis tables
+    // stage the layer geometry and footprints, the x lists of this WFS, the
+    // subaperture map of rows [ca, cb) and, for Hx, the axis tables: all
+    // copies in flight together
     if (threadIdx.x < nps) {
         const LayerDev L = lay[threadIdx.x];
         s_lnx[threadIdx.x] = L.nx;
         s_loff[threadIdx.x] = L.off;
         s_tcol[threadIdx.x] = L.tcol;
+        s_fp[threadIdx.x] = pi.fp[w * nps + threadIdx.x];
     }
     if (threadIdx.x == 0) s_tcol[nps] = ncols;
     {
-        const GatherW *src = pi.x + (size_t)w * ncols * pi.kx;
-        for (int i = threadIdx.x; i < ncols * pi.kx; i += blockDim.x) s_xp[i] = src[i];
+        constexpr int GW = (int)(sizeof(GatherW) / 4), AW = (int)(sizeof(AxisW) / 4);
+        cp_async_words(s_xp, pi.x + (size_t)w * ncols * pi.kx, ncols * pi.kx * GW);
+        if (cb > ca) cp_async_words(s_sid, W.samap + (size_t)ca * nxp, (cb - ca) * nxp);
         if (FROM_X) {
             const AxisW *tw0 = tab + (size_t)w * nps * (nxp + nyp);
             for (int l = 0; l < nps; l++) {
                 const AxisW *tl = tw0 + (size_t)l * (nxp + nyp);
-                for (int i = threadIdx.x; i < nxp + nh; i += blockDim.x)
-                    s_tab[l * ts + i] = tl[i < nxp ? i : nxp + ca + (i - nxp)];
+                cp_async_words(s_tab + l * ts, tl, nxp * AW);                   // x axis
+                cp_async_words(s_tab + l * ts + nxp, tl + nxp + ca, nh * AW);   // y axis, rows [ca, ca+nh)
             }
         }
+        cp_async_wait_all();
         __syncthreads();
     }
     if (FROM_X) {  // Hx for pupil rows [ca, cb + POS): a point's layer taps are issued together
@@ -475,8 +495,7 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
         if (colthr)
             for (int rr = ph; rr < cb - ca; rr += nph) {
                 const int i = rr * nxp + ix;
-                const int s = __ldg(W.samap + (ca + rr) * nxp + ix);
-                s_sid[i] = s;
+                const int s = s_sid[i];  // staged subaperture map
                 if (s < 0) continue;
                 const float *ne = W.neai + 3 * s;
                 const float n0 = ne[0], n1_ = ne[1], n2 = ne[2];
@@ -533,7 +552,7 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
             int l = 0;
             while (l + 1 < nps && c >= s_tcol[l + 1]) l++;
             const int tc = s_tcol[l], lnx = s_lnx[l];
-            const int4 f = pi.fp[w * nps + l];
+            const int4 f = s_fp[l];
             if (c - tc < f.x || c - tc >= f.y) continue;  // no pupil column reaches it: never read
             GatherW e[kMaxPadX];
 #pragma unroll
