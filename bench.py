@@ -356,6 +356,8 @@ def run_gpu(args):
 
     lib = native.load()
     R = Reconstructor(sysm, nbatch=B, device=local, fit=fit)
+    # the pupil-row blocking of the LHS kernel, measured for this batch (outside the timed region)
+    tuned_rows, tuned_ms = R.autotune(reps=20)
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -491,7 +493,9 @@ def run_gpu(args):
                 "config": {"workload": WORKLOAD_TEXT,
                            "instances_per_gpu": B, "ngrad": int(sysm.ngrad), "nact": int(fit.nact),
                            "nxtot": int(sysm.nx_total), "l2": "flushed before every step (256 MiB write)",
-                           "parallelism": f"replicas x{world}"},
+                           "parallelism": f"replicas x{world}",
+                           "autotune": {"pupil_rows": tuned_rows,
+                                        "lhs_ms_by_rows": {str(k): round(v, 4) for k, v in tuned_ms.items()}}},
                 "latency_ms": {"p50": p50, "p99": p99, "note": "one batched step of all instances"},
                 "e2e": {"value": e2e_value, "unit": "steps/s",
                         "h2d_bytes_per_step": int(B * sysm.ngrad * 4),

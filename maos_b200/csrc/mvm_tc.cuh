@@ -19,20 +19,22 @@
 // copies (cp.async.bulk, completing on an mbarrier by byte count): no tensor
 // map, no per-element address arithmetic, no shared-memory bank conflicts.
 //
-// CTA (rb, ks, z): 128 threads, 128 rows x one K slab x one batch tile.
-// Thread 0 keeps up to S-1 stages of copies in flight and issues
-// tcgen05.mma (4 K-steps x 3 terms per 64-column chunk), committing each
-// chunk to the stage's "empty" mbarrier; a stage is refilled once its MMAs
-// completed.  FP8 tiles are widened to BF16 (exact) by all 128 threads into
-// one of two shared-memory tiles between the copy and the MMA.  The
-// epilogue reads the accumulators with tcgen05.ld (warp w owns TMEM lanes
-// 32w..32w+31 = rows) and writes the split-K partials.
+// CTA (rb, ks, z): 160 threads (5 warps), 128 rows x one K slab x one batch
+// tile, with warp roles that meet only on mbarriers:
+//   warp 0, lane 0: copies.  Keeps all S stages in flight; a stage is
+//     refilled as soon as the MMAs that read it completed ("empty").
+//   warp 1, lane 0: MMAs.  Per 64-column chunk, 4 K-steps x 3 terms of
+//     tcgen05.mma (M=128, N = batch tile, K=16) into TMEM, committed to the
+//     stage's "empty" barrier (and, FP8, to the widened tile's "free").
+//   warps 2-4 (FP8 only): widen the stage's FP8 tile to BF16 (exact) into one
+//     of two shared-memory tiles and arrive on its "ready" barrier.
+// The epilogue reads the accumulators with tcgen05.ld (warps 1-4; warp w
+// reaches TMEM lanes 32(w%4).. = rows) and writes the split-K partials.
 //
-// Every mbarrier wait is bounded.  On a timeout the CTA records an error,
-// stops issuing, waits (bounded) for the copies and MMAs it already issued,
-// and still frees its tensor memory.  Abort decisions that all threads act
-// on are taken through __syncthreads_or, so every thread passes the same
-// sequence of barriers.
+// Every mbarrier wait is bounded.  On a timeout a thread raises the CTA's
+// abort flag, every role stops issuing, the copy thread waits (bounded) for
+// the copies it issued, all threads wait (bounded) for the MMAs issued, and
+// the tensor memory is still freed; the error flag tells the host.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
@@ -43,7 +45,8 @@ namespace mb {
 
 constexpr int kTcRows = 128;     // UMMA M
 constexpr int kTcK = 64;         // columns per chunk (4 MMAs of K=16)
-constexpr int kTcThreads = 128;  // 4 warps, one per TMEM lane quarter
+constexpr int kTcThreads = 160;  // copy warp, MMA warp, 3 widening warps (4 epilogue warps)
+constexpr int kTcWiden = 96;     // threads of the widening warps
 constexpr int kTcTerms = 3;      // BF16 terms of the gradients
 constexpr int kTcTileBf16 = kTcRows * kTcK * 2;  // bytes of a BF16 M tile
 constexpr int kTcTileFp8 = kTcRows * kTcK;       // bytes of an FP8 M tile
@@ -105,8 +108,8 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const vo
     return false;
 }
 
-__device__ __forceinline__ void mbar_init(uint32_t bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
+__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(count) : "memory");
 }
 
 // One stage: the M tile and the three gradient-term tiles, both landing on
@@ -187,10 +190,8 @@ k_gsplit(const float *__restrict__ g, long ngrad, int nbatch, long nch, int nz, 
 // the 16-byte FP8 row i, which lands in two BF16 rows of the same row r.
 // Eight consecutive threads write eight different 16-byte rows of one
 // 128-byte core matrix, so the stores are conflict-free.
-__device__ __forceinline__ void tc_widen_fp8(const char *raw, char *tile) {
-#pragma unroll
-    for (int it = 0; it < kTcTileFp8 / 16 / kTcThreads; it++) {
-        const int i = it * kTcThreads + threadIdx.x;
+__device__ __forceinline__ void tc_widen_fp8(const char *raw, char *tile, int tid) {
+    for (int i = tid; i < kTcTileFp8 / 16; i += kTcWiden) {
         const int r = (i >> 5) * 8 + (i & 7), j = (i >> 3) & 3;
         const uint4 q = *reinterpret_cast<const uint4 *>(raw + i * 16);
         const __nv_fp8x2_e4m3 *h = reinterpret_cast<const __nv_fp8x2_e4m3 *>(&q);
@@ -220,9 +221,10 @@ k_mvm_tc(const char *__restrict__ Mt, const char *__restrict__ gs, long nch, int
     constexpr bool kWiden = DT != MB_MVM_BF16;
     constexpr uint32_t idesc = umma_idesc_bf16(N);
     extern __shared__ __align__(128) char tcsm[];
-    __shared__ __align__(8) uint64_t full[S], empty[S], done;
+    __shared__ __align__(8) uint64_t full[S], empty[S], ready[2], tfree[2], done;
     __shared__ uint32_t s_tmem;
-    __shared__ volatile int s_abort;  // hint that shortens waits once a thread gave up
+    __shared__ int s_mmas;
+    __shared__ volatile int s_abort;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int rb = blockIdx.x, ks = blockIdx.y, z = blockIdx.z;
     const long c0 = (long)ks * cps;
@@ -230,109 +232,105 @@ k_mvm_tc(const char *__restrict__ Mt, const char *__restrict__ gs, long nch, int
     const char *ga = Mt + ((size_t)rb * nch + c0) * AB;
     const char *gb = gs + ((size_t)z * nch + c0) * BB;
     char *widen = tcsm + S * SB;  // FP8 only: two BF16 tiles
+    const uint32_t sbase = smem_addr(tcsm);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      :: "r"(smem_addr(&s_tmem)), "r"(NCOL) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 32) {
         for (int i = 0; i < S; i++) {
-            mbar_init(smem_addr(&full[i]));
-            mbar_init(smem_addr(&empty[i]));
+            mbar_init(smem_addr(&full[i]), 1);
+            mbar_init(smem_addr(&empty[i]), 1);
         }
-        mbar_init(smem_addr(&done));
+        for (int i = 0; i < 2; i++) {
+            mbar_init(smem_addr(&ready[i]), kTcWiden);
+            mbar_init(smem_addr(&tfree[i]), 1);
+        }
+        mbar_init(smem_addr(&done), 1);
         s_abort = 0;
+        s_mmas = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    const uint32_t sbase = smem_addr(tcsm);
-    int issued = 0;    // chunks whose copies thread 0 issued
-    int consumed = 0;  // chunks whose copies thread 0 saw land
-    int mmas = 0;      // chunks whose MMAs thread 0 issued
-    bool ok = true;    // this thread's waits all succeeded
 
-    if (threadIdx.x == 0)
-        for (; issued < (nchunk < S ? nchunk : S); issued++)
-            tc_load_stage(smem_addr(&full[issued]), sbase + issued * SB, ga + (size_t)issued * AB, AB,
-                          sbase + issued * SB + AB, gb + (size_t)issued * BB, BB);
-
-    if constexpr (!kWiden) {
-        // BF16: the main loop is thread 0's alone
-        if (threadIdx.x == 0)
+    if (warp == 0) {
+        if (lane == 0) {  // copies
+            auto load = [&](int c) {
+                const int st = c % S;
+                tc_load_stage(smem_addr(&full[st]), sbase + st * SB, ga + (size_t)c * AB, AB, sbase + st * SB + AB,
+                              gb + (size_t)c * BB, BB);
+            };
+            int issued = 0;
+            for (; issued < nchunk && issued < S; issued++) load(issued);
+            for (; issued < nchunk; issued++) {
+                const int c = issued - S;  // the chunk that last used this stage
+                if (!mbar_wait(smem_addr(&empty[c % S]), (uint32_t)((c / S) & 1), &s_abort)) {
+                    s_abort = 1;
+                    break;
+                }
+                load(issued);
+            }
+            // every copy this thread issued has landed before the CTA can exit
+            for (int c = issued - S < 0 ? 0 : issued - S; c < issued; c++)
+                mbar_wait(smem_addr(&full[c % S]), (uint32_t)((c / S) & 1));
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMAs
+            int mmas = 0;
             for (int ch = 0; ch < nchunk; ch++) {
                 const int st = ch % S;
-                if (!mbar_wait(smem_addr(&full[st]), (uint32_t)((ch / S) & 1))) break;
-                consumed = ch + 1;
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                tc_mma_chunk(tmem, sbase + st * SB, sbase + st * SB + AB, N * kTcK * 2, idesc, ch == 0);
-                tc_commit(smem_addr(&empty[st]));
-                mmas = ch + 1;
-                // refill the stage chunk ch-1 used once its MMAs are done
-                if (ch >= 1 && issued < nchunk) {
-                    const int ps = (ch - 1) % S;
-                    if (!mbar_wait(smem_addr(&empty[ps]), (uint32_t)(((ch - 1) / S) & 1))) break;
-                    tc_load_stage(smem_addr(&full[ps]), sbase + ps * SB, ga + (size_t)issued * AB, AB,
-                                  sbase + ps * SB + AB, gb + (size_t)issued * BB, BB);
-                    issued++;
+                if (kWiden && !mbar_wait(smem_addr(&ready[ch & 1]), (uint32_t)((ch >> 1) & 1), &s_abort)) {
+                    s_abort = 1;
+                    break;
                 }
+                if (!mbar_wait(smem_addr(&full[st]), (uint32_t)((ch / S) & 1), &s_abort)) {
+                    s_abort = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t abase = kWiden ? smem_addr(widen + (ch & 1) * kTcTileBf16) : sbase + st * SB;
+                tc_mma_chunk(tmem, abase, sbase + st * SB + AB, N * kTcK * 2, idesc, ch == 0);
+                tc_commit(smem_addr(&empty[st]));
+                if (kWiden) tc_commit(smem_addr(&tfree[ch & 1]));
+                mmas = ch + 1;
             }
-        if (warp == 0) __syncwarp();  // lanes 1..31 block here instead of polling beside lane 0
-    } else {
+            s_mmas = mmas;
+            tc_commit(smem_addr(&done));  // tracks every MMA this thread issued
+        }
+        __syncwarp();
+    } else if (kWiden) {  // widening warps
+        const int tid = threadIdx.x - 64;
         for (int ch = 0; ch < nchunk; ch++) {
-            const int st = ch % S;
-            // the copy landed, and the MMAs of chunk ch-2 (the last reader of
-            // this BF16 tile) completed
-            if (ok) ok = mbar_wait(smem_addr(&full[st]), (uint32_t)((ch / S) & 1), &s_abort);
-            if (ok && ch >= 2) ok = mbar_wait(smem_addr(&empty[(ch - 2) % S]), (uint32_t)(((ch - 2) / S) & 1), &s_abort);
-            if (!ok) s_abort = 1;
-            char *tile = widen + (ch & 1) * kTcTileBf16;
-            if (ok) tc_widen_fp8(tcsm + st * SB, tile);
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (__syncthreads_or(!ok)) break;
-            if (threadIdx.x == 0) {
-                consumed = ch + 1;
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                tc_mma_chunk(tmem, smem_addr(tile), sbase + st * SB + AB, N * kTcK * 2, idesc, ch == 0);
-                tc_commit(smem_addr(&empty[st]));
-                mmas = ch + 1;
-                if (ch >= 1 && issued < nchunk) {
-                    const int ps = (ch - 1) % S;
-                    if (mbar_wait(smem_addr(&empty[ps]), (uint32_t)(((ch - 1) / S) & 1), &s_abort)) {
-                        tc_load_stage(smem_addr(&full[ps]), sbase + ps * SB, ga + (size_t)issued * AB, AB,
-                                      sbase + ps * SB + AB, gb + (size_t)issued * BB, BB);
-                        issued++;
-                    } else {
-                        ok = false;  // seen by every thread at the next barrier
-                        s_abort = 1;
-                    }
-                }
+            if (!mbar_wait(smem_addr(&full[ch % S]), (uint32_t)((ch / S) & 1), &s_abort)) {
+                s_abort = 1;
+                break;
             }
+            // the MMAs of chunk ch-2 (the last reader of this BF16 tile) completed
+            if (ch >= 2 && !mbar_wait(smem_addr(&tfree[ch & 1]), (uint32_t)(((ch - 2) >> 1) & 1), &s_abort)) {
+                s_abort = 1;
+                break;
+            }
+            tc_widen_fp8(tcsm + (ch % S) * SB, widen + (ch & 1) * kTcTileBf16, tid);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_addr(&ready[ch & 1])) : "memory");
         }
     }
-    bool fail = false;
-    if (threadIdx.x == 0) {
-        if (mmas < nchunk) {  // gave up: record it and drain the copies in flight
-            fail = true;
-            atomicExch(err, 1);
-            for (int c = consumed; c < issued; c++) mbar_wait(smem_addr(&full[c % S]), (uint32_t)((c / S) & 1));
-        }
-        tc_commit(smem_addr(&done));  // tracks every MMA this thread issued
-    }
-    if (!mbar_wait(smem_addr(&done), 0)) {
-        fail = true;
-        if (lane == 0) atomicExch(err, 1);
-        mbar_wait(smem_addr(&done), 0);  // bounded, before the accumulators are freed
-    }
-    const bool skip = __syncthreads_or(fail) != 0;
+    bool bad = !mbar_wait(smem_addr(&done), 0);
+    if (bad) mbar_wait(smem_addr(&done), 0);  // bounded, before the accumulators are freed
+    const bool skip = __syncthreads_or(bad) || s_abort || s_mmas < nchunk;
+    if (skip && threadIdx.x == 0) atomicExch(err, 1);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // epilogue: warp w reads TMEM lanes 32w.. (rows), N columns (instances)
-    if (!skip && nchunk > 0) {
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-        const int row = rb * kTcRows + warp * 32 + lane;
+    // epilogue: warps 1-4; warp w reads TMEM lanes 32(w%4).. (rows), N columns (instances)
+    if (!skip && nchunk > 0 && warp >= 1) {
+        const int q = warp & 3;
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16);
+        const int row = rb * kTcRows + q * 32 + lane;
 #pragma unroll
         for (int cc = 0; cc < N; cc += 16) {
             uint32_t r[16];
