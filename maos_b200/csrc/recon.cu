@@ -109,6 +109,7 @@ struct Recon {
     PadIndex pad() const { return PadIndex{xpad.p, ypad.p, footprint.p, kx, ky, maxnx, maxny}; }
     DevBuf<LayerDev> lay;
     std::vector<LayerDev> lay_h;
+    LayerTab laytab{};  // lay_h by value, for kernel parameters
     std::vector<mb_grid> xgrid;   // host copy of the layer grids
     DevBuf<WfsDev> wfs;
     std::vector<std::unique_ptr<DevBuf<int2>>> saptr;
@@ -417,7 +418,7 @@ void Recon::pupil_rows(bool from_x, const float *xin, cudaStream_t s) {
 // k_hxt_rows at the padded y-list width, two instances per thread when the
 // batch has more than one.
 void Recon::hxt_rows(const float *xin, float *out, double *dot_part, int do_l2, int k, cudaStream_t s) {
-    using K = void (*)(const float *, const float *, float *, double *, PadIndex, const LayerDev *, int, int, int,
+    using K = void (*)(const float *, const float *, float *, double *, PadIndex, LayerTab, int, int, int,
                        long, long, int, CgScal, int, int, const int *);
     static const K tab1[kMaxPadY] = {k_hxt_rows<1, 1>, k_hxt_rows<2, 1>, k_hxt_rows<3, 1>, k_hxt_rows<4, 1>,
                                      k_hxt_rows<5, 1>, k_hxt_rows<6, 1>, k_hxt_rows<7, 1>, k_hxt_rows<8, 1>};
@@ -425,7 +426,7 @@ void Recon::hxt_rows(const float *xin, float *out, double *dot_part, int do_l2, 
                                      k_hxt_rows<5, 2>, k_hxt_rows<6, 2>, k_hxt_rows<7, 2>, k_hxt_rows<8, 2>};
     const int ni = nb > 1 ? 2 : 1;
     launch(ni == 2 ? tab2[ky - 1] : tab1[ky - 1], dim3(nblk_x, (nb + ni - 1) / ni), dim3(kThreads), 0, s, tbuf.p,
-           xin, out, dot_part, pad(), lay.p, nps, nwfs, nyp, nxtot, tw, do_l2, scal(), k, nb, act());
+           xin, out, dot_part, pad(), laytab, nps, nwfs, nyp, nxtot, tw, do_l2, scal(), k, nb, act());
 }
 
 void Recon::build_wfs_tables(const mb_recon_desc *d) {
@@ -542,6 +543,8 @@ void Recon::set_l2c(const double *l2c) {
         lay_h[l].l2c = (float)l2c[l];
     }
     lay.upload(lay_h);
+    MB_REQUIRE(nps <= kMaxLayers, "at most %d layers", kMaxLayers);
+    for (int l = 0; l < nps; l++) laytab.l[l] = lay_h[l];  // captured graphs are re-captured by the caller
 }
 
 // FDPCG tables for the half spectrum.  The reference orders the frequency

@@ -570,15 +570,22 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
     }
 }
 
+// The layer geometry passed by value (kernel parameter space), for kernels
+// whose first dependent step is finding a point's layer.
+struct LayerTab {
+    LayerDev l[kMaxLayers];
+};
+
 // y half of Hx^T over all WFS, + L2^T L2 x and p.Ap partials (last block:
 // alpha).  One thread per layer point and NI instances (the index work, the
 // footprint tests and the list entries are shared by the instances, and each
-// dependent step issues NI times the independent loads);
+// dependent step issues NI times the independent loads; the NI block sums
+// and last-block arrivals are taken together);
 // grid: (ceil(nxtot/256), ceil(nb/NI)).  KY is the padded y-list width.
 template <int KY, int NI>
 __global__ void __launch_bounds__(kThreads)
 k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__restrict__ out,
-           double *__restrict__ dot_part, PadIndex pi, const LayerDev *__restrict__ lay, int nps,
+           double *__restrict__ dot_part, PadIndex pi, const __grid_constant__ LayerTab lt, int nps,
            int nwfs, int nyp, long nxtot, long tw, int do_l2, CgScal S, int kit, int nb,
            const int *__restrict__ act) {
     pdl_enter();
@@ -591,15 +598,16 @@ k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__
         any = any || on[q];
     }
     if (!any) return;
-    __shared__ double sh[32];
+    __shared__ double shq[NI][32];
+    __shared__ bool s_last[NI];
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double dotv[NI];
 #pragma unroll
     for (int q = 0; q < NI; q++) dotv[q] = 0;
     if (j < nxtot) {
         int l = 0;
-        while (l + 1 < nps && j >= lay[l + 1].off) l++;
-        const LayerDev L = lay[l];
+        while (l + 1 < nps && j >= lt.l[l + 1].off) l++;
+        const LayerDev L = lt.l[l];
         const int nx = L.nx, ny = L.ny;
         const int jj = (int)(j - L.off);
         const int jy = jj / nx, jx = jj - jy * nx;
@@ -651,13 +659,39 @@ k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__
         }
     }
     if (dot_part) {
+        // block sums of the NI partials (the block_sum tree, NI at a time)
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
         for (int q = 0; q < NI; q++) {
-            if (!on[q]) continue;  // uniform over the CTA
+            const double v = warp_sum(dotv[q]);
+            if (lane == 0) shq[q][wid] = v;
+        }
+        __syncthreads();
+        if (wid == 0)
+#pragma unroll
+            for (int q = 0; q < NI; q++) {
+                double v = lane < (int)(blockDim.x >> 5) ? shq[q][lane] : 0.0;
+                v = warp_sum(v);
+                if (lane == 0 && on[q]) dot_part[(size_t)(b0 + q) * gridDim.x + blockIdx.x] = v;
+            }
+        // last block per instance: alpha_k = (r.z)_k / (p.Ap) (cg_alpha_last, NI counters at once)
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int q = 0; q < NI; q++) s_last[q] = on[q] && atomicAdd(S.cnt + b0 + q, 1u) == gridDim.x - 1;
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < NI; q++) {
+            if (!s_last[q] || threadIdx.x >= 32) continue;
             const int b = b0 + q;
-            const double d = block_sum(dotv[q], sh);
-            if (threadIdx.x == 0) dot_part[(size_t)b * gridDim.x + blockIdx.x] = d;
-            cg_alpha_last(dot_part + (size_t)b * gridDim.x, S, b, kit);
+            const double pap = warp_sum_fresh(dot_part + (size_t)b * gridDim.x, gridDim.x);
+            if (threadIdx.x == 0) {
+                double a = S.sc[(size_t)b * S.nsc + kit] / pap;
+                if (!isfinite(a)) a = 0;  // pcg.c:80-83, pcg.cu:27-30
+                S.ab[2 * b] = (float)a;
+                S.cnt[b] = 0;
+            }
         }
     }
 }

@@ -83,6 +83,37 @@ def test_solve_cold_then_warm(setup):
         assert abs(r2[b] - res2) < 0.05 * res2 + 1e-6
 
 
+def test_update_cn2_reaches_the_captured_step(setup):
+    """gpu_update_recon_cn2 (cuda/gpu.h:50): new layer weights change the
+    regularisation in both the operator and the captured graph step."""
+    import dataclasses
+    from maos_b200.config import TOMOSCALE
+    from maos_b200.geometry import laplacian_coef
+    s, R, o = setup
+    # new Cn2 profile: the layer weights reversed; l2c as the setup derives it
+    wt = np.asarray(s.wt, dtype=np.float64)[::-1].copy()
+    l2c = np.array([(laplacian_coef(s.cfg.r0, w, g.dx) * 0.25) ** 2 * s.cfg.tomo_cxxscale * TOMOSCALE
+                    for w, g in zip(wt, s.xmaps)])
+    assert not np.allclose(l2c, s.l2c)
+    s2 = dataclasses.replace(s, wt=wt, l2c=l2c)
+    o2 = TomoOracle(s2)
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal((2, s.nx_total)) * 1e-7
+    g = rng.standard_normal((2, s.ngrad)) * 1e-6
+    try:
+        R.update_cn2(l2c, s.fdpcg)  # the preconditioner tables are re-sent with it (kept here)
+        got = R.apply_L(x)
+        R.reset()
+        xs, _ = R.tomo(g)
+        for b in range(2):
+            assert rel(got[b], o2.tomo_L(x[b])) < OP_TOL
+            want, _ = tomo_solve(o2, g[b])
+            assert rel(xs[b], want) < SOLVE_TOL
+    finally:
+        R.update_cn2(np.asarray(s.l2c, dtype=np.float64), s.fdpcg)
+        R.reset()
+
+
 def test_batch_instances_are_independent(setup):
     s, R, o = setup
     from maos_b200.recon import Reconstructor
