@@ -622,6 +622,47 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
         idx[i].pad = 0;
         sc[i] = fd->scale ? 1.0 / std::sqrt((double)lay_h[e.l].nx * lay_h[e.l].ny) : 1.0;
     }
+    // The reference's CPU preconditioner keeps the real part of the inverse
+    // FFT of M X over the full spectrum (maos/fdpcg.c:612-644).  Its blocks
+    // are Hermitian-consistent (M at -k equal to conj(M) at k) only to about
+    // 1e-6, so solving half of them and mirroring would be a different
+    // operator, and 30 PCG iterations turn that 1e-6 into 1e-4 of the result.
+    // The real part equals the mirrored half with the Hermitian average of
+    // each block and the block of its negated frequencies:
+    //   Ms[b](i,j) = (M[b](i,j) + conj(M[b'](s(i), s(j)))) / 2,
+    // b' the block holding the negated frequencies, s the member map.
+    std::vector<long> inv(nxtot, -1);
+    for (long i = 0; i < nxtot; i++) {
+        const long q = fd->perm[i];
+        MB_REQUIRE(q >= 0 && q < nxtot && inv[q] < 0, "fdpcg: perm is not a permutation of the spectra");
+        inv[q] = i;
+    }
+    auto negated = [&](long q) {
+        int l = 0;
+        while (l + 1 < nps && q >= xoff[l + 1]) l++;
+        const long local = q - xoff[l];
+        const int nx = lay_h[l].nx, ny = lay_h[l].ny;
+        const long jx = local % nx, jy = local / nx;
+        return xoff[l] + ((ny - jy) % ny) * nx + (nx - jx) % nx;
+    };
+    std::vector<double> ms((size_t)nbh * fd_bs * fd_bs * 2);
+    std::vector<int> sig(fd_bs);
+    for (long b = 0; b < nbh; b++) {
+        long bp = -1;
+        for (int i = 0; i < fd_bs; i++) {
+            const long P = inv[negated(fd->perm[b * fd_bs + i])];
+            if (i == 0) bp = P / fd_bs;
+            MB_REQUIRE(P / fd_bs == bp, "fdpcg: block %ld: its negated frequencies span several blocks", b);
+            sig[i] = (int)(P % fd_bs);
+        }
+        for (int j = 0; j < fd_bs; j++)
+            for (int i = 0; i < fd_bs; i++) {
+                const size_t k = ((size_t)b * fd_bs + j) * fd_bs + i;
+                const size_t kp = ((size_t)bp * fd_bs + sig[j]) * fd_bs + sig[i];
+                ms[2 * k] = 0.5 * (fd->mbinv[2 * k] + fd->mbinv[2 * kp]);
+                ms[2 * k + 1] = 0.5 * (fd->mbinv[2 * k + 1] - fd->mbinv[2 * kp + 1]);
+            }
+    }
     // fold the 1/sqrt(n) of the forward and inverse FFTs into the blocks
     std::vector<cplx> M((size_t)nbh * fd_bs * fd_bs);
     for (long b = 0; b < nbh; b++)
@@ -629,7 +670,7 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
             for (int i = 0; i < fd_bs; i++) {
                 const size_t k = (size_t)b * fd_bs * fd_bs + (size_t)j * fd_bs + i;
                 const double s = sc[b * fd_bs + i] * sc[b * fd_bs + j];
-                M[k] = make_float2((float)(fd->mbinv[2 * k] * s), (float)(fd->mbinv[2 * k + 1] * s));
+                M[k] = make_float2((float)(ms[2 * k] * s), (float)(ms[2 * k + 1] * s));
             }
     fd_M.upload(M);
     fd_idx.upload(idx);
