@@ -235,17 +235,19 @@ class MvmPool(Pool):
         batch, dropped = self.take_batch(drop_stale)
         if not batch:
             return dropped
-        ng = self.type.ngrad
+        ng, na = self.type.ngrad, self.type.nact
         gh = self.g_host.numpy()
-        gh[:] = 0.0
         for slot, req in batch:
             gh[slot * ng:(slot + 1) * ng] = req.grad
+        # rows of idle slots keep stale gradients: their commands are never read,
+        # so only the rows up to the last active slot travel
+        top = max(slot for slot, _ in batch) + 1
         with torch.cuda.stream(self.stream):
-            self.g_dev.copy_(self.g_host, non_blocking=True)
+            self.g_dev[:top * ng].copy_(self.g_host[:top * ng], non_blocking=True)
             native.check(self.lib.mb_mvm_apply_device(self.h, C.c_void_p(self.g_dev.data_ptr()),
                                                       C.c_void_p(self.a_dev.data_ptr()),
                                                       C.c_void_p(self.stream.cuda_stream)), "mb_mvm_apply_device")
-            self.a_host.copy_(self.a_dev, non_blocking=True)
+            self.a_host[:top * na].copy_(self.a_dev[:top * na], non_blocking=True)
         ev = torch.cuda.Event()
         ev.record(self.stream)
         self.inflight = (ev, batch)
@@ -363,6 +365,7 @@ def run_served(types: List[SystemType], systems: List[Tuple[int, float, np.ndarr
         heapq.heappush(events, (rng.exponential(1.0 / rate), sid, 0))
     done_count = {sid: 0 for sid in range(len(systems))}
     pending: Dict[int, List[Request]] = {sid: [] for sid in range(len(systems))}
+    waiting = set()  # systems with requests not yet handed to the server
     left = set()
     while True:
         tn = now()
@@ -370,14 +373,16 @@ def run_served(types: List[SystemType], systems: List[Tuple[int, float, np.ndarr
             ta, sid, k = heapq.heappop(events)
             pool, rate, frames = systems[sid]
             pending[sid].append(Request(ta, sid, k, frames[k % len(frames)]))
+            waiting.add(sid)
             more = steps_per_system is None or k + 1 < steps_per_system
             if more and ta < duration:
                 heapq.heappush(events, (ta + rng.exponential(1.0 / rate), sid, k + 1))
-        for sid in pending:
-            if pending[sid] and srv.admitted(sid):
+        for sid in list(waiting):
+            if srv.admitted(sid):
                 for r in pending[sid]:
                     srv.submit(r)
                 pending[sid] = []
+                waiting.discard(sid)
         before = len(srv.completed)
         srv.step(now)
         for req in srv.completed[before:]:
@@ -386,7 +391,7 @@ def run_served(types: List[SystemType], systems: List[Tuple[int, float, np.ndarr
                     and req.system not in left):
                 left.add(req.system)
                 srv.release(req.system, now())
-        if not events and srv.idle() and not any(pending.values()):
+        if not events and srv.idle() and not waiting:
             break
         if tn > duration * 4 + 30:
             break
