@@ -151,6 +151,10 @@ struct Recon {
     int nblk_a = 0, nblk_f = 0, fnsc = 0;
     long nact = 0;
     RayTables hxp, ha;
+    DevBuf<GatherW> fxpad, fypad;  // HA^T as padded per-axis lists (k_fit_hxt)
+    int fkx = 0, fky = 0, fmaxn = 0;
+    LayerTab dmtab{};
+    FitPad fitpad() const { return FitPad{fxpad.p, fypad.p, fkx, fky, fmaxn}; }
     DevBuf<LayerDev> dmlay;
     std::vector<LayerDev> dmlay_h;
     DevBuf<int> w0_rp, w0_ci;
@@ -369,13 +373,12 @@ void Recon::build_pad() {
                                                              : make_int4(lo[0], hi[0] + 1, lo[1], hi[1] + 1);
         }
     footprint.upload(fp);
-    // pupil rows per CTA: the largest of 16, 8, 4 that still gives about two
-    // waves of 256-thread CTAs on 148 SMs (4 resident each)
-    // pupil rows per CTA: the largest of 16, 8, 4 that still gives about two
-    // waves of 256-thread CTAs on 148 SMs (4 resident each); Recon::autotune
-    // replaces this guess by measurement
+    // pupil rows per CTA: the largest of 16, 8, 4 that still gives at least
+    // two CTAs per SM (148 SMs); this matches the measured optimum of the 30 m
+    // system at 1, 8, 32 and 64 instances.  Recon::autotune replaces the guess
+    // by measurement.
     int rows = 16;
-    while (rows > 4 && (long)((nyp + rows - 1) / rows) * nwfs * nb < 2 * 148 * 4) rows /= 2;
+    while (rows > 4 && (long)((nyp + rows - 1) / rows) * nwfs * nb < 2 * 148) rows /= 2;
     if (const char *e = std::getenv("MAOS_B200_PUPIL_ROWS")) {  // tuning override
         const int v = std::atoi(e);
         if (v >= 1 && v <= 64) rows = v;
@@ -884,7 +887,7 @@ void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulF
     } else {
         launch(k_dot_self, dim3(nblk, nb), dim3(kThreads), 0, s, B.r, B.rz, n, B.S, act());  // z aliases r
     }
-    launch(k_cg_update_p, dim3(nblk, nb), dim3(kThreads), 0, s, B.p, zp, n, B.S, 1, act());
+    launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n, B.S, 1, act());
     for (int k = 0; k < iters; k++) {
         Amul(B.p, B.Ap, B.pap, k);  // its last block leaves alpha_k
         if (XrMmul && k + 1 < iters) {
@@ -895,7 +898,7 @@ void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulF
             if (k + 1 == iters) break;
             if (Mmul) Mmul(B.r, B.z, B.rz, k, 0);  // its last block leaves beta_k
         }
-        launch(k_cg_update_p, dim3(nblk, nb), dim3(kThreads), 0, s, B.p, zp, n, B.S, 0, act());
+        launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n, B.S, 0, act());
     }
 }
 
@@ -919,8 +922,8 @@ void Recon::op_fitR(const float *xin, float *out, cudaStream_t s) {
                                                     nxtot, w1v.p, w1_part.p, act());
     launch(k_fit_w, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, opdf.p, opdw.p, w0_rp.p, w0_ci.p, w0_v.p, w1v.p,
                                                        fwt.p, w1_part.p, nblk_f, nf, nfit, act());
-    launch(k_hxt, dim3(nblk_a, nb), dim3(kThreads), 0, s, opdw.p, nullptr, out, nullptr, ha.gi(), dmlay.p, ndm,
-                                               nfit, nfx, nfy, nact, 0, 1.f, LowRank{}, fscal(), 0, act());
+    launch(k_fit_hxt, dim3(nblk_a, nb), dim3(kThreads), 0, s, opdw.p, nullptr, out, nullptr, fitpad(), dmtab, ndm,
+           nfit, nfx, nfy, nact, LowRank{}, fscal(), 0, act());
 }
 
 // FitL: sum_f wt_f HA_f^T (W0 - W1 W1^T) HA_f a + NW NW^T a   (recon_utils.c:536, fit.cu:213)
@@ -934,8 +937,8 @@ void Recon::op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t
                                                     nact, w1v.p, w1_part.p, act());
     launch(k_fit_w, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, opdf.p, opdw.p, w0_rp.p, w0_ci.p, w0_v.p, w1v.p,
                                                        fwt.p, w1_part.p, nblk_f, nf, nfit, act());
-    launch(k_hxt, dim3(nblk_a, nb), dim3(kThreads), 0, s, opdw.p, ain, out, dot_part, ha.gi(), dmlay.p, ndm, nfit,
-                                               nfx, nfy, nact, 0, 1.f, lr, fscal(), k, act());
+    launch(k_fit_hxt, dim3(nblk_a, nb), dim3(kThreads), 0, s, opdw.p, ain, out, dot_part, fitpad(), dmtab, ndm,
+           nfit, nfx, nfy, nact, lr, fscal(), k, act());
 }
 
 // The DM fit of one step: RHS from the tomography solution, then CG warm-
@@ -990,6 +993,39 @@ void Recon::build_fit(const mb_fit_desc *f) {
                          dy = f->thetay[d] * ht;
                      },
                      true, ha);
+    // HA^T as padded per-axis lists over the DM grids
+    MB_REQUIRE(ndm <= kMaxLayers, "fit: at most %d DMs", kMaxLayers);
+    for (int d = 0; d < ndm; d++) dmtab.l[d] = dmlay_h[d];
+    fkx = fky = 1;
+    fmaxn = 0;
+    for (int d = 0; d < ndm; d++) fmaxn = std::max(fmaxn, std::max(dmlay_h[d].nx, dmlay_h[d].ny));
+    for (int w = 0; w < nfit; w++)
+        for (int d = 0; d < ndm; d++)
+            for (int axis = 0; axis < 2; axis++) {
+                const int tb = ha.h_ptr[(w * ndm + d) * 2 + axis];
+                const int n = axis ? dmlay_h[d].ny : dmlay_h[d].nx;
+                int &K = axis ? fky : fkx;
+                for (int j = 0; j < n; j++) K = std::max(K, ha.h_idxptr[tb + j + 1] - ha.h_idxptr[tb + j]);
+            }
+    MB_REQUIRE(fkx <= kFitPad && fky <= kFitPad, "fit: transposed lists wider than %d (%d, %d)", kFitPad, fkx,
+               fky);
+    {
+        std::vector<GatherW> xq((size_t)nfit * ndm * fmaxn * fkx, GatherW{0, 0.f});
+        std::vector<GatherW> yq((size_t)nfit * ndm * fmaxn * fky, GatherW{0, 0.f});
+        for (int w = 0; w < nfit; w++)
+            for (int d = 0; d < ndm; d++)
+                for (int axis = 0; axis < 2; axis++) {
+                    const int tb = ha.h_ptr[(w * ndm + d) * 2 + axis];
+                    const int n = axis ? dmlay_h[d].ny : dmlay_h[d].nx, K = axis ? fky : fkx;
+                    for (int j = 0; j < n; j++) {
+                        GatherW *dst = (axis ? yq.data() : xq.data()) + ((size_t)(w * ndm + d) * fmaxn + j) * K;
+                        for (int a = ha.h_idxptr[tb + j], e = 0; a < ha.h_idxptr[tb + j + 1]; a++, e++)
+                            dst[e] = ha.h_ent[a];
+                    }
+                }
+        fxpad.upload(xq);
+        fypad.upload(yq);
+    }
     // W0: CSC -> CSR
     std::vector<int> rp(nf + 1, 0), ci;
     std::vector<float> cv;
@@ -1086,7 +1122,7 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                                                                              nxtot, scal(), 0, maxit, 0, act());
                     break;
                 case 3:
-                    launch(k_cg_update_p, dim3(nblk_x, nb), dim3(kThreads), 0, stream, rhs.p, z.p, nxtot, scal(), 0, act());
+                    launch(k_cg_update_p, dim3(nblocks((nxtot + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, stream, rhs.p, z.p, nxtot, scal(), 0, act());
                     break;
                 case 4: op_fdpcg(r.p, z.p, rz_part.p, stream); break;
             }

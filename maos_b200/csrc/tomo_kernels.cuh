@@ -11,7 +11,7 @@
 //   k_pupil_rows  gpu_map2map_do + gpu_gp_do + gpu_gpt_do (tomo.cu:485) + the x half
 //                 of gpu_map2map_do 't', fused per block of pupil rows
 //   k_hxt_rows    y half of gpu_map2map_do 't' + gpu_laplacian_do (tomo.cu:317)
-//   k_hxt         gpu_map2map_do 't' in gather form (DM fit)  -- no atomics
+//   k_fit_hxt     gpu_map2map_do 't' in gather form (DM fit)  -- no atomics
 //   k_fd_*        cufdpcg_t::P (fdpcg.cu:168)                 -- own FFTs, half spectrum
 //   k_cg_*        gpu_pcg scalar kernels (pcg.cu:27-57)       -- FP64 scalars
 #pragma once
@@ -52,6 +52,14 @@ struct LayerDev {
     long off;       // offset inside one instance
     float l2c;      // biharmonic weight
     int tcol;       // first column of this layer in the row buffer of the separable Hx^T
+};
+
+constexpr int kMaxLayers = 16;  // most reconstructed layers (the Hx gather unrolls 8 or 16)
+
+// The layer geometry passed by value (kernel parameter space), for kernels
+// whose first dependent step is finding a point's layer.
+struct LayerTab {
+    LayerDev l[kMaxLayers];
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -270,11 +278,23 @@ struct LowRank {
     int nnw, nblk;
 };
 
-__global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ xin,
-                      float *__restrict__ out, double *__restrict__ dot_part, GatherIndex gi,
-                      const LayerDev *__restrict__ lay, int nps, int nwfs, int nxp, int nyp,
-                      long nxtot, int do_l2, float alpha, LowRank lr, CgScal S, int k,
-                      const int *__restrict__ act) {
+// Fit transpose HA^T in gather form over padded per-axis lists: for DM
+// point (jx, jy) of DM l and fit direction w, the fit-grid points whose
+// bilinear footprint covers it are the products of the x list
+// fx[((w*ndm + l)*maxn + jx)*kx + e] and the y list (padding: weight 0).
+// Every load of a direction depends only on (w, jx, jy), so the loads of
+// several directions are in flight together.  Plus the low-rank NW term and
+// the p.Ap partials (last block: alpha) for FitL.  grid: (ceil(nact/256), nb).
+constexpr int kFitPad = 4;  // widest padded fit list
+struct FitPad {
+    const GatherW *x, *y;
+    int kx, ky, maxn;
+};
+
+__global__ void __launch_bounds__(kThreads)
+k_fit_hxt(const float *__restrict__ opd2, const float *__restrict__ xin, float *__restrict__ out,
+          double *__restrict__ dot_part, FitPad fpd, const __grid_constant__ LayerTab dl, int ndm, int nfit,
+          int nfx, int nfy, long nact, LowRank lr, CgScal S, int k, const int *__restrict__ act) {
     pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
@@ -290,56 +310,44 @@ __global__ void k_hxt(const float *__restrict__ opd2, const float *__restrict__ 
     }
     const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double dotv = 0;
-    if (j < nxtot) {
+    if (j < nact) {
         int l = 0;
-        while (l + 1 < nps && j >= lay[l + 1].off) l++;
-        const LayerDev L = lay[l];
+        while (l + 1 < ndm && j >= dl.l[l + 1].off) l++;
+        const LayerDev L = dl.l[l];
         const int jj = (int)(j - L.off);
         const int jx = jj % L.nx, jy = jj / L.nx;
-        const int np = nxp * nyp;
+        const int np = nfx * nfy;
+        const size_t wsx = (size_t)ndm * fpd.maxn * fpd.kx, wsy = (size_t)ndm * fpd.maxn * fpd.ky;
+        const GatherW *ex0 = fpd.x + ((size_t)l * fpd.maxn + jx) * fpd.kx;
+        const GatherW *ey0 = fpd.y + ((size_t)l * fpd.maxn + jy) * fpd.ky;
+        const float *ob = opd2 + (size_t)b * nfit * np;
         float acc = 0.f;
-        for (int w = 0; w < nwfs; w++) {
-            const int tx = gi.ptr[(w * nps + l) * 2 + 0];
-            const int ty = gi.ptr[(w * nps + l) * 2 + 1];
-            const int ax0 = gi.idx_ptr[tx + jx], ax1 = gi.idx_ptr[tx + jx + 1];
-            const int ay0 = gi.idx_ptr[ty + jy], ay1 = gi.idx_ptr[ty + jy + 1];
-            if (ax0 == ax1 || ay0 == ay1) continue;
-            const float *o = opd2 + ((size_t)b * nwfs + w) * np;
-            for (int ay = ay0; ay < ay1; ay++) {
-                const GatherW ey = gi.ent[ay];
+#pragma unroll 3
+        for (int w = 0; w < nfit; w++) {
+            GatherW ex[kFitPad], ey[kFitPad];
+#pragma unroll
+            for (int e = 0; e < kFitPad; e++) {
+                ex[e] = e < fpd.kx ? ex0[w * wsx + e] : GatherW{0, 0.f};
+                ey[e] = e < fpd.ky ? ey0[w * wsy + e] : GatherW{0, 0.f};
+            }
+            const float *o = ob + (size_t)w * np;
+#pragma unroll
+            for (int ay = 0; ay < kFitPad; ay++) {
+                if (ay >= fpd.ky) break;
                 float rs = 0.f;
-                for (int ax = ax0; ax < ax1; ax++) {
-                    const GatherW ex = gi.ent[ax];
-                    rs += ex.w * o[ey.i * nxp + ex.i];
-                }
-                acc += ey.w * rs;
+#pragma unroll
+                for (int ax = 0; ax < kFitPad; ax++)
+                    if (ax < fpd.kx) rs += ex[ax].w * o[ey[ay].i * nfx + ex[ax].i];
+                acc += ey[ay].w * rs;
             }
         }
-        const float *X = xin ? xin + (size_t)b * nxtot + L.off : nullptr;
-        if (do_l2) {
-            const int nx = L.nx, ny = L.ny;
-            auto at = [&](int dx, int dy) {
-                int xx = jx + dx, yy = jy + dy;
-                xx += (xx < 0) ? nx : 0;
-                xx -= (xx >= nx) ? nx : 0;
-                yy += (yy < 0) ? ny : 0;
-                yy -= (yy >= ny) ? ny : 0;
-                return X[yy * nx + xx];
-            };
-            const float st = 20.f * at(0, 0) -
-                             8.f * (at(-1, 0) + at(1, 0) + at(0, -1) + at(0, 1)) +
-                             2.f * (at(-1, -1) + at(1, -1) + at(-1, 1) + at(1, 1)) +
-                             (at(0, -2) + at(-2, 0) + at(2, 0) + at(0, 2));
-            acc = alpha * acc + alpha * L.l2c * st;
-        } else {
-            acc = alpha * acc;
-        }
+        const float *X = xin ? xin + (size_t)b * nact + L.off : nullptr;
         if (lr.nw) {
             float lt = 0.f;
-            for (int k = 0; k < lr.nnw; k++) lt += lr.nw[(size_t)k * nxtot + j] * s_t[k];
-            acc += alpha * lt;
+            for (int q = 0; q < lr.nnw; q++) lt += lr.nw[(size_t)q * nact + j] * s_t[q];
+            acc += lt;
         }
-        out[(size_t)b * nxtot + j] = acc;
+        out[(size_t)b * nact + j] = acc;
         if (dot_part && X) dotv = (double)acc * (double)X[jj];
     }
     if (dot_part) {
@@ -387,7 +395,6 @@ struct PadIndex {
     int kx, ky, maxnx, maxny;
 };
 
-constexpr int kMaxLayers = 16;  // most reconstructed layers (the Hx gather unrolls 8 or 16)
 constexpr int kMaxPadX = 8;     // widest x list
 constexpr int kMaxPadY = 8;     // widest y list (k_hxt_rows is instantiated up to this)
 
@@ -569,12 +576,6 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
         }
     }
 }
-
-// The layer geometry passed by value (kernel parameter space), for kernels
-// whose first dependent step is finding a point's layer.
-struct LayerTab {
-    LayerDev l[kMaxLayers];
-};
 
 // y half of Hx^T over all WFS, + L2^T L2 x and p.Ap partials (last block:
 // alpha).  One thread per layer point and NI instances (the index work, the
@@ -848,17 +849,46 @@ __global__ void k_cg_update_xr(float *__restrict__ x, float *__restrict__ r,
     }
 }
 
-// p = z + beta p (init: p = z).  grid: (nblk, nb)
+// p = z + beta p (init: p = z).  kUpdP elements per thread (16-byte
+// accesses when n is a multiple of 4); every load is issued before the
+// participation flag and beta are known, so the thread waits one round trip.
+// grid: (ceil(n / (kUpdP * 256)), nb)
+constexpr int kUpdP = 4;
+
 __global__ void k_cg_update_p(float *__restrict__ p, const float *__restrict__ z, long n, CgScal S,
                               int init, const int *__restrict__ act) {
     pdl_enter();
-    if (inactive(act, blockIdx.y)) return;
     const int b = blockIdx.y;
+    const long j = ((long)blockIdx.x * blockDim.x + threadIdx.x) * kUpdP;
+    const size_t o = (size_t)b * n + j;
+    float zv[kUpdP] = {}, pv[kUpdP] = {};
+    const bool vec = (n & 3) == 0 && j + kUpdP <= n;
+    if (vec) {
+        const float4 a = *reinterpret_cast<const float4 *>(z + o);
+        zv[0] = a.x, zv[1] = a.y, zv[2] = a.z, zv[3] = a.w;
+        if (!init) {
+            const float4 c = *reinterpret_cast<const float4 *>(p + o);
+            pv[0] = c.x, pv[1] = c.y, pv[2] = c.z, pv[3] = c.w;
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < kUpdP; u++)
+            if (j + u < n) {
+                zv[u] = z[o + u];
+                if (!init) pv[u] = p[o + u];
+            }
+    }
+    if (inactive(act, b)) return;
     const float be = init ? 0.f : S.ab[2 * b + 1];
-    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < n) {
-        const size_t o = (size_t)b * n + j;
-        p[o] = init ? z[o] : z[o] + be * p[o];
+    float r[kUpdP];
+#pragma unroll
+    for (int u = 0; u < kUpdP; u++) r[u] = init ? zv[u] : zv[u] + be * pv[u];
+    if (vec) {
+        *reinterpret_cast<float4 *>(p + o) = make_float4(r[0], r[1], r[2], r[3]);
+    } else {
+#pragma unroll
+        for (int u = 0; u < kUpdP; u++)
+            if (j + u < n) p[o + u] = r[u];
     }
 }
 
