@@ -1,12 +1,17 @@
 """One batched reconstruction step of a preset, for profilers.
 
     python -m maos_b200.profile_step [--system mcao_30m] [--batch 32] [--steps 1]
+    python -m maos_b200.profile_step --mvm bf16 [--batch 32] [--steps 1]
 
 Builds the system, sets up a reconstructor with the DM fit for `batch`
 instances and runs `steps` graph steps on random gradients; prints "ok".
 Under ncu, each step's kernels appear in order: k_gp, k_pupil_rows (right-hand
 side), k_hxt_rows, then per FDPCG iteration k_pupil_rows, k_hxt_rows,
 k_fd_fwd, k_fd_mul, k_fd_inv, k_cg_update_p, then the fit.
+
+With --mvm, a random control matrix of the system's shape (nact x ngrad) is
+installed in that storage type and `steps` batched MVMs are applied instead
+(k_gsplit, k_mvm_tc, k_mvm_reduce for BF16/FP8 at 4 or more instances).
 """
 from __future__ import annotations
 
@@ -21,9 +26,30 @@ def main():
     ap.add_argument("--system", default="mcao_30m", choices=sorted(config.PRESETS))
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--mvm", choices=["fp32", "bf16", "fp8"], default=None)
     a = ap.parse_args()
     s = geometry.build_tomo(config.PRESETS[a.system]())
     fs = fit_setup.build_fit(s)
+    if a.mvm:
+        import ctypes as C
+        import numpy as np
+        from . import native
+        lib = native.load()
+        M = np.asfortranarray(np.random.default_rng(0).standard_normal((int(fs.nact), int(s.ngrad))))
+        h = C.c_void_p()
+        native.check(lib.mb_mvm_create(M.ctypes.data_as(C.POINTER(C.c_double)), M.shape[0], M.shape[1],
+                                       ["fp32", "bf16", "fp8"].index(a.mvm), a.batch, C.byref(h)), "mb_mvm_create")
+        del M
+        g = torch.randn(a.batch * s.ngrad, device="cuda")
+        out = torch.empty(a.batch * int(fs.nact), device="cuda")
+        st = torch.cuda.Stream()
+        for _ in range(a.steps):
+            native.check(lib.mb_mvm_apply_device(h, C.c_void_p(g.data_ptr()), C.c_void_p(out.data_ptr()),
+                                                 C.c_void_p(st.cuda_stream)), "mb_mvm_apply_device")
+        torch.cuda.synchronize()
+        lib.mb_mvm_free(h)
+        print("ok")
+        return
     R = Reconstructor(s, nbatch=a.batch, fit=fs)
     g = torch.randn(a.batch * s.ngrad, device="cuda") * 1e-6
     st = torch.cuda.Stream()
