@@ -187,8 +187,9 @@ int mb_recon_serve_step(mb_recon *r, const int *active, const float *grad, float
 
 /* Autotuner (no counterpart in the reference): times the tomography
  * operator with each admissible row blocking of its pupil-grid kernel (4, 8,
- * 16 pupil rows per CTA) on this batch size, keeps the fastest and captures
- * the step graphs again.  Results do not depend on the choice.  rows (may be
+ * 16 pupil rows per CTA, and every even split of the pupil rows into blocks
+ * of 4 to 32 rows) on this batch size, keeps the fastest and captures the
+ * step graphs again.  Results do not depend on the choice.  rows (may be
  * NULL): the blocking kept; ms (may be NULL, 3 floats): ms per operator for
  * 4, 8, 16 rows, -1 where a blocking does not fit. */
 int mb_autotune(mb_recon *r, int reps, int *rows, float *ms);

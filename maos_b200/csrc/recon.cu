@@ -373,12 +373,13 @@ void Recon::build_pad() {
                                                              : make_int4(lo[0], hi[0] + 1, lo[1], hi[1] + 1);
         }
     footprint.upload(fp);
-    // pupil rows per CTA: the largest of 16, 8, 4 that still gives at least
-    // two CTAs per SM (148 SMs); this matches the measured optimum of the 30 m
-    // system at 1, 8, 32 and 64 instances.  Recon::autotune replaces the guess
-    // by measurement.
-    int rows = 16;
-    while (rows > 4 && (long)((nyp + rows - 1) / rows) * nwfs * nb < 2 * 148) rows /= 2;
+    // pupil rows per CTA: as many row blocks per WFS as one wave of 4 CTAs on
+    // each of 148 SMs holds, at least 3 and with at least 4 rows per block
+    // (the measured optimum of the 30 m system at 1, 32 and 64 instances);
+    // Recon::autotune replaces the guess by measurement.
+    const long nmax = (nyp + 3) / 4;
+    const long tiles = std::max(3L, std::min(nmax, (long)(4 * 148) / std::max(1L, (long)nwfs * nb)));
+    int rows = (int)((nyp + tiles - 1) / tiles);
     if (const char *e = std::getenv("MAOS_B200_PUPIL_ROWS")) {  // tuning override
         const int v = std::atoi(e);
         if (v >= 1 && v <= 64) rows = v;
@@ -1145,15 +1146,21 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
 // captured again.  ms_out[i]: ms per operator for 4, 8, 16 rows (-1: not
 // admissible).  Returns the rows kept.
 int Recon::autotune(int reps, float *ms_out) {
-    const int cand[3] = {4, 8, 16};
+    // 4, 8 and 16 rows (reported in ms_out), then every even split of the
+    // pupil rows into k blocks (ceil(nyp/k) rows, 4..32)
+    std::vector<int> cand = {4, 8, 16};
+    for (int k = 1; k <= nyp; k++) {
+        const int r = (nyp + k - 1) / k;
+        if (r >= 4 && r <= 32 && std::find(cand.begin(), cand.end(), r) == cand.end()) cand.push_back(r);
+    }
     set_mask(nullptr, stream);
     cudaEvent_t e0, e1;
     MB_CUDA_TRY(cudaEventCreate(&e0));
     MB_CUDA_TRY(cudaEventCreate(&e1));
     int best = prows;
     float tbest = 1e30f;
-    for (int c = 0; c < 3; c++) {
-        if (ms_out) ms_out[c] = -1.f;
+    for (size_t c = 0; c < cand.size(); c++) {
+        if (ms_out && c < 3) ms_out[c] = -1.f;
         if ((size_t)pupil_rows_smem_floats(cand[c], nxp, nps, ncols, kx) * sizeof(float) > 200 * 1024) continue;
         set_pupil_rows(cand[c]);
         op_lhs(p.p, Ap.p, nullptr, stream);  // warm
@@ -1164,7 +1171,7 @@ int Recon::autotune(int reps, float *ms_out) {
         float t = 0;
         MB_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
         t /= reps;
-        if (ms_out) ms_out[c] = t;
+        if (ms_out && c < 3) ms_out[c] = t;
         if (t < tbest) {
             tbest = t;
             best = cand[c];

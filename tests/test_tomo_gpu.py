@@ -159,7 +159,11 @@ def test_autotune_keeps_results():
     try:
         x0, _ = R.tomo(g)
         rows, ms = R.autotune(reps=3)
-        assert rows in ms and ms[rows] == min(ms.values())
+        nyp = s.pmap.nx
+        splits = {-(-nyp // k) for k in range(1, nyp + 1)}
+        assert rows in ms or (4 <= rows <= 32 and rows in splits)  # 4/8/16 or an even split
+        if rows in ms:
+            assert ms[rows] == min(ms.values())
         R.reset()
         x1, _ = R.tomo(g)
         assert np.array_equal(x0, x1)
