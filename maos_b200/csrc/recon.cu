@@ -72,15 +72,13 @@ static void launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, c
     count_launches(1);
 }
 
-// Forward tables for (direction d, source grid t) and their exact transposes
-// as per-axis CSR lists over the source grid (gather form).
+// Forward tables for (direction d, source grid t) on the device, and their
+// exact transposes as per-axis CSR lists over the source grid (gather form)
+// on the host, from which the padded gather lists of the kernels are built.
 struct RayTables {
     DevBuf<AxisW> fwd;
-    DevBuf<int> ptr, idxptr;
-    DevBuf<GatherW> ent;
-    std::vector<int> h_ptr, h_idxptr;  // host copies for tiling decisions
+    std::vector<int> h_ptr, h_idxptr;
     std::vector<GatherW> h_ent;
-    GatherIndex gi() const { return GatherIndex{ptr.p, idxptr.p, ent.p}; }
 };
 
 struct Recon {
@@ -297,9 +295,6 @@ static void build_ray_tables(const mb_grid &og, int ndir, int nt, const mb_grid 
                 idxptr.push_back((int)ent.size());
             }
         }
-    rt.ptr.upload(ptr);
-    rt.idxptr.upload(idxptr);
-    rt.ent.upload(ent);
     rt.h_ptr = std::move(ptr);
     rt.h_idxptr = std::move(idxptr);
     rt.h_ent = std::move(ent);

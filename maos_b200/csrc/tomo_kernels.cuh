@@ -248,17 +248,6 @@ __global__ void k_gp(const float *__restrict__ opd, const float *__restrict__ gi
     }
 }
 
-// ---------------------------------------------------------------------------
-// Hx^T in gather form (+ L2^T L2 regularisation and p.Ap partial for the LHS).
-// Layer points are flattened over all layers; grid: (nblk_x, nb).
-// The transposed table for (w, l, axis) is a CSR list per layer column/row.
-// ---------------------------------------------------------------------------
-struct GatherIndex {
-    const int *ptr;        // [ntab] offsets of each (w,l,axis) CSR in `idx_ptr`
-    const int *idx_ptr;    // concatenated CSR row pointers
-    const GatherW *ent;    // concatenated entries
-};
-
 // alpha_k = (r.z)_k / (p.Ap), reduced by the last block of the p.Ap producer.
 __device__ __forceinline__ void cg_alpha_last(const double *part_b, const CgScal &S, int b, int k) {
     if (last_block(S.cnt + b, gridDim.x) && threadIdx.x < 32) {
