@@ -74,6 +74,14 @@ typedef struct {
     int scale;           /* 1: FFTs scaled by 1/sqrt(nx*ny) (fdpcg->scale) */
     const long *perm;    /* [nb*bs] fdpcg->perm (shift=1, full spectrum) */
     const double *mbinv; /* [nb*bs*bs*2] fdpcg->Mbinv, complex, column-major blocks */
+    /* Optional (both or neither; no reference counterpart): the block matrix
+       before inversion, split into its WFS term [nb*bs*bs*2] (complex,
+       column-major blocks) and its diagonal invpsd term [nb*bs] at the l2c
+       passed with this descriptor.  With them the device keeps the data term,
+       and mb_update_recon_cn2(r, l2c, NULL) rebuilds Mbinv on the GPU (the
+       invpsd term scales with each layer's l2c). */
+    const double *mdata;
+    const double *mdiag;
 } mb_fdpcg_desc;
 
 /* DM fit in grid form (cuda/fit.cu cufit_grid; recon->fit, maos/setup_recon_fit.c):
@@ -129,7 +137,10 @@ void mb_recon_free(mb_recon *r);
 int mb_recon_reset(mb_recon *r);
 /* gpu_update_recon (cuda/gpu.h:49): new NEA (and tip/tilt projector) for one WFS. */
 int mb_update_recon_nea(mb_recon *r, int iwfs, const double *neai, const double *ptt);
-/* gpu_update_recon_cn2 (cuda/gpu.h:50): new layer weights and FDPCG blocks. */
+/* gpu_update_recon_cn2 (cuda/gpu.h:50): new layer weights and FDPCG blocks.
+ * fdpcg NULL (FDPCG on): the blocks are rebuilt on the GPU from the data term
+ * kept at setup (mb_fdpcg_desc.mdata/mdiag), with invpsd scaled by the new
+ * l2c; MB_EINVAL when no data term was given. */
 int mb_update_recon_cn2(mb_recon *r, const double *l2c, const mb_fdpcg_desc *fdpcg);
 
 /* gpu_tomo (cuda/gpu.h:55, curecon_t::tomo cuda/recon.cu:259).

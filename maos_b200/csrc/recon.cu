@@ -119,6 +119,13 @@ struct Recon {
     int fd_nb = 0, fd_bs = 0, fd_nbh = 0;  // blocks, block size, blocks solved (half spectrum)
     DevBuf<cplx> fd_M;
     DevBuf<FdIndex> fd_idx;
+    // device rebuild of the blocks after a Cn2 update (k_fd_prepare, k_fd_fold)
+    bool fd_dev = false;                    // the data term below is present
+    DevBuf<double2> fd_mdata, fd_minv;      // [nb][bs][bs] column-major
+    DevBuf<double> fd_mdiag, fd_sc, fd_lscale;
+    DevBuf<int> fd_mlayer, fd_bp, fd_sig;
+    std::vector<double> fd_l2c_ref;         // l2c at which fd_mdiag holds invpsd
+    std::vector<double> l2c_now;            // l2c last installed
     DevBuf<FdLayer> fd_lay;                 // per layer: FFT geometry and radices
     DevBuf<cplx> fd_tw;                     // twiddle tables exp(-2 pi i k/n)
     int fd_bufn = 0;                        // complex elements per FFT shared buffer
@@ -182,6 +189,7 @@ struct Recon {
     void build_hx_tables(const mb_recon_desc *d);
     void build_pad();
     void set_pupil_rows(int rows);
+    void rebuild_fdpcg_device();
     int autotune(int reps, float *ms_out);
     void pupil_rows(bool from_x, const float *xin, cudaStream_t s);
     void hxt_rows(const float *xin, float *out, double *dot_part, int do_l2, int k, cudaStream_t s);
@@ -544,6 +552,7 @@ void Recon::set_l2c(const double *l2c) {
     lay.upload(lay_h);
     MB_REQUIRE(nps <= kMaxLayers, "at most %d layers", kMaxLayers);
     for (int l = 0; l < nps; l++) laytab.l[l] = lay_h[l];  // captured graphs are re-captured by the caller
+    l2c_now.assign(l2c, l2c + nps);
 }
 
 // FDPCG tables for the half spectrum.  The reference orders the frequency
@@ -645,15 +654,17 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
         return xoff[l] + ((ny - jy) % ny) * nx + (nx - jx) % nx;
     };
     std::vector<double> ms((size_t)nbh * fd_bs * fd_bs * 2);
-    std::vector<int> sig(fd_bs);
+    std::vector<int> bpv(nbh), sigv((size_t)nbh * fd_bs);
     for (long b = 0; b < nbh; b++) {
         long bp = -1;
+        int *sig = sigv.data() + b * fd_bs;
         for (int i = 0; i < fd_bs; i++) {
             const long P = inv[negated(fd->perm[b * fd_bs + i])];
             if (i == 0) bp = P / fd_bs;
             MB_REQUIRE(P / fd_bs == bp, "fdpcg: block %ld: its negated frequencies span several blocks", b);
             sig[i] = (int)(P % fd_bs);
         }
+        bpv[b] = (int)bp;
         for (int j = 0; j < fd_bs; j++)
             for (int i = 0; i < fd_bs; i++) {
                 const size_t k = ((size_t)b * fd_bs + j) * fd_bs + i;
@@ -673,6 +684,24 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
             }
     fd_M.upload(M);
     fd_idx.upload(idx);
+    // the data term for device rebuilds (k_fd_prepare, k_fd_fold)
+    fd_dev = fd->mdata && fd->mdiag;
+    if (fd_dev) {
+        const size_t nel = (size_t)fd_nb * fd_bs * fd_bs;
+        std::vector<double2> md(nel);
+        for (size_t k = 0; k < nel; k++) md[k] = make_double2(fd->mdata[2 * k], fd->mdata[2 * k + 1]);
+        fd_mdata.upload(md);
+        fd_mdiag.upload(std::vector<double>(fd->mdiag, fd->mdiag + (size_t)fd_nb * fd_bs));
+        std::vector<int> ml((size_t)fd_nb * fd_bs);
+        for (long i = 0; i < (long)fd_nb * fd_bs; i++) ml[i] = member(fd->perm[i]).l;
+        fd_mlayer.upload(ml);
+        fd_bp.upload(bpv);
+        fd_sig.upload(sigv);
+        fd_sc.upload(sc);
+        fd_minv.alloc(nel);
+        fd_lscale.alloc(nps);
+        fd_l2c_ref = l2c_now;
+    }
     spec.alloc(acc);
     spec2.alloc(acc);
     spec.zero_async(stream);  // spectra of instances that never ran stay finite
@@ -736,6 +765,27 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
     MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
     MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
 
+}
+
+// FDPCG blocks from the stored data term at the current l2c: the invpsd
+// diagonal scales with each layer's l2c (fdpcg.c:375-403: invpsd is the
+// spectrum of L2^T L2).  Synchronous.
+void Recon::rebuild_fdpcg_device() {
+    MB_REQUIRE(fd_dev, "fdpcg: no data term on the device (mb_fdpcg_desc.mdata/mdiag at setup)");
+    std::vector<double> ls(nps);
+    for (int l = 0; l < nps; l++) {
+        MB_REQUIRE(fd_l2c_ref[l] > 0, "fdpcg: layer %d has no regularisation to scale", l);
+        ls[l] = l2c_now[l] / fd_l2c_ref[l];
+    }
+    MB_CUDA_TRY(cudaMemcpyAsync(fd_lscale.p, ls.data(), nps * sizeof(double), cudaMemcpyHostToDevice, stream));
+    k_fd_prepare<<<(fd_nb + kPrepWarps - 1) / kPrepWarps, 32 * kPrepWarps, 0, stream>>>(
+        fd_mdata.p, fd_mdiag.p, fd_mlayer.p, fd_lscale.p, fd_minv.p, fd_nb, fd_bs);
+    MB_CHECK_LAUNCH();
+    const long n = (long)fd_nbh * fd_bs * fd_bs;
+    k_fd_fold<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(fd_minv.p, fd_bp.p, fd_sig.p, fd_sc.p, fd_M.p,
+                                                             fd_nbh, fd_bs);
+    MB_CHECK_LAUNCH();
+    MB_CUDA_TRY(cudaStreamSynchronize(stream));
 }
 
 void Recon::build(const mb_recon_desc *d) {
@@ -1354,7 +1404,10 @@ int mb_update_recon_cn2(mb_recon *h, const double *l2c, const mb_fdpcg_desc *fd)
     MB_REQUIRE(h && l2c, "invalid arguments");
     MB_CUDA_TRY(cudaStreamSynchronize(h->R.stream));
     h->R.set_l2c(l2c);
-    if (h->R.precond) h->R.build_fdpcg(fd);
+    if (h->R.precond) {
+        if (fd) h->R.build_fdpcg(fd);
+        else h->R.rebuild_fdpcg_device();  // new invpsd from the stored data term, on the GPU
+    }
     h->R.capture_graph();
     MB_API_END
 }

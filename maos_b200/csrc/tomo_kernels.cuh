@@ -1318,6 +1318,150 @@ k_fd_mul(const cplx *__restrict__ X, cplx *__restrict__ Y, const cplx *__restric
     }
 }
 
+// ---------------------------------------------------------------------------
+// FDPCG blocks rebuilt on the device after a Cn2 update (maos/fdpcg.c:331-580
+// fdpcg_prepare, its inversion step).  Per block b, in FP64:
+//   M = Hermitian part of (data term + diag(invpsd * l2c_new / l2c_setup)),
+//   entries below 1e-15 in magnitude dropped (cspdroptol), then
+//   Minv = pseudo-inverse of M with eigenvalues at or below 1e-7 of the
+//   largest dropped (the reference's SVD rule: for a Hermitian M the singular
+//   values are the eigenvalue magnitudes).  The eigensystem comes from cyclic
+//   complex Jacobi rotations, one warp per block: a rotation of columns
+//   p, q by c and s e^{i th} (e^{i th} = M_pq / |M_pq|), then of rows p, q,
+//   lanes owning rows (column step) or columns (row step).  At most
+//   kPrepSweeps sweeps; a sweep is skipped once the off-diagonal norm is
+//   below 1e-15 of the diagonal norm.  Blocks are column-major, (i, j) at
+//   (b*bs + j)*bs + i, as mb_fdpcg_desc.mbinv.
+// ---------------------------------------------------------------------------
+constexpr int kPrepWarps = 4;
+constexpr int kPrepSweeps = 20;
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 zconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 zaxpy(double a, double2 x, double2 y) { return make_double2(a * x.x + y.x, a * x.y + y.y); }
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_allsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// grid: ceil(nb / kPrepWarps) x (32 * kPrepWarps)
+__global__ void __launch_bounds__(32 * kPrepWarps)
+k_fd_prepare(const double2 *__restrict__ mdata, const double *__restrict__ mdiag, const int *__restrict__ mlayer,
+             const double *__restrict__ lscale, double2 *__restrict__ minv, int nb, int bs) {
+    __shared__ double2 sA[kPrepWarps][kMaxBs][kMaxBs + 1];
+    __shared__ double2 sV[kPrepWarps][kMaxBs][kMaxBs + 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * kPrepWarps + warp;
+    if (b >= nb) return;  // whole warps only: no CTA-wide barrier below
+    double2(*A)[kMaxBs + 1] = sA[warp];
+    double2(*V)[kMaxBs + 1] = sV[warp];
+    const double2 *Mb = mdata + (size_t)b * bs * bs;
+    constexpr int kPer = (kMaxBs * kMaxBs + 31) / 32;
+    double2 h[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {  // Hermitian part plus the scaled diagonal
+        const int e = lane + 32 * u;
+        if (e < bs * bs) {
+            const int j = e / bs, i = e - j * bs;
+            const double2 a = Mb[e], at = zconj(Mb[(size_t)i * bs + j]);
+            double2 v = make_double2(0.5 * (a.x + at.x), 0.5 * (a.y + at.y));
+            if (i == j) v.x += mdiag[(size_t)b * bs + i] * lscale[mlayer[(size_t)b * bs + i]];
+            if (sqrt(v.x * v.x + v.y * v.y) < 1e-15) v = make_double2(0.0, 0.0);  // cspdroptol
+            h[u] = v;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {
+        const int e = lane + 32 * u;
+        if (e < bs * bs) {
+            const int j = e / bs, i = e - j * bs;
+            A[i][j] = h[u];
+            V[i][j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+        }
+    }
+    __syncwarp();
+    for (int sweep = 0; sweep < kPrepSweeps; sweep++) {
+        double off = 0, dia = 0;
+        for (int e = lane; e < bs * bs; e += 32) {
+            const int j = e / bs, i = e - j * bs;
+            const double m2 = A[i][j].x * A[i][j].x + A[i][j].y * A[i][j].y;
+            if (i == j) dia += m2;
+            else off += m2;
+        }
+        off = warp_allsum(off);
+        dia = warp_allsum(dia);
+        if (off <= 1e-30 * dia) break;
+        for (int p = 0; p < bs - 1; p++)
+            for (int q = p + 1; q < bs; q++) {
+                const double2 apq = A[p][q];
+                const double r = sqrt(apq.x * apq.x + apq.y * apq.y);
+                if (r == 0.0) continue;  // uniform over the warp
+                const double2 e = make_double2(apq.x / r, apq.y / r);
+                const double tau = (A[q][q].x - A[p][p].x) / (2.0 * r);
+                const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                const double c = 1.0 / sqrt(1.0 + t * t), sn = t * c;
+                const double2 se = make_double2(sn * e.x, sn * e.y), sec = zconj(se);
+                __syncwarp();
+                if (lane < bs) {  // columns p, q of A and V
+                    const double2 cp = A[lane][p], cq = A[lane][q];
+                    A[lane][p] = zaxpy(c, cp, make_double2(-(sec.x * cq.x - sec.y * cq.y), -(sec.x * cq.y + sec.y * cq.x)));
+                    A[lane][q] = zaxpy(c, cq, zmul(se, cp));
+                    const double2 vp = V[lane][p], vq = V[lane][q];
+                    V[lane][p] = zaxpy(c, vp, make_double2(-(sec.x * vq.x - sec.y * vq.y), -(sec.x * vq.y + sec.y * vq.x)));
+                    V[lane][q] = zaxpy(c, vq, zmul(se, vp));
+                }
+                __syncwarp();
+                if (lane < bs) {  // rows p, q of A
+                    const double2 rp = A[p][lane], rq = A[q][lane];
+                    A[p][lane] = zaxpy(c, rp, make_double2(-(se.x * rq.x - se.y * rq.y), -(se.x * rq.y + se.y * rq.x)));
+                    A[q][lane] = zaxpy(c, rq, zmul(sec, rp));
+                }
+                __syncwarp();
+            }
+    }
+    __syncwarp();
+    // pseudo-inverse from the eigensystem
+    double lmax = 0;
+    for (int k = lane; k < bs; k += 32) lmax = fmax(lmax, fabs(A[k][k].x));
+    lmax = warp_max(lmax);
+    const double thr = 1e-7 * lmax;
+    double2 *out = minv + (size_t)b * bs * bs;
+    for (int e = lane; e < bs * bs; e += 32) {
+        const int j = e / bs, i = e - j * bs;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int k = 0; k < bs; k++) {
+            const double lam = A[k][k].x;
+            if (fabs(lam) <= thr) continue;
+            const double2 t2 = zmul(V[i][k], zconj(V[j][k]));
+            acc.x += t2.x / lam;
+            acc.y += t2.y / lam;
+        }
+        out[e] = acc;
+    }
+}
+
+// The blocks the half-spectrum solve uses: Hermitian average with the block
+// of the negated frequencies (partner bp[b], member map sig) and the FFT
+// scaling folded in, as the host does at setup; FP32 out.
+// grid: ceil(nbh*bs*bs / 256) x 256
+__global__ void k_fd_fold(const double2 *__restrict__ minv, const int *__restrict__ bp, const int *__restrict__ sig,
+                          const double *__restrict__ sc, cplx *__restrict__ M, int nbh, int bs) {
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (long)nbh * bs * bs) return;
+    const int b = (int)(k / (bs * bs)), r = (int)(k - (long)b * bs * bs);
+    const int j = r / bs, i = r - j * bs;
+    const long kp = ((long)bp[b] * bs + sig[b * bs + j]) * bs + sig[b * bs + i];
+    const double2 a = minv[k], p = minv[kp];
+    const double s = sc[b * bs + i] * sc[b * bs + j];
+    M[k] = make_float2((float)(0.5 * (a.x + p.x) * s), (float)(0.5 * (a.y - p.y) * s));
+}
+
 // Inverse: half spectra H -> z (instance-major), plus the r.z partial of this
 // (layer, instance); the last CTA of an instance leaves (r.z)_0 or beta.
 // grid: (nps, nb); shared memory as k_fd_fwd.

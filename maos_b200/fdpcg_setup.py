@@ -33,6 +33,12 @@ class FdpcgTables:
     perm: np.ndarray        # int64 [nb*bs]: index into the natural-order concatenated FFT of x
     Mbinv: np.ndarray       # complex128 [nb, bs, bs]
     nxtot: int
+    # M before inversion, split so that a device can rebuild Mbinv after a
+    # Cn2 update: the WFS (data) term, and the diagonal invpsd term at the
+    # layer weights of this setup (it scales with each layer's l2c); both
+    # already multiplied by nx*ny when the oversampling is uniform.
+    mhat_data: np.ndarray = None   # complex128 [nb, bs, bs]
+    mhat_diag: np.ndarray = None   # float64 [nb, bs]
 
 
 def _saselect_center(nxp, nyp, dxp, salocx, salocy, saa):
@@ -157,6 +163,8 @@ def fdpcg_prepare(sysm) -> FdpcgTables:
     perm0, blocks = block_members(nx, ny, os_, adimx, adimy, shift=0)
     perm1, _ = block_members(nx, ny, os_, adimx, adimy, shift=1)
     Mb = np.zeros((nb, bs, bs), dtype=np.complex128)
+    Md = np.zeros((nb, bs, bs), dtype=np.complex128)
+    Mg = np.zeros((nb, bs), dtype=np.float64)
     # member descriptors (layer, shifted jx, shifted jy) in block order
     mem_l = np.concatenate([[ips] * (os_[ips] ** 2) for ips in range(nps)])
     nxp2, nyp2 = nxp // 2, nyp // 2
@@ -168,7 +176,8 @@ def fdpcg_prepare(sysm) -> FdpcgTables:
             off = sum(nx[k] * ny[k] for k in range(l))
             r = m - off
             lj.append((l, r % nx[l], r // nx[l]))
-        M = np.diag([invpsd[l][jy, jx] for (l, jx, jy) in lj]).astype(np.complex128)
+        diag = np.array([invpsd[l][jy, jx] for (l, jx, jy) in lj], dtype=np.float64)
+        M = np.zeros((bs, bs), dtype=np.complex128)
         # pupil frequencies aliasing to this block: centred kx = ix + adimx*m
         for mxp in range(pos):
             for myp in range(pos):
@@ -206,6 +215,10 @@ def fdpcg_prepare(sysm) -> FdpcgTables:
                     M += np.outer(np.conj(v), v) * d
         if not needscale:
             M *= nx[0] * ny[0]
+            diag = diag * (nx[0] * ny[0])
+        Md[b] = M
+        Mg[b] = diag
+        M = M + np.diag(diag)
         M = 0.5 * (M + M.conj().T)
         M[np.abs(M) < 1e-15] = 0  # cspdroptol(Mhat, EPS), EPS = 1e-15 (sys/common.h:88)
         U, s, Vh = np.linalg.svd(M)
@@ -216,4 +229,4 @@ def fdpcg_prepare(sysm) -> FdpcgTables:
         si[first:] = 0.0
         Mb[b] = (Vh.conj().T * si) @ U.conj().T
     return FdpcgTables(bs=bs, nb=nb, adimx=adimx, adimy=adimy, scale=needscale,
-                       perm=perm1, Mbinv=Mb, nxtot=nxtot)
+                       perm=perm1, Mbinv=Mb, nxtot=nxtot, mhat_data=Md, mhat_diag=Mg)

@@ -33,7 +33,8 @@ class MbWfsDesc(C.Structure):
 
 class MbFdpcgDesc(C.Structure):
     _fields_ = [("nb", C.c_int), ("bs", C.c_int), ("scale", C.c_int),
-                ("perm", C.POINTER(C.c_long)), ("mbinv", C.POINTER(C.c_double))]
+                ("perm", C.POINTER(C.c_long)), ("mbinv", C.POINTER(C.c_double)),
+                ("mdata", C.POINTER(C.c_double)), ("mdiag", C.POINTER(C.c_double))]
 
 
 class MbFitDesc(C.Structure):

@@ -46,8 +46,17 @@ def fdpcg_desc(fd, keep: list) -> MbFdpcgDesc:
     mbi[0::2] = mb.real
     mbi[1::2] = mb.imag
     keep += [perm, mbi]
+    md = mg = C.POINTER(C.c_double)()
+    if getattr(fd, "mhat_data", None) is not None and getattr(fd, "mhat_diag", None) is not None:
+        d = np.ascontiguousarray(fd.mhat_data.transpose(0, 2, 1)).ravel()
+        mdi = np.empty(d.size * 2)
+        mdi[0::2] = d.real
+        mdi[1::2] = d.imag
+        mgd = np.ascontiguousarray(fd.mhat_diag, dtype=np.float64).ravel()
+        keep += [mdi, mgd]
+        md, mg = _dptr(mdi), _dptr(mgd)
     return MbFdpcgDesc(int(fd.nb), int(fd.bs), int(fd.scale),
-                       perm.ctypes.data_as(C.POINTER(C.c_long)), _dptr(mbi))
+                       perm.ctypes.data_as(C.POINTER(C.c_long)), _dptr(mbi), md, mg)
 
 
 def fit_desc(fs, keep: list) -> MbFitDesc:

@@ -355,8 +355,19 @@ def run_served(types: List[SystemType], systems: List[Tuple[int, float, np.ndarr
     ``steps_per_system`` completed requests (if given), freeing its slot for
     waiters.  Arrivals stop at ``duration``; the loop then drains the queues.
     Returns (server, completed requests, wall seconds)."""
+    import gc
     rng = np.random.default_rng(seed)
     srv = server or Server(types, hbm_budget, pool_factory=pool_factory, drop_stale=drop_stale)
+    gc_was = gc.isenabled()
+    gc.disable()  # no collector pauses inside the real-time loop
+    try:
+        return _serve_loop(srv, systems, duration, steps_per_system, rng, clock)
+    finally:
+        if gc_was:
+            gc.enable()
+
+
+def _serve_loop(srv, systems, duration, steps_per_system, rng, clock):
     t0 = clock()
     now = lambda: clock() - t0  # noqa: E731
     events = []  # (time, system, step)

@@ -114,6 +114,44 @@ def test_update_cn2_reaches_the_captured_step(setup):
         R.reset()
 
 
+def test_update_cn2_rebuilds_fdpcg_on_device(setup):
+    """mb_update_recon_cn2 without new tables: the FDPCG blocks for the new
+    layer weights are rebuilt on the GPU from the data term kept at setup;
+    they must act like the host fdpcg_prepare of the new weights, and a
+    rebuild at the original weights must give back the original operator."""
+    import dataclasses
+    from maos_b200 import fdpcg_setup
+    from maos_b200.config import TOMOSCALE
+    from maos_b200.geometry import laplacian_coef
+    s, R, o = setup
+    if s.fdpcg is None:
+        pytest.skip("plain CG configuration")
+    wt = np.asarray(s.wt, dtype=np.float64)[::-1].copy()
+    l2c = np.array([(laplacian_coef(s.cfg.r0, w, g.dx) * 0.25) ** 2 * s.cfg.tomo_cxxscale * TOMOSCALE
+                    for w, g in zip(wt, s.xmaps)])
+    s2 = dataclasses.replace(s, wt=wt, l2c=l2c)
+    s2 = dataclasses.replace(s2, fdpcg=fdpcg_setup.fdpcg_prepare(s2))  # host tables of the new weights
+    o2 = TomoOracle(s2)
+    rng = np.random.default_rng(10)
+    x = rng.standard_normal((2, s.nx_total))
+    g = rng.standard_normal((2, s.ngrad)) * 1e-6
+    try:
+        R.update_cn2(l2c)  # no tables: rebuilt on the device
+        z = R.apply_fdpcg(x)
+        R.reset()
+        xs, _ = R.tomo(g)
+        for b in range(2):
+            assert rel(z[b], o2.fdpcg_precond(x[b])) < OP_TOL
+            want, _ = tomo_solve(o2, g[b])
+            assert rel(xs[b], want) < SOLVE_TOL
+    finally:
+        R.update_cn2(np.asarray(s.l2c, dtype=np.float64))  # device rebuild at the setup weights
+        R.reset()
+    z0 = R.apply_fdpcg(x)
+    for b in range(2):
+        assert rel(z0[b], o.fdpcg_precond(x[b])) < OP_TOL
+
+
 def test_batch_instances_are_independent(setup):
     s, R, o = setup
     from maos_b200.recon import Reconstructor
