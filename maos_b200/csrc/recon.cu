@@ -127,6 +127,8 @@ struct Recon {
     std::vector<double> fd_l2c_ref;         // l2c at which fd_mdiag holds invpsd
     std::vector<double> l2c_now;            // l2c last installed
     DevBuf<FdLayer> fd_lay;                 // per layer: FFT geometry and radices
+    FdTab fdtab{};                          // the same, by value for kernel parameters
+    WfsTab wfstab{};                        // wfs_h by value for kernel parameters
     DevBuf<cplx> fd_tw;                     // twiddle tables exp(-2 pi i k/n)
     int fd_bufn = 0;                        // complex elements per FFT shared buffer
     size_t fd_smem = 0;
@@ -416,7 +418,7 @@ void Recon::pupil_rows(bool from_x, const float *xin, cudaStream_t s) {
                            : (p2 ? (few ? k_pupil_rows<false, 2, 8> : k_pupil_rows<false, 2, 16>)
                                  : (few ? k_pupil_rows<false, 1, 8> : k_pupil_rows<false, 1, 16>));
         launch(kern, dim3(ptiles, w1 - w0, nb), dim3(kThreads), pupil_smem, s, 
-            xin, grad.p, tt.p, tbuf.p, hx.fwd.p, lay.p, wfs.p, pad(), w0, nps, nwfs, nxp, nyp, nxtot, ngrad, tw,
+            xin, grad.p, tt.p, tbuf.p, hx.fwd.p, laytab, wfstab, pad(), w0, nps, nwfs, nxp, nyp, nxtot, ngrad, tw,
             ncols, prows, from_x ? 0 : 1, act());
         w0 = w1;
     }
@@ -521,6 +523,8 @@ void Recon::build_wfs_tables(const mb_recon_desc *d) {
         set_neai(w, W.neai, W.ptt);
     }
     wfs.upload(wfs_h);
+    MB_REQUIRE(nwfs <= kMaxWfs, "at most %d WFS", kMaxWfs);
+    for (int w = 0; w < nwfs; w++) wfstab.w[w] = wfs_h[w];
 }
 
 void Recon::set_neai(int w, const double *ne, const double *pt) {
@@ -759,6 +763,7 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
         twn = std::max(twn, F.nx + F.ny);
     }
     fd_lay.upload(fl);
+    for (int l = 0; l < nps; l++) fdtab.l[l] = fl[l];
     fd_tw.upload(tw);
     fd_smem = (2 * (size_t)fd_bufn + twn) * sizeof(cplx);
     MB_REQUIRE(fd_smem <= 200 * 1024, "fdpcg: layer FFT needs %zu bytes of shared memory", fd_smem);
@@ -906,13 +911,13 @@ void Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k
                      float *xupd, const float *pupd, const float *Apupd) {
     // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT,
     // on the half spectrum as in cuda/fdpcg.cu (fdpcg_mul_block_sync_half)
-    launch(k_fd_fwd, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, rin, spec.p, fd_lay.p, fd_tw.p, nxtot, fd_bufn, xupd,
+    launch(k_fd_fwd, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, rin, spec.p, fdtab, fd_tw.p, nxtot, fd_bufn, xupd,
                                                         pupd, Apupd, xupd ? ab.p : nullptr, act());
     const int per = kThreads / fd_bs;
     launch(k_fd_mul, dim3((fd_nbh + per - 1) / per, (nb + kFdInst - 1) / kFdInst), dim3(kThreads), 0, s, 
         spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh, fd_bs, nb, act());
     CgScal S = in_cg ? scal() : CgScal{};
-    launch(k_fd_inv, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, spec2.p, rin, zout, rzp, fd_lay.p, fd_tw.p, nxtot, fd_bufn,
+    launch(k_fd_inv, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, spec2.p, rin, zout, rzp, fdtab, fd_tw.p, nxtot, fd_bufn,
                                                         S, k, init, act());
 }
 
@@ -1395,6 +1400,7 @@ int mb_update_recon_nea(mb_recon *h, int iwfs, const double *neai, const double 
     MB_CUDA_TRY(cudaStreamSynchronize(h->R.stream));
     h->R.set_neai(iwfs, neai, ptt);
     h->R.wfs.upload(h->R.wfs_h);
+    for (int w = 0; w < h->R.nwfs; w++) h->R.wfstab.w[w] = h->R.wfs_h[w];
     h->R.capture_graph();
     MB_API_END
 }

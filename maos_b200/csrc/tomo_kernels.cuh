@@ -61,6 +61,11 @@ constexpr int kMaxLayers = 16;  // most reconstructed layers (the Hx gather unro
 struct LayerTab {
     LayerDev l[kMaxLayers];
 };
+// The WFS descriptors by value, for the same reason.
+constexpr int kMaxWfs = 16;
+struct WfsTab {
+    WfsDev w[kMaxWfs];
+};
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -406,8 +411,8 @@ __host__ __device__ constexpr int pupil_rows_smem_floats(int rows, int nxp, int 
 template <bool FROM_X, int POS, int ML>
 __global__ void __launch_bounds__(kThreads, 4)
 k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const float *__restrict__ tt,
-             float *__restrict__ t, const AxisW *__restrict__ tab, const LayerDev *__restrict__ lay,
-             const WfsDev *__restrict__ wfs, PadIndex pi, int wbase, int nps, int nwfs, int nxp, int nyp,
+             float *__restrict__ t, const AxisW *__restrict__ tab, const __grid_constant__ LayerTab lt,
+             const __grid_constant__ WfsTab wt, PadIndex pi, int wbase, int nps, int nwfs, int nxp, int nyp,
              long nxtot, long ngrad, long tw, int ncols, int rows, int do_tt,
              const int *__restrict__ act) {
     pdl_enter();
@@ -418,7 +423,7 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
     __shared__ int s_lnx[kMaxLayers], s_tcol[kMaxLayers + 1];
     __shared__ long s_loff[kMaxLayers];
     __shared__ int4 s_fp[kMaxLayers];
-    const WfsDev W = wfs[w];
+    const WfsDev &W = wt.w[w];
     const int r0 = blockIdx.x * rows;
     const int r1 = min(nyp, r0 + rows);      // output pupil rows [r0, r1)
     const int ca = max(0, r0 - POS);         // subaperture corner rows [ca, cb)
@@ -440,7 +445,7 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
     // subaperture map of rows [ca, cb) and, for Hx, the axis tables: all
     // copies in flight together
     if (threadIdx.x < nps) {
-        const LayerDev L = lay[threadIdx.x];
+        const LayerDev &L = lt.l[threadIdx.x];
         s_lnx[threadIdx.x] = L.nx;
         s_loff[threadIdx.x] = L.off;
         s_tcol[threadIdx.x] = L.tcol;
@@ -914,6 +919,9 @@ struct FdLayer {
     signed char rx[8], ry[8];
     int px, py;          // two-pass factor pair (index into kFftPairs) along x and y, -1: stages
 };
+struct FdTab {  // per layer, by value (kernel parameter space)
+    FdLayer l[kMaxLayers];
+};
 
 // Lengths the two-pass FFT handles, as n = N1 * N2 (both passes' DFTs held
 // in registers).  The host picks the first pair whose product is n.
@@ -1172,13 +1180,13 @@ constexpr int kFftThreads = 512;  // threads of a layer-FFT CTA
 constexpr int kFdLoads = 5;
 
 __global__ void __launch_bounds__(kFftThreads, 2)
-k_fd_fwd(float *__restrict__ r, cplx *__restrict__ H, const FdLayer *__restrict__ fl, const cplx *__restrict__ tw,
+k_fd_fwd(float *__restrict__ r, cplx *__restrict__ H, const __grid_constant__ FdTab ft, const cplx *__restrict__ tw,
          long nxtot, int bufn, float *__restrict__ xw, const float *__restrict__ pv,
          const float *__restrict__ Apv, const float *__restrict__ ab, const int *__restrict__ act) {
     pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     extern __shared__ cplx fsm[];
-    const FdLayer L = fl[blockIdx.x];
+    const FdLayer &L = ft.l[blockIdx.x];
     const int b = blockIdx.y;
     const int nx = L.nx, ny = L.ny, h = nx / 2 + 1, np2 = ny / 2;
     cplx *A = fsm, *B = fsm + bufn, *twx = fsm + 2 * bufn, *twy = twx + nx;
@@ -1467,13 +1475,13 @@ __global__ void k_fd_fold(const double2 *__restrict__ minv, const int *__restric
 // grid: (nps, nb); shared memory as k_fd_fwd.
 __global__ void __launch_bounds__(kFftThreads, 2)
 k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restrict__ z,
-         double *__restrict__ rz_part, const FdLayer *__restrict__ fl, const cplx *__restrict__ tw, long nxtot,
+         double *__restrict__ rz_part, const __grid_constant__ FdTab ft, const cplx *__restrict__ tw, long nxtot,
          int bufn, CgScal SC, int kit, int init, const int *__restrict__ act) {
     pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     extern __shared__ cplx fsm[];
     __shared__ double sh[32];
-    const FdLayer L = fl[blockIdx.x];
+    const FdLayer &L = ft.l[blockIdx.x];
     const int b = blockIdx.y;
     const int nx = L.nx, ny = L.ny, h = nx / 2 + 1, np2 = ny / 2;
     cplx *A = fsm, *B = fsm + bufn, *twx = fsm + 2 * bufn, *twy = twx + nx;
