@@ -72,6 +72,30 @@ static void launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, c
     count_launches(1);
 }
 
+// A launch in thread-block clusters of `cx` CTAs along x (no PDL).
+template <typename... KArgs, typename... Args>
+static void launch_cluster(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, int cx,
+                           Args &&...args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cx;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+    if (e != cudaSuccess) {
+        set_error("cluster launch: %s", cudaGetErrorString(e));
+        throw CudaError{MB_ECUDA};
+    }
+    count_launches(1);
+}
+
 // Forward tables for (direction d, source grid t) on the device, and their
 // exact transposes as per-axis CSR lists over the source grid (gather form)
 // on the host, from which the padded gather lists of the kernels are built.
@@ -205,9 +229,10 @@ struct Recon {
     void op_hx(const float *xin, cudaStream_t s);
     void op_rhs(const float *g, float *out, cudaStream_t s);
     void op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t s, int k = 0);
-    void op_fdpcg(float *rin, float *zout, double *rz_part, cudaStream_t s, int k = 0, int init = 0,
+    bool op_fdpcg(float *rin, float *zout, double *rz_part, cudaStream_t s, int k = 0, int init = 0,
                   bool in_cg = false, float *xupd = nullptr, const float *pupd = nullptr,
-                  const float *Apupd = nullptr);
+                  const float *Apupd = nullptr, float *pnext = nullptr);
+    bool fd_cluster = false;  // k_fd_inv<true> fits as clusters of nps CTAs
     void enqueue_solve(cudaStream_t s);
     struct CgBufs {
         float *x, *r, *p, *z, *Ap, *rhs;
@@ -215,8 +240,9 @@ struct Recon {
         CgScal S;
     };
     using AmulFn = std::function<void(const float *, float *, double *, int)>;
-    using MmulFn = std::function<void(float *, float *, double *, int, int)>;
-    using XrMmulFn = std::function<void(int)>;
+    // preconditioners return true when they also left p = z + beta p
+    using MmulFn = std::function<bool(float *, float *, double *, int, int)>;
+    using XrMmulFn = std::function<bool(int)>;
     void enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulFn &Amul,
                     const MmulFn &Mmul, cudaStream_t s, const XrMmulFn &XrMmul = XrMmulFn());
     void op_fitR(const float *xin, float *out, cudaStream_t s);
@@ -768,7 +794,29 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
     fd_smem = (2 * (size_t)fd_bufn + twn) * sizeof(cplx);
     MB_REQUIRE(fd_smem <= 200 * 1024, "fdpcg: layer FFT needs %zu bytes of shared memory", fd_smem);
     MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
-    MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
+    MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_inv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
+    MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_inv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_smem));
+    // the CG step's inverse runs as clusters of the nps layer CTAs of an instance when such a cluster fits
+    fd_cluster = false;
+    if (nps <= 16) {
+        if (nps > 8)
+            MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_inv<true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)nps;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(nps, nb);
+        cfg.blockDim = dim3(kFftThreads);
+        cfg.dynamicSmemBytes = fd_smem;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int ncl = 0;
+        fd_cluster = cudaOccupancyMaxActiveClusters(&ncl, k_fd_inv<true>, &cfg) == cudaSuccess && ncl > 0;
+        cudaGetLastError();  // a size the device refuses only means the unclustered path
+        if (const char *e = std::getenv("MAOS_B200_FD_CLUSTER")) fd_cluster = fd_cluster && e[0] != '0';
+    }
 
 }
 
@@ -907,8 +955,8 @@ void Recon::op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t 
     hxt_rows(xin, out, dot_part, 1, k, s);
 }
 
-void Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k, int init, bool in_cg,
-                     float *xupd, const float *pupd, const float *Apupd) {
+bool Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k, int init, bool in_cg,
+                     float *xupd, const float *pupd, const float *Apupd, float *pnext) {
     // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT,
     // on the half spectrum as in cuda/fdpcg.cu (fdpcg_mul_block_sync_half)
     launch(k_fd_fwd, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, rin, spec.p, fdtab, fd_tw.p, nxtot, fd_bufn, xupd,
@@ -917,8 +965,14 @@ void Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k
     launch(k_fd_mul, dim3((fd_nbh + per - 1) / per, (nb + kFdInst - 1) / kFdInst), dim3(kThreads), 0, s, 
         spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh, fd_bs, nb, act());
     CgScal S = in_cg ? scal() : CgScal{};
-    launch(k_fd_inv, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, spec2.p, rin, zout, rzp, fdtab, fd_tw.p, nxtot, fd_bufn,
-                                                        S, k, init, act());
+    if (in_cg && pnext && fd_cluster) {  // the p update inside, clusters of the layer CTAs
+        launch_cluster(k_fd_inv<true>, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, nps, spec2.p, rin, zout, rzp,
+                       fdtab, fd_tw.p, nxtot, fd_bufn, S, k, init, act(), pnext);
+        return true;
+    }
+    launch(k_fd_inv<false>, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, spec2.p, rin, zout, rzp, fdtab, fd_tw.p,
+           nxtot, fd_bufn, S, k, init, act(), (float *)nullptr);
+    return false;
 }
 
 // (Preconditioned) CG with FP64 scalars, the schedule of lib/pcg.c:28 and
@@ -932,24 +986,29 @@ void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulF
     Amul(B.x, B.Ap, nullptr, 0);
     launch(k_cg_init_r, dim3(nblk, nb), dim3(kThreads), 0, s, B.rhs, B.Ap, B.r, B.bb, n, B.S, iters, act());
     float *zp = B.r;
+    bool pdone = false;
     if (Mmul) {
-        Mmul(B.r, B.z, B.rz, 0, 1);
+        pdone = Mmul(B.r, B.z, B.rz, 0, 1);
         zp = B.z;
     } else {
         launch(k_dot_self, dim3(nblk, nb), dim3(kThreads), 0, s, B.r, B.rz, n, B.S, act());  // z aliases r
     }
-    launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n, B.S, 1, act());
+    if (!pdone)
+        launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n, B.S, 1,
+               act());
     for (int k = 0; k < iters; k++) {
         Amul(B.p, B.Ap, B.pap, k);  // its last block leaves alpha_k
         if (XrMmul && k + 1 < iters) {
-            XrMmul(k);  // x, r update and preconditioner; its last block leaves beta_k
+            pdone = XrMmul(k);  // x, r update and preconditioner; beta_k (and p, when it says so)
         } else {
             launch(k_cg_update_xr, dim3(nblk, nb), dim3(kThreads), 0, s, B.x, B.r, B.p, B.Ap, B.rr, n, B.S, k, iters,
                                                               Mmul ? 0 : 1, act());
             if (k + 1 == iters) break;
-            if (Mmul) Mmul(B.r, B.z, B.rz, k, 0);  // its last block leaves beta_k
+            pdone = Mmul ? Mmul(B.r, B.z, B.rz, k, 0) : false;  // beta_k (and p, when it says so)
         }
-        launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n, B.S, 0, act());
+        if (!pdone)
+            launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n, B.S,
+                   0, act());
     }
 }
 
@@ -961,8 +1020,10 @@ void Recon::enqueue_solve(cudaStream_t s) {
     MmulFn M;
     XrMmulFn XM;
     if (precond) {
-        M = [&](float *in, float *out, double *dot, int k, int init) { op_fdpcg(in, out, dot, s, k, init, true); };
-        XM = [&](int k) { op_fdpcg(r.p, z.p, rz_part.p, s, k, 0, true, x.p, p.p, Ap.p); };
+        M = [&](float *in, float *out, double *dot, int k, int init) {
+            return op_fdpcg(in, out, dot, s, k, init, true, nullptr, nullptr, nullptr, p.p);
+        };
+        XM = [&](int k) { return op_fdpcg(r.p, z.p, rz_part.p, s, k, 0, true, x.p, p.p, Ap.p, p.p); };
     }
     enqueue_cg(B, nxtot, nblk_x, maxit, A, M, s, XM);
 }
@@ -1153,10 +1214,12 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
         B * (F * trow + 2 * F * nx) + (double)ypad.n * 8.0,                                // t, p -> Ap
         B * (5 * F * nx),                                              // x,r,p,Ap r/w
         B * (3 * F * nx),                                              // p,z -> p
-        B * (3 * F * nx + 8.0 * nbk * fd_bs + 16.0 * nbk)};           // r (twice), z, M and idx per instance
+        B * ((fd_cluster ? 4 : 3) * F * nx + 8.0 * nbk * fd_bs + 16.0 * nbk)};  // r (twice), z or p r/w, M, idx
     // with the preconditioner, the x/r update of all but the last iteration
-    // runs inside fd_fwd (timed here without it)
-    const int lps[5] = {maxit + 2, maxit + 2, precond ? 1 : maxit, maxit, precond ? maxit : 0};
+    // runs inside fd_fwd (timed here without it), and with the clustered
+    // inverse the p update runs inside fd_inv (timed here with it)
+    const bool pin = precond && fd_cluster;
+    const int lps[5] = {maxit + 2, maxit + 2, precond ? 1 : maxit, pin ? 0 : maxit, precond ? maxit : 0};
     for (int st = 0; st < ns; st++) {
         bytes[st] = by[st];
         launches[st] = lps[st];
@@ -1175,7 +1238,10 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                 case 3:
                     launch(k_cg_update_p, dim3(nblocks((nxtot + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, stream, rhs.p, z.p, nxtot, scal(), 0, act());
                     break;
-                case 4: op_fdpcg(r.p, z.p, rz_part.p, stream); break;
+                case 4:  // as in the CG step (scalars of a scratch iteration; rhs is scratch here)
+                    if (pin) op_fdpcg(r.p, z.p, rz_part.p, stream, 0, 0, true, nullptr, nullptr, nullptr, rhs.p);
+                    else op_fdpcg(r.p, z.p, rz_part.p, stream);
+                    break;
             }
         };
         run_stage();  // warm

@@ -1470,13 +1470,24 @@ __global__ void k_fd_fold(const double2 *__restrict__ minv, const int *__restric
     M[k] = make_float2((float)(0.5 * (a.x + p.x) * s), (float)(0.5 * (a.y - p.y) * s));
 }
 
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 // Inverse: half spectra H -> z (instance-major), plus the r.z partial of this
 // (layer, instance); the last CTA of an instance leaves (r.z)_0 or beta.
 // grid: (nps, nb); shared memory as k_fd_fwd.
+// PU (CG step, launched as clusters of the nps layer CTAs of one instance):
+// the CTAs exchange their r.z partials through distributed shared memory
+// behind a cluster barrier, each forms r.z (same order, same value) and
+// beta, and updates its own layer of p = z + beta p (init: p = z), which
+// replaces the separate p update launch; z is not written.  Rank 0 records
+// the CG scalars as cg_rz_last does.
+template <bool PU>
 __global__ void __launch_bounds__(kFftThreads, 2)
 k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restrict__ z,
          double *__restrict__ rz_part, const __grid_constant__ FdTab ft, const cplx *__restrict__ tw, long nxtot,
-         int bufn, CgScal SC, int kit, int init, const int *__restrict__ act) {
+         int bufn, CgScal SC, int kit, int init, const int *__restrict__ act, float *__restrict__ pv) {
     pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     extern __shared__ cplx fsm[];
@@ -1542,15 +1553,77 @@ k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restr
             if (p < np2) {
                 const cplx q = Zo[p * nx + k];
                 const size_t o0 = base + (size_t)(2 * p) * nx + k, o1 = o0 + nx;
-                z[o0] = q.x;
-                z[o1] = q.y;
+                if (!PU) {
+                    z[o0] = q.x;
+                    z[o1] = q.y;
+                }
                 v += (double)q.x * rv[u][0] + (double)q.y * rv[u][1];
             }
         }
     }
     v = block_sum(v, sh);
-    if (threadIdx.x == 0) rz_part[(size_t)b * gridDim.x + blockIdx.x] = v;
-    if (SC.sc) cg_rz_last(rz_part + (size_t)b * gridDim.x, SC, b, kit, init);
+    if constexpr (!PU) {
+        if (threadIdx.x == 0) rz_part[(size_t)b * gridDim.x + blockIdx.x] = v;
+        if (SC.sc) cg_rz_last(rz_part + (size_t)b * gridDim.x, SC, b, kit, init);
+    } else {
+        __shared__ double s_part, s_be;
+        if (threadIdx.x == 0) s_part = v;
+        cluster_sync_all();  // every rank's partial is in its shared memory
+        if (threadIdx.x < 32) {
+            // lane i reads rank i (the layer order), summed as warp_sum_fresh sums rz_part
+            double t = 0;
+            if (threadIdx.x < (int)gridDim.x) {
+                const unsigned la = (unsigned)__cvta_generic_to_shared(&s_part);
+                unsigned ra;
+                asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(la), "r"((unsigned)threadIdx.x));
+                asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(t) : "r"(ra) : "memory");
+            }
+            t = warp_sum(t);
+            if (threadIdx.x == 0) {
+                const double rz = t;
+                double be = 0;
+                if (!init) {
+                    be = rz / SC.sc[(size_t)b * SC.nsc + kit];
+                    if (!isfinite(be)) be = 0;
+                }
+                s_be = be;
+                if (blockIdx.x == 0) {  // rank 0 keeps the CG scalars
+                    if (init) {
+                        SC.sc[(size_t)b * SC.nsc] = rz;
+                    } else {
+                        SC.ab[2 * b + 1] = (float)be;
+                        SC.sc[(size_t)b * SC.nsc + kit + 1] = rz;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");  // done reading the others
+        const float be = (float)s_be;
+        for (int p0 = x0; x0 < xs && p0 < np2; p0 += kFdLoads * xs) {
+            float pp[kFdLoads][2];
+#pragma unroll
+            for (int u = 0; u < kFdLoads; u++) {
+                const int p = p0 + u * xs;
+                if (p < np2 && !init) {
+                    const size_t o0 = base + (size_t)(2 * p) * nx + k;
+                    pp[u][0] = pv[o0];
+                    pp[u][1] = pv[o0 + nx];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kFdLoads; u++) {
+                const int p = p0 + u * xs;
+                if (p < np2) {
+                    const cplx q = Zo[p * nx + k];
+                    const size_t o0 = base + (size_t)(2 * p) * nx + k;
+                    pv[o0] = init ? q.x : q.x + be * pp[u][0];
+                    pv[o0 + nx] = init ? q.y : q.y + be * pp[u][1];
+                }
+            }
+        }
+        asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");  // no rank leaves while read
+    }
 }
 
 // float <-> double staging helpers for the host-facing API
