@@ -11,10 +11,11 @@
 // matrices, core matrix (r/8, k/8) at ((r/8)*8 + k/8)*128 bytes, row r%8 at
 // 16*(r%8)).  A BF16 tile is 16 KB; an FP8 tile is 8 KB in an order whose
 // 16-byte rows widen to two BF16 core-matrix rows (tc_fp8_off).  The
-// gradients are split once per call by k_gsplit into three BF16 terms
-// g = hi + mid + lo (each the BF16 rounding of what the previous terms left,
-// so the products carry FP32-level accuracy in g; only M's storage type
-// rounds), stored per (batch tile, chunk) as three [N x 64] tiles in the same
+// gradients are split once per call by k_gsplit into two BF16 terms
+// g = hi + lo (lo the BF16 rounding of g - hi), 16 significant bits: each
+// product carries a relative error of at most 2^-17 from g, 500 times below
+// the BF16 storage rounding of M (2^-8) and further below FP8's; they are
+// stored per (batch tile, chunk) as two [N x 64] tiles in the same
 // core-matrix order.  Every pipeline stage is therefore two contiguous bulk
 // copies (cp.async.bulk, completing on an mbarrier by byte count): no tensor
 // map, no per-element address arithmetic, no shared-memory bank conflicts.
@@ -23,7 +24,7 @@
 // tile, with warp roles that meet only on mbarriers:
 //   warp 0, lane 0: copies.  Keeps all S stages in flight; a stage is
 //     refilled as soon as the MMAs that read it completed ("empty").
-//   warp 1, lane 0: MMAs.  Per 64-column chunk, 4 K-steps x 3 terms of
+//   warp 1, lane 0: MMAs.  Per 64-column chunk, 4 K-steps x 2 terms of
 //     tcgen05.mma (M=128, N = batch tile, K=16) into TMEM, committed to the
 //     stage's "empty" barrier (and, FP8, to the widened tile's "free").
 //   warps 2-4 (FP8 only): widen the stage's FP8 tile to BF16 (exact) into one
@@ -47,7 +48,7 @@ constexpr int kTcRows = 128;     // UMMA M
 constexpr int kTcK = 64;         // columns per chunk (4 MMAs of K=16)
 constexpr int kTcThreads = 160;  // copy warp, MMA warp, 3 widening warps (4 epilogue warps)
 constexpr int kTcWiden = 96;     // threads of the widening warps
-constexpr int kTcTerms = 3;      // BF16 terms of the gradients
+constexpr int kTcTerms = 2;      // BF16 terms of the gradients
 constexpr int kTcTileBf16 = kTcRows * kTcK * 2;  // bytes of a BF16 M tile
 constexpr int kTcTileFp8 = kTcRows * kTcK;       // bytes of an FP8 M tile
 
@@ -124,7 +125,7 @@ __device__ __forceinline__ void tc_load_stage(uint32_t bar, uint32_t sa, const v
                  :: "r"(sb), "l"(gb), "r"(bbytes), "r"(bar) : "memory");
 }
 
-// The 12 MMAs of one 64-column chunk: 4 K-steps of 16, 3 gradient terms.
+// The MMAs of one 64-column chunk: 4 K-steps of 16 times kTcTerms gradient terms.
 __device__ __forceinline__ void tc_mma_chunk(uint32_t tmem, uint32_t abase, uint32_t bbase, int term_bytes,
                                              uint32_t idesc, bool first) {
 #pragma unroll
@@ -148,7 +149,7 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
                  : "memory");
 }
 
-// Gradients -> three BF16 terms in per-(batch tile, chunk) core-matrix tiles.
+// Gradients -> kTcTerms BF16 terms in per-(batch tile, chunk) core-matrix tiles.
 // gs: [nz][nch][kTcTerms][N x 64] BF16, zero past nbatch and ngrad.  One
 // thread per 8 columns of one instance; consecutive threads write
 // consecutive 16-byte rows.

@@ -930,7 +930,7 @@ void Recon::build(const mb_recon_desc *d) {
 // operators
 // ---------------------------------------------------------------------------
 void Recon::op_hx(const float *xin, cudaStream_t s) {
-    launch(k_hx, dim3(nblocks(np), nwfs, nb), dim3(kThreads), 0, s, xin, opd.p, hx.fwd.p, lay.p, nps, nwfs,
+    launch(nps <= 8 ? k_hx<8> : k_hx<16>, dim3(nblocks(np), nwfs, nb), dim3(kThreads), 0, s, xin, opd.p, hx.fwd.p, laytab, nps, nwfs,
                                                          nxp, nyp, nxtot, nullptr, nullptr, act());
 }
 
@@ -1030,7 +1030,7 @@ void Recon::enqueue_solve(cudaStream_t s) {
 
 // FitR: sum_f wt_f HA_f^T (W0 - W1 W1^T) Hxp_f x   (recon_utils.c:483, fit.cu:190)
 void Recon::op_fitR(const float *xin, float *out, cudaStream_t s) {
-    launch(k_hx, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, xin, opdf.p, hxp.fwd.p, lay.p, nps, nfit, nfx, nfy,
+    launch(nps <= 8 ? k_hx<8> : k_hx<16>, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, xin, opdf.p, hxp.fwd.p, laytab, nps, nfit, nfx, nfy,
                                                     nxtot, w1v.p, w1_part.p, act());
     launch(k_fit_w, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, opdf.p, opdw.p, w0_rp.p, w0_ci.p, w0_v.p, w1v.p,
                                                        fwt.p, w1_part.p, nblk_f, nf, nfit, act());
@@ -1045,7 +1045,7 @@ void Recon::op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t
         launch(k_lowrank_dot, dim3(nblk_a, nb), dim3(kThreads), 0, s, ain, nwv.p, nw_part.p, nnw, nact, act());
         lr = LowRank{nwv.p, nw_part.p, nnw, nblk_a};
     }
-    launch(k_hx, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, ain, opdf.p, ha.fwd.p, dmlay.p, ndm, nfit, nfx, nfy,
+    launch(ndm <= 8 ? k_hx<8> : k_hx<16>, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, ain, opdf.p, ha.fwd.p, dmtab, ndm, nfit, nfx, nfy,
                                                     nact, w1v.p, w1_part.p, act());
     launch(k_fit_w, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, opdf.p, opdw.p, w0_rp.p, w0_ci.p, w0_v.p, w1v.p,
                                                        fwt.p, w1_part.p, nblk_f, nf, nfit, act());

@@ -147,11 +147,14 @@ __device__ __forceinline__ void pdl_enter() {
 __device__ __forceinline__ bool inactive(const int *act, int b) { return act && __ldg(act + b) == 0; }
 
 // ---------------------------------------------------------------------------
-// Hx: opd[b][w][p] = sum_l bilinear(x_l) at the ray of pupil point p.
+// Hx: opd[b][w][p] = sum_l bilinear(x_l) at the ray of pupil point p.  The
+// layer loop is unrolled to ML (>= nps) so every layer's taps are in flight
+// together; the layer geometry comes by value.
 // grid: (ceil(np/256), nwfs, nb)
 // ---------------------------------------------------------------------------
+template <int ML>
 __global__ void k_hx(const float *__restrict__ x, float *__restrict__ opd,
-                     const AxisW *__restrict__ tab, const LayerDev *__restrict__ lay, int nps,
+                     const AxisW *__restrict__ tab, const __grid_constant__ LayerTab lt, int nps,
                      int nwfs, int nxp, int nyp, long nxtot, const float *__restrict__ w1,
                      double *__restrict__ w1_part, const int *__restrict__ act) {
     pdl_enter();
@@ -164,15 +167,18 @@ __global__ void k_hx(const float *__restrict__ x, float *__restrict__ opd,
     if (p < np) {
         const int ix = p % nxp, iy = p / nxp;
         const float *xb = x + (size_t)b * nxtot;
-        for (int l = 0; l < nps; l++) {
-            const AxisW *t = tab + (size_t)(w * nps + l) * (nxp + nyp);
-            const AxisW tx = t[ix], ty = t[nxp + iy];
-            if (tx.k < 0 || ty.k < 0) continue;
-            const int nx = lay[l].nx;
-            const float *X = xb + lay[l].off + (size_t)ty.k * nx + tx.k;
-            const float a = tx.w0 * X[0] + tx.w1 * X[1];
-            const float c = tx.w0 * X[nx] + tx.w1 * X[nx + 1];
-            acc += ty.w0 * a + ty.w1 * c;
+#pragma unroll
+        for (int l = 0; l < ML; l++) {
+            if (l < nps) {
+                const AxisW *t = tab + (size_t)(w * nps + l) * (nxp + nyp);
+                const AxisW tx = t[ix], ty = t[nxp + iy];
+                const bool ok = tx.k >= 0 && ty.k >= 0;
+                const int nx = lt.l[l].nx;
+                const float *X = xb + lt.l[l].off + (ok ? (size_t)ty.k * nx + tx.k : 0);
+                const float a = tx.w0 * X[0] + tx.w1 * X[1];
+                const float c = tx.w0 * X[nx] + tx.w1 * X[nx + 1];
+                if (ok) acc += ty.w0 * a + ty.w1 * c;
+            }
         }
         opd[((size_t)b * nwfs + w) * np + p] = acc;
     }
