@@ -114,3 +114,28 @@ def build_control_matrix_distributed(sysm, fit, rhs_batch: int = 256, group=None
     cols = column_shard(int(sysm.ngrad), rank, world, rhs_batch)
     local, rep = build_control_matrix(sysm, fit, rhs_batch=rhs_batch, columns=cols, **kw)
     return gather_columns(local, int(sysm.ngrad), group, rhs_batch), rep
+
+
+def main():
+    """python -m maos_b200.mvm_build [--system elt_39m] [--rhs-batch 256]
+    Builds the whole control matrix of a preset on GPU 0 and prints the
+    report (columns, seconds, columns per second, worst tomography residual)
+    as one JSON line."""
+    import argparse
+    import json
+    from . import config, fit_setup, geometry
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--system", default="elt_39m", choices=sorted(config.PRESETS))
+    ap.add_argument("--rhs-batch", type=int, default=256)
+    a = ap.parse_args()
+    sysm = geometry.build_tomo(config.PRESETS[a.system]())
+    fit = fit_setup.build_fit(sysm)
+    M, rep = build_control_matrix(sysm, fit, rhs_batch=a.rhs_batch)
+    rep.update({"system": a.system, "shape": list(M.shape), "ngrad": int(sysm.ngrad),
+                "columns_per_s": rep["columns"] / rep["seconds"],
+                "finite": bool(np.isfinite(M).all())})
+    print(json.dumps(rep))
+
+
+if __name__ == "__main__":
+    main()

@@ -542,3 +542,58 @@ void ref_mkw_amp_get(int *p, int *i, double *x, double *w1) {
     for (long k = 0; k < nnz; k++) { i[k] = last_w0->i[k]; x[k] = last_w0->x[k]; }
     memcpy(w1, last_w1->p, sizeof(double) * last_w1->nx);
 }
+
+/* .bin I/O through the reference's own writer and reader (math/cell.c
+ * writebin, read_by_id), for checking maos_b200.binio. */
+int ref_bin_write_dmat(const char *fn, const double *p, long nx, long ny, const char *header) {
+    dmat *d = dnew(nx, ny);
+    memcpy(d->p, p, sizeof(double) * nx * ny);
+    if (header && header[0]) d->header = strdup(header);
+    writebin(d, "%s", fn);
+    dfree(d);
+    return 0;
+}
+/* a 3 x 1 cell {a, empty, b} */
+int ref_bin_write_dcell3(const char *fn, const double *a, long anx, long any, const double *b, long bnx, long bny) {
+    dcell *c = dcellnew(3, 1);
+    c->p[0] = dnew(anx, any);
+    memcpy(c->p[0]->p, a, sizeof(double) * anx * any);
+    c->p[2] = dnew(bnx, bny);
+    memcpy(c->p[2]->p, b, sizeof(double) * bnx * bny);
+    writebin(c, "%s", fn);
+    dcellfree(c);
+    return 0;
+}
+/* reads a dmat; returns the number of elements copied (-1: too large) */
+long ref_bin_read_dmat(const char *fn, double *p, long cap, long *nx, long *ny, char *hdr, long hcap) {
+    dmat *d = dread("%s", fn);
+    *nx = d->nx;
+    *ny = d->ny;
+    long n = d->nx * d->ny;
+    if (n > cap) { dfree(d); return -1; }
+    memcpy(p, d->p, sizeof(double) * n);
+    if (hdr && hcap > 0) {
+        hdr[0] = 0;
+        if (d->header) { strncpy(hdr, d->header, hcap - 1); hdr[hcap - 1] = 0; }
+    }
+    dfree(d);
+    return n;
+}
+/* reads a dcell; element k's size into nx[k], ny[k] (0 for empty), data concatenated */
+long ref_bin_read_dcell(const char *fn, double *p, long cap, long *ncell, long *nx, long *ny, long kcap) {
+    dcell *c = dcellread("%s", fn);
+    long off = 0;
+    *ncell = c->nx * c->ny;
+    for (long k = 0; k < *ncell && k < kcap; k++) {
+        const dmat *e = c->p[k];
+        nx[k] = e ? e->nx : 0;
+        ny[k] = e ? e->ny : 0;
+        if (e) {
+            if (off + e->nx * e->ny > cap) { dcellfree(c); return -1; }
+            memcpy(p + off, e->p, sizeof(double) * e->nx * e->ny);
+            off += e->nx * e->ny;
+        }
+    }
+    dcellfree(c);
+    return off;
+}

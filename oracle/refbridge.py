@@ -230,6 +230,53 @@ class _Worker:
         return x, y
 
 
+    # .bin files through the reference's writebin / read_by_id (maos_b200.binio checks)
+    def bin_write_dmat(self, fn, a, header=""):
+        a = np.asfortranarray(a, dtype=np.float64)
+        L = self.lib
+        L.ref_bin_write_dmat.argtypes = [ctypes.c_char_p, _D, ctypes.c_long, ctypes.c_long, ctypes.c_char_p]
+        return L.ref_bin_write_dmat(fn.encode(), a.ctypes.data_as(_D), a.shape[0], a.shape[1], header.encode())
+
+    def bin_write_dcell3(self, fn, a, b):
+        a = np.asfortranarray(a, dtype=np.float64)
+        b = np.asfortranarray(b, dtype=np.float64)
+        L = self.lib
+        L.ref_bin_write_dcell3.argtypes = [ctypes.c_char_p, _D, ctypes.c_long, ctypes.c_long, _D, ctypes.c_long,
+                                           ctypes.c_long]
+        return L.ref_bin_write_dcell3(fn.encode(), a.ctypes.data_as(_D), a.shape[0], a.shape[1],
+                                      b.ctypes.data_as(_D), b.shape[0], b.shape[1])
+
+    def bin_read_dmat(self, fn, cap=1 << 20):
+        L = self.lib
+        L.ref_bin_read_dmat.restype = ctypes.c_long
+        buf = np.empty(cap)
+        nx, ny = ctypes.c_long(), ctypes.c_long()
+        hdr = ctypes.create_string_buffer(4096)
+        n = L.ref_bin_read_dmat(fn.encode(), buf.ctypes.data_as(_D), ctypes.c_long(cap), ctypes.byref(nx),
+                                ctypes.byref(ny), hdr, ctypes.c_long(4096))
+        if n < 0:
+            raise ValueError("array larger than the buffer")
+        return buf[:n].reshape((nx.value, ny.value), order="F").copy(), hdr.value.decode()
+
+    def bin_read_dcell(self, fn, cap=1 << 20, kcap=64):
+        L = self.lib
+        L.ref_bin_read_dcell.restype = ctypes.c_long
+        buf = np.empty(cap)
+        nx = (ctypes.c_long * kcap)()
+        ny = (ctypes.c_long * kcap)()
+        nc = ctypes.c_long()
+        n = L.ref_bin_read_dcell(fn.encode(), buf.ctypes.data_as(_D), ctypes.c_long(cap), ctypes.byref(nc), nx, ny,
+                                 ctypes.c_long(kcap))
+        if n < 0:
+            raise ValueError("cell larger than the buffer")
+        out, off = [], 0
+        for k in range(nc.value):
+            m = nx[k] * ny[k]
+            out.append(buf[off:off + m].reshape((nx[k], ny[k]), order="F").copy() if m else None)
+            off += m
+        return out
+
+
 def _serve(conn, nthread, home):
     # The reference formats $HOME/.aos/... into a 64-byte buffer
     # (math/fft.c fnwisdom); run from inside the home folder with HOME="."
