@@ -205,6 +205,24 @@ int mb_recon_serve_step(mb_recon *r, const int *active, const float *grad, float
  * 4, 8, 16 rows, -1 where a blocking does not fit. */
 int mb_autotune(mb_recon *r, int reps, int *rows, float *ms);
 
+/* Servo filter on the device (no GPU counterpart in the reference; the CPU
+ * code is lib/servo.c servo_new / servo_filter / servo_reset, used by
+ * maos/filter.c filter_dm): the integrator that turns the per-step DM
+ * command errors into DM commands, for n values (e.g. nbatch instances x
+ * nact actuators) in FP64 on the device.  ap: the integrator history
+ * coefficients (NULL: {1}); al: extra latency in steps; ep (column-major
+ * ep_nx x ep_ny): ep_nx 1 = type I gain (ep_ny 1, or one per mode with
+ * n a multiple of ep_ny), 2 = PID (2 x 1), 3 = type II (gain, a, T per
+ * column); dt: the loop period.  mb_servo_filter takes one step: d_merr
+ * (device, n doubles) in, d_cmd (device, n doubles) = the new commands
+ * (mint[0]) out, on `stream`. */
+typedef struct mb_servo mb_servo;
+int mb_servo_create(long n, const double *ap, int nap, int al, const double *ep, int ep_nx, int ep_ny, double dt,
+                    mb_servo **out);
+int mb_servo_filter(mb_servo *s, const double *d_merr, double *d_cmd, void *stream);
+int mb_servo_reset(mb_servo *s);
+void mb_servo_free(mb_servo *s);
+
 /* Sizes of the bound geometry. */
 long mb_ngrad(const mb_recon *r);
 long mb_nxtot(const mb_recon *r);

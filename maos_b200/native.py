@@ -100,6 +100,11 @@ SIGNATURES = {
     "mb_mvm_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mb_mvm_apply_noalloc": (C.c_int, [C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_void_p, C.c_void_p,
                                        C.c_int, C.c_void_p]),
+    "mb_servo_create": (C.c_int, [C.c_long, _D, C.c_int, C.c_int, _D, C.c_int, C.c_int, C.c_double,
+                                  C.POINTER(C.c_void_p)]),
+    "mb_servo_filter": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mb_servo_reset": (C.c_int, [C.c_void_p]),
+    "mb_servo_free": (None, [C.c_void_p]),
     "mb_error_string": (C.c_char_p, [C.c_int]),
     "mb_last_error_message": (C.c_char_p, []),
     "mb_version": (C.c_int, []),

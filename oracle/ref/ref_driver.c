@@ -25,6 +25,7 @@
 #include "lib/accphi.h"
 #include "lib/mkh.h"
 #include "lib/mkw.h"
+#include "lib/servo.h"
 
 typedef struct {
     int nwfs, nps, nthread;
@@ -597,3 +598,33 @@ long ref_bin_read_dcell(const char *fn, double *p, long cap, long *ncell, long *
     dcellfree(c);
     return off;
 }
+
+/* servo_new / servo_filter (lib/servo.c) on n command values in one cell;
+ * ep column-major ep_nx x ep_ny; the command after each step is mint[0]. */
+void *ref_servo_new(long n, const double *ap, int nap, int al, double dt, const double *ep, int ep_nx, int ep_ny) {
+    dmat *apm = NULL;
+    if (nap > 0) {
+        apm = dnew(nap, 1);
+        memcpy(apm->p, ap, sizeof(double) * nap);
+    }
+    dmat *epm = dnew(ep_nx, ep_ny);
+    memcpy(epm->p, ep, sizeof(double) * ep_nx * ep_ny);
+    SERVO_T *st = servo_new(NULL, apm, al, dt, epm);
+    dfree(apm);
+    dfree(epm);
+    (void)n;
+    return st;
+}
+int ref_servo_filter(void *h, const double *merr, long n, double *cmd) {
+    SERVO_T *st = (SERVO_T *)h;
+    dcell *m = dcellnew(1, 1);
+    m->p[0] = dnew(n, 1);
+    memcpy(m->p[0]->p, merr, sizeof(double) * n);
+    int up = servo_filter(st, m);
+    dcellfree(m);
+    const dcell *c = st->mint->p[0];
+    if (c && c->p[0]) memcpy(cmd, c->p[0]->p, sizeof(double) * n);
+    else memset(cmd, 0, sizeof(double) * n);
+    return up;
+}
+void ref_servo_free(void *h) { servo_free((SERVO_T *)h); }

@@ -277,6 +277,28 @@ class _Worker:
         return out
 
 
+    # servo_new / servo_filter (lib/servo.c): commands after each of the given errors
+    def servo_run(self, merrs, ap, al, dt, ep):
+        L = self.lib
+        L.ref_servo_new.restype = ctypes.c_void_p
+        L.ref_servo_new.argtypes = [ctypes.c_long, _D, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int,
+                                    ctypes.c_int]
+        L.ref_servo_filter.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D]
+        L.ref_servo_free.argtypes = [ctypes.c_void_p]
+        merrs = np.ascontiguousarray(merrs, dtype=np.float64)
+        nstep, n = merrs.shape
+        apv = np.ascontiguousarray(ap if ap is not None else np.zeros(1), dtype=np.float64)
+        epm = np.asfortranarray(ep, dtype=np.float64)
+        h = L.ref_servo_new(n, apv.ctypes.data_as(_D), 0 if ap is None else len(apv), al, dt, epm.ctypes.data_as(_D),
+                            epm.shape[0], epm.shape[1])
+        out = np.empty((nstep, n))
+        for k in range(nstep):
+            row = np.ascontiguousarray(merrs[k])
+            L.ref_servo_filter(ctypes.c_void_p(h), row.ctypes.data_as(_D), n, out[k].ctypes.data_as(_D))
+        L.ref_servo_free(ctypes.c_void_p(h))
+        return out
+
+
 def _serve(conn, nthread, home):
     # The reference formats $HOME/.aos/... into a 64-byte buffer
     # (math/fft.c fnwisdom); run from inside the home folder with HOME="."
