@@ -223,6 +223,61 @@ int mb_servo_filter(mb_servo *s, const double *d_merr, double *d_cmd, void *stre
 int mb_servo_reset(mb_servo *s);
 void mb_servo_free(mb_servo *s);
 
+/* ---- Geometric Shack-Hartmann WFS (the simulation side upstream of mb_tomo) ----
+ * Replaces the geometric branch of cuda/gpu.h gpu_wfsgrad_queue
+ * (cuda/wfsgrad.cu gpu_wfsgrad_iwfs with powfs.gtype_sim = 0: the OPD of the
+ * atmosphere, cuda/accphi.cu:508 gpu_atm2loc, minus the DMs, :556
+ * gpu_dm2loc, then GS0 * OPD and add_geom_noise_do, cuda/wfsgrad.cu:47),
+ * with the screens of cuda/gpu.h gpu_atm2gpu and the DM commands of
+ * gpu_dmreal2gpu given as arguments.
+ *
+ * Each WFS's OPD points lie on a fine square grid (spacing dx, grid index
+ * (0, 0) at (gox, goy)); subaperture j's nxsa x nxsa points start at grid
+ * index (sa_ix, sa_iy), and its average-gradient stencil (the rows of the
+ * reference's GS0 = mkg(loc, loc, amp, saloc, 1, 0, 0, 1),
+ * maos/setup_powfs.c:565) is stencils[stencil_off[sa_stencil[j]] ...]: the
+ * x weights then the y weights of the (nxsa+2)^2 grid points from
+ * (sa_ix-1, sa_iy-1), row-major.  Per-subaperture arrays are concatenated
+ * over WFS.  nea (may be NULL): per WFS [3][nsa] sqrt-NEA xx, yy, xy (rad).
+ * Atmosphere layer l: an atm_nx x atm_ny map (x fastest) of spacing atm_dx,
+ * origin (atm_ox, atm_oy), height atm_ht, wind (atm_vx, atm_vy) m/s, seen
+ * with wrap-around.  DM m: a dm_nx x dm_ny actuator map (the commands of one
+ * instance are the DM maps concatenated), no wrap-around.  nbatch
+ * instances each have their own atmosphere and DM commands. */
+typedef struct {
+    int nwfs;
+    const int *nsa, *nxsa;
+    const double *dx, *gox, *goy;
+    const double *thetax, *thetay, *hs;    /* rad, rad, m (inf: natural guide star) */
+    const int *sa_ix, *sa_iy, *sa_stencil;
+    int nstencil;
+    const long *stencil_off;
+    const double *stencils;
+    long stencil_len;
+    const double *nea;
+    int natm;
+    const int *atm_nx, *atm_ny;
+    const double *atm_dx, *atm_ox, *atm_oy, *atm_ht, *atm_vx, *atm_vy;
+    int ndm;
+    const int *dm_nx, *dm_ny;
+    const double *dm_dx, *dm_ox, *dm_oy, *dm_ht;
+    double dt;                              /* sim.dt: the atmosphere moves v dt per step */
+    int nbatch;
+} mb_geom_wfs_desc;
+typedef struct mb_geom_wfs mb_geom_wfs;
+int mb_geom_wfs_create(const mb_geom_wfs_desc *d, mb_geom_wfs **out);
+/* Upload one atmosphere layer of one instance (host FP64, stored FP32). */
+int mb_geom_wfs_set_atm(mb_geom_wfs *w, int inst, int layer, const double *screen);
+/* Gradients of step isim (atmosphere shifted by v dt isim): d_dm (device
+ * FP32 [nbatch][nact], NULL: open loop) is subtracted; d_grad (device FP32
+ * [nbatch][ngrad], each WFS x then y) is written; seed != 0 adds the noise,
+ * drawn from (seed, subaperture, WFS, isim, instance). */
+int mb_geom_wfs_grad(mb_geom_wfs *w, long isim, const float *d_dm, float *d_grad, unsigned long long seed,
+                     void *stream);
+long mb_geom_wfs_ngrad(const mb_geom_wfs *w);
+long mb_geom_wfs_nact(const mb_geom_wfs *w);
+void mb_geom_wfs_free(mb_geom_wfs *w);
+
 /* Sizes of the bound geometry. */
 long mb_ngrad(const mb_recon *r);
 long mb_nxtot(const mb_recon *r);

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libmaosb200.so")
-SOURCES = ["csrc/recon.cu", "csrc/mvm.cu", "csrc/servo.cu"]
+SOURCES = ["csrc/recon.cu", "csrc/mvm.cu", "csrc/servo.cu", "csrc/wfs.cu"]
 HEADERS = ["csrc/common.cuh", "csrc/tomo_kernels.cuh", "csrc/mvm_tc.cuh", "../include/maos_b200.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]

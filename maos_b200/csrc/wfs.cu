@@ -1,0 +1,400 @@
+// Geometric Shack-Hartmann WFS on the device: gradients of the atmosphere
+// seen through the DMs, upstream of the reconstruction (the geometric branch
+// of cuda/wfsgrad.cu gpu_wfsgrad_iwfs with gtype_sim = 0, the reference's
+// default for Shack-Hartmann WFS):
+//
+//   OPD(p)  = sum_atm bilinear_wrap(layer, p) - sum_dm bilinear(dm, p)
+//             (cuda/accphi.cu:508 gpu_atm2loc, :556 gpu_dm2loc; the point's
+//             position on a map at height h: p (1 - h/hs) + h theta - v dt isim)
+//   g       = GS0 OPD                       (cuda/wfsgrad.cu:458 cuspmul)
+//   g      += noise                          (cuda/wfsgrad.cu:47 add_geom_noise_do)
+//
+// Instead of writing the OPD of every WFS point to memory and running a
+// sparse product over it, one warp computes one subaperture: the OPD of the
+// (nxsa+2)^2 fine-grid points its average-gradient stencil touches stays in
+// registers (kGeomChunk points per lane at a time), each map is interpolated straight
+// from its layer (read through L1; the layers of a 30 m system are a few MB
+// and stay in L2), and the two stencil dot products are reduced with warp
+// shuffles.  Stencils are shared by all subapertures with the same amplitude
+// neighbourhood.  The noise is two standard normals per subaperture from a
+// counter-based generator (Philox4x32-10, Salmon et al. 2011) keyed by the
+// seed and counted by (subaperture, WFS, step, instance), so any step of any
+// instance can be drawn again.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mb {
+
+constexpr int kGeomMaxWfs = 16;
+constexpr int kGeomMaxScr = 16;   // atmosphere layers + DMs
+constexpr int kGeomWarps = 8;     // subapertures per CTA
+constexpr int kGeomMaxW = 36;     // window side (nxsa + 2)
+constexpr int kGeomChunk = 13;   // window points per lane per pass
+
+struct GeomScr {
+    const float *p;    // [ny][nx], x fastest
+    long inst_stride;  // floats between instances (0: shared)
+    int nx, ny;
+    float alpha;
+    int wrap;
+};
+struct GeomWfsT {
+    int nsa, nxsa, sa_off;
+    long g_off;
+};
+struct GeomCoef {  // screen index = fine-grid index * s + b, this step
+    double sx, bx, sy, by;
+};
+struct GeomTab {
+    int nwfs, nscr;
+    GeomWfsT w[kGeomMaxWfs];
+    GeomScr s[kGeomMaxScr];
+    GeomCoef c[kGeomMaxWfs][kGeomMaxScr];
+};
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        const unsigned lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+        const unsigned lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// grid: (ceil(max nsa / kGeomWarps), nwfs, nbatch); block: kGeomWarps warps.
+// sa_ix/sa_iy: fine-grid index of each subaperture's first point; sa_st its
+// stencil; st_off the offset of each stencil ([2][W*W] floats) in st; nea
+// per WFS [3][nsa] (sqrt-NEA xx, yy, xy) at 3*sa_off.
+__global__ void __launch_bounds__(kGeomWarps * 32)
+k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, const int *__restrict__ sa_iy,
+           const int *__restrict__ sa_st, const float *__restrict__ st, const long *__restrict__ st_off,
+           const float *__restrict__ nea, float *__restrict__ grad, long grad_stride, long isim,
+           unsigned long long seed) {
+    __shared__ int4 sbase[kGeomWarps][kGeomMaxScr];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int iw = blockIdx.y, inst = blockIdx.z;
+    const GeomWfsT &W = t.w[iw];
+    const int isa = blockIdx.x * kGeomWarps + wid;
+    if (isa >= W.nsa) return;  // the whole warp: no block-wide barrier below
+    const int gi = W.sa_off + isa;
+    const int wn = W.nxsa + 2, npts = wn * wn;
+    const int gx0 = sa_ix[gi] - 1, gy0 = sa_iy[gi] - 1;
+    // each map's position of the window's first point: integer part (wrapped
+    // for the atmosphere) and fraction
+    if (lane < t.nscr) {
+        const GeomCoef c = t.c[iw][lane];
+        const GeomScr &S = t.s[lane];
+        const double u = fma((double)gx0, c.sx, c.bx), v = fma((double)gy0, c.sy, c.by);
+        const double fu = floor(u), fv = floor(v);
+        long long iu = (long long)fmin(fmax(fu, -1e9), 1e9), iv = (long long)fmin(fmax(fv, -1e9), 1e9);
+        if (S.wrap) {
+            iu %= S.nx;
+            if (iu < 0) iu += S.nx;
+            iv %= S.ny;
+            if (iv < 0) iv += S.ny;
+        }
+        sbase[wid][lane] = make_int4((int)iu, (int)iv, __float_as_int((float)(u - fu)), __float_as_int((float)(v - fv)));
+    }
+    __syncwarp();
+    const float inv_wn = 1.0f / (float)wn;
+    const float *__restrict__ w = st + st_off[sa_st[gi]];
+    float gx = 0.f, gy = 0.f;
+    // the window in chunks of kGeomChunk points per lane (OPD in registers)
+    for (int k0 = 0; k0 < npts; k0 += 32 * kGeomChunk) {
+        float opd[kGeomChunk];
+#pragma unroll
+        for (int j = 0; j < kGeomChunk; j++) opd[j] = 0.f;
+        for (int s = 0; s < t.nscr; s++) {
+            const GeomScr S = t.s[s];
+            const int4 b = sbase[wid][s];
+            const float sxf = (float)t.c[iw][s].sx, syf = (float)t.c[iw][s].sy;
+            const float fu0 = __int_as_float(b.z), fv0 = __int_as_float(b.w);
+            const float *__restrict__ P = S.p + (long)inst * S.inst_stride;
+#pragma unroll
+            for (int j = 0; j < kGeomChunk; j++) {
+                const int k = k0 + lane + 32 * j;
+                if (k < npts) {
+                    const int r = (int)(((float)k + 0.5f) * inv_wn), cc = k - r * wn;
+                    const float uf = fmaf((float)cc, sxf, fu0), vf = fmaf((float)r, syf, fv0);
+                    const float flu = floorf(uf), flv = floorf(vf);
+                    int iu = b.x + (int)flu, iv = b.y + (int)flv;
+                    const float ax = uf - flu, ay = vf - flv;
+                    if (S.wrap) {
+                        iu += iu < 0 ? S.nx : (iu >= S.nx ? -S.nx : 0);
+                        iv += iv < 0 ? S.ny : (iv >= S.ny ? -S.ny : 0);
+                    } else if (iu < 0 || iu >= S.nx || iv < 0 || iv >= S.ny) {
+                        continue;  // off the map: no contribution (prop_grid without wrap)
+                    }
+                    const int iu1 = iu == S.nx - 1 ? 0 : iu + 1;
+                    const long r0 = (long)iv * S.nx, r1 = (long)(iv == S.ny - 1 ? 0 : iv + 1) * S.nx;
+                    const float m00 = __ldg(P + r0 + iu), m10 = __ldg(P + r0 + iu1);
+                    const float m01 = __ldg(P + r1 + iu), m11 = __ldg(P + r1 + iu1);
+                    opd[j] = fmaf(S.alpha, fmaf(fmaf(m10 - m00, ax, m00), 1.f - ay, fmaf(m11 - m01, ax, m01) * ay),
+                                  opd[j]);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kGeomChunk; j++) {
+            const int k = k0 + lane + 32 * j;
+            if (k < npts) {
+                gx = fmaf(__ldg(w + k), opd[j], gx);
+                gy = fmaf(__ldg(w + npts + k), opd[j], gy);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        gx += __shfl_xor_sync(0xffffffffu, gx, o);
+        gy += __shfl_xor_sync(0xffffffffu, gy, o);
+    }
+    if (lane == 0) {
+        if (seed) {
+            const uint4 o = philox4x32_10(make_uint4((unsigned)isa, (unsigned)iw, (unsigned)isim, (unsigned)inst),
+                                          make_uint2((unsigned)seed, (unsigned)(seed >> 32)));
+            const double u1 = ((double)o.x + 1.0) * 0x1p-32, u2 = (double)o.y * 0x1p-32;
+            const double rr = sqrt(-2.0 * log(u1));
+            double sn, cs;
+            sincospi(2.0 * u2, &sn, &cs);
+            const float n1 = (float)(rr * cs), n2 = (float)(rr * sn);
+            const float *ne = nea + 3L * W.sa_off;
+            gx = fmaf(n1, ne[isa], gx);
+            gy = fmaf(n2, ne[W.nsa + isa], fmaf(n1, ne[2 * W.nsa + isa], gy));
+        }
+        float *g = grad + (long)inst * grad_stride + W.g_off;
+        g[isa] = gx;
+        g[W.nsa + isa] = gy;
+    }
+}
+
+struct GeomWfsHost {
+    int nwfs = 0, natm = 0, ndm = 0, nbatch = 1;
+    long ngrad = 0, nact = 0, atm_stride = 0;
+    int max_nsa = 0;
+    double dt = 0;
+    std::vector<int> nsa, nxsa;
+    std::vector<double> dx, gox, goy, thetax, thetay, hs;
+    std::vector<int> anx, any;
+    std::vector<double> adx, aox, aoy, aht, avx, avy;
+    std::vector<long> aoff;  // layer offsets within one instance
+    std::vector<int> dnx, dny;
+    std::vector<double> ddx, dox, doy, dht;
+    std::vector<long> doff;  // DM offsets within one instance's commands
+    DevBuf<int> sa_ix, sa_iy, sa_st;
+    DevBuf<float> st, nea, atm;
+    DevBuf<long> st_off;
+    bool have_nea = false;
+};
+
+}  // namespace mb
+
+struct mb_geom_wfs {
+    mb::GeomWfsHost H;
+};
+
+extern "C" {
+
+int mb_geom_wfs_create(const mb_geom_wfs_desc *d, mb_geom_wfs **out) {
+    using namespace mb;
+    if (!out || !d || d->nwfs < 1 || d->nwfs > kGeomMaxWfs || d->natm < 0 || d->ndm < 0 ||
+        d->natm + d->ndm > kGeomMaxScr || d->nbatch < 1 || !d->nsa || !d->nxsa || !d->dx || !d->gox || !d->goy ||
+        !d->thetax || !d->thetay || !d->hs || !d->sa_ix || !d->sa_iy || !d->sa_stencil || d->nstencil < 1 ||
+        !d->stencil_off || !d->stencils || d->stencil_len < 1 ||
+        (d->natm && (!d->atm_nx || !d->atm_ny || !d->atm_dx || !d->atm_ox || !d->atm_oy || !d->atm_ht ||
+                     !d->atm_vx || !d->atm_vy)) ||
+        (d->ndm && (!d->dm_nx || !d->dm_ny || !d->dm_dx || !d->dm_ox || !d->dm_oy || !d->dm_ht))) {
+        set_error("mb_geom_wfs_create: invalid descriptor");
+        return MB_EINVAL;
+    }
+    *out = nullptr;
+    mb_geom_wfs *h = new (std::nothrow) mb_geom_wfs();
+    if (!h) return MB_ENOMEM;
+    try {
+        GeomWfsHost &H = h->H;
+        H.nwfs = d->nwfs;
+        H.natm = d->natm;
+        H.ndm = d->ndm;
+        H.nbatch = d->nbatch;
+        H.dt = d->dt;
+        long nsa_tot = 0;
+        for (int i = 0; i < d->nwfs; i++) {
+            if (d->nsa[i] < 1 || d->nxsa[i] < 1 || d->nxsa[i] + 2 > kGeomMaxW || !(d->dx[i] > 0)) {
+                set_error("mb_geom_wfs_create: WFS %d: nsa %d, nxsa %d (window at most %d points across)", i,
+                          d->nsa[i], d->nxsa[i], kGeomMaxW);
+                throw InvalidArg{MB_EINVAL};
+            }
+            H.nsa.push_back(d->nsa[i]);
+            H.nxsa.push_back(d->nxsa[i]);
+            H.dx.push_back(d->dx[i]);
+            H.gox.push_back(d->gox[i]);
+            H.goy.push_back(d->goy[i]);
+            H.thetax.push_back(d->thetax[i]);
+            H.thetay.push_back(d->thetay[i]);
+            H.hs.push_back(d->hs[i]);
+            nsa_tot += d->nsa[i];
+            H.ngrad += 2L * d->nsa[i];
+            if (d->nsa[i] > H.max_nsa) H.max_nsa = d->nsa[i];
+        }
+        std::vector<int> ix(d->sa_ix, d->sa_ix + nsa_tot), iy(d->sa_iy, d->sa_iy + nsa_tot),
+            sid(d->sa_stencil, d->sa_stencil + nsa_tot);
+        std::vector<long> soff(d->stencil_off, d->stencil_off + d->nstencil);
+        // every subaperture's stencil must be one of its WFS's size and inside the table
+        long k = 0;
+        for (int i = 0; i < d->nwfs; i++) {
+            const long len = 2L * (d->nxsa[i] + 2) * (d->nxsa[i] + 2);
+            for (int j = 0; j < d->nsa[i]; j++, k++) {
+                if (sid[k] < 0 || sid[k] >= d->nstencil || soff[sid[k]] < 0 || soff[sid[k]] + len > d->stencil_len ||
+                    ix[k] < 1 || iy[k] < 1) {
+                    set_error("mb_geom_wfs_create: subaperture %d of WFS %d: stencil %d or grid index out of range",
+                              j, i, sid[k]);
+                    throw InvalidArg{MB_EINVAL};
+                }
+            }
+        }
+        H.sa_ix.upload(ix);
+        H.sa_iy.upload(iy);
+        H.sa_st.upload(sid);
+        H.st_off.upload(soff);
+        std::vector<float> stf(d->stencils, d->stencils + d->stencil_len);
+        H.st.upload(stf);
+        if (d->nea) {
+            std::vector<float> nf(d->nea, d->nea + 3 * nsa_tot);
+            H.nea.upload(nf);
+            H.have_nea = true;
+        }
+        for (int l = 0; l < d->natm; l++) {
+            if (d->atm_nx[l] < 2 || d->atm_ny[l] < 2 || !(d->atm_dx[l] > 0)) {
+                set_error("mb_geom_wfs_create: atmosphere layer %d: %d x %d", l, d->atm_nx[l], d->atm_ny[l]);
+                throw InvalidArg{MB_EINVAL};
+            }
+            // the wrap-around of a window needs the window to be smaller than the layer
+            for (int i = 0; i < d->nwfs; i++) {
+                const double sc = std::isfinite(d->hs[i]) ? 1.0 - d->atm_ht[l] / d->hs[i] : 1.0;
+                const double ext = (d->nxsa[i] + 2) * d->dx[i] * std::fabs(sc) / d->atm_dx[l] + 2;
+                if (ext >= d->atm_nx[l] || ext >= d->atm_ny[l]) {
+                    set_error("mb_geom_wfs_create: layer %d smaller than a subaperture window", l);
+                    throw InvalidArg{MB_EINVAL};
+                }
+            }
+            H.anx.push_back(d->atm_nx[l]);
+            H.any.push_back(d->atm_ny[l]);
+            H.adx.push_back(d->atm_dx[l]);
+            H.aox.push_back(d->atm_ox[l]);
+            H.aoy.push_back(d->atm_oy[l]);
+            H.aht.push_back(d->atm_ht[l]);
+            H.avx.push_back(d->atm_vx[l]);
+            H.avy.push_back(d->atm_vy[l]);
+            H.aoff.push_back(H.atm_stride);
+            H.atm_stride += (long)d->atm_nx[l] * d->atm_ny[l];
+        }
+        for (int m = 0; m < d->ndm; m++) {
+            if (d->dm_nx[m] < 2 || d->dm_ny[m] < 2 || !(d->dm_dx[m] > 0)) {
+                set_error("mb_geom_wfs_create: DM %d: %d x %d", m, d->dm_nx[m], d->dm_ny[m]);
+                throw InvalidArg{MB_EINVAL};
+            }
+            H.dnx.push_back(d->dm_nx[m]);
+            H.dny.push_back(d->dm_ny[m]);
+            H.ddx.push_back(d->dm_dx[m]);
+            H.dox.push_back(d->dm_ox[m]);
+            H.doy.push_back(d->dm_oy[m]);
+            H.dht.push_back(d->dm_ht[m]);
+            H.doff.push_back(H.nact);
+            H.nact += (long)d->dm_nx[m] * d->dm_ny[m];
+        }
+        if (H.atm_stride) {
+            H.atm.alloc((size_t)H.atm_stride * H.nbatch);
+            H.atm.zero_async(nullptr);
+        }
+        MB_CUDA_TRY(cudaDeviceSynchronize());
+    } catch (const CudaError &e) {
+        delete h;
+        return e.code;
+    } catch (const InvalidArg &e) {
+        delete h;
+        return e.code;
+    }
+    *out = h;
+    return MB_OK;
+}
+
+void mb_geom_wfs_free(mb_geom_wfs *h) { delete h; }
+
+long mb_geom_wfs_ngrad(const mb_geom_wfs *h) { return h ? h->H.ngrad : -1; }
+long mb_geom_wfs_nact(const mb_geom_wfs *h) { return h ? h->H.nact : -1; }
+
+int mb_geom_wfs_set_atm(mb_geom_wfs *h, int inst, int layer, const double *screen) {
+    if (!h || !screen || inst < 0 || inst >= h->H.nbatch || layer < 0 || layer >= h->H.natm) {
+        mb::set_error("mb_geom_wfs_set_atm: invalid arguments");
+        return MB_EINVAL;
+    }
+    try {
+        mb::GeomWfsHost &H = h->H;
+        const long n = (long)H.anx[layer] * H.any[layer];
+        std::vector<float> f(screen, screen + n);
+        MB_CUDA_TRY(cudaMemcpy(H.atm.p + (size_t)inst * H.atm_stride + H.aoff[layer], f.data(), n * sizeof(float),
+                               cudaMemcpyHostToDevice));
+    } catch (const mb::CudaError &e) {
+        return e.code;
+    }
+    return MB_OK;
+}
+
+int mb_geom_wfs_grad(mb_geom_wfs *h, long isim, const float *d_dm, float *d_grad, unsigned long long seed,
+                     void *stream) {
+    using namespace mb;
+    if (!h || !d_grad || isim < 0 || (seed && !h->H.have_nea)) {
+        set_error("mb_geom_wfs_grad: invalid arguments%s", h && seed && !h->H.have_nea ? " (no NEA tables)" : "");
+        return MB_EINVAL;
+    }
+    try {
+        const GeomWfsHost &H = h->H;
+        GeomTab t;
+        std::memset(&t, 0, sizeof(t));
+        t.nwfs = H.nwfs;
+        int ns = 0;
+        for (int l = 0; l < H.natm; l++, ns++)
+            t.s[ns] = GeomScr{H.atm.p + H.aoff[l], H.atm_stride, H.anx[l], H.any[l], 1.0f, 1};
+        if (d_dm)
+            for (int m = 0; m < H.ndm; m++, ns++)
+                t.s[ns] = GeomScr{d_dm + H.doff[m], H.nact, H.dnx[m], H.dny[m], -1.0f, 0};
+        t.nscr = ns;
+        long goff = 0;
+        int saoff = 0;
+        for (int i = 0; i < H.nwfs; i++) {
+            t.w[i] = GeomWfsT{H.nsa[i], H.nxsa[i], saoff, goff};
+            saoff += H.nsa[i];
+            goff += 2L * H.nsa[i];
+            for (int s = 0; s < ns; s++) {
+                const bool atm = s < H.natm;
+                const int q = atm ? s : s - H.natm;
+                const double ht = atm ? H.aht[q] : H.dht[q];
+                const double sdx = atm ? H.adx[q] : H.ddx[q];
+                const double sox = atm ? H.aox[q] : H.dox[q], soy = atm ? H.aoy[q] : H.doy[q];
+                const double sc = std::isfinite(H.hs[i]) ? 1.0 - ht / H.hs[i] : 1.0;
+                const double dispx = ht * H.thetax[i] - (atm ? H.avx[q] * H.dt * (double)isim : 0.0);
+                const double dispy = ht * H.thetay[i] - (atm ? H.avy[q] * H.dt * (double)isim : 0.0);
+                t.c[i][s] = GeomCoef{H.dx[i] * sc / sdx, (H.gox[i] * sc + dispx - sox) / sdx, H.dx[i] * sc / sdx,
+                                     (H.goy[i] * sc + dispy - soy) / sdx};
+            }
+        }
+        const dim3 grid((unsigned)((H.max_nsa + kGeomWarps - 1) / kGeomWarps), (unsigned)H.nwfs, (unsigned)H.nbatch);
+        k_wfs_geom<<<grid, kGeomWarps * 32, 0, (cudaStream_t)stream>>>(t, H.sa_ix.p, H.sa_iy.p, H.sa_st.p, H.st.p,
+                                                                      H.st_off.p, H.nea.p, d_grad, H.ngrad, isim,
+                                                                      seed);
+        MB_CHECK_LAUNCH();
+    } catch (const CudaError &e) {
+        return e.code;
+    }
+    return MB_OK;
+}
+
+}  // extern "C"

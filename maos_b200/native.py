@@ -54,6 +54,21 @@ class MbReconDesc(C.Structure):
                 ("fit", C.POINTER(MbFitDesc))]
 
 
+_PI = C.POINTER(C.c_int)
+_PD = C.POINTER(C.c_double)
+
+
+class MbGeomWfsDesc(C.Structure):
+    _fields_ = [("nwfs", C.c_int), ("nsa", _PI), ("nxsa", _PI), ("dx", _PD), ("gox", _PD), ("goy", _PD),
+                ("thetax", _PD), ("thetay", _PD), ("hs", _PD), ("sa_ix", _PI), ("sa_iy", _PI),
+                ("sa_stencil", _PI), ("nstencil", C.c_int), ("stencil_off", C.POINTER(C.c_long)),
+                ("stencils", _PD), ("stencil_len", C.c_long), ("nea", _PD), ("natm", C.c_int),
+                ("atm_nx", _PI), ("atm_ny", _PI), ("atm_dx", _PD), ("atm_ox", _PD), ("atm_oy", _PD),
+                ("atm_ht", _PD), ("atm_vx", _PD), ("atm_vy", _PD), ("ndm", C.c_int), ("dm_nx", _PI),
+                ("dm_ny", _PI), ("dm_dx", _PD), ("dm_ox", _PD), ("dm_oy", _PD), ("dm_ht", _PD),
+                ("dt", C.c_double), ("nbatch", C.c_int)]
+
+
 # every symbol the header declares, with (restype, argtypes)
 _D = C.POINTER(C.c_double)
 _F = C.POINTER(C.c_float)
@@ -105,6 +120,12 @@ SIGNATURES = {
     "mb_servo_filter": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mb_servo_reset": (C.c_int, [C.c_void_p]),
     "mb_servo_free": (None, [C.c_void_p]),
+    "mb_geom_wfs_create": (C.c_int, [C.POINTER(MbGeomWfsDesc), C.POINTER(C.c_void_p)]),
+    "mb_geom_wfs_set_atm": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D]),
+    "mb_geom_wfs_grad": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_ulonglong, C.c_void_p]),
+    "mb_geom_wfs_ngrad": (C.c_long, [C.c_void_p]),
+    "mb_geom_wfs_nact": (C.c_long, [C.c_void_p]),
+    "mb_geom_wfs_free": (None, [C.c_void_p]),
     "mb_error_string": (C.c_char_p, [C.c_int]),
     "mb_last_error_message": (C.c_char_p, []),
     "mb_version": (C.c_int, []),

@@ -12,6 +12,9 @@
  *   mkg                    lib/mkg.c:470
  *   dcellpinv (PTT)        used by maos/setup_recon.c:255
  *   prop_grid_stat         lib/accphi.c + lib/prop_grid.c
+ *   prop_grid (loc out)    lib/accphi.c:426
+ *   WFS pts/amp/GS0        maos/setup_powfs.c:328-337,565 (ptsnew, pts2loc,
+ *                          mkamp -> locannular, mkg)
  *
  * The driver fills only the PARMS_T / RECON_T / POWFS_T fields those
  * functions read; everything else stays zero.  All arrays crossing this ABI
@@ -628,3 +631,58 @@ int ref_servo_filter(void *h, const double *merr, long n, double *cmd) {
     return up;
 }
 void ref_servo_free(void *h) { servo_free((SERVO_T *)h); }
+
+/* Geometric WFS of one powfs, built as maos/setup_powfs.c:328-337 and :565 do:
+ * pts of nx x nx points per subaperture at saloc + dx/2, loc = pts2loc(pts),
+ * amp = locannular(loc, D/2, din/2) (maos/utils.c:446 mkamp without a map),
+ * GS0 = mkg(loc, loc, amp, saloc, 1, 0, 0, 1).  Returns nnz of GS0. */
+static loc_t *last_wloc = NULL;
+static dmat *last_wamp = NULL;
+static dsp *last_gs0 = NULL;
+long ref_wfs_gs0(int nsa, double dsa, int nx, const double *salocx, const double *salocy, double D, double din) {
+    const double dx = dsa / nx;
+    pts_t *pts = ptsnew(nsa, dsa, dsa, nx, dx, dx);
+    for (int isa = 0; isa < nsa; isa++) {
+        pts->origx[isa] = salocx[isa] + dx * 0.5;
+        pts->origy[isa] = salocy[isa] + dx * 0.5;
+    }
+    if (last_wloc) locfree(last_wloc);
+    if (last_wamp) dfree(last_wamp);
+    if (last_gs0) dspfree(last_gs0);
+    last_wloc = pts2loc(pts);
+    last_wamp = dnew(last_wloc->nloc, 1);
+    locannular(last_wamp->p, last_wloc, 0, 0, D * 0.5, din * 0.5, 1);
+    loc_t *saloc = locnew(nsa, dsa, dsa);
+    memcpy(saloc->locx, salocx, sizeof(double) * nsa);
+    memcpy(saloc->locy, salocy, sizeof(double) * nsa);
+    last_gs0 = mkg(last_wloc, last_wloc, last_wamp, saloc, 1, 0, 0, 1);
+    locfree(saloc);
+    ptsfree(pts);
+    return last_gs0->p[last_gs0->ny];
+}
+void ref_wfs_gs0_get(double *locx, double *locy, double *amp, int *p, int *i, double *x, long *nrow,
+                     long *ncol) {
+    const long nloc = last_wloc->nloc;
+    memcpy(locx, last_wloc->locx, sizeof(double) * nloc);
+    memcpy(locy, last_wloc->locy, sizeof(double) * nloc);
+    memcpy(amp, last_wamp->p, sizeof(double) * nloc);
+    *nrow = last_gs0->nx;
+    *ncol = last_gs0->ny;
+    long nnz = last_gs0->p[last_gs0->ny];
+    for (long k = 0; k <= last_gs0->ny; k++) p[k] = last_gs0->p[k];
+    for (long k = 0; k < nnz; k++) { i[k] = last_gs0->i[k]; x[k] = last_gs0->x[k]; }
+}
+
+/* out += prop_grid(screen on an nx x ny map, points (locx, locy)): lib/accphi.c:426. */
+void ref_prop_grid(int nx, int ny, double dx, double ox, double oy, const double *screen, long nloc,
+                   const double *locx, const double *locy, double alpha, double displacex, double displacey,
+                   double scale, int wrap, double *out) {
+    map_t *m = mk_map(nx, ny, dx, dx, ox, oy);
+    memcpy(m->p, screen, sizeof(double) * nx * ny);
+    loc_t *loc = locnew(nloc, dx, dx);
+    memcpy(loc->locx, locx, sizeof(double) * nloc);
+    memcpy(loc->locy, locy, sizeof(double) * nloc);
+    prop_grid(m, loc, out, alpha, displacex, displacey, scale, wrap, 0, 0);
+    locfree(loc);
+    mapfree(m);
+}

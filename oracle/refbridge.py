@@ -158,6 +158,36 @@ class _Worker:
                       ctypes.byref(nr), ctypes.byref(nc))
         return p, i, x, nr.value, nc.value
 
+    def wfs_gs0(self, salocx, salocy, dsa, nx, D, din):
+        """The reference's WFS pts loc, amplitude and GS0 (CSC) for one powfs."""
+        L = self.lib
+        L.ref_wfs_gs0.restype = ctypes.c_long
+        nsa = len(salocx)
+        nnz = L.ref_wfs_gs0(nsa, ctypes.c_double(dsa), int(nx), _dp(salocx), _dp(salocy), ctypes.c_double(D),
+                            ctypes.c_double(din))
+        nloc = nsa * nx * nx
+        lx = np.zeros(nloc)
+        ly = np.zeros(nloc)
+        amp = np.zeros(nloc)
+        p = np.zeros(nloc + 1, dtype=np.int32)
+        i = np.zeros(nnz, dtype=np.int32)
+        x = np.zeros(nnz)
+        nr = ctypes.c_long(0)
+        nc = ctypes.c_long(0)
+        L.ref_wfs_gs0_get(lx.ctypes.data_as(_D), ly.ctypes.data_as(_D), amp.ctypes.data_as(_D),
+                          p.ctypes.data_as(_I), i.ctypes.data_as(_I), x.ctypes.data_as(_D),
+                          ctypes.byref(nr), ctypes.byref(nc))
+        return lx, ly, amp, p, i, x, nr.value, nc.value
+
+    def prop_grid(self, grid, screen, locx, locy, alpha, dispx, dispy, scale, wrap, out=None):
+        """out + prop_grid(screen on grid (nx, ny, dx, ox, oy), points) of the reference."""
+        out = np.zeros(len(locx)) if out is None else np.array(out, dtype=np.float64)
+        self.lib.ref_prop_grid(int(grid[0]), int(grid[1]), ctypes.c_double(grid[2]), ctypes.c_double(grid[3]),
+                               ctypes.c_double(grid[4]), _dp(np.asarray(screen).ravel()), ctypes.c_long(len(locx)),
+                               _dp(locx), _dp(locy), ctypes.c_double(alpha), ctypes.c_double(dispx),
+                               ctypes.c_double(dispy), ctypes.c_double(scale), int(wrap), out.ctypes.data_as(_D))
+        return out
+
     def fit_setup(self, fd):
         L = self.lib
         keep = []
