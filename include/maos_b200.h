@@ -268,6 +268,9 @@ typedef struct mb_geom_wfs mb_geom_wfs;
 int mb_geom_wfs_create(const mb_geom_wfs_desc *d, mb_geom_wfs **out);
 /* Upload one atmosphere layer of one instance (host FP64, stored FP32). */
 int mb_geom_wfs_set_atm(mb_geom_wfs *w, int inst, int layer, const double *screen);
+/* Wind of one layer of one instance (m/s; the descriptor's atm_vx, atm_vy
+ * are every instance's at creation). */
+int mb_geom_wfs_set_wind(mb_geom_wfs *w, int inst, int layer, double vx, double vy);
 /* Gradients of step isim (atmosphere shifted by v dt isim): d_dm (device
  * FP32 [nbatch][nact], NULL: open loop) is subtracted; d_grad (device FP32
  * [nbatch][ngrad], each WFS x then y) is written; seed != 0 adds the noise,

@@ -48,11 +48,11 @@ struct GeomWfsT {
     int nsa, nxsa, sa_off;
     long g_off;
 };
-struct GeomCoef {  // screen index = fine-grid index * s + b, this step
+struct GeomCoef {  // screen index = fine-grid index * s + b (before the wind shift)
     double sx, bx, sy, by;
 };
 struct GeomTab {
-    int nwfs, nscr;
+    int nwfs, nscr, natm;
     GeomWfsT w[kGeomMaxWfs];
     GeomScr s[kGeomMaxScr];
     GeomCoef c[kGeomMaxWfs][kGeomMaxScr];
@@ -73,12 +73,13 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
 // grid: (ceil(max nsa / kGeomWarps), nwfs, nbatch); block: kGeomWarps warps.
 // sa_ix/sa_iy: fine-grid index of each subaperture's first point; sa_st its
 // stencil; st_off the offset of each stencil ([2][W*W] floats) in st; nea
-// per WFS [3][nsa] (sqrt-NEA xx, yy, xy) at 3*sa_off.
+// per WFS [3][nsa] (sqrt-NEA xx, yy, xy) at 3*sa_off; wind_px: per instance and
+// atmosphere layer, the shift in layer pixels per step (v dt / dx).
 __global__ void __launch_bounds__(kGeomWarps * 32)
 k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, const int *__restrict__ sa_iy,
            const int *__restrict__ sa_st, const float *__restrict__ st, const long *__restrict__ st_off,
-           const float *__restrict__ nea, float *__restrict__ grad, long grad_stride, long isim,
-           unsigned long long seed) {
+           const float *__restrict__ nea, const double2 *__restrict__ wind_px, float *__restrict__ grad,
+           long grad_stride, long isim, unsigned long long seed) {
     __shared__ int4 sbase[kGeomWarps][kGeomMaxScr];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int iw = blockIdx.y, inst = blockIdx.z;
@@ -93,7 +94,12 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
     if (lane < t.nscr) {
         const GeomCoef c = t.c[iw][lane];
         const GeomScr &S = t.s[lane];
-        const double u = fma((double)gx0, c.sx, c.bx), v = fma((double)gy0, c.sy, c.by);
+        double u = fma((double)gx0, c.sx, c.bx), v = fma((double)gy0, c.sy, c.by);
+        if (lane < t.natm) {  // frozen flow: the layer moves by v dt per step
+            const double2 w = wind_px[(long)inst * t.natm + lane];
+            u = fma(-w.x, (double)isim, u);
+            v = fma(-w.y, (double)isim, v);
+        }
         const double fu = floor(u), fv = floor(v);
         long long iu = (long long)fmin(fmax(fu, -1e9), 1e9), iv = (long long)fmin(fmax(fv, -1e9), 1e9);
         if (S.wrap) {
@@ -184,13 +190,24 @@ struct GeomWfsHost {
     std::vector<int> nsa, nxsa;
     std::vector<double> dx, gox, goy, thetax, thetay, hs;
     std::vector<int> anx, any;
-    std::vector<double> adx, aox, aoy, aht, avx, avy;
+    std::vector<double> adx, aox, aoy, aht;
+    std::vector<double> wind;  // [nbatch][natm][2] m/s
     std::vector<long> aoff;  // layer offsets within one instance
     std::vector<int> dnx, dny;
     std::vector<double> ddx, dox, doy, dht;
     std::vector<long> doff;  // DM offsets within one instance's commands
     DevBuf<int> sa_ix, sa_iy, sa_st;
     DevBuf<float> st, nea, atm;
+    DevBuf<double2> wind_px;
+    void upload_wind() {
+        std::vector<double2> w((size_t)nbatch * natm);
+        for (int i = 0; i < nbatch; i++)
+            for (int l = 0; l < natm; l++) {
+                const size_t k = (size_t)i * natm + l;
+                w[k] = make_double2(wind[2 * k] * dt / adx[l], wind[2 * k + 1] * dt / adx[l]);
+            }
+        wind_px.upload(w);
+    }
     DevBuf<long> st_off;
     bool have_nea = false;
 };
@@ -291,8 +308,6 @@ int mb_geom_wfs_create(const mb_geom_wfs_desc *d, mb_geom_wfs **out) {
             H.aox.push_back(d->atm_ox[l]);
             H.aoy.push_back(d->atm_oy[l]);
             H.aht.push_back(d->atm_ht[l]);
-            H.avx.push_back(d->atm_vx[l]);
-            H.avy.push_back(d->atm_vy[l]);
             H.aoff.push_back(H.atm_stride);
             H.atm_stride += (long)d->atm_nx[l] * d->atm_ny[l];
         }
@@ -310,6 +325,13 @@ int mb_geom_wfs_create(const mb_geom_wfs_desc *d, mb_geom_wfs **out) {
             H.doff.push_back(H.nact);
             H.nact += (long)d->dm_nx[m] * d->dm_ny[m];
         }
+        H.wind.resize((size_t)H.nbatch * H.natm * 2);
+        for (int i = 0; i < H.nbatch; i++)
+            for (int l = 0; l < H.natm; l++) {
+                H.wind[2 * ((size_t)i * H.natm + l)] = d->atm_vx[l];
+                H.wind[2 * ((size_t)i * H.natm + l) + 1] = d->atm_vy[l];
+            }
+        if (H.natm) H.upload_wind();
         if (H.atm_stride) {
             H.atm.alloc((size_t)H.atm_stride * H.nbatch);
             H.atm.zero_async(nullptr);
@@ -348,6 +370,22 @@ int mb_geom_wfs_set_atm(mb_geom_wfs *h, int inst, int layer, const double *scree
     return MB_OK;
 }
 
+int mb_geom_wfs_set_wind(mb_geom_wfs *h, int inst, int layer, double vx, double vy) {
+    if (!h || inst < 0 || inst >= h->H.nbatch || layer < 0 || layer >= h->H.natm) {
+        mb::set_error("mb_geom_wfs_set_wind: invalid arguments");
+        return MB_EINVAL;
+    }
+    try {
+        mb::GeomWfsHost &H = h->H;
+        H.wind[2 * ((size_t)inst * H.natm + layer)] = vx;
+        H.wind[2 * ((size_t)inst * H.natm + layer) + 1] = vy;
+        H.upload_wind();
+    } catch (const mb::CudaError &e) {
+        return e.code;
+    }
+    return MB_OK;
+}
+
 int mb_geom_wfs_grad(mb_geom_wfs *h, long isim, const float *d_dm, float *d_grad, unsigned long long seed,
                      void *stream) {
     using namespace mb;
@@ -367,6 +405,7 @@ int mb_geom_wfs_grad(mb_geom_wfs *h, long isim, const float *d_dm, float *d_grad
             for (int m = 0; m < H.ndm; m++, ns++)
                 t.s[ns] = GeomScr{d_dm + H.doff[m], H.nact, H.dnx[m], H.dny[m], -1.0f, 0};
         t.nscr = ns;
+        t.natm = H.natm;
         long goff = 0;
         int saoff = 0;
         for (int i = 0; i < H.nwfs; i++) {
@@ -380,16 +419,15 @@ int mb_geom_wfs_grad(mb_geom_wfs *h, long isim, const float *d_dm, float *d_grad
                 const double sdx = atm ? H.adx[q] : H.ddx[q];
                 const double sox = atm ? H.aox[q] : H.dox[q], soy = atm ? H.aoy[q] : H.doy[q];
                 const double sc = std::isfinite(H.hs[i]) ? 1.0 - ht / H.hs[i] : 1.0;
-                const double dispx = ht * H.thetax[i] - (atm ? H.avx[q] * H.dt * (double)isim : 0.0);
-                const double dispy = ht * H.thetay[i] - (atm ? H.avy[q] * H.dt * (double)isim : 0.0);
+                const double dispx = ht * H.thetax[i], dispy = ht * H.thetay[i];
                 t.c[i][s] = GeomCoef{H.dx[i] * sc / sdx, (H.gox[i] * sc + dispx - sox) / sdx, H.dx[i] * sc / sdx,
                                      (H.goy[i] * sc + dispy - soy) / sdx};
             }
         }
         const dim3 grid((unsigned)((H.max_nsa + kGeomWarps - 1) / kGeomWarps), (unsigned)H.nwfs, (unsigned)H.nbatch);
         k_wfs_geom<<<grid, kGeomWarps * 32, 0, (cudaStream_t)stream>>>(t, H.sa_ix.p, H.sa_iy.p, H.sa_st.p, H.st.p,
-                                                                      H.st_off.p, H.nea.p, d_grad, H.ngrad, isim,
-                                                                      seed);
+                                                                      H.st_off.p, H.nea.p, H.wind_px.p, d_grad,
+                                                                      H.ngrad, isim, seed);
         MB_CHECK_LAUNCH();
     } catch (const CudaError &e) {
         return e.code;

@@ -122,6 +122,7 @@ SIGNATURES = {
     "mb_servo_free": (None, [C.c_void_p]),
     "mb_geom_wfs_create": (C.c_int, [C.POINTER(MbGeomWfsDesc), C.POINTER(C.c_void_p)]),
     "mb_geom_wfs_set_atm": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D]),
+    "mb_geom_wfs_set_wind": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double]),
     "mb_geom_wfs_grad": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_ulonglong, C.c_void_p]),
     "mb_geom_wfs_ngrad": (C.c_long, [C.c_void_p]),
     "mb_geom_wfs_nact": (C.c_long, [C.c_void_p]),

@@ -125,9 +125,15 @@ class GeomWfs:
         check(self.lib.mb_geom_wfs_set_atm(self.h, int(inst), int(layer), s.ctypes.data_as(C.POINTER(C.c_double))),
               "mb_geom_wfs_set_atm")
 
+    def set_wind(self, inst: int, layer: int, vx: float, vy: float) -> None:
+        check(self.lib.mb_geom_wfs_set_wind(self.h, int(inst), int(layer), float(vx), float(vy)),
+              "mb_geom_wfs_set_wind")
+
     def set_atmosphere(self, inst: int, atm) -> None:
+        """Screens and winds of a FrozenFlowAtmosphere for one instance."""
         for l, s in enumerate(atm.screens):
             self.set_atm(inst, l, s)
+            self.set_wind(inst, l, atm.vx[l], atm.vy[l])
 
     def grad(self, isim: int, dm=None, seed: int = 0, out=None, stream=None):
         """Gradients of step ``isim`` for every instance (device float32

@@ -686,3 +686,45 @@ void ref_prop_grid(int nx, int ny, double dx, double ox, double oy, const double
     locfree(loc);
     mapfree(m);
 }
+
+/* Geometric gradients of nwfs WFS of the powfs last built by ref_wfs_gs0, as
+ * the reference's CPU simulation forms them: OPD on loc = sum over maps of
+ * prop_grid (atmosphere: displacement ht*theta - v*dt*isim, wrap; DMs:
+ * ht*theta, alpha -1, no wrap; scale 1 - ht/hs), then GS0 * OPD
+ * (maos/wfsgrad.c:241 dspmm).  The maps' ray tracing runs as OpenMP tasks
+ * over nthread threads (prop_grid's taskloop).  grad: [nwfs][2 nsa]. */
+void ref_wfs_geom_grads(int nwfs, const double *thetax, const double *thetay, const double *hs, int nscr,
+                        const int *nx, const int *ny, const double *dx, const double *ox, const double *oy,
+                        const double *ht, const double *vx, const double *vy, const double *alpha, const int *wrap,
+                        const double *screens, double dt, long isim, int nthread, double *grad) {
+    map_t **maps = calloc(nscr, sizeof(map_t *));
+    long off = 0;
+    for (int s = 0; s < nscr; s++) {
+        maps[s] = mk_map(nx[s], ny[s], dx[s], dx[s], ox[s], oy[s]);
+        memcpy(maps[s]->p, screens + off, sizeof(double) * nx[s] * ny[s]);
+        off += (long)nx[s] * ny[s];
+    }
+    const long nloc = last_wloc->nloc;
+    dmat **opd = calloc(nwfs, sizeof(dmat *));
+    for (int w = 0; w < nwfs; w++) opd[w] = dnew(nloc, 1);
+#pragma omp parallel num_threads(nthread)
+#pragma omp single
+    for (int w = 0; w < nwfs; w++) {
+        for (int s = 0; s < nscr; s++) {
+            const double sc = isfinite(hs[w]) ? 1. - ht[s] / hs[w] : 1.;
+            prop_grid(maps[s], last_wloc, opd[w]->p, alpha[s], ht[s] * thetax[w] - vx[s] * dt * isim,
+                      ht[s] * thetay[w] - vy[s] * dt * isim, sc, wrap[s], 0, 0);
+        }
+    }
+    const long ng = last_gs0->nx;
+    for (int w = 0; w < nwfs; w++) {
+        dmat *g = dnew(ng, 1);
+        dspmm(&g, last_gs0, opd[w], "nn", 1);
+        memcpy(grad + w * ng, g->p, sizeof(double) * ng);
+        dfree(g);
+        dfree(opd[w]);
+    }
+    free(opd);
+    for (int s = 0; s < nscr; s++) mapfree(maps[s]);
+    free(maps);
+}

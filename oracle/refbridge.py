@@ -177,6 +177,7 @@ class _Worker:
         L.ref_wfs_gs0_get(lx.ctypes.data_as(_D), ly.ctypes.data_as(_D), amp.ctypes.data_as(_D),
                           p.ctypes.data_as(_I), i.ctypes.data_as(_I), x.ctypes.data_as(_D),
                           ctypes.byref(nr), ctypes.byref(nc))
+        self._wfs_ng = int(nr.value)
         return lx, ly, amp, p, i, x, nr.value, nc.value
 
     def prop_grid(self, grid, screen, locx, locy, alpha, dispx, dispy, scale, wrap, out=None):
@@ -187,6 +188,27 @@ class _Worker:
                                _dp(locx), _dp(locy), ctypes.c_double(alpha), ctypes.c_double(dispx),
                                ctypes.c_double(dispy), ctypes.c_double(scale), int(wrap), out.ctypes.data_as(_D))
         return out
+
+    def wfs_geom_grads(self, thetax, thetay, hs, maps, dt, isim, nthread=None):
+        """Geometric gradients [nwfs, 2 nsa] of the powfs last built by
+        wfs_gs0: maps = [(data [ny, nx], dx, ox, oy, ht, vx, vy, alpha, wrap)]."""
+        L = self.lib
+        nw = len(thetax)
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        nx = i32([m[0].shape[1] for m in maps])
+        ny = i32([m[0].shape[0] for m in maps])
+        cols = [f64([m[k] for m in maps]) for k in range(1, 8)]
+        wrap = i32([m[8] for m in maps])
+        scr = f64(np.concatenate([np.ascontiguousarray(m[0], dtype=np.float64).ravel() for m in maps]))
+        th = [f64(thetax), f64(thetay), f64(hs)]
+        out = np.zeros(nw * self._wfs_ng)
+        L.ref_wfs_geom_grads(nw, th[0].ctypes.data_as(_D), th[1].ctypes.data_as(_D), th[2].ctypes.data_as(_D),
+                             len(maps), nx.ctypes.data_as(_I), ny.ctypes.data_as(_I),
+                             *[c.ctypes.data_as(_D) for c in cols], wrap.ctypes.data_as(_I),
+                             scr.ctypes.data_as(_D), ctypes.c_double(dt), ctypes.c_long(isim),
+                             int(nthread or self.nthread), out.ctypes.data_as(_D))
+        return out.reshape(nw, self._wfs_ng)
 
     def fit_setup(self, fd):
         L = self.lib

@@ -120,3 +120,37 @@ def test_invalid_arguments_raise(ltao):
     with pytest.raises(MbError):
         W.set_atm(1, 0, np.zeros(4))
     W.close()
+
+
+def test_loop_closes_on_the_device():
+    """WFS -> tomography + fit -> servo -> DMs -> WFS, all on the GPU, on a
+    frozen atmosphere: the closed-loop gradients shrink to the fitting error."""
+    import torch
+    from conftest import get_fit, get_system
+    from maos_b200.recon import Reconstructor
+    from maos_b200.servo import Servo
+    from maos_b200.turbulence import FrozenFlowAtmosphere
+    from maos_b200.wfs import GeomWfs
+    s = get_system("scao_8m")
+    fit = get_fit("scao_8m")
+    W = GeomWfs.for_system(s, FrozenFlowAtmosphere(s.cfg, 2), fit=fit)
+    R = Reconstructor(s, nbatch=1, fit=fit)
+    S = Servo(fit.nact, ep=[[0.5]], dt=s.cfg.sim_dt)
+    st = torch.cuda.current_stream()
+    dm = torch.zeros(1, fit.nact, dtype=torch.float32, device="cuda")
+    fa = torch.zeros(fit.nact, dtype=torch.float32, device="cuda")
+    rms = []
+    for k in range(20):
+        g = W.grad(0, dm=dm)
+        rms.append(float(g.norm()))
+        R.step_device(g.data_ptr(), st.cuda_stream)
+        R.slot_download(0, fa.data_ptr(), st.cuda_stream)
+        cmd = S.filter(fa.double(), stream=st)
+        dm.copy_(cmd.float()[None, :])
+    torch.cuda.synchronize()
+    print("closed-loop gradient rms / open loop:", [round(r / rms[0], 4) for r in rms])
+    assert rms[-1] < 0.3 * rms[0]
+    assert rms[-1] <= 1.05 * min(rms[10:])
+    R.close()
+    S.close()
+    W.close()

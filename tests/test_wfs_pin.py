@@ -59,3 +59,34 @@ def test_prop_grid_matches_reference(ref_proc):
             ref = ref_proc.call("prop_grid", (nx, ny, dx, ox, oy), scr, x, y, alpha, dxp, dyp, scale, wrap)
             ours = wfs_oracle.prop_grid(scr, ox, oy, dx, x, y, alpha, dxp, dyp, scale, bool(wrap))
             assert np.abs(ours - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_geom_gradients_match_reference(ref_proc):
+    """The whole geometric WFS (atmosphere with wind and wrap-around, a DM,
+    GS0) of the oracle against the reference's prop_grid + GS0 product."""
+    from conftest import get_fit, get_system
+    from maos_b200 import wfs_setup
+    from maos_b200.turbulence import FrozenFlowAtmosphere
+    s = get_system("ltao_8m")
+    fit = get_fit("ltao_8m")
+    geom = wfs_setup.build_geom_wfs(s)
+    P = geom.powfs[0]
+    w = s.wfs[0]
+    ref_proc.call("wfs_gs0", w.salocx, w.salocy, w.dsa, P.nxsa, s.cfg.D, s.cfg.din)
+    atm = FrozenFlowAtmosphere(s.cfg, 4)
+    n, dx = atm.n, atm.dx
+    o = -n / 2 * dx
+    layers = [wfs_oracle.Screen(sc, o, o, dx, float(h), float(atm.vx[l]), float(atm.vy[l]))
+              for l, (sc, h) in enumerate(zip(atm.screens, s.cfg.atm_ht))]
+    a = np.random.default_rng(8).standard_normal(fit.nact) * 1e-7
+    dms = []
+    off = fit.act_offsets()
+    for k, dm in enumerate(fit.dms):
+        dms.append(wfs_oracle.Screen(a[off[k]:off[k + 1]].reshape(dm.amap.ny, dm.amap.nx), dm.amap.ox, dm.amap.oy,
+                                     dm.amap.dx, dm.ht))
+    maps = [(L.data, L.dx, L.ox, L.oy, L.ht, L.vx, L.vy, 1.0, 1) for L in layers]
+    maps += [(D.data, D.dx, D.ox, D.oy, D.ht, 0.0, 0.0, -1.0, 0) for D in dms]
+    isim = 17
+    ref = ref_proc.call("wfs_geom_grads", geom.thetax, geom.thetay, geom.hs, maps, s.cfg.sim_dt, isim).ravel()
+    ours = wfs_oracle.geom_grads(geom, layers, dms, isim, s.cfg.sim_dt)
+    assert np.linalg.norm(ours - ref) <= 1e-12 * np.linalg.norm(ref)
