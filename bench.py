@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--precision-steps", type=int, default=2000)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-wfs", action="store_true")
     return ap.parse_args()
 
 
@@ -247,6 +248,69 @@ def mvm_rates(lib, native, nact: int, ngrad: int, batch: int, stream, M=None):
                      "hbm_frac": nbytes / (ms / 1000.0) / 1e9 / peak}
         lib.mb_mvm_free(h)
     del M
+    return res
+
+
+def wfs_rates(sysm, fit, batch: int, stream, cpu: bool = True):
+    """Geometric WFS gradients on the device (mb_geom_wfs_grad: every WFS
+    of ``batch`` instances, each with its own atmosphere, through the DMs,
+    with noise) per step, and the reference's CPU geometric gradients of one
+    instance (prop_grid + GS0 from oracle/_ref) on this host's cores."""
+    import numpy as np
+    import torch
+    from maos_b200 import wfs_setup
+    from maos_b200.turbulence import FrozenFlowAtmosphere
+    from maos_b200.wfs import GeomWfs
+    geom = wfs_setup.build_geom_wfs(sysm)
+    atms = [FrozenFlowAtmosphere(sysm.cfg, 100 + i) for i in range(4)]
+    W = GeomWfs.for_system(sysm, [atms[i % 4] for i in range(batch)], fit=fit, nbatch=batch, geom=geom)
+    dm = torch.randn(batch, W.nact, device="cuda") * 1e-7
+    with torch.cuda.stream(stream):
+        for k in range(3):
+            W.grad(k, dm=dm, seed=1, stream=stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        n = 20
+        e0.record(stream)
+        for k in range(n):
+            W.grad(k, dm=dm, seed=1, stream=stream)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n
+    P = [geom.powfs[geom.wfs_powfs[i]] for i in range(geom.nwfs)]
+    pts = sum((p.nxsa + 2) ** 2 * len(p.ix0) for p in P)
+    nmap = len(sysm.cfg.atm_ht) + len(fit.dms)
+    res = {"instances": batch, "ms": ms, "steps_per_s": batch * 1000.0 / ms, "kernel": "k_wfs_geom",
+           "wfs": geom.nwfs, "subapertures": int(sum(len(p.ix0) for p in P)), "points_per_subaperture_side": P[0].nxsa,
+           "maps": nmap, "interpolations_per_s": pts * nmap * batch / (ms / 1000.0),
+           "data": "seeded von Karman layers (4 seeds over the instances), random DM commands, noise on"}
+    W.close()
+    if cpu:
+        from oracle import refbridge
+        if refbridge.available():
+            a0 = atms[0]
+            o = -a0.n / 2 * a0.dx
+            maps = [(sc, a0.dx, o, o, float(h), float(a0.vx[l]), float(a0.vy[l]), 1.0, 1)
+                    for l, (sc, h) in enumerate(zip(a0.screens, sysm.cfg.atm_ht))]
+            a = dm[0].double().cpu().numpy()
+            off = fit.act_offsets()
+            for k, d in enumerate(fit.dms):
+                maps.append((a[off[k]:off[k + 1]].reshape(d.amap.ny, d.amap.nx), d.amap.dx, d.amap.ox, d.amap.oy,
+                             d.ht, 0.0, 0.0, -1.0, 0))
+            ncores = os.cpu_count() or 1
+            w0 = sysm.wfs[0]
+            with refbridge.RefProcess(nthread=ncores) as R:
+                R.call("wfs_gs0", w0.salocx, w0.salocy, w0.dsa, P[0].nxsa, sysm.cfg.D, sysm.cfg.din)
+                R.call("wfs_geom_grads", geom.thetax, geom.thetay, geom.hs, maps, sysm.cfg.sim_dt, 0)
+                t0 = time.perf_counter()
+                nstep = 0
+                while nstep < 3 or (time.perf_counter() - t0 < 5.0 and nstep < 20):
+                    R.call("wfs_geom_grads", geom.thetax, geom.thetay, geom.hs, maps, sysm.cfg.sim_dt, nstep)
+                    nstep += 1
+                dt = time.perf_counter() - t0
+            res["cpu_reference"] = {"steps_per_s": nstep / dt, "cores": ncores, "kind": "reference",
+                                    "sample": f"{nstep} steps of one instance (prop_grid of every map onto every "
+                                              f"WFS's points, then GS0) in {dt:.1f} s"}
     return res
 
 
@@ -469,6 +533,9 @@ def run_gpu(args):
         mvm_line["precision"] = precision
     del Mctl
 
+    wfs_line = wfs_rates(sysm, fit, B, stream, cpu=(rank == 0 and not args.no_cpu_baseline)) \
+        if world == 1 and not args.no_wfs else None
+
     served = served_mvm = None
     if world == 1 and not args.no_serve and args.serve_seconds > 0:
         served = served_mix(args.serve_seconds, mcao_frames=fr[0])
@@ -503,6 +570,7 @@ def run_gpu(args):
                         "api": "mb_recon_serve_step, pinned FP32 host buffers",
                         "fp64_gpu_tomo_gpu_fit_steps_per_s": fp64_api_value},
                 "mvm": mvm_line,
+                "wfs_gradients": wfs_line,
                 "served": served,
                 "served_mvm": served_mvm,
                 "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,

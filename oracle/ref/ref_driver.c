@@ -691,8 +691,9 @@ void ref_prop_grid(int nx, int ny, double dx, double ox, double oy, const double
  * the reference's CPU simulation forms them: OPD on loc = sum over maps of
  * prop_grid (atmosphere: displacement ht*theta - v*dt*isim, wrap; DMs:
  * ht*theta, alpha -1, no wrap; scale 1 - ht/hs), then GS0 * OPD
- * (maos/wfsgrad.c:241 dspmm).  The maps' ray tracing runs as OpenMP tasks
- * over nthread threads (prop_grid's taskloop).  grad: [nwfs][2 nsa]. */
+ * (maos/wfsgrad.c:241 dspmm).  One WFS per thread of an OpenMP team of
+ * nthread threads, as maos/sim.c runs wfsgrad_iwfs as one task per WFS;
+ * idle threads take prop_grid's own taskloop chunks.  grad: [nwfs][2 nsa]. */
 void ref_wfs_geom_grads(int nwfs, const double *thetax, const double *thetay, const double *hs, int nscr,
                         const int *nx, const int *ny, const double *dx, const double *ox, const double *oy,
                         const double *ht, const double *vx, const double *vy, const double *alpha, const int *wrap,
@@ -707,8 +708,7 @@ void ref_wfs_geom_grads(int nwfs, const double *thetax, const double *thetay, co
     const long nloc = last_wloc->nloc;
     dmat **opd = calloc(nwfs, sizeof(dmat *));
     for (int w = 0; w < nwfs; w++) opd[w] = dnew(nloc, 1);
-#pragma omp parallel num_threads(nthread)
-#pragma omp single
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthread)
     for (int w = 0; w < nwfs; w++) {
         for (int s = 0; s < nscr; s++) {
             const double sc = isfinite(hs[w]) ? 1. - ht[s] / hs[w] : 1.;
