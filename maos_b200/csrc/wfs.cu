@@ -12,10 +12,13 @@
 // Instead of writing the OPD of every WFS point to memory and running a
 // sparse product over it, one warp computes one subaperture: the OPD of the
 // (nxsa+2)^2 fine-grid points its average-gradient stencil touches stays in
-// registers (kGeomChunk points per lane at a time), each map is interpolated straight
-// from its layer (read through L1; the layers of a 30 m system are a few MB
-// and stay in L2), and the two stencil dot products are reduced with warp
-// shuffles.  Stencils are shared by all subapertures with the same amplitude
+// registers (kGeomChunk points per lane at a time) and the two stencil dot
+// products are reduced with warp shuffles.  A window covers only a few pixels
+// of each map (OPD points are 1/64 m, layers 1/5 to 1/2 m), so the warp
+// copies that block of pixels to shared memory once, interpolates each of its
+// rows along x at every window column, and each point is then one
+// interpolation along y between two of those rows: two shared-memory reads
+// per point and map instead of four gathers.  Stencils are shared by all subapertures with the same amplitude
 // neighbourhood.  The noise is two standard normals per subaperture from a
 // counter-based generator (Philox4x32-10, Salmon et al. 2011) keyed by the
 // seed and counted by (subaperture, WFS, step, instance), so any step of any
@@ -36,6 +39,10 @@ constexpr int kGeomMaxScr = 16;   // atmosphere layers + DMs
 constexpr int kGeomWarps = 8;     // subapertures per CTA
 constexpr int kGeomMaxW = 36;     // window side (nxsa + 2)
 constexpr int kGeomChunk = 13;   // window points per lane per pass
+constexpr int kGeomBlk = 16;     // layer pixels a window spans across, at most
+constexpr int kGeomBlkStride = kGeomBlk + 1;
+constexpr int kGeomHStride = kGeomMaxW;
+constexpr double kGeomMaxStep = (kGeomBlk - 3.0) / (kGeomMaxW - 1.0);  // layer pixels per fine-grid step
 
 struct GeomScr {
     const float *p;    // [ny][nx], x fastest
@@ -75,12 +82,14 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
 // stencil; st_off the offset of each stencil ([2][W*W] floats) in st; nea
 // per WFS [3][nsa] (sqrt-NEA xx, yy, xy) at 3*sa_off; wind_px: per instance and
 // atmosphere layer, the shift in layer pixels per step (v dt / dx).
-__global__ void __launch_bounds__(kGeomWarps * 32)
+__global__ void __launch_bounds__(kGeomWarps * 32, 4)
 k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, const int *__restrict__ sa_iy,
            const int *__restrict__ sa_st, const float *__restrict__ st, const long *__restrict__ st_off,
            const float *__restrict__ nea, const double2 *__restrict__ wind_px, float *__restrict__ grad,
            long grad_stride, long isim, unsigned long long seed) {
     __shared__ int4 sbase[kGeomWarps][kGeomMaxScr];
+    __shared__ float sblk[kGeomWarps][kGeomBlk * kGeomBlkStride];
+    __shared__ float shx[kGeomWarps][kGeomBlk * kGeomHStride];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int iw = blockIdx.y, inst = blockIdx.z;
     const GeomWfsT &W = t.w[iw];
@@ -113,39 +122,71 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
     __syncwarp();
     const float inv_wn = 1.0f / (float)wn;
     const float *__restrict__ w = st + st_off[sa_st[gi]];
+    float *blk = sblk[wid], *hx = shx[wid];
     float gx = 0.f, gy = 0.f;
     // the window in chunks of kGeomChunk points per lane (OPD in registers)
     for (int k0 = 0; k0 < npts; k0 += 32 * kGeomChunk) {
         float opd[kGeomChunk];
 #pragma unroll
         for (int j = 0; j < kGeomChunk; j++) opd[j] = 0.f;
+        const int rlo = k0 / wn, rhi = (min(npts, k0 + 32 * kGeomChunk) - 1) / wn;
         for (int s = 0; s < t.nscr; s++) {
             const GeomScr S = t.s[s];
             const int4 b = sbase[wid][s];
             const float sxf = (float)t.c[iw][s].sx, syf = (float)t.c[iw][s].sy;
             const float fu0 = __int_as_float(b.z), fv0 = __int_as_float(b.w);
             const float *__restrict__ P = S.p + (long)inst * S.inst_stride;
+            // the layer pixels this chunk touches: columns 0..nbu-1 and rows
+            // v0..v0+nbv-1 from the window origin's pixel (the +1 neighbours included)
+            const int v0 = (int)floorf(fmaf((float)rlo, syf, fv0));
+            const int nbv = min((int)floorf(fmaf((float)rhi, syf, fv0)) + 2 - v0, kGeomBlk);
+            const int nbu = min((int)floorf(fmaf((float)(wn - 1), sxf, fu0)) + 2, kGeomBlk);
+            __syncwarp();  // the previous map's tables are no longer read
+            for (int e = lane; e < nbu * nbv; e += 32) {
+                const int bv = e / nbu, bu = e - bv * nbu;
+                int c = b.x + bu, r = b.y + v0 + bv;
+                float val = 0.f;
+                if (S.wrap) {
+                    c -= c >= S.nx ? S.nx : 0;
+                    r -= r >= S.ny ? S.ny : 0;
+                    val = __ldg(P + (long)r * S.nx + c);
+                } else {
+                    c = c == S.nx ? 0 : c;  // the +1 neighbour of the last column is column 0
+                    r = r == S.ny ? 0 : r;
+                    if (c >= 0 && c < S.nx && r >= 0 && r < S.ny) val = __ldg(P + (long)r * S.nx + c);
+                }
+                blk[bv * kGeomBlkStride + bu] = val;
+            }
+            __syncwarp();
+            // each block row interpolated along x at every window column
+            for (int e = lane; e < nbv * wn; e += 32) {
+                const int bv = e / wn, cc = e - bv * wn;
+                const float uf = fmaf((float)cc, sxf, fu0), fl = floorf(uf);
+                const int lu = (int)fl;
+                const float m0 = blk[bv * kGeomBlkStride + lu], m1 = blk[bv * kGeomBlkStride + lu + 1];
+                float hv = fmaf(m1 - m0, uf - fl, m0);
+                if (!S.wrap) {
+                    const int c = b.x + lu;
+                    if (c < 0 || c >= S.nx) hv = 0.f;  // off the map: no contribution
+                }
+                hx[bv * kGeomHStride + cc] = hv;
+            }
+            __syncwarp();
+            // every point of the chunk: along y between two of those rows
 #pragma unroll
             for (int j = 0; j < kGeomChunk; j++) {
                 const int k = k0 + lane + 32 * j;
                 if (k < npts) {
                     const int r = (int)(((float)k + 0.5f) * inv_wn), cc = k - r * wn;
-                    const float uf = fmaf((float)cc, sxf, fu0), vf = fmaf((float)r, syf, fv0);
-                    const float flu = floorf(uf), flv = floorf(vf);
-                    int iu = b.x + (int)flu, iv = b.y + (int)flv;
-                    const float ax = uf - flu, ay = vf - flv;
-                    if (S.wrap) {
-                        iu += iu < 0 ? S.nx : (iu >= S.nx ? -S.nx : 0);
-                        iv += iv < 0 ? S.ny : (iv >= S.ny ? -S.ny : 0);
-                    } else if (iu < 0 || iu >= S.nx || iv < 0 || iv >= S.ny) {
-                        continue;  // off the map: no contribution (prop_grid without wrap)
+                    const float vf = fmaf((float)r, syf, fv0), flv = floorf(vf);
+                    const int lv = (int)flv - v0;
+                    if (lv < 0 || lv + 1 >= nbv) continue;  // never taken: the block covers the chunk
+                    if (!S.wrap) {
+                        const int iv = b.y + (int)flv;
+                        if (iv < 0 || iv >= S.ny) continue;  // off the map: no contribution
                     }
-                    const int iu1 = iu == S.nx - 1 ? 0 : iu + 1;
-                    const long r0 = (long)iv * S.nx, r1 = (long)(iv == S.ny - 1 ? 0 : iv + 1) * S.nx;
-                    const float m00 = __ldg(P + r0 + iu), m10 = __ldg(P + r0 + iu1);
-                    const float m01 = __ldg(P + r1 + iu), m11 = __ldg(P + r1 + iu1);
-                    opd[j] = fmaf(S.alpha, fmaf(fmaf(m10 - m00, ax, m00), 1.f - ay, fmaf(m11 - m01, ax, m01) * ay),
-                                  opd[j]);
+                    const float h0 = hx[lv * kGeomHStride + cc], h1 = hx[(lv + 1) * kGeomHStride + cc];
+                    opd[j] = fmaf(S.alpha, fmaf(h1 - h0, vf - flv, h0), opd[j]);
                 }
             }
         }
@@ -293,13 +334,15 @@ int mb_geom_wfs_create(const mb_geom_wfs_desc *d, mb_geom_wfs **out) {
                 set_error("mb_geom_wfs_create: atmosphere layer %d: %d x %d", l, d->atm_nx[l], d->atm_ny[l]);
                 throw InvalidArg{MB_EINVAL};
             }
-            // the wrap-around of a window needs the window to be smaller than the layer
+            // a window must span at most kGeomBlk layer pixels (and fewer than the layer has)
             for (int i = 0; i < d->nwfs; i++) {
                 const double sc = std::isfinite(d->hs[i]) ? 1.0 - d->atm_ht[l] / d->hs[i] : 1.0;
-                const double ext = (d->nxsa[i] + 2) * d->dx[i] * std::fabs(sc) / d->atm_dx[l] + 2;
-                if (ext >= d->atm_nx[l] || ext >= d->atm_ny[l]) {
-                    set_error("mb_geom_wfs_create: layer %d smaller than a subaperture window", l);
-                    throw InvalidArg{MB_EINVAL};
+                const double step = d->dx[i] * sc / d->atm_dx[l];
+                if (!(sc > 0) || step > kGeomMaxStep || kGeomBlk >= d->atm_nx[l] || kGeomBlk >= d->atm_ny[l]) {
+                    set_error("mb_geom_wfs_create: layer %d: WFS %d steps %.3g layer pixels per OPD point "
+                              "(at most %.3g) on a %d x %d layer", l, i, step, kGeomMaxStep, d->atm_nx[l],
+                              d->atm_ny[l]);
+                    throw InvalidArg{MB_EUNSUP};
                 }
             }
             H.anx.push_back(d->atm_nx[l]);
@@ -315,6 +358,15 @@ int mb_geom_wfs_create(const mb_geom_wfs_desc *d, mb_geom_wfs **out) {
             if (d->dm_nx[m] < 2 || d->dm_ny[m] < 2 || !(d->dm_dx[m] > 0)) {
                 set_error("mb_geom_wfs_create: DM %d: %d x %d", m, d->dm_nx[m], d->dm_ny[m]);
                 throw InvalidArg{MB_EINVAL};
+            }
+            for (int i = 0; i < d->nwfs; i++) {
+                const double sc = std::isfinite(d->hs[i]) ? 1.0 - d->dm_ht[m] / d->hs[i] : 1.0;
+                const double step = d->dx[i] * sc / d->dm_dx[m];
+                if (!(sc > 0) || step > kGeomMaxStep) {
+                    set_error("mb_geom_wfs_create: DM %d: WFS %d steps %.3g actuators per OPD point (at most %.3g)",
+                              m, i, step, kGeomMaxStep);
+                    throw InvalidArg{MB_EUNSUP};
+                }
             }
             H.dnx.push_back(d->dm_nx[m]);
             H.dny.push_back(d->dm_ny[m]);

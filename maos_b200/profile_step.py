@@ -2,12 +2,16 @@
 
     python -m maos_b200.profile_step [--system mcao_30m] [--batch 32] [--steps 1]
     python -m maos_b200.profile_step --mvm bf16 [--batch 32] [--steps 1]
+    python -m maos_b200.profile_step --wfs [--system mcao_30m] [--batch 8] [--steps 1]
 
 Builds the system, sets up a reconstructor with the DM fit for `batch`
 instances and runs `steps` graph steps on random gradients; prints "ok".
 Under ncu, each step's kernels appear in order: k_gp, k_pupil_rows (right-hand
 side), k_hxt_rows, then per FDPCG iteration k_pupil_rows, k_hxt_rows,
 k_fd_fwd, k_fd_mul, k_fd_inv, k_cg_update_p, then the fit.
+
+With --wfs, the system's geometric WFS (every WFS, its atmosphere and DMs,
+noise on) runs `steps` times for `batch` instances instead (k_wfs_geom).
 
 With --mvm, a random control matrix of the system's shape (nact x ngrad) is
 installed in that storage type and `steps` batched MVMs are applied instead
@@ -27,9 +31,21 @@ def main():
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--mvm", choices=["fp32", "bf16", "fp8"], default=None)
+    ap.add_argument("--wfs", action="store_true")
     a = ap.parse_args()
     s = geometry.build_tomo(config.PRESETS[a.system]())
     fs = fit_setup.build_fit(s)
+    if a.wfs:
+        from .turbulence import FrozenFlowAtmosphere
+        from .wfs import GeomWfs
+        W = GeomWfs.for_system(s, FrozenFlowAtmosphere(s.cfg, 1), fit=fs, nbatch=a.batch)
+        dm = torch.randn(a.batch, W.nact, device="cuda") * 1e-7
+        for k in range(a.steps):
+            W.grad(k, dm=dm, seed=1)
+        torch.cuda.synchronize()
+        W.close()
+        print("ok")
+        return
     if a.mvm:
         import ctypes as C
         import numpy as np
