@@ -12,7 +12,7 @@
 // Instead of writing the OPD of every WFS point to memory and running a
 // sparse product over it, one warp computes one subaperture: the OPD of the
 // (nxsa+2)^2 fine-grid points its average-gradient stencil touches stays in
-// registers (kGeomChunk points per lane at a time) and the two stencil dot
+// registers (a band of rows at a time) and the two stencil dot
 // products are reduced with warp shuffles.  A window covers only a few pixels
 // of each map (OPD points are 1/64 m, layers 1/5 to 1/2 m), so the warp
 // copies that block of pixels to shared memory once, interpolates each of its
@@ -38,7 +38,7 @@ constexpr int kGeomMaxWfs = 16;
 constexpr int kGeomMaxScr = 16;   // atmosphere layers + DMs
 constexpr int kGeomWarps = 8;     // subapertures per CTA
 constexpr int kGeomMaxW = 36;     // window side (nxsa + 2)
-constexpr int kGeomChunk = 13;   // window points per lane per pass
+constexpr int kGeomRows = 12;    // window rows per band (OPD in registers)
 constexpr int kGeomBlk = 16;     // layer pixels a window spans across, at most
 constexpr int kGeomBlkStride = kGeomBlk + 1;
 constexpr int kGeomHStride = kGeomMaxW;
@@ -120,30 +120,37 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
         sbase[wid][lane] = make_int4((int)iu, (int)iv, __float_as_int((float)(u - fu)), __float_as_int((float)(v - fv)));
     }
     __syncwarp();
-    const float inv_wn = 1.0f / (float)wn;
     const float *__restrict__ w = st + st_off[sa_st[gi]];
     float *blk = sblk[wid], *hx = shx[wid];
     float gx = 0.f, gy = 0.f;
-    // the window in chunks of kGeomChunk points per lane (OPD in registers)
-    for (int k0 = 0; k0 < npts; k0 += 32 * kGeomChunk) {
-        float opd[kGeomChunk];
+    // Lane c owns window column c (< 32) of a band of kGeomRows rows; the
+    // columns from 32 on (wn > 32: at most 4) are spread over the lanes as
+    // one extra point each.  OPD of the band stays in registers.
+    const int ntail = wn > 32 ? wn - 32 : 0;
+    const bool main_ok = lane < wn;
+    for (int r0 = 0; r0 < wn; r0 += kGeomRows) {
+        const int nr = min(kGeomRows, wn - r0);
+        float opd[kGeomRows];
 #pragma unroll
-        for (int j = 0; j < kGeomChunk; j++) opd[j] = 0.f;
-        const int rlo = k0 / wn, rhi = (min(npts, k0 + 32 * kGeomChunk) - 1) / wn;
+        for (int j = 0; j < kGeomRows; j++) opd[j] = 0.f;
+        float opdt = 0.f;
+        const bool has_tail = lane < nr * ntail;
+        const int tr = has_tail ? r0 + lane / ntail : r0, tc = has_tail ? 32 + lane % ntail : 0;
         for (int s = 0; s < t.nscr; s++) {
             const GeomScr S = t.s[s];
             const int4 b = sbase[wid][s];
             const float sxf = (float)t.c[iw][s].sx, syf = (float)t.c[iw][s].sy;
             const float fu0 = __int_as_float(b.z), fv0 = __int_as_float(b.w);
             const float *__restrict__ P = S.p + (long)inst * S.inst_stride;
-            // the layer pixels this chunk touches: columns 0..nbu-1 and rows
+            // the layer pixels this band touches: columns 0..nbu-1 and rows
             // v0..v0+nbv-1 from the window origin's pixel (the +1 neighbours included)
-            const int v0 = (int)floorf(fmaf((float)rlo, syf, fv0));
-            const int nbv = min((int)floorf(fmaf((float)rhi, syf, fv0)) + 2 - v0, kGeomBlk);
+            const int v0 = (int)floorf(fmaf((float)r0, syf, fv0));
+            const int nbv = min((int)floorf(fmaf((float)(r0 + nr - 1), syf, fv0)) + 2 - v0, kGeomBlk);
             const int nbu = min((int)floorf(fmaf((float)(wn - 1), sxf, fu0)) + 2, kGeomBlk);
+            const float inv_nbu = 1.0f / (float)nbu;
             __syncwarp();  // the previous map's tables are no longer read
             for (int e = lane; e < nbu * nbv; e += 32) {
-                const int bv = e / nbu, bu = e - bv * nbu;
+                const int bv = (int)(((float)e + 0.5f) * inv_nbu), bu = e - bv * nbu;
                 int c = b.x + bu, r = b.y + v0 + bv;
                 float val = 0.f;
                 if (S.wrap) {
@@ -159,44 +166,51 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
             }
             __syncwarp();
             // each block row interpolated along x at every window column
-            for (int e = lane; e < nbv * wn; e += 32) {
-                const int bv = e / wn, cc = e - bv * wn;
-                const float uf = fmaf((float)cc, sxf, fu0), fl = floorf(uf);
+            for (int cc = lane; cc < wn; cc += 32) {
+                const float uf = fmaf((float)cc, sxf, fu0), fl = floorf(uf), ax = uf - fl;
                 const int lu = (int)fl;
-                const float m0 = blk[bv * kGeomBlkStride + lu], m1 = blk[bv * kGeomBlkStride + lu + 1];
-                float hv = fmaf(m1 - m0, uf - fl, m0);
-                if (!S.wrap) {
-                    const int c = b.x + lu;
-                    if (c < 0 || c >= S.nx) hv = 0.f;  // off the map: no contribution
+                const bool ok = S.wrap || (b.x + lu >= 0 && b.x + lu < S.nx);  // off the map: no contribution
+                for (int bv = 0; bv < nbv; bv++) {
+                    const float m0 = blk[bv * kGeomBlkStride + lu], m1 = blk[bv * kGeomBlkStride + lu + 1];
+                    hx[bv * kGeomHStride + cc] = ok ? fmaf(m1 - m0, ax, m0) : 0.f;
                 }
-                hx[bv * kGeomHStride + cc] = hv;
             }
             __syncwarp();
-            // every point of the chunk: along y between two of those rows
+            // every point of the band: along y between two of those rows
 #pragma unroll
-            for (int j = 0; j < kGeomChunk; j++) {
-                const int k = k0 + lane + 32 * j;
-                if (k < npts) {
-                    const int r = (int)(((float)k + 0.5f) * inv_wn), cc = k - r * wn;
-                    const float vf = fmaf((float)r, syf, fv0), flv = floorf(vf);
+            for (int j = 0; j < kGeomRows; j++) {
+                if (j < nr && main_ok) {
+                    const float vf = fmaf((float)(r0 + j), syf, fv0), flv = floorf(vf);
                     const int lv = (int)flv - v0;
-                    if (lv < 0 || lv + 1 >= nbv) continue;  // never taken: the block covers the chunk
-                    if (!S.wrap) {
-                        const int iv = b.y + (int)flv;
-                        if (iv < 0 || iv >= S.ny) continue;  // off the map: no contribution
+                    const bool rok = S.wrap || (b.y + (int)flv >= 0 && b.y + (int)flv < S.ny);
+                    if (rok && lv >= 0 && lv + 1 < nbv) {
+                        const float h0 = hx[lv * kGeomHStride + lane], h1 = hx[(lv + 1) * kGeomHStride + lane];
+                        opd[j] = fmaf(S.alpha, fmaf(h1 - h0, vf - flv, h0), opd[j]);
                     }
-                    const float h0 = hx[lv * kGeomHStride + cc], h1 = hx[(lv + 1) * kGeomHStride + cc];
-                    opd[j] = fmaf(S.alpha, fmaf(h1 - h0, vf - flv, h0), opd[j]);
+                }
+            }
+            if (has_tail) {
+                const float vf = fmaf((float)tr, syf, fv0), flv = floorf(vf);
+                const int lv = (int)flv - v0;
+                const bool rok = S.wrap || (b.y + (int)flv >= 0 && b.y + (int)flv < S.ny);
+                if (rok && lv >= 0 && lv + 1 < nbv) {
+                    const float h0 = hx[lv * kGeomHStride + tc], h1 = hx[(lv + 1) * kGeomHStride + tc];
+                    opdt = fmaf(S.alpha, fmaf(h1 - h0, vf - flv, h0), opdt);
                 }
             }
         }
 #pragma unroll
-        for (int j = 0; j < kGeomChunk; j++) {
-            const int k = k0 + lane + 32 * j;
-            if (k < npts) {
+        for (int j = 0; j < kGeomRows; j++) {
+            if (j < nr && main_ok) {
+                const int k = (r0 + j) * wn + lane;
                 gx = fmaf(__ldg(w + k), opd[j], gx);
                 gy = fmaf(__ldg(w + npts + k), opd[j], gy);
             }
+        }
+        if (has_tail) {
+            const int k = tr * wn + tc;
+            gx = fmaf(__ldg(w + k), opdt, gx);
+            gy = fmaf(__ldg(w + npts + k), opdt, gy);
         }
     }
 #pragma unroll
