@@ -90,6 +90,7 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
     __shared__ int4 sbase[kGeomWarps][kGeomMaxScr];
     __shared__ float sblk[kGeomWarps][kGeomBlk * kGeomBlkStride];
     __shared__ float shx[kGeomWarps][kGeomBlk * kGeomHStride];
+    __shared__ float2 srow[kGeomWarps][kGeomRows];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int iw = blockIdx.y, inst = blockIdx.z;
     const GeomWfsT &W = t.w[iw];
@@ -147,7 +148,7 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
             const int v0 = (int)floorf(fmaf((float)r0, syf, fv0));
             const int nbv = min((int)floorf(fmaf((float)(r0 + nr - 1), syf, fv0)) + 2 - v0, kGeomBlk);
             const int nbu = min((int)floorf(fmaf((float)(wn - 1), sxf, fu0)) + 2, kGeomBlk);
-            const float inv_nbu = 1.0f / (float)nbu;
+            const float inv_nbu = __frcp_rn((float)nbu);
             __syncwarp();  // the previous map's tables are no longer read
             for (int e = lane; e < nbu * nbv; e += 32) {
                 const int bv = (int)(((float)e + 0.5f) * inv_nbu), bu = e - bv * nbu;
@@ -175,27 +176,34 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
                     hx[bv * kGeomHStride + cc] = ok ? fmaf(m1 - m0, ax, m0) : 0.f;
                 }
             }
+            // each band row's pair of interpolated rows (offset in hx, -1 when
+            // the row is off the map) and its fraction along y
+            if (lane < nr) {
+                const float vf = fmaf((float)(r0 + lane), syf, fv0), flv = floorf(vf);
+                const int lv = (int)flv - v0;
+                const bool rok = S.wrap || (b.y + (int)flv >= 0 && b.y + (int)flv < S.ny);
+                srow[wid][lane] = make_float2(__int_as_float(rok && lv >= 0 && lv + 1 < nbv ? lv * kGeomHStride : -1),
+                                              vf - flv);
+            }
             __syncwarp();
             // every point of the band: along y between two of those rows
 #pragma unroll
             for (int j = 0; j < kGeomRows; j++) {
                 if (j < nr && main_ok) {
-                    const float vf = fmaf((float)(r0 + j), syf, fv0), flv = floorf(vf);
-                    const int lv = (int)flv - v0;
-                    const bool rok = S.wrap || (b.y + (int)flv >= 0 && b.y + (int)flv < S.ny);
-                    if (rok && lv >= 0 && lv + 1 < nbv) {
-                        const float h0 = hx[lv * kGeomHStride + lane], h1 = hx[(lv + 1) * kGeomHStride + lane];
-                        opd[j] = fmaf(S.alpha, fmaf(h1 - h0, vf - flv, h0), opd[j]);
+                    const float2 q = srow[wid][j];
+                    const int off = __float_as_int(q.x);
+                    if (off >= 0) {
+                        const float h0 = hx[off + lane], h1 = hx[off + kGeomHStride + lane];
+                        opd[j] = fmaf(S.alpha, fmaf(h1 - h0, q.y, h0), opd[j]);
                     }
                 }
             }
             if (has_tail) {
-                const float vf = fmaf((float)tr, syf, fv0), flv = floorf(vf);
-                const int lv = (int)flv - v0;
-                const bool rok = S.wrap || (b.y + (int)flv >= 0 && b.y + (int)flv < S.ny);
-                if (rok && lv >= 0 && lv + 1 < nbv) {
-                    const float h0 = hx[lv * kGeomHStride + tc], h1 = hx[(lv + 1) * kGeomHStride + tc];
-                    opdt = fmaf(S.alpha, fmaf(h1 - h0, vf - flv, h0), opdt);
+                const float2 q = srow[wid][tr - r0];
+                const int off = __float_as_int(q.x);
+                if (off >= 0) {
+                    const float h0 = hx[off + tc], h1 = hx[off + kGeomHStride + tc];
+                    opdt = fmaf(S.alpha, fmaf(h1 - h0, q.y, h0), opdt);
                 }
             }
         }
