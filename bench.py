@@ -314,6 +314,53 @@ def wfs_rates(sysm, fit, batch: int, stream, cpu: bool = True):
     return res
 
 
+def closed_loop_rates(sysm, fit, R, batch: int, stream, nstep: int = 20):
+    """The whole loop on the device for ``batch`` instances: geometric WFS
+    (through the DMs, noise on) -> tomography + fit (the graph step of R) ->
+    servo (type I, gain 0.5) -> DM commands, per step; CUDA events around
+    ``nstep`` steps after 3 warm-up steps."""
+    import torch
+    from maos_b200 import wfs_setup
+    from maos_b200.servo import Servo
+    from maos_b200.turbulence import FrozenFlowAtmosphere
+    from maos_b200.wfs import GeomWfs
+    nact = int(fit.nact)
+    atms = [FrozenFlowAtmosphere(sysm.cfg, 200 + i) for i in range(4)]
+    W = GeomWfs.for_system(sysm, [atms[i % 4] for i in range(batch)], fit=fit, nbatch=batch,
+                           geom=wfs_setup.build_geom_wfs(sysm))
+    S = Servo(batch * nact, ep=[[0.5]], dt=sysm.cfg.sim_dt)
+    dm = torch.zeros(batch, nact, dtype=torch.float32, device="cuda")
+    fa = torch.zeros(batch, nact, dtype=torch.float32, device="cuda")
+    R.reset()
+    sp = stream.cuda_stream
+
+    def step(k):
+        g = W.grad(k, dm=dm, seed=1, stream=stream)
+        R.step_device(g.data_ptr(), sp)
+        for i in range(batch):
+            R.slot_download(i, fa[i].data_ptr(), sp)
+        cmd = S.filter(fa.view(-1).double(), stream=stream)
+        dm.copy_(cmd.view(batch, nact))
+
+    with torch.cuda.stream(stream):
+        for k in range(3):
+            step(k)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(3, 3 + nstep):
+            step(k)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / nstep
+    W.close()
+    S.close()
+    R.reset()
+    return {"instances": batch, "ms_per_step": ms, "steps_per_s": batch * 1000.0 / ms,
+            "step": "mb_geom_wfs_grad -> mb_recon_step_device -> mb_servo_filter -> DM commands, no host copy",
+            "data": "seeded von Karman layers with frozen flow (4 seeds over the instances), noise on"}
+
+
 SERVE_MIX = (("scao_8m", 26), ("ltao_8m", 26), ("mcao_30m", 12))
 
 
@@ -536,6 +583,8 @@ def run_gpu(args):
     wfs_line = wfs_rates(sysm, fit, B, stream, cpu=(rank == 0 and not args.no_cpu_baseline)) \
         if world == 1 and not args.no_wfs else None
 
+    loop_line = closed_loop_rates(sysm, fit, R, B, stream) if world == 1 and not args.no_wfs else None
+
     served = served_mvm = None
     if world == 1 and not args.no_serve and args.serve_seconds > 0:
         served = served_mix(args.serve_seconds, mcao_frames=fr[0])
@@ -571,6 +620,7 @@ def run_gpu(args):
                         "fp64_gpu_tomo_gpu_fit_steps_per_s": fp64_api_value},
                 "mvm": mvm_line,
                 "wfs_gradients": wfs_line,
+                "closed_loop": loop_line,
                 "served": served,
                 "served_mvm": served_mvm,
                 "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
