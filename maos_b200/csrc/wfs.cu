@@ -38,7 +38,8 @@ constexpr int kGeomMaxWfs = 16;
 constexpr int kGeomMaxScr = 16;   // atmosphere layers + DMs
 constexpr int kGeomWarps = 8;     // subapertures per CTA
 constexpr int kGeomMaxW = 36;     // window side (nxsa + 2)
-constexpr int kGeomRows = 12;    // window rows per band (OPD in registers)
+constexpr int kGeomRows = 17;    // window rows per band (OPD in registers)
+constexpr int kGeomTail = (kGeomRows * (kGeomMaxW - 32) + 31) / 32;  // points of columns >= 32 per lane
 constexpr int kGeomBlk = 16;     // layer pixels a window spans across, at most
 constexpr int kGeomBlkStride = kGeomBlk + 1;
 constexpr int kGeomHStride = kGeomMaxW;
@@ -125,8 +126,9 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
     float *blk = sblk[wid], *hx = shx[wid];
     float gx = 0.f, gy = 0.f;
     // Lane c owns window column c (< 32) of a band of kGeomRows rows; the
-    // columns from 32 on (wn > 32: at most 4) are spread over the lanes as
-    // one extra point each.  OPD of the band stays in registers.
+    // points of the columns from 32 on (wn > 32: at most 4 columns) are dealt
+    // out over the lanes, kGeomTail at most each.  OPD of the band stays in
+    // registers.
     const int ntail = wn > 32 ? wn - 32 : 0;
     const bool main_ok = lane < wn;
     for (int r0 = 0; r0 < wn; r0 += kGeomRows) {
@@ -134,9 +136,14 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
         float opd[kGeomRows];
 #pragma unroll
         for (int j = 0; j < kGeomRows; j++) opd[j] = 0.f;
-        float opdt = 0.f;
-        const bool has_tail = lane < nr * ntail;
-        const int tr = has_tail ? r0 + lane / ntail : r0, tc = has_tail ? 32 + lane % ntail : 0;
+        float opdt[kGeomTail];
+        int tpk[kGeomTail];  // band row << 8 | column of each tail point, -1: none
+#pragma unroll
+        for (int q = 0; q < kGeomTail; q++) {
+            const int tp = lane + 32 * q;
+            opdt[q] = 0.f;
+            tpk[q] = tp < nr * ntail ? (tp / ntail) << 8 | (32 + tp % ntail) : -1;
+        }
         for (int s = 0; s < t.nscr; s++) {
             const GeomScr S = t.s[s];
             const int4 b = sbase[wid][s];
@@ -198,12 +205,16 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
                     }
                 }
             }
-            if (has_tail) {
-                const float2 q = srow[wid][tr - r0];
-                const int off = __float_as_int(q.x);
-                if (off >= 0) {
-                    const float h0 = hx[off + tc], h1 = hx[off + kGeomHStride + tc];
-                    opdt = fmaf(S.alpha, fmaf(h1 - h0, q.y, h0), opdt);
+#pragma unroll
+            for (int q = 0; q < kGeomTail; q++) {
+                if (tpk[q] >= 0) {
+                    const int tc = tpk[q] & 255;
+                    const float2 rq = srow[wid][tpk[q] >> 8];
+                    const int off = __float_as_int(rq.x);
+                    if (off >= 0) {
+                        const float h0 = hx[off + tc], h1 = hx[off + kGeomHStride + tc];
+                        opdt[q] = fmaf(S.alpha, fmaf(h1 - h0, rq.y, h0), opdt[q]);
+                    }
                 }
             }
         }
@@ -215,10 +226,13 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
                 gy = fmaf(__ldg(w + npts + k), opd[j], gy);
             }
         }
-        if (has_tail) {
-            const int k = tr * wn + tc;
-            gx = fmaf(__ldg(w + k), opdt, gx);
-            gy = fmaf(__ldg(w + npts + k), opdt, gy);
+#pragma unroll
+        for (int q = 0; q < kGeomTail; q++) {
+            if (tpk[q] >= 0) {
+                const int k = (r0 + (tpk[q] >> 8)) * wn + (tpk[q] & 255);
+                gx = fmaf(__ldg(w + k), opdt[q], gx);
+                gy = fmaf(__ldg(w + npts + k), opdt[q], gy);
+            }
         }
     }
 #pragma unroll

@@ -154,3 +154,26 @@ def test_loop_closes_on_the_device():
     R.close()
     S.close()
     W.close()
+
+
+def test_widest_subaperture_window_matches_oracle():
+    """34 OPD points across a subaperture (the widest window, 36 x 36: four
+    columns beyond the warp's 32 lanes)."""
+    from conftest import get_fit, get_system
+    from maos_b200 import wfs_setup
+    from maos_b200.turbulence import FrozenFlowAtmosphere
+    from maos_b200.wfs import GeomWfs
+    from oracle import wfs_oracle
+    s = get_system("scao_8m")
+    fit = get_fit("scao_8m")
+    geom = wfs_setup.build_geom_wfs(s, sim_dx=s.wfs[0].dsa / 34)
+    assert geom.powfs[0].nxsa == 34
+    atm = FrozenFlowAtmosphere(s.cfg, 6)
+    W = GeomWfs.for_system(s, atm, fit=fit, geom=geom)
+    import torch
+    a = (np.random.default_rng(4).standard_normal(fit.nact) * 1e-7).astype(np.float32)
+    g = W.grad(9, dm=torch.as_tensor(a, device="cuda")[None, :], seed=3).cpu().numpy()[0]
+    layers, dms = _screens(atm, a.astype(np.float64), fit)
+    ref = wfs_oracle.geom_grads(geom, layers, dms, 9, s.cfg.sim_dt, seed=3)
+    assert rel(g, ref) < TOL
+    W.close()
