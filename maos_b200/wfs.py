@@ -16,8 +16,7 @@ the fit's actuator order) is subtracted.  The tables come from
 from __future__ import annotations
 
 import ctypes as C
-import math
-from typing import List, Optional, Sequence
+from typing import Optional, Sequence
 
 import numpy as np
 

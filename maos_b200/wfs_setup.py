@@ -22,7 +22,6 @@ subapertures needs a few hundred).
 """
 from __future__ import annotations
 
-import math
 from dataclasses import dataclass
 from typing import List
 

@@ -1,7 +1,6 @@
 """Geometric-WFS oracle and tables on the CPU: the noise generator against the
 published Philox4x32-10 known answers, the stencils' structure, and the
 oracle's gradients of known wavefronts."""
-import math
 
 import numpy as np
 import pytest
