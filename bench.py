@@ -330,16 +330,14 @@ def closed_loop_rates(sysm, fit, R, batch: int, stream, nstep: int = 20):
                            geom=wfs_setup.build_geom_wfs(sysm))
     S = Servo(batch * nact, ep=[[0.5]], dt=sysm.cfg.sim_dt)
     dm = torch.zeros(batch, nact, dtype=torch.float32, device="cuda")
-    fa = torch.zeros(batch, nact, dtype=torch.float32, device="cuda")
+    fa = R.fit_solution()   # the fit's commands, in place on the device
     R.reset()
     sp = stream.cuda_stream
 
     def step(k):
         g = W.grad(k, dm=dm, seed=1, stream=stream)
         R.step_device(g.data_ptr(), sp)
-        for i in range(batch):
-            R.slot_download(i, fa[i].data_ptr(), sp)
-        cmd = S.filter(fa.view(-1).double(), stream=stream)
+        cmd = S.filter(fa.reshape(-1).double(), stream=stream)
         dm.copy_(cmd.view(batch, nact))
 
     with torch.cuda.stream(stream):

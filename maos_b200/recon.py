@@ -205,6 +205,20 @@ class Reconstructor:
     def fit_solution_ptr(self) -> int:
         return int(self.lib.mb_fit_solution(self.h))
 
+    def fit_solution(self):
+        """The fit's DM commands of every instance as a torch CUDA float32
+        view [nbatch, nact] of the reconstructor's own buffer (no copy; valid
+        until the next step overwrites it or the reconstructor is closed)."""
+        import torch
+        ptr = self.fit_solution_ptr()
+        if not ptr:
+            raise RuntimeError("reconstructor has no DM fit")
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (self.nbatch, self.nact), "typestr": "<f4",
+                                        "data": (ptr, False), "version": 2, "strides": None}
+        return torch.as_tensor(_View(), device=f"cuda:{torch.cuda.current_device()}")
+
     # serving: instances as slots (no counterpart in the reference)
     def reset_slot(self, slot: int, stream_ptr: int = 0):
         check(self.lib.mb_recon_reset_slot(self.h, int(slot), C.c_void_p(stream_ptr)), "mb_recon_reset_slot")

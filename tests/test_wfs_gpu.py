@@ -144,7 +144,10 @@ def test_loop_closes_on_the_device():
         g = W.grad(0, dm=dm)
         rms.append(float(g.norm()))
         R.step_device(g.data_ptr(), st.cuda_stream)
-        R.slot_download(0, fa.data_ptr(), st.cuda_stream)
+        if k % 2:   # the commands through a copy, or in place on the device
+            R.slot_download(0, fa.data_ptr(), st.cuda_stream)
+        else:
+            fa.copy_(R.fit_solution()[0])
         cmd = S.filter(fa.double(), stream=st)
         dm.copy_(cmd.float()[None, :])
     torch.cuda.synchronize()
