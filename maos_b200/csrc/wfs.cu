@@ -44,6 +44,11 @@ constexpr int kGeomBlk = 16;     // layer pixels a window spans across, at most
 constexpr int kGeomBlkStride = kGeomBlk + 1;
 constexpr int kGeomHStride = kGeomMaxW;
 constexpr double kGeomMaxStep = (kGeomBlk - 3.0) / (kGeomMaxW - 1.0);  // layer pixels per fine-grid step
+// shared-memory bounds the kernel relies on: a band's pixel block is at most
+// kGeomBlk x kGeomBlk, its interpolated rows fit the kGeomBlk x kGeomHStride
+// table, and a tail point's band row fits the 8 bits it is packed in
+static_assert(kGeomMaxStep * (kGeomMaxW - 1) + 3 <= kGeomBlk, "window wider than the pixel block");
+static_assert(kGeomRows <= kGeomMaxW && kGeomRows < 256, "band rows");
 
 struct GeomScr {
     const float *p;    // [ny][nx], x fastest
@@ -185,12 +190,12 @@ k_wfs_geom(const __grid_constant__ GeomTab t, const int *__restrict__ sa_ix, con
             }
             // each band row's pair of interpolated rows (offset in hx, -1 when
             // the row is off the map) and its fraction along y
-            if (lane < nr) {
-                const float vf = fmaf((float)(r0 + lane), syf, fv0), flv = floorf(vf);
+            for (int rr = lane; rr < nr; rr += 32) {  // every band row, whatever kGeomRows is
+                const float vf = fmaf((float)(r0 + rr), syf, fv0), flv = floorf(vf);
                 const int lv = (int)flv - v0;
                 const bool rok = S.wrap || (b.y + (int)flv >= 0 && b.y + (int)flv < S.ny);
-                srow[wid][lane] = make_float2(__int_as_float(rok && lv >= 0 && lv + 1 < nbv ? lv * kGeomHStride : -1),
-                                              vf - flv);
+                srow[wid][rr] = make_float2(__int_as_float(rok && lv >= 0 && lv + 1 < nbv ? lv * kGeomHStride : -1),
+                                            vf - flv);
             }
             __syncwarp();
             // every point of the band: along y between two of those rows
