@@ -69,3 +69,29 @@ def test_oracle_gradients_of_a_tilted_layer(ltao_geom):
         scale = 1.0
         assert np.allclose(gw[:nsa][full], 1e-6 * scale, rtol=1e-9)
         assert np.allclose(gw[nsa:][full], 0.0, atol=1e-15)
+
+
+def test_tables_and_ray_tracing_match_golden_vectors():
+    """Against the reference's own GS0, amplitude and prop_grid of a small
+    partially illuminated pupil (tests/golden/make_wfs_golden.py)."""
+    import os
+    import scipy.sparse as sps
+    from maos_b200 import wfs_setup
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "wfs_cases.npz"))
+    D, DIN, DSA, NXSA = z["params"]
+    P = wfs_setup.build_geom_powfs(z["salocx"], z["salocy"], float(DSA), float(DSA) / int(NXSA), float(D), float(DIN))
+    assert P.nxsa == int(NXSA)
+    gx = np.rint((z["locx"] - P.grid.ox) / P.grid.dx).astype(np.int64)
+    gy = np.rint((z["locy"] - P.grid.oy) / P.grid.dy).astype(np.int64)
+    col = gy * P.grid.nx + gx
+    assert np.array_equal(P.amp.ravel()[col], z["amp"])
+    nr, nc = z["gs0_shape"]
+    Gref = sps.csc_matrix((z["gs0_x"], z["gs0_i"], z["gs0_p"]), shape=(int(nr), int(nc)))
+    G = P.gs0()
+    assert G.nnz == Gref.nnz
+    d = (G[:, col] - Gref).tocoo()
+    assert (np.abs(d.data).max() if d.nnz else 0.0) <= 1e-14 * np.abs(Gref.data).max()
+    nx, ny, dx, ox, oy = z["grid"]
+    for wrap, key in ((True, "prop_wrap"), (False, "prop_nowrap")):
+        ours = wfs_oracle.prop_grid(z["screen"], ox, oy, dx, z["px"], z["py"], 0.8, 0.4, -0.9, 0.9, wrap)
+        assert np.abs(ours - z[key]).max() <= 1e-13 * np.abs(z[key]).max()
