@@ -359,6 +359,42 @@ def closed_loop_rates(sysm, fit, R, batch: int, stream, nstep: int = 20):
             "data": "seeded von Karman layers with frozen flow (4 seeds over the instances), noise on"}
 
 
+def single_instance_rates(preset: str, nsteps: int = 200, warmup: int = 5):
+    """One instance alone: the plain single-instance FP32 path (graph step of
+    tomography + fit, gradients resident) with per-step CUDA events and the
+    L2 flushed before every step; steps/s and p50/p99 step latency."""
+    import numpy as np
+    import torch
+    from maos_b200 import config, fit_setup, geometry, turbulence
+    from maos_b200.recon import Reconstructor
+    sysm = geometry.build_tomo(config.PRESETS[preset]())
+    fit = fit_setup.build_fit(sysm)
+    frames = turbulence.gradient_frames(sysm, seed=1, nframe=4)
+    g = torch.tensor(frames, dtype=torch.float32, device="cuda")
+    R = Reconstructor(sysm, nbatch=1, fit=fit)
+    rows, _ = R.autotune(reps=20)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+    with torch.cuda.stream(stream):
+        for k in range(warmup):
+            R.step_device(g[k % 4].data_ptr(), sp)
+        for k in range(nsteps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            R.step_device(g[k % 4].data_ptr(), sp)
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    t = sorted(a.elapsed_time(b) for a, b in ev)
+    R.close()
+    return {"instances": 1, "steps": nsteps, "steps_per_s": 1000.0 * nsteps / sum(t),
+            "latency_ms": {"p50": statistics.median(t), "p99": t[min(nsteps - 1, int(math.ceil(0.99 * nsteps)) - 1)],
+                           "max": t[-1]},
+            "pupil_rows": rows, "tomo": f"{'FDPCG' if sysm.cfg.tomo_precond else 'CG'} {sysm.cfg.tomo_maxit} it",
+            "fit_it": fit.maxit}
+
+
 SERVE_MIX = (("scao_8m", 26), ("ltao_8m", 26), ("mcao_30m", 12))
 
 
@@ -542,26 +578,34 @@ def run_gpu(args):
         R.fit()
     fp64_api_value = B * K2 / (time.perf_counter() - t0)
 
-    # roofline of the dominant kernel (live timing on the reconstructor's stream)
+    # roofline of every kernel of a CG iteration and of the dominant one (live
+    # CUDA-event timing on the reconstructor's stream; algorithmic bytes per
+    # launch with the tables the instances share counted once per launch)
     ns = lib.mb_num_stages()
     import ctypes as C
     ms = (C.c_float * ns)()
     by = (C.c_double * ns)()
     lp = (C.c_int * ns)()
     native.check(lib.mb_time_stages(R.h, 20, ms, by, lp), "mb_time_stages")
+    peak, peak_kind = measured_peaks()
     stages = []
     for i in range(ns):
-        stages.append({"name": lib.mb_stage_name(i).decode(), "ms": ms[i], "bytes": by[i],
-                       "launches": lp[i], "share_ms": ms[i] * lp[i]})
+        if lp[i] <= 0 or ms[i] <= 0:
+            continue
+        gbs = by[i] / (ms[i] / 1000.0) / 1e9
+        stages.append({"name": lib.mb_stage_name(i).decode(), "ms_per_launch": ms[i], "bytes_per_launch": by[i],
+                       "launches_per_step": lp[i], "share_ms": ms[i] * lp[i], "achieved_gbs": gbs,
+                       "frac": gbs / peak})
     tot_stage = sum(s["share_ms"] for s in stages) or 1.0
     dom = max(stages, key=lambda s: s["share_ms"])
-    peak, peak_kind = measured_peaks()
-    achieved = dom["bytes"] / (dom["ms"] / 1000.0) / 1e9
-    roof = {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak,
-            "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+    roof = {"bound": "hbm", "kernel": dom["name"], "achieved": dom["achieved_gbs"], "peak": peak,
+            "unit": "GB/s", "frac": dom["frac"], "peak_source": peak_kind,
             "traffic": ncu_traffic(dom["name"], B),
+            "bytes_per_launch": dom["bytes_per_launch"], "ms_per_launch": dom["ms_per_launch"],
             "share_of_step": dom["share_ms"] / tot_stage,
-            "stage_ms_per_step": {s["name"]: round(s["share_ms"], 4) for s in stages}}
+            "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in s.items()} for s in stages],
+            "note": "instances' working set is L2-resident: latency-bound kernels, fractions of the HBM copy "
+                    "bandwidth are low by construction"}
 
     # control matrix of this system (batched cold solves of unit gradients,
     # 256 per launch) and the storage precision of its MVM on frozen flow
@@ -582,6 +626,10 @@ def run_gpu(args):
         if world == 1 and not args.no_wfs else None
 
     loop_line = closed_loop_rates(sysm, fit, R, B, stream) if world == 1 and not args.no_wfs else None
+
+    single = None
+    if world == 1:
+        single = {name: single_instance_rates(name) for name in ("mcao_30m", "ltao_8m")}
 
     served = served_mvm = None
     if world == 1 and not args.no_serve and args.serve_seconds > 0:
@@ -611,6 +659,7 @@ def run_gpu(args):
                            "autotune": {"pupil_rows": tuned_rows,
                                         "lhs_ms_by_rows": {str(k): round(v, 4) for k, v in tuned_ms.items()}}},
                 "latency_ms": {"p50": p50, "p99": p99, "note": "one batched step of all instances"},
+                "single_instance": single,
                 "e2e": {"value": e2e_value, "unit": "steps/s",
                         "h2d_bytes_per_step": int(B * sysm.ngrad * 4),
                         "d2h_bytes_per_step": int(B * fit.nact * 4),

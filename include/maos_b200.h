@@ -8,8 +8,8 @@
  * (cuda/gpu.h); the citation is given beside each declaration.  The
  * reference passes its simulator structs (PARMS_T, RECON_T, SIM_T); this ABI
  * takes the same information as flat arrays, so the glue a maintainer adds to
- * maos copies fields out of RECON_T into the descriptors
- * below.
+ * maos (the gpu_* functions of glue/maos_gpu_glue.c) copies fields out of
+ * RECON_T into the descriptors below.
  *
  * Conventions (same as the reference's dmat / map_t / dsp):
  *   - grids: point (ix, iy) sits at (ox + ix*dx, oy + iy*dy), stored at

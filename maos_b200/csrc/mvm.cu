@@ -568,12 +568,16 @@ int mb_mvm_apply_noalloc(const float *d_M, long nact, long ngrad, long ldm, cons
                       "M 16-byte aligned)");
         return MB_EINVAL;
     }
+    // bound each factor before multiplying, so the product cannot overflow
     const long nks = (ngrad + mb::kK - 1) / mb::kK;
-    const long need = nks * (long)nbatch * nact;
-    if (need > MB_NOALLOC_MAX_PARTIALS) {
-        mb::set_error("mb_mvm_apply_noalloc: needs %ld partial sums (%ld K slabs x %d instances x %ld "
-                      "rows); the static scratch holds %d",
-                      need, nks, nbatch, nact, (int)MB_NOALLOC_MAX_PARTIALS);
+    const bool too_big = nact > MB_NOALLOC_MAX_PARTIALS || nks > MB_NOALLOC_MAX_PARTIALS ||
+                         nbatch > MB_NOALLOC_MAX_PARTIALS ||
+                         nks * (long)nbatch > MB_NOALLOC_MAX_PARTIALS / nact;
+    const long need = too_big ? -1 : nks * (long)nbatch * nact;
+    if (too_big || need > MB_NOALLOC_MAX_PARTIALS) {
+        mb::set_error("mb_mvm_apply_noalloc: needs %ld K slabs x %d instances x %ld rows of partial "
+                      "sums; the static scratch holds %d",
+                      nks, nbatch, nact, (int)MB_NOALLOC_MAX_PARTIALS);
         return MB_EINVAL;
     }
     try {

@@ -1188,7 +1188,11 @@ void Recon::build_fit(const mb_fit_desc *f) {
     fcnt.zero_async(stream);
 }
 
-// Time each iteration stage alone and report its algorithmic traffic.
+// Time each kernel of a CG iteration alone and report its algorithmic
+// traffic per launch: every per-instance operand once per instance, and every
+// table the instances share (ray-tracing lists, WFS stencils and NEA, the
+// FDPCG blocks and their member index) once per launch, since one launch
+// reads it for all nb instances.
 void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     const int ns = mb_num_stages();
     set_mask(nullptr, stream);
@@ -1203,44 +1207,60 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     }
     const double nx = (double)nxtot;
     const double trow = (double)nwfs * tw;  // row-buffer floats per instance
-    const double nbk = (double)fd_nbh * fd_bs;
-    double nh = 0;  // half-spectrum bins per instance
+    const double nbk = (double)fd_nbh * fd_bs;  // block members (spectrum bins read by k_fd_mul)
+    double nh = 0;                              // half-spectrum bins per instance
     for (int l = 0; l < nps; l++) nh += (double)lay_h[l].ny * (lay_h[l].nx / 2 + 1);
-    // bytes per launch: each operand read or written once (the row buffer is
-    // an operand of both halves; the halo rows of the pupil blocks are not)
-    (void)nh;
-    double by[5] = {
-        B * (F * nx + F * trow) + (double)hx.fwd.n * 12.0 + tab_wfs + (double)xpad.n * 8.0,  // x -> t
-        B * (F * trow + 2 * F * nx) + (double)ypad.n * 8.0,                                // t, p -> Ap
-        B * (5 * F * nx),                                              // x,r,p,Ap r/w
-        B * (3 * F * nx),                                              // p,z -> p
-        B * ((fd_cluster ? 4 : 3) * F * nx + 8.0 * nbk * fd_bs + 16.0 * nbk)};  // r (twice), z or p r/w, M, idx
-    // with the preconditioner, the x/r update of all but the last iteration
-    // runs inside fd_fwd (timed here without it), and with the clustered
-    // inverse the p update runs inside fd_inv (timed here with it)
+    const double by[7] = {
+        B * (F * nx + F * trow) + (double)hx.fwd.n * sizeof(AxisW) + tab_wfs + (double)xpad.n * sizeof(GatherW),
+        B * (F * trow + 2 * F * nx) + (double)ypad.n * sizeof(GatherW),       // t, p -> Ap
+        B * (6 * F * nx),                                                    // x,r,p,Ap read; x,r written
+        B * (3 * F * nx),                                                    // p,z read; p written
+        B * (6 * F * nx + 8.0 * nh),                          // x,r,p,Ap read; x,r written; spectrum written
+        B * (2 * 8.0 * nbk) + 8.0 * fd_bs * fd_bs * fd_nbh + (double)sizeof(FdIndex) * nbk,  // X, Y; M, idx once
+        B * (8.0 * nh + (fd_cluster ? 3 : 2) * F * nx)};      // spectrum, r read; p read+written (or z written)
+    // launches per step: with the preconditioner the x/r update of all but
+    // the last iteration runs inside k_fd_fwd (timed with it), and with the
+    // clustered inverse the p update runs inside k_fd_inv (timed with it)
     const bool pin = precond && fd_cluster;
-    const int lps[5] = {maxit + 2, maxit + 2, precond ? 1 : maxit, pin ? 0 : maxit, precond ? maxit : 0};
+    const int lps[7] = {maxit + 2, maxit + 2, precond ? 1 : maxit, pin ? 0 : maxit, precond ? maxit : 0,
+                        precond ? maxit : 0, precond ? maxit : 0};
+    const int per = kThreads / std::max(fd_bs, 1);
     for (int st = 0; st < ns; st++) {
         bytes[st] = by[st];
         launches[st] = lps[st];
         ms[st] = 0.f;
         if (st >= 4 && !precond) continue;
+        // the vectors written here are scratch (z, rhs, spectra): the warm
+        // start in x, r and p is left as it was
         auto run_stage = [&]() {
             switch (st) {
                 case 0: pupil_rows(true, p.p, stream); break;
                 case 1: hxt_rows(p.p, Ap.p, pap_part.p, 1, 0, stream); break;
                 case 2:
-                    // alpha reads the current scalars; the vectors are scratch here
-                    // the vectors are scratch here (x, r -> z, rhs)
-                    launch(k_cg_update_xr, dim3(nblk_x, nb), dim3(kThreads), 0, stream, z.p, rhs.p, p.p, Ap.p, rr_part.p,
-                                                                             nxtot, scal(), 0, maxit, 0, act());
+                    launch(k_cg_update_xr, dim3(nblk_x, nb), dim3(kThreads), 0, stream, z.p, rhs.p, p.p, Ap.p,
+                           rr_part.p, nxtot, scal(), 0, maxit, 0, act());
                     break;
                 case 3:
-                    launch(k_cg_update_p, dim3(nblocks((nxtot + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, stream, rhs.p, z.p, nxtot, scal(), 0, act());
+                    launch(k_cg_update_p, dim3(nblocks((nxtot + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0,
+                           stream, rhs.p, z.p, nxtot, scal(), 0, act());
                     break;
-                case 4:  // as in the CG step (scalars of a scratch iteration; rhs is scratch here)
-                    if (pin) op_fdpcg(r.p, z.p, rz_part.p, stream, 0, 0, true, nullptr, nullptr, nullptr, rhs.p);
-                    else op_fdpcg(r.p, z.p, rz_part.p, stream);
+                case 4:
+                    launch(k_fd_fwd, dim3(nps, nb), dim3(kFftThreads), fd_smem, stream, rhs.p, spec.p, fdtab,
+                           fd_tw.p, nxtot, fd_bufn, z.p, p.p, Ap.p, ab.p, act());
+                    break;
+                case 5:
+                    launch(k_fd_mul, dim3((fd_nbh + per - 1) / per, (nb + kFdInst - 1) / kFdInst), dim3(kThreads),
+                           0, stream, spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh, fd_bs, nb, act());
+                    break;
+                case 6:
+                    if (pin)
+                        launch_cluster(k_fd_inv<true>, dim3(nps, nb), dim3(kFftThreads), fd_smem, stream, nps,
+                                       spec2.p, r.p, z.p, rz_part.p, fdtab, fd_tw.p, nxtot, fd_bufn, scal(), 0, 0,
+                                       act(), rhs.p);
+                    else
+                        launch(k_fd_inv<false>, dim3(nps, nb), dim3(kFftThreads), fd_smem, stream, spec2.p, r.p,
+                               z.p, rz_part.p, fdtab, fd_tw.p, nxtot, fd_bufn, CgScal{}, 0, 0, act(),
+                               (float *)nullptr);
                     break;
             }
         };
@@ -1588,7 +1608,8 @@ int mb_apply_fit_L(mb_recon *h, const double *ain, double *aout) {
 
 void *mb_recon_stream(mb_recon *h) { return h ? (void *)h->R.stream : nullptr; }
 
-static const char *kStageNames[] = {"lhs_pupil", "lhs_layer", "cg_update_xr", "cg_update_p", "fdpcg"};
+static const char *kStageNames[] = {"lhs_pupil", "lhs_layer", "cg_update_xr", "cg_update_p",
+                                    "fd_fwd",    "fd_mul",    "fd_inv"};
 int mb_num_stages(void) { return (int)(sizeof(kStageNames) / sizeof(kStageNames[0])); }
 const char *mb_stage_name(int i) { return (i >= 0 && i < mb_num_stages()) ? kStageNames[i] : ""; }
 

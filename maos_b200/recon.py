@@ -142,6 +142,7 @@ class Reconstructor:
         self.sys = sysm
         self.fit_sys = fit
         self.nbatch = nbatch
+        self.device = int(device)
         d, keep = tomo_desc(sysm, nbatch=nbatch, split=split, maxit=maxit, fit=fit)
         h = C.c_void_p()
         check(self.lib.mb_setup_recon(C.byref(d), C.byref(h)), "mb_setup_recon")
@@ -217,7 +218,7 @@ class Reconstructor:
         class _View:
             __cuda_array_interface__ = {"shape": (self.nbatch, self.nact), "typestr": "<f4",
                                         "data": (ptr, False), "version": 2, "strides": None}
-        return torch.as_tensor(_View(), device=f"cuda:{torch.cuda.current_device()}")
+        return torch.as_tensor(_View(), device=f"cuda:{self.device}")
 
     # serving: instances as slots (no counterpart in the reference)
     def reset_slot(self, slot: int, stream_ptr: int = 0):

@@ -5,8 +5,10 @@ during operation (cudaMalloc can synchronise the device and take unbounded
 time), so mb_mvm_apply_noalloc keeps its split-K partial sums in a static
 device array instead.  This test calls it through the C ABI twice in a row
 and compares each result with mb_mvm_apply_device (an mb_mvm built with FP32
-storage) within the MVM tests' tolerance, 1e-5 relative.  It also checks
-that a request too large for the static array is refused with a message.
+storage) and with the FP64 product of the FP32-rounded matrix and gradients,
+within the MVM tests' tolerance, 1e-5 relative.  It also checks that a request
+too large for the static array is refused with a message, including sizes
+whose product would overflow a 64-bit integer.
 """
 import ctypes as C
 
@@ -42,6 +44,8 @@ def test_noalloc_mvm_matches_allocating_entry_point():
     # the caller owns M, the gradients and the output on the device
     Md = torch.zeros(nact, ldm, dtype=torch.float32, device="cuda")
     Md[:, :ngrad] = torch.tensor(M, dtype=torch.float32, device="cuda")
+    # FP64 product of the FP32-rounded operands
+    want64 = g.double().cpu().numpy() @ M.astype(np.float32).astype(np.float64).T
     for call in range(2):
         out = torch.full((nbatch, nact), float("nan"), device="cuda")
         with torch.cuda.stream(stream):
@@ -52,6 +56,9 @@ def test_noalloc_mvm_matches_allocating_entry_point():
         torch.cuda.synchronize()
         err = (torch.linalg.norm(out - want) / torch.linalg.norm(want)).item()
         assert err < TOL, (call, err)
+        o64 = out.double().cpu().numpy()
+        err64 = np.linalg.norm(o64 - want64) / np.linalg.norm(want64)
+        assert err64 < TOL, (call, err64)
 
 
 def test_noalloc_rejects_requests_beyond_the_static_scratch():
@@ -65,3 +72,8 @@ def test_noalloc_rejects_requests_beyond_the_static_scratch():
                                   C.c_void_p(out.data_ptr()), 1, None)
     assert rc == -1
     assert b"static scratch holds" in lib.mb_last_error_message()
+    # factors whose product overflows a signed 64-bit integer are refused too
+    for nact, ngrad, nb in ((1 << 62, 4, 1), (1 << 40, 1 << 40, 1 << 20), (3, 1 << 62, 1)):
+        rc = lib.mb_mvm_apply_noalloc(C.c_void_p(M.data_ptr()), nact, ngrad, 1 << 62, C.c_void_p(g.data_ptr()),
+                                      C.c_void_p(out.data_ptr()), min(nb, 1 << 30), None)
+        assert rc == -1, (nact, ngrad, nb)
