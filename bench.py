@@ -149,7 +149,11 @@ class RefRunner:
         self.R = refbridge.RefProcess(nthread=self.ncores)
         self.R.call("setup", refbridge.system_desc(sysm, split=1))
         self.R.call("fdpcg_set", sysm.fdpcg.Mbinv, sysm.fdpcg.perm, sysm.fdpcg.scale)
-        if fit is not None:
+        # the assembled fit (the reference default): setup_fit, then muv_solve's FR and pcg on FL
+        self.assembled = fit is not None and hasattr(fit, "FLM")
+        if self.assembled:
+            self.R.call("fit_assemble", refbridge.fit_assembled_desc(fit, sysm.cfg))
+        elif fit is not None:
             self.R.call("fit_setup", refbridge.fit_desc(fit))
         self.x = None
         self.a = None
@@ -159,7 +163,10 @@ class RefRunner:
         g = self.frames[self.k % len(self.frames)]
         b = self.R.call("tomoR", g)
         self.x, _ = self.R.call("pcg", b, self.x, int(self.x is not None), self.maxit, 1)
-        if self.fit_maxit:
+        if self.fit_maxit and self.assembled:
+            fb = self.R.call("fitas_rhs", self.x)
+            self.a, _ = self.R.call("fitas_pcg", fb, self.a, int(self.a is not None), self.fit_maxit)
+        elif self.fit_maxit:
             fb = self.R.call("fitR", self.x)
             self.a, _ = self.R.call("fit_pcg", fb, self.a, int(self.a is not None), self.fit_maxit)
         self.k += 1
@@ -183,9 +190,9 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from maos_b200 import config, fit_setup, geometry, turbulence
+    from maos_b200 import config, fit_assemble, geometry, turbulence
     sysm = geometry.build_tomo(config.PRESETS[WORKLOAD]())
-    fit = fit_setup.build_fit(sysm)
+    fit = fit_assemble.build_fit_assembled(sysm)
     frames = turbulence.gradient_frames(sysm, seed=1, nframe=4)
     run = RefRunner(sysm, frames, fit)
     for _ in range(max(1, args.warmup)):
@@ -365,10 +372,10 @@ def single_instance_rates(preset: str, nsteps: int = 200, warmup: int = 5):
     L2 flushed before every step; steps/s and p50/p99 step latency."""
     import numpy as np
     import torch
-    from maos_b200 import config, fit_setup, geometry, turbulence
+    from maos_b200 import config, fit_assemble, geometry, turbulence
     from maos_b200.recon import Reconstructor
     sysm = geometry.build_tomo(config.PRESETS[preset]())
-    fit = fit_setup.build_fit(sysm)
+    fit = fit_assemble.build_fit_assembled(sysm)
     frames = turbulence.gradient_frames(sysm, seed=1, nframe=4)
     g = torch.tensor(frames, dtype=torch.float32, device="cuda")
     R = Reconstructor(sysm, nbatch=1, fit=fit)
@@ -406,12 +413,12 @@ def served_mix(seconds: float, mcao_frames=None, mvm: bool = False):
     the GPU by batched solves) instead of the iterative reconstructor."""
     import numpy as np
     import torch
-    from maos_b200 import config, fit_setup, geometry, serve, turbulence
+    from maos_b200 import config, fit_assemble, geometry, serve, turbulence
     rng = np.random.default_rng(17)
     types, frames = [], []
     for name, n in SERVE_MIX:
         sysm = geometry.build_tomo(config.PRESETS[name]())
-        fs = fit_setup.build_fit(sysm)
+        fs = fit_assemble.build_fit_assembled(sysm)
         types.append(serve.SystemType(name, sysm, fs, capacity=n))
         if name == "mcao_30m" and mcao_frames is not None:
             fr = np.asarray(mcao_frames, dtype=np.float32)
@@ -475,7 +482,7 @@ def served_mix(seconds: float, mcao_frames=None, mvm: bool = False):
 def run_gpu(args):
     import numpy as np
     import torch
-    from maos_b200 import config, fit_setup, geometry, native, turbulence
+    from maos_b200 import config, fit_assemble, fit_setup, geometry, native, turbulence
     from maos_b200.recon import Reconstructor
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -489,7 +496,12 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     sysm = geometry.build_tomo(config.PRESETS[WORKLOAD]())
-    fit = fit_setup.build_fit(sysm)
+    # the reference's default fit: assembled FR/FL over the in-pupil actuators
+    # with slaving, extrapolation and tikcr (gpu.fit=1, fit.square=0)
+    fit = fit_assemble.build_fit_assembled(sysm)
+    # the device WFS and closed loop ray-trace DM maps: the grid-form fit
+    # (gpu.fit=2, fit.square=1) drives them
+    fit_grid = fit_setup.build_fit(sysm)
     B = args.batch
     nframe = 4
     # gradients: 4 frozen-flow frames for each of 4 seeds, tiled over instances
@@ -622,10 +634,16 @@ def run_gpu(args):
         mvm_line["precision"] = precision
     del Mctl
 
-    wfs_line = wfs_rates(sysm, fit, B, stream, cpu=(rank == 0 and not args.no_cpu_baseline)) \
+    wfs_line = wfs_rates(sysm, fit_grid, B, stream, cpu=(rank == 0 and not args.no_cpu_baseline)) \
         if world == 1 and not args.no_wfs else None
 
-    loop_line = closed_loop_rates(sysm, fit, R, B, stream) if world == 1 and not args.no_wfs else None
+    loop_line = None
+    if world == 1 and not args.no_wfs:
+        Rg = Reconstructor(sysm, nbatch=B, device=local, fit=fit_grid)
+        Rg.autotune(reps=10)
+        loop_line = closed_loop_rates(sysm, fit_grid, Rg, B, stream)
+        loop_line["fit"] = "grid form (DM maps on full grids)"
+        Rg.close()
 
     single = None
     if world == 1:

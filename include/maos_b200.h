@@ -84,6 +84,14 @@ typedef struct {
     const double *mdiag;
 } mb_fdpcg_desc;
 
+/* A sparse matrix in compressed sparse column form (the reference's dsp). */
+typedef struct {
+    int nrow, ncol;
+    const int *p;          /* [ncol+1] column starts; NULL: no matrix */
+    const int *i;          /* [nnz] row indices */
+    const double *x;       /* [nnz] values */
+} mb_csc;
+
 /* DM fit in grid form (cuda/fit.cu cufit_grid; recon->fit, maos/setup_recon_fit.c):
  *   FitR x = sum_f wt_f HA_f^T (W0 - W1 W1^T) Hxp_f x
  *   FitL a = sum_f wt_f HA_f^T (W0 - W1 W1^T) HA_f a + NW NW^T a
@@ -106,7 +114,34 @@ typedef struct {
     int nnw;               /* low-rank columns (fit->NW) */
     const double *nw;      /* [nact_total x nnw] column-major, DMs concatenated */
     int maxit;             /* fit.maxit */
+    /* Optional slaving term added to FitL (recon->fit->actslave on the DM
+       grids, applied by cufit_grid::L, cuda/fit.cu:232-234): nact_total x
+       nact_total; p NULL when there is none. */
+    mb_csc actslave;
 } mb_fit_desc;
+
+/* The assembled DM fit, the reference's default GPU fit (gpu.fit=1:
+ * cuda/solve.cu cusolve_sparse over recon->fit->FR and FL, the sparse plus
+ * low-rank MUV_T of lib/muv.c:37):
+ *   rhs  = FR.M x - FR.U (FR.V^T x)
+ *   FL a = FL.M a - FL.U (FL.V^T a)
+ * then CG on FL warm-started from the previous commands (curecon_t::fit,
+ * cuda/recon.cu:277).  Any actuator set works, in particular fit.square=0
+ * (actuators inside the metapupil, the reference default); the actuators of
+ * all DMs are concatenated in recon->aloc order.  FL.M carries the Tikhonov
+ * and slaving terms, and HA inside FR and FL the extrapolation to weakly
+ * coupled actuators, as maos/setup_recon_fit.c:186-293 assembles them. */
+typedef struct {
+    mb_csc frm;            /* nact x nxtot: fit->FR.M, its DM x layer blocks as one matrix */
+    int nfr;               /* columns of FR.U and FR.V (<= 16) */
+    const double *fru;     /* [nact x nfr] column-major (fit->FR.U) */
+    const double *frv;     /* [nxtot x nfr] column-major (fit->FR.V) */
+    mb_csc flm;            /* nact x nact: fit->FL.M */
+    int nfl;               /* columns of FL.U and FL.V (<= 16) */
+    const double *flu;     /* [nact x nfl] column-major (fit->FL.U) */
+    const double *flv;     /* [nact x nfl] column-major (fit->FL.V) */
+    int maxit;             /* fit.maxit */
+} mb_fit_sparse_desc;
 
 /* Everything gpu_setup_recon (cuda/recon.cu:477) reads. */
 typedef struct {
@@ -121,7 +156,10 @@ typedef struct {
     int split;             /* recon.split: non-zero skips tip/tilt removal in the LHS */
     const mb_fdpcg_desc *fdpcg; /* required when precond==1 */
     int nbatch;            /* independent instances sharing these tables (>=1) */
-    const mb_fit_desc *fit; /* optional DM fit (NULL: tomography only) */
+    const mb_fit_desc *fit; /* optional DM fit in grid form (NULL: none) */
+    /* optional assembled DM fit (gpu.fit=1, the reference default); at most
+       one of fit and fit_sparse */
+    const mb_fit_sparse_desc *fit_sparse;
 } mb_recon_desc;
 
 /* gpu_init (cuda/gpu.h:27): select the device for subsequent setups. */

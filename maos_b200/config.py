@@ -89,6 +89,8 @@ class AOConfig:
     fit_tikcr: float = 1e-7
     fit_lrt_piston: bool = True
     fit_lrt_tt: bool = True
+    fit_actslave: bool = True     # slave weakly coupled actuators (fit.actslave)
+    fit_actthres: float = 0.1     # coupling below which an actuator is slaved (fit.actthres)
     dms: List[DmSpec] = field(default_factory=list)
     sim_dt: float = 1.0 / 800
     seed: int = 1

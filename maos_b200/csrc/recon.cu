@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "tomo_kernels.cuh"
+#include "fit_kernels.cuh"
 
 namespace mb {
 
@@ -195,6 +196,25 @@ struct Recon {
     DevBuf<float> fres, fab;
     DevBuf<unsigned> fcnt;
     CgScal fscal() const { return CgScal{fsc.p, fnsc, fab.p, fcnt.p, fres.p}; }
+    // grid fit: slaving term of FitL (CSR), applied into fslv and added by k_fit_hxt
+    bool has_slave = false;
+    DevBuf<int> as_rp;
+    DevBuf<GatherW> as_e;
+    DevBuf<float> fslv;
+    // assembled fit (fit_sparse): FR, FL as CSR (column, value) plus low rank
+    bool fit_sparse = false;
+    int nfr = 0, nfl = 0, nrb_a = 0;       // low-rank columns; 8-row blocks over the actuators
+    DevBuf<int> frm_rp, flm_rp;
+    DevBuf<GatherW> frm_e, flm_e;
+    DevBuf<float> fru, frv, flu, flv;
+    DevBuf<double> lr_part;
+    DevBuf<float> lr_t;
+    DevBuf<unsigned> lr_cnt;
+    void spmv(const DevBuf<int> &rp, const DevBuf<GatherW> &e, int nrow, long ncol, const float *xin, float *out,
+              const float *U, int nq, const float *add, double *dot, int k, cudaStream_t s);
+    void lr_dot(const float *xin, const float *V, int nq, long n, cudaStream_t s);
+    void build_fit_sparse(const mb_fit_sparse_desc *f);
+    void alloc_fit_state();
 
     cudaGraphExec_t graph = nullptr;       // tomography step
     cudaGraphExec_t graph_fit = nullptr;   // fit step
@@ -913,7 +933,9 @@ void Recon::build(const mb_recon_desc *d) {
     MB_CUDA_TRY(cudaMemcpyAsync(active.p, mask_host, (size_t)nb * sizeof(int), cudaMemcpyHostToDevice, stream));
     MB_CUDA_TRY(cudaEventRecord(mask_ev, stream));
     if (precond) build_fdpcg(d->fdpcg);
+    MB_REQUIRE(!(d->fit && d->fit_sparse), "give either the grid-form fit or the assembled fit, not both");
     if (d->fit) build_fit(d->fit);
+    if (d->fit_sparse) build_fit_sparse(d->fit_sparse);
     x.zero_async(stream);
     gin.zero_async(stream);
     sc.zero_async(stream);
@@ -1028,29 +1050,65 @@ void Recon::enqueue_solve(cudaStream_t s) {
     enqueue_cg(B, nxtot, nblk_x, maxit, A, M, s, XM);
 }
 
+// y = M x - U (V'x) for all instances: one warp per row, NI instances per CTA.
+void Recon::spmv(const DevBuf<int> &rp, const DevBuf<GatherW> &e, int nrow, long ncol, const float *xin, float *out,
+                 const float *U, int nq, const float *add, double *dot, int k, cudaStream_t s) {
+    const unsigned ry = (unsigned)((nrow + kThreads / 32 - 1) / (kThreads / 32));
+    const CgScal S = dot ? fscal() : CgScal{};
+    const float *dx = dot ? xin : nullptr;
+#define MB_SPMV(NI)                                                                                            \
+    launch(k_spmv_lr<NI>, dim3((unsigned)((nb + NI - 1) / NI), ry), dim3(kThreads), 0, s, rp.p, e.p, nrow, ncol, \
+           xin, out, U, lr_t.p, nq, add, dx, dot, S, k, nb, act())
+    if (nb == 1) MB_SPMV(1);
+    else if (nb == 2) MB_SPMV(2);
+    else if (nb <= 4) MB_SPMV(4);
+    else MB_SPMV(8);
+#undef MB_SPMV
+}
+
+// t[b][q] = V_q' x_b (FP64 partials, fixed-order total)
+void Recon::lr_dot(const float *xin, const float *V, int nq, long n, cudaStream_t s) {
+    launch(k_lr_dot, dim3(nblocks(n), nb), dim3(kThreads), 0, s, xin, V, nq, n, lr_part.p, lr_t.p, lr_cnt.p, act());
+}
+
 // FitR: sum_f wt_f HA_f^T (W0 - W1 W1^T) Hxp_f x   (recon_utils.c:483, fit.cu:190)
+// assembled: FR.M x - FR.U (FR.V' x)                 (lib/muv.c:37, solve.cu:36)
 void Recon::op_fitR(const float *xin, float *out, cudaStream_t s) {
+    if (fit_sparse) {
+        if (nfr) lr_dot(xin, frv.p, nfr, nxtot, s);
+        spmv(frm_rp, frm_e, (int)nact, nxtot, xin, out, nfr ? fru.p : nullptr, nfr, nullptr, nullptr, 0, s);
+        return;
+    }
     launch(nps <= 8 ? k_hx<8> : k_hx<16>, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, xin, opdf.p, hxp.fwd.p, laytab, nps, nfit, nfx, nfy,
                                                     nxtot, w1v.p, w1_part.p, act());
     launch(k_fit_w, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, opdf.p, opdw.p, w0_rp.p, w0_ci.p, w0_v.p, w1v.p,
                                                        fwt.p, w1_part.p, nblk_f, nf, nfit, act());
     launch(k_fit_hxt, dim3(nblk_a, nb), dim3(kThreads), 0, s, opdw.p, nullptr, out, nullptr, fitpad(), dmtab, ndm,
-           nfit, nfx, nfy, nact, LowRank{}, fscal(), 0, act());
+           nfit, nfx, nfy, nact, LowRank{}, fscal(), 0, (const float *)nullptr, act());
 }
 
-// FitL: sum_f wt_f HA_f^T (W0 - W1 W1^T) HA_f a + NW NW^T a   (recon_utils.c:536, fit.cu:213)
+// FitL: sum_f wt_f HA_f^T (W0 - W1 W1^T) HA_f a + NW NW^T a + actslave a
+//       (recon_utils.c:536, fit.cu:213-235)
+// assembled: FL.M a - FL.U (FL.V' a)                 (lib/muv.c:37, solve.cu:36)
 void Recon::op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t s, int k) {
+    if (fit_sparse) {
+        if (nfl) lr_dot(ain, flv.p, nfl, nact, s);
+        spmv(flm_rp, flm_e, (int)nact, nact, ain, out, nfl ? flu.p : nullptr, nfl, nullptr, dot_part, k, s);
+        return;
+    }
     LowRank lr{};
     if (nnw) {
         launch(k_lowrank_dot, dim3(nblk_a, nb), dim3(kThreads), 0, s, ain, nwv.p, nw_part.p, nnw, nact, act());
         lr = LowRank{nwv.p, nw_part.p, nnw, nblk_a};
     }
+    if (has_slave)
+        spmv(as_rp, as_e, (int)nact, nact, ain, fslv.p, nullptr, 0, nullptr, nullptr, 0, s);
     launch(ndm <= 8 ? k_hx<8> : k_hx<16>, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, ain, opdf.p, ha.fwd.p, dmtab, ndm, nfit, nfx, nfy,
                                                     nact, w1v.p, w1_part.p, act());
     launch(k_fit_w, dim3(nblk_f, nfit, nb), dim3(kThreads), 0, s, opdf.p, opdw.p, w0_rp.p, w0_ci.p, w0_v.p, w1v.p,
                                                        fwt.p, w1_part.p, nblk_f, nf, nfit, act());
     launch(k_fit_hxt, dim3(nblk_a, nb), dim3(kThreads), 0, s, opdw.p, ain, out, dot_part, fitpad(), dmtab, ndm,
-           nfit, nfx, nfy, nact, lr, fscal(), k, act());
+           nfit, nfx, nfy, nact, lr, fscal(), k, has_slave ? (const float *)fslv.p : nullptr, act());
 }
 
 // The DM fit of one step: RHS from the tomography solution, then CG warm-
@@ -1060,6 +1118,93 @@ void Recon::enqueue_fit(cudaStream_t s) {
     CgBufs B{fa.p, fr.p, fp.p, fr.p, fAp.p, frhs.p, f_pap.p, f_rr.p, f_rz.p, f_bb.p, fscal()};
     AmulFn A = [&](const float *in, float *out, double *dot, int k) { op_fitL(in, out, dot, s, k); };
     enqueue_cg(B, nact, nblk_a, fit_maxit, A, MmulFn(), s);
+}
+
+// CSC (the reference's dsp) -> CSR rows of (column, value) pairs.
+static void csc_to_csr(const mb_csc &m, const char *what, std::vector<int> &rp, std::vector<GatherW> &ent) {
+    MB_REQUIRE(m.p && m.nrow > 0 && m.ncol > 0, "%s: empty matrix", what);
+    const long nnz = m.p[m.ncol];
+    MB_REQUIRE(nnz >= 0 && (nnz == 0 || (m.i && m.x)), "%s: missing arrays", what);
+    rp.assign((size_t)m.nrow + 1, 0);
+    for (int c = 0; c < m.ncol; c++)
+        MB_REQUIRE(m.p[c] <= m.p[c + 1], "%s: column pointers decrease at %d", what, c);
+    for (long k = 0; k < nnz; k++) {
+        MB_REQUIRE(m.i[k] >= 0 && m.i[k] < m.nrow, "%s: row index %d out of range", what, m.i[k]);
+        rp[m.i[k] + 1]++;
+    }
+    for (int r = 0; r < m.nrow; r++) rp[r + 1] += rp[r];
+    ent.assign((size_t)nnz, GatherW{0, 0.f});
+    std::vector<int> fill(rp.begin(), rp.end() - 1);
+    for (int c = 0; c < m.ncol; c++)
+        for (int k = m.p[c]; k < m.p[c + 1]; k++) ent[fill[m.i[k]]++] = GatherW{c, (float)m.x[k]};
+}
+
+static void upload_f32(DevBuf<float> &d, const double *h, size_t n) {
+    std::vector<float> t(n);
+    for (size_t i = 0; i < n; i++) t[i] = (float)h[i];
+    d.upload(t);
+}
+
+// CG state and scratch of the fit (both forms), sized by nact.
+void Recon::alloc_fit_state() {
+    nblk_a = (int)nblocks(nact);
+    nrb_a = (int)((nact + kThreads / 32 - 1) / (kThreads / 32));
+    MB_REQUIRE(nrb_a < 65535, "fit: too many actuators (%ld)", nact);
+    fnsc = fit_maxit + 3;
+    const size_t NA = (size_t)nb * nact;
+    fa.alloc(NA); fr.alloc(NA); fp.alloc(NA); fAp.alloc(NA); frhs.alloc(NA);
+    // the p.Ap partials of the sparse operator are per 8-row block, of the grid one per 256 actuators
+    f_pap.alloc((size_t)nb * std::max(nblk_a, nrb_a)); f_rr.alloc((size_t)nb * nblk_a);
+    f_rz.alloc((size_t)nb * nblk_a); f_bb.alloc((size_t)nb * nblk_a);
+    fsc.alloc((size_t)nb * fnsc);
+    fres.alloc(nb);
+    fab.alloc((size_t)nb * 2);
+    fcnt.alloc(nb);
+    fa.zero_async(stream);
+    fsc.zero_async(stream);
+    fres.zero_async(stream);
+    fab.zero_async(stream);
+    fcnt.zero_async(stream);
+}
+
+void Recon::build_fit_sparse(const mb_fit_sparse_desc *f) {
+    MB_REQUIRE(f->maxit >= 1, "fit_sparse: maxit must be >= 1");
+    MB_REQUIRE(f->frm.p && f->flm.p, "fit_sparse: FR.M and FL.M are required");
+    MB_REQUIRE(f->frm.ncol == nxtot, "fit_sparse: FR.M has %d columns, the layers %ld points", f->frm.ncol, nxtot);
+    MB_REQUIRE(f->flm.nrow == f->frm.nrow && f->flm.ncol == f->frm.nrow,
+               "fit_sparse: FL.M must be nact x nact with nact = FR.M rows (%d)", f->frm.nrow);
+    MB_REQUIRE(f->nfr >= 0 && f->nfr <= kMaxLr && f->nfl >= 0 && f->nfl <= kMaxLr,
+               "fit_sparse: at most %d low-rank columns", kMaxLr);
+    MB_REQUIRE((f->nfr == 0 || (f->fru && f->frv)) && (f->nfl == 0 || (f->flu && f->flv)),
+               "fit_sparse: low-rank arrays missing");
+    has_fit = 1;
+    fit_sparse = true;
+    nact = f->frm.nrow;
+    fit_maxit = f->maxit;
+    nfr = f->nfr;
+    nfl = f->nfl;
+    std::vector<int> rp;
+    std::vector<GatherW> ent;
+    csc_to_csr(f->frm, "FR.M", rp, ent);
+    frm_rp.upload(rp);
+    frm_e.upload(ent);
+    csc_to_csr(f->flm, "FL.M", rp, ent);
+    flm_rp.upload(rp);
+    flm_e.upload(ent);
+    if (nfr) {
+        upload_f32(fru, f->fru, (size_t)nact * nfr);
+        upload_f32(frv, f->frv, (size_t)nxtot * nfr);
+    }
+    if (nfl) {
+        upload_f32(flu, f->flu, (size_t)nact * nfl);
+        upload_f32(flv, f->flv, (size_t)nact * nfl);
+    }
+    lr_part.alloc((size_t)nb * kMaxLr * std::max(nblocks(nxtot), nblocks(nact)));
+    lr_t.alloc((size_t)nb * kMaxLr);
+    lr_cnt.alloc(nb);
+    lr_t.zero_async(stream);
+    lr_cnt.zero_async(stream);
+    alloc_fit_state();
 }
 
 void Recon::build_fit(const mb_fit_desc *f) {
@@ -1166,26 +1311,23 @@ void Recon::build_fit(const mb_fit_desc *f) {
     w1v.upload(h1);
     fwt.upload(hw);
     if (nnw) nwv.upload(hn);
-    nblk_a = (int)nblocks(nact);
     nblk_f = (int)nblocks(nf);
-    fnsc = fit_maxit + 3;
-    const size_t NA = (size_t)nb * nact;
-    fa.alloc(NA); fr.alloc(NA); fp.alloc(NA); fAp.alloc(NA); frhs.alloc(NA);
+    if (f->actslave.p) {  // cufit_grid::L's slaving term (cuda/fit.cu:232-234)
+        MB_REQUIRE(f->actslave.nrow == nact && f->actslave.ncol == nact,
+                   "fit: actslave must be %ld x %ld (the DM grids)", nact, nact);
+        std::vector<int> rp;
+        std::vector<GatherW> ent;
+        csc_to_csr(f->actslave, "actslave", rp, ent);
+        as_rp.upload(rp);
+        as_e.upload(ent);
+        has_slave = true;
+        fslv.alloc((size_t)nb * nact);
+    }
+    alloc_fit_state();
     opdf.alloc((size_t)nb * nfit * nf);
     opdw.alloc((size_t)nb * nfit * nf);
     w1_part.alloc((size_t)nb * nfit * nblk_f);
     nw_part.alloc((size_t)nb * std::max(nnw, 1) * nblk_a);
-    f_pap.alloc((size_t)nb * nblk_a); f_rr.alloc((size_t)nb * nblk_a);
-    f_rz.alloc((size_t)nb * nblk_a); f_bb.alloc((size_t)nb * nblk_a);
-    fsc.alloc((size_t)nb * fnsc);
-    fres.alloc(nb);
-    fab.alloc((size_t)nb * 2);
-    fcnt.alloc(nb);
-    fa.zero_async(stream);
-    fsc.zero_async(stream);
-    fres.zero_async(stream);
-    fab.zero_async(stream);
-    fcnt.zero_async(stream);
 }
 
 // Time each kernel of a CG iteration alone and report its algorithmic

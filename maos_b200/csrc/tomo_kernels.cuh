@@ -283,8 +283,9 @@ struct LowRank {
 // bilinear footprint covers it are the products of the x list
 // fx[((w*ndm + l)*maxn + jx)*kx + e] and the y list (padding: weight 0).
 // Every load of a direction depends only on (w, jx, jy), so the loads of
-// several directions are in flight together.  Plus the low-rank NW term and
-// the p.Ap partials (last block: alpha) for FitL.  grid: (ceil(nact/256), nb).
+// several directions are in flight together.  Plus the low-rank NW term, an
+// optional vector added as is (the slaving term), and the p.Ap partials (last
+// block: alpha) for FitL.  grid: (ceil(nact/256), nb).
 constexpr int kFitPad = 4;  // widest padded fit list
 struct FitPad {
     const GatherW *x, *y;
@@ -294,7 +295,8 @@ struct FitPad {
 __global__ void __launch_bounds__(kThreads)
 k_fit_hxt(const float *__restrict__ opd2, const float *__restrict__ xin, float *__restrict__ out,
           double *__restrict__ dot_part, FitPad fpd, const __grid_constant__ LayerTab dl, int ndm, int nfit,
-          int nfx, int nfy, long nact, LowRank lr, CgScal S, int k, const int *__restrict__ act) {
+          int nfx, int nfy, long nact, LowRank lr, CgScal S, int k, const float *__restrict__ addv,
+          const int *__restrict__ act) {
     pdl_enter();
     if (inactive(act, blockIdx.y)) return;
     __shared__ double sh[32];
@@ -347,6 +349,7 @@ k_fit_hxt(const float *__restrict__ opd2, const float *__restrict__ xin, float *
             for (int q = 0; q < lr.nnw; q++) lt += lr.nw[(size_t)q * nact + j] * s_t[q];
             acc += lt;
         }
+        if (addv) acc += addv[(size_t)b * nact + j];  // the slaving term, applied before
         out[(size_t)b * nact + j] = acc;
         if (dot_part && X) dotv = (double)acc * (double)X[jj];
     }

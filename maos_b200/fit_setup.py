@@ -22,12 +22,18 @@ reference's GPU path uses (``cuda/fit.cu`` ``cufit_grid``):
               (setup_recon_fit.c:110-165, ``fit.lrt_piston``/``lrt_tt``),
               restricted to actuators with coupling > 0.1 (``genactcpl``,
               lib/slaving.c:25).
+* ``actslave`` the slaving term ``cufit_grid::L`` adds (cuda/fit.cu:232-234),
+              built by ``lib/slaving.c:63`` slaving from the coupling of each
+              grid actuator (``fit.actslave``, on by default).
+
+The assembled fit with actuators inside the metapupil, the reference's
+default, is ``maos_b200.fit_assemble``.
 """
 from __future__ import annotations
 
 import math
 from dataclasses import dataclass
-from typing import List
+from typing import List, Optional
 
 import numpy as np
 import scipy.sparse as sps
@@ -59,6 +65,7 @@ class FitSystem:
     NW: np.ndarray        # [nact_total, nnw] in compact aloc order (DMs concatenated)
     maxit: int
     HA: list              # HA[f][d]: csr (nfloc x nact_d), for the oracle and setup
+    actslave: Optional[sps.csr_matrix] = None  # nact_total x nact_total, block diagonal
 
     @property
     def nact(self) -> int:
@@ -209,14 +216,17 @@ def build_fit(sysm) -> FitSystem:
     nnw = (ndm if cfg.fit_lrt_piston else 0) + (2 * (ndm - 1) if cfg.fit_lrt_tt else 0)
     off = np.concatenate([[0], np.cumsum([len(dm.act) for dm in dms])])
     NW = np.zeros((int(off[-1]), nnw))
+    # actuator coupling (lib/slaving.c:25 genactcpl)
+    from .fit_assemble import genactcpl, loc_create_map, slaving, square_loc
+    cpl = genactcpl(HA, W1)
+    actslave = None
+    if cfg.fit_actslave:
+        sl = [slaving(loc_create_map(square_loc(dm.amap), 0), cpl[k], cfg.fit_actthres, 1.0 / floc.n)
+              for k, dm in enumerate(dms)]
+        if any(m is not None for m in sl):
+            actslave = sps.block_diag([m if m is not None else sps.csr_matrix((len(dms[k].act),) * 2)
+                                       for k, m in enumerate(sl)], format="csr")
     if nnw:
-        # actuator coupling (lib/slaving.c:25 genactcpl)
-        cpl = []
-        for k in range(ndm):
-            c = sum(HA[f][k].T @ W1 for f in range(nfit))
-            thres = c.max() / nfit
-            c = np.where((c > thres) | (thres == 0), 1.0, c / thres)
-            cpl.append(c)
         inw = 0
         if cfg.fit_lrt_piston:
             for k in range(ndm):
@@ -229,4 +239,4 @@ def build_fit(sysm) -> FitSystem:
                 m = cpl[k] > 0.1
                 NW[off[k]:off[k + 1], inw + 2 * (k - 1)] = np.where(m, dms[k].locx * factor, 0.0)
                 NW[off[k]:off[k + 1], inw + 2 * (k - 1) + 1] = np.where(m, dms[k].locy * factor, 0.0)
-    return FitSystem(floc, thetax, thetay, wt, hs, W0, W1, dms, NW, cfg.fit_maxit, HA)
+    return FitSystem(floc, thetax, thetay, wt, hs, W0, W1, dms, NW, cfg.fit_maxit, HA, actslave)

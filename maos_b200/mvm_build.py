@@ -123,13 +123,13 @@ def main():
     as one JSON line."""
     import argparse
     import json
-    from . import config, fit_setup, geometry
+    from . import config, fit_assemble, geometry
     ap = argparse.ArgumentParser()
     ap.add_argument("--system", default="elt_39m", choices=sorted(config.PRESETS))
     ap.add_argument("--rhs-batch", type=int, default=256)
     a = ap.parse_args()
     sysm = geometry.build_tomo(config.PRESETS[a.system]())
-    fit = fit_setup.build_fit(sysm)
+    fit = fit_assemble.build_fit_assembled(sysm)
     M, rep = build_control_matrix(sysm, fit, rhs_batch=a.rhs_batch)
     rep.update({"system": a.system, "shape": list(M.shape), "ngrad": int(sysm.ngrad),
                 "columns_per_s": rep["columns"] / rep["seconds"],

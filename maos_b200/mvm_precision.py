@@ -36,9 +36,9 @@ def frozen_flow(sysm, fit, nsteps: int, seed: int = 11, dt: float = None, device
     dt = sysm.cfg.sim_dt if dt is None else dt
     atm = DeviceAtmosphere(FrozenFlowAtmosphere(sysm.cfg, seed), device=device)
     rng = np.random.default_rng(seed + 104729)
-    fl = fit.floc
-    fx = torch.as_tensor((fl.ox + np.arange(fl.nx) * fl.dx)[None, :].repeat(fl.ny, 0).ravel(), device=device)
-    fy = torch.as_tensor((fl.oy + np.arange(fl.ny) * fl.dy)[:, None].repeat(fl.nx, 1).ravel(), device=device)
+    px, py = fit_points(fit)
+    fx = torch.as_tensor(px, device=device)
+    fy = torch.as_tensor(py, device=device)
     g = np.empty((nsteps, sysm.ngrad))
     phi = np.empty((nsteps, fx.numel()))
     for k in range(nsteps):
@@ -46,6 +46,26 @@ def frozen_flow(sysm, fit, nsteps: int, seed: int = 11, dt: float = None, device
         phi[k] = atm.opd(fx, fy, float(fit.thetax[0]), float(fit.thetay[0]), float(fit.hs[0]),
                          k * dt).cpu().numpy()
     return g, phi
+
+
+def fit_points(fit):
+    """Coordinates of the fit grid's points (a full grid, or the metapupil
+    points of the assembled fit)."""
+    fl = fit.floc
+    if hasattr(fl, "points"):
+        return fl.points()
+    return ((fl.ox + np.arange(fl.nx) * fl.dx)[None, :].repeat(fl.ny, 0).ravel(),
+            (fl.oy + np.arange(fl.ny) * fl.dy)[:, None].repeat(fl.nx, 1).ravel())
+
+
+def science_HA(fit):
+    """The DM-to-fit-grid ray tracing of fit direction 0 (DMs side by side);
+    for the assembled fit it includes the extrapolation to weakly coupled
+    actuators that maos applies to the commands."""
+    import scipy.sparse as sps
+    if getattr(fit, "HA0", None) is not None:
+        return fit.HA0
+    return sps.hstack([fit.HA[0][d] for d in range(len(fit.dms))]).tocsr()
 
 
 def _wfe(fit, v: np.ndarray) -> np.ndarray:
@@ -84,8 +104,7 @@ def study(sysm, fit, M: np.ndarray, nsteps: int = 400, seed: int = 11, gate: flo
     (nm RMS and as a fraction of the residual) and whether it is within
     ``gate`` of the residual."""
     g, phi = frozen_flow(sysm, fit, nsteps, seed, device=device)
-    import scipy.sparse as sps
-    HA0 = sps.hstack([fit.HA[0][d] for d in range(len(fit.dms))]).tocsr()
+    HA0 = science_HA(fit)
     a64 = g @ np.asarray(M, dtype=np.float64).T
     res = _wfe(fit, phi - (HA0 @ a64.T).T)
     out = {"steps": int(nsteps), "dt_s": float(sysm.cfg.sim_dt), "shape": [int(M.shape[0]), int(M.shape[1])],

@@ -37,13 +37,25 @@ class MbFdpcgDesc(C.Structure):
                 ("mdata", C.POINTER(C.c_double)), ("mdiag", C.POINTER(C.c_double))]
 
 
+class MbCsc(C.Structure):
+    _fields_ = [("nrow", C.c_int), ("ncol", C.c_int), ("p", C.POINTER(C.c_int)), ("i", C.POINTER(C.c_int)),
+                ("x", C.POINTER(C.c_double))]
+
+
 class MbFitDesc(C.Structure):
     _fields_ = [("floc", MbGrid), ("nfit", C.c_int), ("thetax", C.POINTER(C.c_double)),
                 ("thetay", C.POINTER(C.c_double)), ("wt", C.POINTER(C.c_double)),
                 ("hs", C.POINTER(C.c_double)), ("w0_p", C.POINTER(C.c_int)),
                 ("w0_i", C.POINTER(C.c_int)), ("w0_x", C.POINTER(C.c_double)),
                 ("w1", C.POINTER(C.c_double)), ("ndm", C.c_int), ("amap", C.POINTER(MbGrid)),
-                ("nnw", C.c_int), ("nw", C.POINTER(C.c_double)), ("maxit", C.c_int)]
+                ("nnw", C.c_int), ("nw", C.POINTER(C.c_double)), ("maxit", C.c_int),
+                ("actslave", MbCsc)]
+
+
+class MbFitSparseDesc(C.Structure):
+    _fields_ = [("frm", MbCsc), ("nfr", C.c_int), ("fru", C.POINTER(C.c_double)), ("frv", C.POINTER(C.c_double)),
+                ("flm", MbCsc), ("nfl", C.c_int), ("flu", C.POINTER(C.c_double)), ("flv", C.POINTER(C.c_double)),
+                ("maxit", C.c_int)]
 
 
 class MbReconDesc(C.Structure):
@@ -51,7 +63,7 @@ class MbReconDesc(C.Structure):
                 ("l2c", C.POINTER(C.c_double)), ("nwfs", C.c_int),
                 ("wfs", C.POINTER(MbWfsDesc)), ("maxit", C.c_int), ("precond", C.c_int),
                 ("split", C.c_int), ("fdpcg", C.POINTER(MbFdpcgDesc)), ("nbatch", C.c_int),
-                ("fit", C.POINTER(MbFitDesc))]
+                ("fit", C.POINTER(MbFitDesc)), ("fit_sparse", C.POINTER(MbFitSparseDesc))]
 
 
 _PI = C.POINTER(C.c_int)

@@ -26,7 +26,7 @@ from typing import Optional
 import numpy as np
 
 from . import native
-from .native import MbFdpcgDesc, MbFitDesc, MbGrid, MbReconDesc, MbWfsDesc, check
+from .native import MbCsc, MbFdpcgDesc, MbFitDesc, MbFitSparseDesc, MbGrid, MbReconDesc, MbWfsDesc, check
 
 
 def _dptr(a: np.ndarray):
@@ -59,6 +59,33 @@ def fdpcg_desc(fd, keep: list) -> MbFdpcgDesc:
                        perm.ctypes.data_as(C.POINTER(C.c_long)), _dptr(mbi), md, mg)
 
 
+def csc_desc(A, keep: list) -> MbCsc:
+    """A scipy sparse matrix as an ``mb_csc`` (compressed sparse column)."""
+    if A is None:
+        return MbCsc()
+    A = A.tocsc()
+    A.sort_indices()
+    p = np.ascontiguousarray(A.indptr, dtype=np.int32)
+    i = np.ascontiguousarray(A.indices, dtype=np.int32)
+    x = np.ascontiguousarray(A.data, dtype=np.float64)
+    keep += [p, i, x]
+    return MbCsc(int(A.shape[0]), int(A.shape[1]), p.ctypes.data_as(C.POINTER(C.c_int)),
+                 i.ctypes.data_as(C.POINTER(C.c_int)), _dptr(x))
+
+
+def fit_sparse_desc(sf, keep: list) -> MbFitSparseDesc:
+    """Flatten a :class:`maos_b200.fit_assemble.SparseFit` (FR, FL) into an
+    ``mb_fit_sparse_desc``."""
+    cols = []
+    for a in (sf.FRU, sf.FRV, sf.FLU, sf.FLV):
+        c = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"))
+        keep.append(c)
+        cols.append(c)
+    return MbFitSparseDesc(csc_desc(sf.FRM, keep), int(sf.FRU.shape[1]), _dptr(cols[0]), _dptr(cols[1]),
+                           csc_desc(sf.FLM, keep), int(sf.FLU.shape[1]), _dptr(cols[2]), _dptr(cols[3]),
+                           int(sf.maxit))
+
+
 def fit_desc(fs, keep: list) -> MbFitDesc:
     """Flatten a :class:`maos_b200.fit_setup.FitSystem` into an ``mb_fit_desc``."""
     W0 = fs.W0.tocsc()
@@ -73,7 +100,8 @@ def fit_desc(fs, keep: list) -> MbFitDesc:
     return MbFitDesc(_grid(fs.floc), len(fs.thetax), _dptr(arrs[0]), _dptr(arrs[1]), _dptr(arrs[2]),
                      _dptr(arrs[3]), w0p.ctypes.data_as(C.POINTER(C.c_int)),
                      w0i.ctypes.data_as(C.POINTER(C.c_int)), _dptr(arrs[4]), _dptr(arrs[5]),
-                     len(fs.dms), am, int(fs.NW.shape[1]), _dptr(nw), int(fs.maxit))
+                     len(fs.dms), am, int(fs.NW.shape[1]), _dptr(nw), int(fs.maxit),
+                     csc_desc(getattr(fs, "actslave", None), keep))
 
 
 def tomo_desc(sysm, nbatch: int = 1, split: int = 1, maxit: Optional[int] = None, fit=None):
@@ -122,13 +150,18 @@ def tomo_desc(sysm, nbatch: int = 1, split: int = 1, maxit: Optional[int] = None
         keep.append(fd)
         fdp = C.pointer(fd)
     fitp = C.POINTER(MbFitDesc)()
-    if fit is not None:
+    fsp = C.POINTER(MbFitSparseDesc)()
+    if fit is not None and hasattr(fit, "FLM"):   # the assembled fit (maos_b200.fit_assemble)
+        fd = fit_sparse_desc(fit, keep)
+        keep.append(fd)
+        fsp = C.pointer(fd)
+    elif fit is not None:                         # the grid-form fit (maos_b200.fit_setup)
         fd = fit_desc(fit, keep)
         keep.append(fd)
         fitp = C.pointer(fd)
     d = MbReconDesc(_grid(sysm.pmap), len(sysm.xmaps), xm, _dptr(l2c), len(sysm.wfs), ws,
                     int(cfg.tomo_maxit if maxit is None else maxit), int(cfg.tomo_precond),
-                    int(split), fdp, int(nbatch), fitp)
+                    int(split), fdp, int(nbatch), fitp, fsp)
     return d, keep
 
 

@@ -240,7 +240,8 @@ class FitOracle:
 
     ``fit_R``: ``maos/recon_utils.c:483`` FitR with HXF (bilinear ray tracing
     from the layers onto the fit grid along each fit direction);
-    ``fit_L``: ``maos/recon_utils.c:536`` FitL (no slaving term)."""
+    ``fit_L``: ``maos/recon_utils.c:536`` FitL, with the slaving term when
+    the fit system carries one."""
 
     def __init__(self, tomo_sys, fit_sys):
         self.t = tomo_sys
@@ -282,10 +283,31 @@ class FitOracle:
         out = self._hat(xp)
         if self.f.NW.shape[1]:
             out = out + self.f.NW @ (self.f.NW.T @ a)
+        if getattr(self.f, "actslave", None) is not None:  # recon_utils.c:555-557
+            out = out + self.f.actslave @ a
         return alpha * out
 
 
-def fit_solve(fo: FitOracle, x_layers, a0=None, maxit=None):
+class SparseFitOracle:
+    """FP64 assembled DM fit (``lib/muv.c:37`` muv on ``fit->FR`` / ``fit->FL``,
+    the operators ``maos/recon.c:93`` muv_solve applies):
+    ``fit_R x = FR.M x - FR.U (FR.V' x)``, ``fit_L a = FL.M a - FL.U (FL.V' a)``
+    on a :class:`maos_b200.fit_assemble.SparseFit`."""
+
+    def __init__(self, tomo_sys, sf):
+        self.t = tomo_sys
+        self.f = sf
+
+    def fit_R(self, x, alpha=1.0):
+        x = np.asarray(x, dtype=np.float64)
+        return alpha * (self.f.FRM @ x - self.f.FRU @ (self.f.FRV.T @ x))
+
+    def fit_L(self, a, alpha=1.0):
+        a = np.asarray(a, dtype=np.float64)
+        return alpha * (self.f.FLM @ a - self.f.FLU @ (self.f.FLV.T @ a))
+
+
+def fit_solve(fo, x_layers, a0=None, maxit=None):
     """DM fit of one step: FitR then CG on FitL, warm-started from a0 (recon.c:89-93)."""
     maxit = fo.f.maxit if maxit is None else maxit
     rhs = fo.fit_R(x_layers)

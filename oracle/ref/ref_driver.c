@@ -29,6 +29,7 @@
 #include "lib/mkh.h"
 #include "lib/mkw.h"
 #include "lib/servo.h"
+#include "lib/slaving.h"
 
 typedef struct {
     int nwfs, nps, nthread;
@@ -727,4 +728,207 @@ void ref_wfs_geom_grads(int nwfs, const double *thetax, const double *thetay, co
     free(opd);
     for (int s = 0; s < nscr; s++) mapfree(maps[s]);
     free(maps);
+}
+
+/* ------------------------------------------------------------------------
+ * Assembled DM fit (fit.square=0, fit.assemble=1): the reference's own
+ * create_metapupil (math/loc.c:1471), loc_create_map_npad with its ghost
+ * points (math/loc.c:208), mkw_circular (lib/mkw.c:363) and setup_fit
+ * (maos/setup_recon_fit.c:303: HXF, HA, genactcpl, act_extrap, low-rank
+ * terms, slaving, FR and FL assembly), then muv (lib/muv.c:37) and pcg with
+ * muv on FL, as maos/recon.c:93 muv_solve runs them.
+ * ---------------------------------------------------------------------- */
+static loc_t *g_mp_loc = NULL;
+long ref_metapupil(int ndir, const double *dirs, double D, double ht, double dx, double offset, double guard,
+                   int square) {
+    dmat *d = dnew(3, ndir);
+    memcpy(d->p, dirs, sizeof(double) * 3 * ndir);
+    map_t *map = NULL;
+    create_metapupil(&map, 0, 0, d, D, ht, dx, dx, offset, guard, 0, 0, 0, square);
+    if (g_mp_loc) locfree(g_mp_loc);
+    g_mp_loc = map2loc(map, 0);
+    mapfree(map);
+    dfree(d);
+    return g_mp_loc->nloc;
+}
+void ref_metapupil_get(double *x, double *y) {
+    memcpy(x, g_mp_loc->locx, sizeof(double) * g_mp_loc->nloc);
+    memcpy(y, g_mp_loc->locy, sizeof(double) * g_mp_loc->nloc);
+}
+
+static loc_t *mk_loc(long n, const double *x, const double *y, double dx, double ht, int npad) {
+    loc_t *l = locnew(n, dx, dx);
+    memcpy(l->locx, x, sizeof(double) * n);
+    memcpy(l->locy, y, sizeof(double) * n);
+    l->ht = ht;
+    loc_create_map_npad(l, npad, 0, 0);
+    return l;
+}
+
+/* the map of a loc: sizes and origin, then the entries (x fastest) */
+static loc_t *g_map_loc = NULL;
+void ref_loc_map(long n, const double *x, const double *y, double dx, int npad, long *nx, long *ny, double *ox,
+                 double *oy) {
+    if (g_map_loc) locfree(g_map_loc);
+    g_map_loc = mk_loc(n, x, y, dx, 0, npad);
+    *nx = g_map_loc->map->nx;
+    *ny = g_map_loc->map->ny;
+    *ox = g_map_loc->map->ox;
+    *oy = g_map_loc->map->oy;
+}
+void ref_loc_map_get(long *out) {
+    long n = g_map_loc->map->nx * g_map_loc->map->ny;
+    for (long k = 0; k < n; k++) out[k] = (long)g_map_loc->map->p[k];
+}
+
+long ref_mkw_circular(long n, const double *x, const double *y, double dx, int npad, double cx, double cy,
+                      double cr) {
+    loc_t *loc = mk_loc(n, x, y, dx, 0, npad);
+    if (last_w0) dspfree(last_w0);
+    if (last_w1) dfree(last_w1);
+    mkw_circular(loc, cx, cy, cr, &last_w0, &last_w1);
+    locfree(loc);
+    return last_w0->p[last_w0->ny];
+}
+
+static FIT_T *g_afit = NULL;
+static long *g_aaoff = NULL;
+static int g_andm = 0;
+int ref_fit_assemble(void *hh, int nfit, const double *thetax, const double *thetay, const double *wt,
+                     const double *hs, long nf, const double *flocx, const double *flocy, double fdx,
+                     const int *w0p, const int *w0i, const double *w0x, const double *w1, int ndm,
+                     const double *dmht, const double *dmdx, const int *nact, const double *alocx,
+                     const double *alocy, int actslave, int actinterp, double actthres, double tikcr,
+                     int lrt_piston, int lrt_tt) {
+    refh_t *h = hh;
+    FIT_T *fit = calloc(1, sizeof(FIT_T));
+    fit->thetax = dnew(nfit, 1);
+    fit->thetay = dnew(nfit, 1);
+    fit->wt = dnew(nfit, 1);
+    fit->hs = dnew(nfit, 1);
+    for (int i = 0; i < nfit; i++) {
+        fit->thetax->p[i] = thetax[i];
+        fit->thetay->p[i] = thetay[i];
+        fit->wt->p[i] = wt[i];
+        fit->hs->p[i] = hs[i];
+    }
+    fit->xloc = h->recon->xloc;
+    fit->floc = mk_loc(nf, flocx, flocy, fdx, 0, 1);
+    fit->W0 = mk_csc(nf, nf, w0p, w0i, w0x);
+    fit->W1 = dnew(nf, 1);
+    memcpy(fit->W1->p, w1, sizeof(double) * nf);
+    fit->aloc = loccellnew(ndm, 1);
+    free(g_aaoff);
+    g_aaoff = calloc(ndm + 1, sizeof(long));
+    g_andm = ndm;
+    for (int d = 0; d < ndm; d++) {
+        fit->aloc->p[d] = mk_loc(nact[d], alocx + g_aaoff[d], alocy + g_aaoff[d], dmdx[d], dmht[d], 1);
+        g_aaoff[d + 1] = g_aaoff[d] + nact[d];
+    }
+    fit->flag.tikcr = tikcr;
+    fit->flag.actthres = actthres;
+    fit->flag.actslave = actslave;
+    fit->flag.actinterp = actinterp;
+    fit->flag.nfit = nfit;
+    fit->flag.lrt_piston = lrt_piston;
+    fit->flag.lrt_tt = lrt_tt;
+    fit->flag.alg = 1;
+    fit->flag.assemble = 1;
+    fit->flag.maxit = 4;
+    fit->flag.cgwarm = 1;
+    setup_fit(fit, 0);
+    g_afit = fit;
+    return 0;
+}
+
+static dsp *fitas_sp(int which) {
+    switch (which) {
+        case 0: return dspcell2sp((dspcell *)g_afit->FR.M);
+        case 1: return dspcell2sp((dspcell *)g_afit->FL.M);
+        case 2: return g_afit->actinterp ? dspcell2sp(g_afit->actinterp) : NULL;
+        case 3: return g_afit->actslave ? dspcell2sp(g_afit->actslave) : NULL;
+    }
+    return NULL;
+}
+/* which: 0 FR.M, 1 FL.M, 2 actinterp, 3 actslave; CSC; returns nnz (-1: absent) */
+long ref_fitas_sp(int which, int *p, int *i, double *x, long *nrow, long *ncol) {
+    dsp *A = fitas_sp(which);
+    if (!A) return -1;
+    long nnz = A->p[A->ny];
+    *nrow = A->nx;
+    *ncol = A->ny;
+    if (p) {
+        for (long k = 0; k <= A->ny; k++) p[k] = A->p[k];
+        for (long k = 0; k < nnz; k++) { i[k] = A->i[k]; x[k] = A->x[k]; }
+    }
+    dspfree(A);
+    return nnz;
+}
+/* which: 0 FR.U, 1 FR.V, 2 FL.U, 3 FL.V, 4 actcpl, 5 NW; column-major */
+long ref_fitas_dense(int which, double *out, long *nrow, long *ncol) {
+    dcell *c = NULL;
+    switch (which) {
+        case 0: c = g_afit->FR.U; break;
+        case 1: c = g_afit->FR.V; break;
+        case 2: c = g_afit->FL.U; break;
+        case 3: c = g_afit->FL.V; break;
+        case 4: c = g_afit->actcpl; break;
+        case 5: c = g_afit->NW; break;
+    }
+    if (!c) return -1;
+    dmat *m = dcell2m(c);
+    *nrow = m->nx;
+    *ncol = m->ny;
+    if (out) memcpy(out, m->p, sizeof(double) * m->nx * m->ny);
+    long n = m->nx * m->ny;
+    dfree(m);
+    return n;
+}
+static dcell *avec2cell_as(const double *v) {
+    dcell *c = dcellnew(g_andm, 1);
+    for (int d = 0; d < g_andm; d++) {
+        c->p[d] = dnew(g_aaoff[d + 1] - g_aaoff[d], 1);
+        if (v) memcpy(c->p[d]->p, v + g_aaoff[d], sizeof(double) * (g_aaoff[d + 1] - g_aaoff[d]));
+    }
+    return c;
+}
+/* rhs = muv(FR, x) */
+void ref_fitas_rhs(void *hh, const double *xin, double *aout) {
+    refh_t *h = hh;
+    dcell *x = vec2cell(xin, h->xoff, h->nps);
+    dcell *a = NULL;
+    muv(&a, &g_afit->FR, x, 1);
+    cell2vec(aout, a, g_aaoff, g_andm);
+    dcellfree(x);
+    dcellfree(a);
+}
+/* y = muv(FL, a) */
+void ref_fitas_L(const double *ain, double *aout) {
+    dcell *a = avec2cell_as(ain);
+    dcell *y = NULL;
+    muv(&y, &g_afit->FL, a, 1);
+    cell2vec(aout, y, g_aaoff, g_andm);
+    dcellfree(a);
+    dcellfree(y);
+}
+/* pcg on FL (muv) from the warm start in a */
+double ref_fitas_pcg(const double *b, double *a, int warm, int maxit) {
+    dcell *bb = avec2cell_as(b);
+    dcell *aa = avec2cell_as(a);
+    double res = pcg(&aa, muv, &g_afit->FL, NULL, NULL, bb, warm, maxit);
+    cell2vec(a, aa, g_aaoff, g_andm);
+    dcellfree(bb);
+    dcellfree(aa);
+    return res;
+}
+
+/* The grid-form fit's slaving term as the reference builds it for
+ * fit.square=1 (maos/setup_recon_fit.c:72 genactcpl on HA and W1, then :165
+ * slaving with sclsq = 1/nfloc); FitL then adds it (recon_utils.c:555). */
+int ref_fit_setup_slave(double thres) {
+    FIT_T *fit = g_fit;
+    for (int d = 0; d < fit->aloc->nx; d++) loc_create_map(fit->aloc->p[d]);
+    fit->actcpl = genactcpl(fit->HA, fit->W1);
+    fit->actslave = slaving(fit->aloc, fit->actcpl, NULL, NULL, NULL, thres, 1. / fit->floc->nloc);
+    return fit->actslave != NULL;
 }

@@ -233,6 +233,11 @@ class _Worker:
         self.nfit = fd["nfit"]
         return True
 
+    def fit_setup_slave(self, thres=0.1):
+        """Add the reference's own slaving term (genactcpl + slaving) to the grid fit."""
+        self.lib.ref_fit_setup_slave.argtypes = [ctypes.c_double]
+        return bool(self.lib.ref_fit_setup_slave(ctypes.c_double(thres)))
+
     def fitR(self, x, alpha=1.0):
         out = np.zeros(self.na)
         self.lib.ref_fitR(self.h, _dp(x), ctypes.c_double(alpha), out.ctypes.data_as(_D))
@@ -258,6 +263,110 @@ class _Worker:
         x = np.zeros(nnz)
         L.ref_fit_ha(f, d, p.ctypes.data_as(_I), i.ctypes.data_as(_I), x.ctypes.data_as(_D))
         return p, i, x
+
+    # assembled fit (fit.square=0): metapupil locs, loc maps, mkw_circular, setup_fit
+    def metapupil(self, dirs, D, ht, dx, offset, guard, square=0):
+        L = self.lib
+        L.ref_metapupil.restype = ctypes.c_long
+        dd = np.asfortranarray(dirs, dtype=np.float64)
+        n = L.ref_metapupil(dd.shape[1], dd.ctypes.data_as(_D), ctypes.c_double(D), ctypes.c_double(ht),
+                            ctypes.c_double(dx), ctypes.c_double(offset), ctypes.c_double(guard), int(square))
+        x = np.zeros(n)
+        y = np.zeros(n)
+        L.ref_metapupil_get(x.ctypes.data_as(_D), y.ctypes.data_as(_D))
+        return x, y
+
+    def loc_map(self, x, y, dx, npad):
+        L = self.lib
+        nx, ny = ctypes.c_long(), ctypes.c_long()
+        ox, oy = ctypes.c_double(), ctypes.c_double()
+        L.ref_loc_map(ctypes.c_long(len(x)), _dp(x), _dp(y), ctypes.c_double(dx), int(npad), ctypes.byref(nx),
+                      ctypes.byref(ny), ctypes.byref(ox), ctypes.byref(oy))
+        m = np.zeros(nx.value * ny.value, dtype=np.int64)
+        L.ref_loc_map_get(m.ctypes.data_as(_L))
+        return m.reshape(ny.value, nx.value), ox.value, oy.value
+
+    def mkw_circular(self, x, y, dx, npad, cx, cy, cr):
+        L = self.lib
+        L.ref_mkw_circular.restype = ctypes.c_long
+        nnz = L.ref_mkw_circular(ctypes.c_long(len(x)), _dp(x), _dp(y), ctypes.c_double(dx), int(npad),
+                                 ctypes.c_double(cx), ctypes.c_double(cy), ctypes.c_double(cr))
+        n = len(x)
+        p = np.zeros(n + 1, dtype=np.int32)
+        i = np.zeros(nnz, dtype=np.int32)
+        xv = np.zeros(nnz)
+        w1 = np.zeros(n)
+        L.ref_mkw_amp_get(p.ctypes.data_as(_I), i.ctypes.data_as(_I), xv.ctypes.data_as(_D),
+                          w1.ctypes.data_as(_D))
+        return p, i, xv, w1
+
+    def fit_assemble(self, fd):
+        """The reference's setup_fit on the given floc, W0/W1 and aloc."""
+        L = self.lib
+        keep = []
+
+        def d(a):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(a)
+            return a.ctypes.data_as(_D)
+
+        def i32(a):
+            a = np.ascontiguousarray(a, dtype=np.int32)
+            keep.append(a)
+            return a.ctypes.data_as(_I)
+
+        L.ref_fit_assemble(self.h, fd["nfit"], d(fd["thetax"]), d(fd["thetay"]), d(fd["wt"]), d(fd["hs"]),
+                           ctypes.c_long(fd["nf"]), d(fd["flocx"]), d(fd["flocy"]), ctypes.c_double(fd["fdx"]),
+                           i32(fd["w0_p"]), i32(fd["w0_i"]), d(fd["w0_x"]), d(fd["w1"]), fd["ndm"],
+                           d(fd["dmht"]), d(fd["dmdx"]), i32(fd["nact"]), d(fd["alocx"]), d(fd["alocy"]),
+                           int(fd["actslave"]), int(fd["actinterp"]), ctypes.c_double(fd["actthres"]),
+                           ctypes.c_double(fd["tikcr"]), int(fd["lrt_piston"]), int(fd["lrt_tt"]))
+        self.keep += keep
+        self.na = int(np.sum(fd["nact"]))
+        return True
+
+    def fitas_sparse(self, which):
+        """0 FR.M, 1 FL.M, 2 actinterp, 3 actslave as (p, i, x, nrow, ncol) CSC, or None."""
+        L = self.lib
+        L.ref_fitas_sp.restype = ctypes.c_long
+        nr, nc = ctypes.c_long(), ctypes.c_long()
+        nnz = L.ref_fitas_sp(int(which), None, None, None, ctypes.byref(nr), ctypes.byref(nc))
+        if nnz < 0:
+            return None
+        p = np.zeros(nc.value + 1, dtype=np.int32)
+        i = np.zeros(nnz, dtype=np.int32)
+        x = np.zeros(nnz)
+        L.ref_fitas_sp(int(which), p.ctypes.data_as(_I), i.ctypes.data_as(_I), x.ctypes.data_as(_D),
+                       ctypes.byref(nr), ctypes.byref(nc))
+        return p, i, x, nr.value, nc.value
+
+    def fitas_dense(self, which):
+        """0 FR.U, 1 FR.V, 2 FL.U, 3 FL.V, 4 actcpl, 5 NW (column-major), or None."""
+        L = self.lib
+        L.ref_fitas_dense.restype = ctypes.c_long
+        nr, nc = ctypes.c_long(), ctypes.c_long()
+        n = L.ref_fitas_dense(int(which), None, ctypes.byref(nr), ctypes.byref(nc))
+        if n < 0:
+            return None
+        out = np.zeros(n)
+        L.ref_fitas_dense(int(which), out.ctypes.data_as(_D), ctypes.byref(nr), ctypes.byref(nc))
+        return out.reshape((nr.value, nc.value), order="F")
+
+    def fitas_rhs(self, x):
+        out = np.zeros(self.na)
+        self.lib.ref_fitas_rhs(self.h, _dp(x), out.ctypes.data_as(_D))
+        return out
+
+    def fitas_L(self, a):
+        out = np.zeros(self.na)
+        self.lib.ref_fitas_L(_dp(a), out.ctypes.data_as(_D))
+        return out
+
+    def fitas_pcg(self, b, a0, warm, maxit):
+        a = np.array(a0, dtype=np.float64) if a0 is not None else np.zeros(self.na)
+        self.lib.ref_fitas_pcg.restype = ctypes.c_double
+        res = self.lib.ref_fitas_pcg(_dp(b), a.ctypes.data_as(_D), int(warm), int(maxit))
+        return a, res
 
     def mkw_amp(self, grid, amp):
         L = self.lib
@@ -419,6 +528,20 @@ def fit_desc(fs) -> dict:
             "alocx": np.concatenate([d.locx for d in fs.dms]),
             "alocy": np.concatenate([d.locy for d in fs.dms]),
             "nnw": fs.NW.shape[1], "nw": np.asfortranarray(fs.NW).ravel(order="F")}
+
+
+def fit_assembled_desc(sf, cfg) -> dict:
+    """Flatten a maos_b200.fit_assemble.SparseFit's inputs for ``ref_fit_assemble``."""
+    W0 = sf.W0.tocsc()
+    W0.sort_indices()
+    return {"nfit": len(sf.thetax), "thetax": sf.thetax, "thetay": sf.thetay, "wt": sf.wt, "hs": sf.hs,
+            "nf": sf.floc.nloc, "flocx": sf.floc.locx, "flocy": sf.floc.locy, "fdx": sf.floc.dx,
+            "w0_p": W0.indptr, "w0_i": W0.indices, "w0_x": W0.data, "w1": sf.W1,
+            "ndm": len(sf.alocs), "dmht": [a.ht for a in sf.alocs], "dmdx": [a.dx for a in sf.alocs],
+            "nact": [a.nloc for a in sf.alocs], "alocx": np.concatenate([a.locx for a in sf.alocs]),
+            "alocy": np.concatenate([a.locy for a in sf.alocs]),
+            "actslave": int(sf.actslave is not None), "actinterp": 1, "actthres": 0.1, "tikcr": sf.tikcr,
+            "lrt_piston": int(cfg.fit_lrt_piston), "lrt_tt": int(cfg.fit_lrt_tt)}
 
 
 def system_desc(sysm, split: int = 1) -> dict:

@@ -35,6 +35,17 @@ def get_fit(name: str):
     return _FIT_CACHE[name]
 
 
+_AFIT_CACHE = {}
+
+
+def get_fit_assembled(name: str):
+    """Build (once per session) the assembled fit (reference defaults) of a preset."""
+    if name not in _AFIT_CACHE:
+        from maos_b200 import fit_assemble
+        _AFIT_CACHE[name] = fit_assemble.build_fit_assembled(get_system(name))
+    return _AFIT_CACHE[name]
+
+
 @pytest.fixture(scope="session")
 def ltao():
     return get_system("ltao_8m")

@@ -97,7 +97,8 @@ def test_gradient_operator_matches_reference_mkg(ref_proc, ltao):
 @pytest.mark.parametrize("name", ["ltao_8m", "mcao_30m"])
 def test_fit_operators_match_reference(name, ref_proc):
     """FitR/FitL/CG of the oracle vs the reference's FitR/FitL/pcg, whose HA
-    and HXF the driver builds with the reference's own mkh."""
+    and HXF the driver builds with the reference's own mkh, and whose slaving
+    term comes from the reference's own slaving (lib/slaving.c)."""
     from conftest import get_system, get_fit
     from oracle.recon_oracle import FitOracle
     s = get_system(name)
@@ -105,6 +106,8 @@ def test_fit_operators_match_reference(name, ref_proc):
     R = ref_proc
     R.call("setup", refbridge.system_desc(s, split=1))
     R.call("fit_setup", refbridge.fit_desc(fs))
+    # the slaving term of FitL from the reference's own genactcpl + slaving
+    assert R.call("fit_setup_slave", s.cfg.fit_actthres) == (fs.actslave is not None)
     fo = FitOracle(s, fs)
     rng = np.random.default_rng(21)
     x = rng.standard_normal(s.nx_total)
