@@ -186,6 +186,21 @@ int mb_update_recon_cn2(mb_recon *r, const double *l2c, const mb_fdpcg_desc *fdp
  * [nbatch][nxtot].  cgres: optional [nbatch] final CG residual |r|/|b|. */
 int mb_tomo(mb_recon *r, const double *grad, double *opdr, float *cgres);
 
+/* gpu_tomo with maos's own gradient cells (the dcell gradin of
+ * cuda/recon.cu:564, one column per WFS), one instance (nbatch 1): grad[iwfs]
+ * points at that WFS's 2*nsa FP64 gradients, x then y (NULL: zeros).  They are
+ * converted straight from the columns into a pinned staging buffer, with no
+ * concatenated copy.  opdr (may be NULL; NULL entries skipped): per-layer FP64
+ * outputs of nx*ny points (the copy to simu->opdr, cuda/recon.cu:574-580).
+ * cgres: optional final CG residual. */
+int mb_tomo_wfs(mb_recon *r, const double *const *grad, double *const *opdr, float *cgres);
+
+/* gpu_fit when the tomography ran on the CPU (gpu.tomo=0: curecon_t::fit
+ * copies simu->opdr to the device first, cuda/recon.cu:278-281), one instance:
+ * opdr[ips] the host FP64 layer OPD (NULL: zeros); it replaces the device's
+ * layer solution, then the fit runs as in mb_fit.  dmout: [nact] FP64. */
+int mb_fit_opdr(mb_recon *r, const double *const *opdr, double *dmout, float *cgres);
+
 /* gpu_fit (cuda/gpu.h:56, curecon_t::fit cuda/recon.cu:277): DM fit of the
  * current tomography solution.  dmout: [nbatch][nact] host FP64 actuator
  * commands (overwritten, like add2cpu(...,0,...) at recon.cu:285).  cgres:

@@ -216,12 +216,27 @@ struct Recon {
     void build_fit_sparse(const mb_fit_sparse_desc *f);
     void alloc_fit_state();
 
+    // pinned host staging for the FP64 <-> FP32 conversions of the host-buffer calls
+    float *hstage = nullptr;
+    size_t hstage_n = 0;
+    float *stage(size_t n) {
+        if (n > hstage_n) {
+            if (hstage) cudaFreeHost(hstage);
+            hstage = nullptr;
+            hstage_n = 0;
+            MB_CUDA_TRY(cudaHostAlloc(&hstage, n * sizeof(float), cudaHostAllocDefault));
+            hstage_n = n;
+        }
+        return hstage;
+    }
+
     cudaGraphExec_t graph = nullptr;       // tomography step
     cudaGraphExec_t graph_fit = nullptr;   // fit step
     cudaGraphExec_t graph_step = nullptr;  // tomography + fit
     long graph_kernels = 0, graph_fit_kernels = 0, graph_step_kernels = 0;
 
     ~Recon() {
+        if (hstage) cudaFreeHost(hstage);
         if (mask_ev) cudaEventDestroy(mask_ev);
         if (mask_host) cudaFreeHost(mask_host);
         if (graph) cudaGraphExecDestroy(graph);
@@ -1706,6 +1721,65 @@ int mb_fit(mb_recon *h, double *dmout, float *cgres) {
     if (dmout) from_float_dev(dmout, R.fa.p, (size_t)R.nb * R.nact, R.stream);
     if (cgres) MB_CUDA_TRY(cudaMemcpyAsync(cgres, R.fres.p, R.nb * sizeof(float), cudaMemcpyDeviceToHost, R.stream));
     MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
+    MB_API_END
+}
+
+int mb_tomo_wfs(mb_recon *h, const double *const *grad, double *const *opdr, float *cgres) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && grad, "invalid arguments");
+    mb::Recon &R = h->R;
+    MB_REQUIRE(R.nb == 1, "mb_tomo_wfs serves one instance (nbatch %d)", R.nb);
+    float *st = R.stage((size_t)std::max(R.ngrad, R.nxtot));
+    MB_CUDA_TRY(cudaStreamSynchronize(R.stream));  // the staging buffer is free
+    for (int w = 0; w < R.nwfs; w++) {
+        const long n = R.goff[w + 1] - R.goff[w];
+        float *d = st + R.goff[w];
+        if (!grad[w]) {
+            std::fill(d, d + n, 0.f);
+            continue;
+        }
+        for (long i = 0; i < n; i++) {
+            if (!std::isfinite(grad[w][i])) {
+                mb::set_error("gradient %ld of WFS %d is not finite", i, w);
+                return MB_ENUM;
+            }
+            d[i] = (float)grad[w][i];
+        }
+    }
+    MB_CUDA_TRY(cudaMemcpyAsync(R.gin.p, st, (size_t)R.ngrad * sizeof(float), cudaMemcpyHostToDevice, R.stream));
+    R.run_graph(R.stream);
+    if (opdr) MB_CUDA_TRY(cudaMemcpyAsync(st, R.x.p, (size_t)R.nxtot * sizeof(float), cudaMemcpyDeviceToHost, R.stream));
+    if (cgres) MB_CUDA_TRY(cudaMemcpyAsync(cgres, R.res.p, sizeof(float), cudaMemcpyDeviceToHost, R.stream));
+    MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
+    if (opdr)
+        for (int l = 0; l < R.nps; l++)
+            if (opdr[l])
+                for (long i = R.xoff[l]; i < R.xoff[l + 1]; i++) opdr[l][i - R.xoff[l]] = st[i];
+    MB_API_END
+}
+
+int mb_fit_opdr(mb_recon *h, const double *const *opdr, double *dmout, float *cgres) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && opdr, "invalid arguments");
+    mb::Recon &R = h->R;
+    if (!R.has_fit) {
+        mb::set_error("reconstructor was set up without a DM fit");
+        return MB_ESTATE;
+    }
+    MB_REQUIRE(R.nb == 1, "mb_fit_opdr serves one instance (nbatch %d)", R.nb);
+    float *st = R.stage((size_t)std::max<long>(R.nxtot, R.nact));
+    MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
+    for (int l = 0; l < R.nps; l++)
+        for (long i = R.xoff[l]; i < R.xoff[l + 1]; i++) st[i] = opdr[l] ? (float)opdr[l][i - R.xoff[l]] : 0.f;
+    MB_CUDA_TRY(cudaMemcpyAsync(R.x.p, st, (size_t)R.nxtot * sizeof(float), cudaMemcpyHostToDevice, R.stream));
+    R.set_mask(nullptr, R.stream);
+    MB_CUDA_TRY(cudaGraphLaunch(R.graph_fit, R.stream));
+    mb::count_launches(R.graph_fit_kernels);
+    if (dmout) MB_CUDA_TRY(cudaMemcpyAsync(st, R.fa.p, (size_t)R.nact * sizeof(float), cudaMemcpyDeviceToHost, R.stream));
+    if (cgres) MB_CUDA_TRY(cudaMemcpyAsync(cgres, R.fres.p, sizeof(float), cudaMemcpyDeviceToHost, R.stream));
+    MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
+    if (dmout)
+        for (long i = 0; i < R.nact; i++) dmout[i] = st[i];
     MB_API_END
 }
 

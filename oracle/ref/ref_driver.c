@@ -932,3 +932,133 @@ int ref_fit_setup_slave(double thres) {
     fit->actslave = slaving(fit->aloc, fit->actcpl, NULL, NULL, NULL, thres, 1. / fit->floc->nloc);
     return fit->actslave != NULL;
 }
+
+/* ------------------------------------------------------------------------
+ * The gpu_* glue test: PARMS_T / RECON_T / POWFS_T / SIM_T as maos holds them
+ * after setup, for the glue (maos_b200/glue/maos_gpu_glue.c) to read, and the
+ * reference's own CPU tomofit (maos/recon.c:55) on a second SIM_T for the
+ * comparison.  gpu_fit 1: the assembled fit of ref_fit_assemble; 2: the grid
+ * fit of ref_fit_setup (+ ref_fit_setup_slave).
+ * ---------------------------------------------------------------------- */
+static SIM_T *g_cpu_simu = NULL;
+static dcell *g_cpu_dm = NULL;
+static void glue_simu(refh_t *h, SIM_T *s) {
+    s->parms = h->parms;
+    s->recon = h->recon;
+    s->powfs = h->powfs;
+    s->cgres = dcellnew(2, 1);
+    s->cgres->p[0] = dnew(100000, 1);
+    s->cgres->p[1] = dnew(100000, 1);
+    s->isim = s->reconisim = 0;
+}
+int ref_glue_prepare(void *hh, int gpu_fit, int tomo_maxit, int fit_maxit) {
+    refh_t *h = hh;
+    PARMS_T *parms = h->parms;
+    RECON_T *recon = h->recon;
+    FIT_T *fit = gpu_fit == 2 ? g_fit : g_afit;
+    if (!fit) return -1;
+    const int ndm = (int)fit->aloc->nx;
+    parms->recon.alg = 0;
+    if (!parms->dbg.tomo_maxit) parms->dbg.tomo_maxit = lnew(0, 1);
+    parms->gpu.tomo = 1;
+    parms->gpu.fit = gpu_fit;
+    parms->tomo.maxit = tomo_maxit;
+    parms->fit.maxit = fit_maxit;
+    parms->ndm = ndm;
+    parms->fit.nfit = (int)fit->thetax->nx;
+    parms->fit.thetax = fit->thetax;
+    parms->fit.thetay = fit->thetay;
+    parms->fit.wt = fit->wt;
+    parms->fit.hs = fit->hs;
+    recon->fit = fit;
+    recon->aloc = fit->aloc;
+    recon->anloc = lnew(ndm, 1);
+    recon->anx = lnew(ndm, 1);
+    recon->any = lnew(ndm, 1);
+    recon->amap = mapcellnew(ndm, 1);
+    for (int d = 0; d < ndm; d++) {
+        loc_create_map(fit->aloc->p[d]);
+        recon->amap->p[d] = fit->aloc->p[d]->map;
+        recon->amap->p[d]->h = fit->aloc->p[d]->ht;
+        recon->anloc->p[d] = fit->aloc->p[d]->nloc;
+        recon->anx->p[d] = recon->amap->p[d]->nx;
+        recon->any->p[d] = recon->amap->p[d]->ny;
+    }
+    recon->fmap = recon->pmap;
+    recon->W0 = fit->W0;
+    recon->W1 = fit->W1;
+    /* the CPU path: muv_solve on RL/RR (tomography) and FL/FR (fit) */
+    recon->RR.Mfun = TomoR;
+    recon->RR.Mdata = recon;
+    recon->RL.Mfun = TomoL;
+    recon->RL.Mdata = recon;
+    recon->RL.pfun = parms->tomo.precond == 1 ? fdpcg_precond : NULL;
+    recon->RL.pdata = recon;
+    recon->RL.alg = 1;
+    recon->RL.warm = 1;
+    recon->RL.maxit = tomo_maxit;
+    fit->FL.alg = 1;
+    fit->FL.warm = 1;
+    fit->FL.maxit = fit_maxit;
+    if (!fit->FR.M) { /* the grid fit is not assembled: FitR / FitL (recon_utils.c:483,536) */
+        fit->FR.Mfun = FitR;
+        fit->FR.Mdata = fit;
+        fit->FL.Mfun = FitL;
+        fit->FL.Mdata = fit;
+    }
+    glue_simu(h, h->simu);
+    g_cpu_simu = calloc(1, sizeof(SIM_T));
+    glue_simu(h, g_cpu_simu);
+    return ndm;
+}
+void ref_glue_handles(void *hh, void **out) {
+    refh_t *h = hh;
+    out[0] = h->parms;
+    out[1] = h->powfs;
+    out[2] = h->recon;
+    out[3] = h->simu;
+}
+/* gradients as maos hands them: one column of 2 nsa per WFS */
+void *ref_glue_grad_cell(void *hh, const double *g) {
+    refh_t *h = hh;
+    dcell *c = dcellnew(h->nwfs, 1);
+    for (int w = 0; w < h->nwfs; w++) {
+        c->p[w] = dnew(h->goff[w + 1] - h->goff[w], 1);
+        memcpy(c->p[w]->p, g + h->goff[w], sizeof(double) * (h->goff[w + 1] - h->goff[w]));
+    }
+    return c;
+}
+void ref_glue_cell_free(void *c) {
+    dcell *d = c;
+    dcellfree(d);
+}
+long ref_glue_cell_get(void *c, double *out) {
+    dcell *d = c;
+    long off = 0;
+    for (int i = 0; i < d->nx * d->ny; i++)
+        if (d->p[i]) {
+            if (out) memcpy(out + off, d->p[i]->p, sizeof(double) * d->p[i]->nx * d->p[i]->ny);
+            off += d->p[i]->nx * d->p[i]->ny;
+        }
+    return off;
+}
+/* the reference's CPU tomography + fit of one step (its own tomofit) */
+double ref_glue_cpu_step(void *grad, double *dmout) {
+    tomofit(&g_cpu_dm, g_cpu_simu, (dcell *)grad);
+    ref_glue_cell_get(g_cpu_dm, dmout);
+    g_cpu_simu->reconisim++;
+    return g_cpu_simu->cgres->p[1]->p[g_cpu_simu->reconisim - 1];
+}
+/* install a control matrix (nact x ngrad, column-major) as recon->MVM */
+void ref_glue_set_mvm(void *hh, const double *M, long nact, long ngrad) {
+    refh_t *h = hh;
+    dfree(h->recon->MVM);
+    h->recon->MVM = dnew(nact, ngrad);
+    memcpy(h->recon->MVM->p, M, sizeof(double) * nact * ngrad);
+}
+/* a DM command cell shaped like recon->anloc (or the grid sizes) */
+void *ref_glue_dm_cell(void *hh, int grid) {
+    refh_t *h = hh;
+    RECON_T *r = h->recon;
+    return grid ? dcellnew3(h->parms->ndm, 1, r->anx->p, r->any->p) : dcellnew3(h->parms->ndm, 1, r->anloc->p, NULL);
+}

@@ -21,6 +21,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_ref", "libmaosref.so")
+GLUE_LIB = os.path.join(HERE, "_ref", "libmaosgpuglue.so")
 
 
 def available() -> bool:
@@ -390,6 +391,95 @@ class _Worker:
                                 ctypes.c_double(grid[4]), x.ctypes.data_as(_D), y.ctypes.data_as(_D))
         return x, y
 
+
+    # the gpu_* glue (maos_b200/glue/maos_gpu_glue.c) on RECON_T built by the reference
+    def glue_prepare(self, gpu_fit, tomo_maxit, fit_maxit):
+        """PARMS_T / RECON_T / SIM_T as maos holds them after setup (no GPU needed)."""
+        L = self.lib
+        V = ctypes.c_void_p
+        L.ref_glue_prepare.restype = ctypes.c_int
+        nd = L.ref_glue_prepare(self.h, int(gpu_fit), int(tomo_maxit), int(fit_maxit))
+        if nd < 0:
+            raise RuntimeError("no fit set up in the reference driver")
+        L.ref_glue_grad_cell.restype = V
+        L.ref_glue_grad_cell.argtypes = [V, _D]
+        L.ref_glue_cell_get.restype = ctypes.c_long
+        L.ref_glue_cell_get.argtypes = [V, _D]
+        L.ref_glue_cell_free.argtypes = [V]
+        L.ref_glue_cpu_step.restype = ctypes.c_double
+        L.ref_glue_cpu_step.argtypes = [V, _D]
+        L.ref_glue_dm_cell.restype = V
+        L.ref_glue_dm_cell.argtypes = [V, ctypes.c_int]
+        hs = (V * 4)()
+        L.ref_glue_handles(self.h, hs)
+        self.gh = [V(v) for v in hs]  # parms, powfs, recon, simu
+        self.glue_grid = int(gpu_fit) == 2
+        return nd
+
+    def glue_setup(self):
+        """Load the glue and run gpu_init + gpu_setup_recon (needs a GPU)."""
+        V = ctypes.c_void_p
+        G = ctypes.CDLL(GLUE_LIB)
+        G.gpu_init.restype = ctypes.c_int
+        G.gpu_init.argtypes = [V, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        G.gpu_setup_recon.argtypes = [V, V, V]
+        G.gpu_tomo.argtypes = [V, V]
+        G.gpu_fit.argtypes = [ctypes.POINTER(V), V]
+        G.gpu_recon_reset.argtypes = [V]
+        G.gpu_setup_recon_mvm.argtypes = [V, V, V]
+        G.gpu_recon_mvm.argtypes = [ctypes.POINTER(V), V]
+        self.glue = G
+        if not G.gpu_init(self.gh[0], None, 0):
+            raise RuntimeError("gpu_init found no GPU")
+        G.gpu_setup_recon(self.gh[0], self.gh[1], self.gh[2])
+        self.dm_cell = V(0)
+        return True
+
+    def _cell_out(self, c):
+        L = self.lib
+        n = L.ref_glue_cell_get(c, None)
+        out = np.zeros(n)
+        L.ref_glue_cell_get(c, out.ctypes.data_as(_D))
+        return out
+
+    def glue_step(self, g):
+        """gpu_tomo then gpu_fit of one step; the DM commands."""
+        L, G = self.lib, self.glue
+        c = ctypes.c_void_p(L.ref_glue_grad_cell(self.h, _dp(g)))
+        G.gpu_tomo(self.gh[3], c)
+        G.gpu_fit(ctypes.byref(self.dm_cell), self.gh[3])
+        L.ref_glue_cell_free(c)
+        return self._cell_out(self.dm_cell)
+
+    def glue_cpu_step(self, g):
+        """The reference's own CPU tomofit of one step on its own SIM_T."""
+        L = self.lib
+        c = ctypes.c_void_p(L.ref_glue_grad_cell(self.h, _dp(g)))
+        out = np.zeros(self.na)
+        res = L.ref_glue_cpu_step(c, out.ctypes.data_as(_D))
+        L.ref_glue_cell_free(c)
+        return out, res
+
+    def glue_reset(self):
+        self.glue.gpu_recon_reset(self.gh[0])
+
+    def glue_mvm(self, M, g):
+        """gpu_setup_recon_mvm with recon->MVM = M, then gpu_recon_mvm(g)."""
+        L, G = self.lib, self.glue
+        Mf = np.asfortranarray(M, dtype=np.float64)
+        L.ref_glue_set_mvm(self.h, Mf.ctypes.data_as(_D), ctypes.c_long(Mf.shape[0]), ctypes.c_long(Mf.shape[1]))
+        G.gpu_setup_recon_mvm(self.gh[0], self.gh[2], self.gh[1])
+        dm = ctypes.c_void_p(L.ref_glue_dm_cell(self.h, int(self.glue_grid)))
+        c = ctypes.c_void_p(L.ref_glue_grad_cell(self.h, _dp(g)))
+        G.gpu_recon_mvm(ctypes.byref(dm), c)
+        out = self._cell_out(dm)
+        L.ref_glue_cell_free(c)
+        L.ref_glue_cell_free(dm)
+        return out
+
+    def glue_cleanup(self):
+        self.glue.gpu_cleanup()
+        return True
 
     # .bin files through the reference's writebin / read_by_id (maos_b200.binio checks)
     def bin_write_dmat(self, fn, a, header=""):
