@@ -8,7 +8,7 @@
  * (cuda/gpu.h); the citation is given beside each declaration.  The
  * reference passes its simulator structs (PARMS_T, RECON_T, SIM_T); this ABI
  * takes the same information as flat arrays, so the glue a maintainer adds to
- * maos (the gpu_* functions of glue/maos_gpu_glue.c) copies fields out of
+ * maos (the gpu_* functions of maos_b200/glue/maos_gpu_glue.c) copies fields out of
  * RECON_T into the descriptors below.
  *
  * Conventions (same as the reference's dmat / map_t / dsp):
