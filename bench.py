@@ -145,6 +145,7 @@ class RefRunner:
         self.ncores = os.cpu_count() or 1
         self.frames = frames
         self.maxit = sysm.cfg.tomo_maxit
+        self.nx = int(sysm.nx_total)
         self.fit_maxit = fit.maxit if fit is not None else 0
         self.R = refbridge.RefProcess(nthread=self.ncores)
         self.R.call("setup", refbridge.system_desc(sysm, split=1))
@@ -171,6 +172,17 @@ class RefRunner:
             self.a, _ = self.R.call("fit_pcg", fb, self.a, int(self.a is not None), self.fit_maxit)
         self.k += 1
 
+    def precond_ms(self, reps: int = 20) -> float:
+        """ms per call of the reference's fdpcg_precond alone (its FFTs run on
+        the FFTW-API shim, FFTW being absent here), with the worker round trip."""
+        import numpy as np
+        r = np.random.default_rng(1).standard_normal(self.nx)
+        self.R.call("fdpcg_precond", r)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            self.R.call("fdpcg_precond", r)
+        return (time.perf_counter() - t0) / reps * 1000.0
+
     def rate(self, seconds: float):
         """Run warm steps for about `seconds`; returns (steps/s, steps, elapsed)."""
         n = 0
@@ -184,6 +196,20 @@ class RefRunner:
 
     def close(self):
         self.R.close()
+
+
+def fft_note(rate: float, precond_ms: float, maxit: int) -> dict:
+    """The share of the reference CPU step spent in its FDPCG preconditioner
+    (whose FFTs run on this build's FFTW-API shim), and the step rate with
+    that share removed: a bound on how much a faster FFT library could give."""
+    step_ms = 1000.0 / rate
+    pre = precond_ms * maxit
+    rest = max(step_ms - pre, 1e-9)
+    return {"fdpcg_precond_ms_per_call": precond_ms, "fdpcg_precond_share_of_step": min(pre / step_ms, 1.0),
+            "value_without_fdpcg_precond": 1000.0 / rest,
+            "fft_note": "the reference's FFTs run on this build's FFTW-API shim (FFTW is absent); "
+                        "value_without_fdpcg_precond removes the whole preconditioner (FFTs and block solve) "
+                        "from the CPU step, the most a faster FFT library could give"}
 
 
 def run_reference(args):
@@ -204,6 +230,7 @@ def run_reference(args):
         r, n, _dt = run.rate(per)
         rates.append(r)
         total += n
+    pms = run.precond_ms()
     run.close()
     value = statistics.median(rates)
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
@@ -213,7 +240,8 @@ def run_reference(args):
             "config": {"workload": WORKLOAD_TEXT, "instances": 1},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "steps/s", "cores": run.ncores, "kind": "reference",
-                             "sample": f"{total} warm reference CPU steps in {args.steps} samples"},
+                             "sample": f"{total} warm reference CPU steps in {args.steps} samples",
+                             **fft_note(value, pms, sysm.cfg.tomo_maxit)},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -661,9 +689,11 @@ def run_gpu(args):
             run = RefRunner(sysm, fr[0], fit)
             run.step()
             rate, n, dt = run.rate(args.cpu_seconds)
+            pms = run.precond_ms()
             run.close()
             cpu = {"value": rate, "unit": "steps/s", "cores": run.ncores, "kind": "reference",
-                   "sample": f"{n} warm steps of one {WORKLOAD} instance in {dt:.1f} s"}
+                   "sample": f"{n} warm steps of one {WORKLOAD} instance in {dt:.1f} s",
+                   **fft_note(rate, pms, sysm.cfg.tomo_maxit)}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,

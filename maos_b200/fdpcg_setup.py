@@ -11,7 +11,10 @@ reference's ``fdpcg->Mbinv->p[b]`` and ``perm`` its ``fdpcg->perm``.
 
 Per block (complex, ``^H`` = conjugate transpose):
 
-    M = diag(invpsd) + sum_wfs P_w^H diag(|c|^2 (|gx|^2+|gy|^2)) P_w / neam_w^2
+    M = diag(invpsd) + sum_wfs P_w^H Mmid P_w / neam_w^2,
+    Mmid(f1, f2) = (conj(gx_f1) gx_f2 + conj(gy_f1) gy_f2) R(f2 - f1)
+    (R: autocorrelation of the kept selection spectrum, fdpcg_saselect; with
+    only its centre c kept, Mmid = c^2 (|gx|^2+|gy|^2) on the diagonal)
     (scaled by nx*ny when every layer has the same oversampling)
     Mbinv = pinv(Hermitian part of M), singular values below 1e-7 * max dropped
 """
@@ -41,13 +44,16 @@ class FdpcgTables:
     mhat_diag: np.ndarray = None   # float64 [nb, bs]
 
 
-def _saselect_center(nxp, nyp, dxp, salocx, salocy, saa):
-    """fdpcg_saselect (fdpcg.c:71): the clipped selection spectrum.
+def _saselect(nxp, nyp, dxp, salocx, salocy, saa):
+    """fdpcg_saselect (fdpcg.c:71): the clipped selection spectrum, as the
+    autocorrelation of its kept coefficients.
 
-    After clipping every coefficient whose magnitude is below the zero
-    frequency one, only the centre survives (checked here), and the
-    convolution operator built from it is that value times a shift, whose
-    effect cancels in sel^H sel."""
+    The selection spectrum (FFT of the full-subaperture corners on the pupil
+    grid) keeps every coefficient whose magnitude reaches the zero-frequency
+    one; spconvolvop (math/sp.c:926) makes it a cyclic convolution, so the
+    data term's sel^H sel couples pupil frequencies i and i + d with
+    R(d) = sum_s conj(v_{s+d}) v_s over the kept coefficients v.  Returns
+    {(dx, dy): R} (with only the centre kept: {(0, 0): c^2})."""
     xsel = np.zeros((nyp, nxp), dtype=np.complex128)
     offx, offy = nxp // 2, nyp // 2
     for x, y, a in zip(salocx, salocy, saa):
@@ -57,10 +63,13 @@ def _saselect_center(nxp, nyp, dxp, salocx, salocy, saa):
             xsel[iy, ix] = 1.0 / (nxp * nyp)
     f = np.fft.fftshift(np.fft.fft2(np.fft.fftshift(xsel)))
     c = f[nyp // 2, nxp // 2].real
-    keep = np.abs(f) >= c
-    if keep.sum() != 1:
-        raise NotImplementedError("FDPCG subaperture selection couples more than one frequency")
-    return c
+    ky, kx = np.nonzero(np.abs(f) >= c)
+    R = {}
+    for y1, x1 in zip(ky, kx):
+        for y2, x2 in zip(ky, kx):
+            d = ((x1 - x2) % nxp, (y1 - y2) % nyp)
+            R[d] = R.get(d, 0) + np.conj(f[y1, x1]) * f[y2, x2]
+    return R
 
 
 def _fdpcg_g(nx, ny, dx, dsa):
@@ -151,9 +160,8 @@ def fdpcg_prepare(sysm) -> FdpcgTables:
     nb = adimx * adimy
     nxtot = sum(a * b for a, b in zip(nx, ny))
 
-    c = _saselect_center(nxp, nyp, dxp, w0.salocx, w0.salocy, w0.saa)
-    gx, gy = _fdpcg_g(nxp, nyp, dxp, w0.dsa)
-    mmid = (c * c) * (np.abs(gx) ** 2 + np.abs(gy) ** 2)  # [iy, ix] shifted pupil grid
+    Rsel = _saselect(nxp, nyp, dxp, w0.salocx, w0.salocy, w0.saa)
+    gx, gy = _fdpcg_g(nxp, nyp, dxp, w0.dsa)  # [iy, ix] shifted pupil grid
     invpsd = [_invpsd_layer(nx[i], ny[i], sysm.xmaps[i].dx, cfg.r0, sysm.wt[i],
                             cfg.tomo_cxxscale, TOMOSCALE) for i in range(nps)]
     ht = np.array(cfg.atmr_ht, dtype=np.float64)
@@ -178,7 +186,9 @@ def fdpcg_prepare(sysm) -> FdpcgTables:
             lj.append((l, r % nx[l], r // nx[l]))
         diag = np.array([invpsd[l][jy, jx] for (l, jx, jy) in lj], dtype=np.float64)
         M = np.zeros((bs, bs), dtype=np.complex128)
-        # pupil frequencies aliasing to this block: centred kx = ix + adimx*m
+        # pupil frequencies aliasing to this block (centred kx = ix + adimx*m)
+        # and each WFS's propagation vector from them to the block's members
+        pf, pv = [], []
         for mxp in range(pos):
             for myp in range(pos):
                 kx = ix + adimx * mxp
@@ -187,9 +197,7 @@ def fdpcg_prepare(sysm) -> FdpcgTables:
                 ky = (ky + nyp2) % nyp - nyp2
                 pxi, pyi = kx + nxp2, ky + nyp2
                 fxg, fyg = kx * dkx, ky * dky
-                d = mmid[pyi, pxi]
-                if d == 0:
-                    continue
+                vw = []
                 for w in sysm.wfs:
                     v = np.zeros(bs, np.complex128)
                     for a, (l, jx, jy) in enumerate(lj):
@@ -212,7 +220,20 @@ def fdpcg_prepare(sysm) -> FdpcgTables:
                         else:
                             raise ValueError("unsupported layer/pupil sampling ratio")
                         v[a] = val / w.neam
-                    M += np.outer(np.conj(v), v) * d
+                    vw.append(v)
+                pf.append((pxi, pyi))
+                pv.append(vw)
+        # M += P^H Mmid P with Mmid(f1, f2) = sum_g conj(g_f1) g_f2 R(f2 - f1)
+        for i1, (x1, y1) in enumerate(pf):
+            for i2, (x2, y2) in enumerate(pf):
+                r = Rsel.get(((x2 - x1) % nxp, (y2 - y1) % nyp))
+                if r is None:
+                    continue
+                mm = (np.conj(gx[y1, x1]) * gx[y2, x2] + np.conj(gy[y1, x1]) * gy[y2, x2]) * r
+                if mm == 0:
+                    continue
+                for k in range(len(sysm.wfs)):
+                    M += np.outer(np.conj(pv[i1][k]), pv[i2][k]) * mm
         if not needscale:
             M *= nx[0] * ny[0]
             diag = diag * (nx[0] * ny[0])

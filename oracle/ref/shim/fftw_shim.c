@@ -6,7 +6,9 @@
  * smallest prime factor,
  *     X[k] = sum_{r<p} w_n^{r k} Y_r[k mod m],   Y_r = DFT_m( x[r + p j] ),
  * w_n = exp(sign*2*pi*i/n).  Prime lengths fall back to the direct O(n^2) sum.
- * Twiddles come from one table per transform, indexed by (r*k mod n).
+ * Twiddles come from one table per transform dim, made when the plan is made
+ * and indexed by (r*k mod n); a transform's workspace is allocated once per
+ * execution (no allocation per line or per recursion level).
  * Transforms are unnormalised, like FFTW.  Multi-dimensional and "many"
  * transforms are executed line by line over strided views; float plans run
  * through the double-precision kernel.
@@ -18,6 +20,7 @@
 #include <string.h>
 
 typedef double complex cplx;
+static cplx *twiddles(long n, int sign);
 
 enum { K_CPLX = 0, K_SPLIT = 1, K_R2HC = 2, K_HC2R = 3 };
 
@@ -31,13 +34,16 @@ struct maosref_fft_plan {
     fftw_iodim hdims[2];
     void *in, *out;          /* interleaved complex or real arrays */
     void *ri, *ii, *ro, *io; /* split arrays */
+    cplx *tw[3];             /* twiddles of each transform dim (made at plan time) */
 };
 
 /* x: n points; tw: twiddles of the top-level length N (tw[k] = w_N^k);
- * n divides N and w_n^e = tw[e * (N/n)]. */
-static void dft_rec(cplx *x, long n, const cplx *tw, long N, cplx *tmp) {
+ * n divides N and w_n^e = tw[e * (N/n)].  ws: workspace of 2n points (the
+ * children of a level reuse its second half). */
+static void dft_rec(cplx *x, long n, const cplx *tw, long N, cplx *ws) {
     if (n <= 1) return;
     const long ts = N / n;
+    cplx *tmp = ws;
     long p = 0;
     for (long f = 2; f * f <= n; f++) {
         if (n % f == 0) { p = f; break; }
@@ -54,9 +60,7 @@ static void dft_rec(cplx *x, long n, const cplx *tw, long N, cplx *tmp) {
     long m = n / p;
     for (long r = 0; r < p; r++)
         for (long j = 0; j < m; j++) tmp[r * m + j] = x[r + p * j];
-    cplx *scratch = (cplx *)malloc(sizeof(cplx) * m);
-    for (long r = 0; r < p; r++) dft_rec(tmp + r * m, m, tw, N, scratch);
-    free(scratch);
+    for (long r = 0; r < p; r++) dft_rec(tmp + r * m, m, tw, N, ws + n);
     for (long k = 0; k < n; k++) {
         cplx s = 0;
         long km = k % m;
@@ -65,17 +69,20 @@ static void dft_rec(cplx *x, long n, const cplx *tw, long N, cplx *tmp) {
     }
 }
 
-static void dft_line(cplx *buf, long n, int sign) {
-    if (n <= 1) return;
-    cplx *tw = (cplx *)malloc(sizeof(cplx) * n);
+/* twiddles w_n^k = exp(sign 2 pi i k / n), computed once per plan and dim */
+static cplx *twiddles(long n, int sign) {
+    cplx *tw = (cplx *)malloc(sizeof(cplx) * (n > 0 ? n : 1));
     for (long k = 0; k < n; k++) {
         double a = sign * 2.0 * M_PI * (double)k / (double)n;
         tw[k] = cos(a) + I * sin(a);
     }
-    cplx *tmp = (cplx *)malloc(sizeof(cplx) * n);
-    dft_rec(buf, n, tw, n, tmp);
-    free(tmp);
-    free(tw);
+    return tw;
+}
+
+/* one unnormalised line transform with the plan's twiddles; ws: 2n points */
+static void dft_line(cplx *buf, long n, const cplx *tw, cplx *ws) {
+    if (n <= 1) return;
+    dft_rec(buf, n, tw, n, ws);
 }
 
 /* element accessors on the four storage forms */
@@ -140,12 +147,12 @@ static void exec_complex(const struct maosref_fft_plan *pl) {
         for (int i = 0; i < pl->hrank; i++) others[no++] = pl->hdims[i];
         long nlines = 1;
         for (int i = 0; i < no; i++) nlines *= others[i].n;
-        cplx *buf = (cplx *)malloc(sizeof(cplx) * (n > 0 ? n : 1));
+        cplx *buf = (cplx *)malloc(sizeof(cplx) * 3 * (n > 0 ? n : 1));
         for (long l = 0; l < nlines; l++) {
             long rem = l, base = 0;
             for (int i = 0; i < no; i++) { long c = rem % others[i].n; rem /= others[i].n; base += c * others[i].os; }
             for (long j = 0; j < n; j++) buf[j] = load_c(pl, base + j * st);
-            dft_line(buf, n, pl->sign);
+            dft_line(buf, n, pl->tw[d], buf + n);
             for (long j = 0; j < n; j++) store_c(pl, base + j * st, buf[j]);
         }
         free(buf);
@@ -154,13 +161,13 @@ static void exec_complex(const struct maosref_fft_plan *pl) {
 
 static void exec_r2r(const struct maosref_fft_plan *pl) {
     long n = pl->dims[0].n;
-    cplx *buf = (cplx *)malloc(sizeof(cplx) * n);
+    cplx *buf = (cplx *)malloc(sizeof(cplx) * 3 * n);
     double *tmp = (double *)malloc(sizeof(double) * n);
     for (long j = 0; j < n; j++)
         tmp[j] = pl->single ? ((float *)pl->in)[j] : ((double *)pl->in)[j];
     if (pl->kind == K_R2HC) {
         for (long j = 0; j < n; j++) buf[j] = tmp[j];
-        dft_line(buf, n, -1);
+        dft_line(buf, n, pl->tw[0], buf + n);
         /* halfcomplex: r0 r1 .. r_{n/2} i_{(n+1)/2-1} .. i1 */
         for (long k = 0; k <= n / 2; k++) tmp[k] = creal(buf[k]);
         for (long k = 1; k < (n + 1) / 2; k++) tmp[n - k] = cimag(buf[k]);
@@ -170,7 +177,7 @@ static void exec_r2r(const struct maosref_fft_plan *pl) {
             buf[k] = tmp[k] + I * im;
         }
         for (long k = n / 2 + 1; k < n; k++) buf[k] = conj(buf[n - k]);
-        dft_line(buf, n, +1);
+        dft_line(buf, n, pl->tw[0], buf + n);
         for (long j = 0; j < n; j++) tmp[j] = creal(buf[j]);
     }
     for (long j = 0; j < n; j++) {
@@ -232,6 +239,18 @@ static struct maosref_fft_plan *mk_r2r(int n, void *in, void *out, fftw_r2r_kind
     pl->in = in; pl->out = out;
     return pl;
 }
+/* the twiddle tables of a finished plan (r2r: forward for R2HC, backward for HC2R) */
+static struct maosref_fft_plan *with_twiddles(struct maosref_fft_plan *pl) {
+    if (!pl) return pl;
+    const int sign = pl->kind == K_R2HC ? -1 : pl->kind == K_HC2R ? 1 : pl->sign;
+    for (int d = 0; d < pl->rank; d++) pl->tw[d] = twiddles(pl->dims[d].n, sign);
+    return pl;
+}
+static void plan_free(struct maosref_fft_plan *pl) {
+    if (!pl) return;
+    for (int d = 0; d < 3; d++) free(pl->tw[d]);
+    free(pl);
+}
 static void execute_any(const struct maosref_fft_plan *pl) {
     if (!pl) return;
     if (pl->kind == K_R2HC || pl->kind == K_HC2R) exec_r2r(pl);
@@ -240,27 +259,27 @@ static void execute_any(const struct maosref_fft_plan *pl) {
 
 /* ---- double API ---- */
 fftw_plan fftw_plan_dft_1d(int n, fftw_complex *in, fftw_complex *out, int sign, unsigned flags) {
-    (void)flags; return mk_1d(n, in, out, sign, 0);
+    (void)flags; return with_twiddles(mk_1d(n, in, out, sign, 0));
 }
 fftw_plan fftw_plan_dft_2d(int n0, int n1, fftw_complex *in, fftw_complex *out, int sign, unsigned flags) {
-    (void)flags; return mk_2d(n0, n1, in, out, sign, 0);
+    (void)flags; return with_twiddles(mk_2d(n0, n1, in, out, sign, 0));
 }
 fftw_plan fftw_plan_many_dft(int rank, const int *n, int howmany, fftw_complex *in, const int *inembed,
                              int istride, int idist, fftw_complex *out, const int *onembed, int ostride,
                              int odist, int sign, unsigned flags) {
     (void)flags;
-    return mk_many(rank, n, howmany, in, inembed, istride, idist, out, onembed, ostride, odist, sign, 0);
+    return with_twiddles(mk_many(rank, n, howmany, in, inembed, istride, idist, out, onembed, ostride, odist, sign, 0));
 }
 fftw_plan fftw_plan_guru_split_dft(int rank, const fftw_iodim *dims, int howmany_rank,
                                    const fftw_iodim *howmany_dims, double *ri, double *ii, double *ro,
                                    double *io, unsigned flags) {
-    (void)flags; return mk_split(rank, dims, howmany_rank, howmany_dims, ri, ii, ro, io, 0);
+    (void)flags; return with_twiddles(mk_split(rank, dims, howmany_rank, howmany_dims, ri, ii, ro, io, 0));
 }
 fftw_plan fftw_plan_r2r_1d(int n, double *in, double *out, fftw_r2r_kind kind, unsigned flags) {
-    (void)flags; return mk_r2r(n, in, out, kind, 0);
+    (void)flags; return with_twiddles(mk_r2r(n, in, out, kind, 0));
 }
 void fftw_execute(const fftw_plan p) { execute_any(p); }
-void fftw_destroy_plan(fftw_plan p) { free(p); }
+void fftw_destroy_plan(fftw_plan p) { plan_free(p); }
 int fftw_init_threads(void) { return 1; }
 void fftw_plan_with_nthreads(int nthreads) { (void)nthreads; }
 void fftw_cleanup_threads(void) {}
@@ -270,27 +289,27 @@ void fftw_export_wisdom_to_file(FILE *f) { (void)f; }
 
 /* ---- float API ---- */
 fftwf_plan fftwf_plan_dft_1d(int n, fftwf_complex *in, fftwf_complex *out, int sign, unsigned flags) {
-    (void)flags; return mk_1d(n, in, out, sign, 1);
+    (void)flags; return with_twiddles(mk_1d(n, in, out, sign, 1));
 }
 fftwf_plan fftwf_plan_dft_2d(int n0, int n1, fftwf_complex *in, fftwf_complex *out, int sign, unsigned flags) {
-    (void)flags; return mk_2d(n0, n1, in, out, sign, 1);
+    (void)flags; return with_twiddles(mk_2d(n0, n1, in, out, sign, 1));
 }
 fftwf_plan fftwf_plan_many_dft(int rank, const int *n, int howmany, fftwf_complex *in, const int *inembed,
                                int istride, int idist, fftwf_complex *out, const int *onembed, int ostride,
                                int odist, int sign, unsigned flags) {
     (void)flags;
-    return mk_many(rank, n, howmany, in, inembed, istride, idist, out, onembed, ostride, odist, sign, 1);
+    return with_twiddles(mk_many(rank, n, howmany, in, inembed, istride, idist, out, onembed, ostride, odist, sign, 1));
 }
 fftwf_plan fftwf_plan_guru_split_dft(int rank, const fftwf_iodim *dims, int howmany_rank,
                                      const fftwf_iodim *howmany_dims, float *ri, float *ii, float *ro,
                                      float *io, unsigned flags) {
-    (void)flags; return mk_split(rank, dims, howmany_rank, howmany_dims, ri, ii, ro, io, 1);
+    (void)flags; return with_twiddles(mk_split(rank, dims, howmany_rank, howmany_dims, ri, ii, ro, io, 1));
 }
 fftwf_plan fftwf_plan_r2r_1d(int n, float *in, float *out, fftwf_r2r_kind kind, unsigned flags) {
-    (void)flags; return mk_r2r(n, in, out, kind, 1);
+    (void)flags; return with_twiddles(mk_r2r(n, in, out, kind, 1));
 }
 void fftwf_execute(const fftwf_plan p) { execute_any(p); }
-void fftwf_destroy_plan(fftwf_plan p) { free(p); }
+void fftwf_destroy_plan(fftwf_plan p) { plan_free(p); }
 int fftwf_init_threads(void) { return 1; }
 void fftwf_plan_with_nthreads(int nthreads) { (void)nthreads; }
 void fftwf_cleanup_threads(void) {}

@@ -50,8 +50,22 @@ def test_tomo_operators_match_reference(name, split, ref_proc):
     assert rel(o.tomo_L(x, alpha=-0.5), R.call("tomoL", x, -0.5)) < 1e-12
 
 
-def test_fdpcg_tables_and_apply_match_reference(ref_proc, mcao):
-    s = mcao
+def fdpcg_system(name):
+    """A preset with the FDPCG preconditioner: the 30 m system as configured,
+    and the 8 m systems switched to FDPCG, whose clipped subaperture-selection
+    spectrum keeps four frequencies (fdpcg_saselect, maos/fdpcg.c:71)."""
+    from conftest import get_system
+    if name == "mcao_30m":
+        return get_system(name)
+    from maos_b200 import config, geometry
+    cfg = config.PRESETS[name]()
+    cfg.tomo_precond = 1
+    return geometry.build_tomo(cfg)
+
+
+@pytest.mark.parametrize("name", ["mcao_30m", "ltao_8m", "scao_8m"])
+def test_fdpcg_tables_and_apply_match_reference(ref_proc, name):
+    s = fdpcg_system(name)
     R = ref_proc
     R.call("setup", refbridge.system_desc(s, split=1))
     fd = R.call("fdpcg_prepare")

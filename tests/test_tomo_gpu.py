@@ -20,11 +20,21 @@ def rel(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
 
 
-@pytest.fixture(scope="module", params=["ltao_8m", "mcao_30m"])
+def fdpcg_variant(name):
+    """The 8 m LTAO system with the FDPCG preconditioner: its subaperture
+    selection keeps four frequencies (the general fdpcg_saselect case)."""
+    from maos_b200 import config, geometry
+    cfg = config.PRESETS[name]()
+    cfg.tomo_precond = 1
+    return geometry.build_tomo(cfg)
+
+
+@pytest.fixture(scope="module", params=["ltao_8m", "mcao_30m", "ltao_8m_fdpcg"])
 def setup(request):
     from conftest import get_system
     from maos_b200.recon import Reconstructor
-    s = get_system(request.param)
+    name = request.param
+    s = fdpcg_variant(name[:-6]) if name.endswith("_fdpcg") else get_system(name)
     R = Reconstructor(s, nbatch=2)
     yield s, R, TomoOracle(s)
     R.close()
