@@ -252,11 +252,25 @@ int mb_recon_serve_step(mb_recon *r, const int *active, const float *grad, float
 /* Autotuner (no counterpart in the reference): times the tomography
  * operator with each admissible row blocking of its pupil-grid kernel (4, 8,
  * 16 pupil rows per CTA, and every even split of the pupil rows into blocks
- * of 4 to 32 rows) on this batch size, keeps the fastest and captures the
- * step graphs again.  Results do not depend on the choice.  rows (may be
+ * of 4 to 32 rows) on this batch size, keeps the fastest, then times whole
+ * tomography steps with each form of the FDPCG preconditioner
+ * (mb_fdpcg_mode) and keeps the faster, and captures the step graphs again;
+ * the instances restart cold.  The row blocking does not change results, the
+ * preconditioner's form changes them only at FP32 rounding.  rows (may be
  * NULL): the blocking kept; ms (may be NULL, 3 floats): ms per operator for
  * 4, 8, 16 rows, -1 where a blocking does not fit. */
 int mb_autotune(mb_recon *r, int reps, int *rows, float *ms);
+
+/* Form of the FDPCG preconditioner inside the CG step (no counterpart in the
+ * reference; mb_autotune picks the faster for the batch size): 1 = three
+ * kernels (forward FFTs of every (layer, instance), block solve sharing the
+ * blocks over instances, inverse FFTs), 2 = one kernel per step in which the
+ * layers of an instance are split over one thread-block cluster of up to 16
+ * CTAs that exchange rows, columns and block members through distributed
+ * shared memory, 0 = 2 when that cluster fits on the device.  Results agree
+ * to FP32 rounding.  The step graphs are captured again.  Returns the form
+ * in use (1 or 2) or a negative MB_E* code. */
+int mb_fdpcg_mode(mb_recon *r, int mode);
 
 /* Servo filter on the device (no GPU counterpart in the reference; the CPU
  * code is lib/servo.c servo_new / servo_filter / servo_reset, used by

@@ -268,6 +268,15 @@ struct Recon {
                   bool in_cg = false, float *xupd = nullptr, const float *pupd = nullptr,
                   const float *Apupd = nullptr, float *pnext = nullptr);
     bool fd_cluster = false;  // k_fd_inv<true> fits as clusters of nps CTAs
+    // the fused preconditioner (k_fd_fused): an instance's layers split over
+    // one cluster of fused_tab.C CTAs; fd_mode 1 = three kernels, 2 = fused
+    bool fd_fused_ok = false;
+    int fd_mode = 1;
+    FdFusedTab fused_tab{};
+    DevBuf<FdMem> fd_mem;
+    size_t fd_fsmem = 0;
+    void build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector<long> &hoff);
+    void set_fdpcg_mode(int mode);
     void enqueue_solve(cudaStream_t s);
     struct CgBufs {
         float *x, *r, *p, *z, *Ap, *rhs;
@@ -852,7 +861,127 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
         cudaGetLastError();  // a size the device refuses only means the unclustered path
         if (const char *e = std::getenv("MAOS_B200_FD_CLUSTER")) fd_cluster = fd_cluster && e[0] != '0';
     }
+    build_fdpcg_fused(idx, hoff);
+}
 
+// Split each layer over K_l CTAs of an instance's cluster (K_l proportional
+// to its size, at most 16 CTAs in all), the CTAs' row-pair, column and block
+// ranges, the common shared-memory layout, and each block member's owner.
+void Recon::build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector<long> &hoff) {
+    fd_fused_ok = false;
+    fd_mode = 1;
+    long nmin = LONG_MAX;
+    for (int l = 0; l < nps; l++) nmin = std::min(nmin, (long)lay_h[l].nx * lay_h[l].ny);
+    std::vector<int> K(nps);
+    int C = 0;
+    for (int l = 0; l < nps; l++) {
+        const FdLayer &F = fdtab.l[l];
+        K[l] = (int)std::max(1L, std::lround((double)F.nx * F.ny / (double)nmin));
+        K[l] = std::min(K[l], std::min(F.ny / 2, F.nx / 2 + 1));
+        C += K[l];
+    }
+    while (C > kMaxFdParts) {  // take CTAs from the most split layer
+        int lm = 0;
+        for (int l = 1; l < nps; l++)
+            if (K[l] > K[lm]) lm = l;
+        if (K[lm] <= 1) return;  // more layers than cluster CTAs: the three-kernel form only
+        K[lm]--;
+        C--;
+    }
+    FdFusedTab T{};
+    T.C = C;
+    int maxnx = 0, maxny = 0;
+    long nR = kFftThreads, nS = 0, nSR = 0, nSC = 0;
+    int rank = 0;
+    std::vector<int> rbase(nps);
+    for (int l = 0; l < nps; l++) {
+        const FdLayer &F = fdtab.l[l];
+        const int np2 = F.ny / 2, h = F.nx / 2 + 1;
+        maxnx = std::max(maxnx, F.nx);
+        maxny = std::max(maxny, F.ny);
+        rbase[l] = rank;
+        for (int q = 0; q < K[l]; q++, rank++) {
+            FdPart &P = T.c[rank];
+            P.l = (short)l;
+            P.q = (short)q;
+            P.K = (short)K[l];
+            P.rbase = (short)rbase[l];
+            P.p0 = (short)(q * np2 / K[l]);
+            P.p1 = (short)((q + 1) * np2 / K[l]);
+            P.c0 = (short)(q * h / K[l]);
+            P.c1 = (short)((q + 1) * h / K[l]);
+            P.b0 = (int)((long)rank * fd_nbh / C);
+            P.b1 = (int)((long)(rank + 1) * fd_nbh / C);
+            const int npr = P.p1 - P.p0, ncl = P.c1 - P.c0;
+            MB_REQUIRE(npr >= 1 && ncl >= 1, "fdpcg: layer %d split %d is empty", l, q);
+            nR = std::max(nR, (long)npr * F.nx);
+            nS = std::max(nS, (long)(F.px >= 0 ? fft2_scratch(F.px, true, npr) : npr * F.nx));
+            nS = std::max(nS, (long)(F.py >= 0 ? fft2_scratch(F.py, false, ncl) : (long)F.ny * ncl));
+            nSR = std::max(nSR, 2L * npr * h);
+            nSC = std::max(nSC, (long)F.ny * ncl);
+        }
+    }
+    for (int c = 0; c < C; c++)  // the rank's blocks are uniform over the whole cluster
+        MB_REQUIRE(T.c[c].b1 > T.c[c].b0, "fdpcg: fewer frequency blocks than cluster CTAs");
+    T.oTY = maxnx;
+    T.oR = maxnx + maxny;
+    T.oS = (int)(T.oR + nR);
+    T.oSR = (int)(T.oS + nS);
+    T.oSC = (int)(T.oSR + nSR);
+    T.oSY = (int)(T.oSC + nSC);
+    fd_fsmem = (size_t)(T.oSY + nSC) * sizeof(cplx);
+    if (fd_fsmem > 110 * 1024) return;  // two CTAs per SM or the three-kernel form
+    // member owners: the CTA whose columns hold the member's bin
+    std::vector<FdMem> mem(idx.size());
+    for (size_t i = 0; i < idx.size(); i++) {
+        int l = 0;
+        while (l + 1 < nps && idx[i].base >= hoff[l + 1]) l++;
+        const FdLayer &F = fdtab.l[l];
+        const int h = F.nx / 2 + 1;
+        const long pos = idx[i].base - hoff[l];  // instance 0's half spectrum of layer l
+        MB_REQUIRE(pos >= 0 && pos < (long)F.ny * h, "fdpcg: member %zu outside its layer", i);
+        const int ky = (int)(pos / h), kx = (int)(pos % h);
+        int q = K[l] - 1;
+        while (T.c[rbase[l] + q].c0 > kx) q--;
+        const FdPart &O = T.c[rbase[l] + q];
+        mem[i].rank = (short)(rbase[l] + q);
+        mem[i].off = ky * (O.c1 - O.c0) + (kx - O.c0);
+        mem[i].flags = (short)idx[i].flags;
+    }
+    // the cluster must be schedulable
+    if (C > 8) {
+        if (cudaFuncSetAttribute(k_fd_fused, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+    }
+    MB_CUDA_TRY(cudaFuncSetAttribute(k_fd_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd_fsmem));
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C, nb);
+    cfg.blockDim = dim3(kFftThreads);
+    cfg.dynamicSmemBytes = fd_fsmem;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    const bool fits = cudaOccupancyMaxActiveClusters(&ncl, k_fd_fused, &cfg) == cudaSuccess && ncl > 0;
+    cudaGetLastError();
+    if (!fits) return;
+    fd_mem.upload(mem);
+    fused_tab = T;
+    fd_fused_ok = true;
+}
+
+// 1: three kernels per preconditioner (k_fd_fwd, k_fd_mul, k_fd_inv);
+// 2: the fused cluster kernel (when it fits); 0: the fused one when it fits.
+// The step graphs are captured again.
+void Recon::set_fdpcg_mode(int mode) {
+    fd_mode = (mode == 2 || mode == 0) && fd_fused_ok ? 2 : 1;
+    if (graph) capture_graph();
 }
 
 // FDPCG blocks from the stored data term at the current l2c: the invpsd
@@ -996,6 +1125,12 @@ bool Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k
                      float *xupd, const float *pupd, const float *Apupd, float *pnext) {
     // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT,
     // on the half spectrum as in cuda/fdpcg.cu (fdpcg_mul_block_sync_half)
+    if (in_cg && pnext && fd_mode == 2) {  // one launch: layers split over an instance's cluster
+        launch_cluster(k_fd_fused, dim3(fused_tab.C, nb), dim3(kFftThreads), fd_fsmem, s, fused_tab.C, rin, fdtab,
+                       fused_tab, fd_tw.p, fd_M.p, fd_mem.p, fd_bs, nxtot, xupd, Apupd, scal(), k, init, act(),
+                       pnext);
+        return true;
+    }
     launch(k_fd_fwd, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, rin, spec.p, fdtab, fd_tw.p, nxtot, fd_bufn, xupd,
                                                         pupd, Apupd, xupd ? ab.p : nullptr, act());
     const int per = kThreads / fd_bs;
@@ -1367,26 +1502,31 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
     const double nbk = (double)fd_nbh * fd_bs;  // block members (spectrum bins read by k_fd_mul)
     double nh = 0;                              // half-spectrum bins per instance
     for (int l = 0; l < nps; l++) nh += (double)lay_h[l].ny * (lay_h[l].nx / 2 + 1);
-    const double by[7] = {
+    const double by[8] = {
         B * (F * nx + F * trow) + (double)hx.fwd.n * sizeof(AxisW) + tab_wfs + (double)xpad.n * sizeof(GatherW),
         B * (F * trow + 2 * F * nx) + (double)ypad.n * sizeof(GatherW),       // t, p -> Ap
         B * (6 * F * nx),                                                    // x,r,p,Ap read; x,r written
         B * (3 * F * nx),                                                    // p,z read; p written
         B * (6 * F * nx + 8.0 * nh),                          // x,r,p,Ap read; x,r written; spectrum written
         B * (2 * 8.0 * nbk) + 8.0 * fd_bs * fd_bs * fd_nbh + (double)sizeof(FdIndex) * nbk,  // X, Y; M, idx once
-        B * (8.0 * nh + (fd_cluster ? 3 : 2) * F * nx)};      // spectrum, r read; p read+written (or z written)
+        B * (8.0 * nh + (fd_cluster ? 3 : 2) * F * nx),       // spectrum, r read; p read+written (or z written)
+        // fused: x, r, p, Ap read, x, r written, r read again, p written; M and the member table once
+        B * (9 * F * nx) + 8.0 * fd_bs * fd_bs * fd_nbh + (double)sizeof(FdMem) * nbk};
     // launches per step: with the preconditioner the x/r update of all but
     // the last iteration runs inside k_fd_fwd (timed with it), and with the
     // clustered inverse the p update runs inside k_fd_inv (timed with it)
     const bool pin = precond && fd_cluster;
-    const int lps[7] = {maxit + 2, maxit + 2, precond ? 1 : maxit, pin ? 0 : maxit, precond ? maxit : 0,
-                        precond ? maxit : 0, precond ? maxit : 0};
+    const bool fused = precond && fd_mode == 2;
+    const int nsep = precond && !fused ? maxit : 0;
+    const int lps[8] = {maxit + 2, maxit + 2, precond ? 1 : maxit, (pin || fused) ? 0 : maxit, nsep, nsep, nsep,
+                        fused ? maxit : 0};
     const int per = kThreads / std::max(fd_bs, 1);
     for (int st = 0; st < ns; st++) {
         bytes[st] = by[st];
         launches[st] = lps[st];
         ms[st] = 0.f;
         if (st >= 4 && !precond) continue;
+        if (st == 7 && !fd_fused_ok) continue;
         // the vectors written here are scratch (z, rhs, spectra): the warm
         // start in x, r and p is left as it was
         auto run_stage = [&]() {
@@ -1408,6 +1548,11 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                 case 5:
                     launch(k_fd_mul, dim3((fd_nbh + per - 1) / per, (nb + kFdInst - 1) / kFdInst), dim3(kThreads),
                            0, stream, spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh, fd_bs, nb, act());
+                    break;
+                case 7:  // fused: scratch vectors (rhs as r, z as x, Ap, rhs as p)
+                    launch_cluster(k_fd_fused, dim3(fused_tab.C, nb), dim3(kFftThreads), fd_fsmem, stream,
+                                   fused_tab.C, rhs.p, fdtab, fused_tab, fd_tw.p, fd_M.p, fd_mem.p, fd_bs, nxtot,
+                                   z.p, Ap.p, scal(), 0, 0, act(), z.p);
                     break;
                 case 6:
                     if (pin)
@@ -1470,10 +1615,30 @@ int Recon::autotune(int reps, float *ms_out) {
             best = cand[c];
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     set_pupil_rows(best);
     capture_graph();
+    // the preconditioner's form: three kernels, or one fused cluster kernel,
+    // timed as whole tomography steps (graph launches)
+    if (precond && fd_fused_ok) {
+        float tmode[3] = {0, 0, 0};
+        for (int mode = 1; mode <= 2; mode++) {
+            set_fdpcg_mode(mode);
+            MB_CUDA_TRY(cudaGraphLaunch(graph, stream));  // warm
+            MB_CUDA_TRY(cudaEventRecord(e0, stream));
+            const int nrep = std::max(2, reps / 4);
+            for (int i = 0; i < nrep; i++) MB_CUDA_TRY(cudaGraphLaunch(graph, stream));
+            MB_CUDA_TRY(cudaEventRecord(e1, stream));
+            MB_CUDA_TRY(cudaEventSynchronize(e1));
+            MB_CUDA_TRY(cudaEventElapsedTime(&tmode[mode], e0, e1));
+        }
+        set_fdpcg_mode(tmode[2] < tmode[1] ? 2 : 1);
+        // the timing steps moved the warm start: start the instances cold again
+        x.zero_async(stream);
+        if (has_fit) fa.zero_async(stream);
+        MB_CUDA_TRY(cudaStreamSynchronize(stream));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     return best;
 }
 
@@ -1825,7 +1990,7 @@ int mb_apply_fit_L(mb_recon *h, const double *ain, double *aout) {
 void *mb_recon_stream(mb_recon *h) { return h ? (void *)h->R.stream : nullptr; }
 
 static const char *kStageNames[] = {"lhs_pupil", "lhs_layer", "cg_update_xr", "cg_update_p",
-                                    "fd_fwd",    "fd_mul",    "fd_inv"};
+                                    "fd_fwd",    "fd_mul",    "fd_inv",       "fd_fused"};
 int mb_num_stages(void) { return (int)(sizeof(kStageNames) / sizeof(kStageNames[0])); }
 const char *mb_stage_name(int i) { return (i >= 0 && i < mb_num_stages()) ? kStageNames[i] : ""; }
 
@@ -1833,6 +1998,17 @@ int mb_time_stages(mb_recon *h, int reps, float *ms, double *bytes, int *launche
     MB_API_BEGIN
     MB_REQUIRE(h && ms && bytes && launches && reps > 0, "invalid arguments");
     h->R.time_stages(reps, ms, bytes, launches);
+    MB_API_END
+}
+
+int mb_fdpcg_mode(mb_recon *h, int mode) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && mode >= 0 && mode <= 2, "invalid arguments");
+    mb::Recon &R = h->R;
+    MB_REQUIRE(R.precond, "reconstructor has no FDPCG preconditioner");
+    MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
+    R.set_fdpcg_mode(mode);
+    return R.fd_mode;
     MB_API_END
 }
 

@@ -1635,6 +1635,311 @@ k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restr
     }
 }
 
+// ---------------------------------------------------------------------------
+// The whole preconditioner of one CG step in one launch, for small batches.
+//
+// An instance's layers are split over the CTAs of one thread-block cluster
+// (at most 16): layer l gets K_l CTAs, K_l proportional to its size, so a
+// 96 x 96 ground layer is transformed by 4 CTAs and a 48 x 48 one by 1.  A
+// CTA owns a range of row pairs and a range of half-spectrum columns of its
+// layer.  Phases, separated by cluster barriers, with the data exchanged
+// through distributed shared memory (ld/st.shared::cluster):
+//   F1  x += a p, r -= a Ap on its row pairs (the CG update, when ab is set),
+//       row FFTs of r, unpacking into the half-spectrum rows (SR);
+//   F2  its columns gathered from the row owners' SR, column FFTs (SC);
+//   M   its share of the frequency blocks: members gathered from the column
+//       owners' SC, Y = Mbinv X, each stored bin written into its owner's SY;
+//   I1  inverse column FFTs of SY;
+//   I2  its row pairs gathered from the column owners' SY (Hermitian mirror),
+//       inverse row FFTs, then r.z over the cluster, beta and p = z + beta p.
+// Every shared-memory region sits at the same offset in every CTA of the
+// kernel, so a peer's copy is the local address mapped to the peer's rank.
+// ---------------------------------------------------------------------------
+constexpr int kMaxFdParts = 16;  // CTAs in an instance's cluster
+struct FdPart {
+    short l, q, K, rbase;  // layer, split index, splits of the layer, cluster rank of its split 0
+    short p0, p1;          // row pairs [p0, p1)
+    short c0, c1;          // half-spectrum columns [c0, c1)
+    int b0, b1;            // frequency blocks solved [b0, b1)
+};
+struct FdFusedTab {
+    FdPart c[kMaxFdParts];
+    int C;                 // CTAs per instance (cluster size)
+    int oTY, oR, oS, oSR, oSC, oSY;  // shared-memory offsets (complex elements); twiddles x at 0
+};
+// One member of a solved block: the cluster rank that owns its bin, the bin's
+// offset in that CTA's SC / SY, and the conjugate / store flags of FdIndex.
+struct FdMem {
+    int off;
+    short rank;
+    short flags;
+};
+
+__device__ __forceinline__ unsigned dsm_base(const void *local, unsigned rank) {
+    const unsigned la = (unsigned)__cvta_generic_to_shared(local);
+    unsigned ra;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(la), "r"(rank));
+    return ra;
+}
+__device__ __forceinline__ cplx dsm_ld(unsigned a) {
+    float x, y;
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(x), "=f"(y) : "r"(a) : "memory");
+    return make_float2(x, y);
+}
+__device__ __forceinline__ double dsm_ld_f64(unsigned a) {
+    double t;
+    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(t) : "r"(a) : "memory");
+    return t;
+}
+__device__ __forceinline__ void dsm_st(unsigned a, cplx v) {
+    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
+}
+
+// The transform of fft_dir with its result moved back into a (the shared
+// layout peers read needs the result at a fixed place).  Ends with a barrier.
+template <bool ROWS>
+__device__ void fft_dir_inplace(int pair, cplx *a, cplx *b, int n, int count, int ld, const signed char *rad,
+                                int nr, const cplx *tw, bool inv) {
+    const cplx *res = fft_dir<ROWS>(pair, a, b, n, count, ld, rad, nr, tw, inv);
+    if (res != a) {
+        const int tot = ROWS ? count * ld : n * ld;
+        for (int i = threadIdx.x; i < tot; i += blockDim.x) a[i] = res[i];
+        __syncthreads();
+    }
+}
+
+// grid: (C, nb), clusters of C CTAs along x; block: kFftThreads.
+__global__ void __launch_bounds__(kFftThreads, 2)
+k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid_constant__ FdFusedTab fu,
+           const cplx *__restrict__ tw, const cplx *__restrict__ M, const FdMem *__restrict__ mem, int bs,
+           long nxtot, float *__restrict__ xw, const float *__restrict__ Apv, CgScal SC, int kit, int init,
+           const int *__restrict__ act, float *__restrict__ pv) {
+    pdl_enter();
+    // an instance's CTAs are one cluster: all return or none does
+    if (inactive(act, blockIdx.y)) return;
+    extern __shared__ cplx fsm[];
+    __shared__ double sh[32];
+    const FdPart P = fu.c[blockIdx.x];
+    const FdLayer &L = ft.l[P.l];
+    const int b = blockIdx.y;
+    const int nx = L.nx, ny = L.ny, h = nx / 2 + 1;
+    const int npr = P.p1 - P.p0, ncl = P.c1 - P.c0;
+    cplx *twx = fsm, *twy = fsm + fu.oTY, *R = fsm + fu.oR, *S = fsm + fu.oS;
+    cplx *SR = fsm + fu.oSR, *SCb = fsm + fu.oSC, *SY = fsm + fu.oSY;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) twx[i] = tw[L.twx + i];
+    for (int i = threadIdx.x; i < ny; i += blockDim.x) twy[i] = tw[L.twy + i];
+    const size_t base = (size_t)b * nxtot + L.off;
+    float *rb = r + base;
+    const int xs = blockDim.x / nx, x0 = threadIdx.x / nx, xc = threadIdx.x - x0 * nx;  // nx <= blockDim
+    // ---- F1: CG update and row FFTs of this CTA's row pairs
+    if (x0 < xs) {
+        const float a = SC.ab ? SC.ab[2 * b] : 0.f;
+        for (int p0 = P.p0 + x0; p0 < P.p1; p0 += kFdLoads * xs) {
+            float rv[kFdLoads][2], xv[kFdLoads][2], pp[kFdLoads][2], qq[kFdLoads][2];
+#pragma unroll
+            for (int u = 0; u < kFdLoads; u++) {
+                const int p = p0 + u * xs;
+                if (p < P.p1) {
+                    const int o0 = (2 * p) * nx + xc, o1 = o0 + nx;
+                    rv[u][0] = rb[o0];
+                    rv[u][1] = rb[o1];
+                    if (xw) {
+                        xv[u][0] = xw[base + o0];
+                        xv[u][1] = xw[base + o1];
+                        pp[u][0] = pv[base + o0];
+                        pp[u][1] = pv[base + o1];
+                        qq[u][0] = Apv[base + o0];
+                        qq[u][1] = Apv[base + o1];
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kFdLoads; u++) {
+                const int p = p0 + u * xs;
+                if (p < P.p1) {
+                    const int o0 = (2 * p) * nx + xc, o1 = o0 + nx;
+                    float r0 = rv[u][0], r1 = rv[u][1];
+                    if (xw) {
+                        xw[base + o0] = xv[u][0] + a * pp[u][0];
+                        xw[base + o1] = xv[u][1] + a * pp[u][1];
+                        r0 -= a * qq[u][0];
+                        r1 -= a * qq[u][1];
+                        rb[o0] = r0;
+                        rb[o1] = r1;
+                    }
+                    R[(p - P.p0) * nx + xc] = make_float2(r0, r1);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    fft_dir_inplace<true>(L.px, R, S, nx, npr, nx, L.rx, L.nrx, twx, false);
+    {
+        const int hs_ = blockDim.x / h, h0 = threadIdx.x / h, k = threadIdx.x - h0 * h;
+        for (int p = h0; h0 < hs_ && p < npr; p += hs_) {
+            const cplx zk = R[p * nx + k], zm = cconj(R[p * nx + (k == 0 ? 0 : nx - k)]);
+            SR[(2 * p) * h + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+            const cplx d = csub(zk, zm);
+            SR[(2 * p + 1) * h + k] = make_float2(0.5f * d.y, -0.5f * d.x);  // -i/2 (zk - conj(z_-k))
+        }
+    }
+    cluster_sync_all();  // B1: every CTA's half-spectrum rows are in its SR
+    // ---- F2: this CTA's columns from the row owners, column FFTs
+    for (int it = threadIdx.x; it < ny * ncl; it += blockDim.x) {
+        const int i = it / ncl, c = it - i * ncl;  // row i, local column c
+        const int pr = i >> 1;
+        int q = P.K - 1;
+        while (fu.c[P.rbase + q].p0 > pr) q--;
+        const FdPart O = fu.c[P.rbase + q];
+        const unsigned ra = dsm_base(SR, (unsigned)(P.rbase + q));
+        SCb[i * ncl + c] = dsm_ld(ra + 8u * (unsigned)((i - 2 * O.p0) * h + P.c0 + c));
+    }
+    __syncthreads();
+    fft_dir_inplace<false>(L.py, SCb, S, ny, ncl, ncl, L.ry, L.nry, twy, false);
+    cluster_sync_all();  // B2: spectra final in every SC; no SR is read any more
+    // ---- M: this CTA's frequency blocks
+    {
+        const int per = blockDim.x / bs;
+        const int lb = threadIdx.x / bs, i = threadIdx.x - lb * bs;
+        cplx *xsb = R;  // staging of the gathered members (R is free now)
+        for (int blk0 = P.b0; blk0 < P.b1; blk0 += per) {
+            const int blk = blk0 + lb;
+            const bool live = lb < per && blk < P.b1;
+            FdMem e{};
+            cplx m[kMaxBs];
+            if (live) {
+                e = mem[(size_t)blk * bs + i];
+                const cplx *Mb = M + (size_t)blk * bs * bs + i;
+#pragma unroll
+                for (int jj = 0; jj < kMaxBs; jj++) m[jj] = jj < bs ? Mb[jj * bs] : make_float2(0.f, 0.f);
+                cplx xv = dsm_ld(dsm_base(SCb, (unsigned)e.rank) + 8u * (unsigned)e.off);
+                if (e.flags & kFdConj) xv.y = -xv.y;
+                xsb[threadIdx.x] = xv;
+            }
+            __syncthreads();
+            if (live && (e.flags & kFdStore)) {
+                const cplx *xb = xsb + lb * bs;
+                float re = 0.f, im = 0.f;
+#pragma unroll
+                for (int jj = 0; jj < kMaxBs; jj++) {
+                    if (jj < bs) {
+                        const cplx xv = xb[jj];
+                        re += m[jj].x * xv.x - m[jj].y * xv.y;
+                        im += m[jj].x * xv.y + m[jj].y * xv.x;
+                    }
+                }
+                dsm_st(dsm_base(SY, (unsigned)e.rank) + 8u * (unsigned)e.off,
+                       make_float2(re, (e.flags & kFdConj) ? -im : im));
+            }
+            __syncthreads();
+        }
+    }
+    cluster_sync_all();  // B3: every stored bin of every SY written; no SC is read any more
+    // ---- I1: inverse column FFTs
+    fft_dir_inplace<false>(L.py, SY, S, ny, ncl, ncl, L.ry, L.nry, twy, true);
+    cluster_sync_all();  // B4: inverse columns final in every SY
+    // ---- I2: this CTA's row pairs from the column owners, inverse row FFTs
+    for (int it = threadIdx.x; it < npr * nx; it += blockDim.x) {
+        const int pl = it / nx, k = it - pl * nx;
+        const int p = P.p0 + pl;
+        const bool hi = k > nx / 2;
+        const int kk = hi ? nx - k : k;
+        int q = P.K - 1;
+        while (fu.c[P.rbase + q].c0 > kk) q--;
+        const FdPart O = fu.c[P.rbase + q];
+        const int on = O.c1 - O.c0;
+        const unsigned ra = dsm_base(SY, (unsigned)(P.rbase + q)) + 8u * (unsigned)(kk - O.c0);
+        cplx a = dsm_ld(ra + 8u * (unsigned)((2 * p) * on));
+        cplx c = dsm_ld(ra + 8u * (unsigned)((2 * p + 1) * on));
+        if (kk == 0 || kk == nx / 2) {
+            a.y = 0.f;
+            c.y = 0.f;
+        }
+        if (hi) {
+            a = cconj(a);
+            c = cconj(c);
+        }
+        R[pl * nx + k] = make_float2(a.x - c.y, a.y + c.x);  // a + i c
+    }
+    __syncthreads();
+    fft_dir_inplace<true>(L.px, R, S, nx, npr, nx, L.rx, L.nrx, twx, true);
+    double v = 0;
+    if (x0 < xs)
+        for (int p0 = P.p0 + x0; p0 < P.p1; p0 += kFdLoads * xs) {
+            float rv[kFdLoads][2];
+#pragma unroll
+            for (int u = 0; u < kFdLoads; u++) {
+                const int p = p0 + u * xs;
+                if (p < P.p1) {
+                    const size_t o0 = (size_t)(2 * p) * nx + xc;
+                    rv[u][0] = rb[o0];
+                    rv[u][1] = rb[o0 + nx];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kFdLoads; u++) {
+                const int p = p0 + u * xs;
+                if (p < P.p1) {
+                    const cplx q = R[(p - P.p0) * nx + xc];
+                    v += (double)q.x * rv[u][0] + (double)q.y * rv[u][1];
+                }
+            }
+        }
+    v = block_sum(v, sh);
+    __shared__ double s_part, s_be;
+    if (threadIdx.x == 0) s_part = v;
+    cluster_sync_all();  // B5: every rank's r.z partial is in its shared memory; no SY is read any more
+    if (threadIdx.x < 32) {
+        // lane i reads rank i, in rank order
+        double t = 0;
+        if (threadIdx.x < fu.C) t = dsm_ld_f64(dsm_base(&s_part, (unsigned)threadIdx.x));
+        t = warp_sum(t);
+        if (threadIdx.x == 0) {
+            double be = 0;
+            if (!init) {
+                be = t / SC.sc[(size_t)b * SC.nsc + kit];
+                if (!isfinite(be)) be = 0;
+            }
+            s_be = be;
+            if (blockIdx.x == 0) {  // rank 0 keeps the CG scalars
+                if (init) {
+                    SC.sc[(size_t)b * SC.nsc] = t;
+                } else {
+                    SC.ab[2 * b + 1] = (float)be;
+                    SC.sc[(size_t)b * SC.nsc + kit + 1] = t;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");  // done reading the others
+    const float be = (float)s_be;
+    if (x0 < xs)
+        for (int p0 = P.p0 + x0; p0 < P.p1; p0 += kFdLoads * xs) {
+            float pp[kFdLoads][2];
+#pragma unroll
+            for (int u = 0; u < kFdLoads; u++) {
+                const int p = p0 + u * xs;
+                if (p < P.p1 && !init) {
+                    const size_t o0 = base + (size_t)(2 * p) * nx + xc;
+                    pp[u][0] = pv[o0];
+                    pp[u][1] = pv[o0 + nx];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kFdLoads; u++) {
+                const int p = p0 + u * xs;
+                if (p < P.p1) {
+                    const cplx q = R[(p - P.p0) * nx + xc];
+                    const size_t o0 = base + (size_t)(2 * p) * nx + xc;
+                    pv[o0] = init ? q.x : q.x + be * pp[u][0];
+                    pv[o0 + nx] = init ? q.y : q.y + be * pp[u][1];
+                }
+            }
+        }
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");  // no rank leaves while read
+}
+
 // float <-> double staging helpers for the host-facing API
 __global__ void k_scale_copy(const float *__restrict__ a, float *__restrict__ o, float s, long n) {
     pdl_enter();

@@ -95,6 +95,7 @@ SIGNATURES = {
     "mb_tomo": (C.c_int, [C.c_void_p, _D, _D, _F]),
     "mb_tomo_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mb_fit": (C.c_int, [C.c_void_p, _D, _F]),
+    "mb_fdpcg_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "mb_tomo_wfs": (C.c_int, [C.c_void_p, C.POINTER(_D), C.POINTER(_D), _F]),
     "mb_fit_opdr": (C.c_int, [C.c_void_p, C.POINTER(_D), _D, _F]),
     "mb_recon_step_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

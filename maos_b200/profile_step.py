@@ -96,7 +96,19 @@ def main():
         torch.cuda.synchronize()
         nk = lib.mb_kernel_launches(1)
         print(f"{a.system} batch {a.batch} fit {a.fit}: step {e0.elapsed_time(e1) / 50:.4f} ms, {nk} kernels, "
-              f"pupil rows {rows}")
+              f"pupil rows {rows}, fdpcg form {lib.mb_fdpcg_mode(R.h, 0) if s.fdpcg is not None else 0}")
+        if s.fdpcg is not None:
+            for mode in (1, 2):
+                got = R.fdpcg_mode(mode)
+                for _ in range(3):
+                    R.step_device(g.data_ptr(), st.cuda_stream)
+                with torch.cuda.stream(st):
+                    e0.record(st)
+                    for _ in range(50):
+                        R.step_device(g.data_ptr(), st.cuda_stream)
+                    e1.record(st)
+                torch.cuda.synchronize()
+                print(f"  fdpcg form {got}: step {e0.elapsed_time(e1) / 50:.4f} ms")
         ns = lib.mb_num_stages()
         ms, by, lp = (C.c_float * ns)(), (C.c_double * ns)(), (C.c_int * ns)()
         native.check(lib.mb_time_stages(R.h, 50, ms, by, lp), "mb_time_stages")

@@ -207,6 +207,15 @@ class Reconstructor:
         check(self.lib.mb_autotune(self.h, int(reps), C.byref(rows), ms), "mb_autotune")
         return rows.value, {r: ms[i] for i, r in enumerate((4, 8, 16)) if ms[i] >= 0}
 
+    def fdpcg_mode(self, mode: int) -> int:
+        """Form of the FDPCG preconditioner in the CG step (mb_fdpcg_mode):
+        1 three kernels, 2 one fused cluster kernel, 0 the fused one when it
+        fits; returns the form in use."""
+        rc = self.lib.mb_fdpcg_mode(self.h, int(mode))
+        if rc < 0:
+            check(rc, "mb_fdpcg_mode")
+        return rc
+
     def reset(self):
         check(self.lib.mb_recon_reset(self.h), "mb_recon_reset")
 

@@ -217,3 +217,44 @@ def test_autotune_keeps_results():
         assert np.array_equal(x0, x1)
     finally:
         R.close()
+
+
+def test_fused_preconditioner_matches_the_oracle(setup):
+    """The fused FDPCG step (mb_fdpcg_mode 2: one cluster kernel per CG step,
+    the layers split over its CTAs) solves to the oracle's tolerance, agrees
+    with the three-kernel form to FP32 rounding, and gives an instance the
+    same result (bit for bit) alone and beside another."""
+    s, R, o = setup
+    if s.fdpcg is None:
+        pytest.skip("plain CG configuration")
+    from maos_b200.recon import Reconstructor
+    rng = np.random.default_rng(15)
+    g1 = rng.standard_normal((2, s.ngrad)) * 1e-6
+    g2 = g1 + rng.standard_normal((2, s.ngrad)) * 1e-7
+    xs = {}
+    try:
+        for mode in (1, 2):
+            if R.fdpcg_mode(mode) != mode:
+                pytest.skip("the fused cluster does not fit on this device")
+            R.reset()
+            x1, _ = R.tomo(g1)
+            x2, r2 = R.tomo(g2)
+            xs[mode] = (x1, x2)
+        for b in range(2):
+            w1, _ = tomo_solve(o, g1[b])
+            w2, res2 = tomo_solve(o, g2[b], x0=w1)
+            assert rel(xs[2][0][b], w1) < SOLVE_TOL
+            assert rel(xs[2][1][b], w2) < SOLVE_TOL
+            assert rel(xs[2][1][b], xs[1][1][b]) < SOLVE_TOL
+        # alone and in a batch of two: identical bits
+        R1 = Reconstructor(s, nbatch=1)
+        try:
+            assert R1.fdpcg_mode(2) == 2
+            R1.reset()
+            a1, _ = R1.tomo(g1[1:2])
+            a2, _ = R1.tomo(g2[1:2])
+        finally:
+            R1.close()
+        assert np.array_equal(a2[0], xs[2][1][1])
+    finally:
+        R.fdpcg_mode(1)
