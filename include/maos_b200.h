@@ -267,9 +267,9 @@ int mb_autotune(mb_recon *r, int reps, int *rows, float *ms);
  * blocks over instances, inverse FFTs), 2 = one kernel per step in which the
  * layers of an instance are split over one thread-block cluster of up to 16
  * CTAs that exchange rows, columns and block members through distributed
- * shared memory, 0 = 2 when that cluster fits on the device.  Results agree
- * to FP32 rounding.  The step graphs are captured again.  Returns the form
- * in use (1 or 2) or a negative MB_E* code. */
+ * shared memory, 0 = 2 when that cluster fits on the device, -1 = no change
+ * (query).  Results agree to FP32 rounding.  The step graphs are captured
+ * again.  Returns the form in use (1 or 2) or a negative MB_E* code. */
 int mb_fdpcg_mode(mb_recon *r, int mode);
 
 /* Servo filter on the device (no GPU counterpart in the reference; the CPU

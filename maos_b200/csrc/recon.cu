@@ -2003,9 +2003,10 @@ int mb_time_stages(mb_recon *h, int reps, float *ms, double *bytes, int *launche
 
 int mb_fdpcg_mode(mb_recon *h, int mode) {
     MB_API_BEGIN
-    MB_REQUIRE(h && mode >= 0 && mode <= 2, "invalid arguments");
+    MB_REQUIRE(h && mode >= -1 && mode <= 2, "invalid arguments");
     mb::Recon &R = h->R;
     MB_REQUIRE(R.precond, "reconstructor has no FDPCG preconditioner");
+    if (mode < 0) return R.fd_mode;
     MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
     R.set_fdpcg_mode(mode);
     return R.fd_mode;

@@ -40,6 +40,8 @@ def main():
     ap.add_argument("--wfs", action="store_true")
     ap.add_argument("--fit", choices=["assembled", "grid"], default="assembled")
     ap.add_argument("--stages", action="store_true")
+    ap.add_argument("--fdpcg-mode", type=int, default=1, choices=[0, 1, 2],
+                    help="form of the FDPCG preconditioner (mb_fdpcg_mode) for the plain steps")
     a = ap.parse_args()
     s = geometry.build_tomo(config.PRESETS[a.system]())
     fs = fit_setup.build_fit(s) if (a.fit == "grid" or a.wfs) else fit_assemble.build_fit_assembled(s)
@@ -96,7 +98,7 @@ def main():
         torch.cuda.synchronize()
         nk = lib.mb_kernel_launches(1)
         print(f"{a.system} batch {a.batch} fit {a.fit}: step {e0.elapsed_time(e1) / 50:.4f} ms, {nk} kernels, "
-              f"pupil rows {rows}, fdpcg form {lib.mb_fdpcg_mode(R.h, 0) if s.fdpcg is not None else 0}")
+              f"pupil rows {rows}, fdpcg form {lib.mb_fdpcg_mode(R.h, -1) if s.fdpcg is not None else 0}")
         if s.fdpcg is not None:
             for mode in (1, 2):
                 got = R.fdpcg_mode(mode)
@@ -117,6 +119,8 @@ def main():
                   f"{ms[i] * lp[i]:.4f} ms")
         R.close()
         return
+    if s.fdpcg is not None:
+        R.fdpcg_mode(a.fdpcg_mode)
     for _ in range(a.steps):
         R.step_device(g.data_ptr(), st.cuda_stream)
     torch.cuda.synchronize()
