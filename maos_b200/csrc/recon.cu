@@ -41,6 +41,7 @@ static std::atomic<long> g_launches{0};
 void count_launches(long n) { g_launches += n; }
 
 static inline unsigned nblocks(long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
+constexpr int kCgRestart = 100;  // lib/pcg.c:61
 
 // Every kernel of the reconstructor is launched through here.  With
 // MAOS_B200_PDL=1 the launches carry programmatic stream serialisation (the
@@ -1147,9 +1148,11 @@ bool Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k
     return false;
 }
 
-// (Preconditioned) CG with FP64 scalars, the schedule of lib/pcg.c:28 and
-// cuda/pcg.cu:87 (the restart every 100/500 iterations is never reached for
-// the iteration counts used per step).  x holds the warm start.
+// (Preconditioned) CG with FP64 scalars, the schedule of lib/pcg.c:28: the
+// residual is recomputed from x every kCgRestart = 100 iterations as the
+// reference's CPU solver does (its GPU solver, cuda/pcg.cu:87, every 500),
+// which matters to the long solves of the control-matrix build.  x holds the
+// warm start.
 // XrMmul, when given, performs the x/r update of a non-final iteration
 // together with the preconditioner.
 void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulFn &Amul,
@@ -1163,12 +1166,27 @@ void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulF
         pdone = Mmul(B.r, B.z, B.rz, 0, 1);
         zp = B.z;
     } else {
-        launch(k_dot_self, dim3(nblk, nb), dim3(kThreads), 0, s, B.r, B.rz, n, B.S, act());  // z aliases r
+        launch(k_dot_self, dim3(nblk, nb), dim3(kThreads), 0, s, B.r, B.rz, n, B.S, 0, act());  // z aliases r
     }
     if (!pdone)
         launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n, B.S, 1,
                act());
     for (int k = 0; k < iters; k++) {
+        if (k > 0 && k % kCgRestart == 0) {
+            // restart as lib/pcg.c:61 does every 100 iterations: r = b - A x,
+            // z = M r, p = z, (r.z)_k afresh (the p of the previous step is dropped)
+            Amul(B.x, B.Ap, nullptr, 0);
+            launch(k_cg_init_r, dim3(nblk, nb), dim3(kThreads), 0, s, B.rhs, B.Ap, B.r, B.bb, n, B.S, iters, act());
+            if (Mmul) {
+                pdone = Mmul(B.r, B.z, B.rz, k, 1);
+            } else {
+                launch(k_dot_self, dim3(nblk, nb), dim3(kThreads), 0, s, B.r, B.rz, n, B.S, k, act());
+                pdone = false;
+            }
+            if (!pdone)
+                launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n,
+                       B.S, 1, act());
+        }
         Amul(B.p, B.Ap, B.pap, k);  // its last block leaves alpha_k
         if (XrMmul && k + 1 < iters) {
             pdone = XrMmul(k);  // x, r update and preconditioner; beta_k (and p, when it says so)

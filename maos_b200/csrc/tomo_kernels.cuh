@@ -782,8 +782,8 @@ __device__ __forceinline__ void cg_rz_last(const double *part_b, const CgScal &S
     if (last_block(S.cnt + b, gridDim.x) && threadIdx.x < 32) {
         const double rz = warp_sum_fresh(part_b, gridDim.x);
         if (threadIdx.x == 0) {
-            if (init) {
-                S.sc[(size_t)b * S.nsc] = rz;
+            if (init) {  // start (or restart, lib/pcg.c:61) at iteration k
+                S.sc[(size_t)b * S.nsc + k] = rz;
             } else {
                 double be = rz / S.sc[(size_t)b * S.nsc + k];
                 if (!isfinite(be)) be = 0;
@@ -795,8 +795,9 @@ __device__ __forceinline__ void cg_rz_last(const double *part_b, const CgScal &S
     }
 }
 
-// v.v partials and (when z aliases r) the start-of-CG r.z.  grid: (nblk, nb)
-__global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ part, long n, CgScal S,
+// v.v partials and (when z aliases r) the r.z of a CG start or restart at
+// iteration k.  grid: (nblk, nb)
+__global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ part, long n, CgScal S, int k,
                            const int *__restrict__ act) {
     pdl_enter();
     if (inactive(act, blockIdx.y)) return;
@@ -810,7 +811,7 @@ __global__ void k_dot_self(const float *__restrict__ v, double *__restrict__ par
     }
     t = block_sum(t, sh);
     if (threadIdx.x == 0) part[(size_t)b * gridDim.x + blockIdx.x] = t;
-    cg_rz_last(part + (size_t)b * gridDim.x, S, b, 0, 1);
+    cg_rz_last(part + (size_t)b * gridDim.x, S, b, k, 1);
 }
 
 // x += alpha p; r -= alpha Ap; r.r partials.  The last block either finishes
@@ -1597,8 +1598,8 @@ k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restr
                 }
                 s_be = be;
                 if (blockIdx.x == 0) {  // rank 0 keeps the CG scalars
-                    if (init) {
-                        SC.sc[(size_t)b * SC.nsc] = rz;
+                    if (init) {  // start (or restart) at iteration kit
+                        SC.sc[(size_t)b * SC.nsc + kit] = rz;
                     } else {
                         SC.ab[2 * b + 1] = (float)be;
                         SC.sc[(size_t)b * SC.nsc + kit + 1] = rz;
@@ -1902,8 +1903,8 @@ k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid
             }
             s_be = be;
             if (blockIdx.x == 0) {  // rank 0 keeps the CG scalars
-                if (init) {
-                    SC.sc[(size_t)b * SC.nsc] = t;
+                if (init) {  // start (or restart) at iteration kit
+                    SC.sc[(size_t)b * SC.nsc + kit] = t;
                 } else {
                     SC.ab[2 * b + 1] = (float)be;
                     SC.sc[(size_t)b * SC.nsc + kit + 1] = t;

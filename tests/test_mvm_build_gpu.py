@@ -3,8 +3,11 @@
 The build applies the batched tomography + fit to unit gradients (256
 right-hand sides per batched solve, FP32 with FP64 CG scalars); 64 seeded
 columns are compared with the FP64 oracle solving the same cold-started
-problems with the same iteration counts.  Tolerance: 5e-3 relative L2 per
-column (FP32 CG over 100+ iterations against FP64).
+problems with the same iteration counts (100 tomography, 40 fit).
+Tolerance: 1e-4 relative L2 per column, the DM-command gate; measured on a
+B200 the columns agree to 1.4e-6 (median) and 8e-6 (worst).  Beyond 100
+iterations the device CG restarts from the residual as the reference's CPU
+solver does (lib/pcg.c:61); a 300-iteration column case is checked too.
 
 The precision study then applies the built matrix to frozen-flow gradients in
 FP32, BF16 and FP8-E4M3 storage and measures the DM-command error as
@@ -18,7 +21,7 @@ from oracle.recon_oracle import FitOracle, TomoOracle, fit_solve, tomo_solve
 
 pytestmark = pytest.mark.gpu
 
-COL_TOL = 5e-3
+COL_TOL = 1e-4
 TOMO_IT, FIT_IT = 100, 40
 
 
@@ -64,3 +67,23 @@ def test_mvm_storage_precision_gate(ltao_matrix):
     assert d["bf16"]["within_gate"], d["bf16"]
     assert d["bf16"]["fraction_of_residual"] < d["fp8_e4m3"]["fraction_of_residual"]
     assert np.isfinite(d["fp8_e4m3"]["command_error_wfe_nm"])
+
+
+def test_columns_past_the_cg_restart():
+    """300 tomography iterations: the device CG restarts at 100 and 200 as
+    lib/pcg.c does, so the columns still follow the FP64 oracle's restarted
+    solve.  FP32 rounding grows over the longer solve of this ill-conditioned
+    unit-gradient problem: 1e-3."""
+    from conftest import get_fit, get_system
+    from maos_b200.mvm_build import build_control_matrix
+    s, fs = get_system("ltao_8m"), get_fit("ltao_8m")
+    cols = np.sort(np.random.default_rng(65).choice(s.ngrad, 8, replace=False))
+    M, _ = build_control_matrix(s, fs, rhs_batch=8, tomo_maxit=300, fit_maxit=FIT_IT, columns=cols)
+    to, fo = TomoOracle(s), FitOracle(s, fs)
+    for k, c in enumerate(cols):
+        g = np.zeros(s.ngrad)
+        g[c] = 1e-6
+        x, _ = tomo_solve(to, g, maxit=300)
+        a, _ = fit_solve(fo, x, maxit=FIT_IT)
+        want = a / 1e-6
+        assert np.linalg.norm(M[:, k] - want) <= 1e-3 * np.linalg.norm(want), int(c)
