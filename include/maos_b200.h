@@ -68,6 +68,26 @@ typedef struct {
     const double *ptt;
 } mb_wfs_desc;
 
+/* What the device needs to form the FDPCG block matrices' data term itself
+ * (the WFS sum of maos/fdpcg.c:427-480: prop' (gx' sel' sel gx + gy' sel' sel
+ * gy) prop / neam^2 per WFS), so a change of the WFS noise is absorbed on the
+ * GPU (mb_update_recon_neam).  All of it is geometry fixed at setup except
+ * neam. */
+typedef struct {
+    int nxp, nyp;          /* pupil frequency grid of the data term (nx0/os0 * tomo.pos) */
+    double dxp;            /* its sampling (recon->ploc->dx) */
+    int pos;               /* pupil frequencies aliasing to one block, per axis (tomo.pos) */
+    int adimx, adimy;      /* blocks per axis (nx0/os0, ny0/os0) */
+    const double *gx, *gy; /* [nyp][nxp] complex (re, im), fftshifted: average-gradient
+                              transfer functions (fdpcg.c:199 fdpcg_g) */
+    int nsel;              /* entries of the selection autocorrelation */
+    const int *sel_dx, *sel_dy; /* their shifts on the pupil frequency grid (mod nxp, nyp) */
+    const double *sel_r;   /* [nsel] complex (re, im): R(d) = sum_s conj(v_{s+d}) v_s over the
+                              kept coefficients v of fdpcg_saselect (fdpcg.c:71) */
+    int needscale;         /* fdpcg->scale: 0 multiplies the term by nx0*ny0 (fdpcg.c:498) */
+    const double *neam;    /* [nwfs] mean NEA per WFS at setup (recon->neam, TOMOSCALE units) */
+} mb_fdpcg_geom;
+
 /* Fourier-domain preconditioner tables (recon->fdpcg, maos/fdpcg.c:331). */
 typedef struct {
     int nb, bs;          /* blocks and block size */
@@ -82,6 +102,10 @@ typedef struct {
        invpsd term scales with each layer's l2c). */
     const double *mdata;
     const double *mdiag;
+    /* Optional (needs mdiag; no reference counterpart): the data term's
+       geometry; the device then forms the data term itself (mdata may be
+       NULL) and mb_update_recon_neam rebuilds the blocks for new noise. */
+    const mb_fdpcg_geom *geom;
 } mb_fdpcg_desc;
 
 /* A sparse matrix in compressed sparse column form (the reference's dsp). */
@@ -180,6 +204,16 @@ int mb_update_recon_nea(mb_recon *r, int iwfs, const double *neai, const double 
  * kept at setup (mb_fdpcg_desc.mdata/mdiag), with invpsd scaled by the new
  * l2c; MB_EINVAL when no data term was given. */
 int mb_update_recon_cn2(mb_recon *r, const double *l2c, const mb_fdpcg_desc *fdpcg);
+
+/* The FDPCG part of gpu_update_recon (cuda/gpu.h:49; maos recomputes
+ * recon->fdpcg with fdpcg_prepare after the noise changes): new mean NEA per
+ * WFS (recon->neam), the data term formed on the device from the geometry of
+ * mb_fdpcg_desc.geom, the blocks inverted and folded on the device, in place
+ * (the step graphs keep working).  MB_EINVAL when no geometry was given. */
+int mb_update_recon_neam(mb_recon *r, const double *neam);
+/* The device's FDPCG data term [nb][bs][bs] complex (re, im), column-major
+ * blocks, as mb_fdpcg_desc.mdata (for checks). */
+int mb_fdpcg_data(mb_recon *r, double *out);
 
 /* gpu_tomo (cuda/gpu.h:55, curecon_t::tomo cuda/recon.cu:259).
  * grad: [nbatch][ngrad] host FP64 gradients.  opdr: optional host output

@@ -277,6 +277,17 @@ struct Recon {
     DevBuf<FdMem> fd_mem;
     size_t fd_fsmem = 0;
     void build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector<long> &hoff);
+    // the FDPCG data term's geometry (mb_fdpcg_geom), for k_fd_data
+    bool fd_geom = false;
+    FdGeomDev fdg{};
+    DevBuf<int4> fdg_mem;
+    DevBuf<int2> fdg_blk, fdg_seld;
+    DevBuf<double2> fdg_gx, fdg_gy, fdg_selr;
+    DevBuf<double> fdg_neam, fdg_thx, fdg_thy, fdg_lht;
+    DevBuf<int> fdg_lnx, fdg_lny;
+    std::vector<double> wfs_thx, wfs_thy;
+    void build_fdpcg_geom(const mb_fdpcg_desc *fd);
+    void form_fdpcg_data(const double *neam);
     void set_fdpcg_mode(int mode);
     void enqueue_solve(cudaStream_t s);
     struct CgBufs {
@@ -760,12 +771,17 @@ void Recon::build_fdpcg(const mb_fdpcg_desc *fd) {
     fd_M.upload(M);
     fd_idx.upload(idx);
     // the data term for device rebuilds (k_fd_prepare, k_fd_fold)
-    fd_dev = fd->mdata && fd->mdiag;
+    fd_dev = fd->mdiag && (fd->mdata || fd->geom);
+    fd_geom = false;
     if (fd_dev) {
         const size_t nel = (size_t)fd_nb * fd_bs * fd_bs;
-        std::vector<double2> md(nel);
-        for (size_t k = 0; k < nel; k++) md[k] = make_double2(fd->mdata[2 * k], fd->mdata[2 * k + 1]);
-        fd_mdata.upload(md);
+        if (fd->geom) {  // the data term formed on the device from its geometry
+            build_fdpcg_geom(fd);
+        } else {
+            std::vector<double2> md(nel);
+            for (size_t k = 0; k < nel; k++) md[k] = make_double2(fd->mdata[2 * k], fd->mdata[2 * k + 1]);
+            fd_mdata.upload(md);
+        }
         fd_mdiag.upload(std::vector<double>(fd->mdiag, fd->mdiag + (size_t)fd_nb * fd_bs));
         std::vector<int> ml((size_t)fd_nb * fd_bs);
         for (long i = 0; i < (long)fd_nb * fd_bs; i++) ml[i] = member(fd->perm[i]).l;
@@ -977,6 +993,96 @@ void Recon::build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector
     fd_fused_ok = true;
 }
 
+// The data term's geometry on the device: per block its base pupil
+// frequency, per member its layer and shifted frequency (from fd->perm, the
+// natural-order FFT index), the transfer functions, the selection
+// autocorrelation, the layer heights and WFS directions; then the data term
+// at the setup's mean NEA.
+void Recon::build_fdpcg_geom(const mb_fdpcg_desc *fd) {
+    const mb_fdpcg_geom *g = fd->geom;
+    MB_REQUIRE(g->nxp > 0 && g->nyp > 0 && g->dxp > 0 && g->pos >= 1 && g->pos <= 4 && g->adimx > 0 &&
+                   g->adimy > 0 && g->gx && g->gy && g->neam && g->nsel >= 0 && g->nsel <= 64 &&
+                   (g->nsel == 0 || (g->sel_dx && g->sel_dy && g->sel_r)),
+               "fdpcg geometry: invalid sizes or missing arrays");
+    MB_REQUIRE(nwfs <= kMaxWfs, "fdpcg geometry: at most %d WFS", kMaxWfs);
+    fdg.nxp = g->nxp;
+    fdg.nyp = g->nyp;
+    fdg.pos = g->pos;
+    fdg.adimx = g->adimx;
+    fdg.adimy = g->adimy;
+    fdg.nsel = g->nsel;
+    fdg.needscale = g->needscale;
+    fdg.nwfs = nwfs;
+    fdg.bs = fd_bs;
+    fdg.dxp = g->dxp;
+    fdg.scale0 = (double)lay_h[0].nx * lay_h[0].ny;
+    std::vector<int> lnx(nps), lny(nps);
+    std::vector<double> lht(nps);
+    for (int l = 0; l < nps; l++) {
+        lnx[l] = lay_h[l].nx;
+        lny[l] = lay_h[l].ny;
+        lht[l] = xgrid[l].ht;
+        const int ratio = g->nxp / lnx[l];
+        MB_REQUIRE(ratio <= 2 && g->nyp / lny[l] == ratio, "fdpcg geometry: layer %d sampled at 1/%d of the pupil",
+                   l, ratio);
+    }
+    std::vector<int4> mem((size_t)fd_nb * fd_bs);
+    std::vector<int2> blk(fd_nb);
+    for (long i = 0; i < (long)fd_nb * fd_bs; i++) {
+        const long q = fd->perm[i];
+        int l = 0;
+        while (l + 1 < nps && q >= xoff[l + 1]) l++;
+        const long local = q - xoff[l];
+        const int nx = lay_h[l].nx, ny = lay_h[l].ny;
+        const int jx = (int)(local % nx), jy = (int)(local / nx);
+        mem[i] = make_int4(l, (jx + nx / 2) % nx, (jy + ny / 2) % ny, 0);
+        if (i % fd_bs == 0) {  // member 0 of a block: layer 0, the block's own frequency
+            MB_REQUIRE(l == 0, "fdpcg geometry: block %ld does not start on layer 0", i / fd_bs);
+            blk[i / fd_bs] = make_int2(jx >= nx / 2 ? jx - nx : jx, jy >= ny / 2 ? jy - ny : jy);
+        }
+    }
+    std::vector<double2> gx((size_t)g->nxp * g->nyp), gy(gx.size()), sr(std::max(g->nsel, 1));
+    for (size_t k = 0; k < gx.size(); k++) {
+        gx[k] = make_double2(g->gx[2 * k], g->gx[2 * k + 1]);
+        gy[k] = make_double2(g->gy[2 * k], g->gy[2 * k + 1]);
+    }
+    std::vector<int2> sd(std::max(g->nsel, 1), make_int2(-1, -1));
+    for (int k = 0; k < g->nsel; k++) {
+        sd[k] = make_int2(((g->sel_dx[k] % g->nxp) + g->nxp) % g->nxp, ((g->sel_dy[k] % g->nyp) + g->nyp) % g->nyp);
+        sr[k] = make_double2(g->sel_r[2 * k], g->sel_r[2 * k + 1]);
+    }
+    fdg_mem.upload(mem);
+    fdg_blk.upload(blk);
+    fdg_gx.upload(gx);
+    fdg_gy.upload(gy);
+    fdg_seld.upload(sd);
+    fdg_selr.upload(sr);
+    fdg_thx.upload(wfs_thx);
+    fdg_thy.upload(wfs_thy);
+    fdg_lht.upload(lht);
+    fdg_lnx.upload(lnx);
+    fdg_lny.upload(lny);
+    fdg_neam.alloc(nwfs);
+    fd_mdata.alloc((size_t)fd_nb * fd_bs * fd_bs);
+    fd_geom = true;
+    form_fdpcg_data(g->neam);
+}
+
+// The data term at mean NEA neam [nwfs] (host), into fd_mdata.  Synchronous.
+void Recon::form_fdpcg_data(const double *neam) {
+    for (int w = 0; w < nwfs; w++)
+        MB_REQUIRE(neam[w] > 0 && std::isfinite(neam[w]), "fdpcg: neam of WFS %d is %g", w, neam[w]);
+    MB_CUDA_TRY(cudaMemcpyAsync(fdg_neam.p, neam, nwfs * sizeof(double), cudaMemcpyHostToDevice, stream));
+    const int npf = fdg.pos * fdg.pos;
+    const size_t smem = ((size_t)npf * nwfs * fd_bs + (size_t)npf * npf) * sizeof(double2);
+    MB_REQUIRE(smem <= 48 * 1024, "fdpcg geometry: %zu bytes of shared memory per block", smem);
+    k_fd_data<<<fd_nb, kFdDataThreads, smem, stream>>>(fdg, fdg_mem.p, fdg_blk.p, fdg_gx.p, fdg_gy.p, fdg_seld.p,
+                                                       fdg_selr.p, fdg_neam.p, fdg_thx.p, fdg_thy.p, fdg_lht.p,
+                                                       fdg_lnx.p, fdg_lny.p, fd_mdata.p);
+    MB_CHECK_LAUNCH();
+    MB_CUDA_TRY(cudaStreamSynchronize(stream));
+}
+
 // 1: three kernels per preconditioner (k_fd_fwd, k_fd_mul, k_fd_inv);
 // 2: the fused cluster kernel (when it fits); 0: the fused one when it fits.
 // The step graphs are captured again.
@@ -1041,10 +1147,14 @@ void Recon::build(const mb_recon_desc *d) {
     goff.assign(nwfs + 1, 0);
     nsa.resize(nwfs);
     int nsamax = 0;
+    wfs_thx.resize(nwfs);
+    wfs_thy.resize(nwfs);
     for (int w = 0; w < nwfs; w++) {
         nsa[w] = d->wfs[w].nsa;
         nsamax = std::max(nsamax, nsa[w]);
         goff[w + 1] = goff[w] + 2L * nsa[w];
+        wfs_thx[w] = d->wfs[w].thetax;
+        wfs_thy[w] = d->wfs[w].thetay;
     }
     ngrad = goff[nwfs];
     set_l2c(d->l2c);
@@ -1828,6 +1938,33 @@ int mb_update_recon_nea(mb_recon *h, int iwfs, const double *neai, const double 
     h->R.wfs.upload(h->R.wfs_h);
     for (int w = 0; w < h->R.nwfs; w++) h->R.wfstab.w[w] = h->R.wfs_h[w];
     h->R.capture_graph();
+    MB_API_END
+}
+
+int mb_update_recon_neam(mb_recon *h, const double *neam) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && neam, "invalid arguments");
+    mb::Recon &R = h->R;
+    if (!R.precond || !R.fd_geom || !R.fd_dev) {
+        mb::set_error("mb_update_recon_neam: no FDPCG data-term geometry (mb_fdpcg_desc.geom, .mdiag) at setup");
+        return MB_EINVAL;
+    }
+    MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
+    R.form_fdpcg_data(neam);
+    R.rebuild_fdpcg_device();
+    MB_API_END
+}
+
+int mb_fdpcg_data(mb_recon *h, double *out) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && out, "invalid arguments");
+    mb::Recon &R = h->R;
+    if (!R.precond || !R.fd_dev) {
+        mb::set_error("mb_fdpcg_data: no FDPCG data term on the device");
+        return MB_EINVAL;
+    }
+    MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
+    MB_CUDA_TRY(cudaMemcpy(out, R.fd_mdata.p, R.fd_mdata.n * sizeof(double2), cudaMemcpyDeviceToHost));
     MB_API_END
 }
 

@@ -1480,6 +1480,101 @@ __global__ void k_fd_fold(const double2 *__restrict__ minv, const int *__restric
     M[k] = make_float2((float)(0.5 * (a.x + p.x) * s), (float)(0.5 * (a.y - p.y) * s));
 }
 
+// ---------------------------------------------------------------------------
+// The FDPCG blocks' data term formed on the device (maos/fdpcg.c:427-480), in
+// FP64, one CTA per frequency block b:
+//   D_b = sum_w sum_{f1,f2} P_w(f1)^H Mmid(f1, f2) P_w(f2) / neam_w^2,
+//   Mmid(f1, f2) = (conj(gx_f1) gx_f2 + conj(gy_f1) gy_f2) R(f2 - f1),
+// f over the pupil frequencies aliasing to the block (pos x pos of them),
+// P_w(f)[a] the propagation of pupil frequency f to member a (layer l at
+// shifted frequency (jx, jy)) along WFS w: exp(2 pi i (fx dx_w + fy dy_w))
+// with dx_w = ht_l theta_w, times the bilinear alias factor when the layer
+// is sampled at half the pupil rate (fdpcg.c:253 fdpcg_prop); zero when f
+// does not map to the member.  The v table and the Mmid table are formed once
+// per block in shared memory.  out: [nb][bs][bs] column-major, as
+// mb_fdpcg_desc.mdata.
+// ---------------------------------------------------------------------------
+struct FdGeomDev {
+    int nxp, nyp, pos, adimx, adimy, nsel, needscale, nwfs, bs;
+    double dxp, scale0;  // pupil sampling; nx0*ny0
+};
+constexpr int kFdDataThreads = 256;
+
+__global__ void __launch_bounds__(kFdDataThreads)
+k_fd_data(FdGeomDev G, const int4 *__restrict__ mem, const int2 *__restrict__ blk,
+          const double2 *__restrict__ gx, const double2 *__restrict__ gy, const int2 *__restrict__ seld,
+          const double2 *__restrict__ selr, const double *__restrict__ neam, const double *__restrict__ thx,
+          const double *__restrict__ thy, const double *__restrict__ lht, const int *__restrict__ lnx,
+          const int *__restrict__ lny, double2 *__restrict__ out) {
+    extern __shared__ double2 fdsm[];
+    __shared__ int s_kx[16], s_ky[16];
+    const int b = blockIdx.x, bs = G.bs, nw = G.nwfs;
+    const int npf = G.pos * G.pos;
+    double2 *v = fdsm, *mm = fdsm + (size_t)npf * nw * bs;
+    const double dkx = 1.0 / (G.nxp * G.dxp), dky = 1.0 / (G.nyp * G.dxp);
+    if (threadIdx.x < npf) {  // pupil frequencies of this block, centred
+        const int mxp = threadIdx.x / G.pos, myp = threadIdx.x - mxp * G.pos;
+        const int2 bk = blk[b];
+        const int kx = bk.x + G.adimx * mxp, ky = bk.y + G.adimy * myp;
+        s_kx[threadIdx.x] = ((kx + G.nxp / 2) % G.nxp + G.nxp) % G.nxp - G.nxp / 2;
+        s_ky[threadIdx.x] = ((ky + G.nyp / 2) % G.nyp + G.nyp) % G.nyp - G.nyp / 2;
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < npf * nw * bs; it += blockDim.x) {
+        const int f = it / (nw * bs), w = (it / bs) % nw, a = it % bs;
+        const int4 m = mem[(size_t)b * bs + a];  // layer, shifted jx, shifted jy
+        const int nx = lnx[m.x], ny = lny[m.x];
+        const int kx = s_kx[f], ky = s_ky[f];
+        double2 val = make_double2(0.0, 0.0);
+        if ((kx + nx / 2 + nx) % nx == m.y && (ky + ny / 2 + ny) % ny == m.z) {
+            const double fx = (m.y - nx / 2) * dkx, fy = (m.z - ny / 2) * dky;
+            const double ph = 2.0 * M_PI * (fx * (lht[m.x] * thx[w]) + fy * (lht[m.x] * thy[w]));
+            double sn, cs;
+            sincos(ph, &sn, &cs);
+            double amp = 1.0;
+            if (G.nxp / nx == 2)
+                amp = (1.0 + cos(2.0 * M_PI * (kx * dkx) * G.dxp)) * (1.0 + cos(2.0 * M_PI * (ky * dky) * G.dxp)) * 0.5;
+            val = make_double2(cs * amp / neam[w], sn * amp / neam[w]);
+        }
+        v[((size_t)f * nw + w) * bs + a] = val;
+    }
+    for (int it = threadIdx.x; it < npf * npf; it += blockDim.x) {
+        const int f1 = it / npf, f2 = it - f1 * npf;
+        const int p1x = s_kx[f1] + G.nxp / 2, p1y = s_ky[f1] + G.nyp / 2;
+        const int p2x = s_kx[f2] + G.nxp / 2, p2y = s_ky[f2] + G.nyp / 2;
+        const int dx = ((p2x - p1x) % G.nxp + G.nxp) % G.nxp, dy = ((p2y - p1y) % G.nyp + G.nyp) % G.nyp;
+        double2 r = make_double2(0.0, 0.0);
+        for (int k = 0; k < G.nsel; k++)
+            if (seld[k].x == dx && seld[k].y == dy) r = selr[k];
+        const double2 a1 = gx[(size_t)p1y * G.nxp + p1x], a2 = gx[(size_t)p2y * G.nxp + p2x];
+        const double2 c1 = gy[(size_t)p1y * G.nxp + p1x], c2 = gy[(size_t)p2y * G.nxp + p2x];
+        const double2 g = make_double2(a1.x * a2.x + a1.y * a2.y + c1.x * c2.x + c1.y * c2.y,
+                                       a1.x * a2.y - a1.y * a2.x + c1.x * c2.y - c1.y * c2.x);  // conj(g1) g2
+        mm[it] = make_double2(g.x * r.x - g.y * r.y, g.x * r.y + g.y * r.x);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < bs * bs; e += blockDim.x) {
+        const int i = e % bs, j = e / bs;  // row (member i), column (member j)
+        double re = 0.0, im = 0.0;
+        for (int f1 = 0; f1 < npf; f1++)
+            for (int f2 = 0; f2 < npf; f2++) {
+                const double2 q = mm[f1 * npf + f2];
+                if (q.x == 0.0 && q.y == 0.0) continue;
+                for (int w = 0; w < nw; w++) {
+                    const double2 a = v[((size_t)f1 * nw + w) * bs + i], c = v[((size_t)f2 * nw + w) * bs + j];
+                    const double ur = a.x * c.x + a.y * c.y, ui = a.x * c.y - a.y * c.x;  // conj(a) c
+                    re += ur * q.x - ui * q.y;
+                    im += ur * q.y + ui * q.x;
+                }
+            }
+        if (!G.needscale) {
+            re *= G.scale0;
+            im *= G.scale0;
+        }
+        out[((size_t)b * bs + j) * bs + i] = make_double2(re, im);
+    }
+}
+
 __device__ __forceinline__ void cluster_sync_all() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }

@@ -42,6 +42,10 @@ class FdpcgTables:
     # already multiplied by nx*ny when the oversampling is uniform.
     mhat_data: np.ndarray = None   # complex128 [nb, bs, bs]
     mhat_diag: np.ndarray = None   # float64 [nb, bs]
+    # The geometry a device needs to form mhat_data itself when the noise
+    # changes: the pupil frequency grid, the average-gradient transfer
+    # functions, the selection autocorrelation and each WFS's mean NEA.
+    geom: dict = None
 
 
 def _saselect(nxp, nyp, dxp, salocx, salocy, saa):
@@ -249,5 +253,8 @@ def fdpcg_prepare(sysm) -> FdpcgTables:
         first = np.argmax(s <= thr) if np.any(s <= thr) else len(s)
         si[first:] = 0.0
         Mb[b] = (Vh.conj().T * si) @ U.conj().T
+    geom = {"nxp": nxp, "nyp": nyp, "dxp": dxp, "pos": pos, "adimx": adimx, "adimy": adimy,
+            "gx": gx, "gy": gy, "sel": Rsel, "needscale": needscale,
+            "neam": np.array([w.neam for w in sysm.wfs], dtype=np.float64)}
     return FdpcgTables(bs=bs, nb=nb, adimx=adimx, adimy=adimy, scale=needscale,
-                       perm=perm1, Mbinv=Mb, nxtot=nxtot, mhat_data=Md, mhat_diag=Mg)
+                       perm=perm1, Mbinv=Mb, nxtot=nxtot, mhat_data=Md, mhat_diag=Mg, geom=geom)

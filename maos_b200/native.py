@@ -31,10 +31,18 @@ class MbWfsDesc(C.Structure):
                 ("ptt", C.POINTER(C.c_double))]
 
 
+class MbFdpcgGeom(C.Structure):
+    _fields_ = [("nxp", C.c_int), ("nyp", C.c_int), ("dxp", C.c_double), ("pos", C.c_int), ("adimx", C.c_int),
+                ("adimy", C.c_int), ("gx", C.POINTER(C.c_double)), ("gy", C.POINTER(C.c_double)),
+                ("nsel", C.c_int), ("sel_dx", C.POINTER(C.c_int)), ("sel_dy", C.POINTER(C.c_int)),
+                ("sel_r", C.POINTER(C.c_double)), ("needscale", C.c_int), ("neam", C.POINTER(C.c_double))]
+
+
 class MbFdpcgDesc(C.Structure):
     _fields_ = [("nb", C.c_int), ("bs", C.c_int), ("scale", C.c_int),
                 ("perm", C.POINTER(C.c_long)), ("mbinv", C.POINTER(C.c_double)),
-                ("mdata", C.POINTER(C.c_double)), ("mdiag", C.POINTER(C.c_double))]
+                ("mdata", C.POINTER(C.c_double)), ("mdiag", C.POINTER(C.c_double)),
+                ("geom", C.POINTER(MbFdpcgGeom))]
 
 
 class MbCsc(C.Structure):
@@ -96,6 +104,8 @@ SIGNATURES = {
     "mb_tomo_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mb_fit": (C.c_int, [C.c_void_p, _D, _F]),
     "mb_fdpcg_mode": (C.c_int, [C.c_void_p, C.c_int]),
+    "mb_update_recon_neam": (C.c_int, [C.c_void_p, _D]),
+    "mb_fdpcg_data": (C.c_int, [C.c_void_p, _D]),
     "mb_tomo_wfs": (C.c_int, [C.c_void_p, C.POINTER(_D), C.POINTER(_D), _F]),
     "mb_fit_opdr": (C.c_int, [C.c_void_p, C.POINTER(_D), _D, _F]),
     "mb_recon_step_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

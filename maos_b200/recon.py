@@ -26,7 +26,8 @@ from typing import Optional
 import numpy as np
 
 from . import native
-from .native import MbCsc, MbFdpcgDesc, MbFitDesc, MbFitSparseDesc, MbGrid, MbReconDesc, MbWfsDesc, check
+from .native import (MbCsc, MbFdpcgDesc, MbFdpcgGeom, MbFitDesc, MbFitSparseDesc, MbGrid, MbReconDesc,
+                     MbWfsDesc, check)
 
 
 def _dptr(a: np.ndarray):
@@ -55,8 +56,29 @@ def fdpcg_desc(fd, keep: list) -> MbFdpcgDesc:
         mgd = np.ascontiguousarray(fd.mhat_diag, dtype=np.float64).ravel()
         keep += [mdi, mgd]
         md, mg = _dptr(mdi), _dptr(mgd)
+    gp = C.POINTER(MbFdpcgGeom)()
+    g = getattr(fd, "geom", None)
+    if g is not None and mg:
+        def cplx(a):
+            a = np.ascontiguousarray(a, dtype=np.complex128).ravel()
+            o = np.empty(2 * a.size)
+            o[0::2] = a.real
+            o[1::2] = a.imag
+            keep.append(o)
+            return _dptr(o)
+        sel = sorted(g["sel"].items())
+        sdx = np.ascontiguousarray([k[0] for k, _ in sel], dtype=np.int32)
+        sdy = np.ascontiguousarray([k[1] for k, _ in sel], dtype=np.int32)
+        neam = np.ascontiguousarray(g["neam"], dtype=np.float64)
+        keep += [sdx, sdy, neam]
+        geo = MbFdpcgGeom(int(g["nxp"]), int(g["nyp"]), float(g["dxp"]), int(g["pos"]), int(g["adimx"]),
+                          int(g["adimy"]), cplx(g["gx"]), cplx(g["gy"]), len(sel),
+                          sdx.ctypes.data_as(C.POINTER(C.c_int)), sdy.ctypes.data_as(C.POINTER(C.c_int)),
+                          cplx([v for _, v in sel]), int(g["needscale"]), _dptr(neam))
+        keep.append(geo)
+        gp = C.pointer(geo)
     return MbFdpcgDesc(int(fd.nb), int(fd.bs), int(fd.scale),
-                       perm.ctypes.data_as(C.POINTER(C.c_long)), _dptr(mbi), md, mg)
+                       perm.ctypes.data_as(C.POINTER(C.c_long)), _dptr(mbi), md, mg, gp)
 
 
 def csc_desc(A, keep: list) -> MbCsc:
@@ -323,6 +345,20 @@ class Reconstructor:
         check(self.lib.mb_update_recon_nea(self.h, iwfs, _dptr(ne),
                                            _dptr(pt) if pt is not None else C.POINTER(C.c_double)()),
               "mb_update_recon_nea")
+
+    def update_neam(self, neam):
+        """The FDPCG part of gpu_update_recon: new mean NEA per WFS, the data
+        term and blocks rebuilt on the device (mb_update_recon_neam)."""
+        v = np.ascontiguousarray(neam, dtype=np.float64)
+        check(self.lib.mb_update_recon_neam(self.h, _dptr(v)), "mb_update_recon_neam")
+
+    def fdpcg_data(self):
+        """The device's FDPCG data term as complex [nb, bs, bs] (row, column)."""
+        fd = self.sys.fdpcg
+        out = np.empty(fd.nb * fd.bs * fd.bs * 2)
+        check(self.lib.mb_fdpcg_data(self.h, _dptr(out)), "mb_fdpcg_data")
+        c = (out[0::2] + 1j * out[1::2]).reshape(fd.nb, fd.bs, fd.bs)  # [b][col][row]
+        return c.transpose(0, 2, 1)
 
     def update_cn2(self, l2c, fd=None):
         keep = []

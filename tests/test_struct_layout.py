@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 INC = os.path.join(HERE, "..", "include")
 
 PAIRS = [("mb_grid", native.MbGrid), ("mb_wfs_desc", native.MbWfsDesc), ("mb_fdpcg_desc", native.MbFdpcgDesc),
+         ("mb_fdpcg_geom", native.MbFdpcgGeom),
          ("mb_csc", native.MbCsc), ("mb_fit_desc", native.MbFitDesc),
          ("mb_fit_sparse_desc", native.MbFitSparseDesc), ("mb_recon_desc", native.MbReconDesc),
          ("mb_geom_wfs_desc", native.MbGeomWfsDesc)]

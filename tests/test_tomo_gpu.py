@@ -258,3 +258,59 @@ def test_fused_preconditioner_matches_the_oracle(setup):
         assert np.array_equal(a2[0], xs[2][1][1])
     finally:
         R.fdpcg_mode(1)
+
+
+def test_fdpcg_data_term_formed_and_rebuilt_on_device(setup):
+    """f2, the FDPCG part of gpu_update_recon on the device: the block
+    matrices' data term (maos/fdpcg.c:427-480) is formed on the GPU from its
+    geometry and equals the host setup's at FP64 round-off; after the noise of
+    one WFS changes, mb_update_recon_nea + mb_update_recon_neam rebuild the
+    data term and the blocks on the device, again equal to the host setup's
+    at the new noise, and the preconditioner and the solve follow the oracle
+    built at the new noise."""
+    import dataclasses
+    import time
+    from maos_b200 import fdpcg_setup
+    s, R, o = setup
+    if s.fdpcg is None:
+        pytest.skip("plain CG configuration")
+    want = s.fdpcg.mhat_data
+    got = R.fdpcg_data()
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    # the noise of WFS 1 rises by 1.5 (its PTT is unchanged by a uniform scale)
+    sc = 1.5
+    wfs = list(s.wfs)
+    w = wfs[1]
+    wfs[1] = dataclasses.replace(w, saneai=w.saneai / sc ** 2, sanea=w.sanea * sc ** 2, neam=w.neam * sc)
+    s2 = dataclasses.replace(s, wfs=wfs, fdpcg=None)
+    s2 = dataclasses.replace(s2, fdpcg=fdpcg_setup.fdpcg_prepare(s2))
+    nsa = w.nsa
+
+    def neai_of(wt):
+        return np.stack([wt.saneai[:nsa], wt.saneai[nsa:], np.zeros(nsa)], axis=1).ravel()
+
+    try:
+        R.update_nea(1, neai_of(wfs[1]), w.PTT)
+        R.lib.mb_kernel_launches(1)
+        t0 = time.perf_counter()
+        R.update_neam(s2.fdpcg.geom["neam"])
+        dt = time.perf_counter() - t0
+        got2 = R.fdpcg_data()
+        want2 = s2.fdpcg.mhat_data
+        assert np.abs(got2 - want2).max() <= 1e-12 * np.abs(want2).max()
+        assert np.abs(want2 - want).max() > 1e-3 * np.abs(want).max()  # the change is real
+        o2 = TomoOracle(s2)
+        x = np.random.default_rng(8).standard_normal((2, s.nx_total))
+        z = R.apply_fdpcg(x)
+        for b in range(2):
+            assert rel(z[b], o2.fdpcg_precond(x[b])) < OP_TOL
+        g = np.random.default_rng(9).standard_normal((2, s.ngrad)) * 1e-6
+        R.reset()
+        xs, _ = R.tomo(g)
+        for b in range(2):
+            w2, _ = tomo_solve(o2, g[b])
+            assert rel(xs[b], w2) < SOLVE_TOL
+        print(f"device rebuild of the FDPCG data term and blocks: {dt * 1e3:.3f} ms")
+    finally:
+        R.update_nea(1, neai_of(w), w.PTT)
+        R.update_neam(s.fdpcg.geom["neam"])
