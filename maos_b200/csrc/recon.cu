@@ -947,7 +947,7 @@ void Recon::build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector
     T.oSC = (int)(T.oSR + nSR);
     T.oSY = (int)(T.oSC + nSC);
     fd_fsmem = (size_t)(T.oSY + nSC) * sizeof(cplx);
-    if (fd_fsmem > 110 * 1024) return;  // two CTAs per SM or the three-kernel form
+    if (fd_fsmem > 200 * 1024) return;  // else the three-kernel form
     // member owners: the CTA whose columns hold the member's bin
     std::vector<FdMem> mem(idx.size());
     for (size_t i = 0; i < idx.size(); i++) {

@@ -400,6 +400,7 @@ struct PadIndex {
 
 constexpr int kMaxPadX = 8;     // widest x list
 constexpr int kMaxPadY = 8;     // widest y list (k_hxt_rows is instantiated up to this)
+constexpr int kHxtWfs = 6;      // WFS whose gathers k_hxt_rows issues together for one instance
 
 // Dynamic shared memory of k_pupil_rows, in floats, for `rows` output rows.
 __host__ __device__ constexpr int pupil_rows_smem_floats(int rows, int nxp, int nps, int ncols, int kx) {
@@ -622,24 +623,59 @@ k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__
         float acc[NI];
 #pragma unroll
         for (int q = 0; q < NI; q++) acc[q] = 0.f;
+        if constexpr (NI == 1) {
+            // one instance: the lists of kHxtWfs WFS are loaded together, then
+            // all their row-buffer values, so the WFS cost two round trips
+            // instead of two each (same sums, same order)
+            for (int w0 = 0; w0 < nwfs; w0 += kHxtWfs) {
+                GatherW ge[kHxtWfs][KY];
+                bool in[kHxtWfs];
+#pragma unroll
+                for (int u = 0; u < kHxtWfs; u++) {
+                    const int w = w0 + u;
+                    in[u] = false;
+                    if (w < nwfs) {
+                        const int4 f = pi.fp[w * nps + l];
+                        in[u] = !(jx < f.x || jx >= f.y || jy < f.z || jy >= f.w);
+                    }
+#pragma unroll
+                    for (int k = 0; k < KY; k++) ge[u][k] = in[u] ? e[(size_t)w * estep + k] : GatherW{0, 0.f};
+                }
+                float tv[kHxtWfs][KY];
+#pragma unroll
+                for (int u = 0; u < kHxtWfs; u++)
+#pragma unroll
+                    for (int k = 0; k < KY; k++)
+                        tv[u][k] = (in[u] && on[0]) ? tl[(size_t)(w0 + u) * tw + ge[u][k].i * nx] : 0.f;
+#pragma unroll
+                for (int u = 0; u < kHxtWfs; u++) {
+                    if (!in[u]) continue;
+                    float sy = 0.f;
+#pragma unroll
+                    for (int k = 0; k < KY; k++) sy += ge[u][k].w * tv[u][k];
+                    acc[0] += sy;
+                }
+            }
+        } else {
 #pragma unroll 2
-        for (int w = 0; w < nwfs; w++, e += estep, tl += tw) {
-            const int4 f = pi.fp[w * nps + l];
-            if (jx < f.x || jx >= f.y || jy < f.z || jy >= f.w) continue;  // outside this WFS's footprint
-            GatherW ge[KY];
-            float tv[NI][KY];
+            for (int w = 0; w < nwfs; w++, e += estep, tl += tw) {
+                const int4 f = pi.fp[w * nps + l];
+                if (jx < f.x || jx >= f.y || jy < f.z || jy >= f.w) continue;  // outside this WFS's footprint
+                GatherW ge[KY];
+                float tv[NI][KY];
 #pragma unroll
-            for (int k = 0; k < KY; k++) ge[k] = e[k];
+                for (int k = 0; k < KY; k++) ge[k] = e[k];
 #pragma unroll
-            for (int q = 0; q < NI; q++)
+                for (int q = 0; q < NI; q++)
 #pragma unroll
-                for (int k = 0; k < KY; k++) tv[q][k] = on[q] ? tl[q * tinst + ge[k].i * nx] : 0.f;
+                    for (int k = 0; k < KY; k++) tv[q][k] = on[q] ? tl[q * tinst + ge[k].i * nx] : 0.f;
 #pragma unroll
-            for (int q = 0; q < NI; q++) {
-                float sy = 0.f;
+                for (int q = 0; q < NI; q++) {
+                    float sy = 0.f;
 #pragma unroll
-                for (int k = 0; k < KY; k++) sy += ge[k].w * tv[q][k];
-                acc[q] += sy;
+                    for (int k = 0; k < KY; k++) sy += ge[k].w * tv[q][k];
+                    acc[q] += sy;
+                }
             }
         }
 #pragma unroll
@@ -1804,8 +1840,9 @@ __device__ void fft_dir_inplace(int pair, cplx *a, cplx *b, int n, int count, in
     }
 }
 
-// grid: (C, nb), clusters of C CTAs along x; block: kFftThreads.
-__global__ void __launch_bounds__(kFftThreads, 2)
+// grid: (C, nb), clusters of C CTAs along x; block: kFftThreads (one CTA
+// per SM: the registers carry r, p and a block row between phases).
+__global__ void __launch_bounds__(kFftThreads, 1)
 k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid_constant__ FdFusedTab fu,
            const cplx *__restrict__ tw, const cplx *__restrict__ M, const FdMem *__restrict__ mem, int bs,
            long nxtot, float *__restrict__ xw, const float *__restrict__ Apv, CgScal SC, int kit, int init,
@@ -1827,11 +1864,15 @@ k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid
     const size_t base = (size_t)b * nxtot + L.off;
     float *rb = r + base;
     const int xs = blockDim.x / nx, x0 = threadIdx.x / nx, xc = threadIdx.x - x0 * nx;  // nx <= blockDim
-    // ---- F1: CG update and row FFTs of this CTA's row pairs
+    // ---- F1: CG update and row FFTs of this CTA's row pairs.  When a thread's
+    // rows fit one pass (one = true), the updated r and the old p stay in its
+    // registers for the r.z and the p update at the end.
+    const bool one = npr <= kFdLoads * xs;
+    float rv[kFdLoads][2], pp[kFdLoads][2];
     if (x0 < xs) {
         const float a = SC.ab ? SC.ab[2 * b] : 0.f;
         for (int p0 = P.p0 + x0; p0 < P.p1; p0 += kFdLoads * xs) {
-            float rv[kFdLoads][2], xv[kFdLoads][2], pp[kFdLoads][2], qq[kFdLoads][2];
+            float xv[kFdLoads][2], qq[kFdLoads][2];
 #pragma unroll
             for (int u = 0; u < kFdLoads; u++) {
                 const int p = p0 + u * xs;
@@ -1862,6 +1903,8 @@ k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid
                         r1 -= a * qq[u][1];
                         rb[o0] = r0;
                         rb[o1] = r1;
+                        rv[u][0] = r0;
+                        rv[u][1] = r1;
                     }
                     R[(p - P.p0) * nx + xc] = make_float2(r0, r1);
                 }
@@ -1893,42 +1936,35 @@ k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid
     __syncthreads();
     fft_dir_inplace<false>(L.py, SCb, S, ny, ncl, ncl, L.ry, L.nry, twy, false);
     cluster_sync_all();  // B2: spectra final in every SC; no SR is read any more
-    // ---- M: this CTA's frequency blocks
-    {
-        const int per = blockDim.x / bs;
-        const int lb = threadIdx.x / bs, i = threadIdx.x - lb * bs;
-        cplx *xsb = R;  // staging of the gathered members (R is free now)
-        for (int blk0 = P.b0; blk0 < P.b1; blk0 += per) {
-            const int blk = blk0 + lb;
-            const bool live = lb < per && blk < P.b1;
-            FdMem e{};
-            cplx m[kMaxBs];
-            if (live) {
-                e = mem[(size_t)blk * bs + i];
-                const cplx *Mb = M + (size_t)blk * bs * bs + i;
+    // ---- M: this CTA's frequency blocks; a thread takes one row i of a block
+    // and gathers the block's members itself (no barrier in the phase)
+    for (int it = threadIdx.x; it < (P.b1 - P.b0) * bs; it += blockDim.x) {
+        const int blk = P.b0 + it / bs, i = it % bs;
+        const FdMem e = mem[(size_t)blk * bs + i];
+        if (!(e.flags & kFdStore)) continue;
+        const FdMem *eb = mem + (size_t)blk * bs;
+        const cplx *Mb = M + (size_t)blk * bs * bs + i;
+        cplx m[kMaxBs], xv[kMaxBs];
 #pragma unroll
-                for (int jj = 0; jj < kMaxBs; jj++) m[jj] = jj < bs ? Mb[jj * bs] : make_float2(0.f, 0.f);
-                cplx xv = dsm_ld(dsm_base(SCb, (unsigned)e.rank) + 8u * (unsigned)e.off);
-                if (e.flags & kFdConj) xv.y = -xv.y;
-                xsb[threadIdx.x] = xv;
+        for (int jj = 0; jj < kMaxBs; jj++) {
+            m[jj] = jj < bs ? Mb[jj * bs] : make_float2(0.f, 0.f);
+            if (jj < bs) {
+                const FdMem ej = eb[jj];
+                xv[jj] = dsm_ld(dsm_base(SCb, (unsigned)ej.rank) + 8u * (unsigned)ej.off);
+                if (ej.flags & kFdConj) xv[jj].y = -xv[jj].y;
+            } else {
+                xv[jj] = make_float2(0.f, 0.f);
             }
-            __syncthreads();
-            if (live && (e.flags & kFdStore)) {
-                const cplx *xb = xsb + lb * bs;
-                float re = 0.f, im = 0.f;
-#pragma unroll
-                for (int jj = 0; jj < kMaxBs; jj++) {
-                    if (jj < bs) {
-                        const cplx xv = xb[jj];
-                        re += m[jj].x * xv.x - m[jj].y * xv.y;
-                        im += m[jj].x * xv.y + m[jj].y * xv.x;
-                    }
-                }
-                dsm_st(dsm_base(SY, (unsigned)e.rank) + 8u * (unsigned)e.off,
-                       make_float2(re, (e.flags & kFdConj) ? -im : im));
-            }
-            __syncthreads();
         }
+        float re = 0.f, im = 0.f;
+#pragma unroll
+        for (int jj = 0; jj < kMaxBs; jj++) {
+            if (jj < bs) {
+                re += m[jj].x * xv[jj].x - m[jj].y * xv[jj].y;
+                im += m[jj].x * xv[jj].y + m[jj].y * xv[jj].x;
+            }
+        }
+        dsm_st(dsm_base(SY, (unsigned)e.rank) + 8u * (unsigned)e.off, make_float2(re, (e.flags & kFdConj) ? -im : im));
     }
     cluster_sync_all();  // B3: every stored bin of every SY written; no SC is read any more
     // ---- I1: inverse column FFTs
@@ -1962,14 +1998,15 @@ k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid
     double v = 0;
     if (x0 < xs)
         for (int p0 = P.p0 + x0; p0 < P.p1; p0 += kFdLoads * xs) {
-            float rv[kFdLoads][2];
+            if (!one) {
 #pragma unroll
-            for (int u = 0; u < kFdLoads; u++) {
-                const int p = p0 + u * xs;
-                if (p < P.p1) {
-                    const size_t o0 = (size_t)(2 * p) * nx + xc;
-                    rv[u][0] = rb[o0];
-                    rv[u][1] = rb[o0 + nx];
+                for (int u = 0; u < kFdLoads; u++) {
+                    const int p = p0 + u * xs;
+                    if (p < P.p1) {
+                        const size_t o0 = (size_t)(2 * p) * nx + xc;
+                        rv[u][0] = rb[o0];
+                        rv[u][1] = rb[o0 + nx];
+                    }
                 }
             }
 #pragma unroll
@@ -2012,14 +2049,15 @@ k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid
     const float be = (float)s_be;
     if (x0 < xs)
         for (int p0 = P.p0 + x0; p0 < P.p1; p0 += kFdLoads * xs) {
-            float pp[kFdLoads][2];
+            if (!one || !xw) {  // the old p is in registers only after a CG update pass
 #pragma unroll
-            for (int u = 0; u < kFdLoads; u++) {
-                const int p = p0 + u * xs;
-                if (p < P.p1 && !init) {
-                    const size_t o0 = base + (size_t)(2 * p) * nx + xc;
-                    pp[u][0] = pv[o0];
-                    pp[u][1] = pv[o0 + nx];
+                for (int u = 0; u < kFdLoads; u++) {
+                    const int p = p0 + u * xs;
+                    if (p < P.p1 && !init) {
+                        const size_t o0 = base + (size_t)(2 * p) * nx + xc;
+                        pp[u][0] = pv[o0];
+                        pp[u][1] = pv[o0 + nx];
+                    }
                 }
             }
 #pragma unroll

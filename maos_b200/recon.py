@@ -340,8 +340,14 @@ class Reconstructor:
         return res
 
     def update_nea(self, iwfs: int, neai: np.ndarray, ptt: Optional[np.ndarray]):
-        ne = np.ascontiguousarray(neai, dtype=np.float64)
-        pt = np.ascontiguousarray(ptt, dtype=np.float64) if ptt is not None else None
+        """gpu_update_recon for one WFS: inverse NEA [nsa][3] (cx, cy, cxy) and
+        the tip/tilt projector, 2 x 2nsa (passed column-major, as the ABI
+        takes it) or None."""
+        ne = np.ascontiguousarray(neai, dtype=np.float64).ravel()
+        pt = None
+        if ptt is not None:
+            pt = np.asarray(ptt, dtype=np.float64)
+            pt = np.ascontiguousarray(pt.ravel(order="F") if pt.ndim == 2 else pt)
         check(self.lib.mb_update_recon_nea(self.h, iwfs, _dptr(ne),
                                            _dptr(pt) if pt is not None else C.POINTER(C.c_double)()),
               "mb_update_recon_nea")
