@@ -1936,35 +1936,43 @@ k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid
     __syncthreads();
     fft_dir_inplace<false>(L.py, SCb, S, ny, ncl, ncl, L.ry, L.nry, twy, false);
     cluster_sync_all();  // B2: spectra final in every SC; no SR is read any more
-    // ---- M: this CTA's frequency blocks; a thread takes one row i of a block
-    // and gathers the block's members itself (no barrier in the phase)
-    for (int it = threadIdx.x; it < (P.b1 - P.b0) * bs; it += blockDim.x) {
-        const int blk = P.b0 + it / bs, i = it % bs;
-        const FdMem e = mem[(size_t)blk * bs + i];
-        if (!(e.flags & kFdStore)) continue;
-        const FdMem *eb = mem + (size_t)blk * bs;
-        const cplx *Mb = M + (size_t)blk * bs * bs + i;
-        cplx m[kMaxBs], xv[kMaxBs];
+    // ---- M: this CTA's frequency blocks: a thread gathers one member of a
+    // block into shared memory, then forms its row of Y = Mbinv X
+    {
+        const int per = blockDim.x / bs;
+        const int lb = threadIdx.x / bs, i = threadIdx.x - lb * bs;
+        cplx *xsb = R;  // staging of the gathered members (R is free now)
+        for (int blk0 = P.b0; blk0 < P.b1; blk0 += per) {
+            const int blk = blk0 + lb;
+            const bool live = lb < per && blk < P.b1;
+            FdMem e{};
+            cplx m[kMaxBs];
+            if (live) {
+                e = mem[(size_t)blk * bs + i];
+                const cplx *Mb = M + (size_t)blk * bs * bs + i;
 #pragma unroll
-        for (int jj = 0; jj < kMaxBs; jj++) {
-            m[jj] = jj < bs ? Mb[jj * bs] : make_float2(0.f, 0.f);
-            if (jj < bs) {
-                const FdMem ej = eb[jj];
-                xv[jj] = dsm_ld(dsm_base(SCb, (unsigned)ej.rank) + 8u * (unsigned)ej.off);
-                if (ej.flags & kFdConj) xv[jj].y = -xv[jj].y;
-            } else {
-                xv[jj] = make_float2(0.f, 0.f);
+                for (int jj = 0; jj < kMaxBs; jj++) m[jj] = jj < bs ? Mb[jj * bs] : make_float2(0.f, 0.f);
+                cplx xv = dsm_ld(dsm_base(SCb, (unsigned)e.rank) + 8u * (unsigned)e.off);
+                if (e.flags & kFdConj) xv.y = -xv.y;
+                xsb[threadIdx.x] = xv;
             }
-        }
-        float re = 0.f, im = 0.f;
+            __syncthreads();
+            if (live && (e.flags & kFdStore)) {
+                const cplx *xb = xsb + lb * bs;
+                float re = 0.f, im = 0.f;
 #pragma unroll
-        for (int jj = 0; jj < kMaxBs; jj++) {
-            if (jj < bs) {
-                re += m[jj].x * xv[jj].x - m[jj].y * xv[jj].y;
-                im += m[jj].x * xv[jj].y + m[jj].y * xv[jj].x;
+                for (int jj = 0; jj < kMaxBs; jj++) {
+                    if (jj < bs) {
+                        const cplx xv = xb[jj];
+                        re += m[jj].x * xv.x - m[jj].y * xv.y;
+                        im += m[jj].x * xv.y + m[jj].y * xv.x;
+                    }
+                }
+                dsm_st(dsm_base(SY, (unsigned)e.rank) + 8u * (unsigned)e.off,
+                       make_float2(re, (e.flags & kFdConj) ? -im : im));
             }
+            __syncthreads();
         }
-        dsm_st(dsm_base(SY, (unsigned)e.rank) + 8u * (unsigned)e.off, make_float2(re, (e.flags & kFdConj) ? -im : im));
     }
     cluster_sync_all();  // B3: every stored bin of every SY written; no SC is read any more
     // ---- I1: inverse column FFTs

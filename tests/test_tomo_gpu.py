@@ -212,6 +212,10 @@ def test_autotune_keeps_results():
         assert rows in ms or (4 <= rows <= 32 and rows in splits)  # 4/8/16 or an even split
         if rows in ms:
             assert ms[rows] == min(ms.values())
+        # the blocking changes no bit; the preconditioner's form (which the
+        # autotuner also picks) only FP32 rounding: compare in the first form
+        if s.fdpcg is not None:
+            R.fdpcg_mode(1)
         R.reset()
         x1, _ = R.tomo(g)
         assert np.array_equal(x0, x1)
