@@ -308,22 +308,29 @@ k_mvm_tc(const char *__restrict__ Mt, const char *__restrict__ gs, long nch, int
     } else if (kWiden) {  // widening warps
         const int tid = threadIdx.x - 64;
         for (int ch = 0; ch < nchunk; ch++) {
-            if (!mbar_wait(smem_addr(&full[ch % S]), (uint32_t)((ch / S) & 1), &s_abort)) {
-                s_abort = 1;
-                break;
+            // one lane per warp polls the barriers; the others wait at the
+            // shuffle instead of spinning on the mbarrier unit
+            int ok = 1;
+            if (lane == 0) {
+                ok = mbar_wait(smem_addr(&full[ch % S]), (uint32_t)((ch / S) & 1), &s_abort);
+                // the MMAs of chunk ch-2 (the last reader of this BF16 tile) completed
+                if (ok && ch >= 2) ok = mbar_wait(smem_addr(&tfree[ch & 1]), (uint32_t)(((ch - 2) >> 1) & 1), &s_abort);
+                if (!ok) s_abort = 1;
             }
-            // the MMAs of chunk ch-2 (the last reader of this BF16 tile) completed
-            if (ch >= 2 && !mbar_wait(smem_addr(&tfree[ch & 1]), (uint32_t)(((ch - 2) >> 1) & 1), &s_abort)) {
-                s_abort = 1;
-                break;
-            }
+            if (!__shfl_sync(0xffffffffu, ok, 0)) break;
             tc_widen_fp8(tcsm + (ch % S) * SB, widen + (ch & 1) * kTcTileBf16, tid);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_addr(&ready[ch & 1])) : "memory");
         }
     }
-    bool bad = !mbar_wait(smem_addr(&done), 0);
-    if (bad) mbar_wait(smem_addr(&done), 0);  // bounded, before the accumulators are freed
+    // one thread waits for the MMAs (bounded, twice before the accumulators
+    // are freed); the rest of the CTA waits at the barrier, not on the mbarrier
+    bool bad = false;
+    if (threadIdx.x == 0) {
+        bad = !mbar_wait(smem_addr(&done), 0);
+        if (bad) mbar_wait(smem_addr(&done), 0);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    }
     const bool skip = __syncthreads_or(bad) || s_abort || s_mmas < nchunk;
     if (skip && threadIdx.x == 0) atomicExch(err, 1);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
