@@ -252,7 +252,8 @@ struct Mvm {
     bool tiled = false;  // m holds the tensor-core tiles (mvm_tc.cuh) instead of rows
     long nch = 0;        // 64-column chunks per row when tiled (ldm / 64)
     DevBuf<unsigned char> m;  // raw storage
-    DevBuf<unsigned char> gs;  // tiled: the gradients' BF16 terms (k_gsplit)
+    DevBuf<unsigned char> gs;  // tiled: the gradients' BF16 or E4M3 terms (k_gsplit, k_gsplit8)
+    DevBuf<unsigned> gmax;     // tiled FP8: each instance's max|g| (the terms' scales)
     DevBuf<float> scale, part, g, out;
     DevBuf<int> err;  // set when a tensor-core MMA wait timed out
     cudaStream_t stream = nullptr;
@@ -303,14 +304,23 @@ struct Mvm {
             attr = true;
         }
         const int nz = (nbatch + N - 1) / N;
-        const long items = (long)nz * nch * N * 8;
-        k_gsplit<N><<<(unsigned)((items + 255) / 256), 256, 0, s>>>(dg, ngrad, nbatch, nch, nz,
-                                                                    reinterpret_cast<char *>(gs.p));
+        if constexpr (DT == MB_MVM_BF16) {
+            const long items = (long)nz * nch * N * 8;
+            k_gsplit<N><<<(unsigned)((items + 255) / 256), 256, 0, s>>>(dg, ngrad, nbatch, nch, nz,
+                                                                        reinterpret_cast<char *>(gs.p));
+        } else {
+            MB_CUDA_TRY(cudaMemsetAsync(gmax.p, 0, (size_t)nz * N * sizeof(unsigned), s));
+            k_gmax<<<dim3((unsigned)std::min<long>((ngrad + 255) / 256, 16), nbatch), 256, 0, s>>>(dg, ngrad, gmax.p);
+            MB_CHECK_LAUNCH();
+            const long items = (long)nz * nch * N * 4;
+            k_gsplit8<N><<<(unsigned)((items + 255) / 256), 256, 0, s>>>(dg, ngrad, nbatch, nch, nz, gmax.p,
+                                                                         reinterpret_cast<char *>(gs.p));
+        }
         MB_CHECK_LAUNCH();
         const dim3 grid((nact + kTcRows - 1) / kTcRows, nks, nz);
         k_mvm_tc<DT, N><<<grid, kTcThreads, smem, s>>>(reinterpret_cast<const char *>(m.p),
-                                                      reinterpret_cast<const char *>(gs.p), nch, kK / kTcK, part.p,
-                                                      nact, nbatch, err.p);
+                                                      reinterpret_cast<const char *>(gs.p), gmax.p, nch, kK / kTcK,
+                                                      part.p, nact, nbatch, err.p);
         MB_CHECK_LAUNCH();
         const long n = (long)nact * nbatch;
         k_mvm_reduce<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part.p, dtype == MB_MVM_FP8 ? scale.p : nullptr,
@@ -519,6 +529,7 @@ int mb_mvm_create(const double *Mcol, long nact, long ngrad, int dtype, int nbat
         if (V.tiled) {
             const int N = nbatch <= 16 ? 16 : nbatch <= 32 ? 32 : 64;
             V.gs.alloc((size_t)((nbatch + N - 1) / N) * V.nch * mb::tc_b_bytes(N));
+            if (dtype == MB_MVM_FP8) V.gmax.alloc((size_t)((nbatch + N - 1) / N) * N);
         }
         V.scale.upload(sc);
         V.err.alloc(1);

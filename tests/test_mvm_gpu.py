@@ -27,7 +27,7 @@ def rounded(M, dtype):
 
 
 @pytest.mark.parametrize("dtype", [0, 1, 2])
-@pytest.mark.parametrize("nbatch", [1, 3, 8, 20])
+@pytest.mark.parametrize("nbatch", [1, 3, 8, 20, 40])
 def test_mvm_matches_rounded_product(dtype, nbatch):
     from maos_b200 import native
     lib = native.load()
@@ -49,3 +49,33 @@ def test_mvm_matches_rounded_product(dtype, nbatch):
     assert err < 1e-5, err
     storage = np.linalg.norm(out - g @ M.T) / np.linalg.norm(g @ M.T)
     assert storage < (1e-5, 1e-2, 8e-2)[dtype]
+
+
+@pytest.mark.parametrize("dtype", [1, 2])
+def test_tensor_core_mvm_wide_dynamic_range(dtype):
+    """Gradients spanning twelve decades within each instance, one instance all
+    zero, on the tensor-core path (batch >= 4): the BF16 path's two terms and
+    the FP8 path's four power-of-two-scaled E4M3 terms still give the product
+    of the rounded matrix to 1e-5 per instance, and exactly zero for the zero
+    instance."""
+    from maos_b200 import native
+    lib = native.load()
+    rng = np.random.default_rng(40 + dtype)
+    nact, ngrad, nbatch = 300, 2500, 12
+    M = rng.standard_normal((nact, ngrad))
+    g = rng.standard_normal((nbatch, ngrad)) * 10.0 ** rng.uniform(-6, 6, (nbatch, ngrad))
+    g[0] = 0
+    g[1] *= 1e-20  # small, still clear of FP32 subnormals in the BF16 low term
+    h = C.c_void_p()
+    Mc = np.asfortranarray(M)
+    native.check(lib.mb_mvm_create(Mc.ctypes.data_as(C.POINTER(C.c_double)), nact, ngrad, dtype,
+                                   nbatch, C.byref(h)), "mb_mvm_create")
+    out = np.empty((nbatch, nact))
+    native.check(lib.mb_recon_mvm(h, g.ctypes.data_as(C.POINTER(C.c_double)),
+                                  out.ctypes.data_as(C.POINTER(C.c_double))), "mb_recon_mvm")
+    lib.mb_mvm_free(h)
+    want = g.astype(np.float32).astype(np.float64) @ rounded(M, dtype).T
+    assert np.all(out[0] == 0)
+    for b in range(1, nbatch):
+        err = np.linalg.norm(out[b] - want[b]) / np.linalg.norm(want[b])
+        assert err < 1e-5, (b, err)
