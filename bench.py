@@ -422,12 +422,48 @@ def single_instance_rates(preset: str, nsteps: int = 200, warmup: int = 5):
             ev[k][1].record(stream)
     torch.cuda.synchronize()
     t = sorted(a.elapsed_time(b) for a, b in ev)
+    updates = table_updates(R, sysm)
     R.close()
-    return {"instances": 1, "steps": nsteps, "steps_per_s": 1000.0 * nsteps / sum(t),
-            "latency_ms": {"p50": statistics.median(t), "p99": t[min(nsteps - 1, int(math.ceil(0.99 * nsteps)) - 1)],
-                           "max": t[-1]},
-            "pupil_rows": rows, "tomo": f"{'FDPCG' if sysm.cfg.tomo_precond else 'CG'} {sysm.cfg.tomo_maxit} it",
-            "fit_it": fit.maxit}
+    out = {"instances": 1, "steps": nsteps, "steps_per_s": 1000.0 * nsteps / sum(t),
+           "latency_ms": {"p50": statistics.median(t), "p99": t[min(nsteps - 1, int(math.ceil(0.99 * nsteps)) - 1)],
+                          "max": t[-1]},
+           "pupil_rows": rows, "tomo": f"{'FDPCG' if sysm.cfg.tomo_precond else 'CG'} {sysm.cfg.tomo_maxit} it",
+           "fit_it": fit.maxit}
+    if updates:
+        out["table_updates_ms"] = updates
+    return out
+
+
+def table_updates(R, sysm, reps: int = 5):
+    """Host wall time (to completion on the device) of the reconstructor's
+    table updates, each rebuilding every table it affects on the GPU:
+    gpu_update_recon for one WFS (its NEA and tip/tilt projector, then the
+    FDPCG data term and blocks from the new mean NEA) and gpu_update_recon_cn2
+    (the L2 weights and the FDPCG blocks, no host tables).  The median of
+    `reps` calls, the original values re-installed each time."""
+    import numpy as np
+    import torch
+    if sysm.fdpcg is None:
+        return None
+    w = sysm.wfs[1]
+    nsa = w.nsa
+    neai = np.stack([w.saneai[:nsa], w.saneai[nsa:], np.zeros(nsa)], axis=1).ravel()
+    neam = np.asarray(sysm.fdpcg.geom["neam"], dtype=np.float64)
+    l2c = np.asarray(sysm.l2c, dtype=np.float64)
+    tn, tc = [], []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        R.update_nea(1, neai, w.PTT)
+        R.update_neam(neam)
+        torch.cuda.synchronize()
+        tn.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        R.update_cn2(l2c)
+        torch.cuda.synchronize()
+        tc.append(time.perf_counter() - t0)
+    return {"nea_one_wfs_with_fdpcg_rebuild": 1e3 * statistics.median(tn),
+            "cn2_with_fdpcg_rebuild": 1e3 * statistics.median(tc)}
 
 
 SERVE_MIX = (("scao_8m", 26), ("ltao_8m", 26), ("mcao_30m", 12))

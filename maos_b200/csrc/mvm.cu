@@ -15,6 +15,7 @@
 #include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstdint>
@@ -253,7 +254,8 @@ struct Mvm {
     long nch = 0;        // 64-column chunks per row when tiled (ldm / 64)
     DevBuf<unsigned char> m;  // raw storage
     DevBuf<unsigned char> gs;  // tiled: the gradients' BF16 or E4M3 terms (k_gsplit, k_gsplit8)
-    DevBuf<unsigned> gmax;     // tiled FP8: each instance's max|g| (the terms' scales)
+    DevBuf<int> kexp;          // tiled FP8: each instance's scale exponent (k_gsplit8)
+    DevBuf<int> cnt;           // tiled: stream-K arrival counter per (batch tile, row block)
     DevBuf<float> scale, part, g, out;
     DevBuf<int> err;  // set when a tensor-core MMA wait timed out
     cudaStream_t stream = nullptr;
@@ -295,36 +297,83 @@ struct Mvm {
         }();
         return on;
     }
+    // Stream-K layout of the tensor-core path, fixed at creation.
+    int tc_nrb = 0, tc_P = 0, tc_maxp = 0;
+    long tc_W = 0;
+    template <int DT, int N>
+    static int tc_resident() {  // CTAs of k_mvm_tc<DT, N> resident on the device
+        static int n = 0;
+        if (!n) {
+            constexpr int smem = tc_smem_bytes(DT, N);
+            MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_tc<DT, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            // all of the unified L1 as shared memory, so that two rings fit an SM
+            // (the occupancy query and the launch both follow this preference)
+            MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_tc<DT, N>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                             (int)cudaSharedmemCarveoutMaxShared));
+            // CTAs per SM from the kernel's own limits (shared memory, registers,
+            // threads); a persistent CTA never waits for another, so a count
+            // above what is resident only costs a second wave
+            int dev = 0, nsm = 0, smsm = 0, rsv = 0, thr = 0;
+            MB_CUDA_TRY(cudaGetDevice(&dev));
+            MB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+            MB_CUDA_TRY(cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+            MB_CUDA_TRY(cudaDeviceGetAttribute(&rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+            MB_CUDA_TRY(cudaDeviceGetAttribute(&thr, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
+            cudaFuncAttributes fa{};
+            MB_CUDA_TRY(cudaFuncGetAttributes(&fa, k_mvm_tc<DT, N>));
+            const long regs = (long)((fa.numRegs * 32 + 255) / 256 * 256) * (kTcThreads / 32);
+            const long by_smem = smsm / ((long)smem + (long)fa.sharedSizeBytes + rsv);
+            const long by_regs = 65536 / std::max<long>(regs, 1);
+            const long occ = std::max<long>(1, std::min({by_smem, by_regs, (long)(thr / kTcThreads), 2L}));
+            n = (int)(nsm * occ);
+        }
+        return n;
+    }
+    template <int DT, int N>
+    void plan_tc() {
+        const int nz = (nbatch + N - 1) / N;
+        tc_nrb = (nact + kTcRows - 1) / kTcRows;
+        const long nchu = (nch + tc_unit_chunks(DT) - 1) / tc_unit_chunks(DT);
+        tc_W = (long)nz * tc_nrb * nchu;
+        tc_P = (int)std::min<long>(tc_resident<DT, N>(), tc_W);
+        tc_maxp = tc_max_pieces(nchu, tc_W, tc_P);
+        gs.alloc((size_t)nz * nch * tc_b_bytes(N));
+        gs.zero_async(stream);
+        if (DT == MB_MVM_FP8) kexp.alloc((size_t)nz * N);
+        part.alloc((size_t)nz * tc_nrb * tc_maxp * N * kTcRows);
+        cnt.alloc((size_t)nz * tc_nrb);
+        cnt.zero_async(stream);
+    }
+    template <int DT>
+    void plan_tc_dt() {
+        if (nbatch <= 16) plan_tc<DT, 16>();
+        else if (nbatch <= 32) plan_tc<DT, 32>();
+        else plan_tc<DT, 64>();
+    }
     template <int DT, int N>
     void launch_tc(const float *dg, float *dout, cudaStream_t s) {
         constexpr int smem = tc_smem_bytes(DT, N);
-        static bool attr = false;
-        if (!attr) {
-            MB_CUDA_TRY(cudaFuncSetAttribute(k_mvm_tc<DT, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            attr = true;
-        }
-        const int nz = (nbatch + N - 1) / N;
+        const int nz = (nbatch + N - 1) / N, ncnt = nz * tc_nrb;
         if constexpr (DT == MB_MVM_BF16) {
             const long items = (long)nz * nch * N * 8;
             k_gsplit<N><<<(unsigned)((items + 255) / 256), 256, 0, s>>>(dg, ngrad, nbatch, nch, nz,
-                                                                        reinterpret_cast<char *>(gs.p));
+                                                                        reinterpret_cast<char *>(gs.p), cnt.p, ncnt);
         } else {
-            MB_CUDA_TRY(cudaMemsetAsync(gmax.p, 0, (size_t)nz * N * sizeof(unsigned), s));
-            k_gmax<<<dim3((unsigned)std::min<long>((ngrad + 255) / 256, 16), nbatch), 256, 0, s>>>(dg, ngrad, gmax.p);
-            MB_CHECK_LAUNCH();
-            const long items = (long)nz * nch * N * 4;
-            k_gsplit8<N><<<(unsigned)((items + 255) / 256), 256, 0, s>>>(dg, ngrad, nbatch, nch, nz, gmax.p,
-                                                                         reinterpret_cast<char *>(gs.p));
+            const long share = (nch * 4 + kSplitCta - 1) / kSplitCta * 64;  // bytes of the largest share
+            const bool stage = share <= 96 * 1024;
+            static bool attr = false;
+            if (!attr) {
+                MB_CUDA_TRY(cudaFuncSetAttribute(k_gsplit8<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+                attr = true;
+            }
+            k_gsplit8<N><<<dim3(kSplitCta, nbatch), 256, stage ? (size_t)share : 0, s>>>(
+                dg, ngrad, nch, kexp.p, reinterpret_cast<char *>(gs.p), cnt.p, ncnt, stage);
         }
         MB_CHECK_LAUNCH();
-        const dim3 grid((nact + kTcRows - 1) / kTcRows, nks, nz);
-        k_mvm_tc<DT, N><<<grid, kTcThreads, smem, s>>>(reinterpret_cast<const char *>(m.p),
-                                                      reinterpret_cast<const char *>(gs.p), gmax.p, nch, kK / kTcK,
-                                                      part.p, nact, nbatch, err.p);
-        MB_CHECK_LAUNCH();
-        const long n = (long)nact * nbatch;
-        k_mvm_reduce<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part.p, dtype == MB_MVM_FP8 ? scale.p : nullptr,
-                                                                dout, nact, nbatch, nks);
+        k_mvm_tc<DT, N><<<tc_P, kTcThreads, smem, s>>>(
+            reinterpret_cast<const char *>(m.p), reinterpret_cast<const char *>(gs.p), kexp.p,
+            DT == MB_MVM_FP8 ? scale.p : nullptr, tc_nrb, nch, tc_W, tc_P, tc_maxp, part.p, cnt.p, dout, nact, nbatch,
+            err.p);
         MB_CHECK_LAUNCH();
     }
     template <int DT>
@@ -527,16 +576,18 @@ int mb_mvm_create(const double *Mcol, long nact, long ngrad, int dtype, int nbat
             MB_CUDA_TRY(cudaMemcpy(V.m.p, h8.data(), nel, cudaMemcpyHostToDevice));
         }
         if (V.tiled) {
-            const int N = nbatch <= 16 ? 16 : nbatch <= 32 ? 32 : 64;
-            V.gs.alloc((size_t)((nbatch + N - 1) / N) * V.nch * mb::tc_b_bytes(N));
-            if (dtype == MB_MVM_FP8) V.gmax.alloc((size_t)((nbatch + N - 1) / N) * N);
+            if (dtype == MB_MVM_BF16) V.plan_tc_dt<MB_MVM_BF16>();
+            else V.plan_tc_dt<MB_MVM_FP8>();
+        } else {
+            V.part.alloc((size_t)V.nks * nbatch * nact);
         }
         V.scale.upload(sc);
         V.err.alloc(1);
         V.err.zero_async(V.stream);
-        V.part.alloc((size_t)V.nks * nbatch * nact);
         V.g.alloc((size_t)nbatch * ngrad);
         V.out.alloc((size_t)nbatch * nact);
+        // the zeroed buffers are ready before a caller's stream uses them
+        MB_CUDA_TRY(cudaStreamSynchronize(V.stream));
     } catch (const mb::CudaError &e) {
         delete h;
         return e.code;
