@@ -469,6 +469,66 @@ def table_updates(R, sysm, reps: int = 5):
 SERVE_MIX = (("scao_8m", 26), ("ltao_8m", 26), ("mcao_30m", 12))
 
 
+def grouped_mix(nsteps: int = 30, warmup: int = 3):
+    """The served mix's 64 instances of three geometries (26 8 m SCAO, 26 8 m
+    LTAO, 12 30 m MCAO) all stepped at once, two ways: one group graph per
+    step (mb_group_step_device: the tomography operators one launch over all
+    64 instances) and the three reconstructors' own step graphs on three
+    streams.  Device time per step (CUDA events, L2 flushed before every
+    step), instance steps/s and kernel launches per step."""
+    import numpy as np
+    import torch
+    from maos_b200 import config, fit_assemble, geometry, turbulence
+    from maos_b200.recon import Reconstructor, ReconGroup
+    rs, gs = [], []
+    for name, n in SERVE_MIX:
+        sysm = geometry.build_tomo(config.PRESETS[name]())
+        R = Reconstructor(sysm, nbatch=n, fit=fit_assemble.build_fit_assembled(sysm))
+        R.autotune(reps=5)
+        rs.append(R)
+        fr = turbulence.gradient_frames(sysm, seed=5, nframe=4).astype(np.float32)
+        gs.append(torch.tensor(np.stack([fr[k % 4] for k in range(n)]), device="cuda"))
+    G = ReconGroup(rs)
+    lib = rs[0].lib
+    main = torch.cuda.Stream()
+    side = [torch.cuda.Stream() for _ in rs]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ninst = sum(n for _, n in SERVE_MIX)
+
+    def run(grouped: bool):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+        for k in range(warmup + nsteps):
+            with torch.cuda.stream(main):
+                flush.fill_(float(k))
+                if k >= warmup:
+                    ev[k - warmup][0].record(main)
+                if grouped:
+                    G.step_device([g.data_ptr() for g in gs], main.cuda_stream)
+                else:
+                    for R, g, q in zip(rs, gs, side):
+                        q.wait_stream(main)
+                        R.step_device(g.data_ptr(), q.cuda_stream)
+                    for q in side:
+                        main.wait_stream(q)
+                if k >= warmup:
+                    ev[k - warmup][1].record(main)
+        torch.cuda.synchronize()
+        t = sorted(a.elapsed_time(b) for a, b in ev)
+        return {"ms_per_step": statistics.median(t), "instance_steps_per_s": 1000.0 * ninst / statistics.median(t)}
+
+    lib.mb_kernel_launches(1)
+    pools = run(False)
+    pools["launches_per_step"] = lib.mb_kernel_launches(1) / (warmup + nsteps)
+    grouped = run(True)
+    grouped["launches_per_step"] = lib.mb_kernel_launches(1) / (warmup + nsteps)
+    G.close()
+    for R in rs:
+        R.close()
+    return {"mix": " + ".join(f"{n} {name}" for name, n in SERVE_MIX), "instances": ninst,
+            "step": "tomography (FDPCG 30 it for mcao_30m, CG 30 it for the 8 m types) + assembled fit 4 it",
+            "group": grouped, "three_streams": pools}
+
+
 def served_mix(seconds: float, mcao_frames=None, mvm: bool = False):
     """The served mix: 64 systems (26 8 m SCAO, 26 8 m LTAO, 12 30 m MCAO), each
     sending Poisson requests at a rate drawn from U[500, 1000] Hz, all admitted,
@@ -713,6 +773,10 @@ def run_gpu(args):
     if world == 1:
         single = {name: single_instance_rates(name) for name in ("mcao_30m", "ltao_8m")}
 
+    grouped = None
+    if world == 1 and not args.no_serve:
+        grouped = grouped_mix()
+
     served = served_mvm = None
     if world == 1 and not args.no_serve and args.serve_seconds > 0:
         served = served_mix(args.serve_seconds, mcao_frames=fr[0])
@@ -752,6 +816,7 @@ def run_gpu(args):
                 "mvm": mvm_line,
                 "wfs_gradients": wfs_line,
                 "closed_loop": loop_line,
+                "grouped_mix": grouped,
                 "served": served,
                 "served_mvm": served_mvm,
                 "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,

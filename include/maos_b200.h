@@ -246,6 +246,31 @@ int mb_fit(mb_recon *r, double *dmout, float *cgres);
 int mb_recon_step_device(mb_recon *r, const float *d_grad, void *stream);
 /* Device pointer to the FP32 DM commands [nbatch][nact]. */
 const float *mb_fit_solution(mb_recon *r);
+
+/* Reconstructors of different geometries stepped together (uneven
+ * instances: e.g. 8 m SCAO, 8 m LTAO and 30 m MCAO pools).  No counterpart in
+ * the reference, which runs one reconstructor per simulation (curecon_t,
+ * cuda/recon.cu:477).  One captured graph advances every member by one step
+ * (tomography + fit, as mb_recon_step_device): the tomography operators (the
+ * RHS and each CG iteration's A p, k_pupil_rows + k_hxt_rows) are one launch
+ * over all members' instances, each block reading its member's tables from
+ * a per-member argument table; each member's CG vector updates,
+ * preconditioner and fit run between them, members overlapping.  A member's
+ * result equals its own mb_recon_step_device's.  Members must share the
+ * device and the tomography iteration count; at creation their padded list
+ * widths are made equal (exact zeros added; their own graphs are
+ * recaptured).  A member stays owned by the caller and must outlive the
+ * group; after a member's tables change (updates, autotune) the next step
+ * recaptures the group's graph.  At most 8 members per grouped launch (more
+ * members take more launches). */
+typedef struct mb_group mb_group;
+int mb_group_create(mb_recon *const *members, int n, mb_group **out);
+/* d_grad[i]: member i's FP32 gradients [nbatch_i][ngrad_i] on the device;
+ * the commands stay in each member's mb_fit_solution. */
+int mb_group_step_device(mb_group *g, const float *const *d_grad, void *stream);
+/* Kernel launches of one group step (the captured graph's kernels). */
+long mb_group_graph_kernels(const mb_group *g);
+void mb_group_free(mb_group *g);
 long mb_nact(const mb_recon *r);
 
 /* Device-resident form of mb_tomo for batched serving and benchmarks:

@@ -235,6 +235,7 @@ struct Recon {
     cudaGraphExec_t graph_fit = nullptr;   // fit step
     cudaGraphExec_t graph_step = nullptr;  // tomography + fit
     long graph_kernels = 0, graph_fit_kernels = 0, graph_step_kernels = 0;
+    long graph_version = 0;  // counts recaptures (a ReconGroup recaptures after a member did)
 
     ~Recon() {
         if (hstage) cudaFreeHost(hstage);
@@ -249,12 +250,16 @@ struct Recon {
     // ------------------------------------------------------------------
     void build(const mb_recon_desc *d);
     void build_hx_tables(const mb_recon_desc *d);
-    void build_pad();
+    void build_pad(int min_kx = 1, int min_ky = 1);
     void set_pupil_rows(int rows);
     void rebuild_fdpcg_device();
     int autotune(int reps, float *ms_out);
     void pupil_rows(bool from_x, const float *xin, cudaStream_t s);
     void hxt_rows(const float *xin, float *out, double *dot_part, int do_l2, int k, cudaStream_t s);
+    // the arguments of those launches (also gathered by a ReconGroup)
+    PupilArgs pupil_args(bool from_x, const float *xin, int w0) const;
+    HxtArgs hxt_args(const float *xin, float *out, double *dot_part, int do_l2, int k) const;
+    int hxt_ni() const { return nb > 1 ? 2 : 1; }
     void build_wfs_tables(const mb_recon_desc *d);
     void build_fdpcg(const mb_fdpcg_desc *fd);
     void build_fit(const mb_fit_desc *f);
@@ -301,12 +306,27 @@ struct Recon {
     using XrMmulFn = std::function<bool(int)>;
     void enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulFn &Amul,
                     const MmulFn &Mmul, cudaStream_t s, const XrMmulFn &XrMmul = XrMmulFn());
+    // One CG solve taken apart at its operator applications, so that a
+    // ReconGroup can apply the operator of several reconstructors in one
+    // launch: after A x -> cg_init; after A p_k -> cg_post (true: done).
+    struct CgRun {
+        CgBufs B;
+        long n;
+        int nblk, iters;
+        MmulFn Mmul;
+        XrMmulFn XrMmul;
+        float *zp;
+    };
+    void cg_init(CgRun &c, int k, cudaStream_t s);
+    bool cg_post(CgRun &c, int k, cudaStream_t s);
+    CgRun solve_run(cudaStream_t s);  // the tomography CG (its preconditioner launched on s)
+    void op_rhs_gp(const float *g, cudaStream_t s);  // the first launch of op_rhs (gradient weighting)
     void op_fitR(const float *xin, float *out, cudaStream_t s);
     void op_fitL(const float *ain, float *out, double *dot_part, cudaStream_t s, int k = 0);
     void enqueue_fit(cudaStream_t s);
     void time_stages(int reps, float *ms, double *bytes, int *launches);
     void capture_graph();
-    cudaGraphExec_t capture(const std::function<void(cudaStream_t)> &body, long &nkernels);
+    void capture(const std::function<void(cudaStream_t)> &body, long &nkernels, cudaGraphExec_t &exec);
     void run_graph(cudaStream_t s);
 };
 
@@ -405,15 +425,17 @@ void Recon::build_hx_tables(const mb_recon_desc *d) {
 }
 
 // Fixed-width copies of the transposed x and y lists of every (WFS, layer),
-// padded with (index 0, weight 0) after the real entries, and the pupil-row
-// blocking of k_pupil_rows.
-void Recon::build_pad() {
+// padded with (index 0, weight 0) after the real entries (at least min_kx /
+// min_ky wide: a ReconGroup gives its members one width, and the padding
+// adds exact zeros), and the pupil-row blocking of k_pupil_rows.
+void Recon::build_pad(int min_kx, int min_ky) {
     maxnx = maxny = 0;
     for (int l = 0; l < nps; l++) {
         maxnx = std::max(maxnx, lay_h[l].nx);
         maxny = std::max(maxny, lay_h[l].ny);
     }
-    kx = ky = 1;
+    kx = std::max(1, min_kx);
+    ky = std::max(1, min_ky);
     for (int w = 0; w < nwfs; w++)
         for (int l = 0; l < nps; l++)
             for (int axis = 0; axis < 2; axis++) {
@@ -487,37 +509,73 @@ void Recon::set_pupil_rows(int rows) {
         MB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pupil_smem));
 }
 
+PupilArgs Recon::pupil_args(bool from_x, const float *xin, int w0) const {
+    return PupilArgs{xin,    grad.p, tt.p,   tbuf.p, hx.fwd.p, laytab, wfstab, pad(), w0,    nps, nwfs, nxp,
+                     nyp,    nxtot,  ngrad,  tw,     ncols,    prows,  from_x ? 0 : 1, act()};
+}
+
+// The k_pupil_rows instantiation for a subaperture/pupil ratio and layer count.
+using PupilKern = void (*)(const float *, const float *, const float *, float *, const AxisW *, LayerTab, WfsTab,
+                           PadIndex, int, int, int, int, int, long, long, long, int, int, int, const int *);
+static PupilKern pupil_kern(bool from_x, bool p2, bool few) {
+    return from_x ? (p2 ? (few ? k_pupil_rows<true, 2, 8> : k_pupil_rows<true, 2, 16>)
+                        : (few ? k_pupil_rows<true, 1, 8> : k_pupil_rows<true, 1, 16>))
+                  : (p2 ? (few ? k_pupil_rows<false, 2, 8> : k_pupil_rows<false, 2, 16>)
+                        : (few ? k_pupil_rows<false, 1, 8> : k_pupil_rows<false, 1, 16>));
+}
+using PupilGroupKern = void (*)(GroupTab<PupilArgs>);
+static PupilGroupKern pupil_group_kern(bool from_x, bool p2, bool few) {
+    return from_x ? (p2 ? (few ? k_pupil_rows_group<true, 2, 8> : k_pupil_rows_group<true, 2, 16>)
+                        : (few ? k_pupil_rows_group<true, 1, 8> : k_pupil_rows_group<true, 1, 16>))
+                  : (p2 ? (few ? k_pupil_rows_group<false, 2, 8> : k_pupil_rows_group<false, 2, 16>)
+                        : (few ? k_pupil_rows_group<false, 1, 8> : k_pupil_rows_group<false, 1, 16>));
+}
+
 // Launch k_pupil_rows over every WFS: one launch per run of consecutive WFS
 // with the same subaperture/pupil ratio.
 void Recon::pupil_rows(bool from_x, const float *xin, cudaStream_t s) {
     for (int w0 = 0; w0 < nwfs;) {
         int w1 = w0 + 1;
         while (w1 < nwfs && wfs_h[w1].pos == wfs_h[w0].pos) w1++;
-        const bool p2 = wfs_h[w0].pos == 2;
-        const bool few = nps <= 8;
-        auto kern = from_x ? (p2 ? (few ? k_pupil_rows<true, 2, 8> : k_pupil_rows<true, 2, 16>)
-                                 : (few ? k_pupil_rows<true, 1, 8> : k_pupil_rows<true, 1, 16>))
-                           : (p2 ? (few ? k_pupil_rows<false, 2, 8> : k_pupil_rows<false, 2, 16>)
-                                 : (few ? k_pupil_rows<false, 1, 8> : k_pupil_rows<false, 1, 16>));
-        launch(kern, dim3(ptiles, w1 - w0, nb), dim3(kThreads), pupil_smem, s, 
-            xin, grad.p, tt.p, tbuf.p, hx.fwd.p, laytab, wfstab, pad(), w0, nps, nwfs, nxp, nyp, nxtot, ngrad, tw,
-            ncols, prows, from_x ? 0 : 1, act());
+        const PupilArgs a = pupil_args(from_x, xin, w0);
+        launch(pupil_kern(from_x, wfs_h[w0].pos == 2, nps <= 8), dim3(ptiles, w1 - w0, nb), dim3(kThreads),
+               pupil_smem, s, a.x, a.grad, a.tt, a.t, a.tab, a.lt, a.wt, a.pi, a.wbase, a.nps, a.nwfs, a.nxp, a.nyp,
+               a.nxtot, a.ngrad, a.tw, a.ncols, a.rows, a.do_tt, a.act);
         w0 = w1;
     }
+}
+
+HxtArgs Recon::hxt_args(const float *xin, float *out, double *dot_part, int do_l2, int k) const {
+    return HxtArgs{tbuf.p, xin, out, dot_part, pad(), laytab, nps, nwfs, nyp, nxtot, tw, do_l2, scal(), k, nb, act()};
+}
+
+using HxtKern = void (*)(const float *, const float *, float *, double *, PadIndex, LayerTab, int, int, int, long,
+                         long, int, CgScal, int, int, const int *);
+static HxtKern hxt_kern(int ky, int ni) {
+    static const HxtKern tab1[kMaxPadY] = {k_hxt_rows<1, 1>, k_hxt_rows<2, 1>, k_hxt_rows<3, 1>, k_hxt_rows<4, 1>,
+                                           k_hxt_rows<5, 1>, k_hxt_rows<6, 1>, k_hxt_rows<7, 1>, k_hxt_rows<8, 1>};
+    static const HxtKern tab2[kMaxPadY] = {k_hxt_rows<1, 2>, k_hxt_rows<2, 2>, k_hxt_rows<3, 2>, k_hxt_rows<4, 2>,
+                                           k_hxt_rows<5, 2>, k_hxt_rows<6, 2>, k_hxt_rows<7, 2>, k_hxt_rows<8, 2>};
+    return ni == 2 ? tab2[ky - 1] : tab1[ky - 1];
+}
+using HxtGroupKern = void (*)(GroupTab<HxtArgs>);
+static HxtGroupKern hxt_group_kern(int ky, int ni) {
+    static const HxtGroupKern tab1[kMaxPadY] = {k_hxt_rows_group<1, 1>, k_hxt_rows_group<2, 1>, k_hxt_rows_group<3, 1>,
+                                                k_hxt_rows_group<4, 1>, k_hxt_rows_group<5, 1>, k_hxt_rows_group<6, 1>,
+                                                k_hxt_rows_group<7, 1>, k_hxt_rows_group<8, 1>};
+    static const HxtGroupKern tab2[kMaxPadY] = {k_hxt_rows_group<1, 2>, k_hxt_rows_group<2, 2>, k_hxt_rows_group<3, 2>,
+                                                k_hxt_rows_group<4, 2>, k_hxt_rows_group<5, 2>, k_hxt_rows_group<6, 2>,
+                                                k_hxt_rows_group<7, 2>, k_hxt_rows_group<8, 2>};
+    return ni == 2 ? tab2[ky - 1] : tab1[ky - 1];
 }
 
 // k_hxt_rows at the padded y-list width, two instances per thread when the
 // batch has more than one.
 void Recon::hxt_rows(const float *xin, float *out, double *dot_part, int do_l2, int k, cudaStream_t s) {
-    using K = void (*)(const float *, const float *, float *, double *, PadIndex, LayerTab, int, int, int,
-                       long, long, int, CgScal, int, int, const int *);
-    static const K tab1[kMaxPadY] = {k_hxt_rows<1, 1>, k_hxt_rows<2, 1>, k_hxt_rows<3, 1>, k_hxt_rows<4, 1>,
-                                     k_hxt_rows<5, 1>, k_hxt_rows<6, 1>, k_hxt_rows<7, 1>, k_hxt_rows<8, 1>};
-    static const K tab2[kMaxPadY] = {k_hxt_rows<1, 2>, k_hxt_rows<2, 2>, k_hxt_rows<3, 2>, k_hxt_rows<4, 2>,
-                                     k_hxt_rows<5, 2>, k_hxt_rows<6, 2>, k_hxt_rows<7, 2>, k_hxt_rows<8, 2>};
-    const int ni = nb > 1 ? 2 : 1;
-    launch(ni == 2 ? tab2[ky - 1] : tab1[ky - 1], dim3(nblk_x, (nb + ni - 1) / ni), dim3(kThreads), 0, s, tbuf.p,
-           xin, out, dot_part, pad(), laytab, nps, nwfs, nyp, nxtot, tw, do_l2, scal(), k, nb, act());
+    const int ni = hxt_ni();
+    const HxtArgs a = hxt_args(xin, out, dot_part, do_l2, k);
+    launch(hxt_kern(ky, ni), dim3(nblk_x, (nb + ni - 1) / ni), dim3(kThreads), 0, s, a.t, a.xin, a.out, a.dot_part,
+           a.pi, a.lt, a.nps, a.nwfs, a.nyp, a.nxtot, a.tw, a.do_l2, a.S, a.kit, a.nb, a.act);
 }
 
 void Recon::build_wfs_tables(const mb_recon_desc *d) {
@@ -1211,10 +1269,14 @@ void Recon::op_hx(const float *xin, cudaStream_t s) {
                                                          nxp, nyp, nxtot, nullptr, nullptr, act());
 }
 
-void Recon::op_rhs(const float *g, float *out, cudaStream_t s) {
-    // TomoR: x = Hx^T GP^T NEA^-1 (I - TT PTT) g   (recon_utils.c:397, tomo.cu:607)
+void Recon::op_rhs_gp(const float *g, cudaStream_t s) {
     launch(k_gp, dim3(nblk_tt, nwfs, nb), dim3(kThreads), 0, s, nullptr, g, grad.p, tt_part.p, wfs.p, nwfs,
                                                       nxp, np, ngrad, 1, tt.p, cnt_tt.p, act());
+}
+
+void Recon::op_rhs(const float *g, float *out, cudaStream_t s) {
+    // TomoR: x = Hx^T GP^T NEA^-1 (I - TT PTT) g   (recon_utils.c:397, tomo.cu:607)
+    op_rhs_gp(g, s);
     pupil_rows(false, nullptr, s);
     hxt_rows(nullptr, out, nullptr, 0, 0, s);
 }
@@ -1258,6 +1320,39 @@ bool Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k
     return false;
 }
 
+void Recon::cg_init(CgRun &c, int k, cudaStream_t s) {
+    // after Ap = A x: r = b - A x, b.b, z = M r, (r.z)_k, p = z
+    const CgBufs &B = c.B;
+    launch(k_cg_init_r, dim3(c.nblk, nb), dim3(kThreads), 0, s, B.rhs, B.Ap, B.r, B.bb, c.n, B.S, c.iters, act());
+    bool pdone = false;
+    if (c.Mmul) {
+        pdone = c.Mmul(B.r, B.z, B.rz, k, 1);
+    } else {
+        launch(k_dot_self, dim3(c.nblk, nb), dim3(kThreads), 0, s, B.r, B.rz, c.n, B.S, k, act());  // z aliases r
+    }
+    if (!pdone)
+        launch(k_cg_update_p, dim3(nblocks((c.n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, c.zp, c.n, B.S,
+               1, act());
+}
+
+bool Recon::cg_post(CgRun &c, int k, cudaStream_t s) {
+    // after Ap = A p_k (whose last block left alpha_k)
+    const CgBufs &B = c.B;
+    bool pdone;
+    if (c.XrMmul && k + 1 < c.iters) {
+        pdone = c.XrMmul(k);  // x, r update and preconditioner; beta_k (and p, when it says so)
+    } else {
+        launch(k_cg_update_xr, dim3(c.nblk, nb), dim3(kThreads), 0, s, B.x, B.r, B.p, B.Ap, B.rr, c.n, B.S, k,
+               c.iters, c.Mmul ? 0 : 1, act());
+        if (k + 1 == c.iters) return true;
+        pdone = c.Mmul ? c.Mmul(B.r, B.z, B.rz, k, 0) : false;  // beta_k (and p, when it says so)
+    }
+    if (!pdone)
+        launch(k_cg_update_p, dim3(nblocks((c.n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, c.zp, c.n, B.S,
+               0, act());
+    return false;
+}
+
 // (Preconditioned) CG with FP64 scalars, the schedule of lib/pcg.c:28: the
 // residual is recomputed from x every kCgRestart = 100 iterations as the
 // reference's CPU solver does (its GPU solver, cuda/pcg.cu:87, every 500),
@@ -1267,65 +1362,40 @@ bool Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k
 // together with the preconditioner.
 void Recon::enqueue_cg(const CgBufs &B, long n, int nblk, int iters, const AmulFn &Amul,
                        const MmulFn &Mmul, cudaStream_t s, const XrMmulFn &XrMmul) {
-    // r = b - A x ; b.b
+    CgRun c{B, n, nblk, iters, Mmul, XrMmul, Mmul ? B.z : B.r};
     Amul(B.x, B.Ap, nullptr, 0);
-    launch(k_cg_init_r, dim3(nblk, nb), dim3(kThreads), 0, s, B.rhs, B.Ap, B.r, B.bb, n, B.S, iters, act());
-    float *zp = B.r;
-    bool pdone = false;
-    if (Mmul) {
-        pdone = Mmul(B.r, B.z, B.rz, 0, 1);
-        zp = B.z;
-    } else {
-        launch(k_dot_self, dim3(nblk, nb), dim3(kThreads), 0, s, B.r, B.rz, n, B.S, 0, act());  // z aliases r
-    }
-    if (!pdone)
-        launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n, B.S, 1,
-               act());
+    cg_init(c, 0, s);
     for (int k = 0; k < iters; k++) {
         if (k > 0 && k % kCgRestart == 0) {
             // restart as lib/pcg.c:61 does every 100 iterations: r = b - A x,
             // z = M r, p = z, (r.z)_k afresh (the p of the previous step is dropped)
             Amul(B.x, B.Ap, nullptr, 0);
-            launch(k_cg_init_r, dim3(nblk, nb), dim3(kThreads), 0, s, B.rhs, B.Ap, B.r, B.bb, n, B.S, iters, act());
-            if (Mmul) {
-                pdone = Mmul(B.r, B.z, B.rz, k, 1);
-            } else {
-                launch(k_dot_self, dim3(nblk, nb), dim3(kThreads), 0, s, B.r, B.rz, n, B.S, k, act());
-                pdone = false;
-            }
-            if (!pdone)
-                launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n,
-                       B.S, 1, act());
+            cg_init(c, k, s);
         }
         Amul(B.p, B.Ap, B.pap, k);  // its last block leaves alpha_k
-        if (XrMmul && k + 1 < iters) {
-            pdone = XrMmul(k);  // x, r update and preconditioner; beta_k (and p, when it says so)
-        } else {
-            launch(k_cg_update_xr, dim3(nblk, nb), dim3(kThreads), 0, s, B.x, B.r, B.p, B.Ap, B.rr, n, B.S, k, iters,
-                                                              Mmul ? 0 : 1, act());
-            if (k + 1 == iters) break;
-            pdone = Mmul ? Mmul(B.r, B.z, B.rz, k, 0) : false;  // beta_k (and p, when it says so)
-        }
-        if (!pdone)
-            launch(k_cg_update_p, dim3(nblocks((n + kUpdP - 1) / kUpdP), nb), dim3(kThreads), 0, s, B.p, zp, n, B.S,
-                   0, act());
+        if (cg_post(c, k, s)) break;
     }
+}
+
+Recon::CgRun Recon::solve_run(cudaStream_t s) {
+    CgRun c{CgBufs{x.p, r.p, p.p, z.p, Ap.p, rhs.p, pap_part.p, rr_part.p, rz_part.p, bb_part.p, scal()},
+            nxtot, nblk_x, maxit, MmulFn(), XrMmulFn(), r.p};
+    if (precond) {
+        c.Mmul = [this, s](float *in, float *out, double *dot, int k, int init) {
+            return op_fdpcg(in, out, dot, s, k, init, true, nullptr, nullptr, nullptr, p.p);
+        };
+        c.XrMmul = [this, s](int k) { return op_fdpcg(r.p, z.p, rz_part.p, s, k, 0, true, x.p, p.p, Ap.p, p.p); };
+        c.zp = z.p;
+    }
+    return c;
 }
 
 // The whole per-step tomography: RHS, then (FD)PCG from the warm start in x.
 void Recon::enqueue_solve(cudaStream_t s) {
     op_rhs(gin.p, rhs.p, s);
-    CgBufs B{x.p, r.p, p.p, z.p, Ap.p, rhs.p, pap_part.p, rr_part.p, rz_part.p, bb_part.p, scal()};
+    CgRun c = solve_run(s);
     AmulFn A = [&](const float *in, float *out, double *dot, int k) { op_lhs(in, out, dot, s, k); };
-    MmulFn M;
-    XrMmulFn XM;
-    if (precond) {
-        M = [&](float *in, float *out, double *dot, int k, int init) {
-            return op_fdpcg(in, out, dot, s, k, init, true, nullptr, nullptr, nullptr, p.p);
-        };
-        XM = [&](int k) { return op_fdpcg(r.p, z.p, rz_part.p, s, k, 0, true, x.p, p.p, Ap.p, p.p); };
-    }
-    enqueue_cg(B, nxtot, nblk_x, maxit, A, M, s, XM);
+    enqueue_cg(c.B, c.n, c.nblk, c.iters, A, c.Mmul, s, c.XrMmul);
 }
 
 // y = M x - U (V'x) for all instances: one warp per row, NI instances per CTA.
@@ -1770,7 +1840,11 @@ int Recon::autotune(int reps, float *ms_out) {
     return best;
 }
 
-cudaGraphExec_t Recon::capture(const std::function<void(cudaStream_t)> &body, long &nkernels) {
+// Capture `body` into `exec`: an existing executable graph of the same shape
+// (a table update changes kernel arguments, not the launch sequence) is
+// updated in place, which costs a fraction of a new instantiation.
+static void capture_into(cudaStream_t stream, const std::function<void(cudaStream_t)> &body, long &nkernels,
+                         cudaGraphExec_t &exec) {
     cudaGraph_t g = nullptr;
     const long before = g_launches.load();
     MB_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -1784,31 +1858,40 @@ cudaGraphExec_t Recon::capture(const std::function<void(cudaStream_t)> &body, lo
     MB_CUDA_TRY(cudaStreamEndCapture(stream, &g));
     nkernels = g_launches.load() - before;
     g_launches -= nkernels;  // captured, not launched
-    cudaGraphExec_t ge = nullptr;
-    cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    if (exec) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(exec, g, &info) == cudaSuccess) {
+            cudaGraphDestroy(g);
+            return;
+        }
+        (void)cudaGetLastError();  // not updatable: instantiate anew
+        cudaGraphExecDestroy(exec);
+        exec = nullptr;
+    }
+    const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
+        exec = nullptr;
         set_error("cudaGraphInstantiate: %s", cudaGetErrorString(e));
         throw CudaError{MB_ECUDA};
     }
-    return ge;
+}
+
+void Recon::capture(const std::function<void(cudaStream_t)> &body, long &nkernels, cudaGraphExec_t &exec) {
+    capture_into(stream, body, nkernels, exec);
 }
 
 void Recon::capture_graph() {
-    for (cudaGraphExec_t *gp : {&graph, &graph_fit, &graph_step})
-        if (*gp) {
-            cudaGraphExecDestroy(*gp);
-            *gp = nullptr;
-        }
-    graph = capture([&](cudaStream_t s) { enqueue_solve(s); }, graph_kernels);
+    graph_version++;
+    capture([&](cudaStream_t s) { enqueue_solve(s); }, graph_kernels, graph);
     if (has_fit) {
-        graph_fit = capture([&](cudaStream_t s) { enqueue_fit(s); }, graph_fit_kernels);
-        graph_step = capture(
+        capture([&](cudaStream_t s) { enqueue_fit(s); }, graph_fit_kernels, graph_fit);
+        capture(
             [&](cudaStream_t s) {
                 enqueue_solve(s);
                 enqueue_fit(s);
             },
-            graph_step_kernels);
+            graph_step_kernels, graph_step);
     }
 }
 
@@ -1827,6 +1910,226 @@ void Recon::run_graph(cudaStream_t s) {
     MB_CUDA_TRY(cudaGraphLaunch(graph, s));
     count_launches(graph_kernels);
 }
+
+// ---------------------------------------------------------------------------
+// ReconGroup: reconstructors of different geometries (uneven instances)
+// stepped together in one graph.  The tomography operators -- the RHS and
+// every CG iteration's A p (k_pupil_rows: Hx, GP, NEA, GP^T, x half of Hx^T;
+// k_hxt_rows: y half of Hx^T, L2, p.Ap and alpha) -- are one launch for all
+// members (GroupTab: per-member arguments and block ranges); each member's
+// own CG vector updates, preconditioner and DM fit run between them on the
+// member's side stream, so those of different members overlap.  Every
+// member's arithmetic is that of its own step, so a member's result is the
+// same in the group as alone.  Members share the CG iteration count; their
+// padded list widths are made equal (the padding adds exact zeros).
+// ---------------------------------------------------------------------------
+struct ReconGroup {
+    std::vector<Recon *> m;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaStream_t> side;
+    cudaEvent_t fork_ev = nullptr;
+    std::vector<cudaEvent_t> join_ev;
+    cudaGraphExec_t graph = nullptr;
+    long graph_kernels = 0;
+    std::vector<long> versions;  // members' graph_version at the group's capture
+    int device = 0, maxit = 0;
+    size_t pupil_smem = 0;
+
+    ~ReconGroup() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (auto e : join_ev) cudaEventDestroy(e);
+        if (fork_ev) cudaEventDestroy(fork_ev);
+        for (auto q : side) cudaStreamDestroy(q);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void fork(cudaStream_t s) {
+        MB_CUDA_TRY(cudaEventRecord(fork_ev, s));
+        for (auto q : side) MB_CUDA_TRY(cudaStreamWaitEvent(q, fork_ev, 0));
+    }
+    void join(cudaStream_t s) {
+        for (size_t i = 0; i < m.size(); i++) {
+            MB_CUDA_TRY(cudaEventRecord(join_ev[i], side[i]));
+            MB_CUDA_TRY(cudaStreamWaitEvent(s, join_ev[i], 0));
+        }
+    }
+    // k_pupil_rows of the listed members in as few launches as their
+    // subaperture/pupil ratios and layer counts allow (one for the presets)
+    void pupil_rows(bool from_x, const std::vector<int> &who, const std::vector<const float *> &xin,
+                    cudaStream_t s) {
+        struct E {
+            PupilArgs a;
+            uint3 grid;
+            int key;
+            size_t smem;
+        };
+        std::vector<E> es;
+        for (int i : who) {
+            const Recon &R = *m[i];
+            for (int w0 = 0; w0 < R.nwfs;) {
+                int w1 = w0 + 1;
+                while (w1 < R.nwfs && R.wfs_h[w1].pos == R.wfs_h[w0].pos) w1++;
+                es.push_back(E{R.pupil_args(from_x, xin[i], w0),
+                               make_uint3((unsigned)R.ptiles, (unsigned)(w1 - w0), (unsigned)R.nb),
+                               (R.wfs_h[w0].pos == 2 ? 2 : 0) + (R.nps <= 8 ? 1 : 0), R.pupil_smem});
+                w0 = w1;
+            }
+        }
+        for (int key = 0; key < 4; key++) {
+            std::vector<const E *> b;
+            for (const E &e : es)
+                if (e.key == key) b.push_back(&e);
+            for (size_t c0 = 0; c0 < b.size(); c0 += kMaxGroup) {
+                GroupTab<PupilArgs> g{};
+                g.n = (int)std::min(b.size() - c0, (size_t)kMaxGroup);
+                g.start[0] = 0;
+                for (int e = 0; e < g.n; e++) {
+                    const E &x = *b[c0 + e];
+                    MB_REQUIRE(x.smem <= pupil_smem, "group: a member's pupil rows need %zu bytes of shared memory",
+                               x.smem);
+                    g.a[e] = x.a;
+                    g.grid[e] = x.grid;
+                    g.start[e + 1] = g.start[e] + x.grid.x * x.grid.y * x.grid.z;
+                }
+                launch(pupil_group_kern(from_x, key & 2, key & 1), dim3(g.start[g.n]), dim3(kThreads), pupil_smem, s,
+                       g);
+            }
+        }
+    }
+    void hxt_rows(const std::vector<int> &who, const std::vector<const float *> &xin, const std::vector<float *> &out,
+                  const std::vector<double *> &dot, int do_l2, int k, cudaStream_t s) {
+        int ni = 1;
+        for (int i : who) ni = std::max(ni, m[i]->hxt_ni());
+        for (int ky = 1; ky <= kMaxPadY; ky++) {
+            std::vector<int> b;
+            for (int i : who)
+                if (m[i]->ky == ky) b.push_back(i);
+            for (size_t c0 = 0; c0 < b.size(); c0 += kMaxGroup) {
+                GroupTab<HxtArgs> g{};
+                g.n = (int)std::min(b.size() - c0, (size_t)kMaxGroup);
+                g.start[0] = 0;
+                for (int e = 0; e < g.n; e++) {
+                    const int i = b[c0 + e];
+                    const Recon &R = *m[i];
+                    g.a[e] = R.hxt_args(xin[i], out[i], dot[i], do_l2, k);
+                    g.grid[e] = make_uint3((unsigned)R.nblk_x, (unsigned)((R.nb + ni - 1) / ni), 1u);
+                    g.start[e + 1] = g.start[e] + g.grid[e].x * g.grid[e].y;
+                }
+                launch(hxt_group_kern(ky, ni), dim3(g.start[g.n]), dim3(kThreads), 0, s, g);
+            }
+        }
+    }
+    // A p for every member (TomoL): grouped where the tip/tilt split allows
+    void lhs(const std::vector<const float *> &xin, const std::vector<float *> &out, const std::vector<double *> &dot,
+             int k, cudaStream_t s) {
+        std::vector<int> who;
+        for (int i = 0; i < (int)m.size(); i++) {
+            if (m[i]->split) who.push_back(i);
+            else m[i]->op_lhs(xin[i], out[i], dot[i], s, k);
+        }
+        if (who.empty()) return;
+        pupil_rows(true, who, xin, s);
+        hxt_rows(who, xin, out, dot, 1, k, s);
+    }
+    void enqueue(cudaStream_t s) {
+        const int n = (int)m.size();
+        std::vector<int> all(n);
+        for (int i = 0; i < n; i++) all[i] = i;
+        std::vector<const float *> none(n, nullptr), xs(n), ps(n);
+        std::vector<float *> rhs(n), Ap(n);
+        std::vector<double *> nod(n, nullptr), pap(n);
+        for (int i = 0; i < n; i++) {
+            xs[i] = m[i]->x.p;
+            ps[i] = m[i]->p.p;
+            rhs[i] = m[i]->rhs.p;
+            Ap[i] = m[i]->Ap.p;
+            pap[i] = m[i]->pap_part.p;
+        }
+        // RHS: gradient weighting per member, then the two operator halves for all
+        fork(s);
+        for (int i = 0; i < n; i++) m[i]->op_rhs_gp(m[i]->gin.p, side[i]);
+        join(s);
+        pupil_rows(false, all, none, s);
+        hxt_rows(all, none, rhs, nod, 0, 0, s);
+        // CG from the warm start, iteration by iteration
+        std::vector<Recon::CgRun> run;
+        for (int i = 0; i < n; i++) run.push_back(m[i]->solve_run(side[i]));
+        std::vector<bool> done(n, false);
+        lhs(xs, Ap, nod, 0, s);
+        fork(s);
+        for (int i = 0; i < n; i++) m[i]->cg_init(run[i], 0, side[i]);
+        join(s);
+        for (int k = 0; k < maxit; k++) {
+            if (k > 0 && k % kCgRestart == 0) {
+                lhs(xs, Ap, nod, 0, s);
+                fork(s);
+                for (int i = 0; i < n; i++) m[i]->cg_init(run[i], k, side[i]);
+                join(s);
+            }
+            lhs(ps, Ap, pap, k, s);
+            fork(s);
+            for (int i = 0; i < n; i++)
+                if (!done[i]) done[i] = m[i]->cg_post(run[i], k, side[i]);
+            join(s);
+        }
+        // DM fits, overlapping
+        fork(s);
+        for (int i = 0; i < n; i++)
+            if (m[i]->has_fit) m[i]->enqueue_fit(side[i]);
+        join(s);
+    }
+    void capture() {
+        // the grouped k_pupil_rows runs with the largest member's shared memory,
+        // taken now: a member's pupil-row blocking (autotune) may have changed
+        pupil_smem = 0;
+        for (Recon *r : m) pupil_smem = std::max(pupil_smem, r->pupil_smem);
+        for (bool fx : {false, true})
+            for (int key = 0; key < 4; key++)
+                MB_CUDA_TRY(cudaFuncSetAttribute(pupil_group_kern(fx, key & 2, key & 1),
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pupil_smem));
+        capture_into(stream, [&](cudaStream_t s) { enqueue(s); }, graph_kernels, graph);
+        versions.clear();
+        for (Recon *r : m) versions.push_back(r->graph_version);
+    }
+    void build() {
+        MB_REQUIRE(!m.empty(), "empty group");
+        device = m[0]->device;
+        maxit = m[0]->maxit;
+        int kx = 1, ky = 1;
+        for (Recon *r : m) {
+            MB_REQUIRE(r->device == device, "members on different devices (%d, %d)", device, r->device);
+            MB_REQUIRE(r->maxit == maxit, "members with different CG iteration counts (%d, %d)", maxit, r->maxit);
+            kx = std::max(kx, r->kx);
+            ky = std::max(ky, r->ky);
+        }
+        for (size_t i = 0; i < m.size(); i++)
+            for (size_t j = 0; j < i; j++) MB_REQUIRE(m[i] != m[j], "a reconstructor appears twice in the group");
+        MB_CUDA_TRY(cudaSetDevice(device));
+        // one list width for all members (their own graphs are recaptured)
+        for (Recon *r : m)
+            if (r->kx != kx || r->ky != ky) {
+                const int rows = r->prows;
+                r->build_pad(kx, ky);
+                r->set_pupil_rows(rows);
+                r->capture_graph();
+            }
+        MB_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        MB_CUDA_TRY(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+        for (size_t i = 0; i < m.size(); i++) {
+            cudaStream_t q;
+            MB_CUDA_TRY(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+            side.push_back(q);
+            cudaEvent_t e;
+            MB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            join_ev.push_back(e);
+        }
+        capture();
+    }
+    bool stale() const {
+        for (size_t i = 0; i < m.size(); i++)
+            if (m[i]->graph_version != versions[i]) return true;
+        return false;
+    }
+};
 
 }  // namespace mb
 
@@ -2119,6 +2422,58 @@ int mb_recon_step_device(mb_recon *h, const float *d_grad, void *stream) {
     mb::count_launches(R.graph_step_kernels);
     MB_API_END
 }
+
+struct mb_group {
+    mb::ReconGroup G;
+};
+
+int mb_group_create(mb_recon *const *members, int n, mb_group **out) {
+    if (!out) {
+        mb::set_error("out is NULL");
+        return MB_EINVAL;
+    }
+    *out = nullptr;
+    MB_API_BEGIN
+    MB_REQUIRE(members && n >= 1, "no members");
+    auto *g = new mb_group();
+    try {
+        for (int i = 0; i < n; i++) {
+            MB_REQUIRE(members[i], "member %d is NULL", i);
+            g->G.m.push_back(&members[i]->R);
+        }
+        g->G.build();
+    } catch (...) {
+        delete g;
+        throw;
+    }
+    *out = g;
+    MB_API_END
+}
+
+int mb_group_step_device(mb_group *g, const float *const *d_grad, void *stream) {
+    MB_API_BEGIN
+    MB_REQUIRE(g && d_grad, "invalid arguments");
+    mb::ReconGroup &G = g->G;
+    for (size_t i = 0; i < G.m.size(); i++) {
+        MB_REQUIRE(d_grad[i], "gradients of member %zu are NULL", i);
+        MB_REQUIRE(G.m[i]->has_fit, "member %zu was set up without a DM fit", i);
+    }
+    if (G.stale()) G.capture();  // a member's tables changed (update, autotune)
+    cudaStream_t s = (cudaStream_t)stream;
+    for (size_t i = 0; i < G.m.size(); i++) {
+        mb::Recon &R = *G.m[i];
+        MB_CUDA_TRY(cudaMemcpyAsync(R.gin.p, d_grad[i], (size_t)R.nb * R.ngrad * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, s));
+        R.set_mask(nullptr, s);
+    }
+    MB_CUDA_TRY(cudaGraphLaunch(G.graph, s));
+    mb::count_launches(G.graph_kernels);
+    MB_API_END
+}
+
+long mb_group_graph_kernels(const mb_group *g) { return g ? g->G.graph_kernels : -1; }
+
+void mb_group_free(mb_group *g) { delete g; }
 
 int mb_apply_fit_R(mb_recon *h, const double *xin, double *aout) {
     MB_API_BEGIN

@@ -418,23 +418,62 @@ __host__ __device__ constexpr int pupil_rows_smem_floats(int rows, int nxp, int 
 // for the pupil-grid stages and whole layer columns for the x half of Hx^T,
 // so per-item index arithmetic is a few adds; index tables are staged in
 // shared memory and a pupil point's layer taps are issued together.
+// Grouped launches: one grid over the blocks of several reconstructors of
+// different geometries (uneven instances advanced by one launch of an
+// operator).  Entry e covers flat blocks [start[e], start[e+1]) with its own
+// grid shape and its own arguments (tables, vectors, sizes); a block finds
+// its entry and runs the operator's body with the entry's block index.
+constexpr int kMaxGroup = 8;
+template <class A>
+struct GroupTab {
+    int n;
+    unsigned start[kMaxGroup + 1];
+    uint3 grid[kMaxGroup];
+    A a[kMaxGroup];
+};
+template <class A>
+__device__ __forceinline__ int group_entry(const GroupTab<A> &g, uint3 &bid) {
+    int e = 0;
+    while (e + 1 < g.n && blockIdx.x >= g.start[e + 1]) e++;
+    const unsigned l = blockIdx.x - g.start[e];
+    const uint3 d = g.grid[e];
+    bid = make_uint3(l % d.x, (l / d.x) % d.y, l / (d.x * d.y));
+    return e;
+}
+
+// Arguments of one k_pupil_rows launch.
+struct PupilArgs {
+    const float *x, *grad, *tt;
+    float *t;
+    const AxisW *tab;
+    LayerTab lt;
+    WfsTab wt;
+    PadIndex pi;
+    int wbase, nps, nwfs, nxp, nyp;
+    long nxtot, ngrad, tw;
+    int ncols, rows, do_tt;
+    const int *act;
+};
+
+// The body takes its block index as `bid` (blockIdx, or a block of one
+// member of a grouped launch, k_pupil_rows_group).
 template <bool FROM_X, int POS, int ML>
-__global__ void __launch_bounds__(kThreads, 4)
-k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const float *__restrict__ tt,
-             float *__restrict__ t, const AxisW *__restrict__ tab, const __grid_constant__ LayerTab lt,
-             const __grid_constant__ WfsTab wt, PadIndex pi, int wbase, int nps, int nwfs, int nxp, int nyp,
-             long nxtot, long ngrad, long tw, int ncols, int rows, int do_tt,
-             const int *__restrict__ act) {
+__device__ __forceinline__ void
+pupil_rows_body(const uint3 bid, const float *__restrict__ x, const float *__restrict__ grad,
+                const float *__restrict__ tt, float *__restrict__ t, const AxisW *__restrict__ tab,
+                const LayerTab &lt, const WfsTab &wt, const PadIndex &pi, int wbase, int nps, int nwfs, int nxp,
+                int nyp, long nxtot, long ngrad, long tw, int ncols, int rows, int do_tt,
+                const int *__restrict__ act) {
     pdl_enter();
     constexpr int N1 = POS + 1;
-    const int w = wbase + blockIdx.y, b = blockIdx.z;
+    const int w = wbase + bid.y, b = bid.z;
     if (inactive(act, b)) return;
     extern __shared__ float sm[];
     __shared__ int s_lnx[kMaxLayers], s_tcol[kMaxLayers + 1];
     __shared__ long s_loff[kMaxLayers];
     __shared__ int4 s_fp[kMaxLayers];
     const WfsDev &W = wt.w[w];
-    const int r0 = blockIdx.x * rows;
+    const int r0 = bid.x * rows;
     const int r1 = min(nyp, r0 + rows);      // output pupil rows [r0, r1)
     const int ca = max(0, r0 - POS);         // subaperture corner rows [ca, cb)
     const int cb = min(nyp - POS, r1);
@@ -581,20 +620,41 @@ k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const 
     }
 }
 
+template <bool FROM_X, int POS, int ML>
+__global__ void __launch_bounds__(kThreads, 4)
+k_pupil_rows(const float *__restrict__ x, const float *__restrict__ grad, const float *__restrict__ tt,
+             float *__restrict__ t, const AxisW *__restrict__ tab, const __grid_constant__ LayerTab lt,
+             const __grid_constant__ WfsTab wt, PadIndex pi, int wbase, int nps, int nwfs, int nxp, int nyp,
+             long nxtot, long ngrad, long tw, int ncols, int rows, int do_tt,
+             const int *__restrict__ act) {
+    pupil_rows_body<FROM_X, POS, ML>(blockIdx, x, grad, tt, t, tab, lt, wt, pi, wbase, nps, nwfs, nxp, nyp, nxtot,
+                                     ngrad, tw, ncols, rows, do_tt, act);
+}
+// grid: (sum of the entries' blocks); dynamic shared memory: the largest entry's.
+template <bool FROM_X, int POS, int ML>
+__global__ void __launch_bounds__(kThreads, 4)
+k_pupil_rows_group(const __grid_constant__ GroupTab<PupilArgs> g) {
+    uint3 bid;
+    const PupilArgs &a = g.a[group_entry(g, bid)];
+    pupil_rows_body<FROM_X, POS, ML>(bid, a.x, a.grad, a.tt, a.t, a.tab, a.lt, a.wt, a.pi, a.wbase, a.nps, a.nwfs,
+                                     a.nxp, a.nyp, a.nxtot, a.ngrad, a.tw, a.ncols, a.rows, a.do_tt, a.act);
+}
+
 // y half of Hx^T over all WFS, + L2^T L2 x and p.Ap partials (last block:
 // alpha).  One thread per layer point and NI instances (the index work, the
 // footprint tests and the list entries are shared by the instances, and each
 // dependent step issues NI times the independent loads; the NI block sums
 // and last-block arrivals are taken together);
 // grid: (ceil(nxtot/256), ceil(nb/NI)).  KY is the padded y-list width.
+// The body takes its block index `bid` and the x extent of its grid `gx`.
 template <int KY, int NI>
-__global__ void __launch_bounds__(kThreads)
-k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__restrict__ out,
-           double *__restrict__ dot_part, PadIndex pi, const __grid_constant__ LayerTab lt, int nps,
-           int nwfs, int nyp, long nxtot, long tw, int do_l2, CgScal S, int kit, int nb,
-           const int *__restrict__ act) {
+__device__ __forceinline__ void
+hxt_rows_body(const uint3 bid, const unsigned gx, const float *__restrict__ t, const float *__restrict__ xin,
+              float *__restrict__ out, double *__restrict__ dot_part, const PadIndex &pi, const LayerTab &lt,
+              int nps, int nwfs, int nyp, long nxtot, long tw, int do_l2, const CgScal &S, int kit, int nb,
+              const int *__restrict__ act) {
     pdl_enter();
-    const int b0 = blockIdx.y * NI;
+    const int b0 = bid.y * NI;
     bool on[NI];
     bool any = false;
 #pragma unroll
@@ -605,7 +665,7 @@ k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__
     if (!any) return;
     __shared__ double shq[NI][32];
     __shared__ bool s_last[NI];
-    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long j = (long)bid.x * blockDim.x + threadIdx.x;
     double dotv[NI];
 #pragma unroll
     for (int q = 0; q < NI; q++) dotv[q] = 0;
@@ -712,20 +772,20 @@ k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__
             for (int q = 0; q < NI; q++) {
                 double v = lane < (int)(blockDim.x >> 5) ? shq[q][lane] : 0.0;
                 v = warp_sum(v);
-                if (lane == 0 && on[q]) dot_part[(size_t)(b0 + q) * gridDim.x + blockIdx.x] = v;
+                if (lane == 0 && on[q]) dot_part[(size_t)(b0 + q) * gx + bid.x] = v;
             }
         // last block per instance: alpha_k = (r.z)_k / (p.Ap) (cg_alpha_last, NI counters at once)
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0)
 #pragma unroll
-            for (int q = 0; q < NI; q++) s_last[q] = on[q] && atomicAdd(S.cnt + b0 + q, 1u) == gridDim.x - 1;
+            for (int q = 0; q < NI; q++) s_last[q] = on[q] && atomicAdd(S.cnt + b0 + q, 1u) == gx - 1;
         __syncthreads();
 #pragma unroll
         for (int q = 0; q < NI; q++) {
             if (!s_last[q] || threadIdx.x >= 32) continue;
             const int b = b0 + q;
-            const double pap = warp_sum_fresh(dot_part + (size_t)b * gridDim.x, gridDim.x);
+            const double pap = warp_sum_fresh(dot_part + (size_t)b * gx, gx);
             if (threadIdx.x == 0) {
                 double a = S.sc[(size_t)b * S.nsc + kit] / pap;
                 if (!isfinite(a)) a = 0;  // pcg.c:80-83, pcg.cu:27-30
@@ -734,6 +794,39 @@ k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__
             }
         }
     }
+}
+
+template <int KY, int NI>
+__global__ void __launch_bounds__(kThreads)
+k_hxt_rows(const float *__restrict__ t, const float *__restrict__ xin, float *__restrict__ out,
+           double *__restrict__ dot_part, PadIndex pi, const __grid_constant__ LayerTab lt, int nps,
+           int nwfs, int nyp, long nxtot, long tw, int do_l2, CgScal S, int kit, int nb,
+           const int *__restrict__ act) {
+    hxt_rows_body<KY, NI>(blockIdx, gridDim.x, t, xin, out, dot_part, pi, lt, nps, nwfs, nyp, nxtot, tw, do_l2, S,
+                          kit, nb, act);
+}
+// Arguments of one k_hxt_rows launch.
+struct HxtArgs {
+    const float *t, *xin;
+    float *out;
+    double *dot_part;
+    PadIndex pi;
+    LayerTab lt;
+    int nps, nwfs, nyp;
+    long nxtot, tw;
+    int do_l2;
+    CgScal S;
+    int kit, nb;
+    const int *act;
+};
+template <int KY, int NI>
+__global__ void __launch_bounds__(kThreads)
+k_hxt_rows_group(const __grid_constant__ GroupTab<HxtArgs> g) {
+    uint3 bid;
+    const int e = group_entry(g, bid);
+    const HxtArgs &a = g.a[e];
+    hxt_rows_body<KY, NI>(bid, g.grid[e].x, a.t, a.xin, a.out, a.dot_part, a.pi, a.lt, a.nps, a.nwfs, a.nyp, a.nxtot,
+                          a.tw, a.do_l2, a.S, a.kit, a.nb, a.act);
 }
 
 // ---------------------------------------------------------------------------

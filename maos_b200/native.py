@@ -109,6 +109,10 @@ SIGNATURES = {
     "mb_tomo_wfs": (C.c_int, [C.c_void_p, C.POINTER(_D), C.POINTER(_D), _F]),
     "mb_fit_opdr": (C.c_int, [C.c_void_p, C.POINTER(_D), _D, _F]),
     "mb_recon_step_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mb_group_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
+    "mb_group_step_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p]),
+    "mb_group_graph_kernels": (C.c_long, [C.c_void_p]),
+    "mb_group_free": (None, [C.c_void_p]),
     "mb_fit_solution": (C.c_void_p, [C.c_void_p]),
     "mb_nact": (C.c_long, [C.c_void_p]),
     "mb_apply_fit_R": (C.c_int, [C.c_void_p, _D, _D]),

@@ -401,3 +401,42 @@ class Reconstructor:
         out = np.empty((self.nbatch, len(self.sys.wfs), np_))
         check(self.lib.mb_apply_hx(self.h, _dptr(xi), _dptr(out)), "mb_apply_hx")
         return out
+
+
+class ReconGroup:
+    """Reconstructors of different geometries stepped together
+    (mb_group_*): one graph per step, the tomography operators launched once
+    for all members' instances, each member's CG updates, preconditioner and
+    fit in between.  Members stay owned by the caller and must outlive the
+    group; each member's result equals its own step's."""
+
+    def __init__(self, members):
+        self.members = list(members)
+        self.lib = self.members[0].lib
+        hs = (C.c_void_p * len(self.members))(*[r.h for r in self.members])
+        h = C.c_void_p()
+        check(self.lib.mb_group_create(hs, len(self.members), C.byref(h)), "mb_group_create")
+        self.h = h
+
+    @property
+    def graph_kernels(self) -> int:
+        """Kernel launches of one group step."""
+        return int(self.lib.mb_group_graph_kernels(self.h))
+
+    def step_device(self, d_grad_ptrs, stream_ptr: int = 0):
+        """One step of every member: d_grad_ptrs[i] points to member i's FP32
+        gradients [nbatch_i, ngrad_i] on the device; the commands stay in each
+        member's fit_solution()."""
+        ptrs = (C.c_void_p * len(self.members))(*[C.c_void_p(int(p)) for p in d_grad_ptrs])
+        check(self.lib.mb_group_step_device(self.h, ptrs, C.c_void_p(stream_ptr)), "mb_group_step_device")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mb_group_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
