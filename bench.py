@@ -639,6 +639,8 @@ def run_gpu(args):
     R = Reconstructor(sysm, nbatch=B, device=local, fit=fit)
     # the pupil-row blocking of the LHS kernel, measured for this batch (outside the timed region)
     tuned_rows, tuned_ms = R.autotune(reps=20)
+    tuned_fd = {"fdpcg_form": R.fdpcg_mode(-1), "fdpcg_block_solve_instances_per_cta": R.fdpcg_shape()} \
+        if sysm.fdpcg is not None else {}
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -804,7 +806,7 @@ def run_gpu(args):
                            "instances_per_gpu": B, "ngrad": int(sysm.ngrad), "nact": int(fit.nact),
                            "nxtot": int(sysm.nx_total), "l2": "flushed before every step (256 MiB write)",
                            "parallelism": f"replicas x{world}",
-                           "autotune": {"pupil_rows": tuned_rows,
+                           "autotune": {"pupil_rows": tuned_rows, **tuned_fd,
                                         "lhs_ms_by_rows": {str(k): round(v, 4) for k, v in tuned_ms.items()}}},
                 "latency_ms": {"p50": p50, "p99": p99, "note": "one batched step of all instances"},
                 "single_instance": single,

@@ -313,7 +313,8 @@ int mb_recon_serve_step(mb_recon *r, const int *active, const float *grad, float
  * 16 pupil rows per CTA, and every even split of the pupil rows into blocks
  * of 4 to 32 rows) on this batch size, keeps the fastest, then times whole
  * tomography steps with each form of the FDPCG preconditioner
- * (mb_fdpcg_mode) and keeps the faster, and captures the step graphs again;
+ * (mb_fdpcg_mode; the three-kernel form at each batch shape of
+ * mb_fdpcg_shape) and keeps the fastest, and captures the step graphs again;
  * the instances restart cold.  The row blocking does not change results, the
  * preconditioner's form changes them only at FP32 rounding.  rows (may be
  * NULL): the blocking kept; ms (may be NULL, 3 floats): ms per operator for
@@ -330,6 +331,13 @@ int mb_autotune(mb_recon *r, int reps, int *rows, float *ms);
  * (query).  Results agree to FP32 rounding.  The step graphs are captured
  * again.  Returns the form in use (1 or 2) or a negative MB_E* code. */
 int mb_fdpcg_mode(mb_recon *r, int mode);
+
+/* Batch shape of the three-kernel FDPCG form (no counterpart in the
+ * reference): instances per CTA of the block solve, 2, 4, 8 or 16 (more read
+ * the shared block matrices fewer times, fewer give more CTAs), -1 = query.
+ * Results do not depend on it.  The step graphs are captured again.  Returns
+ * the shape in use or a negative MB_E* code. */
+int mb_fdpcg_shape(mb_recon *r, int ni);
 
 /* Servo filter on the device (no GPU counterpart in the reference; the CPU
  * code is lib/servo.c servo_new / servo_filter / servo_reset, used by

@@ -278,6 +278,8 @@ struct Recon {
     // one cluster of fused_tab.C CTAs; fd_mode 1 = three kernels, 2 = fused
     bool fd_fused_ok = false;
     int fd_mode = 1;
+    int fd_mul_ni = kFdInst;  // instances per k_fd_mul CTA (the form-1 batch shape)
+    void fd_mul(cudaStream_t s);
     FdFusedTab fused_tab{};
     DevBuf<FdMem> fd_mem;
     size_t fd_fsmem = 0;
@@ -1294,6 +1296,17 @@ void Recon::op_lhs(const float *xin, float *out, double *dot_part, cudaStream_t 
     hxt_rows(xin, out, dot_part, 1, k, s);
 }
 
+// The block solve of every (half-spectrum block, instance), fd_mul_ni
+// instances per CTA.
+void Recon::fd_mul(cudaStream_t s) {
+    using K = void (*)(const cplx *, cplx *, const cplx *, const FdIndex *, int, int, int, const int *);
+    const K k = fd_mul_ni == 2 ? k_fd_mul<2> : fd_mul_ni == 4 ? k_fd_mul<4> : fd_mul_ni == 16 ? k_fd_mul<16>
+                                                                                            : k_fd_mul<8>;
+    const int per = kThreads / fd_bs;
+    launch(k, dim3((fd_nbh + per - 1) / per, (nb + fd_mul_ni - 1) / fd_mul_ni), dim3(kThreads), 0, s, spec.p, spec2.p,
+           fd_M.p, fd_idx.p, fd_nbh, fd_bs, nb, act());
+}
+
 bool Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k, int init, bool in_cg,
                      float *xupd, const float *pupd, const float *Apupd, float *pnext) {
     // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT,
@@ -1306,9 +1319,7 @@ bool Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k
     }
     launch(k_fd_fwd, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, rin, spec.p, fdtab, fd_tw.p, nxtot, fd_bufn, xupd,
                                                         pupd, Apupd, xupd ? ab.p : nullptr, act());
-    const int per = kThreads / fd_bs;
-    launch(k_fd_mul, dim3((fd_nbh + per - 1) / per, (nb + kFdInst - 1) / kFdInst), dim3(kThreads), 0, s, 
-        spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh, fd_bs, nb, act());
+    fd_mul(s);
     CgScal S = in_cg ? scal() : CgScal{};
     if (in_cg && pnext && fd_cluster) {  // the p update inside, clusters of the layer CTAs
         launch_cluster(k_fd_inv<true>, dim3(nps, nb), dim3(kFftThreads), fd_smem, s, nps, spec2.p, rin, zout, rzp,
@@ -1743,10 +1754,7 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                     launch(k_fd_fwd, dim3(nps, nb), dim3(kFftThreads), fd_smem, stream, rhs.p, spec.p, fdtab,
                            fd_tw.p, nxtot, fd_bufn, z.p, p.p, Ap.p, ab.p, act());
                     break;
-                case 5:
-                    launch(k_fd_mul, dim3((fd_nbh + per - 1) / per, (nb + kFdInst - 1) / kFdInst), dim3(kThreads),
-                           0, stream, spec.p, spec2.p, fd_M.p, fd_idx.p, fd_nbh, fd_bs, nb, act());
-                    break;
+                case 5: fd_mul(stream); break;
                 case 7:  // fused: scratch vectors (rhs as r, z as x, Ap, rhs as p)
                     launch_cluster(k_fd_fused, dim3(fused_tab.C, nb), dim3(kFftThreads), fd_fsmem, stream,
                                    fused_tab.C, rhs.p, fdtab, fused_tab, fd_tw.p, fd_M.p, fd_mem.p, fd_bs, nxtot,
@@ -1817,19 +1825,39 @@ int Recon::autotune(int reps, float *ms_out) {
     capture_graph();
     // the preconditioner's form: three kernels, or one fused cluster kernel,
     // timed as whole tomography steps (graph launches)
-    if (precond && fd_fused_ok) {
-        float tmode[3] = {0, 0, 0};
-        for (int mode = 1; mode <= 2; mode++) {
-            set_fdpcg_mode(mode);
+    if (precond) {
+        // the three-kernel form with 2, 4, 8 or 16 instances per block-solve
+        // CTA (the batch shape; shapes above twice the batch are skipped),
+        // and the fused form when its cluster fits
+        auto time_graph = [&]() {
             MB_CUDA_TRY(cudaGraphLaunch(graph, stream));  // warm
             MB_CUDA_TRY(cudaEventRecord(e0, stream));
             const int nrep = std::max(2, reps / 4);
             for (int i = 0; i < nrep; i++) MB_CUDA_TRY(cudaGraphLaunch(graph, stream));
             MB_CUDA_TRY(cudaEventRecord(e1, stream));
             MB_CUDA_TRY(cudaEventSynchronize(e1));
-            MB_CUDA_TRY(cudaEventElapsedTime(&tmode[mode], e0, e1));
+            float t = 0;
+            MB_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+            return t;
+        };
+        int best_ni = fd_mul_ni, best_mode = 1;
+        float tb = 1e30f;
+        for (int ni : {2, 4, 8, 16}) {
+            if (ni > 2 * nb && ni != 2) continue;
+            fd_mul_ni = ni;
+            set_fdpcg_mode(1);  // recaptures
+            const float t = time_graph();
+            if (t < tb) {
+                tb = t;
+                best_ni = ni;
+            }
         }
-        set_fdpcg_mode(tmode[2] < tmode[1] ? 2 : 1);
+        fd_mul_ni = best_ni;
+        if (fd_fused_ok) {
+            set_fdpcg_mode(2);
+            if (time_graph() < tb) best_mode = 2;
+        }
+        set_fdpcg_mode(best_mode);
         // the timing steps moved the warm start: start the instances cold again
         x.zero_async(stream);
         if (has_fit) fa.zero_async(stream);
@@ -1934,6 +1962,7 @@ struct ReconGroup {
     std::vector<long> versions;  // members' graph_version at the group's capture
     int device = 0, maxit = 0;
     size_t pupil_smem = 0;
+    std::vector<int> order;  // members by decreasing work per grouped launch
 
     ~ReconGroup() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -2022,7 +2051,7 @@ struct ReconGroup {
     void lhs(const std::vector<const float *> &xin, const std::vector<float *> &out, const std::vector<double *> &dot,
              int k, cudaStream_t s) {
         std::vector<int> who;
-        for (int i = 0; i < (int)m.size(); i++) {
+        for (int i : order) {
             if (m[i]->split) who.push_back(i);
             else m[i]->op_lhs(xin[i], out[i], dot[i], s, k);
         }
@@ -2032,8 +2061,7 @@ struct ReconGroup {
     }
     void enqueue(cudaStream_t s) {
         const int n = (int)m.size();
-        std::vector<int> all(n);
-        for (int i = 0; i < n; i++) all[i] = i;
+        const std::vector<int> &all = order;
         std::vector<const float *> none(n, nullptr), xs(n), ps(n);
         std::vector<float *> rhs(n), Ap(n);
         std::vector<double *> nod(n, nullptr), pap(n);
@@ -2103,6 +2131,13 @@ struct ReconGroup {
         }
         for (size_t i = 0; i < m.size(); i++)
             for (size_t j = 0; j < i; j++) MB_REQUIRE(m[i] != m[j], "a reconstructor appears twice in the group");
+        // grouped launches list the member with the most unknowns first, so
+        // its blocks (the longest chains) are scheduled first
+        order.resize(m.size());
+        for (size_t i = 0; i < m.size(); i++) order[i] = (int)i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return (long)m[a]->nb * m[a]->nxtot > (long)m[b]->nb * m[b]->nxtot;
+        });
         MB_CUDA_TRY(cudaSetDevice(device));
         // one list width for all members (their own graphs are recaptured)
         for (Recon *r : m)
@@ -2520,6 +2555,19 @@ int mb_fdpcg_mode(mb_recon *h, int mode) {
     MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
     R.set_fdpcg_mode(mode);
     return R.fd_mode;
+    MB_API_END
+}
+
+int mb_fdpcg_shape(mb_recon *h, int ni) {
+    MB_API_BEGIN
+    MB_REQUIRE(h && (ni == -1 || ni == 2 || ni == 4 || ni == 8 || ni == 16), "invalid arguments");
+    mb::Recon &R = h->R;
+    MB_REQUIRE(R.precond, "reconstructor has no FDPCG preconditioner");
+    if (ni < 0) return R.fd_mul_ni;
+    MB_CUDA_TRY(cudaStreamSynchronize(R.stream));
+    R.fd_mul_ni = ni;
+    if (R.graph) R.capture_graph();
+    return R.fd_mul_ni;
     MB_API_END
 }
 

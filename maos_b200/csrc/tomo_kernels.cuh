@@ -1408,14 +1408,17 @@ k_fd_fwd(float *__restrict__ r, cplx *__restrict__ H, const __grid_constant__ Fd
 // Per-frequency block solve on the blocks of the non-positive x frequencies
 // (the leading blocks of the reference's ordering, which reach every stored
 // bin): Y_i = sum_j M[blk][j*bs+i] X_j.  A CTA takes floor(256/bs) whole
-// blocks and up to kFdInst instances: a thread keeps its row of M in
+// blocks and up to NI instances: a thread keeps its row of M in
 // registers for all of them, gathers its own member X_i of every instance
 // at once (one round trip, not one per instance), stages them in shared
 // memory, then forms its row of each instance from the block's members.
-// grid: (ceil(nblk / floor(256/bs)), ceil(nbatch / kFdInst))
-constexpr int kFdInst = 8;
+// NI (2, 4, 8 or 16) is the batch shape mb_autotune picks: more instances
+// per CTA read M fewer times, fewer give more CTAs.
+// grid: (ceil(nblk / floor(256/bs)), ceil(nbatch / NI))
+constexpr int kFdInst = 8;  // default instances per CTA
 constexpr int kMaxBs = 16;
 
+template <int kFdInst>
 __global__ void __launch_bounds__(kThreads)
 k_fd_mul(const cplx *__restrict__ X, cplx *__restrict__ Y, const cplx *__restrict__ M,
          const FdIndex *__restrict__ idx, int nblk, int bs, int nbatch, const int *__restrict__ act) {

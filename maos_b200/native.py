@@ -104,6 +104,7 @@ SIGNATURES = {
     "mb_tomo_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mb_fit": (C.c_int, [C.c_void_p, _D, _F]),
     "mb_fdpcg_mode": (C.c_int, [C.c_void_p, C.c_int]),
+    "mb_fdpcg_shape": (C.c_int, [C.c_void_p, C.c_int]),
     "mb_update_recon_neam": (C.c_int, [C.c_void_p, _D]),
     "mb_fdpcg_data": (C.c_int, [C.c_void_p, _D]),
     "mb_tomo_wfs": (C.c_int, [C.c_void_p, C.POINTER(_D), C.POINTER(_D), _F]),

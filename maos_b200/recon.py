@@ -238,6 +238,14 @@ class Reconstructor:
             check(rc, "mb_fdpcg_mode")
         return rc
 
+    def fdpcg_shape(self, ni: int = -1) -> int:
+        """Instances per block-solve CTA of the three-kernel FDPCG form
+        (mb_fdpcg_shape): 2, 4, 8 or 16, -1 to query; returns the shape in use."""
+        rc = self.lib.mb_fdpcg_shape(self.h, int(ni))
+        if rc < 0:
+            check(rc, "mb_fdpcg_shape")
+        return rc
+
     def reset(self):
         check(self.lib.mb_recon_reset(self.h), "mb_recon_reset")
 

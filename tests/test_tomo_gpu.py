@@ -223,6 +223,28 @@ def test_autotune_keeps_results():
         R.close()
 
 
+def test_fdpcg_batch_shape_keeps_results():
+    """The three-kernel FDPCG form's batch shape (instances per block-solve
+    CTA, mb_fdpcg_shape, chosen by the autotuner) changes no bit of the
+    solution, at an instance count that leaves partial CTAs for most shapes."""
+    from conftest import get_system
+    from maos_b200.recon import Reconstructor
+    s = get_system("mcao_30m")
+    g = np.random.default_rng(19).standard_normal((5, s.ngrad)) * 1e-6
+    R = Reconstructor(s, nbatch=5)
+    try:
+        R.fdpcg_mode(1)
+        assert R.fdpcg_shape() == 8
+        x0, _ = R.tomo(g)
+        for ni in (2, 4, 16):
+            assert R.fdpcg_shape(ni) == ni
+            R.reset()
+            x1, _ = R.tomo(g)
+            assert np.array_equal(x0, x1), ni
+    finally:
+        R.close()
+
+
 def test_fused_preconditioner_matches_the_oracle(setup):
     """The fused FDPCG step (mb_fdpcg_mode 2: one cluster kernel per CG step,
     the layers split over its CTAs) solves to the oracle's tolerance, agrees
