@@ -529,10 +529,11 @@ def grouped_mix(nsteps: int = 30, warmup: int = 3):
             "group": grouped, "three_streams": pools}
 
 
-def served_mix(seconds: float, mcao_frames=None, mvm: bool = False):
+def served_mix(seconds: float, mcao_frames=None, mvm: bool = False, rate_scale: float = 1.0):
     """The served mix: 64 systems (26 8 m SCAO, 26 8 m LTAO, 12 30 m MCAO), each
-    sending Poisson requests at a rate drawn from U[500, 1000] Hz, all admitted,
-    warm state resident, newest frame wins when a system falls behind.
+    sending Poisson requests at a rate drawn from U[500, 1000] Hz (times
+    rate_scale), all admitted, warm state resident, newest frame wins when a
+    system falls behind.
     mvm: every type is served by the BF16 MVM of its control matrix (built on
     the GPU by batched solves) instead of the iterative reconstructor."""
     import numpy as np
@@ -552,7 +553,7 @@ def served_mix(seconds: float, mcao_frames=None, mvm: bool = False):
     systems = []
     for t, (name, n) in enumerate(SERVE_MIX):
         for _ in range(n):
-            systems.append((t, float(rng.uniform(500.0, 1000.0)), frames[t]))
+            systems.append((t, rate_scale * float(rng.uniform(500.0, 1000.0)), frames[t]))
     budget = sum(serve.slot_footprint_bytes(t) * t.capacity for t in types)
     build_s = None
     if mvm:
@@ -585,7 +586,7 @@ def served_mix(seconds: float, mcao_frames=None, mvm: bool = False):
     out = {"mix": " + ".join(f"{n} {name}" for name, n in SERVE_MIX),
            "path": "BF16 MVM of each type's control matrix" if mvm else "FDPCG/CG tomography + fit, FP32",
            "control_matrix_build_s": build_s,
-           "rate_hz": "U[500,1000] Poisson per system", "seconds": seconds,
+           "rate_hz": f"U[{500 * rate_scale:g},{1000 * rate_scale:g}] Poisson per system", "seconds": seconds,
            "policy": "one masked batch per pool in flight, newest frame wins",
            "hbm_budget_bytes": int(budget),
            "served_steps_per_s": len(done) / seconds, "offered_per_s": (len(done) + len(srv.dropped)) / seconds,
@@ -779,9 +780,11 @@ def run_gpu(args):
     if world == 1 and not args.no_serve:
         grouped = grouped_mix()
 
-    served = served_mvm = None
+    served = served_mvm = served_low = None
     if world == 1 and not args.no_serve and args.serve_seconds > 0:
         served = served_mix(args.serve_seconds, mcao_frames=fr[0])
+        # the same systems at a quarter of the rates, which one GPU sustains
+        served_low = served_mix(args.serve_seconds, mcao_frames=fr[0], rate_scale=0.25)
         served_mvm = served_mix(args.serve_seconds, mcao_frames=fr[0], mvm=True)
 
     cpu = None
@@ -820,6 +823,7 @@ def run_gpu(args):
                 "closed_loop": loop_line,
                 "grouped_mix": grouped,
                 "served": served,
+                "served_sustained_rate": served_low,
                 "served_mvm": served_mvm,
                 "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
                 "cpu_baseline": cpu}
