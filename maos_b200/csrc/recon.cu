@@ -949,15 +949,36 @@ void Recon::build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector
     fd_mode = 1;
     long nmin = LONG_MAX;
     for (int l = 0; l < nps; l++) nmin = std::min(nmin, (long)lay_h[l].nx * lay_h[l].ny);
+    // CTAs per layer proportional to its size, scaled up to as many as the
+    // cluster holds (kMaxFdParts, or MAOS_B200_FD_CTAS, a tuning override)
+    int cmax = kMaxFdParts;
+    if (const char *e = std::getenv("MAOS_B200_FD_CTAS")) {
+        const int v = std::atoi(e);
+        if (v >= 1 && v <= kMaxFdParts) cmax = v;
+    }
     std::vector<int> K(nps);
     int C = 0;
-    for (int l = 0; l < nps; l++) {
-        const FdLayer &F = fdtab.l[l];
-        K[l] = (int)std::max(1L, std::lround((double)F.nx * F.ny / (double)nmin));
-        K[l] = std::min(K[l], std::min(F.ny / 2, F.nx / 2 + 1));
-        C += K[l];
+    auto split = [&](double scale) {
+        int c = 0;
+        for (int l = 0; l < nps; l++) {
+            const FdLayer &F = fdtab.l[l];
+            K[l] = (int)std::max(1L, std::lround(scale * F.nx * F.ny / (double)nmin));
+            K[l] = std::min(K[l], std::min(F.ny / 2, F.nx / 2 + 1));
+            c += K[l];
+        }
+        return c;
+    };
+    double sbest = 1.0;
+    int cbest = split(1.0);
+    for (double sc = 1.05; sc <= 8.0; sc += 0.05) {
+        const int c = split(sc);
+        if (c <= cmax && c > cbest) {
+            cbest = c;
+            sbest = sc;
+        }
     }
-    while (C > kMaxFdParts) {  // take CTAs from the most split layer
+    C = split(sbest);
+    while (C > cmax) {  // take CTAs from the most split layer
         int lm = 0;
         for (int l = 1; l < nps; l++)
             if (K[l] > K[lm]) lm = l;
