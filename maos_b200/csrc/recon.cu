@@ -1812,11 +1812,12 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
 // admissible).  Returns the rows kept.
 int Recon::autotune(int reps, float *ms_out) {
     // 4, 8 and 16 rows (reported in ms_out), then every even split of the
-    // pupil rows into k blocks (ceil(nyp/k) rows, 4..32)
+    // pupil rows into k blocks (ceil(nyp/k) rows, 1..32: one 30 m instance
+    // runs fastest with 2)
     std::vector<int> cand = {4, 8, 16};
     for (int k = 1; k <= nyp; k++) {
         const int r = (nyp + k - 1) / k;
-        if (r >= 4 && r <= 32 && std::find(cand.begin(), cand.end(), r) == cand.end()) cand.push_back(r);
+        if (r >= 1 && r <= 32 && std::find(cand.begin(), cand.end(), r) == cand.end()) cand.push_back(r);
     }
     set_mask(nullptr, stream);
     cudaEvent_t e0, e1;

@@ -209,7 +209,7 @@ def test_autotune_keeps_results():
         rows, ms = R.autotune(reps=3)
         nyp = s.pmap.nx
         splits = {-(-nyp // k) for k in range(1, nyp + 1)}
-        assert rows in ms or (4 <= rows <= 32 and rows in splits)  # 4/8/16 or an even split
+        assert rows in ms or (1 <= rows <= 32 and rows in splits)  # 4/8/16 or an even split
         if rows in ms:
             assert ms[rows] == min(ms.values())
         # the blocking changes no bit; the preconditioner's form (which the
