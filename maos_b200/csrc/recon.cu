@@ -116,6 +116,7 @@ struct Recon {
     int maxit = 0, precond = 0, split = 1;
     int nsc = 0;            // scalars per instance
     int nblk_x = 0;         // blocks over nxtot
+    int hxt_threads = kThreads, nblk_hxt = 0;  // k_hxt_rows's CTA size (autotuned) and CTAs per instance
     int nblk_tt = 0;        // blocks over the largest nsa
     std::vector<long> xoff, goff;
     std::vector<int> nsa;
@@ -576,8 +577,8 @@ static HxtGroupKern hxt_group_kern(int ky, int ni) {
 void Recon::hxt_rows(const float *xin, float *out, double *dot_part, int do_l2, int k, cudaStream_t s) {
     const int ni = hxt_ni();
     const HxtArgs a = hxt_args(xin, out, dot_part, do_l2, k);
-    launch(hxt_kern(ky, ni), dim3(nblk_x, (nb + ni - 1) / ni), dim3(kThreads), 0, s, a.t, a.xin, a.out, a.dot_part,
-           a.pi, a.lt, a.nps, a.nwfs, a.nyp, a.nxtot, a.tw, a.do_l2, a.S, a.kit, a.nb, a.act);
+    launch(hxt_kern(ky, ni), dim3(nblk_hxt, (nb + ni - 1) / ni), dim3(hxt_threads), 0, s, a.t, a.xin, a.out,
+           a.dot_part, a.pi, a.lt, a.nps, a.nwfs, a.nyp, a.nxtot, a.tw, a.do_l2, a.S, a.kit, a.nb, a.act);
 }
 
 void Recon::build_wfs_tables(const mb_recon_desc *d) {
@@ -1243,6 +1244,7 @@ void Recon::build(const mb_recon_desc *d) {
     build_pad();
     build_wfs_tables(d);
     nblk_x = (int)nblocks(nxtot);
+    nblk_hxt = nblk_x;
     nblk_tt = (int)nblocks(nsamax);
     nsc = maxit + 3;
     const size_t NX = (size_t)nb * nxtot;
@@ -1252,7 +1254,7 @@ void Recon::build(const mb_recon_desc *d) {
     grad.alloc((size_t)nb * ngrad);
     gin.alloc((size_t)nb * ngrad);
     tt_part.alloc((size_t)nb * nwfs * nblk_tt * 2);
-    pap_part.alloc((size_t)nb * nblk_x);
+    pap_part.alloc((size_t)nb * nblocks(nxtot, 64));  // room for k_hxt_rows CTAs down to 64 threads
     rr_part.alloc((size_t)nb * nblk_x);
     rz_part.alloc((size_t)nb * nblk_x);
     bb_part.alloc((size_t)nb * nblk_x);
@@ -1844,6 +1846,29 @@ int Recon::autotune(int reps, float *ms_out) {
         }
     }
     set_pupil_rows(best);
+    // k_hxt_rows's CTA size: 256, 128 or 64 threads (smaller CTAs spread a
+    // small batch over more SMs)
+    {
+        int bt = hxt_threads;
+        float tb = 1e30f;
+        for (int th : {256, 128, 64}) {
+            hxt_threads = th;
+            nblk_hxt = (int)nblocks(nxtot, th);
+            op_lhs(p.p, Ap.p, nullptr, stream);  // warm
+            MB_CUDA_TRY(cudaEventRecord(e0, stream));
+            for (int i = 0; i < reps; i++) op_lhs(p.p, Ap.p, nullptr, stream);
+            MB_CUDA_TRY(cudaEventRecord(e1, stream));
+            MB_CUDA_TRY(cudaEventSynchronize(e1));
+            float t = 0;
+            MB_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+            if (t < tb) {
+                tb = t;
+                bt = th;
+            }
+        }
+        hxt_threads = bt;
+        nblk_hxt = (int)nblocks(nxtot, bt);
+    }
     capture_graph();
     // the preconditioner's form: three kernels, or one fused cluster kernel,
     // timed as whole tomography steps (graph launches)
