@@ -311,7 +311,8 @@ int mb_recon_serve_step(mb_recon *r, const int *active, const float *grad, float
 /* Autotuner (no counterpart in the reference): times the tomography
  * operator with each admissible row blocking of its pupil-grid kernel (4, 8,
  * 16 pupil rows per CTA, and every even split of the pupil rows into blocks
- * of 1 to 32 rows) on this batch size, keeps the fastest, then times whole
+ * of 1 to 32 rows) and the y-half kernel's CTA size (256, 128 or 64 threads)
+ * on this batch size, keeps the fastest, then times whole
  * tomography steps with each form of the FDPCG preconditioner
  * (mb_fdpcg_mode; the three-kernel form at each batch shape of
  * mb_fdpcg_shape) and keeps the fastest, and captures the step graphs again;

@@ -987,10 +987,12 @@ void Recon::build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector
         K[lm]--;
         C--;
     }
+    for (int l = 0; l < nps; l++)
+        if (fdtab.l[l].nx > kFusedThreads) return;  // a row per thread: the three-kernel form only
     FdFusedTab T{};
     T.C = C;
     int maxnx = 0, maxny = 0;
-    long nR = kFftThreads, nS = 0, nSR = 0, nSC = 0;
+    long nR = kFusedThreads, nS = 0, nSR = 0, nSC = 0;
     int rank = 0;
     std::vector<int> rbase(nps);
     for (int l = 0; l < nps; l++) {
@@ -1062,7 +1064,7 @@ void Recon::build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector
     at[0].val.clusterDim.z = 1;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(C, nb);
-    cfg.blockDim = dim3(kFftThreads);
+    cfg.blockDim = dim3(kFusedThreads);
     cfg.dynamicSmemBytes = fd_fsmem;
     cfg.attrs = at;
     cfg.numAttrs = 1;
@@ -1335,7 +1337,7 @@ bool Recon::op_fdpcg(float *rin, float *zout, double *rzp, cudaStream_t s, int k
     // fdpcg_precond (maos/fdpcg.c:661): FFT -> permute -> block solve -> permute back -> IFFT,
     // on the half spectrum as in cuda/fdpcg.cu (fdpcg_mul_block_sync_half)
     if (in_cg && pnext && fd_mode == 2) {  // one launch: layers split over an instance's cluster
-        launch_cluster(k_fd_fused, dim3(fused_tab.C, nb), dim3(kFftThreads), fd_fsmem, s, fused_tab.C, rin, fdtab,
+        launch_cluster(k_fd_fused, dim3(fused_tab.C, nb), dim3(kFusedThreads), fd_fsmem, s, fused_tab.C, rin, fdtab,
                        fused_tab, fd_tw.p, fd_M.p, fd_mem.p, fd_bs, nxtot, xupd, Apupd, scal(), k, init, act(),
                        pnext);
         return true;
@@ -1779,7 +1781,7 @@ void Recon::time_stages(int reps, float *ms, double *bytes, int *launches) {
                     break;
                 case 5: fd_mul(stream); break;
                 case 7:  // fused: scratch vectors (rhs as r, z as x, Ap, rhs as p)
-                    launch_cluster(k_fd_fused, dim3(fused_tab.C, nb), dim3(kFftThreads), fd_fsmem, stream,
+                    launch_cluster(k_fd_fused, dim3(fused_tab.C, nb), dim3(kFusedThreads), fd_fsmem, stream,
                                    fused_tab.C, rhs.p, fdtab, fused_tab, fd_tw.p, fd_M.p, fd_mem.p, fd_bs, nxtot,
                                    z.p, Ap.p, scal(), 0, 0, act(), z.p);
                     break;

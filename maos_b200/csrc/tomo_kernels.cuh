@@ -1307,6 +1307,9 @@ __device__ cplx *fft_dir(int pair, cplx *a, cplx *b, int n, int count, int ld, c
 static_assert(kNumFftPairs == 17, "fft_dir lists one case per factor pair");
 
 constexpr int kFftThreads = 512;  // threads of a layer-FFT CTA
+// threads of a k_fd_fused CTA (one 30 m instance's step: 1.09-1.12 ms with
+// 512, 1.16-1.17 with 256, 1.37 with 1024, which spills)
+constexpr int kFusedThreads = 512;
 
 // Forward: r (instance-major) -> half spectra H.  grid: (nps, nb), block:
 // kFftThreads; dynamic shared memory: two buffers of `bufn` complex values,
@@ -1936,9 +1939,9 @@ __device__ void fft_dir_inplace(int pair, cplx *a, cplx *b, int n, int count, in
     }
 }
 
-// grid: (C, nb), clusters of C CTAs along x; block: kFftThreads (one CTA
+// grid: (C, nb), clusters of C CTAs along x; block: kFusedThreads (one CTA
 // per SM: the registers carry r, p and a block row between phases).
-__global__ void __launch_bounds__(kFftThreads, 1)
+__global__ void __launch_bounds__(kFusedThreads, 1)
 k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid_constant__ FdFusedTab fu,
            const cplx *__restrict__ tw, const cplx *__restrict__ M, const FdMem *__restrict__ mem, int bs,
            long nxtot, float *__restrict__ xw, const float *__restrict__ Apv, CgScal SC, int kit, int init,
