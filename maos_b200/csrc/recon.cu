@@ -458,11 +458,11 @@ void Recon::build_pad(int min_kx, int min_ky) {
             for (int axis = 0; axis < 2; axis++) {
                 const int tb = hx.h_ptr[(w * nps + l) * 2 + axis];
                 const int n = axis ? lay_h[l].ny : lay_h[l].nx;
-                for (int j = 0; j < n; j++) {
-                    GatherW *d = axis ? yp.data() + ((size_t)(w * nps + l) * maxny + j) * ky
-                                      : xp.data() + ((size_t)w * ncols + lay_h[l].tcol + j) * kx;
-                    for (int a = hx.h_idxptr[tb + j], k = 0; a < hx.h_idxptr[tb + j + 1]; a++, k++) d[k] = hx.h_ent[a];
-                }
+                for (int j = 0; j < n; j++)
+                    for (int a = hx.h_idxptr[tb + j], k = 0; a < hx.h_idxptr[tb + j + 1]; a++, k++) {
+                        if (axis) yp[((size_t)(w * nps + l) * maxny + j) * ky + k] = hx.h_ent[a];
+                        else xp[((size_t)w * kx + k) * ncols + lay_h[l].tcol + j] = hx.h_ent[a];  // entry-major
+                    }
             }
     xpad.upload(xp);
     ypad.upload(yp);

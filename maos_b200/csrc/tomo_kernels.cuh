@@ -392,7 +392,7 @@ __device__ __forceinline__ void cp_async_words(void *dst, const void *src, int n
 }
 
 struct PadIndex {
-    const GatherW *x;   // [(w*ncols + tcol_l + jx)*kx + e]   (per WFS, all layers' columns)
+    const GatherW *x;   // [(w*kx + e)*ncols + tcol_l + jx]   (per WFS, entry-major over all layers' columns)
     const GatherW *y;   // [((w*nps + l)*maxny + jy)*ky + e]
     const int4 *fp;     // [w*nps + l]: footprint of the WFS on the layer: columns [x, y), rows [z, w)
     int kx, ky, maxnx, maxny;
@@ -606,7 +606,7 @@ pupil_rows_body(const uint3 bid, const float *__restrict__ x, const float *__res
             if (c - tc < f.x || c - tc >= f.y) continue;  // no pupil column reaches it: never read
             GatherW e[kMaxPadX];
 #pragma unroll
-            for (int k = 0; k < kMaxPadX; k++) e[k] = k < kx ? s_xp[c * kx + k] : GatherW{0, 0.f};
+            for (int k = 0; k < kMaxPadX; k++) e[k] = k < kx ? s_xp[k * ncols + c] : GatherW{0, 0.f};  // no bank conflicts
             float *dst = tb + (size_t)nyp * tc + (size_t)r0 * lnx + (c - tc);
             for (int r = 0; r < nr; r++) {
                 const float *o = s_opd2 + r * nxp;
