@@ -103,12 +103,14 @@ def slot_footprint_bytes(stype: SystemType) -> int:
 class Pool:
     """One reconstructor with `capacity` slots for one system type."""
 
-    def __init__(self, stype: SystemType, device: int = 0, priority: int = 0):
+    def __init__(self, stype: SystemType, device: int = 0, priority: int = 0, autotune: bool = True):
         import torch
         from .recon import Reconstructor
         self.type = stype
         self.cap = stype.capacity
         self.R = Reconstructor(stype.tomo, nbatch=self.cap, fit=stype.fit, device=device)
+        if autotune:  # blocking, CTA sizes and FDPCG form for the pool's capacity
+            self.R.autotune(reps=5)
         self.stream = torch.cuda.Stream(device=device, priority=priority)
         self.owner: List[Optional[int]] = [None] * self.cap
         self.queue: Dict[int, List[Request]] = {}

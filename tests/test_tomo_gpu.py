@@ -198,7 +198,10 @@ def test_integrated_tip_tilt_split0(name):
 
 
 def test_autotune_keeps_results():
-    """The autotuner only changes the pupil-row blocking: same solution bit for bit."""
+    """The autotuner changes blockings and launch shapes only: the pupil-row
+    blocking changes no bit; the y-half CTA size changes the order of the
+    FP64 p.Ap partial sums and the preconditioner's form changes FP32
+    rounding, so the solution agrees to FP32 rounding."""
     from conftest import get_system
     from maos_b200.recon import Reconstructor
     s = get_system("mcao_30m")
@@ -212,13 +215,11 @@ def test_autotune_keeps_results():
         assert rows in ms or (1 <= rows <= 32 and rows in splits)  # 4/8/16 or an even split
         if rows in ms:
             assert ms[rows] == min(ms.values())
-        # the blocking changes no bit; the preconditioner's form (which the
-        # autotuner also picks) only FP32 rounding: compare in the first form
         if s.fdpcg is not None:
             R.fdpcg_mode(1)
         R.reset()
         x1, _ = R.tomo(g)
-        assert np.array_equal(x0, x1)
+        assert rel(x1, x0) < SOLVE_TOL
     finally:
         R.close()
 
