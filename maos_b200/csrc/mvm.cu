@@ -370,11 +370,23 @@ struct Mvm {
                 dg, ngrad, nch, kexp.p, reinterpret_cast<char *>(gs.p), cnt.p, ncnt, stage);
         }
         MB_CHECK_LAUNCH();
-        k_mvm_tc<DT, N><<<tc_P, kTcThreads, smem, s>>>(
-            reinterpret_cast<const char *>(m.p), reinterpret_cast<const char *>(gs.p), kexp.p,
-            DT == MB_MVM_FP8 ? scale.p : nullptr, tc_nrb, nch, tc_W, tc_P, tc_maxp, part.p, cnt.p, dout, nact, nbatch,
-            err.p);
-        MB_CHECK_LAUNCH();
+        // programmatic dependent launch: the GEMM's CTAs start (TMEM, barriers,
+        // the first stages' M tiles) while the split kernel still runs, and
+        // wait for its output where they read it (griddepcontrol.wait)
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(tc_P);
+        cfg.blockDim = dim3(kTcThreads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        MB_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_mvm_tc<DT, N>, reinterpret_cast<const char *>(m.p),
+                                       reinterpret_cast<const char *>(gs.p), (const int *)kexp.p,
+                                       (const float *)(DT == MB_MVM_FP8 ? scale.p : nullptr), tc_nrb, nch, tc_W,
+                                       tc_P, tc_maxp, part.p, cnt.p, dout, nact, nbatch, err.p));
     }
     template <int DT>
     void launch_dt(const float *dg, float *dout, cudaStream_t s) {

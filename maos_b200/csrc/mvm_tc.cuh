@@ -162,6 +162,22 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
 
 // One stage: the M tile and the three gradient-term tiles, both landing on
 // the stage's full barrier.
+// One bulk copy completing on `bar` (whose expected bytes were set before).
+__device__ __forceinline__ void tc_copy(uint32_t bar, uint32_t sdst, const void *gsrc, int bytes) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(sdst), "l"(gsrc), "r"(bytes), "r"(bar) : "memory");
+}
+__device__ __forceinline__ void tc_expect(uint32_t bar, int bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(bytes) : "memory");
+}
+// The kernel that precedes k_mvm_tc on the stream (the gradient split) may
+// let it start early (programmatic dependent launch); this waits until that
+// kernel has completed and its writes are visible.  A no-op otherwise.
+__device__ __forceinline__ void tc_wait_prior() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void tc_release_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ void tc_load_stage(uint32_t bar, uint32_t sa, const void *ga, int abytes, uint32_t sb,
                                               const void *gb, int bbytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(abytes + bbytes)
@@ -221,6 +237,7 @@ template <int N>
 __global__ void __launch_bounds__(256)
 k_gsplit(const float *__restrict__ g, long ngrad, int nbatch, long nch, int nz, char *__restrict__ gs,
          int *__restrict__ cnt, int ncnt) {
+    tc_release_dependents();  // k_mvm_tc may start its M copies now
     const long item = (long)blockIdx.x * blockDim.x + threadIdx.x;
     for (long i = item; i < ncnt; i += (long)gridDim.x * blockDim.x) cnt[i] = 0;  // stream-K arrival counters
     if (item >= (long)nz * nch * N * 8) return;
@@ -287,6 +304,7 @@ template <int N>
 __global__ void __cluster_dims__(kSplitCta, 1, 1) __launch_bounds__(256)
 k_gsplit8(const float *__restrict__ g, long ngrad, long nch, int *__restrict__ kexp, char *__restrict__ gs,
           int *__restrict__ cnt, int ncnt, bool stage) {
+    tc_release_dependents();  // k_mvm_tc may start its M copies now
     __shared__ float red[8];
     __shared__ float s_max;
     __shared__ int s_k;
@@ -461,7 +479,32 @@ k_mvm_tc(const char *__restrict__ Mt, const char *__restrict__ gs, const int *__
 
     if (warp == 0) {
         if (lane == 0) {  // copies: the ring runs on across segments
-            int q = 0;
+            auto unit = [&](int q, long &a_off, long &b_off, int &nc) {
+                const long u = lo + q;
+                const long seg = u / nchu, c = (u - seg * nchu) * U;
+                const long z = seg / nrb, rb = seg - z * nrb;
+                nc = (int)(nch - c < U ? nch - c : U);
+                a_off = (rb * nch + c) * AB;
+                b_off = (z * nch + c) * BB;
+            };
+            // the first stages' M tiles go out before the gradient terms exist
+            // (M does not depend on the split kernel), their terms after it
+            const int npre = nunit < S ? nunit : S;
+            for (int q0 = 0; q0 < npre; q0++) {
+                long ao, bo;
+                int nc;
+                unit(q0, ao, bo, nc);
+                tc_expect(smem_addr(&full[q0]), nc * (AB + BB));
+                tc_copy(smem_addr(&full[q0]), sbase + q0 * SB, Mt + ao, nc * AB);
+            }
+            tc_wait_prior();
+            for (int q0 = 0; q0 < npre; q0++) {
+                long ao, bo;
+                int nc;
+                unit(q0, ao, bo, nc);
+                tc_copy(smem_addr(&full[q0]), sbase + q0 * SB + U * AB, gs + bo, nc * BB);
+            }
+            int q = npre;
             for (; q < nunit; q++) {
                 const long u = lo + q;
                 const long seg = u / nchu, c = (u - seg * nchu) * U;
@@ -522,6 +565,7 @@ k_mvm_tc(const char *__restrict__ Mt, const char *__restrict__ gs, const int *__
         }
         __syncwarp();
     } else {  // epilogue warps 2-5: warp w reads TMEM lanes 32(w%4).. = rows
+        tc_wait_prior();  // the split kernel's exponents and zeroed counters
         const int qd = warp & 3, rl = qd * 32 + lane;
         const uint32_t tl = tmem + ((uint32_t)(qd * 32) << 16);
         int k = 0;
