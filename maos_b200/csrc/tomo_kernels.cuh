@@ -2012,27 +2012,24 @@ k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid
     }
     __syncthreads();
     fft_dir_inplace<true>(L.px, R, S, nx, npr, nx, L.rx, L.nrx, twx, false);
-    {
+    {  // unpack into half-spectrum rows, each bin stored straight into its
+       // column owner's SC (distributed shared memory: stores, no round trip)
         const int hs_ = blockDim.x / h, h0 = threadIdx.x / h, k = threadIdx.x - h0 * h;
+        int q = P.K - 1;  // the column owner of bin k
+        while (fu.c[P.rbase + q].c0 > k) q--;
+        const FdPart O = fu.c[P.rbase + q];
+        const int on = O.c1 - O.c0;
+        const unsigned oa = dsm_base(SCb, (unsigned)(P.rbase + q)) + 8u * (unsigned)(k - O.c0);
         for (int p = h0; h0 < hs_ && p < npr; p += hs_) {
             const cplx zk = R[p * nx + k], zm = cconj(R[p * nx + (k == 0 ? 0 : nx - k)]);
-            SR[(2 * p) * h + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
             const cplx d = csub(zk, zm);
-            SR[(2 * p + 1) * h + k] = make_float2(0.5f * d.y, -0.5f * d.x);  // -i/2 (zk - conj(z_-k))
+            const int i = 2 * (P.p0 + p);  // the layer row of the first of the pair
+            dsm_st(oa + 8u * (unsigned)(i * on), make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y)));
+            dsm_st(oa + 8u * (unsigned)((i + 1) * on), make_float2(0.5f * d.y, -0.5f * d.x));  // -i/2 (zk - conj(z_-k))
         }
     }
-    cluster_sync_all();  // B1: every CTA's half-spectrum rows are in its SR
-    // ---- F2: this CTA's columns from the row owners, column FFTs
-    for (int it = threadIdx.x; it < ny * ncl; it += blockDim.x) {
-        const int i = it / ncl, c = it - i * ncl;  // row i, local column c
-        const int pr = i >> 1;
-        int q = P.K - 1;
-        while (fu.c[P.rbase + q].p0 > pr) q--;
-        const FdPart O = fu.c[P.rbase + q];
-        const unsigned ra = dsm_base(SR, (unsigned)(P.rbase + q));
-        SCb[i * ncl + c] = dsm_ld(ra + 8u * (unsigned)((i - 2 * O.p0) * h + P.c0 + c));
-    }
-    __syncthreads();
+    cluster_sync_all();  // B1: every CTA's columns are complete in its SC
+    // ---- F2: column FFTs of this CTA's columns
     fft_dir_inplace<false>(L.py, SCb, S, ny, ncl, ncl, L.ry, L.nry, twy, false);
     cluster_sync_all();  // B2: spectra final in every SC; no SR is read any more
     // ---- M: this CTA's frequency blocks: a thread gathers one member of a
@@ -2074,33 +2071,30 @@ k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid
         }
     }
     cluster_sync_all();  // B3: every stored bin of every SY written; no SC is read any more
-    // ---- I1: inverse column FFTs
+    // ---- I1: inverse column FFTs, then each column's row pairs stored straight
+    // into the row owners' R as a + i c (and, mirrored, at nx - k)
     fft_dir_inplace<false>(L.py, SY, S, ny, ncl, ncl, L.ry, L.nry, twy, true);
-    cluster_sync_all();  // B4: inverse columns final in every SY
-    // ---- I2: this CTA's row pairs from the column owners, inverse row FFTs
-    for (int it = threadIdx.x; it < npr * nx; it += blockDim.x) {
-        const int pl = it / nx, k = it - pl * nx;
-        const int p = P.p0 + pl;
-        const bool hi = k > nx / 2;
-        const int kk = hi ? nx - k : k;
-        int q = P.K - 1;
-        while (fu.c[P.rbase + q].c0 > kk) q--;
-        const FdPart O = fu.c[P.rbase + q];
-        const int on = O.c1 - O.c0;
-        const unsigned ra = dsm_base(SY, (unsigned)(P.rbase + q)) + 8u * (unsigned)(kk - O.c0);
-        cplx a = dsm_ld(ra + 8u * (unsigned)((2 * p) * on));
-        cplx c = dsm_ld(ra + 8u * (unsigned)((2 * p + 1) * on));
+    for (int it = threadIdx.x; it < (ny / 2) * ncl; it += blockDim.x) {
+        const int p = it / ncl, cl = it - p * ncl;  // layer row pair p, local column cl
+        const int kk = P.c0 + cl;
+        cplx a = SY[(2 * p) * ncl + cl], c = SY[(2 * p + 1) * ncl + cl];
         if (kk == 0 || kk == nx / 2) {
             a.y = 0.f;
             c.y = 0.f;
         }
-        if (hi) {
+        int q = P.K - 1;  // the row owner of pair p
+        while (fu.c[P.rbase + q].p0 > p) q--;
+        const unsigned ra = dsm_base(R, (unsigned)(P.rbase + q)) +
+                            8u * (unsigned)((p - fu.c[P.rbase + q].p0) * nx);
+        dsm_st(ra + 8u * (unsigned)kk, make_float2(a.x - c.y, a.y + c.x));  // a + i c
+        if (kk > 0 && kk < nx / 2) {
             a = cconj(a);
             c = cconj(c);
+            dsm_st(ra + 8u * (unsigned)(nx - kk), make_float2(a.x - c.y, a.y + c.x));
         }
-        R[pl * nx + k] = make_float2(a.x - c.y, a.y + c.x);  // a + i c
     }
-    __syncthreads();
+    cluster_sync_all();  // B4: every CTA's row pairs are complete in its R
+    // ---- I2: inverse row FFTs
     fft_dir_inplace<true>(L.px, R, S, nx, npr, nx, L.rx, L.nrx, twx, true);
     double v = 0;
     if (x0 < xs)
