@@ -992,7 +992,7 @@ void Recon::build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector
     FdFusedTab T{};
     T.C = C;
     int maxnx = 0, maxny = 0;
-    long nR = kFusedThreads, nS = 0, nSR = 0, nSC = 0;
+    long nR = kFusedThreads, nS = 0, nSC = 0;
     int rank = 0;
     std::vector<int> rbase(nps);
     for (int l = 0; l < nps; l++) {
@@ -1018,7 +1018,6 @@ void Recon::build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector
             nR = std::max(nR, (long)npr * F.nx);
             nS = std::max(nS, (long)(F.px >= 0 ? fft2_scratch(F.px, true, npr) : npr * F.nx));
             nS = std::max(nS, (long)(F.py >= 0 ? fft2_scratch(F.py, false, ncl) : (long)F.ny * ncl));
-            nSR = std::max(nSR, 2L * npr * h);
             nSC = std::max(nSC, (long)F.ny * ncl);
         }
     }
@@ -1027,8 +1026,7 @@ void Recon::build_fdpcg_fused(const std::vector<FdIndex> &idx, const std::vector
     T.oTY = maxnx;
     T.oR = maxnx + maxny;
     T.oS = (int)(T.oR + nR);
-    T.oSR = (int)(T.oS + nS);
-    T.oSC = (int)(T.oSR + nSR);
+    T.oSC = (int)(T.oS + nS);
     T.oSY = (int)(T.oSC + nSC);
     fd_fsmem = (size_t)(T.oSY + nSC) * sizeof(cplx);
     if (fd_fsmem > 200 * 1024) return;  // else the three-kernel form

@@ -1876,13 +1876,15 @@ k_fd_inv(const cplx *__restrict__ H, const float *__restrict__ r, float *__restr
 // layer.  Phases, separated by cluster barriers, with the data exchanged
 // through distributed shared memory (ld/st.shared::cluster):
 //   F1  x += a p, r -= a Ap on its row pairs (the CG update, when ab is set),
-//       row FFTs of r, unpacking into the half-spectrum rows (SR);
-//   F2  its columns gathered from the row owners' SR, column FFTs (SC);
+//       row FFTs of r, unpacking into half-spectrum rows stored straight into
+//       the column owners' SC (stores into the receiver's shared memory before
+//       the barrier: no remote load waits on a round trip);
+//   F2  column FFTs (SC);
 //   M   its share of the frequency blocks: members gathered from the column
 //       owners' SC, Y = Mbinv X, each stored bin written into its owner's SY;
-//   I1  inverse column FFTs of SY;
-//   I2  its row pairs gathered from the column owners' SY (Hermitian mirror),
-//       inverse row FFTs, then r.z over the cluster, beta and p = z + beta p.
+//   I1  inverse column FFTs of SY, row pairs stored straight into the row
+//       owners' R (Hermitian mirror);
+//   I2  inverse row FFTs, then r.z over the cluster, beta and p = z + beta p.
 // Every shared-memory region sits at the same offset in every CTA of the
 // kernel, so a peer's copy is the local address mapped to the peer's rank.
 // ---------------------------------------------------------------------------
@@ -1896,7 +1898,7 @@ struct FdPart {
 struct FdFusedTab {
     FdPart c[kMaxFdParts];
     int C;                 // CTAs per instance (cluster size)
-    int oTY, oR, oS, oSR, oSC, oSY;  // shared-memory offsets (complex elements); twiddles x at 0
+    int oTY, oR, oS, oSC, oSY;  // shared-memory offsets (complex elements); twiddles x at 0
 };
 // One member of a solved block: the cluster rank that owns its bin, the bin's
 // offset in that CTA's SC / SY, and the conjugate / store flags of FdIndex.
@@ -1957,7 +1959,7 @@ k_fd_fused(float *__restrict__ r, const __grid_constant__ FdTab ft, const __grid
     const int nx = L.nx, ny = L.ny, h = nx / 2 + 1;
     const int npr = P.p1 - P.p0, ncl = P.c1 - P.c0;
     cplx *twx = fsm, *twy = fsm + fu.oTY, *R = fsm + fu.oR, *S = fsm + fu.oS;
-    cplx *SR = fsm + fu.oSR, *SCb = fsm + fu.oSC, *SY = fsm + fu.oSY;
+    cplx *SCb = fsm + fu.oSC, *SY = fsm + fu.oSY;
     for (int i = threadIdx.x; i < nx; i += blockDim.x) twx[i] = tw[L.twx + i];
     for (int i = threadIdx.x; i < ny; i += blockDim.x) twy[i] = tw[L.twy + i];
     const size_t base = (size_t)b * nxtot + L.off;
