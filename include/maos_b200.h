@@ -315,7 +315,9 @@ int mb_recon_serve_step(mb_recon *r, const int *active, const float *grad, float
  * on this batch size, keeps the fastest, then times whole
  * tomography steps with each form of the FDPCG preconditioner
  * (mb_fdpcg_mode; the three-kernel form at each batch shape of
- * mb_fdpcg_shape) and keeps the fastest, and captures the step graphs again;
+ * mb_fdpcg_shape) and keeps the fastest, then whole steps with and without
+ * programmatic dependent launch between the graph's kernels (faster for one
+ * instance, slower for a few), and captures the step graphs again;
  * the instances restart cold.  The row blocking does not change results, the
  * preconditioner's form changes them only at FP32 rounding.  rows (may be
  * NULL): the blocking kept; ms (may be NULL, 3 floats): ms per operator for

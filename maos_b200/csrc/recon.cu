@@ -43,15 +43,22 @@ void count_launches(long n) { g_launches += n; }
 static inline unsigned nblocks(long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
 constexpr int kCgRestart = 100;  // lib/pcg.c:61
 
-// Every kernel of the reconstructor is launched through here.  With
-// MAOS_B200_PDL=1 the launches carry programmatic stream serialisation (the
-// kernels open with pdl_enter), so a kernel's launch and CTA ramp overlap
-// the tail of its predecessor: that shortens stream-launched sequences by
-// 1-2 us per kernel on B200, but measured no gain for the captured step
-// graph, which is the product path, so it is off by default.
+// Every kernel of the reconstructor is launched through here.  While a
+// reconstructor that the autotuner set to it captures its graphs (PdlScope),
+// or with MAOS_B200_PDL=1, the launches carry programmatic stream
+// serialisation (the kernels open with pdl_enter), so a kernel's launch and
+// CTA ramp overlap the tail of its predecessor: one 30 m instance's step
+// 1.04 against 1.09 ms, but 1.48 against 1.40 ms at 4 instances, hence a
+// per-reconstructor choice.  Cluster launches go without it.
+static thread_local bool g_pdl_on = false;
+struct PdlScope {
+    bool old;
+    explicit PdlScope(bool on) : old(g_pdl_on) { g_pdl_on = on; }
+    ~PdlScope() { g_pdl_on = old; }
+};
 static bool pdl_enabled() {
-    static const bool on = std::getenv("MAOS_B200_PDL") != nullptr;
-    return on;
+    static const bool env = std::getenv("MAOS_B200_PDL") != nullptr;
+    return g_pdl_on || env;
 }
 
 template <typename... KArgs, typename... Args>
@@ -237,6 +244,7 @@ struct Recon {
     cudaGraphExec_t graph_step = nullptr;  // tomography + fit
     long graph_kernels = 0, graph_fit_kernels = 0, graph_step_kernels = 0;
     long graph_version = 0;  // counts recaptures (a ReconGroup recaptures after a member did)
+    bool pdl = false;        // the step graphs' launches overlap their predecessors' tails (autotuned)
 
     ~Recon() {
         if (hstage) cudaFreeHost(hstage);
@@ -1905,6 +1913,27 @@ int Recon::autotune(int reps, float *ms_out) {
             if (time_graph() < tb) best_mode = 2;
         }
         set_fdpcg_mode(best_mode);
+    }
+    // launches with or without programmatic dependent launch, timed as whole
+    // steps (graph launches)
+    {
+        float tp[2] = {0, 0};
+        for (int on = 0; on < 2; on++) {
+            pdl = on != 0;
+            capture_graph();
+            cudaGraphExec_t g = has_fit ? graph_step : graph;
+            MB_CUDA_TRY(cudaGraphLaunch(g, stream));  // warm
+            MB_CUDA_TRY(cudaEventRecord(e0, stream));
+            const int nrep = std::max(2, reps / 4);
+            for (int i = 0; i < nrep; i++) MB_CUDA_TRY(cudaGraphLaunch(g, stream));
+            MB_CUDA_TRY(cudaEventRecord(e1, stream));
+            MB_CUDA_TRY(cudaEventSynchronize(e1));
+            MB_CUDA_TRY(cudaEventElapsedTime(&tp[on], e0, e1));
+        }
+        pdl = tp[1] < tp[0];
+        capture_graph();
+    }
+    {
         // the timing steps moved the warm start: start the instances cold again
         x.zero_async(stream);
         if (has_fit) fa.zero_async(stream);
@@ -1958,6 +1987,7 @@ void Recon::capture(const std::function<void(cudaStream_t)> &body, long &nkernel
 
 void Recon::capture_graph() {
     graph_version++;
+    PdlScope ps(pdl);
     capture([&](cudaStream_t s) { enqueue_solve(s); }, graph_kernels, graph);
     if (has_fit) {
         capture([&](cudaStream_t s) { enqueue_fit(s); }, graph_fit_kernels, graph_fit);
