@@ -44,22 +44,24 @@ static inline unsigned nblocks(long n, int t = kThreads) { return (unsigned)((n 
 constexpr int kCgRestart = 100;  // lib/pcg.c:61
 
 // Every kernel of the reconstructor is launched through here.  While a
-// reconstructor that the autotuner set to it captures its graphs (PdlScope),
-// or with MAOS_B200_PDL=1, the launches carry programmatic stream
+// reconstructor captures its graphs (PdlScope) with the mode the autotuner
+// chose, or with MAOS_B200_PDL=1, the launches carry programmatic stream
 // serialisation (the kernels open with pdl_enter), so a kernel's launch and
-// CTA ramp overlap the tail of its predecessor: one 30 m instance's step
-// 1.04 against 1.09 ms, but 1.48 against 1.40 ms at 4 instances, hence a
-// per-reconstructor choice.  Cluster launches go without it.
-static thread_local bool g_pdl_on = false;
+// CTA ramp overlap the tail of its predecessor.  Mode 0: none; 1: the plain
+// launches; 2: the cluster launches too.  Measured on the 30 m system: one
+// instance 1.02 ms with mode 1, 1.06 with 2, 1.09 with 0; four instances
+// best with 0; 32 instances 3.49 ms with 2 against 3.56.
+static thread_local int g_pdl_mode = 0;
 struct PdlScope {
-    bool old;
-    explicit PdlScope(bool on) : old(g_pdl_on) { g_pdl_on = on; }
-    ~PdlScope() { g_pdl_on = old; }
+    int old;
+    explicit PdlScope(int mode) : old(g_pdl_mode) { g_pdl_mode = mode; }
+    ~PdlScope() { g_pdl_mode = old; }
 };
 static bool pdl_enabled() {
     static const bool env = std::getenv("MAOS_B200_PDL") != nullptr;
-    return g_pdl_on || env;
+    return g_pdl_mode >= 1 || env;
 }
+static bool pdl_cluster_enabled() { return g_pdl_mode >= 2; }
 
 template <typename... KArgs, typename... Args>
 static void launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args &&...args) {
@@ -81,22 +83,24 @@ static void launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, c
     count_launches(1);
 }
 
-// A launch in thread-block clusters of `cx` CTAs along x (no PDL).
+// A launch in thread-block clusters of `cx` CTAs along x.
 template <typename... KArgs, typename... Args>
 static void launch_cluster(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, int cx,
                            Args &&...args) {
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = (unsigned)cx;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = pdl_cluster_enabled() ? 1 : 0;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
     if (e != cudaSuccess) {
         set_error("cluster launch: %s", cudaGetErrorString(e));
@@ -244,7 +248,7 @@ struct Recon {
     cudaGraphExec_t graph_step = nullptr;  // tomography + fit
     long graph_kernels = 0, graph_fit_kernels = 0, graph_step_kernels = 0;
     long graph_version = 0;  // counts recaptures (a ReconGroup recaptures after a member did)
-    bool pdl = false;        // the step graphs' launches overlap their predecessors' tails (autotuned)
+    int pdl = 0;             // programmatic dependent launch in the step graphs (PdlScope mode, autotuned)
 
     ~Recon() {
         if (hstage) cudaFreeHost(hstage);
@@ -1917,9 +1921,9 @@ int Recon::autotune(int reps, float *ms_out) {
     // launches with or without programmatic dependent launch, timed as whole
     // steps (graph launches)
     {
-        float tp[2] = {0, 0};
-        for (int on = 0; on < 2; on++) {
-            pdl = on != 0;
+        float tp[3] = {0, 0, 0};
+        for (int on = 0; on < 3; on++) {
+            pdl = on;
             capture_graph();
             cudaGraphExec_t g = has_fit ? graph_step : graph;
             MB_CUDA_TRY(cudaGraphLaunch(g, stream));  // warm
@@ -1930,7 +1934,7 @@ int Recon::autotune(int reps, float *ms_out) {
             MB_CUDA_TRY(cudaEventSynchronize(e1));
             MB_CUDA_TRY(cudaEventElapsedTime(&tp[on], e0, e1));
         }
-        pdl = tp[1] < tp[0];
+        pdl = tp[1] < tp[0] ? (tp[2] < tp[1] ? 2 : 1) : (tp[2] < tp[0] ? 2 : 0);
         capture_graph();
     }
     {
